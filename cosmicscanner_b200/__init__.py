@@ -1,0 +1,243 @@
+"""cosmicscanner_b200 — B200 (sm_100a) matrix-free mixed-model path of CosmicScanner.
+
+Python mirror of the reference's C++ interfaces over the library's C ABI
+(``include/cosmicscanner_b200.h``):
+
+* :class:`Genotypes`        — ``PlinkReader`` (libCosmicCore/src/plink_reader.h)
+* :class:`KinshipOperator`  — ``KinshipOperator`` / ``createKinshipOperator``
+                              (src/kinship_operator.h:18-101)
+* :class:`LmmEngine`        — ``LmmEngine::prepareLowRankMatrixFree`` / ``scan``
+                              (src/lmm_engine.h:108-131)
+
+Every compute call runs the CUDA kernels in ``libcosmicscanner_b200.so``; there is
+no CPU fallback.  A missing library or CUDA device raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+
+PRECISION = {"fp64": 0, "mixed": 1}
+
+
+class CosmicError(RuntimeError):
+    """Raised when a library call returns a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class InvalidArgument(CosmicError, ValueError):
+    pass
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = _abi.lib().cs_last_error().decode()
+        if rc == _abi.CS_ERR_INVALID_ARGUMENT:
+            raise InvalidArgument(rc, msg)
+        raise CosmicError(rc, msg)
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _prec(p):
+    return PRECISION[p] if isinstance(p, str) else int(p)
+
+
+class Genotypes:
+    """Resident packed genotype matrix (+ per-SNP mean and 1/sd over all samples)."""
+
+    def __init__(self, handle, n_samples: int, n_snps: int):
+        self._h = handle
+        self.n_samples = n_samples
+        self.n_snps = n_snps
+
+    @classmethod
+    def from_bed_bytes(cls, bed: np.ndarray, n_samples: int, n_snps: int) -> "Genotypes":
+        bed = np.ascontiguousarray(bed, dtype=np.uint8)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_genotypes_create(_ptr(bed), bed.nbytes, n_samples, n_snps, C.byref(h)))
+        return cls(h, n_samples, n_snps)
+
+    @classmethod
+    def open_plink(cls, prefix: str) -> "Genotypes":
+        h = C.c_void_p()
+        _check(_abi.lib().cs_genotypes_open_plink(prefix.encode(), C.byref(h)))
+        n, m, bps = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(_abi.lib().cs_genotypes_info(h, C.byref(n), C.byref(m), C.byref(bps)))
+        return cls(h, n.value, m.value)
+
+    def stats(self):
+        m = self.n_snps
+        mean, inv_std, s = np.zeros(m), np.zeros(m), np.zeros(m)
+        count = np.zeros(m, dtype=np.int32)
+        _check(_abi.lib().cs_genotypes_stats(self._h, _ptr(mean), _ptr(inv_std), _ptr(count), _ptr(s)))
+        return {"mean": mean, "inv_std": inv_std, "count": count, "sum": s}
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_genotypes_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class KinshipOperator:
+    """K = Z Z^T / M over a sample / variant selection; mirrors cosmic::KinshipOperator."""
+
+    def __init__(self, genotypes: Genotypes, keep=None, variants=None):
+        self._g = genotypes  # keeps the matrix alive, like the reference's non-owning reader
+        self._keep = None if keep is None or len(keep) == 0 else np.ascontiguousarray(keep, dtype=np.int32)
+        self._var = None if variants is None or len(variants) == 0 else np.ascontiguousarray(variants, dtype=np.int32)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_kinship_create(
+            genotypes._h, _ptr(self._keep), 0 if self._keep is None else len(self._keep),
+            _ptr(self._var), 0 if self._var is None else len(self._var), C.byref(h)))
+        self._h = h
+        r, m = C.c_int64(), C.c_int64()
+        _check(_abi.lib().cs_kinship_info(h, C.byref(r), C.byref(m)))
+        self._rows, self._m = r.value, m.value
+
+    def rows(self) -> int:
+        return self._rows
+
+    def cols(self) -> int:
+        return self._rows
+
+    def numVariants(self) -> int:
+        return self._m
+
+    def isDense(self) -> bool:
+        return False
+
+    def apply(self, X, precision="fp64") -> np.ndarray:
+        """out = K X for a vector (rows,) or matrix (rows, k); host arrays."""
+        X = np.asarray(X, dtype=np.float64)
+        vec = X.ndim == 1
+        Xf = np.asfortranarray(X.reshape(-1, 1) if vec else X)
+        if Xf.shape[0] != self._rows:
+            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
+                                  "PlinkKinshipOperator::apply: dimension mismatch")
+        k = Xf.shape[1]
+        out = np.zeros((self._rows, k), order="F")
+        _check(_abi.lib().cs_kinship_apply_host(self._h, _ptr(Xf), self._rows, k, _ptr(out),
+                                                self._rows, _prec(precision)))
+        return out[:, 0] if vec else out
+
+    applyTranspose = apply
+
+    def apply_device(self, X_ptr: int, ldx: int, k: int, Y_ptr: int, ldy: int,
+                     precision="fp64", stream: int = 0):
+        """Device-pointer apply (column-major, leading dimensions in elements)."""
+        _check(_abi.lib().cs_kinship_apply(self._h, C.c_void_p(X_ptr), ldx, k, C.c_void_p(Y_ptr),
+                                           ldy, _prec(precision), C.c_void_p(stream)))
+
+    def trace(self) -> float:
+        t = C.c_double()
+        _check(_abi.lib().cs_kinship_trace(self._h, C.byref(t)))
+        return t.value
+
+    def getDiagonal(self) -> np.ndarray:
+        d = np.zeros(self._rows)
+        _check(_abi.lib().cs_kinship_diagonal(self._h, _ptr(d)))
+        return d
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_kinship_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def createKinshipOperator(reader: Genotypes, keep_indices=None, variant_indices=None):
+    return KinshipOperator(reader, keep_indices, variant_indices)
+
+
+class LowRankDiagnostics(C.Structure):
+    _fields_ = [
+        ("requested_rank", C.c_int32), ("effective_rank", C.c_int32),
+        ("sketch_size", C.c_int32), ("trace_threshold_met", C.c_int32),
+        ("residual_eigenvalue", C.c_double), ("relative_frobenius_error", C.c_double),
+        ("trace", C.c_double), ("trace_fraction", C.c_double),
+        ("sigma2_g", C.c_double), ("sigma2_e", C.c_double), ("delta", C.c_double),
+        ("log_eta", C.c_double), ("reml_objective", C.c_double), ("seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class LmmEngine:
+    """Low-rank matrix-free LMM: mirrors LmmEngine (src/lmm_engine.cpp:897-1361)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(_abi.lib().cs_lmm_create(C.byref(h)))
+        self._h = h
+        self.diagnostics = None
+
+    def prepareLowRankMatrixFree(self, y, X, kinship: KinshipOperator, rank=256, oversample=10,
+                                 seed=42, trace_threshold=0.95, min_rank=1, precision="fp64"):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        # the reference receives covariates as Eigen::MatrixXf and casts them to double
+        X = np.asfortranarray(np.asarray(X, dtype=np.float32).astype(np.float64))
+        d = LowRankDiagnostics()
+        _check(_abi.lib().cs_lmm_prepare_lowrank_matrix_free(
+            self._h, kinship._h, _ptr(y), _ptr(X), X.shape[1], rank, oversample, seed,
+            trace_threshold, min_rank, _prec(precision), C.byref(d)))
+        self.diagnostics = d.as_dict()
+        self._n = kinship.rows()
+        return self.diagnostics
+
+    def getSigma2g(self):
+        return self.diagnostics["sigma2_g"]
+
+    def getSigma2e(self):
+        return self.diagnostics["sigma2_e"]
+
+    def lowrank_basis(self):
+        r = self.diagnostics["effective_rank"]
+        U = np.zeros((self._n, r), order="F")
+        lam = np.zeros(r)
+        _check(_abi.lib().cs_lmm_lowrank_basis(self._h, _ptr(U), self._n, _ptr(lam)))
+        return U, lam
+
+    def scan(self, reader: Genotypes, keep_indices, min_maf=0.01, precision="fp64"):
+        keep = np.ascontiguousarray(keep_indices, dtype=np.int32)
+        m = reader.n_snps
+        out = {k: np.zeros(m) for k in ("beta", "se", "p", "log10p", "freq")}
+        tested = np.zeros(m, dtype=np.int32)
+        _check(_abi.lib().cs_lmm_scan(self._h, reader._h, _ptr(keep), len(keep), min_maf,
+                                      _prec(precision), _ptr(out["beta"]), _ptr(out["se"]),
+                                      _ptr(out["p"]), _ptr(out["log10p"]), _ptr(out["freq"]),
+                                      _ptr(tested)))
+        out["tested"] = tested.astype(bool)
+        return out
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_lmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,77 @@
+"""ctypes declarations of the C ABI in include/cosmicscanner_b200.h."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcosmicscanner_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "cosmicscanner_b200.h")
+
+CS_OK = 0
+CS_ERR_INVALID_ARGUMENT = -1
+CS_ERR_CUDA = -2
+CS_ERR_IO = -3
+CS_ERR_FORMAT = -4
+CS_ERR_NUMERIC = -5
+CS_ERR_NOT_CONVERGED = -6
+CS_ERR_UNSUPPORTED = -7
+
+_P = C.c_void_p
+_I64 = C.c_int64
+_D = C.c_double
+_I = C.c_int
+
+_SIGNATURES = {
+    "cs_last_error": ([], C.c_char_p),
+    "cs_version": ([], C.c_char_p),
+    "cs_genotypes_create": ([_P, C.c_size_t, _I64, _I64, _P], _I),
+    "cs_genotypes_open_plink": ([C.c_char_p, _P], _I),
+    "cs_genotypes_info": ([_P, _P, _P, _P], _I),
+    "cs_genotypes_stats": ([_P, _P, _P, _P, _P], _I),
+    "cs_genotypes_destroy": ([_P], None),
+    "cs_kinship_create": ([_P, _P, _I64, _P, _I64, _P], _I),
+    "cs_kinship_info": ([_P, _P, _P], _I),
+    "cs_kinship_apply": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
+    "cs_kinship_apply_host": ([_P, _P, _I64, _I64, _P, _I64, _I], _I),
+    "cs_kinship_trace": ([_P, _P], _I),
+    "cs_kinship_diagonal": ([_P, _P], _I),
+    "cs_kinship_destroy": ([_P], None),
+    "cs_lmm_create": ([_P], _I),
+    "cs_lmm_prepare_lowrank_matrix_free": (
+        [_P, _P, _P, _P, _I64, _I, _I, _I64, _D, _I, _I, _P], _I),
+    "cs_lmm_lowrank_basis": ([_P, _P, _I64, _P], _I),
+    "cs_lmm_scan": ([_P, _P, _P, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
+    "cs_lmm_destroy": ([_P], None),
+}
+
+_lib = None
+
+
+def declared_functions() -> list[str]:
+    """Function names declared in the public header."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cs_[a-z0-9_]+)\s*\(", text)))
+
+
+def load(path: str = LIB_PATH):
+    """Loads the shared library; raises if it has not been built."""
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m cosmicscanner_b200.build` "
+            "(the package has no CPU fallback)")
+    L = C.CDLL(path)
+    for name, (args, res) in _SIGNATURES.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    return L
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = load()
+    return _lib

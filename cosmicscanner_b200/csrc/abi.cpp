@@ -1,0 +1,192 @@
+// C ABI: status codes + thread-local error text around the C++ implementation.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "cs_internal.h"
+
+namespace cs {
+cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_samples,
+                                 int64_t n_snps);
+cs_genotypes* genotypes_open_plink(const std::string& prefix);
+cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                           const int32_t* variants, int64_t n_var);
+void kinship_apply_colmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                            int64_t ldy, int precision, cudaStream_t s);
+void kinship_diagonal(cs_kinship* op, double* diag_host);
+cs_lmm* lmm_create();
+void lmm_destroy(cs_lmm* l);
+void lmm_prepare_lowrank(cs_lmm* lmm, cs_kinship* op, const double* y, const double* X, int64_t p,
+                         int rank, int oversample, int64_t seed, double trace_threshold,
+                         int min_rank, int precision, cs_lowrank_diagnostics* diag);
+void lmm_lowrank_basis(const cs_lmm* lmm, double* U, int64_t ldu, double* lambda);
+void lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+              double min_maf, int precision, double* beta, double* se, double* pvalue,
+              double* log10p, double* freq, int32_t* tested);
+}  // namespace cs
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return CS_OK;
+    } catch (const cs::Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return CS_ERR_INVALID_ARGUMENT;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CS_ERR_INVALID_ARGUMENT;
+    }
+}
+
+void require(bool ok, const char* msg) {
+    if (!ok) cs::fail(CS_ERR_INVALID_ARGUMENT, msg);
+}
+}  // namespace
+
+extern "C" {
+
+const char* cs_last_error(void) { return g_last_error.c_str(); }
+const char* cs_version(void) { return "cosmicscanner_b200 0.1.0 (sm_100a)"; }
+
+int cs_genotypes_create(const uint8_t* bed_bytes, size_t n_bytes, int64_t n_samples,
+                        int64_t n_snps, cs_genotypes** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = cs::genotypes_from_bed(bed_bytes, n_bytes, n_samples, n_snps);
+    });
+}
+
+int cs_genotypes_open_plink(const char* prefix, cs_genotypes** out) {
+    return guarded([&] {
+        require(out != nullptr && prefix != nullptr, "null argument");
+        *out = cs::genotypes_open_plink(prefix);
+    });
+}
+
+int cs_genotypes_info(const cs_genotypes* g, int64_t* n_samples, int64_t* n_snps,
+                      int64_t* bytes_per_snp) {
+    return guarded([&] {
+        require(g != nullptr, "null genotypes handle");
+        if (n_samples) *n_samples = g->n_samples;
+        if (n_snps) *n_snps = g->n_snps;
+        if (bytes_per_snp) *bytes_per_snp = g->bytes_per_snp;
+    });
+}
+
+int cs_genotypes_stats(const cs_genotypes* g, double* mean, double* inv_std, int32_t* count,
+                       double* sum) {
+    return guarded([&] {
+        require(g != nullptr, "null genotypes handle");
+        const size_t M = (size_t)g->n_snps;
+        if (mean) std::memcpy(mean, g->mean.data(), M * 8);
+        if (inv_std) std::memcpy(inv_std, g->inv_std.data(), M * 8);
+        if (count) std::memcpy(count, g->count.data(), M * 4);
+        if (sum) std::memcpy(sum, g->sum.data(), M * 8);
+    });
+}
+
+void cs_genotypes_destroy(cs_genotypes* g) { delete g; }
+
+int cs_kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                      const int32_t* variants, int64_t n_variants, cs_kinship** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = cs::kinship_create(g, keep, n_keep, variants, n_variants);
+    });
+}
+
+int cs_kinship_info(const cs_kinship* op, int64_t* rows, int64_t* num_variants) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        if (rows) *rows = op->rows;
+        if (num_variants) *num_variants = op->num_variants;
+    });
+}
+
+int cs_kinship_apply(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                     int64_t ldy, int precision, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        cs::kinship_apply_colmajor(op, X, ldx, k, Y, ldy, precision, (cudaStream_t)stream);
+    });
+}
+
+int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                          int64_t ldy, int precision) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        if (k < 0) cs::fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+        if (ldx < op->rows || ldy < op->rows)
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator::apply: dimension mismatch");
+        if (k == 0) return;
+        const int64_t n = op->rows;
+        cs::DeviceBuffer<double> dx;
+        dx.resize(n * k);
+        CS_CUDA(cudaMemcpy2D(dx.get(), n * 8, X, ldx * 8, n * 8, k, cudaMemcpyHostToDevice));
+        cs::kinship_apply_colmajor(op, dx.get(), n, k, dx.get(), n, precision, 0);
+        CS_CUDA(cudaMemcpy2D(Y, ldy * 8, dx.get(), n * 8, n * 8, k, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cs_kinship_trace(const cs_kinship* op, double* trace) {
+    return guarded([&] {
+        require(op != nullptr && trace != nullptr, "null argument");
+        *trace = op->trace;
+    });
+}
+
+int cs_kinship_diagonal(cs_kinship* op, double* diag) {
+    return guarded([&] {
+        require(op != nullptr && diag != nullptr, "null argument");
+        cs::kinship_diagonal(op, diag);
+    });
+}
+
+void cs_kinship_destroy(cs_kinship* op) { delete op; }
+
+int cs_lmm_create(cs_lmm** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = cs::lmm_create();
+    });
+}
+
+int cs_lmm_prepare_lowrank_matrix_free(cs_lmm* lmm, cs_kinship* op, const double* y,
+                                       const double* X, int64_t p, int rank, int oversample,
+                                       int64_t seed, double trace_threshold, int min_rank,
+                                       int precision, cs_lowrank_diagnostics* diag) {
+    return guarded([&] {
+        require(lmm != nullptr && op != nullptr && y != nullptr, "null argument");
+        cs::lmm_prepare_lowrank(lmm, op, y, X, p, rank, oversample, seed, trace_threshold,
+                                min_rank, precision, diag);
+    });
+}
+
+int cs_lmm_lowrank_basis(const cs_lmm* lmm, double* U, int64_t ldu, double* lambda) {
+    return guarded([&] {
+        require(lmm != nullptr, "null lmm handle");
+        cs::lmm_lowrank_basis(lmm, U, ldu, lambda);
+    });
+}
+
+int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                double min_maf, int precision, double* beta, double* se, double* pvalue,
+                double* log10p, double* freq, int32_t* tested) {
+    return guarded([&] {
+        require(lmm != nullptr && g != nullptr, "null argument");
+        cs::lmm_scan(lmm, g, keep, n_keep, min_maf, precision, beta, se, pvalue, log10p, freq,
+                     tested);
+    });
+}
+
+void cs_lmm_destroy(cs_lmm* lmm) { cs::lmm_destroy(lmm); }
+
+}  // extern "C"

@@ -1,0 +1,155 @@
+// Internal definitions shared by the CUDA library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cosmicscanner_b200.h"
+
+namespace cs {
+
+// Error carried from the implementation to the C ABI, where it becomes a status
+// code plus a thread-local message (no C++ exception crosses the ABI).
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
+};
+
+[[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) fail(CS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CS_CUDA(call) ::cs::check_cuda((call), #call)
+#define CS_LAUNCH(what) ::cs::check_cuda(cudaGetLastError(), what)
+
+// PLINK 2-bit codes (libCosmicCore/src/plink_reader.cpp:12-21):
+// 00 -> 2 copies of A1, 01 -> missing, 10 -> 1, 11 -> 0.
+constexpr uint8_t kMissingByte = 0x55;  // four missing codes
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Packed rows are padded to this many bytes (256 samples): every kernel may read
+// whole 64-byte segments; padding samples carry the missing code and so contribute
+// nothing to any product or count.
+constexpr int64_t kRowAlign = 64;
+
+// Device allocation that frees itself.
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    void resize(size_t n) {
+        if (n <= count) return;
+        release();
+        if (n == 0) return;
+        CS_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+        count = n;
+    }
+    T* get() const { return ptr; }
+};
+
+}  // namespace cs
+
+// Opaque handle bodies.
+struct cs_genotypes {
+    int64_t n_samples = 0;      // rows of the .fam
+    int64_t n_snps = 0;         // rows of the .bim
+    int64_t bytes_per_snp = 0;  // ceil(n/4), the .bed stride
+    int64_t stride = 0;         // device row pitch (bytes_per_snp padded to kRowAlign)
+    cs::DeviceBuffer<uint8_t> packed;
+    // per-SNP statistics over all samples (plink_reader.cpp:187-239), device + host
+    cs::DeviceBuffer<double> d_mean, d_inv_std;
+    std::vector<double> mean, inv_std;
+    std::vector<int32_t> count;
+    std::vector<double> sum;
+    int device = 0;
+};
+
+// A packed matrix of selected rows x selected samples with everything the kernels need.
+struct cs_packed_view {
+    const uint8_t* rows = nullptr;  // device, rows x stride bytes
+    int64_t n_rows = 0;
+    int64_t n_samples = 0;
+    int64_t stride = 0;
+};
+
+namespace cs {
+struct Workspace {
+    DeviceBuffer<double> partial;
+    DeviceBuffer<double> tmp_a, tmp_b, tmp_c;
+};
+struct MixedOperator;  // tensor-core form (kinship_mixed.cu)
+void destroy_mixed(MixedOperator* m);
+}  // namespace cs
+
+// Kinship operator over a (keep, variants) selection of a cs_genotypes matrix.
+struct cs_kinship {
+    const cs_genotypes* g = nullptr;
+    int64_t rows = 0;          // analysed samples
+    int64_t num_variants = 0;  // selected variants (the 1/M scaling counts all of them)
+    cs_packed_view view;       // packed rows the kernels read (own copy or g->packed)
+    cs::DeviceBuffer<uint8_t> own_packed;
+    int64_t n_active = 0;                  // rows of `view` (selected variants with 1/sd != 0)
+    std::vector<double> mean, inv_std;     // per view row
+    std::vector<int32_t> counts;           // per view row: counts of codes 00,01,10,11
+    cs::DeviceBuffer<double> d_lut;        // per view row: {(2-mu)s, 0, (1-mu)s, -mu s}
+    cs::DeviceBuffer<double> d_lut_sq;     // squared entries (diagonal)
+    cs::DeviceBuffer<double> d_mean, d_inv_std;
+    cs::DeviceBuffer<int32_t> d_counts;
+    double trace = 0.0;
+    cs::Workspace ws;
+    cs::DeviceBuffer<double> buf_x, buf_u, buf_y;
+    cs::MixedOperator* mixed = nullptr;
+    ~cs_kinship() { cs::destroy_mixed(mixed); }
+};
+
+namespace cs {
+
+// Y_rm (rows x ldy) = K X_rm (rows x ldx), both row-major device buffers, k columns.
+// Y may equal X.  precision: CS_PRECISION_*.
+void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                            int64_t ldy, int precision, cudaStream_t s);
+void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                         int64_t ldy, cudaStream_t s);
+
+// Per-row genotype code counts over a view's samples: c[4*t + code].
+void row_code_counts(const cs_packed_view& v, int32_t* d_counts, cudaStream_t s);
+
+// Decode-GEMM kernels (FP64).  lut[4*t + code] gives the value of code in row t.
+//   pass_a:  out[t, c] = sum_i lut_t[code(t, i)] * V[i, c]      (rows t, V row-major n x ldv)
+//   pass_b:  out[i, c] = sum_t lut_t[code(t, i)] * W[t, c]      (W row-major rows x ldw)
+// Results are row-major with leading dimension ldo; `scale` multiplies the result.
+void decode_gemm_rows_fp64(const cs_packed_view& v, const double* d_lut, const double* V,
+                           int64_t ldv, int64_t k, double* out, int64_t ldo, Workspace& ws,
+                           cudaStream_t s);
+void decode_gemm_samples_fp64(const cs_packed_view& v, const double* d_lut, const double* W,
+                              int64_t ldw, int64_t k, double* out, int64_t ldo, double scale,
+                              Workspace& ws, cudaStream_t s);
+
+// Repack selected rows/samples of a packed matrix into a new padded matrix.
+void repack(const uint8_t* src, int64_t src_stride, const int32_t* d_rows, int64_t n_rows,
+            const int32_t* d_keep, int64_t n_keep, uint8_t* dst, int64_t dst_stride,
+            cudaStream_t s);
+
+// Column-major (ld) <-> row-major (n x kp, zero padded) conversion on the device.
+void colmajor_to_rowmajor(const double* src, int64_t ld, int64_t n, int64_t k, double* dst,
+                          int64_t kp, cudaStream_t s);
+void rowmajor_to_colmajor(const double* src, int64_t kp, int64_t n, int64_t k, double* dst,
+                          int64_t ld, cudaStream_t s);
+
+int num_sms();
+
+}  // namespace cs

@@ -1,0 +1,188 @@
+// Kinship operator K = Z Z^T / M over a sample / variant selection
+// (src/kinship_operator.h:53-95, src/kinship_operator.cpp:29-374).
+//
+// Layout: the operator reads one packed matrix `view` whose rows are the selected
+// variants and whose samples are the selected samples, padded to kRowAlign bytes with the
+// missing code.  With the identity selection it is the resident genotype matrix itself;
+// otherwise the selection is materialised once at construction by a repack kernel, so
+// every apply streams contiguous rows (a keep list becomes a gather only once, not on
+// every apply as in kinship_operator.cpp:127-134).  Selected variants with 1/sd == 0
+// contribute nothing and are dropped from the copy, while the 1/M scaling still counts
+// them, as the reference does (kinship_operator.cpp:63-64, 96).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "cs_internal.h"
+
+namespace cs {
+
+cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                           const int32_t* variants, int64_t n_var) {
+    if (g == nullptr) fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: null reader");
+    const int64_t N = g->n_samples, M = g->n_snps;
+    bool identity = true;
+    if (keep && n_keep > 0) {
+        for (int64_t i = 0; i < n_keep; ++i)
+            if (keep[i] < 0 || keep[i] >= N)
+                fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: sample index out of range");
+        identity = (n_keep == N);
+        for (int64_t i = 0; identity && i < N; ++i) identity = keep[i] == i;
+    } else {
+        keep = nullptr;
+        n_keep = 0;
+    }
+    if (variants && n_var > 0) {
+        for (int64_t j = 0; j < n_var; ++j)
+            if (variants[j] < 0 || variants[j] >= M)
+                fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: variant index out of range");
+    } else {
+        variants = nullptr;
+        n_var = 0;
+    }
+    auto* op = new cs_kinship();
+    try {
+        op->g = g;
+        op->rows = keep ? n_keep : N;
+        op->num_variants = variants ? n_var : M;
+        if (op->num_variants == 0) fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: no variants selected");
+        cudaStream_t s = 0;
+        std::vector<int32_t> active;
+        if (!variants && identity) {
+            op->view = cs_packed_view{g->packed.get(), M, N, g->stride};
+            op->n_active = M;
+            op->mean = g->mean;
+            op->inv_std = g->inv_std;
+        } else {
+            active.reserve(op->num_variants);
+            for (int64_t t = 0; t < op->num_variants; ++t) {
+                const int32_t j = variants ? variants[t] : (int32_t)t;
+                if (g->inv_std[j] != 0.0) active.push_back(j);
+            }
+            op->n_active = (int64_t)active.size();
+            const int64_t stride = round_up((op->rows + 3) / 4, kRowAlign);
+            op->own_packed.resize(std::max<int64_t>(1, op->n_active * stride));
+            DeviceBuffer<int32_t> d_rows, d_keep;
+            d_rows.resize(std::max<int64_t>(1, op->n_active));
+            if (op->n_active)
+                CS_CUDA(cudaMemcpyAsync(d_rows.get(), active.data(), op->n_active * 4,
+                                        cudaMemcpyHostToDevice, s));
+            if (!identity) {
+                d_keep.resize(n_keep);
+                CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, n_keep * 4, cudaMemcpyHostToDevice, s));
+            }
+            repack(g->packed.get(), g->stride, d_rows.get(), op->n_active,
+                   identity ? nullptr : d_keep.get(), op->rows, op->own_packed.get(), stride, s);
+            CS_CUDA(cudaStreamSynchronize(s));
+            op->view = cs_packed_view{op->own_packed.get(), op->n_active, op->rows, stride};
+            op->mean.resize(op->n_active);
+            op->inv_std.resize(op->n_active);
+            for (int64_t t = 0; t < op->n_active; ++t) {
+                op->mean[t] = g->mean[active[t]];
+                op->inv_std[t] = g->inv_std[active[t]];
+            }
+        }
+        const int64_t R = op->n_active;
+        // code counts over the operator's samples (trace, mixed-form corrections)
+        op->counts.assign(4 * R, 0);
+        op->d_counts.resize(std::max<int64_t>(1, 4 * R));
+        if (R) {
+            row_code_counts(op->view, op->d_counts.get(), s);
+            CS_CUDA(cudaMemcpyAsync(op->counts.data(), op->d_counts.get(), 16 * R,
+                                    cudaMemcpyDeviceToHost, s));
+        }
+        std::vector<double> lut(4 * R), lut_sq(4 * R);
+        double total = 0.0;
+        CS_CUDA(cudaStreamSynchronize(s));
+        for (int64_t t = 0; t < R; ++t) {
+            const double mu = op->mean[t], is = op->inv_std[t];
+            // kinship_operator.cpp:276-277 decode values; code 01 (missing) -> 0
+            lut[4 * t + 0] = (2.0 - mu) * is;
+            lut[4 * t + 1] = 0.0;
+            lut[4 * t + 2] = (1.0 - mu) * is;
+            lut[4 * t + 3] = -mu * is;
+            for (int q = 0; q < 4; ++q) lut_sq[4 * t + q] = lut[4 * t + q] * lut[4 * t + q];
+            // trace(): sum over observed calls of z^2 (kinship_operator.cpp:306-344)
+            total += op->counts[4 * t + 0] * lut_sq[4 * t + 0] +
+                     op->counts[4 * t + 2] * lut_sq[4 * t + 2] +
+                     op->counts[4 * t + 3] * lut_sq[4 * t + 3];
+        }
+        op->trace = total / (double)op->num_variants;
+        op->d_lut.resize(std::max<int64_t>(1, 4 * R));
+        op->d_lut_sq.resize(std::max<int64_t>(1, 4 * R));
+        op->d_mean.resize(std::max<int64_t>(1, R));
+        op->d_inv_std.resize(std::max<int64_t>(1, R));
+        if (R) {
+            CS_CUDA(cudaMemcpy(op->d_lut.get(), lut.data(), 32 * R, cudaMemcpyHostToDevice));
+            CS_CUDA(cudaMemcpy(op->d_lut_sq.get(), lut_sq.data(), 32 * R, cudaMemcpyHostToDevice));
+            CS_CUDA(cudaMemcpy(op->d_mean.get(), op->mean.data(), 8 * R, cudaMemcpyHostToDevice));
+            CS_CUDA(cudaMemcpy(op->d_inv_std.get(), op->inv_std.data(), 8 * R, cudaMemcpyHostToDevice));
+        }
+    } catch (...) {
+        delete op;
+        throw;
+    }
+    return op;
+}
+
+// FP64 form: U = Z^T X (pass over rows), Y = Z U / M (pass over samples).
+static void kinship_apply_fp64(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                               int64_t ldy, cudaStream_t s) {
+    const int64_t R = op->n_active;
+    const double scale = 1.0 / (double)op->num_variants;
+    if (R == 0) {
+        // every selected variant is monomorphic: K = 0
+        CS_CUDA(cudaMemset2DAsync(Y, ldy * 8, 0, k * 8, op->rows, s));
+        return;
+    }
+    op->buf_u.resize(R * k);
+    decode_gemm_rows_fp64(op->view, op->d_lut.get(), X, ldx, k, op->buf_u.get(), k, op->ws, s);
+    decode_gemm_samples_fp64(op->view, op->d_lut.get(), op->buf_u.get(), k, k, Y, ldy, scale,
+                             op->ws, s);
+}
+
+void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                            int64_t ldy, int precision, cudaStream_t s) {
+    if (k <= 0) return;
+    if (precision == CS_PRECISION_MIXED)
+        kinship_apply_mixed(op, X, ldx, k, Y, ldy, s);
+    else if (precision == CS_PRECISION_FP64)
+        kinship_apply_fp64(op, X, ldx, k, Y, ldy, s);
+    else
+        fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
+}
+
+// Public column-major apply (device pointers): transposes in and out around the kernels.
+void kinship_apply_colmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                            int64_t ldy, int precision, cudaStream_t s) {
+    if (k < 0) fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+    if (k == 0) return;
+    if (ldx < op->rows || ldy < op->rows)
+        fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator::apply: dimension mismatch");
+    const int64_t n = op->rows;
+    op->buf_x.resize(n * k);
+    op->buf_y.resize(n * k);
+    colmajor_to_rowmajor(X, ldx, n, k, op->buf_x.get(), k, s);
+    kinship_apply_rowmajor(op, op->buf_x.get(), k, k, op->buf_y.get(), k, precision, s);
+    rowmajor_to_colmajor(op->buf_y.get(), k, n, k, Y, ldy, s);
+}
+
+void kinship_diagonal(cs_kinship* op, double* diag_host) {
+    const int64_t n = op->rows, R = op->n_active;
+    if (R == 0) {
+        std::fill(diag_host, diag_host + n, 0.0);
+        return;
+    }
+    cudaStream_t s = 0;
+    DeviceBuffer<double> ones, d;
+    ones.resize(R);
+    d.resize(n);
+    std::vector<double> h(R, 1.0);
+    CS_CUDA(cudaMemcpy(ones.get(), h.data(), 8 * R, cudaMemcpyHostToDevice));
+    decode_gemm_samples_fp64(op->view, op->d_lut_sq.get(), ones.get(), 1, 1, d.get(), 1,
+                             1.0 / (double)op->num_variants, op->ws, s);
+    CS_CUDA(cudaMemcpy(diag_host, d.get(), 8 * n, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace cs

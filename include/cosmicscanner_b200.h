@@ -1,0 +1,127 @@
+/*
+ * cosmicscanner_b200 — C ABI of the B200 (sm_100a) matrix-free mixed-model path.
+ *
+ * Every entry point returns an int status (CS_OK = 0, negative on error) and never
+ * throws; cs_last_error() returns the message of the calling thread's last failure.
+ * Handles are opaque.  Dense matrices are column-major with an explicit leading
+ * dimension, as Eigen stores them in the reference; "_host" entry points take host
+ * pointers and synchronise, the others take device pointers and a cudaStream_t
+ * (passed as void*, NULL = the legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces (file:line in the
+ * CosmicScanner sources).
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CS_OK = 0,
+    CS_ERR_INVALID_ARGUMENT = -1, /* dimension / index errors: std::runtime_error in the reference */
+    CS_ERR_CUDA = -2,             /* CUDA runtime or library failure */
+    CS_ERR_IO = -3,               /* file cannot be opened / read */
+    CS_ERR_FORMAT = -4,           /* bad .bed magic or unsupported mode */
+    CS_ERR_NUMERIC = -5,          /* singular system, failed factorisation, non-finite values */
+    CS_ERR_NOT_CONVERGED = -6,    /* iteration limit reached where convergence is required */
+    CS_ERR_UNSUPPORTED = -7,      /* configuration the library does not implement */
+};
+
+/* Arithmetic of an operator apply. */
+enum {
+    CS_PRECISION_FP64 = 0,  /* FP64 decode-GEMM (the plain form) */
+    CS_PRECISION_MIXED = 1, /* tensor-core form: exact genotypes x split right-hand sides */
+};
+
+typedef struct cs_genotypes cs_genotypes;
+typedef struct cs_kinship cs_kinship;
+typedef struct cs_lmm cs_lmm;
+
+const char* cs_last_error(void);
+const char* cs_version(void);
+
+/* ---------------------------------------------------------------- genotypes
+ * Replaces PlinkReader::load / openBed (libCosmicCore/src/plink_reader.cpp:28-92)
+ * and PlinkReader::computeStats (plink_reader.cpp:187-239).  The packed SNP-major
+ * matrix is copied to HBM once and stays resident; statistics (mean, 1/sd over all
+ * .fam samples) are computed on the device, bit-exact with the reference. */
+int cs_genotypes_create(const uint8_t* bed_bytes, size_t n_bytes, int64_t n_samples,
+                        int64_t n_snps, cs_genotypes** out);
+/* Reads prefix.fam / prefix.bim (line counts) and prefix.bed. */
+int cs_genotypes_open_plink(const char* prefix, cs_genotypes** out);
+int cs_genotypes_info(const cs_genotypes* g, int64_t* n_samples, int64_t* n_snps,
+                      int64_t* bytes_per_snp);
+/* Host copies of the per-SNP statistics (any output may be NULL). */
+int cs_genotypes_stats(const cs_genotypes* g, double* mean, double* inv_std, int32_t* count,
+                       double* sum);
+void cs_genotypes_destroy(cs_genotypes* g);
+
+/* ---------------------------------------------------------------- kinship operator
+ * Replaces cosmic::KinshipOperator / PlinkKinshipOperator (src/kinship_operator.h:18-95)
+ * and createKinshipOperator (src/kinship_operator.cpp:370-374):
+ * K = Z Z^T / M over the selected samples (keep, NULL = all) and variants (NULL = all);
+ * Z = (G - mean) * inv_std with missing calls contributing zero.  Out-of-range
+ * indices and an empty variant set fail with CS_ERR_INVALID_ARGUMENT, as the reference
+ * constructor throws. */
+int cs_kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                      const int32_t* variants, int64_t n_variants, cs_kinship** out);
+/* rows() / cols() / numVariants() (kinship_operator.h:22-27). */
+int cs_kinship_info(const cs_kinship* op, int64_t* rows, int64_t* num_variants);
+/* apply(const MatrixXd& X, MatrixXd& out) / apply_block (kinship_operator.cpp:220-302):
+ * Y = K X for X rows() x k.  Y may alias X.  k == 0 is a no-op.  Device pointers. */
+int cs_kinship_apply(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                     int64_t ldy, int precision, void* stream);
+/* Same with host pointers (synchronous). */
+int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                          int64_t ldy, int precision);
+/* trace() and getDiagonal() (kinship_operator.cpp:306-368); diag is a host array. */
+int cs_kinship_trace(const cs_kinship* op, double* trace);
+int cs_kinship_diagonal(cs_kinship* op, double* diag);
+void cs_kinship_destroy(cs_kinship* op);
+
+/* ---------------------------------------------------------------- low-rank LMM engine
+ * Replaces LmmEngine::prepareLowRankMatrixFree (src/lmm_engine.cpp:897-1095):
+ * randomized subspace iteration on K (Omega ~ N(0,1) from mt19937_64(seed), two power
+ * iterations, QR, eigendecomposition of Q^T K Q), trace-fraction rank selection, tail-mean
+ * residual eigenvalue, then REML over log(eta) by an 81-point grid and golden-section
+ * search.  y has rows() entries, X is rows() x p column-major (the reference receives X
+ * as MatrixXf: callers mirroring it pass FP32-rounded values).  Host pointers. */
+typedef struct {
+    int32_t requested_rank;
+    int32_t effective_rank;
+    int32_t sketch_size;
+    int32_t trace_threshold_met;
+    double residual_eigenvalue;
+    double relative_frobenius_error;
+    double trace;
+    double trace_fraction;
+    double sigma2_g;
+    double sigma2_e;
+    double delta;
+    double log_eta;
+    double reml_objective;
+    double seconds;
+} cs_lowrank_diagnostics;
+
+int cs_lmm_create(cs_lmm** out);
+int cs_lmm_prepare_lowrank_matrix_free(cs_lmm* lmm, cs_kinship* op, const double* y,
+                                       const double* X, int64_t p, int rank, int oversample,
+                                       int64_t seed, double trace_threshold, int min_rank,
+                                       int precision, cs_lowrank_diagnostics* diag);
+/* Low-rank basis after preparation: U (rows() x rank, column-major, host) and eigenvalues. */
+int cs_lmm_lowrank_basis(const cs_lmm* lmm, double* U, int64_t ldu, double* lambda);
+/* Replaces LmmEngine::scan(PlinkReader, ...) -> scanLowRank (src/lmm_engine.cpp:1269-1361)
+ * for every SNP of g (no chromosome filter): keep lists the analysed samples in the order
+ * of y.  Per-SNP host outputs of length n_snps; tested[j] = 0 where the reference writes no
+ * row (MAF filter, variance <= 1e-12).  Any output may be NULL. */
+int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                double min_maf, int precision, double* beta, double* se, double* pvalue,
+                double* log10p, double* freq, int32_t* tested);
+void cs_lmm_destroy(cs_lmm* lmm);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,233 @@
+"""ctypes loader for the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+The oracle restates the reference CosmicScanner algorithms on the CPU in FP64
+(oracle.cpp cites the reference file:line of every function).  Only the tests,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use it, and
+only as the checker: the product library never loads it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile liboracle.so in place (make); returns its path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class LowRankResult(C.Structure):
+    _fields_ = [
+        ("rank", C.c_int32), ("sketch_size", C.c_int32),
+        ("residual_eigenvalue", C.c_double), ("relative_frobenius_error", C.c_double),
+        ("trace", C.c_double), ("trace_fraction", C.c_double),
+        ("trace_threshold_met", C.c_int32),
+        ("sigma2_g", C.c_double), ("sigma2_e", C.c_double), ("delta", C.c_double),
+        ("best_log_eta", C.c_double), ("best_objective", C.c_double),
+    ]
+
+
+_P = C.c_void_p
+_I64 = C.c_int64
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or (
+            os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "oracle.cpp"))
+        ):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        sel = [_P, _I64, _P, _I64]  # keep, n_keep, variants, n_var
+        L.orc_compute_stats.argtypes = [_P, _I64, _I64, _I64, _P, _P, _P, _P]
+        L.orc_kinship_apply_vector.argtypes = [_P, _I64, _I64, _P, _P] + sel + [_P, _P, C.c_int]
+        L.orc_kinship_apply_vector.restype = C.c_int
+        L.orc_kinship_apply_block.argtypes = [_P, _I64, _I64, _P, _P] + sel + [_P, _I64, _I64, _P, _I64, C.c_int]
+        L.orc_kinship_apply_block.restype = C.c_int
+        L.orc_kinship_trace.argtypes = [_P, _I64, _I64, _P, _P] + sel
+        L.orc_kinship_trace.restype = C.c_double
+        L.orc_kinship_diagonal.argtypes = [_P, _I64, _I64, _P, _P] + sel + [_P]
+        L.orc_dense_z.argtypes = [_P, _I64, _I64, _P, _P] + sel + [_P, _I64]
+        L.orc_kinship_batch_fixture.argtypes = [C.c_int, C.c_int, C.c_uint64, _P, C.c_int, _P, C.c_int, _P, _P]
+        L.orc_normal_matrix.argtypes = [C.c_uint64, _I64, _I64, _P]
+        L.orc_prepare_marker.argtypes = [_P, _I64, C.c_double, _P, _P, _P]
+        L.orc_prepare_marker.restype = C.c_int
+        L.orc_chisq_prob.argtypes = [C.c_double, C.c_int]
+        L.orc_chisq_prob.restype = C.c_double
+        L.orc_lowrank_prepare.argtypes = [_P, _I64, _I64, _P, _P] + sel + [
+            _P, _P, _I64, C.c_int, C.c_int, C.c_uint64, C.c_double, C.c_int, C.c_int, _P, _P, _P]
+        L.orc_lowrank_prepare.restype = C.c_int
+        L.orc_lowrank_reml.argtypes = [_P, _P, _I64, _I64, C.c_double, _P, _P, _I64, _P]
+        L.orc_lowrank_reml.restype = C.c_int
+        L.orc_scan_lowrank.argtypes = [_P, _I64, _I64, _I64, _P, _I64, _P, _P, _I64, C.c_double,
+                                       C.c_double, C.c_double, _P, _P, _I64, C.c_double,
+                                       _P, _P, _P, _P, _P, _P]
+        L.orc_scan_lowrank.restype = C.c_int
+        L.orc_pcg_solve.argtypes = [_P, _I64, _I64, _P, _P] + sel + [
+            C.c_double, C.c_double, _P, C.c_double, C.c_int, _P]
+        L.orc_pcg_solve.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Bed:
+    """Packed SNP-major BED rows (magic skipped) with the reference's per-SNP stats."""
+
+    def __init__(self, rows: np.ndarray, n_samples: int):
+        self.rows = np.ascontiguousarray(rows, dtype=np.uint8)
+        self.n = int(n_samples)
+        self.m = int(self.rows.shape[0])
+        self.stride = int(self.rows.shape[1])
+        self.mean = np.zeros(self.m)
+        self.inv_std = np.zeros(self.m)
+        self.count = np.zeros(self.m, dtype=np.int32)
+        self.sum = np.zeros(self.m)
+        lib().orc_compute_stats(_ptr(self.rows), self.n, self.m, self.stride, _ptr(self.mean),
+                                _ptr(self.inv_std), _ptr(self.count), _ptr(self.sum))
+
+    def _sel(self, keep, variants):
+        keep = _i32(keep)
+        variants = _i32(variants)
+        args = [_ptr(keep), 0 if keep is None else len(keep),
+                _ptr(variants), self.m if variants is None else len(variants)]
+        return args, (keep, variants)
+
+    def rows_for(self, keep):
+        return self.n if keep is None else len(keep)
+
+    def apply_vector(self, v, keep=None, variants=None, n_threads=1):
+        args, hold = self._sel(keep, variants)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        out = np.zeros(self.rows_for(keep))
+        rc = lib().orc_kinship_apply_vector(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                            _ptr(self.inv_std), *args, _ptr(v), _ptr(out), n_threads)
+        if rc != 0:
+            raise RuntimeError("oracle apply_vector failed")
+        return out
+
+    def apply_block(self, X, keep=None, variants=None, n_threads=1):
+        args, hold = self._sel(keep, variants)
+        X = np.asfortranarray(X, dtype=np.float64)
+        n, k = X.shape
+        out = np.zeros((n, k), order="F")
+        rc = lib().orc_kinship_apply_block(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                           _ptr(self.inv_std), *args, _ptr(X), n, k, _ptr(out), n,
+                                           n_threads)
+        if rc != 0:
+            raise RuntimeError("oracle apply_block failed")
+        return out
+
+    def trace(self, keep=None, variants=None):
+        args, hold = self._sel(keep, variants)
+        return lib().orc_kinship_trace(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                       _ptr(self.inv_std), *args)
+
+    def diagonal(self, keep=None, variants=None):
+        args, hold = self._sel(keep, variants)
+        out = np.zeros(self.rows_for(keep))
+        lib().orc_kinship_diagonal(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                   _ptr(self.inv_std), *args, _ptr(out))
+        return out
+
+    def dense_z(self, keep=None, variants=None):
+        args, hold = self._sel(keep, variants)
+        nr = self.rows_for(keep)
+        nv = self.m if variants is None else len(variants)
+        z = np.zeros((nr, nv), order="F")
+        lib().orc_dense_z(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                          _ptr(self.inv_std), *args, _ptr(z), nr)
+        return z
+
+    def lowrank_prepare(self, y, X, rank, keep=None, variants=None, oversample=10, seed=42,
+                        trace_threshold=0.95, min_rank=1, n_threads=1):
+        args, hold = self._sel(keep, variants)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        n, p = X.shape
+        U = np.zeros((n, rank), order="F")
+        lam = np.zeros(rank)
+        res = LowRankResult()
+        rc = lib().orc_lowrank_prepare(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                       _ptr(self.inv_std), *args, _ptr(y), _ptr(X), p, rank,
+                                       oversample, seed, trace_threshold, min_rank, n_threads,
+                                       _ptr(U), _ptr(lam), C.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"oracle lowrank_prepare failed ({rc})")
+        r = res.rank
+        return np.asfortranarray(U[:, :r]), lam[:r].copy(), res
+
+    def scan_lowrank(self, keep, U, lam, r0, sigma2_g, sigma2_e, y, X, min_maf=0.01):
+        keep = _i32(keep)
+        U = np.asfortranarray(U, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(X, dtype=np.float64)
+        n, p = X.shape
+        out = {k: np.full(self.m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
+        tested = np.zeros(self.m, dtype=np.int32)
+        rc = lib().orc_scan_lowrank(_ptr(self.rows), self.n, self.stride, self.m, _ptr(keep), n,
+                                    _ptr(U), _ptr(lam), U.shape[1], r0, sigma2_g, sigma2_e,
+                                    _ptr(y), _ptr(X), p, min_maf, _ptr(out["beta"]),
+                                    _ptr(out["se"]), _ptr(out["p"]), _ptr(out["log10p"]),
+                                    _ptr(out["freq"]), _ptr(tested))
+        if rc != 0:
+            raise RuntimeError("oracle scan_lowrank failed")
+        out["tested"] = tested.astype(bool)
+        return out
+
+    def pcg_solve(self, b, sg2, se2, tol, max_iter, keep=None, variants=None):
+        args, hold = self._sel(keep, variants)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        it = lib().orc_pcg_solve(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
+                                 _ptr(self.inv_std), *args, sg2, se2, _ptr(b), tol, max_iter, _ptr(x))
+        return x, it
+
+
+def kinship_batch_fixture(n=37, m=1031, seed=8128, rows=None, widths=(1, 7, 41)):
+    """Regenerates tests/test_kinship_batch.cpp's BED bytes and omega draws exactly."""
+    rows = np.asarray(rows if rows is not None else [], dtype=np.int32)
+    widths = np.asarray(widths, dtype=np.int32)
+    stride = (n + 3) // 4
+    bed = np.zeros(3 + m * stride, dtype=np.uint8)
+    total = int(sum(int(r) * int(w) for r in rows for w in widths))
+    omega = np.zeros(max(total, 1))
+    lib().orc_kinship_batch_fixture(n, m, seed, _ptr(bed), len(rows), _ptr(rows), len(widths),
+                                    _ptr(widths), _ptr(omega) if total else None)
+    return bed, omega[:total]
+
+
+def normal_matrix(seed, n, cols):
+    out = np.zeros((n, cols), order="F")
+    lib().orc_normal_matrix(seed, n, cols, _ptr(out))
+    return out
+
+
+def chisq_prob(stat, df=1):
+    return lib().orc_chisq_prob(float(stat), int(df))
+
+
+def prepare_marker(raw, min_maf=0.01):
+    raw = np.ascontiguousarray(raw, dtype=np.float64)
+    vals = np.zeros_like(raw)
+    f = C.c_double()
+    obs = C.c_int32()
+    ok = lib().orc_prepare_marker(_ptr(raw), len(raw), min_maf, _ptr(vals), C.byref(f), C.byref(obs))
+    return bool(ok), vals, f.value, obs.value

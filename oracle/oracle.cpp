@@ -1,0 +1,875 @@
+// CPU oracle for the matrix-free mixed-model path — TEST INFRASTRUCTURE ONLY.
+// Restates the reference CosmicScanner algorithms in plain FP64 loops (no Eigen,
+// which is absent here).  Each function cites the reference file:line it follows.
+// Only the tests and bench.py's CPU-baseline leg load this library.
+#include "oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <stdexcept>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+// libCosmicCore/src/plink_reader.cpp:18-21 lookup table; kinship_operator.cpp:18-20.
+const float kLookup[4] = {2.0f, NAN, 1.0f, 0.0f};
+const float kDosage[4] = {2.0f, 0.0f, 1.0f, 0.0f};
+const double kObserved[4] = {1.0, 0.0, 1.0, 1.0};
+
+inline int code_at(const uint8_t* row, int64_t sample) {
+    return (row[sample >> 2] >> ((sample & 3) * 2)) & 3;
+}
+
+struct Selection {
+    const uint8_t* bed;
+    int64_t n_fam, stride;
+    const double* mean;
+    const double* inv_std;
+    const int32_t* keep;
+    int64_t n_keep;
+    const int32_t* variants;
+    int64_t n_var;
+    bool identity;
+    int64_t rows() const { return keep ? n_keep : n_fam; }
+    int64_t cols() const { return n_var; }
+    int64_t snp(int64_t t) const { return variants ? variants[t] : t; }
+    int64_t sample(int64_t r) const { return identity ? r : keep[r]; }
+    const uint8_t* row(int64_t t) const { return bed + snp(t) * stride; }
+};
+
+// kinship_operator.cpp:35-64: an explicit keep equal to 0..n-1 is the identity path.
+Selection make_selection(const uint8_t* bed, int64_t n_fam, int64_t stride, const double* mean,
+                         const double* inv_std, const int32_t* keep, int64_t n_keep,
+                         const int32_t* variants, int64_t n_var) {
+    Selection s{bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var, true};
+    if (keep) {
+        s.identity = (n_keep == n_fam);
+        for (int64_t i = 0; s.identity && i < n_fam; ++i) s.identity = keep[i] == i;
+    }
+    return s;
+}
+
+// libgomp static schedule without chunk: the first (m % w) workers take one extra iteration.
+void static_range(int64_t m, int workers, int w, int64_t* lo, int64_t* hi) {
+    const int64_t q = m / workers, r = m % workers;
+    *lo = w * q + std::min<int64_t>(w, r);
+    *hi = *lo + q + (w < r ? 1 : 0);
+}
+
+// kinship_operator.cpp:74-137 (multiplyZt)
+void multiply_zt(const Selection& s, const double* v, double* u) {
+    const int64_t n = s.rows();
+    for (int64_t t = 0; t < s.cols(); ++t) {
+        const int64_t j = s.snp(t);
+        const double inv_std = s.inv_std[j];
+        u[t] = 0.0;
+        if (inv_std == 0.0) continue;
+        const double mean = s.mean[j];
+        const uint8_t* col = s.row(t);
+        double sum_xv = 0.0, sum_v = 0.0;
+        if (s.identity) {
+            const int64_t full = n >> 2;
+            for (int64_t b = 0; b < full; ++b) {
+                const uint8_t byte = col[b];
+                const int64_t r = b << 2;
+                const double v0 = v[r], v1 = v[r + 1], v2 = v[r + 2], v3 = v[r + 3];
+                sum_xv += v0 * kDosage[byte & 3] + v1 * kDosage[(byte >> 2) & 3] +
+                          v2 * kDosage[(byte >> 4) & 3] + v3 * kDosage[(byte >> 6) & 3];
+                sum_v += v0 * kObserved[byte & 3] + v1 * kObserved[(byte >> 2) & 3] +
+                         v2 * kObserved[(byte >> 4) & 3] + v3 * kObserved[(byte >> 6) & 3];
+            }
+            for (int64_t r = full << 2; r < n; ++r) {
+                const int code = code_at(col, r);
+                if (code == 1) continue;
+                sum_xv += static_cast<double>(kDosage[code]) * v[r];
+                sum_v += v[r];
+            }
+        } else {
+            for (int64_t r = 0; r < n; ++r) {
+                const int code = code_at(col, s.keep[r]);
+                if (code == 1) continue;
+                sum_xv += static_cast<double>(kDosage[code]) * v[r];
+                sum_v += v[r];
+            }
+        }
+        u[t] = (sum_xv - mean * sum_v) * inv_std;
+    }
+}
+
+// kinship_operator.cpp:139-209 (multiplyZ) with worker-order reduction.
+void multiply_z(const Selection& s, const double* u, double* y, int n_threads) {
+    const int64_t n = s.rows(), m = s.cols();
+    std::fill(y, y + n, 0.0);
+    auto accumulate = [&](int64_t t, double* dest) {
+        const int64_t j = s.snp(t);
+        const double inv_std = s.inv_std[j];
+        if (inv_std == 0.0) return;
+        const double mean = s.mean[j];
+        const double weight = u[t] * inv_std;
+        const uint8_t* col = s.row(t);
+        if (s.identity) {
+            const double vmap[4] = {(2.0 - mean) * weight, 0.0, (1.0 - mean) * weight,
+                                    (0.0 - mean) * weight};
+            const int64_t full = n >> 2;
+            for (int64_t b = 0; b < full; ++b) {
+                const uint8_t byte = col[b];
+                const int64_t r = b << 2;
+                dest[r] += vmap[byte & 3];
+                dest[r + 1] += vmap[(byte >> 2) & 3];
+                dest[r + 2] += vmap[(byte >> 4) & 3];
+                dest[r + 3] += vmap[(byte >> 6) & 3];
+            }
+            for (int64_t r = full << 2; r < n; ++r) dest[r] += vmap[code_at(col, r)];
+        } else {
+            for (int64_t r = 0; r < n; ++r) {
+                const int code = code_at(col, s.keep[r]);
+                if (code == 1) continue;
+                dest[r] += (static_cast<double>(kDosage[code]) - mean) * weight;
+            }
+        }
+    };
+    const int workers = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(n_threads, m)));
+    if (workers == 1) {
+        for (int64_t t = 0; t < m; ++t) accumulate(t, y);
+        return;
+    }
+    std::vector<double> local(static_cast<size_t>(n) * workers, 0.0);
+#pragma omp parallel for num_threads(workers) schedule(static, 1)
+    for (int w = 0; w < workers; ++w) {
+        int64_t lo, hi;
+        static_range(m, workers, w, &lo, &hi);
+        for (int64_t t = lo; t < hi; ++t) accumulate(t, local.data() + static_cast<size_t>(w) * n);
+    }
+    for (int w = 0; w < workers; ++w)
+        for (int64_t r = 0; r < n; ++r) y[r] += local[static_cast<size_t>(w) * n + r];
+}
+
+// ---------------------------------------------------------------- small dense algebra
+// Column-major helpers, plain loops.
+
+// Householder QR of A (n x k, ld n, n >= k), returns thin Q (n x k) in place of A.
+// Follows Eigen's makeHouseholder convention (beta = -sign(c0) * norm).
+void householder_thin_q(double* A, int64_t n, int64_t k) {
+    std::vector<double> tau(k, 0.0);
+    for (int64_t j = 0; j < k; ++j) {
+        double* col = A + j * n;
+        const double c0 = col[j];
+        double tail = 0.0;
+        for (int64_t i = j + 1; i < n; ++i) tail += col[i] * col[i];
+        if (tail <= std::numeric_limits<double>::min()) {
+            tau[j] = 0.0;
+            for (int64_t i = j + 1; i < n; ++i) col[i] = 0.0;
+            continue;
+        }
+        double beta = std::sqrt(c0 * c0 + tail);
+        if (c0 >= 0.0) beta = -beta;
+        const double scale = 1.0 / (c0 - beta);
+        for (int64_t i = j + 1; i < n; ++i) col[i] *= scale;
+        tau[j] = (beta - c0) / beta;
+        col[j] = beta;
+        // apply H = I - tau v v^T to the trailing columns (v = [1; col[j+1:]])
+#pragma omp parallel for schedule(static)
+        for (int64_t c = j + 1; c < k; ++c) {
+            double* a = A + c * n;
+            double dot = a[j];
+            for (int64_t i = j + 1; i < n; ++i) dot += col[i] * a[i];
+            dot *= tau[j];
+            a[j] -= dot;
+            for (int64_t i = j + 1; i < n; ++i) a[i] -= dot * col[i];
+        }
+    }
+    // Form Q = H_0 ... H_{k-1} [I_k; 0] by backward accumulation.
+    std::vector<double> Q(static_cast<size_t>(n) * k, 0.0);
+    for (int64_t c = 0; c < k; ++c) Q[c * n + c] = 1.0;
+    for (int64_t j = k - 1; j >= 0; --j) {
+        const double* v = A + j * n;
+        if (tau[j] == 0.0) continue;
+#pragma omp parallel for schedule(static)
+        for (int64_t c = j; c < k; ++c) {
+            double* q = Q.data() + c * n;
+            double dot = q[j];
+            for (int64_t i = j + 1; i < n; ++i) dot += v[i] * q[i];
+            dot *= tau[j];
+            q[j] -= dot;
+            for (int64_t i = j + 1; i < n; ++i) q[i] -= dot * v[i];
+        }
+    }
+    std::memcpy(A, Q.data(), sizeof(double) * Q.size());
+}
+
+// Cyclic Jacobi eigensolver for a symmetric k x k matrix (column-major).
+// Returns eigenvalues ascending (like Eigen's SelfAdjointEigenSolver) and vectors.
+void jacobi_eigh(const double* S, int64_t k, double* evals, double* evecs) {
+    std::vector<double> A(S, S + k * k);
+    for (int64_t i = 0; i < k; ++i)
+        for (int64_t j = 0; j < k; ++j) evecs[i + j * k] = (i == j) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int64_t j = 0; j < k; ++j)
+            for (int64_t i = 0; i < k; ++i) {
+                if (i != j) off += A[i + j * k] * A[i + j * k];
+                else diag += A[i + j * k] * A[i + j * k];
+            }
+        if (off <= 1e-30 * diag || off == 0.0) break;
+        for (int64_t p = 0; p < k - 1; ++p)
+            for (int64_t q = p + 1; q < k; ++q) {
+                const double apq = A[p + q * k];
+                if (std::abs(apq) < 1e-300) continue;
+                const double app = A[p + p * k], aqq = A[q + q * k];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) /
+                                 (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int64_t r = 0; r < k; ++r) {
+                    const double arp = A[r + p * k], arq = A[r + q * k];
+                    A[r + p * k] = c * arp - s * arq;
+                    A[r + q * k] = s * arp + c * arq;
+                }
+                for (int64_t r = 0; r < k; ++r) {
+                    const double apr = A[p + r * k], aqr = A[q + r * k];
+                    A[p + r * k] = c * apr - s * aqr;
+                    A[q + r * k] = s * apr + c * aqr;
+                }
+                for (int64_t r = 0; r < k; ++r) {
+                    const double vrp = evecs[r + p * k], vrq = evecs[r + q * k];
+                    evecs[r + p * k] = c * vrp - s * vrq;
+                    evecs[r + q * k] = s * vrp + c * vrq;
+                }
+            }
+    }
+    std::vector<int64_t> order(k);
+    for (int64_t i = 0; i < k; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(),
+              [&](int64_t a, int64_t b) { return A[a + a * k] < A[b + b * k]; });
+    std::vector<double> V(evecs, evecs + k * k);
+    for (int64_t c = 0; c < k; ++c) {
+        evals[c] = A[order[c] + order[c] * k];
+        for (int64_t r = 0; r < k; ++r) evecs[r + c * k] = V[r + order[c] * k];
+    }
+}
+
+// LDL^T of a small SPD matrix (p x p).  Returns false when a pivot is not positive
+// (Eigen LDLT::isPositive() in the reference objective).
+bool ldlt(const double* A, int64_t p, std::vector<double>& L, std::vector<double>& D) {
+    L.assign(p * p, 0.0);
+    D.assign(p, 0.0);
+    for (int64_t j = 0; j < p; ++j) {
+        double d = A[j + j * p];
+        for (int64_t s = 0; s < j; ++s) d -= L[j + s * p] * L[j + s * p] * D[s];
+        D[j] = d;
+        if (!(d > 0.0)) return false;
+        L[j + j * p] = 1.0;
+        for (int64_t i = j + 1; i < p; ++i) {
+            double v = A[i + j * p];
+            for (int64_t s = 0; s < j; ++s) v -= L[i + s * p] * L[j + s * p] * D[s];
+            L[i + j * p] = v / d;
+        }
+    }
+    return true;
+}
+
+void ldlt_solve(const std::vector<double>& L, const std::vector<double>& D, int64_t p, double* b) {
+    for (int64_t i = 0; i < p; ++i)
+        for (int64_t s = 0; s < i; ++s) b[i] -= L[i + s * p] * b[s];
+    for (int64_t i = 0; i < p; ++i) b[i] /= D[i];
+    for (int64_t i = p - 1; i >= 0; --i)
+        for (int64_t s = i + 1; s < p; ++s) b[i] -= L[s + i * p] * b[s];
+}
+
+// src/lmm_engine.cpp:22-58 (gamma_q): series / continued fraction, 1e-7 tolerance.
+double gamma_q(double a, double x) {
+    if (x < 0.0 || a <= 0.0) return 1.0;
+    if (x < a + 1.0) {
+        double ap = a, sum = 1.0 / a, del = sum;
+        for (int i = 0; i < 100; ++i) {
+            ap += 1.0;
+            del *= x / ap;
+            sum += del;
+            if (std::abs(del) < std::abs(sum) * 1e-7)
+                return 1.0 - sum * std::exp(-x + a * std::log(x) - std::lgamma(a));
+        }
+    } else {
+        double b = x + 1.0 - a, c = 1.0 / 1e-30, d = 1.0 / b, h = d;
+        for (int i = 1; i <= 100; ++i) {
+            const double an = -i * (i - a);
+            b += 2.0;
+            d = an * d + b;
+            if (std::abs(d) < 1e-30) d = 1e-30;
+            c = b + an / c;
+            if (std::abs(c) < 1e-30) c = 1e-30;
+            d = 1.0 / d;
+            const double del = d * c;
+            h *= del;
+            if (std::abs(del - 1.0) < 1e-7) return std::exp(-x + a * std::log(x) - std::lgamma(a)) * h;
+        }
+    }
+    return 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_compute_stats(const uint8_t* bed, int64_t n_samples, int64_t n_snps, int64_t stride,
+                       double* mean, double* inv_std, int32_t* count_out, double* sum_out) {
+    for (int64_t j = 0; j < n_snps; ++j) {
+        const uint8_t* col = bed + j * stride;
+        double sum = 0.0, sum_sq = 0.0;
+        int count = 0;
+        for (int64_t i = 0; i < n_samples; ++i) {
+            const float val = kLookup[(col[i / 4] >> ((i % 4) * 2)) & 3];
+            if (!std::isnan(val)) {
+                sum += val;
+                sum_sq += val * val;
+                count++;
+            }
+        }
+        (void)sum_sq;
+        if (count_out) count_out[j] = count;
+        if (sum_out) sum_out[j] = sum;
+        if (count > 0) {
+            const double m = sum / count;
+            const double p = m / 2.0;
+            const double var = 2.0 * p * (1.0 - p);
+            mean[j] = m;
+            inv_std[j] = (var < 1e-9) ? 0.0 : 1.0 / std::sqrt(var);
+        } else {
+            mean[j] = 0.0;
+            inv_std[j] = 0.0;
+        }
+    }
+}
+
+int orc_kinship_apply_vector(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                             const double* mean, const double* inv_std,
+                             const int32_t* keep, int64_t n_keep,
+                             const int32_t* variants, int64_t n_var,
+                             const double* v, double* out, int n_threads) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    if (s.cols() == 0) return -1;
+    std::vector<double> u(s.cols()), w(s.rows());
+    multiply_zt(s, v, u.data());
+    multiply_z(s, u.data(), w.data(), std::max(1, n_threads));
+    const double scaling = 1.0 / static_cast<double>(s.cols());
+    for (int64_t r = 0; r < s.rows(); ++r) out[r] = scaling * w[r];
+    return 0;
+}
+
+int orc_kinship_apply_block(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                            const double* mean, const double* inv_std,
+                            const int32_t* keep, int64_t n_keep,
+                            const int32_t* variants, int64_t n_var,
+                            const double* X, int64_t ldx, int64_t k,
+                            double* out, int64_t ldo, int n_threads) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    const int64_t n = s.rows(), m = s.cols();
+    if (m == 0) return -1;
+    std::vector<double> result(static_cast<size_t>(n) * k, 0.0);
+    const int64_t block = 512;
+    std::vector<double> z, proj;
+    for (int64_t first = 0; first < m; first += block) {
+        const int64_t count = std::min(block, m - first);
+        z.assign(static_cast<size_t>(n) * count, 0.0);
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static)
+        for (int64_t j = 0; j < count; ++j) {
+            const int64_t snp = s.snp(first + j);
+            const double mu = mean[snp], is = inv_std[snp];
+            double* dest = z.data() + j * n;
+            if (is == 0.0) continue;
+            const double values[4] = {(2.0 - mu) * is, 0.0, (1.0 - mu) * is, -mu * is};
+            const uint8_t* col = bed + snp * stride;
+            for (int64_t r = 0; r < n; ++r) dest[r] = values[code_at(col, s.sample(r))];
+        }
+        proj.assign(static_cast<size_t>(count) * k, 0.0);  // count x k
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static) collapse(2)
+        for (int64_t c = 0; c < k; ++c)
+            for (int64_t j = 0; j < count; ++j) {
+                const double* zc = z.data() + j * n;
+                const double* xc = X + c * ldx;
+                double acc = 0.0;
+                for (int64_t r = 0; r < n; ++r) acc += zc[r] * xc[r];
+                proj[j + c * count] = acc;
+            }
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static)
+        for (int64_t c = 0; c < k; ++c) {
+            double* rc = result.data() + c * n;
+            for (int64_t j = 0; j < count; ++j) {
+                const double pj = proj[j + c * count];
+                const double* zc = z.data() + j * n;
+                for (int64_t r = 0; r < n; ++r) rc[r] += zc[r] * pj;
+            }
+        }
+    }
+    const double scaling = 1.0 / static_cast<double>(m);
+    for (int64_t c = 0; c < k; ++c)
+        for (int64_t r = 0; r < n; ++r) out[r + c * ldo] = result[r + c * n] * scaling;
+    return 0;
+}
+
+double orc_kinship_trace(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                         const double* mean, const double* inv_std,
+                         const int32_t* keep, int64_t n_keep,
+                         const int32_t* variants, int64_t n_var) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    double total = 0.0;
+    for (int64_t t = 0; t < s.cols(); ++t) {
+        const int64_t j = s.snp(t);
+        if (inv_std[j] == 0.0) continue;
+        const uint8_t* col = s.row(t);
+        double sum_sq = 0.0;
+        for (int64_t r = 0; r < s.rows(); ++r) {
+            const int code = code_at(col, s.sample(r));
+            if (code == 1) continue;
+            const double z = (static_cast<double>(kDosage[code]) - mean[j]) * inv_std[j];
+            sum_sq += z * z;
+        }
+        total += sum_sq;
+    }
+    return (1.0 / static_cast<double>(s.cols())) * total;
+}
+
+void orc_kinship_diagonal(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                          const double* mean, const double* inv_std,
+                          const int32_t* keep, int64_t n_keep,
+                          const int32_t* variants, int64_t n_var, double* diag) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    const double scaling = 1.0 / static_cast<double>(s.cols());
+    std::fill(diag, diag + s.rows(), 0.0);
+    for (int64_t t = 0; t < s.cols(); ++t) {
+        const int64_t j = s.snp(t);
+        if (inv_std[j] == 0.0) continue;
+        const uint8_t* col = s.row(t);
+        for (int64_t r = 0; r < s.rows(); ++r) {
+            const int code = code_at(col, keep ? keep[r] : r);
+            if (code == 1) continue;
+            const double z = (static_cast<double>(kDosage[code]) - mean[j]) * inv_std[j];
+            diag[r] += scaling * z * z;
+        }
+    }
+}
+
+void orc_dense_z(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                 const double* mean, const double* inv_std,
+                 const int32_t* keep, int64_t n_keep,
+                 const int32_t* variants, int64_t n_var, double* z, int64_t ldz) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    for (int64_t t = 0; t < s.cols(); ++t) {
+        const int64_t j = s.snp(t);
+        const uint8_t* col = bed + j * stride;
+        for (int64_t r = 0; r < s.rows(); ++r) {
+            const float dosage = kLookup[code_at(col, keep ? keep[r] : r)];
+            z[r + t * ldz] = std::isnan(dosage) ? 0.0 : (dosage - mean[j]) * inv_std[j];
+        }
+    }
+}
+
+void orc_kinship_batch_fixture(int n, int m, uint64_t seed, uint8_t* bed_out,
+                               int n_sel, const int32_t* rows, int n_widths,
+                               const int32_t* widths, double* omega_out) {
+    std::mt19937_64 rng(seed);
+    const int stride = (n + 3) / 4;
+    bed_out[0] = 0x6c;
+    bed_out[1] = 0x1b;
+    bed_out[2] = 0x01;
+    for (int j = 0; j < m; ++j)
+        for (int b = 0; b < stride; ++b) {
+            unsigned char byte = 0;
+            for (int k = 0; k < 4; ++k) {
+                const unsigned char code = j % 31 == 0 ? 3 : j % 37 == 0 ? 1 : rng() % 4;
+                byte |= code << (2 * k);
+            }
+            bed_out[3 + static_cast<size_t>(j) * stride + b] = byte;
+        }
+    if (!omega_out) return;
+    size_t off = 0;
+    for (int s = 0; s < n_sel; ++s)
+        for (int w = 0; w < n_widths; ++w) {
+            std::normal_distribution<double> normal;
+            for (int j = 0; j < widths[w]; ++j)
+                for (int i = 0; i < rows[s]; ++i) omega_out[off++] = normal(rng);
+        }
+}
+
+void orc_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out) {
+    std::mt19937_64 generator(seed);
+    std::normal_distribution<double> normal(0.0, 1.0);
+    for (int64_t j = 0; j < cols; ++j)
+        for (int64_t i = 0; i < n; ++i) out[i + j * n] = normal(generator);
+}
+
+int orc_prepare_marker(const double* raw, int64_t n, double min_maf, double* values,
+                       double* freq, int32_t* observed_out) {
+    double dosage_sum = 0.0;
+    int observed = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (std::isnan(raw[i])) continue;
+        dosage_sum += raw[i];
+        ++observed;
+    }
+    *observed_out = observed;
+    *freq = 0.0;
+    if (observed == 0) return 0;
+    const double af = dosage_sum / (2.0 * observed);
+    *freq = af;
+    const int passes = observed >= 3 && std::min(af, 1.0 - af) >= min_maf;
+    double encoded_sum = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        values[i] = raw[i];
+        if (std::isfinite(values[i])) encoded_sum += values[i];
+    }
+    const double encoded_mean = encoded_sum / observed;
+    for (int64_t i = 0; i < n; ++i) {
+        if (!std::isfinite(values[i])) values[i] = encoded_mean;
+        values[i] -= encoded_mean;
+    }
+    return passes;
+}
+
+double orc_chisq_prob(double stat, int df) {
+    if (stat <= 0) return 1.0;
+    return gamma_q(df / 2.0, stat / 2.0);
+}
+
+int orc_lowrank_reml(const double* U, const double* lam, int64_t n, int64_t rank, double r0,
+                     const double* y, const double* X, int64_t p, orc_lowrank_result* res) {
+    const int64_t df = n - p;
+    if (df <= 0) return -1;
+    // apply_ratio_inverse(eta, rhs) = base*rhs + U diag(1/(1+eta*lambda) - base) U^T rhs
+    auto ratio_inverse = [&](double eta, const double* rhs, int64_t cols, double* out) {
+        const double base = 1.0 / (1.0 + eta * r0);
+        std::vector<double> utr(rank * cols, 0.0);
+        for (int64_t c = 0; c < cols; ++c)
+            for (int64_t j = 0; j < rank; ++j) {
+                double acc = 0.0;
+                for (int64_t i = 0; i < n; ++i) acc += U[i + j * n] * rhs[i + c * n];
+                utr[j + c * rank] = acc * (1.0 / (1.0 + eta * lam[j]) - base);
+            }
+        for (int64_t c = 0; c < cols; ++c)
+            for (int64_t i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int64_t j = 0; j < rank; ++j) acc += U[i + j * n] * utr[j + c * rank];
+                out[i + c * n] = base * rhs[i + c * n] + acc;
+            }
+    };
+    auto objective = [&](double log_eta, double* quadratic) {
+        const double eta = std::exp(log_eta);
+        std::vector<double> rx(n * p), info(p * p), ry(n), beta(p), resid(n), rr(n);
+        ratio_inverse(eta, X, p, rx.data());
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) {
+                double acc = 0.0;
+                for (int64_t i = 0; i < n; ++i) acc += X[i + a * n] * rx[i + b * n];
+                info[a + b * p] = acc;
+            }
+        std::vector<double> L, D;
+        if (!ldlt(info.data(), p, L, D)) return std::numeric_limits<double>::infinity();
+        ratio_inverse(eta, y, 1, ry.data());
+        for (int64_t a = 0; a < p; ++a) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += X[i + a * n] * ry[i];
+            beta[a] = acc;
+        }
+        ldlt_solve(L, D, p, beta.data());
+        for (int64_t i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int64_t a = 0; a < p; ++a) acc += X[i + a * n] * beta[a];
+            resid[i] = y[i] - acc;
+        }
+        ratio_inverse(eta, resid.data(), 1, rr.data());
+        double qf = 0.0;
+        for (int64_t i = 0; i < n; ++i) qf += resid[i] * rr[i];
+        if (!(qf > 0.0) || !std::isfinite(qf)) return std::numeric_limits<double>::infinity();
+        if (quadratic) *quadratic = qf;
+        double logdet_r = (n - rank) * std::log1p(eta * r0);
+        for (int64_t j = 0; j < rank; ++j) logdet_r += std::log(1.0 + eta * lam[j]);
+        double logdet_x = 0.0;
+        for (int64_t a = 0; a < p; ++a) logdet_x += std::log(std::max(std::abs(D[a]), 1e-300));
+        return logdet_r + logdet_x + df * std::log(qf / static_cast<double>(df));
+    };
+    const int grid = 81;
+    int best_index = 0;
+    double best_log_eta = -12.0;
+    double best_obj = objective(best_log_eta, nullptr);
+    for (int i = 1; i < grid; ++i) {
+        const double cand = -12.0 + 24.0 * i / static_cast<double>(grid - 1);
+        const double v = objective(cand, nullptr);
+        if (v < best_obj) {
+            best_obj = v;
+            best_log_eta = cand;
+            best_index = i;
+        }
+    }
+    double left = -12.0 + 24.0 * std::max(0, best_index - 1) / static_cast<double>(grid - 1);
+    double right = -12.0 + 24.0 * std::min(grid - 1, best_index + 1) / static_cast<double>(grid - 1);
+    const double golden = (std::sqrt(5.0) - 1.0) / 2.0;
+    double c = right - golden * (right - left), d = left + golden * (right - left);
+    double fc = objective(c, nullptr), fd = objective(d, nullptr);
+    for (int it = 0; it < 80 && right - left > 1e-8; ++it) {
+        if (fc < fd) {
+            right = d; d = c; fd = fc; c = right - golden * (right - left);
+            fc = objective(c, nullptr);
+        } else {
+            left = c; c = d; fc = fd; d = left + golden * (right - left);
+            fd = objective(d, nullptr);
+        }
+    }
+    best_log_eta = 0.5 * (left + right);
+    double quadratic = 0.0;
+    best_obj = objective(best_log_eta, &quadratic);
+    if (!std::isfinite(best_obj)) return -2;
+    res->best_log_eta = best_log_eta;
+    res->best_objective = best_obj;
+    res->delta = std::exp(-best_log_eta);
+    res->sigma2_e = quadratic / static_cast<double>(df);
+    res->sigma2_g = std::exp(best_log_eta) * res->sigma2_e;
+    return 0;
+}
+
+int orc_lowrank_prepare(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                        const double* mean, const double* inv_std,
+                        const int32_t* keep, int64_t n_keep,
+                        const int32_t* variants, int64_t n_var,
+                        const double* y, const double* X, int64_t p,
+                        int rank, int oversample, uint64_t seed,
+                        double trace_threshold, int min_rank, int n_threads,
+                        double* U_out, double* lambda_out, orc_lowrank_result* res) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    const int64_t n = s.rows();
+    if (rank <= 0 || rank >= n) return -1;
+    const int64_t sk = std::min<int64_t>(n, rank + std::max(0, oversample));
+    std::vector<double> omega(n * sk), sample(n * sk), q(n * sk);
+    orc_normal_matrix(seed, n, sk, omega.data());
+    auto apply = [&](const double* in, double* out) {
+        orc_kinship_apply_block(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var,
+                                in, n, sk, out, n, n_threads);
+    };
+    apply(omega.data(), sample.data());
+    for (int it = 0; it < 2; ++it) {
+        q = sample;
+        householder_thin_q(q.data(), n, sk);
+        apply(q.data(), sample.data());
+    }
+    q = sample;
+    householder_thin_q(q.data(), n, sk);
+    std::vector<double> kq(n * sk), small(sk * sk);
+    apply(q.data(), kq.data());
+#pragma omp parallel for schedule(static) collapse(2)
+    for (int64_t b = 0; b < sk; ++b)
+        for (int64_t a = 0; a < sk; ++a) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += q[i + a * n] * kq[i + b * n];
+            small[a + b * sk] = acc;
+        }
+    std::vector<double> evals(sk), evecs(sk * sk);
+    jacobi_eigh(small.data(), sk, evals.data(), evecs.data());
+    std::vector<double> lead(rank);
+    for (int j = 0; j < rank; ++j) lead[j] = std::max(0.0, evals[sk - 1 - j]);
+    const double total_trace = orc_kinship_trace(bed, n_fam, stride, mean, inv_std, keep, n_keep,
+                                                 variants, n_var);
+    int selected = rank;
+    bool met = trace_threshold <= 0.0;
+    if (trace_threshold > 0.0 && total_trace > 0.0) {
+        double retained = 0.0;
+        const int first_allowed = std::min(rank, std::max(1, min_rank));
+        for (int j = 0; j < rank; ++j) {
+            retained += lead[j];
+            if (j + 1 >= first_allowed && retained / total_trace >= trace_threshold) {
+                selected = j + 1;
+                met = true;
+                break;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < selected; ++j) {
+        const int64_t src = sk - 1 - j;
+        for (int64_t i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int64_t a = 0; a < sk; ++a) acc += q[i + a * n] * evecs[a + src * sk];
+            U_out[i + j * n] = acc;
+        }
+    }
+    double lam_sum = 0.0, lam_sq = 0.0;
+    for (int j = 0; j < selected; ++j) {
+        lambda_out[j] = lead[j];
+        lam_sum += lead[j];
+        lam_sq += lead[j] * lead[j];
+    }
+    const double r0 = std::max(0.0, (total_trace - lam_sum) / static_cast<double>(n - selected));
+    const double approx_sq = lam_sq + (n - selected) * r0 * r0;
+    double cross = r0 * total_trace;
+    for (int j = 0; j < selected; ++j) cross += (lead[j] - r0) * lead[j];
+    const double resid_sq = std::max(0.0, total_trace * total_trace + approx_sq - 2.0 * cross);
+    res->rank = selected;
+    res->sketch_size = static_cast<int32_t>(sk);
+    res->residual_eigenvalue = r0;
+    res->relative_frobenius_error =
+        std::sqrt(resid_sq) / std::max(total_trace, std::numeric_limits<double>::min());
+    res->trace = total_trace;
+    res->trace_fraction = total_trace > 0.0 ? lam_sum / total_trace : 0.0;
+    res->trace_threshold_met = met;
+    return orc_lowrank_reml(U_out, lambda_out, n, selected, r0, y, X, p, res);
+}
+
+int orc_scan_lowrank(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
+                     const int32_t* keep, int64_t n,
+                     const double* U, const double* lam, int64_t rank, double r0,
+                     double sg2, double se2,
+                     const double* y, const double* X, int64_t p, double min_maf,
+                     double* beta_out, double* se_out, double* pval_out, double* log10p_out,
+                     double* freq_out, int32_t* tested) {
+    (void)n_fam;
+    // applyLowRankVinv, src/lmm_engine.cpp:1097-1105
+    const double base = 1.0 / std::max(1e-12, sg2 * r0 + se2);
+    std::vector<double> corr(rank);
+    for (int64_t j = 0; j < rank; ++j) corr[j] = 1.0 / (sg2 * lam[j] + se2) - base;
+    auto vinv = [&](const double* rhs, double* out) {
+        std::vector<double> t(rank);
+        for (int64_t j = 0; j < rank; ++j) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += U[i + j * n] * rhs[i];
+            t[j] = acc * corr[j];
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int64_t j = 0; j < rank; ++j) acc += U[i + j * n] * t[j];
+            out[i] = base * rhs[i] + acc;
+        }
+    };
+    // :1273-1285 null quantities
+    std::vector<double> vx(n * p), info(p * p), info_inv(p * p), vy(n), beta(p), resid(n), py(n);
+    for (int64_t a = 0; a < p; ++a) vinv(X + a * n, vx.data() + a * n);
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t b = 0; b < p; ++b) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += X[i + a * n] * vx[i + b * n];
+            info[a + b * p] = acc;
+        }
+    std::vector<double> L, D;
+    if (!ldlt(info.data(), p, L, D)) return -1;
+    for (int64_t c = 0; c < p; ++c) {
+        std::vector<double> e(p, 0.0);
+        e[c] = 1.0;
+        ldlt_solve(L, D, p, e.data());
+        for (int64_t r = 0; r < p; ++r) info_inv[r + c * p] = e[r];
+    }
+    vinv(y, vy.data());
+    for (int64_t a = 0; a < p; ++a) {
+        double acc = 0.0;
+        for (int64_t b = 0; b < p; ++b) {
+            double xb = 0.0;
+            for (int64_t i = 0; i < n; ++i) xb += X[i + b * n] * vy[i];
+            acc += info_inv[a + b * p] * xb;
+        }
+        beta[a] = acc;
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int64_t a = 0; a < p; ++a) acc += X[i + a * n] * beta[a];
+        resid[i] = y[i] - acc;
+    }
+    vinv(resid.data(), py.data());
+    // per-marker (:1337-1358), then the block formulas of :1309-1320
+    std::vector<double> raw(n), g(n), vg(n), xvg(p), mid(p);
+#pragma omp parallel for schedule(dynamic, 16) firstprivate(raw, g, vg, xvg, mid)
+    for (int64_t j = 0; j < n_snps; ++j) {
+        tested[j] = 0;
+        const uint8_t* row = bed + j * stride;
+        for (int64_t i = 0; i < n; ++i) {
+            const int code = code_at(row, keep[i]);
+            raw[i] = code == 1 ? std::numeric_limits<double>::quiet_NaN()
+                               : (code == 0 ? 2.0 : (code == 2 ? 1.0 : 0.0));
+        }
+        double f = 0.0;
+        int32_t obs = 0;
+        if (!orc_prepare_marker(raw.data(), n, min_maf, g.data(), &f, &obs)) continue;
+        vinv(g.data(), vg.data());
+        double score = 0.0, var = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            score += g[i] * py[i];
+            var += g[i] * vg[i];
+        }
+        for (int64_t a = 0; a < p; ++a) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += X[i + a * n] * vg[i];
+            xvg[a] = acc;
+        }
+        for (int64_t a = 0; a < p; ++a) {
+            double acc = 0.0;
+            for (int64_t b = 0; b < p; ++b) acc += info_inv[a + b * p] * xvg[b];
+            mid[a] = acc;
+        }
+        for (int64_t a = 0; a < p; ++a) var -= xvg[a] * mid[a];
+        if (!(var > 1e-12) || !std::isfinite(var)) continue;
+        const double stat = score / std::sqrt(var);
+        const double pv = orc_chisq_prob(stat * stat, 1);
+        tested[j] = 1;
+        freq_out[j] = f;
+        beta_out[j] = score / var;
+        se_out[j] = 1.0 / std::sqrt(var);
+        pval_out[j] = pv;
+        log10p_out[j] = pv > 0.0 ? -std::log10(pv) : 300.0;
+    }
+    return 0;
+}
+
+int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                  const double* mean, const double* inv_std,
+                  const int32_t* keep, int64_t n_keep,
+                  const int32_t* variants, int64_t n_var,
+                  double sg2, double se2, const double* b, double tol, int max_iter,
+                  double* x) {
+    Selection s = make_selection(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var);
+    const int64_t n = s.rows();
+    auto mult = [&](const double* v, double* out) {
+        std::vector<double> kv(n);
+        orc_kinship_apply_vector(bed, n_fam, stride, mean, inv_std, keep, n_keep, variants, n_var,
+                                 v, kv.data(), 1);
+        for (int64_t i = 0; i < n; ++i) out[i] = sg2 * kv[i] + se2 * v[i];
+    };
+    const double precond = 1.0 / (sg2 + se2);
+    std::vector<double> r(n), z(n), pdir(n), ap(n);
+    std::fill(x, x + n, 0.0);
+    mult(x, ap.data());
+    double rn = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        r[i] = b[i] - ap[i];
+        rn += r[i] * r[i];
+    }
+    if (std::sqrt(rn) < 1e-20) return 0;
+    double rsold = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        z[i] = r[i] * precond;
+        pdir[i] = z[i];
+        rsold += r[i] * z[i];
+    }
+    for (int it = 0; it < max_iter; ++it) {
+        mult(pdir.data(), ap.data());
+        double pap = 0.0;
+        for (int64_t i = 0; i < n; ++i) pap += pdir[i] * ap[i];
+        const double alpha = rsold / pap;
+        rn = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] += alpha * pdir[i];
+            r[i] -= alpha * ap[i];
+            rn += r[i] * r[i];
+        }
+        if (std::sqrt(rn) < tol) return it + 1;
+        double rsnew = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            z[i] = r[i] * precond;
+            rsnew += r[i] * z[i];
+        }
+        for (int64_t i = 0; i < n; ++i) pdir[i] = z[i] + (rsnew / rsold) * pdir[i];
+        rsold = rsnew;
+    }
+    return max_iter;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+/*
+ * CPU oracle for the matrix-free mixed-model path — TEST INFRASTRUCTURE ONLY.
+ *
+ * This library restates, in plain loops over FP64, the reference CosmicScanner
+ * algorithms that the CUDA library replaces.  It exists so the tests (and the
+ * CPU-baseline leg of bench.py) can check the GPU results on the same inputs.
+ * Nothing in the product links or calls it.
+ *
+ * Parity status: the kinship-operator restatement is pinned against the
+ * reference's own known-answer recipe (tests/test_kinship_batch.cpp: dense
+ * Z Z^T / M within 1e-10, trace, empty RHS, bad dimensions), regenerated here
+ * byte-for-byte from the same mt19937_64 seed.  The sketch / REML / scan
+ * restatements have no golden outputs in the reference (Eigen is not available
+ * in this container, so the reference cannot be built): parity unpinned for
+ * those, beyond agreement with an independent dense FP64 computation.
+ *
+ * Matrices are column-major with explicit leading dimensions, like Eigen's
+ * default storage in the reference.  `bed` always points at the first SNP row
+ * (the 3 magic bytes already skipped); row j starts at bed + j*stride.
+ */
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* libCosmicCore/src/plink_reader.cpp:187-239 (PlinkReader::computeStats). */
+void orc_compute_stats(const uint8_t* bed, int64_t n_samples, int64_t n_snps, int64_t stride,
+                       double* mean, double* inv_std, int32_t* count, double* sum);
+
+/* src/kinship_operator.cpp:74-218: multiplyZt + multiplyZ + scaling (vector apply).
+ * keep == NULL means all samples; variants == NULL means all SNPs.
+ * n_threads reproduces the per-worker buffers reduced in worker order. */
+int orc_kinship_apply_vector(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                             const double* mean, const double* inv_std,
+                             const int32_t* keep, int64_t n_keep,
+                             const int32_t* variants, int64_t n_var,
+                             const double* v, double* out, int n_threads);
+
+/* src/kinship_operator.cpp:225-302 (apply_block): 512-SNP decode to FP64 z, z^T X, z*proj. */
+int orc_kinship_apply_block(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                            const double* mean, const double* inv_std,
+                            const int32_t* keep, int64_t n_keep,
+                            const int32_t* variants, int64_t n_var,
+                            const double* X, int64_t ldx, int64_t k,
+                            double* out, int64_t ldo, int n_threads);
+
+/* src/kinship_operator.cpp:306-368 */
+double orc_kinship_trace(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                         const double* mean, const double* inv_std,
+                         const int32_t* keep, int64_t n_keep,
+                         const int32_t* variants, int64_t n_var);
+void orc_kinship_diagonal(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                          const double* mean, const double* inv_std,
+                          const int32_t* keep, int64_t n_keep,
+                          const int32_t* variants, int64_t n_var, double* diag);
+
+/* Dense Z (rows x numVariants, column-major) exactly as tests/test_kinship_batch.cpp:61-72
+ * builds it from float dosages: z = (dosage - mean) * inv_std, NaN -> 0. */
+void orc_dense_z(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                 const double* mean, const double* inv_std,
+                 const int32_t* keep, int64_t n_keep,
+                 const int32_t* variants, int64_t n_var, double* z, int64_t ldz);
+
+/* The fixture of tests/test_kinship_batch.cpp:26-43: writes 3 + m*ceil(n/4) BED bytes
+ * (magic included) into bed_out, drawn from mt19937_64(seed); then continues the SAME
+ * engine to draw the omega matrices of the test's loop (:47-80): for each of the
+ * n_sel selections with rows[s] rows, for each width in widths[0..n_widths), a fresh
+ * std::normal_distribution draws width*rows values column by column.  Writes them
+ * consecutively to omega_out (may be NULL to skip). */
+void orc_kinship_batch_fixture(int n, int m, uint64_t seed, uint8_t* bed_out,
+                               int n_sel, const int32_t* rows, int n_widths,
+                               const int32_t* widths, double* omega_out);
+
+/* n*cols standard normals from mt19937_64(seed) and one std::normal_distribution<double>,
+ * filled column by column (src/lmm_engine.cpp:917-922). */
+void orc_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out);
+
+/* src/genetics/genotype_encoding.h:33-81, additive model, HWE disabled.
+ * raw: n values, NaN = missing.  Writes centred values; returns passes_maf. */
+int orc_prepare_marker(const double* raw, int64_t n, double min_maf, double* values,
+                       double* freq, int32_t* observed);
+
+/* src/lmm_engine.cpp:22-64 */
+double orc_chisq_prob(double stat, int df);
+
+/* Low-rank matrix-free null model, src/lmm_engine.cpp:897-1095.
+ * Inputs: the operator's selection, y (n), X (n x p, column-major, already FP32-rounded
+ * by the caller when mirroring the reference's MatrixXf covariates).
+ * Outputs: U (n x rank_out, ld n; caller provides n*rank), lambda (rank), scalars. */
+typedef struct {
+    int32_t rank;            /* selected rank */
+    int32_t sketch_size;
+    double residual_eigenvalue;
+    double relative_frobenius_error;
+    double trace;
+    double trace_fraction;
+    int32_t trace_threshold_met;
+    double sigma2_g, sigma2_e, delta, best_log_eta, best_objective;
+} orc_lowrank_result;
+
+int orc_lowrank_prepare(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                        const double* mean, const double* inv_std,
+                        const int32_t* keep, int64_t n_keep,
+                        const int32_t* variants, int64_t n_var,
+                        const double* y, const double* X, int64_t p,
+                        int rank, int oversample, uint64_t seed,
+                        double trace_threshold, int min_rank, int n_threads,
+                        double* U_out, double* lambda_out, orc_lowrank_result* res);
+
+/* Low-rank REML search only (grid + golden), given a basis: src/lmm_engine.cpp:1010-1073. */
+int orc_lowrank_reml(const double* U, const double* lambda, int64_t n, int64_t rank, double r0,
+                     const double* y, const double* X, int64_t p, orc_lowrank_result* res);
+
+/* src/lmm_engine.cpp:1269-1361 (scanLowRank) for all SNPs of the reader, no chromosome
+ * filter.  keep lists the analysed samples (n entries).  Per-SNP outputs (n_snps each);
+ * tested[j] = 1 when the SNP produced a row. */
+int orc_scan_lowrank(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
+                     const int32_t* keep, int64_t n,
+                     const double* U, const double* lambda, int64_t rank, double r0,
+                     double sigma2_g, double sigma2_e,
+                     const double* y, const double* X, int64_t p, double min_maf,
+                     double* beta, double* se, double* pval, double* log10p,
+                     double* freq, int32_t* tested);
+
+/* libCosmicCore/src/matrix_free_pcg.h:20-68 on the operator A = sg2*K + se2*I with the
+ * scalar preconditioner 1/(sg2+se2); absolute stopping ||r|| < tol.  Returns iterations. */
+int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
+                  const double* mean, const double* inv_std,
+                  const int32_t* keep, int64_t n_keep,
+                  const int32_t* variants, int64_t n_var,
+                  double sg2, double se2, const double* b, double tol, int max_iter,
+                  double* x);
+
+#ifdef __cplusplus
+}
+#endif

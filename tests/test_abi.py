@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every function the public header declares (no GPU)."""
+import ctypes
+import os
+import subprocess
+
+from cosmicscanner_b200 import _abi
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _abi.load()
+    declared = _abi.declared_functions()
+    assert len(declared) >= 19
+    missing = [name for name in declared if not hasattr(lib, name)]
+    assert not missing, missing
+    # every declared function also has a ctypes signature in the Python binding
+    assert sorted(_abi._SIGNATURES) == declared
+
+
+def test_exported_symbols_are_c_linkage():
+    out = subprocess.run(["nm", "-D", "--defined-only", _abi.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    for name in _abi.declared_functions():
+        assert name in exported, name
+
+
+def test_version_and_error_without_device_work():
+    lib = _abi.load()
+    assert b"sm_100a" in lib.cs_version()
+    # argument validation happens before any device work
+    handle = ctypes.c_void_p()
+    rc = lib.cs_genotypes_create(None, 0, 4, 1, ctypes.byref(handle))
+    assert rc == _abi.CS_ERR_FORMAT
+    assert b"too small" in lib.cs_last_error()
+    bad = (ctypes.c_uint8 * 4)(0x6C, 0x1B, 0x00, 0)
+    rc = lib.cs_genotypes_create(bad, 4, 4, 1, ctypes.byref(handle))
+    assert rc == _abi.CS_ERR_FORMAT
+    assert b"SNP-major" in lib.cs_last_error()
+    rc = lib.cs_genotypes_create(bad, 4, 0, 1, ctypes.byref(handle))
+    assert rc == _abi.CS_ERR_INVALID_ARGUMENT
+
+
+def test_package_fails_loudly_without_library(tmp_path):
+    missing = os.path.join(tmp_path, "nope.so")
+    try:
+        _abi.load(missing)
+    except RuntimeError as e:
+        assert "no CPU fallback" in str(e)
+    else:
+        raise AssertionError("load of a missing library must raise")

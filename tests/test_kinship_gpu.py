@@ -1,0 +1,103 @@
+"""GPU kinship operator against the CPU oracle (the reference's batch-equivalence checks).
+
+Mirrors tests/test_kinship_batch.cpp of the reference: the regenerated 37 x 1031 fixture,
+six selections, RHS widths 1/7/41, relative error < 1e-10 against the dense Z Z^T / M,
+transpose == apply, aliasing, bitwise repeatability, trace, empty RHS, bad dimensions.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.test_oracle import M, N, compare, selections
+
+pytestmark = pytest.mark.gpu
+
+cs = pytest.importorskip("cosmicscanner_b200")
+
+
+@pytest.fixture(scope="module")
+def fixture():
+    sels = selections()
+    rows = [N if k is None else len(k) for k, _ in sels]
+    bed, omega = oracle.kinship_batch_fixture(N, M, 8128, rows=rows)
+    ref = oracle.Bed(bed[3:].reshape(M, -1), N)
+    g = cs.Genotypes.from_bed_bytes(bed, N, M)
+    return bed, omega, sels, rows, ref, g
+
+
+def test_stats_bit_exact(fixture):
+    *_, ref, g = fixture
+    st = g.stats()
+    assert np.array_equal(st["mean"], ref.mean)
+    assert np.array_equal(st["inv_std"], ref.inv_std)
+    assert np.array_equal(st["count"], ref.count)
+    assert np.array_equal(st["sum"], ref.sum)
+
+
+def test_batch_equivalence(fixture):
+    bed, omega, sels, rows, ref, g = fixture
+    off = 0
+    for (keep, snps), r in zip(sels, rows):
+        op = cs.createKinshipOperator(g, keep, snps)
+        assert op.rows() == r and op.cols() == r
+        assert op.numVariants() == (M if snps is None else len(snps))
+        z = ref.dense_z(keep, snps)
+        K = z @ z.T / z.shape[1]
+        assert abs(op.trace() - np.trace(K)) < 1e-10
+        compare(op.getDiagonal(), np.diag(K))
+        for w in (1, 7, 41):
+            om = omega[off:off + r * w].reshape(w, r).T
+            off += r * w
+            res = op.apply(om)
+            compare(res, K @ om)
+            compare(res, ref.apply_block(om, keep, snps))
+            vec = op.apply(om[:, 0])
+            compare(vec, K @ om[:, 0])
+            compare(op.applyTranspose(om[:, 0]), vec)
+            again = op.apply(om)
+            assert np.array_equal(again, res), "repeat is not bitwise deterministic"
+        empty = op.apply(np.zeros((r, 0)))
+        assert empty.shape == (r, 0)
+        with pytest.raises(cs.InvalidArgument):
+            op.apply(np.zeros((r + 1, 1)))
+
+
+def test_device_alias_and_wide_rhs(fixture):
+    torch = pytest.importorskip("torch")
+    bed, omega, sels, rows, ref, g = fixture
+    op = cs.createKinshipOperator(g)
+    rng = np.random.default_rng(7)
+    for k in (1, 3, 8, 20, 33, 64, 65, 130, 266):
+        X = rng.standard_normal((N, k))
+        expect = ref.apply_block(X)
+        t = torch.tensor(X.T.copy(), device="cuda")  # row-major (k, N) == column-major (N, k)
+        op.apply_device(t.data_ptr(), N, k, t.data_ptr(), N)  # Y aliases X
+        torch.cuda.synchronize()
+        compare(t.cpu().numpy().T, expect)
+
+
+def test_selection_errors(fixture):
+    *_, g = fixture
+    with pytest.raises(cs.InvalidArgument):
+        cs.createKinshipOperator(g, [0, N])
+    with pytest.raises(cs.InvalidArgument):
+        cs.createKinshipOperator(g, None, [M])
+    with pytest.raises(cs.InvalidArgument):
+        cs.createKinshipOperator(g, None, [-1])
+
+
+def test_larger_random_matrix():
+    synth = pytest.importorskip("cosmicscanner_b200.synth")
+    d = synth.cohort(1500, 4000, 11, missing=0.02)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    rng = np.random.default_rng(3)
+    keep = np.sort(rng.choice(d["n"], 1100, replace=False))
+    variants = np.arange(0, d["m"], 2)
+    for kp, vp in ((None, None), (keep, variants)):
+        op = cs.createKinshipOperator(g, kp, vp)
+        X = rng.standard_normal((op.rows(), 70))
+        compare(op.apply(X), ref.apply_block(X, kp, vp, n_threads=8))
+        assert abs(op.trace() - ref.trace(kp, vp)) < 1e-9 * abs(ref.trace(kp, vp))

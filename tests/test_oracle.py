@@ -1,0 +1,111 @@
+"""The CPU oracle against the reference's own known-answer checks (no GPU).
+
+tests/test_kinship_batch.cpp of the reference builds a 37 x 1031 BED fixture from
+mt19937_64(8128), runs six sample/variant selections, and requires the matrix-free
+operator to equal the dense Z Z^T / M within 1e-10 (plus trace, empty RHS and bad
+dimensions).  The fixture is regenerated byte-for-byte by the oracle (same engine,
+same draw order) and the same checks pin the oracle's restatement.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+N, M = 37, 1031
+SUBSET = [35, 1, 20, 3, 4, 31, 7, 8, 10, 12, 14, 16, 18, 22, 24, 26, 28, 30, 32, 34]
+
+
+def selections():
+    identity = list(range(N))
+    permuted = [N - 1 - i for i in range(N)]
+    repeated = [i // 2 for i in range(N)]
+    variants = [j for j in range(M) if j % 3 != 1]
+    out = []
+    for s in range(6):
+        keep = SUBSET if s == 1 else identity if s == 3 else permuted if s == 4 else \
+            repeated if s == 5 else None
+        out.append((keep, None if s == 0 else variants))
+    return out
+
+
+@pytest.fixture(scope="module")
+def fixture():
+    sels = selections()
+    rows = [N if k is None else len(k) for k, _ in sels]
+    bed, omega = oracle.kinship_batch_fixture(N, M, 8128, rows=rows)
+    return bed, omega, sels, rows
+
+
+def compare(actual, expected):
+    rel = np.abs(actual - expected).max() / max(1e-30, np.abs(expected).max())
+    scaled = (np.abs(actual - expected) / (1.0 + np.abs(expected))).max()
+    assert rel < 1e-10 and scaled < 1e-10, (rel, scaled)
+
+
+def test_fixture_bytes(fixture):
+    bed, omega, _, rows = fixture
+    assert bed[:3].tolist() == [0x6C, 0x1B, 0x01]
+    assert len(bed) == 3 + M * ((N + 3) // 4)
+    rowsb = bed[3:].reshape(M, -1)
+    assert (rowsb[0] == 0xFF).all()            # j % 31 == 0 -> code 3 everywhere
+    assert (rowsb[37] == 0x55).all()           # j % 37 == 0 -> all missing
+    assert len(omega) == sum(r * w for r in rows for w in (1, 7, 41))
+    assert np.isfinite(omega).all() and abs(omega.mean()) < 0.05
+
+
+def test_stats_by_hand(fixture):
+    bed = fixture[0]
+    B = oracle.Bed(bed[3:].reshape(M, -1), N)
+    assert B.inv_std[0] == 0.0 and B.mean[0] == 0.0      # all hom A2: monomorphic
+    assert B.inv_std[37] == 0.0 and B.mean[37] == 0.0    # all missing
+    j = 1
+    row = bed[3:].reshape(M, -1)[j]
+    codes = [(row[i // 4] >> (2 * (i % 4))) & 3 for i in range(N)]
+    dos = [{0: 2.0, 2: 1.0, 3: 0.0}[c] for c in codes if c != 1]
+    mean = sum(dos) / len(dos)
+    p = mean / 2.0
+    assert B.mean[j] == mean
+    assert B.inv_std[j] == 1.0 / np.sqrt(2.0 * p * (1.0 - p))
+    assert B.count[j] == len(dos)
+
+
+def test_operator_matches_dense(fixture):
+    bed, omega, sels, rows = fixture
+    B = oracle.Bed(bed[3:].reshape(M, -1), N)
+    off = 0
+    for (keep, snps), r in zip(sels, rows):
+        z = B.dense_z(keep, snps)
+        K = z @ z.T / z.shape[1]
+        assert abs(B.trace(keep, snps) - np.trace(K)) < 1e-10
+        compare(B.diagonal(keep, snps), np.diag(K))
+        for w in (1, 7, 41):
+            om = omega[off:off + r * w].reshape(w, r).T
+            off += r * w
+            blk = B.apply_block(om, keep, snps, n_threads=4)
+            compare(blk, K @ om)
+            for threads in (1, 2, 4, 8):
+                vec = B.apply_vector(om[:, 0], keep, snps, n_threads=threads)
+                compare(vec, K @ om[:, 0])
+            again = B.apply_vector(om[:, 0], keep, snps, n_threads=4)
+            assert (again == B.apply_vector(om[:, 0], keep, snps, n_threads=4)).all()
+
+
+def test_chisq_prob_matches_regularised_gamma():
+    scipy = pytest.importorskip("scipy.special")
+    for stat in (1e-6, 0.01, 0.5, 1.0, 3.84, 10.0, 30.0, 80.0):
+        ref = scipy.gammaincc(0.5, stat / 2.0)
+        got = oracle.chisq_prob(stat, 1)
+        assert abs(got - ref) <= 2e-6 * ref + 1e-300, (stat, got, ref)
+    assert oracle.chisq_prob(0.0, 1) == 1.0
+    assert oracle.chisq_prob(-1.0, 1) == 1.0
+
+
+def test_prepare_marker():
+    raw = np.array([2.0, np.nan, 1.0, 0.0, 1.0, np.nan, 2.0])
+    ok, vals, freq, obs = oracle.prepare_marker(raw, 0.01)
+    assert ok and obs == 5
+    assert freq == 6.0 / 10.0
+    mean = 6.0 / 5.0
+    assert np.allclose(vals, np.where(np.isnan(raw), 0.0, raw - mean), atol=0)
+    ok, *_ = oracle.prepare_marker(np.array([0.0, 0.0, np.nan]), 0.01)
+    assert not ok                                # fewer than 3 observed / monomorphic
