@@ -170,6 +170,29 @@ def createKinshipOperator(reader: Genotypes, keep_indices=None, variant_indices=
     return KinshipOperator(reader, keep_indices, variant_indices)
 
 
+def profile_enable(on: bool = True):
+    """Starts (and resets) or stops CUDA-event timing of the library's kernels."""
+    _check(_abi.lib().cs_profile_enable(1 if on else 0))
+
+
+def profile_summary() -> dict:
+    """Per kernel name: launches, summed device ms, algorithmic flops and bytes."""
+    import json
+
+    need = C.c_size_t()
+    _check(_abi.lib().cs_profile_summary(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value + 1024)
+    _check(_abi.lib().cs_profile_summary(buf, len(buf), None))
+    return json.loads(buf.value.decode())
+
+
+def launch_count() -> int:
+    """Process-wide number of kernel launches the library has made."""
+    n = C.c_int64()
+    _check(_abi.lib().cs_launch_count(C.byref(n)))
+    return n.value
+
+
 class LowRankDiagnostics(C.Structure):
     _fields_ = [
         ("requested_rank", C.c_int32), ("effective_rank", C.c_int32),
@@ -241,3 +264,39 @@ class LmmEngine:
             self.close()
         except Exception:
             pass
+
+
+def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
+    """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
+    MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""
+    freq = stats["mean"] / 2.0
+    maf = np.minimum(freq, 1.0 - freq)
+    ok = (stats["inv_std"] != 0.0) & ~(maf < min_maf) & ~(np.abs(maf) < 1e-8)
+    return np.nonzero(ok)[0].astype(np.int32)
+
+
+def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=256,
+                        oversample=10, seed=42, trace_threshold=0.95, min_rank=1,
+                        min_maf=0.01, precision="fp64", genotypes: Genotypes | None = None):
+    """The `gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback --no-loco`
+    path (src/gwas_scanner.cpp:121-129, 254-346, 447) from host buffers: upload + stats,
+    GRM variant selection, operator, low-rank REML null model, scan of every SNP.
+    Returns (results dict, diagnostics dict)."""
+    g = genotypes if genotypes is not None else Genotypes.from_bed_bytes(bed, n_samples, n_snps)
+    keep_arr = np.arange(n_samples, dtype=np.int32) if keep is None else np.asarray(keep, np.int32)
+    variants = grm_variant_selection(g.stats(), min_maf)
+    if len(variants) == 0:
+        raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
+                              "Matrix-free GRM selection produced no variants")
+    op = KinshipOperator(g, None if keep is None else keep_arr, variants)
+    rank_eff = max(1, min(rank, op.rows() - 1))
+    eng = LmmEngine()
+    diag = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
+                                        seed=seed, trace_threshold=trace_threshold,
+                                        min_rank=min_rank, precision=precision)
+    res = eng.scan(g, keep_arr, min_maf=min_maf, precision=precision)
+    op.close()
+    eng.close()
+    if genotypes is None:
+        g.close()
+    return res, diag

@@ -1,6 +1,7 @@
 // C ABI: status codes + thread-local error text around the C++ implementation.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <string>
 
@@ -188,5 +189,28 @@ int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t
 }
 
 void cs_lmm_destroy(cs_lmm* lmm) { cs::lmm_destroy(lmm); }
+
+int cs_profile_enable(int on) {
+    return guarded([&] { cs::prof::set_enabled(on != 0); });
+}
+
+int cs_profile_summary(char* buf, size_t len, size_t* needed) {
+    return guarded([&] {
+        const std::string js = cs::prof::summary_json();
+        if (needed) *needed = js.size() + 1;
+        if (buf && len > 0) {
+            const size_t n = std::min(len - 1, js.size());
+            std::memcpy(buf, js.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+int cs_launch_count(int64_t* count) {
+    return guarded([&] {
+        require(count != nullptr, "null argument");
+        *count = cs::prof::launches();
+    });
+}
 
 }  // extern "C"

@@ -152,4 +152,26 @@ void rowmajor_to_colmajor(const double* src, int64_t kp, int64_t n, int64_t k, d
 
 int num_sms();
 
+namespace prof {
+// Counts one kernel launch; with profiling enabled, times it with events on stream s.
+// flops / bytes are the launch's algorithmic work, reported beside the time.
+class Scope {
+   public:
+    Scope(const char* name, cudaStream_t s, double flops = 0.0, double bytes = 0.0);
+    ~Scope();
+    Scope(const Scope&) = delete;
+    Scope& operator=(const Scope&) = delete;
+
+   private:
+    const char* name_;
+    cudaStream_t s_;
+    double flops_, bytes_;
+    cudaEvent_t a_ = nullptr;
+};
+bool enabled();
+void set_enabled(bool on);
+int64_t launches();
+std::string summary_json();
+}  // namespace prof
+
 }  // namespace cs

@@ -155,6 +155,7 @@ int num_sms() {
 void row_code_counts(const cs_packed_view& v, int32_t* d_counts, cudaStream_t s) {
     if (v.n_rows == 0) return;
     const int threads = 256;
+    prof::Scope ps("row_code_counts", s, 0.0, (double)v.n_rows * ((v.n_samples + 3) / 4));
     k_row_code_counts<<<grid_for(v.n_rows * 32, threads), threads, 0, s>>>(v.rows, v.n_rows,
                                                                           v.stride, d_counts);
     CS_LAUNCH("row_code_counts");
@@ -164,6 +165,7 @@ void repack(const uint8_t* src, int64_t src_stride, const int32_t* d_rows, int64
             const int32_t* d_keep, int64_t n_keep, uint8_t* dst, int64_t dst_stride,
             cudaStream_t s) {
     if (n_rows == 0) return;
+    prof::Scope ps("repack", s, 0.0, (double)n_rows * dst_stride);
     k_repack<<<grid_for(n_rows * dst_stride, 256), 256, 0, s>>>(src, src_stride, d_rows, n_rows,
                                                                d_keep, n_keep, dst, dst_stride);
     CS_LAUNCH("repack");
@@ -172,6 +174,7 @@ void repack(const uint8_t* src, int64_t src_stride, const int32_t* d_rows, int64
 void colmajor_to_rowmajor(const double* src, int64_t ld, int64_t n, int64_t k, double* dst,
                           int64_t kp, cudaStream_t s) {
     if (n * kp == 0) return;
+    prof::Scope ps("colmajor_to_rowmajor", s, 0.0, 16.0 * n * kp);
     k_col_to_row<<<grid_for(n * kp, 256), 256, 0, s>>>(src, ld, n, k, dst, kp);
     CS_LAUNCH("colmajor_to_rowmajor");
 }
@@ -179,6 +182,7 @@ void colmajor_to_rowmajor(const double* src, int64_t ld, int64_t n, int64_t k, d
 void rowmajor_to_colmajor(const double* src, int64_t kp, int64_t n, int64_t k, double* dst,
                           int64_t ld, cudaStream_t s) {
     if (n * k == 0) return;
+    prof::Scope ps("rowmajor_to_colmajor", s, 0.0, 16.0 * n * k);
     k_row_to_col<<<grid_for(n * k, 256), 256, 0, s>>>(src, kp, n, k, dst, ld);
     CS_LAUNCH("rowmajor_to_colmajor");
 }
@@ -211,6 +215,7 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
             CS_CUDA(cudaMemcpy2DAsync(g->packed.get(), g->stride, bed + 3, bps, bps, M,
                                       cudaMemcpyHostToDevice, s));
             if (n_samples % 4) {
+                prof::Scope ps("sanitize_tail", s);
                 k_sanitize_tail<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(
                     g->packed.get(), M, g->stride, bps - 1, (int)(n_samples % 4));
                 CS_LAUNCH("sanitize_tail");
@@ -230,6 +235,7 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
             sum.resize(M);
             cs_packed_view v{g->packed.get(), M, n_samples, g->stride};
             row_code_counts(v, counts.get(), s);
+            prof::Scope ps("stats_from_counts", s);
             k_stats_from_counts<<<(unsigned)((M + 255) / 256), 256, 0, s>>>(
                 counts.get(), M, g->d_mean.get(), g->d_inv_std.get(), cnt.get(), sum.get());
             CS_LAUNCH("stats_from_counts");

@@ -34,9 +34,16 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
         n_keep = 0;
     }
     if (variants && n_var > 0) {
-        for (int64_t j = 0; j < n_var; ++j)
+        bool all = (n_var == M);
+        for (int64_t j = 0; j < n_var; ++j) {
             if (variants[j] < 0 || variants[j] >= M)
                 fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: variant index out of range");
+            all = all && variants[j] == j;
+        }
+        if (all) {  // every SNP in file order: the resident matrix serves as is
+            variants = nullptr;
+            n_var = 0;
+        }
     } else {
         variants = nullptr;
         n_var = 0;

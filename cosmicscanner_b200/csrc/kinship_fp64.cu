@@ -260,12 +260,19 @@ void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, in
         kscale = 1.0;
     }
     dim3 grid((unsigned)gx, (unsigned)gy, (unsigned)splits);
-    kern<<<grid, kThreads, smem, s>>>(v.rows, v.n_rows, v.n_samples, v.stride, lut, in, ldi, k,
-                                      dst, ldd, chunk, kscale);
-    CS_LAUNCH(ROWS ? "decode_gemm_rows_fp64" : "decode_gemm_samples_fp64");
+    {
+        // algorithmic work: 2 R K k flops, one pass over the packed rows
+        prof::Scope ps(ROWS ? "decode_gemm_rows_fp64" : "decode_gemm_samples_fp64", s,
+                       2.0 * (double)R * (double)K * (double)k,
+                       (double)v.n_rows * (double)((v.n_samples + 3) / 4));
+        kern<<<grid, kThreads, smem, s>>>(v.rows, v.n_rows, v.n_samples, v.stride, lut, in, ldi,
+                                          k, dst, ldd, chunk, kscale);
+        CS_LAUNCH(ROWS ? "decode_gemm_rows_fp64" : "decode_gemm_samples_fp64");
+    }
     if (splits > 1) {
         const int64_t total = R * k;
         const int blocks = (int)std::min<int64_t>((total + 255) / 256, 32LL * num_sms());
+        prof::Scope ps("reduce_splits", s, 0.0, 8.0 * (double)(splits + 1) * total);
         k_reduce_splits<<<std::max(blocks, 1), 256, 0, s>>>(ws.partial.get(), (int)splits, R, k,
                                                             k, out, ldo, scale);
         CS_LAUNCH("reduce_splits");

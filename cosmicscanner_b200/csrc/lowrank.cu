@@ -90,6 +90,7 @@ void generate_omega(uint64_t seed, int64_t n, int64_t cols, double* d_out, int64
     scratch.resize(2 * pairs);
     CS_CUDA(cudaMemcpyAsync(scratch.get(), xy.data(), 16 * pairs, cudaMemcpyHostToDevice, s));
     const int blocks = (int)std::min<int64_t>((count + 255) / 256, 32LL * num_sms());
+    prof::Scope ps("polar_pairs", s, 0.0, 16.0 * count);
     k_polar_pairs<<<std::max(blocks, 1), 256, 0, s>>>(scratch.get(), count, n, ld, d_out);
     CS_LAUNCH("polar_pairs");
     CS_CUDA(cudaStreamSynchronize(s));  // xy leaves scope
@@ -672,6 +673,7 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
     P.beta = d_beta.get(); P.se = d_se.get(); P.pval = d_p.get(); P.log10p = d_l10.get();
     P.tested = d_tested.get();
     const int blocks = (int)std::min<int64_t>((M * 32 + 255) / 256, 64LL * num_sms());
+    prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
     k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
     CS_LAUNCH("scan_epilogue");
     std::vector<int32_t> t(M);

@@ -122,6 +122,16 @@ int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t
                 double* log10p, double* freq, int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
 
+/* ---------------------------------------------------------------- instrumentation
+ * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and
+ * PlinkKinshipOperator::BlockProfile (src/kinship_operator.h:55-63): a process-wide count
+ * of the library's kernel launches, and optional CUDA-event timing per kernel name with
+ * the algorithmic FLOPs / bytes of each launch.  Enabling resets the records; the summary
+ * (JSON) synchronises the device. */
+int cs_profile_enable(int on);
+int cs_profile_summary(char* buf, size_t len, size_t* needed);
+int cs_launch_count(int64_t* count);
+
 #ifdef __cplusplus
 }
 #endif
