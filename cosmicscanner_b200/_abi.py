@@ -35,6 +35,7 @@ _SIGNATURES = {
     "cs_kinship_info": ([_P, _P, _P], _I),
     "cs_kinship_apply": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
     "cs_kinship_apply_host": ([_P, _P, _I64, _I64, _P, _I64, _I], _I),
+    "cs_kinship_apply_noalloc": ([_P, _P, _I64, _I64, _P, _I64, _P], _I),
     "cs_kinship_trace": ([_P, _P], _I),
     "cs_kinship_diagonal": ([_P, _P], _I),
     "cs_kinship_destroy": ([_P], None),

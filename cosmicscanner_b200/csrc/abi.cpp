@@ -16,6 +16,8 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
 void kinship_apply_colmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                             int64_t ldy, int precision, cudaStream_t s);
 void kinship_diagonal(cs_kinship* op, double* diag_host);
+void kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                           int64_t ldy, cudaStream_t s);
 cs_lmm* lmm_create();
 void lmm_destroy(cs_lmm* l);
 void lmm_prepare_lowrank(cs_lmm* lmm, cs_kinship* op, const double* y, const double* X, int64_t p,
@@ -134,6 +136,14 @@ int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t 
         CS_CUDA(cudaMemcpy2D(dx.get(), n * 8, X, ldx * 8, n * 8, k, cudaMemcpyHostToDevice));
         cs::kinship_apply_colmajor(op, dx.get(), n, k, dx.get(), n, precision, 0);
         CS_CUDA(cudaMemcpy2D(Y, ldy * 8, dx.get(), n * 8, n * 8, k, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cs_kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                             int64_t ldy, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        cs::kinship_apply_noalloc(op, X, ldx, k, Y, ldy, (cudaStream_t)stream);
     });
 }
 

@@ -229,7 +229,8 @@ __global__ void k_reduce_splits(const double* __restrict__ part, int splits, int
 
 template <int BM, int BN, int TM, int TN, bool ROWS>
 void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, int64_t ldi,
-                int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s) {
+                int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s,
+                int64_t max_splits) {
     using C = Cfg<BM, BN, TM, TN>;
     const size_t smem = C::smem_a + C::smem_b + (ROWS ? C::smem_p : 0);
     auto kern = ROWS ? k_rows_fp64<BM, BN, TM, TN> : k_samples_fp64<BM, BN, TM, TN>;
@@ -246,7 +247,7 @@ void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, in
     const int64_t target = 4LL * num_sms();
     int64_t splits = std::max<int64_t>(1, std::min<int64_t>((target + gx * gy - 1) / (gx * gy),
                                                             (K + unit - 1) / unit));
-    splits = std::min<int64_t>(splits, 64);
+    splits = std::min<int64_t>(splits, max_splits);
     int64_t chunk = (K + splits - 1) / splits;
     chunk = round_up(std::max<int64_t>(chunk, 1), ROWS ? 128 : C::SUBK);
     splits = std::max<int64_t>(1, (K + chunk - 1) / chunk);
@@ -281,18 +282,19 @@ void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, in
 
 template <bool ROWS>
 void dispatch(const cs_packed_view& v, const double* lut, const double* in, int64_t ldi,
-              int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s) {
+              int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s,
+              int64_t max_splits = 64) {
     if (k <= 0) return;
     if (k == 1)
-        launch_cfg<256, 1, 1, 1, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        launch_cfg<256, 1, 1, 1, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
     else if (k <= 8)
-        launch_cfg<128, 8, 4, 1, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        launch_cfg<128, 8, 4, 1, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
     else if (k <= 32)
-        launch_cfg<64, 32, 4, 2, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        launch_cfg<64, 32, 4, 2, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
     else if (k <= 64)
-        launch_cfg<64, 64, 4, 4, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        launch_cfg<64, 64, 4, 4, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
     else
-        launch_cfg<64, 128, 4, 8, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        launch_cfg<64, 128, 4, 8, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
 }
 
 }  // namespace
@@ -307,6 +309,22 @@ void decode_gemm_samples_fp64(const cs_packed_view& v, const double* d_lut, cons
                               int64_t ldw, int64_t k, double* out, int64_t ldo, double scale,
                               Workspace& ws, cudaStream_t s) {
     dispatch<false>(v, d_lut, W, ldw, k, out, ldo, scale, ws, s);
+}
+
+// Single-slice forms: each CTA covers the whole contraction, so no partial tiles and no
+// workspace are needed (used where the caller cannot allocate).
+void decode_gemm_rows_fp64_unsplit(const cs_packed_view& v, const double* d_lut, const double* V,
+                                   int64_t ldv, int64_t k, double* out, int64_t ldo,
+                                   cudaStream_t s) {
+    Workspace unused;
+    dispatch<true>(v, d_lut, V, ldv, k, out, ldo, 1.0, unused, s, 1);
+}
+
+void decode_gemm_samples_fp64_unsplit(const cs_packed_view& v, const double* d_lut,
+                                      const double* W, int64_t ldw, int64_t k, double* out,
+                                      int64_t ldo, double scale, cudaStream_t s) {
+    Workspace unused;
+    dispatch<false>(v, d_lut, W, ldw, k, out, ldo, scale, unused, s, 1);
 }
 
 }  // namespace cs

@@ -77,6 +77,16 @@ int cs_kinship_apply(cs_kinship* op, const double* X, int64_t ldx, int64_t k, do
 /* Same with host pointers (synchronous). */
 int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                           int64_t ldy, int precision);
+/* No counterpart in the reference.  The FP64 Y = K X of cs_kinship_apply for callers that
+ * cannot let the library allocate device memory (a process that has reserved HBM for its
+ * own pool, or a request loop that cannot absorb cudaMalloc's synchronisation).  Scratch
+ * comes from a fixed 16 MiB array in the library's device memory, so it needs
+ * (2 * rows() + selected variants) * k <= 2^21 doubles, else CS_ERR_INVALID_ARGUMENT.
+ * Allocates nothing.  The first call on a device looks up the array's device address and
+ * should come before any stream capture.  Calls share the array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller.  Device pointers. */
+int cs_kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
+                             int64_t ldy, void* stream);
 /* trace() and getDiagonal() (kinship_operator.cpp:306-368); diag is a host array. */
 int cs_kinship_trace(const cs_kinship* op, double* trace);
 int cs_kinship_diagonal(cs_kinship* op, double* diag);
