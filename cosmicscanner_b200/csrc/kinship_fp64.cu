@@ -31,12 +31,88 @@ struct Cfg {
     static_assert((BM / TM) * (BN / TN) == kThreads, "thread layout");
     static constexpr size_t smem_a = sizeof(double) * SUBK * BM;
     static constexpr size_t smem_b = sizeof(double) * SUBK * BN;
-    static constexpr size_t smem_p = (size_t)BM * 32;  // rows pass: 128-sample packed window
+    static constexpr size_t smem_p = (size_t)BM * 32 + sizeof(double) * 4 * BM;  // rows pass:
+                                       // 128-sample packed window + per-row lookup table
 };
+
+
+// Column owned by thread tx for its j-th output: pairs of adjacent columns, strided by
+// 2*TX between pairs, so that a warp's 16-byte shared-memory reads of a B row are
+// contiguous (conflict-free) and the A row reads are broadcasts.
+template <int BN, int TN>
+__device__ __forceinline__ int tile_col(int tx, int j) {
+    constexpr int TX = BN / TN;
+    if constexpr (TN == 1) return tx;
+    else return 2 * tx + 2 * TX * (j >> 1) + (j & 1);
+}
+
+// SUBK-step rank-1 updates of the TM x TN register tile from As[SUBK][BM], Bs[SUBK][BN].
+template <int BM, int BN, int TM, int TN, int SUBK>
+__device__ __forceinline__ void tile_fma(const double* __restrict__ As,
+                                         const double* __restrict__ Bs, int tx, int ty,
+                                         double (&acc)[TM][TN]) {
+    constexpr int TX = BN / TN;
+#pragma unroll 4
+    for (int kk = 0; kk < SUBK; ++kk) {
+        double a[TM], b[TN];
+        const double* ap = As + kk * BM + ty * TM;
+        if constexpr (TM % 2 == 0) {
+#pragma unroll
+            for (int i = 0; i < TM / 2; ++i) {
+                const double2 v = reinterpret_cast<const double2*>(ap)[i];
+                a[2 * i] = v.x;
+                a[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < TM; ++i) a[i] = ap[i];
+        }
+        const double* bp = Bs + kk * BN;
+        if constexpr (TN % 2 == 0) {
+#pragma unroll
+            for (int q = 0; q < TN / 2; ++q) {
+                const double2 v = *reinterpret_cast<const double2*>(bp + 2 * tx + 2 * TX * q);
+                b[2 * q] = v.x;
+                b[2 * q + 1] = v.y;
+            }
+        } else {
+            b[0] = bp[tx];
+        }
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+            for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+}
+
+// Bs[kk][n] = src[(r0 + kk) * ld + c0 + n] for rows r0 + kk < r_end and columns < k, else 0.
+template <int BN, int SUBK>
+__device__ __forceinline__ void load_b_tile(double* __restrict__ Bs, const double* __restrict__ src,
+                                            int64_t ld, int64_t r0, int64_t r_end, int64_t c0,
+                                            int64_t k, int tid) {
+    if (BN >= 2 && (ld & 1) == 0 && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+        for (int idx = tid; idx < SUBK * BN / 2; idx += kThreads) {
+            const int kk = idx / (BN / 2), n = 2 * (idx % (BN / 2));
+            const int64_t r = r0 + kk, c = c0 + n;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < r_end) {
+                if (c + 1 < k) v = __ldg(reinterpret_cast<const double2*>(src + r * ld + c));
+                else if (c < k) v.x = __ldg(src + r * ld + c);
+            }
+            *reinterpret_cast<double2*>(Bs + kk * BN + n) = v;
+        }
+    } else {
+        for (int idx = tid; idx < SUBK * BN; idx += kThreads) {
+            const int kk = idx / BN, n = idx % BN;
+            const int64_t r = r0 + kk, c = c0 + n;
+            Bs[idx] = (r < r_end && c < k) ? __ldg(src + r * ld + c) : 0.0;
+        }
+    }
+}
 
 // ---------------------------------------------------------------- rows pass (Z^T V)
 template <int BM, int BN, int TM, int TN>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_samples, int64_t stride,
             const double* __restrict__ lut, const double* __restrict__ V, int64_t ldv, int64_t k,
             double* __restrict__ out, int64_t ldo, int64_t chunk, double scale) {
@@ -45,7 +121,8 @@ k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sample
     extern __shared__ __align__(16) unsigned char smem[];
     double* As = reinterpret_cast<double*>(smem);                 // [SUBK][BM]
     double* Bs = As + SUBK * BM;                                   // [SUBK][BN]
-    uint8_t* Ps = reinterpret_cast<uint8_t*>(Bs + SUBK * BN);      // [BM][32]
+    double* Ls = Bs + SUBK * BN;                                   // [4][BM] lookup table
+    uint8_t* Ps = reinterpret_cast<uint8_t*>(Ls + 4 * BM);         // [BM][32]
 
     const int tid = threadIdx.x;
     const int tx = tid % (BN / TN), ty = tid / (BN / TN);
@@ -57,10 +134,9 @@ k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sample
     // decode role: row dm, two bytes starting at byte db of each SUBK-sample step
     const int dm = tid % BM;
     const int db = (tid / BM) * 2;
-    double l0 = 0.0, l1 = 0.0, l2 = 0.0, l3 = 0.0;
-    if (row0 + dm < n_rows) {
-        const double* L = lut + 4 * (row0 + dm);
-        l0 = L[0]; l1 = L[1]; l2 = L[2]; l3 = L[3];
+    for (int idx = tid; idx < 4 * BM; idx += kThreads) {
+        const int r = idx >> 2, code = idx & 3;
+        Ls[code * BM + r] = (row0 + r < n_rows) ? __ldg(lut + 4 * (row0 + r) + code) : 0.0;
     }
 
     double acc[TM][TN];
@@ -91,29 +167,13 @@ k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sample
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const uint32_t code = (b >> (2 * q)) & 3u;
-                        const double val = code == 0 ? l0 : code == 1 ? l1 : code == 2 ? l2 : l3;
-                        As[(4 * (db + j) + q) * BM + dm] = val;
+                        As[(4 * (db + j) + q) * BM + dm] = Ls[code * BM + dm];
                     }
                 }
             }
-            for (int idx = tid; idx < SUBK * BN; idx += kThreads) {
-                const int kk = idx / BN, n = idx % BN;
-                const int64_t smp = s0 + kk, col = col0 + n;
-                Bs[idx] = (smp < s_end && col < k) ? __ldg(V + smp * ldv + col) : 0.0;
-            }
+            load_b_tile<BN, SUBK>(Bs, V, ldv, s0, s_end, col0, k, tid);
             __syncthreads();
-#pragma unroll 4
-            for (int kk = 0; kk < SUBK; ++kk) {
-                double a[TM], b[TN];
-#pragma unroll
-                for (int i = 0; i < TM; ++i) a[i] = As[kk * BM + ty * TM + i];
-#pragma unroll
-                for (int j = 0; j < TN; ++j) b[j] = Bs[kk * BN + tx * TN + j];
-#pragma unroll
-                for (int i = 0; i < TM; ++i)
-#pragma unroll
-                    for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-            }
+            tile_fma<BM, BN, TM, TN, SUBK>(As, Bs, tx, ty, acc);
             __syncthreads();
         }
     }
@@ -124,7 +184,7 @@ k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sample
         if (t >= n_rows) continue;
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
-            const int64_t c = col0 + tx * TN + j;
+            const int64_t c = col0 + tile_col<BN, TN>(tx, j);
             if (c < k) dst[t * ldo + c] = acc[i][j] * scale;
         }
     }
@@ -132,7 +192,7 @@ k_rows_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sample
 
 // ---------------------------------------------------------------- samples pass (Z W)
 template <int BM, int BN, int TM, int TN>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_samples_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_samples,
                int64_t stride, const double* __restrict__ lut, const double* __restrict__ W,
                int64_t ldw, int64_t k, double* __restrict__ out, int64_t ldo, int64_t chunk,
@@ -180,24 +240,9 @@ k_samples_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sam
                     code == 0 ? l0 : code == 1 ? l1 : code == 2 ? l2 : l3;
             }
         }
-        for (int idx = tid; idx < SUBK * BN; idx += kThreads) {
-            const int kk = idx / BN, n = idx % BN;
-            const int64_t t = t0 + kk, col = col0 + n;
-            Bs[idx] = (t < t_end && col < k) ? __ldg(W + t * ldw + col) : 0.0;
-        }
+        load_b_tile<BN, SUBK>(Bs, W, ldw, t0, t_end, col0, k, tid);
         __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < SUBK; ++kk) {
-            double a[TM], b[TN];
-#pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = As[kk * BM + ty * TM + i];
-#pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Bs[kk * BN + tx * TN + j];
-#pragma unroll
-            for (int i = 0; i < TM; ++i)
-#pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
+        tile_fma<BM, BN, TM, TN, SUBK>(As, Bs, tx, ty, acc);
         __syncthreads();
     }
     double* dst = out + (int64_t)blockIdx.z * n_samples * ldo;
@@ -207,7 +252,7 @@ k_samples_fp64(const uint8_t* __restrict__ packed, int64_t n_rows, int64_t n_sam
         if (s >= n_samples) continue;
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
-            const int64_t c = col0 + tx * TN + j;
+            const int64_t c = col0 + tile_col<BN, TN>(tx, j);
             if (c < k) dst[s * ldo + c] = acc[i][j] * scale;
         }
     }
