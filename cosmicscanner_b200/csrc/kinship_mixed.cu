@@ -1,16 +1,726 @@
-// Tensor-core (mixed-precision) form of the kinship operator.
+// Tensor-core (mixed-precision) form of the kinship operator Y = Z Z^T X / M.
+//
+// Arithmetic.  Both passes run on tcgen05.mma kind::i8 with exact int32 accumulation:
+//  * the genotype tile enters as int8 dosages G in {0, 1, 2} (missing -> 0) together with
+//    an int8 missing-indicator tile, both decoded from the packed 2-bit rows in shared
+//    memory (a 128-SNP x 128-sample tile, 128-byte swizzled);
+//  * right-hand sides are quantised per column into three int8 pieces (base 254) after
+//    centring: x' = (x - mean) * 127 / max|x - mean| ~ q1 + q2/254 + q3/254^2, i.e. about
+//    23 significant bits, so the only rounding is this quantisation (~6e-8 of the column
+//    maximum per element); all products and sums up to 2^31 are exact.
+// Rows pass (U = Z^T X): with S_t, n_t the exact allele sum and observed count of row t,
+//   u_t / s_t = mean * (S_t - mu_t n_t) + ( sum_i G_ti x'_i + mu_t sum_{i missing} x'_i
+//               - mu_t sum_i x'_i ) / scale
+// (the centring identity of src/kinship_operator.cpp:135 with the missing-call terms split
+// out).  Samples pass (Y = Z W / M, W = s o U):
+//   y_i = ( sum_t G_ti w_t + sum_t miss_ti mu_t w_t - sum_t mu_t w_t ) / M
+// with W and (mu o W) quantised the same way.  Each pass is one MMA of the dosage tile
+// against the pieces plus one of the missing-indicator tile (same pieces in the rows pass,
+// the (mu o W) pieces in the samples pass).
+//
+// Kernel structure (one CTA per SM, 14 warps): warp 0 issues TMA loads of the packed tile
+// and of the quantised pieces into a ring of stages; warps 2-9 decode; warp 1 issues the
+// MMAs from one thread into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and
+// write FP64 slice partials.  The decoded tile (SNP rows x samples) serves as a K-major A
+// operand in the rows pass and as an MN-major A operand in the samples pass.  Every wait
+// is bounded; a timeout leaves a status code that the host reports as an error.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
 #include "cs_internal.h"
+#include "sm100.cuh"
 
 namespace cs {
 
-struct MixedOperator {};
+namespace {
+
+using namespace sm100;
+
+constexpr int kTile = 128;        // MMA M, and SNP rows / samples per decoded tile
+constexpr int kKBlock = 128;      // K elements (int8) per stage: one 128-byte swizzle row
+constexpr int kMaxKc = 80;        // column-tile width cap (6 * 80 TMEM columns)
+constexpr int kWarps = 14;
+constexpr int kThreads = kWarps * 32;
+constexpr int kDecodeWarp0 = 2, kDecodeWarps = 8;
+constexpr int kEpiWarp0 = 10;
+constexpr uint32_t kTmemCols = 512;
+constexpr double kBase = 254.0;
+
+constexpr int kATileBytes = kTile * kKBlock;     // 16 KB
+constexpr int kPackedBytes = kTile * 32;         // 128 rows x 32 B
+
+template <bool ROWS>
+struct Layout {
+    static constexpr int kPieces = ROWS ? 3 : 6;  // B rows per column: pieces (x2 for mu o W)
+    static constexpr int kStages = ROWS ? 3 : 2;
+    static constexpr int kBBytes = kPieces * kMaxKc * 128;
+    static constexpr int kStageBytes = 2 * kATileBytes + kBBytes + kPackedBytes;
+    static constexpr int kSmem = kStages * kStageBytes + 1024 + 256;
+    static __host__ __device__ constexpr int a(int s) { return s * kStageBytes; }
+    static __host__ __device__ constexpr int am(int s) { return s * kStageBytes + kATileBytes; }
+    static __host__ __device__ constexpr int b(int s) { return s * kStageBytes + 2 * kATileBytes; }
+    static __host__ __device__ constexpr int p(int s) {
+        return s * kStageBytes + 2 * kATileBytes + kBBytes;
+    }
+};
+
+struct PassArgs {
+    int n_tiles, n_ctiles, n_splits;
+    int kb_total, kb_per_split;  // K-blocks of the contraction, per slice
+    int kc, kp;                  // column tile width, padded column count
+    const double* mu;            // rows pass: mu_t per SNP row (epilogue)
+    const double* inv_f2;        // samples pass: 1 / scale of W per column
+    const double* inv_f3;        // samples pass: 1 / scale of (mu o W) per column
+    double* part;                // [n_splits][kp][ld] FP64 slice partials
+    int64_t ld;                  // padded output rows
+    int* status;
+};
+
+// One packed byte (4 codes) -> 4 int8 dosages and 4 missing indicators via byte permutes
+// of the tables {2, 0, 1, 0} and {0, 1, 0, 0} indexed by the codes.
+__device__ __forceinline__ void decode_byte(uint32_t x, uint32_t& dos, uint32_t& mis) {
+    const uint32_t sel = (x & 3u) | ((x & 0xCu) << 2) | ((x & 0x30u) << 4) | ((x & 0xC0u) << 6);
+    dos = __byte_perm(0x00010002u, 0u, sel);
+    mis = __byte_perm(0x00000100u, 0u, sel);
+}
+
+// 16 codes (one 32-bit word) -> 16 int8 dosages and 16 indicators.
+__device__ __forceinline__ void decode_word(uint32_t w, uint4& dos, uint4& mis) {
+    decode_byte(w & 0xFFu, dos.x, mis.x);
+    decode_byte((w >> 8) & 0xFFu, dos.y, mis.y);
+    decode_byte((w >> 16) & 0xFFu, dos.z, mis.z);
+    decode_byte(w >> 24, dos.w, mis.w);
+}
+
+template <bool ROWS>
+__global__ void __launch_bounds__(kThreads, 1)
+k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+             PassArgs P) {
+    using L = Layout<ROWS>;
+    constexpr int S = L::kStages;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * L::kStageBytes);
+    uint64_t* full = bars;             // TMA landed (1 arrival + tx bytes)
+    uint64_t* dec = bars + S;          // decoded (one arrival per decode warp)
+    uint64_t* empty = bars + 2 * S;    // the stage's MMAs completed (commit)
+    uint64_t* acc_full = bars + 3 * S; // accumulator ready for the epilogue (commit)
+    uint64_t* acc_empty = acc_full + 1;  // accumulator drained (one arrival per epilogue warp)
+    uint64_t* drained = acc_empty + 1;   // MMA thread's own work complete at exit
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kc = P.kc, kp = P.kp;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&dec[s], kDecodeWarps);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(acc_empty, 4);
+        mbar_init(drained, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    const int units = P.n_tiles * P.n_ctiles * P.n_splits;
+    auto unit_coords = [&](int u, int& tile, int& ct, int& split, int& kb0, int& kb1) {
+        tile = u % P.n_tiles;
+        const int rest = u / P.n_tiles;
+        ct = rest % P.n_ctiles;
+        split = rest / P.n_ctiles;
+        kb0 = split * P.kb_per_split;
+        kb1 = min(P.kb_total, kb0 + P.kb_per_split);
+    };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer
+        if (elect_one()) {
+            prefetch_tensormap(&tm_a);
+            prefetch_tensormap(&tm_b);
+            const uint32_t bytes = (uint32_t)(kPackedBytes + L::kPieces * kc * 128);
+            uint32_t j = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int s = j % S;
+                    if (!(ok = mbar_wait(&empty[s], ((j / S) & 1) ^ 1, P.status, kTimeoutTma))) break;
+                    mbar_arrive_expect_tx(&full[s], bytes);
+                    // packed tile: 128 SNP rows x 32 bytes (128 samples)
+                    if (ROWS)
+                        tma_load_2d(smem + L::p(s), &tm_a, kb * 32, tile * kTile, &full[s]);
+                    else
+                        tma_load_2d(smem + L::p(s), &tm_a, tile * 32, kb * kKBlock, &full[s]);
+                    for (int q = 0; q < L::kPieces; ++q)
+                        tma_load_2d(smem + L::b(s) + q * kc * 128, &tm_b, kb * kKBlock,
+                                    q * kp + ct * kc, &full[s]);
+                }
+            }
+            // leave no copy in flight
+            for (uint32_t q = (j >= (uint32_t)S ? j - S : 0); q < j; ++q)
+                mbar_wait(&full[q % S], (q / S) & 1, P.status, kTimeoutTma, 1u << 20);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (elect_one()) {
+            // s8 x s8 -> s32; rows pass: K-major A (SNP rows x samples); samples pass:
+            // MN-major A (the same tile read as samples x SNPs)
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
+                                   ((uint32_t)((3 * kc) >> 3) << 17) | ((uint32_t)(kTile >> 4) << 24);
+            uint32_t j = 0;
+            int ui = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                if (!(ok = mbar_wait(acc_empty, (ui & 1) ^ 1, P.status, kTimeoutMma))) break;
+                tc_fence_after();
+                const uint32_t acc_main = tmem_base, acc_miss = tmem_base + 3 * kc;
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int s = j % S;
+                    const uint32_t ph = (j / S) & 1;
+                    if (!(ok = mbar_wait(&full[s], ph, P.status, kTimeoutMma))) break;
+                    if (!(ok = mbar_wait(&dec[s], ph, P.status, kTimeoutMma))) break;
+                    tc_fence_after();
+                    const uint32_t a = smem_addr(smem + L::a(s));
+                    const uint32_t am = smem_addr(smem + L::am(s));
+                    const uint32_t b = smem_addr(smem + L::b(s));
+                    const uint32_t bm = ROWS ? b : b + 3 * kc * 128;
+#pragma unroll
+                    for (int ks = 0; ks < kKBlock / 32; ++ks) {
+                        const uint32_t accum = (kb == kb0 && ks == 0) ? 0u : 1u;
+                        const uint32_t aoff = ROWS ? ks * 32 : ks * 4096;  // 32 K elements
+                        const uint64_t da = smem_desc_sw128(a + aoff, 16, 1024);
+                        const uint64_t dm = smem_desc_sw128(am + aoff, 16, 1024);
+                        const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
+                        const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
+                        mma_i8(acc_main, da, db, idesc, accum);
+                        mma_i8(acc_miss, dm, dbm, idesc, accum);
+                    }
+                    mma_commit(&empty[s]);
+                }
+                if (ok) mma_commit(acc_full);
+            }
+            mma_commit(drained);
+            mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
+        }
+    } else if (warp < kEpiWarp0) {
+        // ------------------------------------------------------------ decoders
+        // thread d: SNP row d % 128, 64 samples (16 packed bytes) starting at 64 * (d / 128)
+        const int d = threadIdx.x - kDecodeWarp0 * 32;
+        const int r = d & 127, h = d >> 7;
+        const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
+        uint32_t j = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+            int tile, ct, split, kb0, kb1;
+            unit_coords(u, tile, ct, split, kb0, kb1);
+            for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                const int s = j % S;
+                if (!(ok = mbar_wait(&full[s], (j / S) & 1, P.status, kTimeoutDecode))) break;
+                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(s) + r * 32 + h * 16);
+                unsigned char* a = smem + L::a(s);
+                unsigned char* am = smem + L::am(s);
+                const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
+#pragma unroll
+                for (int cj = 0; cj < 4; ++cj) {
+                    uint4 dos, mis;
+                    decode_word(words[cj], dos, mis);
+                    const int chunk = 4 * h + cj;  // 16 samples per 16-byte chunk
+                    const int off = rbase + ((chunk ^ (r & 7)) << 4);
+                    *reinterpret_cast<uint4*>(a + off) = dos;
+                    *reinterpret_cast<uint4*>(am + off) = mis;
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&dec[s]);
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        int ui = 0;
+        bool ok = true;
+        const double ib = 1.0 / kBase, ib2 = 1.0 / (kBase * kBase);
+        for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
+            int tile, ct, split, kb0, kb1;
+            unit_coords(u, tile, ct, split, kb0, kb1);
+            if (!(ok = mbar_wait(acc_full, ui & 1, P.status, kTimeoutEpilogue))) break;
+            tc_fence_after();
+            const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
+            const uint32_t tb = tmem_base + ((uint32_t)(32 * q) << 16);
+            const double mu = ROWS ? P.mu[row] : 0.0;
+            double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
+            for (int c0 = 0; c0 < kc; c0 += 16) {
+                int32_t m1[16], m2[16], m3[16], x1[16], x2[16], x3[16];
+                tmem_ld16i(tb + c0, m1);
+                tmem_ld16i(tb + kc + c0, m2);
+                tmem_ld16i(tb + 2 * kc + c0, m3);
+                tmem_ld16i(tb + 3 * kc + c0, x1);
+                tmem_ld16i(tb + 4 * kc + c0, x2);
+                tmem_ld16i(tb + 5 * kc + c0, x3);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                    const double xv = (double)x1[i] + (double)x2[i] * ib + (double)x3[i] * ib2;
+                    double v;
+                    if (ROWS) {
+                        v = mv + mu * xv;
+                    } else {
+                        const int c = ct * kc + c0 + i;
+                        v = mv * P.inv_f2[c] + xv * P.inv_f3[c];
+                    }
+                    dst[(int64_t)(c0 + i) * P.ld] = v;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acc_empty);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, kTmemCols);
+    }
+}
+
+// ---------------------------------------------------------------- operand preparation
+// Quantises v (already centred and multiplied by 127 / max) into three int8 pieces of base 254;
+// returns the represented value.
+__device__ __forceinline__ double quantise3(double v, int8_t& q1, int8_t& q2, int8_t& q3) {
+    const double a = rint(v);
+    const double r1 = (v - a) * kBase;
+    const double b = rint(r1);
+    const double r2 = (r1 - b) * kBase;
+    const double c = rint(r2);
+    q1 = (int8_t)a;
+    q2 = (int8_t)b;
+    q3 = (int8_t)c;
+    return a + b / kBase + c / (kBase * kBase);
+}
+
+// Per-column sums of a row-major FP64 matrix over row blocks: part[b][c].
+__global__ void k_col_partial_sums(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
+                                   int64_t rows_per_block, double* __restrict__ part) {
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+    const int64_t r1 = min(n, r0 + rows_per_block);
+    for (int64_t c = threadIdx.x; c < k; c += blockDim.x) {
+        double s = 0.0;
+        for (int64_t r = r0; r < r1; ++r) s += X[r * ld + c];
+        part[(int64_t)blockIdx.x * k + c] = s;
+    }
+}
+
+// out[c] = scale * sum_b part[b][c] (fixed order); resets maxbits[c] when given.
+__global__ void k_sum_partials(const double* __restrict__ part, int nb, int64_t k, double scale,
+                               double* __restrict__ out, unsigned long long* __restrict__ maxbits) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < k;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
+        out[c] = s * scale;
+        if (maxbits) maxbits[c] = 0ull;
+    }
+}
+
+// maxbits[c] = max |X[r,c] - mean[c]| as IEEE bits (atomicMax on non-negative doubles is
+// order independent, hence deterministic).
+__global__ void k_col_absmax(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
+                             const double* __restrict__ mean, unsigned long long* __restrict__ maxbits) {
+    const int64_t total = n * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = idx / k, c = idx - r * k;
+        const double v = fabs(X[r * ld + c] - mean[c]);
+        atomicMax(maxbits + c, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__device__ __forceinline__ double quant_factor(unsigned long long bits) {
+    const double m = __longlong_as_double((long long)bits);
+    return m > 0.0 ? 127.0 / m : 0.0;
+}
+
+// Rows-pass operand B1[q*kp + c][i] (int8, i < n_pad) and per-block sums of the
+// represented values (Q_c, reduced in fixed order).
+__global__ void k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n,
+                                     int64_t k, int64_t kp, int64_t n_pad,
+                                     const double* __restrict__ mean,
+                                     const unsigned long long* __restrict__ maxbits,
+                                     int8_t* __restrict__ B, int64_t rows_per_block,
+                                     double* __restrict__ qpart) {
+    // block b handles samples [b * rows_per_block, ...) of every column
+    const int64_t i0 = (int64_t)blockIdx.x * rows_per_block;
+    const int64_t i1 = min(n_pad, i0 + rows_per_block);
+    for (int64_t c = 0; c < kp; ++c) {
+        const double f = c < k ? quant_factor(maxbits[c]) : 0.0;
+        double s = 0.0;
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            int8_t q1 = 0, q2 = 0, q3 = 0;
+            if (c < k && i < n) s += quantise3((X[i * ld + c] - mean[c]) * f, q1, q2, q3);
+            B[c * n_pad + i] = q1;
+            B[(kp + c) * n_pad + i] = q2;
+            B[(2 * kp + c) * n_pad + i] = q3;
+        }
+        // fixed-order block reduction
+        __shared__ double red[256];
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && c < k) qpart[(int64_t)blockIdx.x * k + c] = red[0];
+        __syncthreads();
+    }
+}
+
+// Rows-pass reduction: u_tc = s_t (mean_c exc_t + (sum_z part[z][c][t] - mu_t Q_c) / f_c),
+// W[t][c] = s_t u_tc; maxima of |W| and |mu W| per column.
+__global__ void k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t ld,
+                              int64_t R, int64_t k, const double* __restrict__ s_row,
+                              const double* __restrict__ exc_row, const double* __restrict__ mu,
+                              const double* __restrict__ mean, const double* __restrict__ qsum,
+                              const unsigned long long* __restrict__ maxbits_in,
+                              double* __restrict__ W, unsigned long long* __restrict__ max_w,
+                              unsigned long long* __restrict__ max_muw) {
+    const int64_t total = R * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / R, t = idx - c * R;
+        double acc = 0.0;
+        for (int z = 0; z < splits; ++z) acc += part[((int64_t)z * kp + c) * ld + t];
+        const double f = quant_factor(maxbits_in[c]);
+        const double inner = f > 0.0 ? (acc - mu[t] * qsum[c]) / f : 0.0;
+        const double u = s_row[t] * (mean[c] * exc_row[t] + inner);
+        const double w = s_row[t] * u;
+        W[t * k + c] = w;
+        atomicMax(max_w + c, (unsigned long long)__double_as_longlong(fabs(w)));
+        atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(fabs(mu[t] * w)));
+    }
+}
+
+// Samples-pass operand B2: pieces of W f2 (rows q*kp + c) and of (mu o W) f3 (rows
+// (3 + q) kp + c), t < r_pad; 1/f2, 1/f3 per column.
+__global__ void k_split_samples_operand(const double* __restrict__ W, int64_t R, int64_t k,
+                                        int64_t kp, int64_t r_pad, const double* __restrict__ mu,
+                                        const unsigned long long* __restrict__ max_w,
+                                        const unsigned long long* __restrict__ max_muw,
+                                        int8_t* __restrict__ B, double* __restrict__ inv_f2,
+                                        double* __restrict__ inv_f3) {
+    const int64_t total = kp * r_pad;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / r_pad, t = idx - c * r_pad;
+        int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0;
+        const double f2 = c < k ? quant_factor(max_w[c]) : 0.0;
+        const double f3 = c < k ? quant_factor(max_muw[c]) : 0.0;
+        if (c < k && t < R) {
+            const double w = W[t * k + c];
+            quantise3(w * f2, a1, a2, a3);
+            quantise3(mu[t] * w * f3, b1, b2, b3);
+        }
+        if (t == 0) {
+            inv_f2[c] = f2 > 0.0 ? 1.0 / f2 : 0.0;
+            inv_f3[c] = f3 > 0.0 ? 1.0 / f3 : 0.0;
+        }
+        B[c * r_pad + t] = a1;
+        B[(kp + c) * r_pad + t] = a2;
+        B[(2 * kp + c) * r_pad + t] = a3;
+        B[(3 * kp + c) * r_pad + t] = b1;
+        B[(4 * kp + c) * r_pad + t] = b2;
+        B[(5 * kp + c) * r_pad + t] = b3;
+    }
+}
+
+// c0[b][c] = sum_{t in block b} mu_t W[t][c]
+__global__ void k_centring_partials(const double* __restrict__ W, int64_t R, int64_t k,
+                                    int64_t rows_per_block, const double* __restrict__ mu,
+                                    double* __restrict__ part) {
+    const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+    const int64_t r1 = min(R, r0 + rows_per_block);
+    for (int64_t c = threadIdx.x; c < k; c += blockDim.x) {
+        double s = 0.0;
+        for (int64_t t = r0; t < r1; ++t) s += mu[t] * W[t * k + c];
+        part[(int64_t)blockIdx.x * k + c] = s;
+    }
+}
+
+// Samples-pass reduction: Y[i][c] = (sum_z part[z][c][i] - c0_c) / M.
+__global__ void k_reduce_samples(const double* __restrict__ part, int splits, int64_t kp,
+                                 int64_t ld, int64_t n, int64_t k, const double* __restrict__ c0,
+                                 double inv_m, double* __restrict__ Y, int64_t ldy) {
+    const int64_t total = n * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / n, i = idx - c * n;
+        double acc = 0.0;
+        for (int z = 0; z < splits; ++z) acc += part[((int64_t)z * kp + c) * ld + i];
+        Y[i * ldy + c] = (acc - c0[c]) * inv_m;
+    }
+}
+
+// ---------------------------------------------------------------- tensor maps
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    if (!fn) fail(CS_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    return fn;
+}
+
+// 2D uint8 tensor map: inner extent `inner` bytes, `outer` rows of `row_bytes`.
+CUtensorMap make_map_u8(const void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+                        uint32_t box_inner, uint32_t box_outer, bool swizzle) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base),
+                                   dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        fail(CS_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return m;
+}
+
+int blocks_for(int64_t work) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 16LL * num_sms()));
+}
+
+// Number of K slices so that about `target` work units cover the GPU.
+int choose_splits(int64_t units_per_split, int kb_total, int64_t target) {
+    int64_t s = (target + units_per_split - 1) / units_per_split;
+    s = std::max<int64_t>(1, std::min<int64_t>(s, std::max(1, kb_total / 8)));
+    return (int)s;
+}
+
+}  // namespace
+
+struct MixedOperator {
+    int64_t R = 0, n = 0, r_pad = 0, n_pad = 0;
+    DeviceBuffer<double> mu, s, exc;
+    CUtensorMap tm_rows{}, tm_samples{};
+    DeviceBuffer<int8_t> b1, b2;
+    DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f2, inv_f3;
+    DeviceBuffer<unsigned long long> max1, max_w, max_muw;
+    CUtensorMap tm_b1{}, tm_b2{};
+    const void* tm_b1_base = nullptr;
+    const void* tm_b2_base = nullptr;
+    int64_t tm_kp = -1;
+    DeviceBuffer<int> status;
+};
 
 void destroy_mixed(MixedOperator* m) { delete m; }
 
+static MixedOperator* mixed_for(cs_kinship* op) {
+    if (op->mixed) return op->mixed;
+    auto* m = new MixedOperator();
+    try {
+        const int64_t R = op->n_active, n = op->rows;
+        m->R = R;
+        m->n = n;
+        m->r_pad = round_up(std::max<int64_t>(R, 1), kTile);
+        m->n_pad = round_up(std::max<int64_t>(n, 1), kTile);
+        std::vector<double> mu(m->r_pad, 0.0), sv(m->r_pad, 0.0), ex(m->r_pad, 0.0);
+        for (int64_t t = 0; t < R; ++t) {
+            const double mt = op->mean[t];
+            mu[t] = mt;
+            sv[t] = op->inv_std[t];
+            const int64_t c00 = op->counts[4 * t], c10 = op->counts[4 * t + 2], c11 = op->counts[4 * t + 3];
+            ex[t] = (double)(2 * c00 + c10) - mt * (double)(c00 + c10 + c11);  // S_t - mu_t n_t
+        }
+        m->mu.resize(m->r_pad);
+        m->s.resize(m->r_pad);
+        m->exc.resize(m->r_pad);
+        CS_CUDA(cudaMemcpy(m->mu.get(), mu.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
+        CS_CUDA(cudaMemcpy(m->s.get(), sv.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
+        CS_CUDA(cudaMemcpy(m->exc.get(), ex.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
+        // packed genotype tiles: 32 bytes (128 samples) x 128 SNP rows; rows past R read as
+        // zeros and meet zero B rows (samples pass) or land in discarded output rows
+        m->tm_rows = make_map_u8(op->view.rows, op->view.stride, R, op->view.stride, 32, kTile, false);
+        m->tm_samples = m->tm_rows;
+        m->status.resize(1);
+        CS_CUDA(cudaMemset(m->status.get(), 0, sizeof(int)));
+        static bool configured = false;
+        if (!configured) {
+            CS_CUDA(cudaFuncSetAttribute(k_mixed_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Layout<true>::kSmem));
+            CS_CUDA(cudaFuncSetAttribute(k_mixed_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         Layout<false>::kSmem));
+            configured = true;
+        }
+    } catch (...) {
+        delete m;
+        throw;
+    }
+    op->mixed = m;
+    return m;
+}
+
 void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                          int64_t ldy, cudaStream_t s) {
-    (void)op; (void)X; (void)ldx; (void)k; (void)Y; (void)ldy; (void)s;
-    fail(CS_ERR_UNSUPPORTED, "mixed-precision operator not built yet");
+    if (k <= 0) return;
+    const int64_t n = op->rows, R = op->n_active;
+    if (R == 0) {
+        CS_CUDA(cudaMemset2DAsync(Y, ldy * 8, 0, k * 8, n, s));
+        return;
+    }
+    MixedOperator* m = mixed_for(op);
+    const int n_ctiles = (int)((k + kMaxKc - 1) / kMaxKc);
+    const int kc = (int)round_up((k + n_ctiles - 1) / n_ctiles, 16);
+    const int64_t kp = (int64_t)kc * n_ctiles;
+    const int64_t r_pad = m->r_pad, n_pad = m->n_pad;
+    const int kb1 = (int)(n_pad / kKBlock), kb2 = (int)(r_pad / kKBlock);
+    const int64_t tiles1 = r_pad / kTile, tiles2 = n_pad / kTile;
+    const int64_t target = 8LL * num_sms();
+    const int splits1 = choose_splits(tiles1 * n_ctiles, kb1, target);
+    const int splits2 = choose_splits(tiles2 * n_ctiles, kb2, target);
+    const int kbs1 = (kb1 + splits1 - 1) / splits1, kbs2 = (kb2 + splits2 - 1) / splits2;
+    const int nb = (int)std::min<int64_t>(512, std::max<int64_t>(1, std::max(n_pad, R) / 128));
+    m->b1.resize(3 * kp * n_pad);
+    m->b2.resize(6 * kp * r_pad);
+    m->part.resize(std::max<int64_t>((int64_t)splits1 * kp * r_pad, (int64_t)splits2 * kp * n_pad));
+    m->colpart.resize((int64_t)nb * k);
+    for (auto* b : {&m->mean1, &m->qsum, &m->c0}) b->resize(k);
+    for (auto* b : {&m->inv_f2, &m->inv_f3}) b->resize(kp);
+    for (auto* b : {&m->max1, &m->max_w, &m->max_muw}) b->resize(k);
+    m->W.resize(R * k);
+    if (m->tm_b1_base != m->b1.get() || m->tm_kp != kp)
+        m->tm_b1 = make_map_u8(m->b1.get(), n_pad, 3 * kp, n_pad, kKBlock, kc, true);
+    if (m->tm_b2_base != m->b2.get() || m->tm_kp != kp)
+        m->tm_b2 = make_map_u8(m->b2.get(), r_pad, 6 * kp, r_pad, kKBlock, kc, true);
+    m->tm_b1_base = m->b1.get();
+    m->tm_b2_base = m->b2.get();
+    m->tm_kp = kp;
+    const int grid = num_sms();
+    // ---- rows pass: U = Z^T X
+    {
+        const int64_t rpb = (n + nb - 1) / nb;
+        const int nbu = (int)((n + rpb - 1) / rpb);
+        const int64_t ipb = (n_pad + nb - 1) / nb;
+        const int nbi = (int)((n_pad + ipb - 1) / ipb);
+        {
+            prof::Scope ps("mixed_prep_rows_operand", s, 0.0, 24.0 * n * k + 3.0 * kp * n_pad);
+            k_col_partial_sums<<<nbu, 128, 0, s>>>(X, ldx, n, k, rpb, m->colpart.get());
+            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbu, k, 1.0 / (double)n,
+                                             m->mean1.get(), m->max1.get());
+            k_col_absmax<<<blocks_for(n * k), 256, 0, s>>>(X, ldx, n, k, m->mean1.get(), m->max1.get());
+            k_split_rows_operand<<<nbi, 256, 0, s>>>(X, ldx, n, k, kp, n_pad, m->mean1.get(),
+                                                     m->max1.get(), m->b1.get(), ipb,
+                                                     m->colpart.get());
+            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbi, k, 1.0, m->qsum.get(), nullptr);
+            CS_LAUNCH("mixed rows operand");
+        }
+        PassArgs P{};
+        P.n_tiles = (int)tiles1;
+        P.n_ctiles = n_ctiles;
+        P.n_splits = splits1;
+        P.kb_total = kb1;
+        P.kb_per_split = kbs1;
+        P.kc = kc;
+        P.kp = (int)kp;
+        P.mu = m->mu.get();
+        P.part = m->part.get();
+        P.ld = r_pad;
+        P.status = m->status.get();
+        {
+            // algorithmic work: 2 n R k flops, one pass over the packed rows
+            prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
+                           (double)R * (double)((n + 3) / 4));
+            k_mixed_pass<true><<<grid, kThreads, Layout<true>::kSmem, s>>>(m->tm_rows, m->tm_b1, P);
+            CS_LAUNCH("kinship_rows_tc");
+        }
+        CS_CUDA(cudaMemsetAsync(m->max_w.get(), 0, 8 * k, s));
+        CS_CUDA(cudaMemsetAsync(m->max_muw.get(), 0, 8 * k, s));
+        {
+            prof::Scope ps("mixed_reduce_rows", s, 0.0, 8.0 * splits1 * kp * R + 8.0 * R * k);
+            k_reduce_rows<<<blocks_for(R * k), 256, 0, s>>>(
+                m->part.get(), splits1, kp, r_pad, R, k, m->s.get(), m->exc.get(), m->mu.get(),
+                m->mean1.get(), m->qsum.get(), m->max1.get(), m->W.get(), m->max_w.get(),
+                m->max_muw.get());
+            CS_LAUNCH("reduce_rows");
+        }
+    }
+    // ---- samples pass: Y = Z W / M
+    {
+        const int64_t rpb = (R + nb - 1) / nb;
+        const int nbr = (int)((R + rpb - 1) / rpb);
+        {
+            prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 16.0 * R * k + 6.0 * kp * r_pad);
+            k_split_samples_operand<<<blocks_for(kp * r_pad), 256, 0, s>>>(
+                m->W.get(), R, k, kp, r_pad, m->mu.get(), m->max_w.get(), m->max_muw.get(),
+                m->b2.get(), m->inv_f2.get(), m->inv_f3.get());
+            k_centring_partials<<<nbr, 128, 0, s>>>(m->W.get(), R, k, rpb, m->mu.get(), m->colpart.get());
+            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbr, k, 1.0, m->c0.get(), nullptr);
+            CS_LAUNCH("mixed samples operand");
+        }
+        PassArgs P{};
+        P.n_tiles = (int)tiles2;
+        P.n_ctiles = n_ctiles;
+        P.n_splits = splits2;
+        P.kb_total = kb2;
+        P.kb_per_split = kbs2;
+        P.kc = kc;
+        P.kp = (int)kp;
+        P.inv_f2 = m->inv_f2.get();
+        P.inv_f3 = m->inv_f3.get();
+        P.part = m->part.get();
+        P.ld = n_pad;
+        P.status = m->status.get();
+        {
+            prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
+                           (double)R * (double)((n + 3) / 4));
+            k_mixed_pass<false><<<grid, kThreads, Layout<false>::kSmem, s>>>(m->tm_samples, m->tm_b2, P);
+            CS_LAUNCH("kinship_samples_tc");
+        }
+        {
+            prof::Scope ps("mixed_reduce_samples", s, 0.0, 8.0 * splits2 * kp * n + 8.0 * n * k);
+            k_reduce_samples<<<blocks_for(n * k), 256, 0, s>>>(
+                m->part.get(), splits2, kp, n_pad, n, k, m->c0.get(),
+                1.0 / (double)op->num_variants, Y, ldy);
+            CS_LAUNCH("reduce_samples");
+        }
+    }
+    int status = 0;
+    CS_CUDA(cudaMemcpyAsync(&status, m->status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    if (status != 0) {
+        cudaMemset(m->status.get(), 0, sizeof(int));
+        fail(CS_ERR_CUDA, "tensor-core kinship kernel gave up waiting (status " +
+                              std::to_string(status) + ")");
+    }
 }
 
 }  // namespace cs
