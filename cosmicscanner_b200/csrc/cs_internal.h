@@ -125,6 +125,14 @@ void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_
 void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                          int64_t ldy, cudaStream_t s);
 
+// Tensor-core projection for the scan: T[t][c] = sum_i (g_ti - m_t)[observed] B[i][c] over
+// every row of a packed view, m_t = row_mean[t] (kinship_mixed.cu).
+struct MixedScan;
+MixedScan* mixed_scan_create(const cs_packed_view& v, const double* row_mean, const int32_t* counts);
+void mixed_scan_destroy(MixedScan* m);
+void mixed_scan_project(MixedScan* m, const double* B, int64_t ldb, int64_t k, double* T,
+                        int64_t ldt, cudaStream_t s);
+
 // Per-row genotype code counts over a view's samples: c[4*t + code].
 void row_code_counts(const cs_packed_view& v, int32_t* d_counts, cudaStream_t s);
 

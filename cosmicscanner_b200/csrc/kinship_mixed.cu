@@ -301,7 +301,13 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
 }
 
 // ---------------------------------------------------------------- operand preparation
-// Quantises v (already centred and multiplied by 127 / max) into three int8 pieces of base 254;
+// All reductions here are deterministic: block-level trees in a fixed order, per-block
+// partials summed in block order, and maxima through atomicMax on non-negative doubles
+// (order independent).  Tiles are 32 columns x 64 rows so that row-major FP64 inputs are
+// read with coalesced 256-byte rows and column-major outputs written with coalesced runs.
+constexpr int kPrepCols = 32, kPrepRows = 64;
+
+// Quantises v (centred and multiplied by 127 / max) into three int8 pieces of base 254;
 // returns the represented value.
 __device__ __forceinline__ double quantise3(double v, int8_t& q1, int8_t& q2, int8_t& q3) {
     const double a = rint(v);
@@ -313,6 +319,11 @@ __device__ __forceinline__ double quantise3(double v, int8_t& q1, int8_t& q2, in
     q2 = (int8_t)b;
     q3 = (int8_t)c;
     return a + b / kBase + c / (kBase * kBase);
+}
+
+__device__ __forceinline__ double quant_factor(unsigned long long bits) {
+    const double m = __longlong_as_double((long long)bits);
+    return m > 0.0 ? 127.0 / m : 0.0;
 }
 
 // Per-column sums of a row-major FP64 matrix over row blocks: part[b][c].
@@ -339,106 +350,154 @@ __global__ void k_sum_partials(const double* __restrict__ part, int nb, int64_t 
     }
 }
 
-// maxbits[c] = max |X[r,c] - mean[c]| as IEEE bits (atomicMax on non-negative doubles is
-// order independent, hence deterministic).
-__global__ void k_col_absmax(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
-                             const double* __restrict__ mean, unsigned long long* __restrict__ maxbits) {
-    const int64_t total = n * k;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = idx / k, c = idx - r * k;
-        const double v = fabs(X[r * ld + c] - mean[c]);
-        atomicMax(maxbits + c, (unsigned long long)__double_as_longlong(v));
+// Tile (blockIdx.x: 64 rows, blockIdx.y: 32 columns) of |X - mean| maxima: one atomicMax
+// per column per block.
+__global__ void __launch_bounds__(256)
+k_col_absmax(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
+             const double* __restrict__ mean, unsigned long long* __restrict__ maxbits) {
+    __shared__ double red[8][kPrepCols];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t c = (int64_t)blockIdx.y * kPrepCols + tx;
+    const int64_t r0 = (int64_t)blockIdx.x * kPrepRows;
+    double m = 0.0;
+    if (c < k) {
+        const double mc = mean[c];
+        for (int64_t r = r0 + ty; r < min(n, r0 + kPrepRows); r += 8) m = fmax(m, fabs(X[r * ld + c] - mc));
+    }
+    red[ty][tx] = m;
+    __syncthreads();
+    if (ty == 0 && c < k) {
+        for (int j = 1; j < 8; ++j) m = fmax(m, red[j][tx]);
+        atomicMax(maxbits + c, (unsigned long long)__double_as_longlong(m));
     }
 }
 
-__device__ __forceinline__ double quant_factor(unsigned long long bits) {
-    const double m = __longlong_as_double((long long)bits);
-    return m > 0.0 ? 127.0 / m : 0.0;
-}
-
-// Rows-pass operand B1[q*kp + c][i] (int8, i < n_pad) and per-block sums of the
-// represented values (Q_c, reduced in fixed order).
-__global__ void k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n,
-                                     int64_t k, int64_t kp, int64_t n_pad,
-                                     const double* __restrict__ mean,
-                                     const unsigned long long* __restrict__ maxbits,
-                                     int8_t* __restrict__ B, int64_t rows_per_block,
-                                     double* __restrict__ qpart) {
-    // block b handles samples [b * rows_per_block, ...) of every column
-    const int64_t i0 = (int64_t)blockIdx.x * rows_per_block;
-    const int64_t i1 = min(n_pad, i0 + rows_per_block);
-    for (int64_t c = 0; c < kp; ++c) {
+// Rows-pass operand: B1[q*kp + c][i] (int8 pieces of (x_ic - mean_c) 127 / max_c, i < n_pad)
+// and per-tile sums of the represented values qpart[blockIdx.x][c].
+__global__ void __launch_bounds__(256)
+k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k, int64_t kp,
+                     int64_t n_pad, const double* __restrict__ mean,
+                     const unsigned long long* __restrict__ maxbits, int8_t* __restrict__ B,
+                     double* __restrict__ qpart) {
+    __shared__ double tile[kPrepRows][kPrepCols + 1];
+    __shared__ double red[8][kPrepCols];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int64_t c0 = (int64_t)blockIdx.y * kPrepCols, r0 = (int64_t)blockIdx.x * kPrepRows;
+    for (int rr = ty; rr < kPrepRows; rr += 8) {
+        const int64_t r = r0 + rr, c = c0 + tx;
+        tile[rr][tx] = (r < n && c < k) ? X[r * ld + c] : 0.0;
+    }
+    __syncthreads();
+    // each warp handles 4 columns; lane covers rows lane and lane + 32
+    double qs[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int cc = 0; cc < 4; ++cc) {
+        const int col = ty * 4 + cc;
+        const int64_t c = c0 + col;
+        if (c >= kp) continue;
         const double f = c < k ? quant_factor(maxbits[c]) : 0.0;
-        double s = 0.0;
-        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const double mc = c < k ? mean[c] : 0.0;
+        for (int rr = tx; rr < kPrepRows; rr += 32) {
+            const int64_t i = r0 + rr;
+            if (i >= n_pad) continue;
             int8_t q1 = 0, q2 = 0, q3 = 0;
-            if (c < k && i < n) s += quantise3((X[i * ld + c] - mean[c]) * f, q1, q2, q3);
+            if (c < k && i < n) qs[cc] += quantise3((tile[rr][col] - mc) * f, q1, q2, q3);
             B[c * n_pad + i] = q1;
             B[(kp + c) * n_pad + i] = q2;
             B[(2 * kp + c) * n_pad + i] = q3;
         }
-        // fixed-order block reduction
-        __shared__ double red[256];
-        red[threadIdx.x] = s;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0 && c < k) qpart[(int64_t)blockIdx.x * k + c] = red[0];
-        __syncthreads();
+    }
+    for (int cc = 0; cc < 4; ++cc) {
+        double v = qs[cc];
+        for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (tx == 0) red[0][ty * 4 + cc] = v;  // lane 0 of warp ty owns columns 4ty..4ty+3
+    }
+    __syncthreads();
+    if (threadIdx.x < kPrepCols) {
+        const int64_t c = c0 + threadIdx.x;
+        if (c < k) qpart[(int64_t)blockIdx.x * k + c] = red[0][threadIdx.x];
     }
 }
 
-// Rows-pass reduction: u_tc = s_t (mean_c exc_t + (sum_z part[z][c][t] - mu_t Q_c) / f_c),
-// W[t][c] = s_t u_tc; maxima of |W| and |mu W| per column.
-__global__ void k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t ld,
-                              int64_t R, int64_t k, const double* __restrict__ s_row,
-                              const double* __restrict__ exc_row, const double* __restrict__ mu,
-                              const double* __restrict__ mean, const double* __restrict__ qsum,
-                              const unsigned long long* __restrict__ maxbits_in,
-                              double* __restrict__ W, unsigned long long* __restrict__ max_w,
-                              unsigned long long* __restrict__ max_muw) {
-    const int64_t total = R * k;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = idx / R, t = idx - c * R;
+// Rows-pass reduction, one column per blockIdx.y and 2048 rows per blockIdx.x:
+//   inner_tc = (sum_z part[z][c][t] - mu_t Q_c) / f_c + mean_c exc_t
+// out = inner * s_t^spow written column-major (out[c * out_ld + t]) or row-major
+// (out[t * out_ld + c]); optional maxima of |out| and |mu out| per column.
+__global__ void __launch_bounds__(256)
+k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t ld, int64_t R,
+              int64_t k, const double* __restrict__ s_row, int spow,
+              const double* __restrict__ exc_row, const double* __restrict__ mu,
+              const double* __restrict__ mean, const double* __restrict__ qsum,
+              const unsigned long long* __restrict__ maxbits_in, double* __restrict__ out,
+              int64_t out_ld, int colmajor, unsigned long long* __restrict__ max_w,
+              unsigned long long* __restrict__ max_muw) {
+    __shared__ double red_w[8], red_m[8];
+    const int64_t c = blockIdx.y;
+    const double f = quant_factor(maxbits_in[c]);
+    const double inv_f = f > 0.0 ? 1.0 / f : 0.0;
+    const double mc = mean[c], qc = qsum[c];
+    double mw = 0.0, mm = 0.0;
+    const int64_t t0 = (int64_t)blockIdx.x * 2048;
+    for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) {
         double acc = 0.0;
         for (int z = 0; z < splits; ++z) acc += part[((int64_t)z * kp + c) * ld + t];
-        const double f = quant_factor(maxbits_in[c]);
-        const double inner = f > 0.0 ? (acc - mu[t] * qsum[c]) / f : 0.0;
-        const double u = s_row[t] * (mean[c] * exc_row[t] + inner);
-        const double w = s_row[t] * u;
-        W[t * k + c] = w;
-        atomicMax(max_w + c, (unsigned long long)__double_as_longlong(fabs(w)));
-        atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(fabs(mu[t] * w)));
+        double v = (acc - mu[t] * qc) * inv_f + mc * exc_row[t];
+        if (s_row) {
+            v *= s_row[t];
+            if (spow == 2) v *= s_row[t];
+        }
+        if (colmajor) out[c * out_ld + t] = v;
+        else out[t * out_ld + c] = v;
+        mw = fmax(mw, fabs(v));
+        mm = fmax(mm, fabs(mu[t] * v));
+    }
+    if (max_w) {
+        for (int off = 16; off; off >>= 1) {
+            mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
+            mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            red_w[threadIdx.x >> 5] = mw;
+            red_m[threadIdx.x >> 5] = mm;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int j = 1; j < 8; ++j) {
+                mw = fmax(mw, red_w[j]);
+                mm = fmax(mm, red_m[j]);
+            }
+            atomicMax(max_w + c, (unsigned long long)__double_as_longlong(mw));
+            atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(mm));
+        }
     }
 }
 
-// Samples-pass operand B2: pieces of W f2 (rows q*kp + c) and of (mu o W) f3 (rows
-// (3 + q) kp + c), t < r_pad; 1/f2, 1/f3 per column.
-__global__ void k_split_samples_operand(const double* __restrict__ W, int64_t R, int64_t k,
-                                        int64_t kp, int64_t r_pad, const double* __restrict__ mu,
-                                        const unsigned long long* __restrict__ max_w,
-                                        const unsigned long long* __restrict__ max_muw,
-                                        int8_t* __restrict__ B, double* __restrict__ inv_f2,
-                                        double* __restrict__ inv_f3) {
-    const int64_t total = kp * r_pad;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = idx / r_pad, t = idx - c * r_pad;
+// Samples-pass operand from W^T (column-major, k x R): pieces of W f2 (rows q kp + c) and
+// of (mu o W) f3 (rows (3 + q) kp + c), t < r_pad; 1/f2, 1/f3 per column; and per-block
+// sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].  Grid: (r_pad / 2048, kp).
+__global__ void __launch_bounds__(256)
+k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int64_t kp,
+                        int64_t r_pad, const double* __restrict__ mu,
+                        const unsigned long long* __restrict__ max_w,
+                        const unsigned long long* __restrict__ max_muw, int8_t* __restrict__ B,
+                        double* __restrict__ inv_f2, double* __restrict__ inv_f3,
+                        double* __restrict__ cpart) {
+    __shared__ double red[8];
+    const int64_t c = blockIdx.y;
+    const double f2 = c < k ? quant_factor(max_w[c]) : 0.0;
+    const double f3 = c < k ? quant_factor(max_muw[c]) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        inv_f2[c] = f2 > 0.0 ? 1.0 / f2 : 0.0;
+        inv_f3[c] = f3 > 0.0 ? 1.0 / f3 : 0.0;
+    }
+    double cs = 0.0;
+    const int64_t t0 = (int64_t)blockIdx.x * 2048;
+    for (int64_t t = t0 + threadIdx.x; t < min(r_pad, t0 + 2048); t += 256) {
         int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0;
-        const double f2 = c < k ? quant_factor(max_w[c]) : 0.0;
-        const double f3 = c < k ? quant_factor(max_muw[c]) : 0.0;
         if (c < k && t < R) {
-            const double w = W[t * k + c];
+            const double w = Wt[c * R + t];
             quantise3(w * f2, a1, a2, a3);
             quantise3(mu[t] * w * f3, b1, b2, b3);
-        }
-        if (t == 0) {
-            inv_f2[c] = f2 > 0.0 ? 1.0 / f2 : 0.0;
-            inv_f3[c] = f3 > 0.0 ? 1.0 / f3 : 0.0;
+            cs += mu[t] * w;
         }
         B[c * r_pad + t] = a1;
         B[(kp + c) * r_pad + t] = a2;
@@ -447,18 +506,12 @@ __global__ void k_split_samples_operand(const double* __restrict__ W, int64_t R,
         B[(4 * kp + c) * r_pad + t] = b2;
         B[(5 * kp + c) * r_pad + t] = b3;
     }
-}
-
-// c0[b][c] = sum_{t in block b} mu_t W[t][c]
-__global__ void k_centring_partials(const double* __restrict__ W, int64_t R, int64_t k,
-                                    int64_t rows_per_block, const double* __restrict__ mu,
-                                    double* __restrict__ part) {
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
-    const int64_t r1 = min(R, r0 + rows_per_block);
-    for (int64_t c = threadIdx.x; c < k; c += blockDim.x) {
-        double s = 0.0;
-        for (int64_t t = r0; t < r1; ++t) s += mu[t] * W[t * k + c];
-        part[(int64_t)blockIdx.x * k + c] = s;
+    for (int off = 16; off; off >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cs;
+    __syncthreads();
+    if (threadIdx.x == 0 && c < k) {
+        for (int j = 1; j < 8; ++j) cs += red[j];
+        cpart[(int64_t)blockIdx.x * k + c] = cs;
     }
 }
 
@@ -469,7 +522,7 @@ __global__ void k_reduce_samples(const double* __restrict__ part, int splits, in
     const int64_t total = n * k;
     for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
          idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = idx / n, i = idx - c * n;
+        const int64_t i = idx / k, c = idx - i * k;  // c fastest: coalesced Y rows
         double acc = 0.0;
         for (int z = 0; z < splits; ++z) acc += part[((int64_t)z * kp + c) * ld + i];
         Y[i * ldy + c] = (acc - c0[c]) * inv_m;
@@ -528,59 +581,248 @@ int choose_splits(int64_t units_per_split, int kb_total, int64_t target) {
 
 }  // namespace
 
-struct MixedOperator {
+struct MixedRows {
+    // a packed view with per-row centring statistics, ready for the rows pass
     int64_t R = 0, n = 0, r_pad = 0, n_pad = 0;
-    DeviceBuffer<double> mu, s, exc;
-    CUtensorMap tm_rows{}, tm_samples{};
+    DeviceBuffer<double> mu, exc, s;
+    CUtensorMap tm{};
+};
+
+struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f2, inv_f3;
     DeviceBuffer<unsigned long long> max1, max_w, max_muw;
     CUtensorMap tm_b1{}, tm_b2{};
     const void* tm_b1_base = nullptr;
     const void* tm_b2_base = nullptr;
-    int64_t tm_kp = -1;
+    int64_t tm_b1_key = -1, tm_b2_key = -1;
     DeviceBuffer<int> status;
 };
 
+struct MixedOperator {
+    MixedRows rows;
+    MixedWorkspace ws;
+};
+
 void destroy_mixed(MixedOperator* m) { delete m; }
+
+namespace {
+
+void configure_kernels() {
+    static std::once_flag once;
+    static cudaError_t err = cudaSuccess;
+    std::call_once(once, [] {
+        err = cudaFuncSetAttribute(k_mixed_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   Layout<true>::kSmem);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_mixed_pass<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       Layout<false>::kSmem);
+    });
+    check_cuda(err, "configure tensor-core kernels");
+}
+
+// Per-row statistics: mu_t, exc_t = S_t - mu_t n_t (from code counts c00, c01, c10, c11),
+// optional multiplier s_t.
+void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const int32_t* counts,
+               const double* s_or_null) {
+    configure_kernels();
+    r.R = v.n_rows;
+    r.n = v.n_samples;
+    r.r_pad = round_up(std::max<int64_t>(r.R, 1), kTile);
+    r.n_pad = round_up(std::max<int64_t>(r.n, 1), kTile);
+    std::vector<double> mu(r.r_pad, 0.0), ex(r.r_pad, 0.0), sv(r.r_pad, 0.0);
+    for (int64_t t = 0; t < r.R; ++t) {
+        const double mt = mean[t];
+        mu[t] = mt;
+        const int64_t c00 = counts[4 * t], c10 = counts[4 * t + 2], c11 = counts[4 * t + 3];
+        ex[t] = (double)(2 * c00 + c10) - mt * (double)(c00 + c10 + c11);
+        sv[t] = s_or_null ? s_or_null[t] : 1.0;
+    }
+    r.mu.resize(r.r_pad);
+    r.exc.resize(r.r_pad);
+    r.s.resize(r.r_pad);
+    CS_CUDA(cudaMemcpy(r.mu.get(), mu.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemcpy(r.exc.get(), ex.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemcpy(r.s.get(), sv.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
+    // packed tiles: 32 bytes (128 samples) x 128 SNP rows; rows past R read as zeros and
+    // either land in discarded output rows (rows pass) or meet zero B rows (samples pass)
+    r.tm = make_map_u8(v.rows, v.stride, std::max<int64_t>(r.R, 1), v.stride, 32, kTile, false);
+}
+
+struct Tiling {
+    int n_ctiles, kc;
+    int64_t kp;
+};
+
+Tiling tiling_for(int64_t k) {
+    Tiling t;
+    t.n_ctiles = (int)((k + kMaxKc - 1) / kMaxKc);
+    t.kc = (int)round_up((k + t.n_ctiles - 1) / t.n_ctiles, 16);
+    t.kp = (int64_t)t.kc * t.n_ctiles;
+    return t;
+}
+
+void check_status(MixedWorkspace& ws, cudaStream_t s) {
+    int status = 0;
+    CS_CUDA(cudaMemcpyAsync(&status, ws.status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    if (status != 0) {
+        cudaMemset(ws.status.get(), 0, sizeof(int));
+        fail(CS_ERR_CUDA, "tensor-core kinship kernel gave up waiting (status " +
+                              std::to_string(status) + ")");
+    }
+}
+
+// Rows pass over a MixedRows context: for X (n x k, row-major ldx),
+//   out_tc = s_t^spow ( sum_i (G_ti - mu_t)[obs] x_ic )  (mean-imputed centred dosages)
+// written column-major (out[c * out_ld + t]) or row-major.  With want_max, also the
+// per-column maxima of |out| and |mu out| (samples-pass operand scales).
+void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, int64_t k,
+               double* out, int64_t out_ld, bool colmajor, int spow, bool want_max,
+               cudaStream_t s) {
+    const Tiling tl = tiling_for(k);
+    const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
+    const int kb = (int)(n_pad / kKBlock);
+    const int64_t tiles = r_pad / kTile;
+    const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    const int kbs = (kb + splits - 1) / splits;
+    const int rt = (int)((n_pad + kPrepRows - 1) / kPrepRows);
+    const int nbs = (int)std::min<int64_t>(512, std::max<int64_t>(1, n / 128));
+    const int64_t rpb = (n + nbs - 1) / nbs;
+    const int nbu = (int)((n + rpb - 1) / rpb);
+    ws.b1.resize(3 * kp * n_pad);
+    ws.part.resize((int64_t)splits * kp * r_pad);
+    ws.colpart.resize((int64_t)std::max(rt, nbu) * k);
+    ws.mean1.resize(k);
+    ws.qsum.resize(k);
+    ws.max1.resize(k);
+    ws.max_w.resize(k);
+    ws.max_muw.resize(k);
+    if (!ws.status.get()) {
+        ws.status.resize(1);
+        CS_CUDA(cudaMemset(ws.status.get(), 0, sizeof(int)));
+    }
+    const int64_t key = kp * 1000003 + n_pad;
+    if (ws.tm_b1_base != ws.b1.get() || ws.tm_b1_key != key) {
+        ws.tm_b1 = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, tl.kc, true);
+        ws.tm_b1_base = ws.b1.get();
+        ws.tm_b1_key = key;
+    }
+    {
+        prof::Scope ps("mixed_prep_rows_operand", s, 0.0, 24.0 * n * k + 3.0 * kp * n_pad);
+        k_col_partial_sums<<<nbu, 128, 0, s>>>(X, ldx, n, k, rpb, ws.colpart.get());
+        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), nbu, k, 1.0 / (double)n,
+                                         ws.mean1.get(), ws.max1.get());
+        dim3 g1((unsigned)((n + kPrepRows - 1) / kPrepRows), (unsigned)((k + kPrepCols - 1) / kPrepCols));
+        k_col_absmax<<<g1, 256, 0, s>>>(X, ldx, n, k, ws.mean1.get(), ws.max1.get());
+        dim3 g2((unsigned)rt, (unsigned)((kp + kPrepCols - 1) / kPrepCols));
+        k_split_rows_operand<<<g2, 256, 0, s>>>(X, ldx, n, k, kp, n_pad, ws.mean1.get(),
+                                                ws.max1.get(), ws.b1.get(), ws.colpart.get());
+        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), rt, k, 1.0, ws.qsum.get(), nullptr);
+        CS_LAUNCH("mixed rows operand");
+    }
+    PassArgs P{};
+    P.n_tiles = (int)tiles;
+    P.n_ctiles = tl.n_ctiles;
+    P.n_splits = splits;
+    P.kb_total = kb;
+    P.kb_per_split = kbs;
+    P.kc = tl.kc;
+    P.kp = (int)kp;
+    P.mu = r.mu.get();
+    P.part = ws.part.get();
+    P.ld = r_pad;
+    P.status = ws.status.get();
+    {
+        // algorithmic work: 2 n R k flops, one pass over the packed rows
+        prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
+                       (double)R * (double)((n + 3) / 4));
+        k_mixed_pass<true><<<num_sms(), kThreads, Layout<true>::kSmem, s>>>(r.tm, ws.tm_b1, P);
+        CS_LAUNCH("kinship_rows_tc");
+    }
+    if (want_max) {
+        CS_CUDA(cudaMemsetAsync(ws.max_w.get(), 0, 8 * k, s));
+        CS_CUDA(cudaMemsetAsync(ws.max_muw.get(), 0, 8 * k, s));
+    }
+    {
+        prof::Scope ps("mixed_reduce_rows", s, 0.0, 8.0 * splits * kp * R + 8.0 * R * k);
+        dim3 g((unsigned)((R + 2047) / 2048), (unsigned)k);
+        k_reduce_rows<<<g, 256, 0, s>>>(ws.part.get(), splits, kp, r_pad, R, k, r.s.get(), spow,
+                                        r.exc.get(), r.mu.get(), ws.mean1.get(), ws.qsum.get(),
+                                        ws.max1.get(), out, out_ld, colmajor ? 1 : 0,
+                                        want_max ? ws.max_w.get() : nullptr,
+                                        want_max ? ws.max_muw.get() : nullptr);
+        CS_LAUNCH("reduce_rows");
+    }
+}
+
+// Samples pass: Y (n x k, row-major ldy) = (Z W) / M for W^T (k x R, column-major) with the
+// per-column maxima computed by rows_pass(want_max).
+void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
+                  double* Y, int64_t ldy, cudaStream_t s) {
+    const Tiling tl = tiling_for(k);
+    const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
+    const int kb = (int)(r_pad / kKBlock);
+    const int64_t tiles = n_pad / kTile;
+    const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    const int kbs = (kb + splits - 1) / splits;
+    const int nrb = (int)((r_pad + 2047) / 2048);
+    ws.b2.resize(6 * kp * r_pad);
+    ws.part.resize((int64_t)splits * kp * n_pad);
+    ws.colpart.resize((int64_t)nrb * k);
+    ws.inv_f2.resize(kp);
+    ws.inv_f3.resize(kp);
+    ws.c0.resize(k);
+    const int64_t key = kp * 1000003 + r_pad;
+    if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
+        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc, true);
+        ws.tm_b2_base = ws.b2.get();
+        ws.tm_b2_key = key;
+    }
+    {
+        prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + 6.0 * kp * r_pad);
+        dim3 g((unsigned)nrb, (unsigned)kp);
+        k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), ws.max_w.get(),
+                                                  ws.max_muw.get(), ws.b2.get(), ws.inv_f2.get(),
+                                                  ws.inv_f3.get(), ws.colpart.get());
+        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get(), nullptr);
+        CS_LAUNCH("mixed samples operand");
+    }
+    PassArgs P{};
+    P.n_tiles = (int)tiles;
+    P.n_ctiles = tl.n_ctiles;
+    P.n_splits = splits;
+    P.kb_total = kb;
+    P.kb_per_split = kbs;
+    P.kc = tl.kc;
+    P.kp = (int)kp;
+    P.inv_f2 = ws.inv_f2.get();
+    P.inv_f3 = ws.inv_f3.get();
+    P.part = ws.part.get();
+    P.ld = n_pad;
+    P.status = ws.status.get();
+    {
+        prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
+                       (double)R * (double)((n + 3) / 4));
+        k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2, P);
+        CS_LAUNCH("kinship_samples_tc");
+    }
+    {
+        prof::Scope ps("mixed_reduce_samples", s, 0.0, 8.0 * splits * kp * n + 8.0 * n * k);
+        k_reduce_samples<<<blocks_for(n * k), 256, 0, s>>>(ws.part.get(), splits, kp, n_pad, n, k,
+                                                           ws.c0.get(), inv_m, Y, ldy);
+        CS_LAUNCH("reduce_samples");
+    }
+}
+
+}  // namespace
 
 static MixedOperator* mixed_for(cs_kinship* op) {
     if (op->mixed) return op->mixed;
     auto* m = new MixedOperator();
     try {
-        const int64_t R = op->n_active, n = op->rows;
-        m->R = R;
-        m->n = n;
-        m->r_pad = round_up(std::max<int64_t>(R, 1), kTile);
-        m->n_pad = round_up(std::max<int64_t>(n, 1), kTile);
-        std::vector<double> mu(m->r_pad, 0.0), sv(m->r_pad, 0.0), ex(m->r_pad, 0.0);
-        for (int64_t t = 0; t < R; ++t) {
-            const double mt = op->mean[t];
-            mu[t] = mt;
-            sv[t] = op->inv_std[t];
-            const int64_t c00 = op->counts[4 * t], c10 = op->counts[4 * t + 2], c11 = op->counts[4 * t + 3];
-            ex[t] = (double)(2 * c00 + c10) - mt * (double)(c00 + c10 + c11);  // S_t - mu_t n_t
-        }
-        m->mu.resize(m->r_pad);
-        m->s.resize(m->r_pad);
-        m->exc.resize(m->r_pad);
-        CS_CUDA(cudaMemcpy(m->mu.get(), mu.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
-        CS_CUDA(cudaMemcpy(m->s.get(), sv.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
-        CS_CUDA(cudaMemcpy(m->exc.get(), ex.data(), 8 * m->r_pad, cudaMemcpyHostToDevice));
-        // packed genotype tiles: 32 bytes (128 samples) x 128 SNP rows; rows past R read as
-        // zeros and meet zero B rows (samples pass) or land in discarded output rows
-        m->tm_rows = make_map_u8(op->view.rows, op->view.stride, R, op->view.stride, 32, kTile, false);
-        m->tm_samples = m->tm_rows;
-        m->status.resize(1);
-        CS_CUDA(cudaMemset(m->status.get(), 0, sizeof(int)));
-        static bool configured = false;
-        if (!configured) {
-            CS_CUDA(cudaFuncSetAttribute(k_mixed_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Layout<true>::kSmem));
-            CS_CUDA(cudaFuncSetAttribute(k_mixed_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Layout<false>::kSmem));
-            configured = true;
-        }
+        init_rows(m->rows, op->view, op->mean.data(), op->counts.data(), op->inv_std.data());
     } catch (...) {
         delete m;
         throw;
@@ -598,129 +840,37 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
         return;
     }
     MixedOperator* m = mixed_for(op);
-    const int n_ctiles = (int)((k + kMaxKc - 1) / kMaxKc);
-    const int kc = (int)round_up((k + n_ctiles - 1) / n_ctiles, 16);
-    const int64_t kp = (int64_t)kc * n_ctiles;
-    const int64_t r_pad = m->r_pad, n_pad = m->n_pad;
-    const int kb1 = (int)(n_pad / kKBlock), kb2 = (int)(r_pad / kKBlock);
-    const int64_t tiles1 = r_pad / kTile, tiles2 = n_pad / kTile;
-    const int64_t target = 8LL * num_sms();
-    const int splits1 = choose_splits(tiles1 * n_ctiles, kb1, target);
-    const int splits2 = choose_splits(tiles2 * n_ctiles, kb2, target);
-    const int kbs1 = (kb1 + splits1 - 1) / splits1, kbs2 = (kb2 + splits2 - 1) / splits2;
-    const int nb = (int)std::min<int64_t>(512, std::max<int64_t>(1, std::max(n_pad, R) / 128));
-    m->b1.resize(3 * kp * n_pad);
-    m->b2.resize(6 * kp * r_pad);
-    m->part.resize(std::max<int64_t>((int64_t)splits1 * kp * r_pad, (int64_t)splits2 * kp * n_pad));
-    m->colpart.resize((int64_t)nb * k);
-    for (auto* b : {&m->mean1, &m->qsum, &m->c0}) b->resize(k);
-    for (auto* b : {&m->inv_f2, &m->inv_f3}) b->resize(kp);
-    for (auto* b : {&m->max1, &m->max_w, &m->max_muw}) b->resize(k);
-    m->W.resize(R * k);
-    if (m->tm_b1_base != m->b1.get() || m->tm_kp != kp)
-        m->tm_b1 = make_map_u8(m->b1.get(), n_pad, 3 * kp, n_pad, kKBlock, kc, true);
-    if (m->tm_b2_base != m->b2.get() || m->tm_kp != kp)
-        m->tm_b2 = make_map_u8(m->b2.get(), r_pad, 6 * kp, r_pad, kKBlock, kc, true);
-    m->tm_b1_base = m->b1.get();
-    m->tm_b2_base = m->b2.get();
-    m->tm_kp = kp;
-    const int grid = num_sms();
-    // ---- rows pass: U = Z^T X
-    {
-        const int64_t rpb = (n + nb - 1) / nb;
-        const int nbu = (int)((n + rpb - 1) / rpb);
-        const int64_t ipb = (n_pad + nb - 1) / nb;
-        const int nbi = (int)((n_pad + ipb - 1) / ipb);
-        {
-            prof::Scope ps("mixed_prep_rows_operand", s, 0.0, 24.0 * n * k + 3.0 * kp * n_pad);
-            k_col_partial_sums<<<nbu, 128, 0, s>>>(X, ldx, n, k, rpb, m->colpart.get());
-            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbu, k, 1.0 / (double)n,
-                                             m->mean1.get(), m->max1.get());
-            k_col_absmax<<<blocks_for(n * k), 256, 0, s>>>(X, ldx, n, k, m->mean1.get(), m->max1.get());
-            k_split_rows_operand<<<nbi, 256, 0, s>>>(X, ldx, n, k, kp, n_pad, m->mean1.get(),
-                                                     m->max1.get(), m->b1.get(), ipb,
-                                                     m->colpart.get());
-            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbi, k, 1.0, m->qsum.get(), nullptr);
-            CS_LAUNCH("mixed rows operand");
-        }
-        PassArgs P{};
-        P.n_tiles = (int)tiles1;
-        P.n_ctiles = n_ctiles;
-        P.n_splits = splits1;
-        P.kb_total = kb1;
-        P.kb_per_split = kbs1;
-        P.kc = kc;
-        P.kp = (int)kp;
-        P.mu = m->mu.get();
-        P.part = m->part.get();
-        P.ld = r_pad;
-        P.status = m->status.get();
-        {
-            // algorithmic work: 2 n R k flops, one pass over the packed rows
-            prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
-                           (double)R * (double)((n + 3) / 4));
-            k_mixed_pass<true><<<grid, kThreads, Layout<true>::kSmem, s>>>(m->tm_rows, m->tm_b1, P);
-            CS_LAUNCH("kinship_rows_tc");
-        }
-        CS_CUDA(cudaMemsetAsync(m->max_w.get(), 0, 8 * k, s));
-        CS_CUDA(cudaMemsetAsync(m->max_muw.get(), 0, 8 * k, s));
-        {
-            prof::Scope ps("mixed_reduce_rows", s, 0.0, 8.0 * splits1 * kp * R + 8.0 * R * k);
-            k_reduce_rows<<<blocks_for(R * k), 256, 0, s>>>(
-                m->part.get(), splits1, kp, r_pad, R, k, m->s.get(), m->exc.get(), m->mu.get(),
-                m->mean1.get(), m->qsum.get(), m->max1.get(), m->W.get(), m->max_w.get(),
-                m->max_muw.get());
-            CS_LAUNCH("reduce_rows");
-        }
+    m->ws.W.resize(R * k);
+    // W^T = s o s o (Z-centred)^T X: the rows pass output already scaled for the samples pass
+    rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s);
+    samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s);
+    check_status(m->ws, s);
+}
+
+// Scan projection on tensor cores: T[t][c] = sum_i (g_ti - m_t)[observed] B[i][c] for every row
+// of a packed view (the analysed samples), m_t = per-row mean of the observed dosages.
+struct MixedScan {
+    MixedRows rows;
+    MixedWorkspace ws;
+};
+
+MixedScan* mixed_scan_create(const cs_packed_view& v, const double* row_mean, const int32_t* counts) {
+    auto* m = new MixedScan();
+    try {
+        init_rows(m->rows, v, row_mean, counts, nullptr);
+    } catch (...) {
+        delete m;
+        throw;
     }
-    // ---- samples pass: Y = Z W / M
-    {
-        const int64_t rpb = (R + nb - 1) / nb;
-        const int nbr = (int)((R + rpb - 1) / rpb);
-        {
-            prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 16.0 * R * k + 6.0 * kp * r_pad);
-            k_split_samples_operand<<<blocks_for(kp * r_pad), 256, 0, s>>>(
-                m->W.get(), R, k, kp, r_pad, m->mu.get(), m->max_w.get(), m->max_muw.get(),
-                m->b2.get(), m->inv_f2.get(), m->inv_f3.get());
-            k_centring_partials<<<nbr, 128, 0, s>>>(m->W.get(), R, k, rpb, m->mu.get(), m->colpart.get());
-            k_sum_partials<<<1, 256, 0, s>>>(m->colpart.get(), nbr, k, 1.0, m->c0.get(), nullptr);
-            CS_LAUNCH("mixed samples operand");
-        }
-        PassArgs P{};
-        P.n_tiles = (int)tiles2;
-        P.n_ctiles = n_ctiles;
-        P.n_splits = splits2;
-        P.kb_total = kb2;
-        P.kb_per_split = kbs2;
-        P.kc = kc;
-        P.kp = (int)kp;
-        P.inv_f2 = m->inv_f2.get();
-        P.inv_f3 = m->inv_f3.get();
-        P.part = m->part.get();
-        P.ld = n_pad;
-        P.status = m->status.get();
-        {
-            prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
-                           (double)R * (double)((n + 3) / 4));
-            k_mixed_pass<false><<<grid, kThreads, Layout<false>::kSmem, s>>>(m->tm_samples, m->tm_b2, P);
-            CS_LAUNCH("kinship_samples_tc");
-        }
-        {
-            prof::Scope ps("mixed_reduce_samples", s, 0.0, 8.0 * splits2 * kp * n + 8.0 * n * k);
-            k_reduce_samples<<<blocks_for(n * k), 256, 0, s>>>(
-                m->part.get(), splits2, kp, n_pad, n, k, m->c0.get(),
-                1.0 / (double)op->num_variants, Y, ldy);
-            CS_LAUNCH("reduce_samples");
-        }
-    }
-    int status = 0;
-    CS_CUDA(cudaMemcpyAsync(&status, m->status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-    CS_CUDA(cudaStreamSynchronize(s));
-    if (status != 0) {
-        cudaMemset(m->status.get(), 0, sizeof(int));
-        fail(CS_ERR_CUDA, "tensor-core kinship kernel gave up waiting (status " +
-                              std::to_string(status) + ")");
-    }
+    return m;
+}
+
+void mixed_scan_destroy(MixedScan* m) { delete m; }
+
+void mixed_scan_project(MixedScan* m, const double* B, int64_t ldb, int64_t k, double* T,
+                        int64_t ldt, cudaStream_t s) {
+    rows_pass(m->rows, m->ws, B, ldb, k, T, ldt, false, 1, false, s);
+    check_status(m->ws, s);
 }
 
 }  // namespace cs

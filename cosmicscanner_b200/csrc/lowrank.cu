@@ -621,7 +621,7 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         CS_CUDA(cudaMemcpyAsync(counts.data(), d_counts.get(), 16 * M, cudaMemcpyDeviceToHost, s));
         CS_CUDA(cudaStreamSynchronize(s));
     }
-    std::vector<double> lut(4 * M, 0.0), gn2(M, 0.0), fr(M, 0.0);
+    std::vector<double> lut(4 * M, 0.0), gn2(M, 0.0), fr(M, 0.0), row_mean(M, 0.0);
     std::vector<uint8_t> pass(M, 0);
     for (int64_t j = 0; j < M; ++j) {
         const int64_t c00 = counts[4 * j], c10 = counts[4 * j + 2], c11 = counts[4 * j + 3];
@@ -634,6 +634,7 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         pass[j] = obs >= 3 && std::min(af, 1.0 - af) >= min_maf;
         if (!pass[j]) continue;
         const double mean = dosage_sum / (double)obs;  // encoded mean (additive model)
+        row_mean[j] = mean;
         lut[4 * j + 0] = 2.0 - mean;
         lut[4 * j + 1] = 0.0;  // missing -> mean -> centred 0
         lut[4 * j + 2] = 1.0 - mean;
@@ -663,9 +664,19 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         CS_CUDA(cudaMemcpyAsync(d_inv.get(), info_inv.data(), 8 * p * p, cudaMemcpyHostToDevice, s));
     }
     // ---- T = G_c^T [U | X | py]: the per-SNP projections (the scan's GEMM)
-    (void)precision;  // the FP64 decode-GEMM serves both forms of the scan for now
-    Workspace ws;
-    decode_gemm_rows_fp64(v, d_lut.get(), Bm, bw, bw, d_T.get(), bw, ws, s);
+    if (precision == CS_PRECISION_MIXED) {
+        MixedScan* ms = mixed_scan_create(v, row_mean.data(), counts.data());
+        try {
+            mixed_scan_project(ms, Bm, bw, bw, d_T.get(), bw, s);
+        } catch (...) {
+            mixed_scan_destroy(ms);
+            throw;
+        }
+        mixed_scan_destroy(ms);
+    } else {
+        Workspace ws;
+        decode_gemm_rows_fp64(v, d_lut.get(), Bm, bw, bw, d_T.get(), bw, ws, s);
+    }
     ScanParams P;
     P.n_snps = M; P.rank = r; P.p = p; P.ldt = bw; P.base = base;
     P.T = d_T.get(); P.c = d_cv.get(); P.UtX = d_utx.get(); P.info_inv = d_inv.get();

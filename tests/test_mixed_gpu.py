@@ -1,0 +1,103 @@
+"""Tensor-core (int8 tcgen05) form of the kinship operator and of the low-rank LMM.
+
+Tolerances are those stated for the mixed form against the FP64 oracle: every operator
+apply within 1e-6 relative error (max-norm per column), variance components and BETA/SE
+within 1e-5 relative, -log10 P within 1e-3 absolute.  Cases cover the reference's
+partial-byte fixture (N=37), sample subsets, repeated / permuted rows, LOCO-like variant
+masks, intercept-like columns and column counts that span several column tiles.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.test_oracle import M, N, selections
+
+pytestmark = pytest.mark.gpu
+
+cs = pytest.importorskip("cosmicscanner_b200")
+synth = pytest.importorskip("cosmicscanner_b200.synth")
+
+
+def colwise_rel(Y, E):
+    scale = np.maximum(np.abs(E).max(axis=0), 1e-300)
+    return (np.abs(Y - E).max(axis=0) / scale)
+
+
+def test_batch_fixture_mixed():
+    sels = selections()
+    rows = [N if k is None else len(k) for k, _ in sels]
+    bed, omega = oracle.kinship_batch_fixture(N, M, 8128, rows=rows)
+    ref = oracle.Bed(bed[3:].reshape(M, -1), N)
+    g = cs.Genotypes.from_bed_bytes(bed, N, M)
+    off = 0
+    for (keep, snps), r in zip(sels, rows):
+        op = cs.createKinshipOperator(g, keep, snps)
+        for w in (1, 7, 41):
+            om = omega[off:off + r * w].reshape(w, r).T
+            off += r * w
+            E = ref.apply_block(om, keep, snps)
+            Y = op.apply(om, precision="mixed")
+            assert colwise_rel(Y, E).max() < 1e-6
+            again = op.apply(om, precision="mixed")
+            assert np.array_equal(again, Y), "mixed apply is not bitwise repeatable"
+
+
+@pytest.mark.parametrize("k", [1, 5, 16, 65, 68, 81, 266])
+def test_operator_mixed_random(k):
+    d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    op = cs.createKinshipOperator(g)
+    rng = np.random.default_rng(k)
+    X = rng.standard_normal((d["n"], k))
+    if k > 2:
+        X[:, 0] = 1.0           # intercept: K 1 ~ 0, compared in absolute terms below
+        X[:, 1] += 25.0         # large column mean
+    E = ref.apply_block(X, n_threads=8)
+    Y = op.apply(X, precision="mixed")
+    rel = colwise_rel(Y, E)
+    if k > 2:
+        assert np.abs(Y[:, 0] - E[:, 0]).max() < 1e-6 * np.abs(E[:, 2:]).max()
+        assert rel[1:].max() < 1e-6, rel.max()
+    else:
+        assert rel.max() < 1e-6
+
+
+def test_operator_mixed_selection():
+    d = synth.cohort(3000, 2500, 23, missing=0.03, n_causal=10)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    rng = np.random.default_rng(4)
+    keep = rng.choice(d["n"], 2100, replace=False).astype(np.int32)     # unsorted subset
+    variants = np.sort(rng.choice(d["m"], 1700, replace=False)).astype(np.int32)
+    op = cs.createKinshipOperator(g, keep, variants)
+    X = rng.standard_normal((len(keep), 33))
+    E = ref.apply_block(X, keep, variants, n_threads=8)
+    assert colwise_rel(op.apply(X, precision="mixed"), E).max() < 1e-6
+
+
+def test_lowrank_mixed_matches_oracle():
+    d = synth.cohort(1500, 4000, 29, missing=0.02, n_causal=60, h2=0.5)
+    n = d["n"]
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), n)
+    g = cs.Genotypes.from_bed_bytes(d["bed"], n, d["m"])
+    y = d["y"]
+    X = d["X"].astype(np.float32).astype(np.float64)
+    U_o, lam_o, res = ref.lowrank_prepare(y, X, 60, n_threads=8)
+    op = cs.createKinshipOperator(g)
+    eng = cs.LmmEngine()
+    diag = eng.prepareLowRankMatrixFree(y, X, op, rank=60, precision="mixed")
+    assert diag["effective_rank"] == res.rank
+    for key in ("sigma2_g", "sigma2_e"):
+        assert abs(diag[key] - getattr(res, key)) <= 1e-5 * abs(getattr(res, key)), key
+    keep = np.arange(n)
+    out = eng.scan(g, keep, precision="mixed")
+    exp = ref.scan_lowrank(keep, U_o, lam_o, res.residual_eigenvalue, res.sigma2_g,
+                           res.sigma2_e, y, X)
+    t = exp["tested"]
+    assert np.array_equal(out["tested"], t)
+    assert np.array_equal(out["freq"][t], exp["freq"][t])
+    for key in ("beta", "se"):
+        err = np.abs(out[key][t] - exp[key][t]).max() / np.abs(exp[key][t]).max()
+        assert err < 1e-5, (key, err)
+    assert np.abs(out["log10p"][t] - exp["log10p"][t]).max() < 1e-3
