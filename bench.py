@@ -40,7 +40,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=50000)
     ap.add_argument("--m", type=int, default=100000)
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -140,10 +140,11 @@ def fp64_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def cpu_reference_sample(d, n_threads, m_sample=600, k=RANK + OVERSAMPLE):
-    """Times the reference's CPU algorithm (oracle restatement, OpenMP) on a bounded sample:
-    one apply_block with 266 right-hand sides over m_sample SNPs, and the low-rank scan of
-    m_sample SNPs; extrapolates to the full job: 4 applies + scan over all M SNPs."""
+def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
+    """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
+    (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
+    sides and scanLowRank's block GEMMs, both over m_sample of the M SNPs; extrapolated to
+    the whole job (4 applies + the scan over all M SNPs).  QR, eigh and REML are excluded."""
     import oracle
 
     n, m = d["n"], d["m"]
@@ -153,19 +154,19 @@ def cpu_reference_sample(d, n_threads, m_sample=600, k=RANK + OVERSAMPLE):
     rng = np.random.default_rng(0)
     Om = rng.standard_normal((n, k))
     t0 = time.perf_counter()
-    B.apply_block(Om, n_threads=n_threads)
+    oracle.apply_block_blas(rows, n, B.mean, B.inv_std, Om)
     t_apply = time.perf_counter() - t0
     U = np.linalg.qr(rng.standard_normal((n, RANK)))[0]
     lam = np.sort(rng.uniform(1, 5, RANK))[::-1].copy()
     X = d["X"].astype(np.float32).astype(np.float64)
     t0 = time.perf_counter()
-    B.scan_lowrank(np.arange(n), U, lam, 0.9, 0.4, 0.6, d["y"], X)
+    oracle.scan_lowrank_blas(rows, n, U, lam, 0.9, 0.4, 0.6, d["y"], X)
     t_scan = time.perf_counter() - t0
     scale = m / m_sample
     est = (4 * t_apply + t_scan) * scale
-    sample = (f"apply_block (266 RHS) + scanLowRank over {m_sample} of {m} SNPs at N={n}, "
-              f"extrapolated x{scale:.0f} to 4 applies + scan (QR/eigh/REML excluded): "
-              f"apply {t_apply:.2f}s, scan {t_scan:.2f}s")
+    sample = (f"numpy-BLAS restatement of apply_block (266 RHS) + scanLowRank block GEMMs "
+              f"over {m_sample} of {m} SNPs at N={n}, x{scale:.1f} to 4 applies + scan "
+              f"(QR/eigh/REML excluded): apply {t_apply:.2f}s, scan {t_scan:.2f}s")
     return est, sample, t_apply + t_scan
 
 
@@ -179,7 +180,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     for _ in range(args.warmup):
-        cpu_reference_sample(d, threads, m_sample=64)
+        cpu_reference_sample(d, threads, m_sample=256)
     vals = []
     sample = ""
     for _ in range(args.steps):
@@ -328,6 +329,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,
+            "host_stages": prof.get("host", []),
             "sigma2_g": eng.getSigma2g(), "sigma2_e": eng.getSigma2e(),
             "tested": int(res["tested"].sum()),
         }

@@ -186,6 +186,14 @@ def profile_summary() -> dict:
     return json.loads(buf.value.decode())
 
 
+def normal_matrix(seed: int, n: int, cols: int) -> np.ndarray:
+    """The reference's Gaussian test matrix (mt19937_64 + std::normal_distribution), drawn on
+    the device: n x cols, filled column by column."""
+    out = np.zeros((n, cols), order="F")
+    _check(_abi.lib().cs_normal_matrix(seed, n, cols, _ptr(out)))
+    return out
+
+
 def launch_count() -> int:
     """Process-wide number of kernel launches the library has made."""
     n = C.c_int64()

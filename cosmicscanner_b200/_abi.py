@@ -45,6 +45,7 @@ _SIGNATURES = {
     "cs_lmm_lowrank_basis": ([_P, _P, _I64, _P], _I),
     "cs_lmm_scan": ([_P, _P, _P, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_lmm_destroy": ([_P], None),
+    "cs_normal_matrix": ([C.c_uint64, _I64, _I64, _P], _I),
     "cs_profile_enable": ([_I], _I),
     "cs_profile_summary": ([C.c_char_p, C.c_size_t, _P], _I),
     "cs_launch_count": ([_P], _I),

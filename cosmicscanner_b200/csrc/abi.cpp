@@ -200,6 +200,20 @@ int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t
 
 void cs_lmm_destroy(cs_lmm* lmm) { cs::lmm_destroy(lmm); }
 
+int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out) {
+    return guarded([&] {
+        require(n >= 0 && cols >= 0 && (out != nullptr || n * cols == 0), "bad arguments");
+        if (n * cols == 0) return;
+        cs::OmegaWorkspace ws;
+        cs::DeviceBuffer<double> d, t;
+        d.resize(n * cols);
+        t.resize(n * cols);
+        cs::generate_omega_device(seed, n, cols, d.get(), cols, ws, 0);
+        cs::rowmajor_to_colmajor(d.get(), cols, n, cols, t.get(), n, 0);
+        CS_CUDA(cudaMemcpy(out, t.get(), 8 * n * cols, cudaMemcpyDeviceToHost));
+    });
+}
+
 int cs_profile_enable(int on) {
     return guarded([&] { cs::prof::set_enabled(on != 0); });
 }

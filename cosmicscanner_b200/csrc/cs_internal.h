@@ -76,6 +76,7 @@ struct cs_genotypes {
     std::vector<int32_t> count;
     std::vector<double> sum;
     int device = 0;
+    uint64_t uid = 0;  // distinct for every matrix created in the process (cache keys)
 };
 
 // A packed matrix of selected rows x selected samples with everything the kernels need.
@@ -124,6 +125,17 @@ void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_
                             int64_t ldy, int precision, cudaStream_t s);
 void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                          int64_t ldy, cudaStream_t s);
+
+// The reference's Gaussian test matrix (std::normal_distribution over std::mt19937_64) on the
+// device, written row-major n x ld (omega.cu).
+struct OmegaWorkspace {
+    DeviceBuffer<uint64_t> state, raw;
+    DeviceBuffer<int32_t> counts;
+    DeviceBuffer<int64_t> offsets;
+    DeviceBuffer<double> pairs;
+};
+void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out, int64_t ld,
+                           OmegaWorkspace& ws, cudaStream_t s);
 
 // Tensor-core projection for the scan: T[t][c] = sum_i (g_ti - m_t)[observed] B[i][c] over
 // every row of a packed view, m_t = row_mean[t] (kinship_mixed.cu).
@@ -175,6 +187,18 @@ class Scope {
     cudaStream_t s_;
     double flops_, bytes_;
     cudaEvent_t a_ = nullptr;
+};
+// Wall-clock time of a host-side stage, reported with the kernels when profiling is on.
+class HostScope {
+   public:
+    explicit HostScope(const char* name);
+    ~HostScope();
+    HostScope(const HostScope&) = delete;
+    HostScope& operator=(const HostScope&) = delete;
+
+   private:
+    const char* name_;
+    double t0_ = -1.0;
 };
 bool enabled();
 void set_enabled(bool on);

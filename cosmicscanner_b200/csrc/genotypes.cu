@@ -5,6 +5,7 @@
 //   libCosmicCore/src/plink_reader.cpp:187-239 computeStats (mean, 1/sqrt(2p(1-p)))
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -201,6 +202,8 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
         fail(CS_ERR_FORMAT, "Invalid .bed file: " + std::to_string(n_bytes) +
                                 " bytes < expected " + std::to_string(3 + n_snps * bps));
     auto* g = new cs_genotypes();
+    static std::atomic<uint64_t> next_uid{1};
+    g->uid = next_uid.fetch_add(1);
     try {
         CS_CUDA(cudaGetDevice(&g->device));
         g->n_samples = n_samples;

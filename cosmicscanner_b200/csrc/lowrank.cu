@@ -30,8 +30,23 @@ struct cs_lmm {
     cs::DeviceBuffer<double> d_U;  // n x rank, row-major
     cublasHandle_t blas = nullptr;
     cs::DeviceBuffer<double> d_a, d_b, d_c, d_d;
+    // persistent work buffers (grown on demand, never freed between calls)
+    cs::DeviceBuffer<double> omega, sample, q, scratch, gram, small;
+    cs::OmegaWorkspace omega_ws;
+    // scan: analysed-sample view of the genotypes and its tensor-core context, cached
+    // for repeated scans of the same (genotypes, keep) pair
+    uint64_t scan_g_uid = 0;
+    std::vector<int32_t> scan_keep;
+    cs::DeviceBuffer<uint8_t> scan_own;
+    cs_packed_view scan_view;
+    std::vector<int32_t> scan_counts;
+    cs::MixedScan* scan_mixed = nullptr;
+    cs::DeviceBuffer<int32_t> d_counts, d_tested;
+    cs::DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
+    cs::DeviceBuffer<uint8_t> d_pass;
     ~cs_lmm() {
         if (blas) cublasDestroy(blas);
+        cs::mixed_scan_destroy(scan_mixed);
     }
 };
 
@@ -43,58 +58,6 @@ void check_blas(cublasStatus_t st, const char* what) {
     if (st != CUBLAS_STATUS_SUCCESS) fail(CS_ERR_CUDA, std::string(what) + ": cuBLAS status " + std::to_string((int)st));
 }
 #define CS_BLAS(call) check_blas((call), #call)
-
-// ---------------------------------------------------------------- Omega
-// The reference draws Omega column by column from std::normal_distribution<double> over
-// mt19937_64(seed) (lmm_engine.cpp:917-922).  libstdc++ implements the Marsaglia polar
-// method: uniforms u = double(raw)/2^64, x = 2u - 1, y = 2u' - 1, accept r2 = x^2 + y^2 in
-// (0, 1], return y*mult then x*mult with mult = sqrt(-2 log(r2) / r2).  The host runs the
-// sequential engine and the acceptance test; the device evaluates log/sqrt per pair.
-__global__ void k_polar_pairs(const double* __restrict__ xy, int64_t count, int64_t n,
-                              int64_t ld, double* __restrict__ out) {
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t pair = idx >> 1;
-        const double x = xy[2 * pair], y = xy[2 * pair + 1];
-        const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
-        const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
-        const double v = (idx & 1) ? __dmul_rn(x, mult) : __dmul_rn(y, mult);
-        // draw idx fills column idx / n, row idx % n; written row-major n x ld
-        const int64_t col = idx / n, row = idx - col * n;
-        out[row * ld + col] = v;
-    }
-}
-
-inline double canonical(uint64_t r) {
-    double u = (double)r / 18446744073709551616.0;
-    if (u >= 1.0) u = std::nextafter(1.0, 0.0);
-    return u;
-}
-
-void generate_omega(uint64_t seed, int64_t n, int64_t cols, double* d_out, int64_t ld,
-                    DeviceBuffer<double>& scratch, cudaStream_t s) {
-    const int64_t count = n * cols;
-    const int64_t pairs = (count + 1) / 2;
-    std::vector<double> xy((size_t)2 * pairs);
-    std::mt19937_64 gen(seed);
-    for (int64_t q = 0; q < pairs; ++q) {
-        double x, y, r2;
-        do {
-            x = 2.0 * canonical(gen()) - 1.0;
-            y = 2.0 * canonical(gen()) - 1.0;
-            r2 = x * x + y * y;
-        } while (r2 > 1.0 || r2 == 0.0);
-        xy[2 * q] = x;
-        xy[2 * q + 1] = y;
-    }
-    scratch.resize(2 * pairs);
-    CS_CUDA(cudaMemcpyAsync(scratch.get(), xy.data(), 16 * pairs, cudaMemcpyHostToDevice, s));
-    const int blocks = (int)std::min<int64_t>((count + 255) / 256, 32LL * num_sms());
-    prof::Scope ps("polar_pairs", s, 0.0, 16.0 * count);
-    k_polar_pairs<<<std::max(blocks, 1), 256, 0, s>>>(scratch.get(), count, n, ld, d_out);
-    CS_LAUNCH("polar_pairs");
-    CS_CUDA(cudaStreamSynchronize(s));  // xy leaves scope
-}
 
 // ---------------------------------------------------------------- QR
 // Thin QR of Y (n x k row-major) by Cholesky-QR repeated until the Gram matrix is the
@@ -157,6 +120,7 @@ struct RemlData {
     double r0;
     const double* lambda;
     std::vector<double> XtX, Xty, UtX, Uty;  // UtX rank x p col-major
+    double yty = 0.0;
     const double* X;
     const double* y;
 };
@@ -182,14 +146,13 @@ double reml_objective(const RemlData& d, double log_eta, double* quadratic) {
     if (!la::ldlt(info, (int)p, L, D)) return std::numeric_limits<double>::infinity();
     std::vector<double> beta = xry;
     la::ldlt_solve(L, D, (int)p, beta.data());
-    // residual r = y - X beta (explicit N-vector, like the reference)
-    double rr = 0.0;
-    for (int64_t i = 0; i < n; ++i) {
-        double fit = 0.0;
-        for (int64_t a = 0; a < p; ++a) fit += d.X[i + a * n] * beta[a];
-        const double e = d.y[i] - fit;
-        rr += e * e;
+    // residual r = y - X beta: r^T r = y^T y - 2 beta^T X^T y + beta^T X^T X beta
+    double rr = d.yty;
+    for (int64_t a = 0; a < p; ++a) {
+        rr -= 2.0 * beta[a] * d.Xty[a];
+        for (int64_t b = 0; b < p; ++b) rr += beta[a] * d.XtX[a + b * p] * beta[b];
     }
+    (void)n;
     double qf = base * rr;
     for (int64_t j = 0; j < r; ++j) {
         double ur = d.Uty[j];
@@ -389,18 +352,27 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     const int64_t sk = std::min<int64_t>(n, rank + std::max(0, oversample));
     cudaStream_t s = 0;
     CS_BLAS(cublasSetStream(l->blas, s));
-    DeviceBuffer<double> omega, sample, q, scratch, gram, small;
+    DeviceBuffer<double>&omega = l->omega, &sample = l->sample, &q = l->q, &scratch = l->scratch,
+                         &gram = l->gram, &small = l->small;
     omega.resize(n * sk);
     sample.resize(n * sk);
     q.resize(n * sk);
-    generate_omega((uint64_t)seed, n, sk, omega.get(), sk, scratch, s);
-    kinship_apply_rowmajor(op, omega.get(), sk, sk, sample.get(), sk, precision, s);
-    for (int it = 0; it < 2; ++it) {
+    {
+        prof::HostScope hs("lowrank_omega");
+        generate_omega_device((uint64_t)seed, n, sk, omega.get(), sk, l->omega_ws, s);
+    }
+    {
+        prof::HostScope hs("lowrank_subspace_iteration");
+        kinship_apply_rowmajor(op, omega.get(), sk, sk, sample.get(), sk, precision, s);
+        for (int it = 0; it < 2; ++it) {
+            cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
+            kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
+        }
         cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
         kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
+        CS_CUDA(cudaStreamSynchronize(s));
     }
-    cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
-    kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
+    prof::HostScope hs_eig("lowrank_eigh_rank_reml");
     // B = Q^T K Q (sk x sk)
     small.resize(sk * sk);
     const double one = 1.0, zero = 0.0;
@@ -435,7 +407,6 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
         for (int64_t a = 0; a < sk; ++a) wtop[a + j * sk] = evecs[a + (sk - 1 - j) * sk];
     gram.resize(sk * selected);
     CS_CUDA(cudaMemcpyAsync(gram.get(), wtop.data(), 8 * sk * selected, cudaMemcpyHostToDevice, s));
-    l->d_U.release();
     l->d_U.resize(n * selected);
     CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_T, CUBLAS_OP_N, selected, (int)n, (int)sk, &one,
                         gram.get(), (int)sk, q.get(), (int)sk, &zero, l->d_U.get(), selected));
@@ -477,6 +448,7 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
         for (int64_t i = 0; i < n; ++i) acc += X[i + a * n] * y[i];
         d.Xty[a] = acc;
     }
+    for (int64_t i = 0; i < n; ++i) d.yty += y[i] * y[i];
     d.UtX.assign(UtZ.begin(), UtZ.begin() + selected * p);
     d.Uty.assign(UtZ.begin() + selected * p, UtZ.begin() + selected * (p + 1));
     double ble, bo, quad;
@@ -597,30 +569,41 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         CS_BLAS(cublasDgemv(l->blas, CUBLAS_OP_T, (int)r, (int)n, &one, l->d_U.get(), (int)r,
                             l->d_d.get(), 1, &one, Bm + r + p, (int)bw));
     }
-    // ---- packed view of the analysed samples over every SNP
-    bool identity = n_keep == g->n_samples;
-    for (int64_t i = 0; identity && i < n_keep; ++i) identity = keep[i] == i;
-    DeviceBuffer<uint8_t> own;
-    cs_packed_view v{g->packed.get(), M, g->n_samples, g->stride};
-    if (!identity) {
-        const int64_t stride = round_up((n + 3) / 4, kRowAlign);
-        own.resize(std::max<int64_t>(1, M * stride));
-        DeviceBuffer<int32_t> d_keep;
-        d_keep.resize(n);
-        CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, 4 * n, cudaMemcpyHostToDevice, s));
-        repack(g->packed.get(), g->stride, nullptr, M, d_keep.get(), n, own.get(), stride, s);
-        CS_CUDA(cudaStreamSynchronize(s));
-        v = cs_packed_view{own.get(), M, n, stride};
+    // ---- packed view of the analysed samples over every SNP (cached per genotypes + keep)
+    prof::HostScope hs_scan("scan_host_setup");
+    const bool cached = l->scan_g_uid == g->uid && (int64_t)l->scan_keep.size() == n_keep &&
+                        std::memcmp(l->scan_keep.data(), keep, 4 * n_keep) == 0;
+    if (!cached) {
+        mixed_scan_destroy(l->scan_mixed);
+        l->scan_mixed = nullptr;
+        bool identity = n_keep == g->n_samples;
+        for (int64_t i = 0; identity && i < n_keep; ++i) identity = keep[i] == i;
+        l->scan_view = cs_packed_view{g->packed.get(), M, g->n_samples, g->stride};
+        if (!identity) {
+            const int64_t stride = round_up((n + 3) / 4, kRowAlign);
+            l->scan_own.resize(std::max<int64_t>(1, M * stride));
+            DeviceBuffer<int32_t> d_keep;
+            d_keep.resize(n);
+            CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, 4 * n, cudaMemcpyHostToDevice, s));
+            repack(g->packed.get(), g->stride, nullptr, M, d_keep.get(), n, l->scan_own.get(),
+                   stride, s);
+            CS_CUDA(cudaStreamSynchronize(s));
+            l->scan_view = cs_packed_view{l->scan_own.get(), M, n, stride};
+        }
+        l->scan_counts.assign(4 * M, 0);
+        l->d_counts.resize(std::max<int64_t>(1, 4 * M));
+        if (M) {
+            row_code_counts(l->scan_view, l->d_counts.get(), s);
+            CS_CUDA(cudaMemcpyAsync(l->scan_counts.data(), l->d_counts.get(), 16 * M,
+                                    cudaMemcpyDeviceToHost, s));
+            CS_CUDA(cudaStreamSynchronize(s));
+        }
+        l->scan_g_uid = g->uid;
+        l->scan_keep.assign(keep, keep + n_keep);
     }
+    const cs_packed_view& v = l->scan_view;
+    const std::vector<int32_t>& counts = l->scan_counts;
     // ---- per-SNP encoding over the analysed samples (genotype_encoding.h:33-81)
-    DeviceBuffer<int32_t> d_counts;
-    d_counts.resize(std::max<int64_t>(1, 4 * M));
-    std::vector<int32_t> counts(4 * M);
-    if (M) {
-        row_code_counts(v, d_counts.get(), s);
-        CS_CUDA(cudaMemcpyAsync(counts.data(), d_counts.get(), 16 * M, cudaMemcpyDeviceToHost, s));
-        CS_CUDA(cudaStreamSynchronize(s));
-    }
     std::vector<double> lut(4 * M, 0.0), gn2(M, 0.0), fr(M, 0.0), row_mean(M, 0.0);
     std::vector<uint8_t> pass(M, 0);
     for (int64_t j = 0; j < M; ++j) {
@@ -632,8 +615,8 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         const double af = dosage_sum / (2.0 * (double)obs);
         fr[j] = af;
         pass[j] = obs >= 3 && std::min(af, 1.0 - af) >= min_maf;
-        if (!pass[j]) continue;
-        const double mean = dosage_sum / (double)obs;  // encoded mean (additive model)
+        // the encoded mean (additive model); rows that fail the filter are never reported
+        const double mean = dosage_sum / (double)obs;
         row_mean[j] = mean;
         lut[4 * j + 0] = 2.0 - mean;
         lut[4 * j + 1] = 0.0;  // missing -> mean -> centred 0
@@ -642,57 +625,53 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
         const int64_t sq = 4 * c00 + c10;  // sum of squared dosages
         gn2[j] = (double)(obs * sq - isum * isum) / (double)obs;
     }
-    DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
-    DeviceBuffer<uint8_t> d_pass;
-    DeviceBuffer<int32_t> d_tested;
-    d_lut.resize(std::max<int64_t>(1, 4 * M));
-    d_T.resize(std::max<int64_t>(1, M * bw));
-    d_gn2.resize(std::max<int64_t>(1, M));
-    d_pass.resize(std::max<int64_t>(1, M));
-    d_cv.resize(std::max<int64_t>(1, r));
-    d_utx.resize(std::max<int64_t>(1, r * p));
-    d_inv.resize(std::max<int64_t>(1, p * p));
-    for (auto* b : {&d_beta, &d_se, &d_p, &d_l10}) b->resize(std::max<int64_t>(1, M));
-    d_tested.resize(std::max<int64_t>(1, M));
+    l->d_lut.resize(std::max<int64_t>(1, 4 * M));
+    l->d_T.resize(std::max<int64_t>(1, M * bw));
+    l->d_gn2.resize(std::max<int64_t>(1, M));
+    l->d_pass.resize(std::max<int64_t>(1, M));
+    l->d_cv.resize(std::max<int64_t>(1, r));
+    l->d_utx.resize(std::max<int64_t>(1, r * p));
+    l->d_inv.resize(std::max<int64_t>(1, p * p));
+    for (auto* b : {&l->d_beta, &l->d_se, &l->d_p, &l->d_l10}) b->resize(std::max<int64_t>(1, M));
+    l->d_tested.resize(std::max<int64_t>(1, M));
     if (M == 0) return;
-    CS_CUDA(cudaMemcpyAsync(d_lut.get(), lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
-    CS_CUDA(cudaMemcpyAsync(d_gn2.get(), gn2.data(), 8 * M, cudaMemcpyHostToDevice, s));
-    CS_CUDA(cudaMemcpyAsync(d_pass.get(), pass.data(), M, cudaMemcpyHostToDevice, s));
-    CS_CUDA(cudaMemcpyAsync(d_cv.get(), c.data(), 8 * r, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_gn2.get(), gn2.data(), 8 * M, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), pass.data(), M, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_cv.get(), c.data(), 8 * r, cudaMemcpyHostToDevice, s));
     if (p) {
-        CS_CUDA(cudaMemcpyAsync(d_utx.get(), UtX, 8 * r * p, cudaMemcpyHostToDevice, s));
-        CS_CUDA(cudaMemcpyAsync(d_inv.get(), info_inv.data(), 8 * p * p, cudaMemcpyHostToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(l->d_utx.get(), UtX, 8 * r * p, cudaMemcpyHostToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(l->d_inv.get(), info_inv.data(), 8 * p * p, cudaMemcpyHostToDevice, s));
     }
     // ---- T = G_c^T [U | X | py]: the per-SNP projections (the scan's GEMM)
     if (precision == CS_PRECISION_MIXED) {
-        MixedScan* ms = mixed_scan_create(v, row_mean.data(), counts.data());
-        try {
-            mixed_scan_project(ms, Bm, bw, bw, d_T.get(), bw, s);
-        } catch (...) {
-            mixed_scan_destroy(ms);
-            throw;
+        if (!cached || !l->scan_mixed) {
+            mixed_scan_destroy(l->scan_mixed);
+            l->scan_mixed = nullptr;
+            l->scan_mixed = mixed_scan_create(v, row_mean.data(), counts.data());
         }
-        mixed_scan_destroy(ms);
+        mixed_scan_project(l->scan_mixed, Bm, bw, bw, l->d_T.get(), bw, s);
     } else {
         Workspace ws;
-        decode_gemm_rows_fp64(v, d_lut.get(), Bm, bw, bw, d_T.get(), bw, ws, s);
+        decode_gemm_rows_fp64(v, l->d_lut.get(), Bm, bw, bw, l->d_T.get(), bw, ws, s);
     }
     ScanParams P;
     P.n_snps = M; P.rank = r; P.p = p; P.ldt = bw; P.base = base;
-    P.T = d_T.get(); P.c = d_cv.get(); P.UtX = d_utx.get(); P.info_inv = d_inv.get();
-    P.gnorm2 = d_gn2.get(); P.pass = d_pass.get();
-    P.beta = d_beta.get(); P.se = d_se.get(); P.pval = d_p.get(); P.log10p = d_l10.get();
-    P.tested = d_tested.get();
+    P.T = l->d_T.get(); P.c = l->d_cv.get(); P.UtX = l->d_utx.get(); P.info_inv = l->d_inv.get();
+    P.gnorm2 = l->d_gn2.get(); P.pass = l->d_pass.get();
+    P.beta = l->d_beta.get(); P.se = l->d_se.get(); P.pval = l->d_p.get();
+    P.log10p = l->d_l10.get();
+    P.tested = l->d_tested.get();
     const int blocks = (int)std::min<int64_t>((M * 32 + 255) / 256, 64LL * num_sms());
     prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
     k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
     CS_LAUNCH("scan_epilogue");
     std::vector<int32_t> t(M);
-    CS_CUDA(cudaMemcpyAsync(t.data(), d_tested.get(), 4 * M, cudaMemcpyDeviceToHost, s));
-    if (beta) CS_CUDA(cudaMemcpyAsync(beta, d_beta.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (se) CS_CUDA(cudaMemcpyAsync(se, d_se.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (pvalue) CS_CUDA(cudaMemcpyAsync(pvalue, d_p.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (log10p) CS_CUDA(cudaMemcpyAsync(log10p, d_l10.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaMemcpyAsync(t.data(), l->d_tested.get(), 4 * M, cudaMemcpyDeviceToHost, s));
+    if (beta) CS_CUDA(cudaMemcpyAsync(beta, l->d_beta.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (se) CS_CUDA(cudaMemcpyAsync(se, l->d_se.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (pvalue) CS_CUDA(cudaMemcpyAsync(pvalue, l->d_p.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (log10p) CS_CUDA(cudaMemcpyAsync(log10p, l->d_l10.get(), 8 * M, cudaMemcpyDeviceToHost, s));
     CS_CUDA(cudaStreamSynchronize(s));
     for (int64_t j = 0; j < M; ++j) {
         if (tested) tested[j] = t[j];

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -29,6 +30,11 @@ std::atomic<bool> g_enabled{false};
 std::mutex g_mu;
 std::vector<Record> g_records;
 std::vector<cudaEvent_t> g_pool;
+std::map<std::string, std::pair<int64_t, double>> g_host;  // name -> (calls, seconds)
+
+double now_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 cudaEvent_t take_event() {
     if (!g_pool.empty()) {
@@ -61,6 +67,19 @@ Scope::~Scope() {
     g_records.push_back(Record{name_, a_, b, flops_, bytes_});
 }
 
+HostScope::HostScope(const char* name) : name_(name) {
+    if (enabled()) t0_ = now_seconds();
+}
+
+HostScope::~HostScope() {
+    if (t0_ < 0.0) return;
+    const double dt = now_seconds() - t0_;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto& e = g_host[name_];
+    e.first += 1;
+    e.second += dt;
+}
+
 int64_t launches() { return g_launches.load(); }
 
 void set_enabled(bool on) {
@@ -70,6 +89,7 @@ void set_enabled(bool on) {
         g_pool.push_back(r.b);
     }
     g_records.clear();
+    g_host.clear();
     g_enabled = on;
 }
 
@@ -100,6 +120,15 @@ std::string summary_json() {
                       "\"flops\": %.6e, \"bytes\": %.6e}",
                       first ? "" : ", ", kv.first.c_str(), (long long)kv.second.n, kv.second.ms,
                       kv.second.max_ms, kv.second.flops, kv.second.bytes);
+        out += buf;
+        first = false;
+    }
+    out += "], \"host\": [";
+    first = true;
+    for (auto& kv : g_host) {
+        std::snprintf(buf, sizeof buf, "%s{\"name\": \"%s\", \"calls\": %lld, \"ms\": %.6f}",
+                      first ? "" : ", ", kv.first.c_str(), (long long)kv.second.first,
+                      kv.second.second * 1e3);
         out += buf;
         first = false;
     }

@@ -132,6 +132,12 @@ int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t
                 double* log10p, double* freq, int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
 
+/* The test matrix of src/lmm_engine.cpp:917-922 (also libCosmicCore/src/rng.h:27-33):
+ * n x cols standard normals drawn column by column from std::normal_distribution<double>
+ * over std::mt19937_64(seed), generated on the device (engine, polar acceptance, transform)
+ * and copied to `out` (host, column-major, ld = n). */
+int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out);
+
 /* ---------------------------------------------------------------- instrumentation
  * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and
  * PlinkKinshipOperator::BlockProfile (src/kinship_operator.h:55-63): a process-wide count

@@ -231,3 +231,54 @@ def prepare_marker(raw, min_maf=0.01):
     obs = C.c_int32()
     ok = lib().orc_prepare_marker(_ptr(raw), len(raw), min_maf, _ptr(vals), C.byref(f), C.byref(obs))
     return bool(ok), vals, f.value, obs.value
+
+
+# ---------------------------------------------------------------- BLAS restatements
+# Timed CPU baseline: the reference's block algorithms with its GEMMs done by numpy's
+# multithreaded BLAS, standing in for Eigen's blocked GEMM (src/kinship_operator.cpp:225-302,
+# src/lmm_engine.cpp:1269-1361).  Decode tables follow src/kinship_operator.cpp:276-283.
+
+def _decode_block(rows, n, values):
+    """rows: (b, stride) packed bytes; values: (b, 4) per-row code values -> (n, b) FP64."""
+    codes = np.stack([(rows >> (2 * q)) & 3 for q in range(4)], axis=2).reshape(rows.shape[0], -1)[:, :n]
+    return np.take_along_axis(values, codes.astype(np.int64), axis=1).T.copy()
+
+
+def apply_block_blas(rows, n, mean, inv_std, X, block=512):
+    """K X over all rows of `rows` (m x stride packed, magic skipped), FP64, BLAS GEMMs."""
+    m = rows.shape[0]
+    out = np.zeros((n, X.shape[1]))
+    for first in range(0, m, block):
+        r = rows[first:first + block]
+        mu, s = mean[first:first + block], inv_std[first:first + block]
+        vals = np.stack([(2.0 - mu) * s, np.zeros_like(mu), (1.0 - mu) * s, -mu * s], axis=1)
+        z = _decode_block(r, n, vals)
+        out += z @ (z.T @ X)
+    return out / m
+
+
+def scan_lowrank_blas(rows, n, U, lam, r0, sg2, se2, y, X, min_maf=0.01, block=512):
+    """scanLowRank (identity keep) with BLAS GEMMs per 512-SNP block; returns -log10 P."""
+    base = 1.0 / max(1e-12, sg2 * r0 + se2)
+    corr = 1.0 / (sg2 * lam + se2) - base
+    vinv = lambda R: base * R + U @ (corr[:, None] * (U.T @ R))
+    vx = vinv(X)
+    info_inv = np.linalg.inv(X.T @ vx)
+    beta = info_inv @ (X.T @ vinv(y[:, None])).ravel()
+    py = vinv((y - X @ beta)[:, None]).ravel()
+    out = np.full(rows.shape[0], np.nan)
+    for first in range(0, rows.shape[0], block):
+        r = rows[first:first + block]
+        raw = _decode_block(r, n, np.tile(np.array([2.0, np.nan, 1.0, 0.0]), (r.shape[0], 1)))
+        obs = ~np.isnan(raw)
+        cnt = obs.sum(axis=0)
+        mean = np.nansum(raw, axis=0) / np.maximum(cnt, 1)
+        G = np.where(obs, raw - mean, 0.0)
+        vg = vinv(G)
+        score = G.T @ py
+        xvg = X.T @ vg
+        var = (G * vg).sum(axis=0) - (xvg * (info_inv @ xvg)).sum(axis=0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            out[first:first + block] = -np.log10(np.maximum(
+                np.exp(-0.5 * score ** 2 / var), 1e-300))
+    return out
