@@ -44,30 +44,39 @@ using namespace sm100;
 
 constexpr int kTile = 128;        // MMA M, and SNP rows / samples per decoded tile
 constexpr int kKBlock = 128;      // K elements (int8) per stage: one 128-byte swizzle row
-constexpr int kMaxKc = 80;        // column-tile width cap (6 * 80 TMEM columns)
+constexpr int kMaxKc = 80;        // column-tile width cap (TMEM: rows pass 6 x 80 columns)
 constexpr int kWarps = 14;
 constexpr int kThreads = kWarps * 32;
 constexpr int kDecodeWarp0 = 2, kDecodeWarps = 8;
 constexpr int kEpiWarp0 = 10;
 constexpr uint32_t kTmemCols = 512;
 constexpr double kBase = 254.0;
+constexpr int kDecStages = 2;
 
 constexpr int kATileBytes = kTile * kKBlock;     // 16 KB
 constexpr int kPackedBytes = kTile * 32;         // 128 rows x 32 B
 
+// Shared memory: a ring of decoded tiles {dosages, missing indicators} and a deeper ring of
+// TMA stages {packed tile, B pieces}, so that TMA latency is covered independently of the
+// decode buffers.  Rows pass: 3 B pieces, 4 TMA stages, accumulator = 6 kc TMEM columns
+// (main and missing sums kept apart).  Samples pass: 6 B pieces (W and mu o W with one
+// scale), 2 TMA stages, accumulator = 3 kc columns, double-buffered.
 template <bool ROWS>
 struct Layout {
-    static constexpr int kPieces = ROWS ? 3 : 6;  // B rows per column: pieces (x2 for mu o W)
-    static constexpr int kStages = ROWS ? 3 : 2;
+    static constexpr int kPieces = ROWS ? 3 : 6;
+    static constexpr int kTmaStages = ROWS ? 4 : 2;
+    static constexpr int kAccCols = ROWS ? 6 * kMaxKc : 3 * kMaxKc;
+    static constexpr int kAccBufs = ROWS ? 1 : 2;
+    static constexpr uint32_t kAccStride = 256;
     static constexpr int kBBytes = kPieces * kMaxKc * 128;
-    static constexpr int kStageBytes = 2 * kATileBytes + kBBytes + kPackedBytes;
-    static constexpr int kSmem = kStages * kStageBytes + 1024 + 256;
-    static __host__ __device__ constexpr int a(int s) { return s * kStageBytes; }
-    static __host__ __device__ constexpr int am(int s) { return s * kStageBytes + kATileBytes; }
-    static __host__ __device__ constexpr int b(int s) { return s * kStageBytes + 2 * kATileBytes; }
-    static __host__ __device__ constexpr int p(int s) {
-        return s * kStageBytes + 2 * kATileBytes + kBBytes;
-    }
+    static constexpr int kTmaBytes = kBBytes + kPackedBytes;
+    static constexpr int kDecBytes = 2 * kATileBytes;
+    static constexpr int kSmem = kDecStages * kDecBytes + kTmaStages * kTmaBytes + 1024 + 256;
+    static __host__ __device__ constexpr int a(int d) { return d * kDecBytes; }
+    static __host__ __device__ constexpr int am(int d) { return d * kDecBytes + kATileBytes; }
+    static __host__ __device__ constexpr int b(int s) { return kDecStages * kDecBytes + s * kTmaBytes; }
+    static __host__ __device__ constexpr int p(int s) { return b(s) + kBBytes; }
+    static __host__ __device__ constexpr int bars() { return kDecStages * kDecBytes + kTmaStages * kTmaBytes; }
 };
 
 struct PassArgs {
@@ -75,8 +84,7 @@ struct PassArgs {
     int kb_total, kb_per_split;  // K-blocks of the contraction, per slice
     int kc, kp;                  // column tile width, padded column count
     const double* mu;            // rows pass: mu_t per SNP row (epilogue)
-    const double* inv_f2;        // samples pass: 1 / scale of W per column
-    const double* inv_f3;        // samples pass: 1 / scale of (mu o W) per column
+    const double* inv_f;         // samples pass: 1 / quantisation factor per column
     double* part;                // [n_splits][kp][ld] FP64 slice partials
     int64_t ld;                  // padded output rows
     int* status;
@@ -103,29 +111,35 @@ __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              PassArgs P) {
     using L = Layout<ROWS>;
-    constexpr int S = L::kStages;
+    constexpr int ST = L::kTmaStages, SD = kDecStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * L::kStageBytes);
-    uint64_t* full = bars;             // TMA landed (1 arrival + tx bytes)
-    uint64_t* dec = bars + S;          // decoded (one arrival per decode warp)
-    uint64_t* empty = bars + 2 * S;    // the stage's MMAs completed (commit)
-    uint64_t* acc_full = bars + 3 * S; // accumulator ready for the epilogue (commit)
-    uint64_t* acc_empty = acc_full + 1;  // accumulator drained (one arrival per epilogue warp)
-    uint64_t* drained = acc_empty + 1;   // MMA thread's own work complete at exit
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bars());
+    uint64_t* full_t = bars;              // TMA landed (1 arrival + tx bytes)
+    uint64_t* empty_t = full_t + ST;      // MMAs reading the stage done (commit)
+    uint64_t* full_d = empty_t + ST;      // decoded (one arrival per decode warp)
+    uint64_t* empty_d = full_d + SD;      // MMAs reading the decoded tile done (commit)
+    uint64_t* acc_full = empty_d + SD;    // accumulator ready for the epilogue (commit)
+    uint64_t* acc_empty = acc_full + NB;  // accumulator drained (one arrival per epilogue warp)
+    uint64_t* drained = acc_empty + NB;   // MMA thread's own work complete at exit
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kc = P.kc, kp = P.kp;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&dec[s], kDecodeWarps);
-            mbar_init(&empty[s], 1);
+        for (int s = 0; s < ST; ++s) {
+            mbar_init(&full_t[s], 1);
+            mbar_init(&empty_t[s], 1);
         }
-        mbar_init(acc_full, 1);
-        mbar_init(acc_empty, 4);
+        for (int d = 0; d < SD; ++d) {
+            mbar_init(&full_d[d], kDecodeWarps);
+            mbar_init(&empty_d[d], 1);
+        }
+        for (int b = 0; b < NB; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 4);
+        }
         mbar_init(drained, 1);
         fence_mbar_init();
     }
@@ -157,22 +171,22 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                    const int s = j % S;
-                    if (!(ok = mbar_wait(&empty[s], ((j / S) & 1) ^ 1, P.status, kTimeoutTma))) break;
-                    mbar_arrive_expect_tx(&full[s], bytes);
+                    const int s = j % ST;
+                    if (!(ok = mbar_wait(&empty_t[s], ((j / ST) & 1) ^ 1, P.status, kTimeoutTma))) break;
+                    mbar_arrive_expect_tx(&full_t[s], bytes);
                     // packed tile: 128 SNP rows x 32 bytes (128 samples)
                     if (ROWS)
-                        tma_load_2d(smem + L::p(s), &tm_a, kb * 32, tile * kTile, &full[s]);
+                        tma_load_2d(smem + L::p(s), &tm_a, kb * 32, tile * kTile, &full_t[s]);
                     else
-                        tma_load_2d(smem + L::p(s), &tm_a, tile * 32, kb * kKBlock, &full[s]);
+                        tma_load_2d(smem + L::p(s), &tm_a, tile * 32, kb * kKBlock, &full_t[s]);
                     for (int q = 0; q < L::kPieces; ++q)
                         tma_load_2d(smem + L::b(s) + q * kc * 128, &tm_b, kb * kKBlock,
-                                    q * kp + ct * kc, &full[s]);
+                                    q * kp + ct * kc, &full_t[s]);
                 }
             }
             // leave no copy in flight
-            for (uint32_t q = (j >= (uint32_t)S ? j - S : 0); q < j; ++q)
-                mbar_wait(&full[q % S], (q / S) & 1, P.status, kTimeoutTma, 1u << 20);
+            for (uint32_t q = (j >= (uint32_t)ST ? j - ST : 0); q < j; ++q)
+                mbar_wait(&full_t[q % ST], (q / ST) & 1, P.status, kTimeoutTma, 1u << 20);
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
@@ -187,42 +201,45 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
-                if (!(ok = mbar_wait(acc_empty, (ui & 1) ^ 1, P.status, kTimeoutMma))) break;
+                const int buf = ui % NB;
+                if (!(ok = mbar_wait(&acc_empty[buf], ((ui / NB) & 1) ^ 1, P.status, kTimeoutMma))) break;
                 tc_fence_after();
-                const uint32_t acc_main = tmem_base, acc_miss = tmem_base + 3 * kc;
+                const uint32_t acc_main = tmem_base + buf * L::kAccStride;
+                const uint32_t acc_miss = ROWS ? acc_main + 3 * kc : acc_main;
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                    const int s = j % S;
-                    const uint32_t ph = (j / S) & 1;
-                    if (!(ok = mbar_wait(&full[s], ph, P.status, kTimeoutMma))) break;
-                    if (!(ok = mbar_wait(&dec[s], ph, P.status, kTimeoutMma))) break;
+                    const int s = j % ST, d = j % SD;
+                    if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutMma))) break;
+                    if (!(ok = mbar_wait(&full_d[d], (j / SD) & 1, P.status, kTimeoutMma))) break;
                     tc_fence_after();
-                    const uint32_t a = smem_addr(smem + L::a(s));
-                    const uint32_t am = smem_addr(smem + L::am(s));
+                    const uint32_t a = smem_addr(smem + L::a(d));
+                    const uint32_t am = smem_addr(smem + L::am(d));
                     const uint32_t b = smem_addr(smem + L::b(s));
                     const uint32_t bm = ROWS ? b : b + 3 * kc * 128;
 #pragma unroll
                     for (int ks = 0; ks < kKBlock / 32; ++ks) {
-                        const uint32_t accum = (kb == kb0 && ks == 0) ? 0u : 1u;
+                        const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
                         const uint32_t aoff = ROWS ? ks * 32 : ks * 4096;  // 32 K elements
                         const uint64_t da = smem_desc_sw128(a + aoff, 16, 1024);
                         const uint64_t dm = smem_desc_sw128(am + aoff, 16, 1024);
                         const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
                         const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
-                        mma_i8(acc_main, da, db, idesc, accum);
-                        mma_i8(acc_miss, dm, dbm, idesc, accum);
+                        mma_i8(acc_main, da, db, idesc, first);
+                        // rows pass: separate missing-call sums; samples pass: same columns
+                        mma_i8(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
                     }
-                    mma_commit(&empty[s]);
+                    mma_commit(&empty_t[s]);
+                    mma_commit(&empty_d[d]);
                 }
-                if (ok) mma_commit(acc_full);
+                if (ok) mma_commit(&acc_full[buf]);
             }
             mma_commit(drained);
             mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
         }
     } else if (warp < kEpiWarp0) {
         // ------------------------------------------------------------ decoders
-        // thread d: SNP row d % 128, 64 samples (16 packed bytes) starting at 64 * (d / 128)
-        const int d = threadIdx.x - kDecodeWarp0 * 32;
-        const int r = d & 127, h = d >> 7;
+        // thread dt: SNP row dt % 128, 64 samples (16 packed bytes) starting at 64 * (dt / 128)
+        const int dt = threadIdx.x - kDecodeWarp0 * 32;
+        const int r = dt & 127, h = dt >> 7;
         const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
         uint32_t j = 0;
         bool ok = true;
@@ -230,11 +247,12 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                const int s = j % S;
-                if (!(ok = mbar_wait(&full[s], (j / S) & 1, P.status, kTimeoutDecode))) break;
+                const int s = j % ST, d = j % SD;
+                if (!(ok = mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode))) break;
+                if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
                 const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(s) + r * 32 + h * 16);
-                unsigned char* a = smem + L::a(s);
-                unsigned char* am = smem + L::am(s);
+                unsigned char* a = smem + L::a(d);
+                unsigned char* am = smem + L::am(d);
                 const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
 #pragma unroll
                 for (int cj = 0; cj < 4; ++cj) {
@@ -247,7 +265,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&dec[s]);
+                if (lane == 0) mbar_arrive(&full_d[d]);
             }
         }
     } else {
@@ -259,37 +277,40 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
-            if (!(ok = mbar_wait(acc_full, ui & 1, P.status, kTimeoutEpilogue))) break;
+            const int buf = ui % NB;
+            if (!(ok = mbar_wait(&acc_full[buf], (ui / NB) & 1, P.status, kTimeoutEpilogue))) break;
             tc_fence_after();
             const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
-            const uint32_t tb = tmem_base + ((uint32_t)(32 * q) << 16);
+            const uint32_t tb = tmem_base + buf * L::kAccStride + ((uint32_t)(32 * q) << 16);
             const double mu = ROWS ? P.mu[row] : 0.0;
             double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
             for (int c0 = 0; c0 < kc; c0 += 16) {
-                int32_t m1[16], m2[16], m3[16], x1[16], x2[16], x3[16];
+                int32_t m1[16], m2[16], m3[16];
                 tmem_ld16i(tb + c0, m1);
                 tmem_ld16i(tb + kc + c0, m2);
                 tmem_ld16i(tb + 2 * kc + c0, m3);
-                tmem_ld16i(tb + 3 * kc + c0, x1);
-                tmem_ld16i(tb + 4 * kc + c0, x2);
-                tmem_ld16i(tb + 5 * kc + c0, x3);
+                if (ROWS) {
+                    int32_t x1[16], x2[16], x3[16];
+                    tmem_ld16i(tb + 3 * kc + c0, x1);
+                    tmem_ld16i(tb + 4 * kc + c0, x2);
+                    tmem_ld16i(tb + 5 * kc + c0, x3);
 #pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
-                    const double xv = (double)x1[i] + (double)x2[i] * ib + (double)x3[i] * ib2;
-                    double v;
-                    if (ROWS) {
-                        v = mv + mu * xv;
-                    } else {
-                        const int c = ct * kc + c0 + i;
-                        v = mv * P.inv_f2[c] + xv * P.inv_f3[c];
+                    for (int i = 0; i < 16; ++i) {
+                        const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                        const double xv = (double)x1[i] + (double)x2[i] * ib + (double)x3[i] * ib2;
+                        dst[(int64_t)(c0 + i) * P.ld] = mv + mu * xv;
                     }
-                    dst[(int64_t)(c0 + i) * P.ld] = v;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                        dst[(int64_t)(c0 + i) * P.ld] = mv * P.inv_f[ct * kc + c0 + i];
+                    }
                 }
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(acc_empty);
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);
         }
     }
     tc_fence_before();
@@ -471,32 +492,29 @@ k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t l
     }
 }
 
-// Samples-pass operand from W^T (column-major, k x R): pieces of W f2 (rows q kp + c) and
-// of (mu o W) f3 (rows (3 + q) kp + c), t < r_pad; 1/f2, 1/f3 per column; and per-block
-// sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].  Grid: (r_pad / 2048, kp).
+// Samples-pass operand from W^T (column-major, k x R): pieces of W f (rows q kp + c) and of
+// (mu o W) f (rows (3 + q) kp + c), t < r_pad, with ONE factor f = 127 / max(|W|, |mu W|)
+// per column so that both MMAs accumulate into the same TMEM columns; 1/f per column; and
+// per-block sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].
+// Grid: (r_pad / 2048, kp).
 __global__ void __launch_bounds__(256)
 k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int64_t kp,
                         int64_t r_pad, const double* __restrict__ mu,
                         const unsigned long long* __restrict__ max_w,
                         const unsigned long long* __restrict__ max_muw, int8_t* __restrict__ B,
-                        double* __restrict__ inv_f2, double* __restrict__ inv_f3,
-                        double* __restrict__ cpart) {
+                        double* __restrict__ inv_f, double* __restrict__ cpart) {
     __shared__ double red[8];
     const int64_t c = blockIdx.y;
-    const double f2 = c < k ? quant_factor(max_w[c]) : 0.0;
-    const double f3 = c < k ? quant_factor(max_muw[c]) : 0.0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        inv_f2[c] = f2 > 0.0 ? 1.0 / f2 : 0.0;
-        inv_f3[c] = f3 > 0.0 ? 1.0 / f3 : 0.0;
-    }
+    const double f = c < k ? quant_factor(max(max_w[c], max_muw[c])) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) inv_f[c] = f > 0.0 ? 1.0 / f : 0.0;
     double cs = 0.0;
     const int64_t t0 = (int64_t)blockIdx.x * 2048;
     for (int64_t t = t0 + threadIdx.x; t < min(r_pad, t0 + 2048); t += 256) {
         int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0;
         if (c < k && t < R) {
             const double w = Wt[c * R + t];
-            quantise3(w * f2, a1, a2, a3);
-            quantise3(mu[t] * w * f3, b1, b2, b3);
+            quantise3(w * f, a1, a2, a3);
+            quantise3(mu[t] * w * f, b1, b2, b3);
             cs += mu[t] * w;
         }
         B[c * r_pad + t] = a1;
@@ -590,7 +608,7 @@ struct MixedRows {
 
 struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
-    DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f2, inv_f3;
+    DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
     DeviceBuffer<unsigned long long> max1, max_w, max_muw;
     CUtensorMap tm_b1{}, tm_b2{};
     const void* tm_b1_base = nullptr;
@@ -771,8 +789,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     ws.b2.resize(6 * kp * r_pad);
     ws.part.resize((int64_t)splits * kp * n_pad);
     ws.colpart.resize((int64_t)nrb * k);
-    ws.inv_f2.resize(kp);
-    ws.inv_f3.resize(kp);
+    ws.inv_f.resize(kp);
     ws.c0.resize(k);
     const int64_t key = kp * 1000003 + r_pad;
     if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
@@ -784,8 +801,8 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
         prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + 6.0 * kp * r_pad);
         dim3 g((unsigned)nrb, (unsigned)kp);
         k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), ws.max_w.get(),
-                                                  ws.max_muw.get(), ws.b2.get(), ws.inv_f2.get(),
-                                                  ws.inv_f3.get(), ws.colpart.get());
+                                                  ws.max_muw.get(), ws.b2.get(), ws.inv_f.get(),
+                                                  ws.colpart.get());
         k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get(), nullptr);
         CS_LAUNCH("mixed samples operand");
     }
@@ -797,8 +814,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     P.kb_per_split = kbs;
     P.kc = tl.kc;
     P.kp = (int)kp;
-    P.inv_f2 = ws.inv_f2.get();
-    P.inv_f3 = ws.inv_f3.get();
+    P.inv_f = ws.inv_f.get();
     P.part = ws.part.get();
     P.ld = n_pad;
     P.status = ws.status.get();
