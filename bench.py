@@ -269,6 +269,7 @@ def main():
 
     # ---- end to end through the public API from pinned host buffers
     e2e_ms = []
+    cs.profile_enable(True)
     for _ in range(max(1, args.e2e_steps)):
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
@@ -279,6 +280,8 @@ def main():
         t1.record()
         torch.cuda.synchronize()
         e2e_ms.append(t0.elapsed_time(t1))
+    e2e_prof = cs.profile_summary()
+    cs.profile_enable(False)
     e2e_s = float(np.mean(e2e_ms)) / 1e3
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda")
@@ -325,7 +328,8 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "pinned_host": bool(pinned)},
+                    "d2h_bytes_per_step": int(d2h), "pinned_host": bool(pinned),
+                    "ms_each": e2e_ms, "host_stages": e2e_prof.get("host", [])},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,

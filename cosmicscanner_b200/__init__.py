@@ -8,6 +8,8 @@ Python mirror of the reference's C++ interfaces over the library's C ABI
                               (src/kinship_operator.h:18-101)
 * :class:`LmmEngine`        — ``LmmEngine::prepareLowRankMatrixFree`` / ``scan``
                               (src/lmm_engine.h:108-131)
+* :class:`MatrixFreePCG`    — ``MatrixFreePCG`` (libCosmicCore/src/matrix_free_pcg.h:9-75)
+* :class:`StcgVce`          — ``STCG_VCE`` (libCosmicCore/src/stcg_vce.h:7-54)
 
 Every compute call runs the CUDA kernels in ``libcosmicscanner_b200.so``; there is
 no CPU fallback.  A missing library or CUDA device raises immediately.
@@ -265,6 +267,140 @@ class LmmEngine:
     def close(self):
         if self._h:
             _abi.lib().cs_lmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- PCG and AI-REML
+
+def pcg_solve_device(op: KinshipOperator, B_ptr: int, ldb: int, k: int, X_ptr: int, ldx: int,
+                     sigma2_g: float, sigma2_e: float, tol: float = 1e-10, max_iter: int = 2000,
+                     relative: bool = False, precision="fp64", kinship_divisor: float = 0.0,
+                     stream: int = 0) -> np.ndarray:
+    """MatrixFreePCG::solve (libCosmicCore/src/matrix_free_pcg.h:20-68) for k right-hand sides
+    of (sigma2_g K + sigma2_e I) X = B on device column-major buffers; returns iterations."""
+    it = np.zeros(max(k, 1), dtype=np.int32)
+    _check(_abi.lib().cs_pcg_solve(op._h, float(kinship_divisor), float(sigma2_g), float(sigma2_e),
+                                   C.c_void_p(B_ptr), ldb, k, C.c_void_p(X_ptr), ldx, float(tol),
+                                   int(relative), int(max_iter), _prec(precision), _ptr(it),
+                                   C.c_void_p(stream)))
+    return it[:k]
+
+
+class MatrixFreePCG:
+    """Host-array convenience over :func:`pcg_solve_device` (device memory through torch)."""
+
+    def __init__(self, op: KinshipOperator, sigma2_g: float, sigma2_e: float, precision="fp64",
+                 kinship_divisor: float = 0.0):
+        self.op, self.sg2, self.se2 = op, sigma2_g, sigma2_e
+        self.precision, self.divisor = precision, kinship_divisor
+        self.iterations = None
+
+    def solve(self, b, tol: float = 1e-8, max_iter: int = 1000, relative: bool = False):
+        import torch
+
+        b = np.asarray(b, dtype=np.float64)
+        vec = b.ndim == 1
+        B = b.reshape(len(b), -1) if vec else b
+        n, k = B.shape
+        dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()  # column-major n x k
+        dX = torch.zeros_like(dB)
+        self.iterations = pcg_solve_device(self.op, dB.data_ptr(), n, k, dX.data_ptr(), n,
+                                           self.sg2, self.se2, tol, max_iter, relative,
+                                           self.precision, self.divisor,
+                                           torch.cuda.current_stream().cuda_stream)
+        torch.cuda.current_stream().synchronize()
+        x = dX.cpu().numpy().T
+        return x[:, 0].copy() if vec else np.asfortranarray(x)
+
+
+class VceOptions(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32), ("tol", C.c_double), ("mc_samples", C.c_int32),
+        ("pcg_tol", C.c_double), ("pcg_relative", C.c_int32), ("pcg_max_iter", C.c_int32),
+        ("slq_probes", C.c_int32), ("slq_steps", C.c_int32), ("probe_seed", C.c_uint64),
+        ("precision", C.c_int32),
+    ]
+
+
+class VceResult(C.Structure):
+    _fields_ = [
+        ("sigma2_g", C.c_double), ("sigma2_pe", C.c_double), ("sigma2_e", C.c_double),
+        ("logl", C.c_double), ("iterations", C.c_int32), ("converged", C.c_int32),
+        ("pcg_iterations", C.c_int64), ("operator_applies", C.c_int64),
+        ("operator_columns", C.c_int64), ("seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class StcgVce:
+    """STCG_VCE (libCosmicCore/src/stcg_vce.h:7-54): matrix-free AI-REML with PCG solves and
+    Hutchinson trace probes.  ``rec_to_row=None`` is the single-record LMM (records are the
+    operator's rows); ``with_pe`` adds the permanent-environment component."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(_abi.lib().cs_vce_create(C.byref(h)))
+        self._h = h
+        self.result = None
+        self._rows = 0
+        self._p = 0
+
+    @staticmethod
+    def default_options(**overrides) -> VceOptions:
+        o = VceOptions()
+        _abi.lib().cs_vce_default_options(C.byref(o))
+        for k, v in overrides.items():
+            if k == "precision":
+                v = _prec(v)
+            setattr(o, k, v)
+        return o
+
+    def solve(self, op: KinshipOperator, y, X, rec_to_row=None, with_pe=False,
+              kinship_divisor: float = 0.0, **options) -> dict:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
+        rmap = None if rec_to_row is None else np.ascontiguousarray(rec_to_row, dtype=np.int32)
+        opt = self.default_options(**options)
+        res = VceResult()
+        _check(_abi.lib().cs_vce_solve_stcg(self._h, op._h, float(kinship_divisor), _ptr(rmap),
+                                            len(y), int(bool(with_pe)), _ptr(y), _ptr(X),
+                                            X.shape[1], C.byref(opt), C.byref(res)))
+        self.result = res.as_dict()
+        self._rows = op.rows()
+        self._p = X.shape[1]
+        return self.result
+
+    def getVarE(self):
+        return self.result["sigma2_e"]
+
+    def getVarsU(self):
+        return [self.result["sigma2_g"], self.result["sigma2_pe"]]
+
+    def solution(self):
+        beta = np.zeros(self._p)
+        a = np.zeros(self._rows)
+        pe = np.zeros(self._rows)
+        _check(_abi.lib().cs_vce_solution(self._h, _ptr(beta), _ptr(a), _ptr(pe)))
+        return beta, a, pe
+
+    def history(self) -> np.ndarray:
+        it = C.c_int64()
+        _check(_abi.lib().cs_vce_history(self._h, None, C.byref(it)))
+        out = np.zeros(5 * max(it.value, 1))
+        _check(_abi.lib().cs_vce_history(self._h, _ptr(out), C.byref(it)))
+        return out[:5 * it.value].reshape(-1, 5)
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_vce_destroy(self._h)
             self._h = None
 
     def __del__(self):

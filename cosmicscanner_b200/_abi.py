@@ -46,6 +46,13 @@ _SIGNATURES = {
     "cs_lmm_scan": ([_P, _P, _P, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_lmm_destroy": ([_P], None),
     "cs_normal_matrix": ([C.c_uint64, _I64, _I64, _P], _I),
+    "cs_pcg_solve": ([_P, _D, _D, _D, _P, _I64, _I64, _P, _I64, _D, _I, _I, _I, _P, _P], _I),
+    "cs_vce_default_options": ([_P], None),
+    "cs_vce_create": ([_P], _I),
+    "cs_vce_solve_stcg": ([_P, _P, _D, _P, _I64, _I, _P, _P, _I64, _P, _P], _I),
+    "cs_vce_solution": ([_P, _P, _P, _P], _I),
+    "cs_vce_history": ([_P, _P, _P], _I),
+    "cs_vce_destroy": ([_P], None),
     "cs_profile_enable": ([_I], _I),
     "cs_profile_summary": ([C.c_char_p, C.c_size_t, _P], _I),
     "cs_launch_count": ([_P], _I),

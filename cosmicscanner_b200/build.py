@@ -18,6 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcosmicscanner_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+CUDA_INCLUDE = "/usr/local/cuda/include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,9 +51,15 @@ def _compile(src: str, force: bool, verbose: bool) -> str:
     if (not force and os.path.exists(obj)
             and os.path.getmtime(obj) >= max(os.path.getmtime(path), _headers_mtime())):
         return obj
-    cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
-           "-Xcompiler", "-fPIC,-O2,-Wall,-Wno-unused-function", "--expt-relaxed-constexpr",
-           "-I", INCLUDE, "-c", path, "-o", obj]
+    if src.endswith(".cpp"):
+        # host-only translation units: the system g++ with OpenMP (small dense algebra)
+        cmd = [_host_cxx(), "-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-fopenmp",
+               "-Wall", "-Wno-unused-function", "-I", INCLUDE, "-I", CUDA_INCLUDE, "-c",
+               path, "-o", obj]
+    else:
+        cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
+               "-Xcompiler", "-fPIC,-O2,-Wall,-Wno-unused-function", "--expt-relaxed-constexpr",
+               "-I", INCLUDE, "-c", path, "-o", obj]
     if src.endswith(".cu") and verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -71,7 +78,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-shared", "-o", LIB, *objs,
-               "-lcublas", "-lcudart"]
+               "-lcublas", "-lcudart", "-Xcompiler", "-fopenmp"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

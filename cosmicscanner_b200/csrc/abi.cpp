@@ -27,6 +27,17 @@ void lmm_lowrank_basis(const cs_lmm* lmm, double* U, int64_t ldu, double* lambda
 void lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
               double min_maf, int precision, double* beta, double* se, double* pvalue,
               double* log10p, double* freq, int32_t* tested);
+void vce_default_options(cs_vce_options* o);
+cs_vce* vce_create();
+void vce_destroy(cs_vce* v);
+void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* rec_to_row,
+                    int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
+                    const cs_vce_options* opt, cs_vce_result* res);
+void vce_solution(const cs_vce* v, double* beta, double* a_rows, double* pe_rows);
+void vce_history(const cs_vce* v, double* out, int64_t* n_iter);
+void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, const double* B,
+                      int64_t ldb, int64_t k, double* X, int64_t ldx, double tol, int relative,
+                      int max_iter, int precision, int32_t* iterations, cudaStream_t s);
 }  // namespace cs
 
 namespace {
@@ -213,6 +224,54 @@ int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out) {
         CS_CUDA(cudaMemcpy(out, t.get(), 8 * n * cols, cudaMemcpyDeviceToHost));
     });
 }
+
+int cs_pcg_solve(cs_kinship* op, double kinship_divisor, double sigma2_g, double sigma2_e,
+                 const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx, double tol,
+                 int relative, int max_iter, int precision, int32_t* iterations, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        require(k == 0 || (B != nullptr && X != nullptr), "null argument");
+        cs::pcg_solve_public(op, kinship_divisor, sigma2_g, sigma2_e, B, ldb, k, X, ldx, tol,
+                             relative, max_iter, precision, iterations, (cudaStream_t)stream);
+    });
+}
+
+void cs_vce_default_options(cs_vce_options* opt) {
+    if (opt) cs::vce_default_options(opt);
+}
+
+int cs_vce_create(cs_vce** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = cs::vce_create();
+    });
+}
+
+int cs_vce_solve_stcg(cs_vce* vce, cs_kinship* op, double kinship_divisor,
+                      const int32_t* rec_to_row, int64_t n_records, int with_pe, const double* y,
+                      const double* X, int64_t p, const cs_vce_options* opt, cs_vce_result* res) {
+    return guarded([&] {
+        require(vce != nullptr && op != nullptr && res != nullptr, "null argument");
+        cs::vce_solve_stcg(vce, op, kinship_divisor, rec_to_row, n_records, with_pe, y, X, p, opt,
+                           res);
+    });
+}
+
+int cs_vce_solution(const cs_vce* vce, double* beta, double* a_rows, double* pe_rows) {
+    return guarded([&] {
+        require(vce != nullptr, "null vce handle");
+        cs::vce_solution(vce, beta, a_rows, pe_rows);
+    });
+}
+
+int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations) {
+    return guarded([&] {
+        require(vce != nullptr, "null vce handle");
+        cs::vce_history(vce, out, n_iterations);
+    });
+}
+
+void cs_vce_destroy(cs_vce* vce) { cs::vce_destroy(vce); }
 
 int cs_profile_enable(int on) {
     return guarded([&] { cs::prof::set_enabled(on != 0); });

@@ -201,6 +201,7 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
     if ((int64_t)n_bytes < 3 + n_snps * bps)
         fail(CS_ERR_FORMAT, "Invalid .bed file: " + std::to_string(n_bytes) +
                                 " bytes < expected " + std::to_string(3 + n_snps * bps));
+    prof::HostScope hs("genotypes_upload_stats");
     auto* g = new cs_genotypes();
     static std::atomic<uint64_t> next_uid{1};
     g->uid = next_uid.fetch_add(1);

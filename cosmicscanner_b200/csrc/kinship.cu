@@ -20,6 +20,7 @@ namespace cs {
 
 cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
                            const int32_t* variants, int64_t n_var) {
+    prof::HostScope hs("kinship_create");
     if (g == nullptr) fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: null reader");
     const int64_t N = g->n_samples, M = g->n_snps;
     bool identity = true;

@@ -6,6 +6,9 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace cs {
 namespace la {
@@ -42,16 +45,18 @@ std::vector<double> upper_inverse(const std::vector<double>& R, int n) {
 
 bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
           std::vector<double>& V) {
+    // A (row-major == column-major for a symmetric matrix) from the lower triangle
     std::vector<double> A((size_t)n * n);
     for (int c = 0; c < n; ++c)
         for (int r = 0; r < n; ++r) {
             const int lo_r = std::max(r, c), lo_c = std::min(r, c);
             A[r + (size_t)c * n] = A_in[lo_r + (size_t)lo_c * n];
         }
-    V.assign((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) V[i + (size_t)i * n] = 1.0;
-    std::vector<double> v(n), p(n), w(n);
-    // Householder reduction to tridiagonal form, accumulating V = H_0 H_1 ...
+    // Qt: transpose of the accumulated orthogonal factor, row-major: Qt[j][k] = Q[k][j]
+    std::vector<double> Qt((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Qt[(size_t)i * n + i] = 1.0;
+    std::vector<double> v(n), p(n), w(n), qv(n);
+    // Householder reduction to tridiagonal form: A <- H A H, Q <- Q H
     for (int k = 0; k + 2 < n; ++k) {
         double norm2 = 0.0;
         for (int i = k + 1; i < n; ++i) norm2 += A[i + (size_t)k * n] * A[i + (size_t)k * n];
@@ -67,29 +72,49 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
         vn = std::sqrt(vn);
         if (vn == 0.0) continue;
         for (int i = k + 1; i < n; ++i) v[i] /= vn;
-        // A <- H A H with H = I - 2 v v^T: A' = A - 2 (v w^T + w v^T), w = p - (v^T p) v
-        for (int i = 0; i < n; ++i) {
+        // p = A v (A symmetric: column c of A dotted with v)
+#pragma omp parallel for schedule(static) if (n > 96)
+        for (int c = 0; c < n; ++c) {
+            const double* col = A.data() + (size_t)c * n;
             double s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += A[i + (size_t)j * n] * v[j];
-            p[i] = s;
+            for (int j = k + 1; j < n; ++j) s += col[j] * v[j];
+            p[c] = s;
         }
         double kappa = 0.0;
         for (int i = k + 1; i < n; ++i) kappa += v[i] * p[i];
         for (int i = 0; i < n; ++i) w[i] = p[i] - kappa * v[i];
-        for (int c = 0; c < n; ++c)
-            for (int r = 0; r < n; ++r)
-                A[r + (size_t)c * n] -= 2.0 * (v[r] * w[c] + w[r] * v[c]);
-        // V <- V H
-        for (int r = 0; r < n; ++r) {
-            double s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += V[r + (size_t)j * n] * v[j];
-            for (int j = k + 1; j < n; ++j) V[r + (size_t)j * n] -= 2.0 * s * v[j];
+        // A' = A - 2 (v w^T + w v^T)
+#pragma omp parallel for schedule(static) if (n > 96)
+        for (int c = 0; c < n; ++c) {
+            double* col = A.data() + (size_t)c * n;
+            const double vc = v[c], wc = w[c];
+            for (int r = 0; r < n; ++r) col[r] -= 2.0 * (v[r] * wc + w[r] * vc);
+        }
+        // Q <- Q H: Q[r][j] -= 2 (Q v)_r v_j, i.e. Qt[j][r] -= 2 v_j qv_r
+        for (int r = 0; r < n; ++r) qv[r] = 0.0;
+        for (int j = k + 1; j < n; ++j) {
+            const double vj = v[j];
+            const double* row = Qt.data() + (size_t)j * n;
+            for (int r = 0; r < n; ++r) qv[r] += row[r] * vj;
+        }
+#pragma omp parallel for schedule(static) if (n > 96)
+        for (int j = k + 1; j < n; ++j) {
+            double* row = Qt.data() + (size_t)j * n;
+            const double vj = 2.0 * v[j];
+            for (int r = 0; r < n; ++r) row[r] -= vj * qv[r];
         }
     }
     std::vector<double> d(n), e(n, 0.0);
     for (int i = 0; i < n; ++i) d[i] = A[i + (size_t)i * n];
     for (int i = 0; i + 1 < n; ++i) e[i] = A[i + 1 + (size_t)i * n];
-    // Implicit QL with shifts on (d, e); e[i] couples d[i] and d[i+1].
+    // Implicit QL with shifts on (d, e); the plane rotations are recorded and applied to
+    // the eigenvector rows afterwards, in parallel (e[i] couples d[i] and d[i+1]).
+    struct Rot {
+        int i;
+        double c, s;
+    };
+    std::vector<Rot> rots;
+    rots.reserve((size_t)n * 8);
     for (int l = 0; l < n; ++l) {
         int iter = 0;
         int m;
@@ -106,7 +131,7 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
                 double s = 1.0, c = 1.0, pp = 0.0;
                 int i;
                 for (i = m - 1; i >= l; --i) {
-                    double f = s * e[i];
+                    const double f = s * e[i];
                     const double b = c * e[i];
                     r = std::hypot(f, g);
                     e[i + 1] = r;
@@ -122,11 +147,7 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
                     pp = s * r;
                     d[i + 1] = g + pp;
                     g = c * r - b;
-                    for (int k = 0; k < n; ++k) {
-                        f = V[k + (size_t)(i + 1) * n];
-                        V[k + (size_t)(i + 1) * n] = s * V[k + (size_t)i * n] + c * f;
-                        V[k + (size_t)i * n] = c * V[k + (size_t)i * n] - s * f;
-                    }
+                    rots.push_back(Rot{i, c, s});
                 }
                 if (r == 0.0 && i >= l) continue;
                 d[l] -= pp;
@@ -135,16 +156,35 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
             }
         } while (m != l);
     }
+    // eigenvectors: rows of Q (= columns of Qt) rotated in sequence; each row independently
+    std::vector<double> Vr((size_t)n * n);  // row-major: Vr[r][j] = Q[r][j]
+    for (int j = 0; j < n; ++j)
+        for (int r = 0; r < n; ++r) Vr[(size_t)r * n + j] = Qt[(size_t)j * n + r];
+#pragma omp parallel
+    {
+#ifdef _OPENMP
+        const int nt = omp_get_num_threads(), tid = omp_get_thread_num();
+#else
+        const int nt = 1, tid = 0;
+#endif
+        const int r0 = (int)((int64_t)n * tid / nt), r1 = (int)((int64_t)n * (tid + 1) / nt);
+        for (const Rot& rt : rots)
+            for (int r = r0; r < r1; ++r) {
+                double* row = Vr.data() + (size_t)r * n;
+                const double f = row[rt.i + 1];
+                row[rt.i + 1] = rt.s * row[rt.i] + rt.c * f;
+                row[rt.i] = rt.c * row[rt.i] - rt.s * f;
+            }
+    }
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
     std::sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
     evals.resize(n);
-    std::vector<double> W((size_t)n * n);
+    V.assign((size_t)n * n, 0.0);
     for (int c = 0; c < n; ++c) {
         evals[c] = d[order[c]];
-        for (int r = 0; r < n; ++r) W[r + (size_t)c * n] = V[r + (size_t)order[c] * n];
+        for (int r = 0; r < n; ++r) V[r + (size_t)c * n] = Vr[(size_t)r * n + order[c]];
     }
-    V.swap(W);
     return true;
 }
 

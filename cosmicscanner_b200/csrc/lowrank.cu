@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <optional>
 #include <random>
 
 #include "cs_internal.h"
@@ -60,54 +61,42 @@ void check_blas(cublasStatus_t st, const char* what) {
 #define CS_BLAS(call) check_blas((call), #call)
 
 // ---------------------------------------------------------------- QR
-// Thin QR of Y (n x k row-major) by Cholesky-QR repeated until the Gram matrix is the
-// identity to working precision (two passes normally; a shifted first pass when Y is
-// ill-conditioned).  Any orthonormal basis of span(Y) gives the same subspace iteration
-// as the reference's HouseholderQR (lmm_engine.cpp:931-941): Q is unique up to column
-// signs, which cancel in Q^T K Q and in U = Q W.
-// Y is used as scratch (cuBLAS does not multiply in place): the passes ping-pong
-// between Y and Q and the result always ends in Q.
+// Thin QR of Y (n x k row-major) by Cholesky-QR2: two passes of G = Y^T Y, G = R^T R,
+// Y <- Y R^{-1} (a triangular solve on the device); a first pass whose Gram matrix is not
+// numerically positive definite is shifted (shifted Cholesky-QR) and a third pass added.
+// Any orthonormal basis of span(Y) gives the same subspace iteration as the reference's
+// HouseholderQR (lmm_engine.cpp:931-941): Q is unique up to column signs, which cancel
+// in Q^T K Q and in U = Q W.  Y is left unchanged; the result is written to Q.
 void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q,
                  DeviceBuffer<double>& d_gram, cudaStream_t s) {
     const double one = 1.0, zero = 0.0;
     d_gram.resize(2 * k * k);
     double* G = d_gram.get();
-    double* Rinv_d = G + k * k;
+    double* Rd = G + k * k;
     std::vector<double> g(k * k), R;
-    double* src = Y;
-    double* dst = Q;
-    for (int pass = 0; pass < 4; ++pass) {
-        CS_BLAS(cublasSetStream(blas, s));
-        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, src,
-                            (int)k, src, (int)k, &zero, G, (int)k));
+    CS_CUDA(cudaMemcpyAsync(Q, Y, 8 * n * k, cudaMemcpyDeviceToDevice, s));
+    CS_BLAS(cublasSetStream(blas, s));
+    int passes = 2;
+    for (int pass = 0; pass < passes; ++pass) {
+        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, Q,
+                            (int)k, Q, (int)k, &zero, G, (int)k));
         CS_CUDA(cudaMemcpyAsync(g.data(), G, 8 * k * k, cudaMemcpyDeviceToHost, s));
         CS_CUDA(cudaStreamSynchronize(s));
-        double off = 0.0, tr = 0.0;
-        for (int64_t j = 0; j < k; ++j)
-            for (int64_t i = 0; i < k; ++i) {
-                if (i == j) tr += g[i + j * k];
-                else off = std::max(off, std::abs(g[i + j * k]));
-            }
-        if (pass > 0) {
-            double dev = off;
-            for (int64_t j = 0; j < k; ++j) dev = std::max(dev, std::abs(g[j + j * k] - 1.0));
-            if (dev < 1e-13 || pass == 3) break;
-        }
         if (!la::cholesky_upper(g, (int)k, R)) {
             // shifted Cholesky-QR: G + sigma I is safely positive definite
+            double tr = 0.0;
+            for (int64_t j = 0; j < k; ++j) tr += g[j + j * k];
             const double shift = 11.0 * (double)(n * k + k * (k + 1)) * 2.2e-16 * tr;
             for (int64_t j = 0; j < k; ++j) g[j + j * k] += shift;
             if (!la::cholesky_upper(g, (int)k, R))
                 fail(CS_ERR_NUMERIC, "QR of the sketch failed (rank-deficient sketch)");
+            passes = std::min(passes + 1, 4);
         }
-        std::vector<double> Rinv = la::upper_inverse(R, (int)k);
-        CS_CUDA(cudaMemcpyAsync(Rinv_d, Rinv.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
-        // Q^c = Rinv^T Y^c  (row-major Q = Y Rinv)
-        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)k, (int)n, (int)k, &one, Rinv_d,
-                            (int)k, src, (int)k, &zero, dst, (int)k));
-        std::swap(src, dst);
+        CS_CUDA(cudaMemcpyAsync(Rd, R.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
+        // row-major Q = Q R^{-1}  <=>  column-major Q^c = R^{-T} Q^c: solve R^T X = Q^c
+        CS_BLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
+                            CUBLAS_DIAG_NON_UNIT, (int)k, (int)n, &one, Rd, (int)k, Q, (int)k));
     }
-    if (src != Q) CS_CUDA(cudaMemcpyAsync(Q, src, 8 * n * k, cudaMemcpyDeviceToDevice, s));
     CS_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -330,6 +319,7 @@ __global__ void k_scan_epilogue(ScanParams P) {
 }  // namespace
 
 cs_lmm* lmm_create() {
+    prof::HostScope hs("lmm_create");
     auto* l = new cs_lmm();
     if (cublasCreate(&l->blas) != CUBLAS_STATUS_SUCCESS) {
         delete l;
@@ -338,7 +328,10 @@ cs_lmm* lmm_create() {
     return l;
 }
 
-void lmm_destroy(cs_lmm* l) { delete l; }
+void lmm_destroy(cs_lmm* l) {
+    prof::HostScope hs("lmm_destroy");
+    delete l;
+}
 
 void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const double* X, int64_t p,
                          int rank, int oversample, int64_t seed, double trace_threshold,
@@ -372,7 +365,8 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
         kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
         CS_CUDA(cudaStreamSynchronize(s));
     }
-    prof::HostScope hs_eig("lowrank_eigh_rank_reml");
+    std::optional<prof::HostScope> hs_stage;
+    hs_stage.emplace("lowrank_eigh");
     // B = Q^T K Q (sk x sk)
     small.resize(sk * sk);
     const double one = 1.0, zero = 0.0;
@@ -401,6 +395,8 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
             }
         }
     }
+    hs_stage.reset();
+    hs_stage.emplace("lowrank_basis_reml");
     // U = Q W_top (n x selected, row-major): U^c = W_top^T Q^c
     std::vector<double> wtop(sk * selected);
     for (int j = 0; j < selected; ++j)

@@ -7,7 +7,7 @@
 //     n = 312, m = 156, r = 31, a = 0xB5026F5AA96619E9, tempering (29, d), (17, b), (37, c),
 //     43, seeding multiplier 6364136223846793005) is the linear recurrence
 //     x[k] = x[k - 156] ^ twist(x[k - 312], x[k - 311]), so 156 consecutive words depend only
-//     on earlier words: one CTA advances the stream 156 words per step.
+//     on earlier words: one warp advances the stream 156 words per step.
 //  2. Marsaglia's polar method as libstdc++ implements it: uniforms u = double(raw) / 2^64
 //     (clamped below 1), x = 2u - 1, y = 2u' - 1 from consecutive draws, an attempt is
 //     accepted when r2 = x^2 + y^2 is in (0, 1]; accepted attempts are compacted in order.
@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "cs_internal.h"
+#include "vce_internal.h"
 
 namespace cs {
 
@@ -37,34 +38,55 @@ __device__ __forceinline__ uint64_t temper(uint64_t y) {
     return y;
 }
 
-// One CTA of 156 threads: continues the sequence from the 312 words in `state`
-// (x[K-312 .. K-1]), writes n_out tempered outputs x[K ..], then the new last 312 words.
-__global__ void __launch_bounds__(kMtM, 1)
+// One warp continues the sequence from the 312 words in `state` (x[K-312 .. K-1]), writes
+// n_out tempered outputs x[K ..], then stores the new last 312 words (the engine advances by
+// n_out rounded up to a multiple of 156).  Step s produces x[K + 156 s + t], t = 0..155, from x[. - 312] and x[. - 311]
+// (step s - 2, slots t and t + 1; slot 0 of step s - 1 for t = 155) and x[. - 156] (step
+// s - 1, slot t).  Lane l owns slots t = l + 32 j, j = 0..4, and keeps the words of the two
+// previous steps in registers, so a step needs shuffles only: no shared memory and no
+// block barrier on the recurrence's critical path.
+__global__ void __launch_bounds__(32, 1)
 k_mt64(uint64_t* __restrict__ state, int64_t n_out, uint64_t* __restrict__ out) {
-    __shared__ uint64_t ring[kRing];
-    const int tid = threadIdx.x;
-    for (int i = tid; i < kMtN; i += kMtM) ring[i] = state[i];
-    __syncthreads();
-    // local index L = global index - (K - 312); ring slot = L mod 468
-    int a = 0, b = 1, c = kMtM, w = kMtN;  // slots of L-312, L-311, L-156, L for L = 312 + tid
-    a += tid; b += tid; c += tid; w += tid;
-    a %= kRing; b %= kRing; c %= kRing; w %= kRing;
-    for (int64_t base = 0; base < n_out; base += kMtM) {
-        const uint64_t y = (ring[a] & kUpper) | (ring[b] & kLower);
-        const uint64_t v = ring[c] ^ (y >> 1) ^ ((y & 1ull) ? kMatA : 0ull);
-        ring[w] = v;  // slot of L - 468: no thread reads it in this step
-        if (base + tid < n_out) out[base + tid] = temper(v);
-        __syncthreads();
-        a += kMtM; b += kMtM; c += kMtM; w += kMtM;
-        if (a >= kRing) a -= kRing;
-        if (b >= kRing) b -= kRing;
-        if (c >= kRing) c -= kRing;
-        if (w >= kRing) w -= kRing;
+    const int lane = threadIdx.x;
+    constexpr int kSlots = 5;
+    uint64_t p2[kSlots], p1[kSlots];
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) {
+        const int t = lane + 32 * j;
+        p2[j] = t < kMtM ? state[t] : 0ull;
+        p1[j] = t < kMtM ? state[kMtM + t] : 0ull;
     }
-    // last 312 words in order: local indices steps*156 .. steps*156 + 311
     const int64_t steps = (n_out + kMtM - 1) / kMtM;
-    const int start = (int)((steps * kMtM) % kRing);
-    for (int i = tid; i < kMtN; i += kMtM) state[i] = ring[(start + i) % kRing];
+    for (int64_t st = 0; st < steps; ++st) {
+        uint64_t nw[kSlots];
+        const uint64_t first_prev = __shfl_sync(0xffffffffu, p1[0], 0);  // slot 0, step s-1
+#pragma unroll
+        for (int j = 0; j < kSlots; ++j) {
+            const uint64_t down = __shfl_down_sync(0xffffffffu, p2[j], 1);
+            const uint64_t wrap = __shfl_sync(0xffffffffu, j + 1 < kSlots ? p2[j + 1] : 0ull, 0);
+            const int t = lane + 32 * j;
+            uint64_t nb = lane < 31 ? down : wrap;  // word of slot t + 1, step s - 2
+            if (t == kMtM - 1) nb = first_prev;
+            const uint64_t y = (p2[j] & kUpper) | (nb & kLower);
+            nw[j] = p1[j] ^ (y >> 1) ^ ((y & 1ull) ? kMatA : 0ull);
+        }
+        uint64_t* o = out + st * kMtM;
+#pragma unroll
+        for (int j = 0; j < kSlots; ++j) {
+            const int t = lane + 32 * j;
+            if (t < kMtM && st * kMtM + t < n_out) o[t] = temper(nw[j]);
+            p2[j] = p1[j];
+            p1[j] = nw[j];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) {
+        const int t = lane + 32 * j;
+        if (t < kMtM) {
+            state[t] = p2[j];
+            state[kMtM + t] = p1[j];
+        }
+    }
 }
 
 __device__ __forceinline__ double canonical(uint64_t r) {
@@ -148,6 +170,26 @@ __global__ void k_polar(const double* __restrict__ pairs, int64_t count, int64_t
     }
 }
 
+// out[i * ld + t] = +1 / -1 from the top bit of draw t * n + i
+// (std::uniform_int_distribution<int>(0, 1) over mt19937_64 returns the draw's top bit).
+__global__ void k_rademacher(const uint64_t* __restrict__ raw, int64_t n, int64_t cols,
+                             double* __restrict__ out, int64_t ld) {
+    const int64_t total = n * cols;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = e / n, i = e - t * n;
+        out[i * ld + t] = (raw[e] >> 63) ? 1.0 : -1.0;
+    }
+}
+
+std::vector<uint64_t> seeded_state(uint64_t seed) {
+    std::vector<uint64_t> st(kMtN);
+    st[0] = seed;
+    for (int i = 1; i < kMtN; ++i)
+        st[i] = 6364136223846793005ull * (st[i - 1] ^ (st[i - 1] >> 62)) + (uint64_t)i;
+    return st;
+}
+
 }  // namespace
 
 // Omega (n x cols, written row-major with leading dimension ld) on the device.
@@ -157,10 +199,7 @@ void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out
     if (count == 0) return;
     const int64_t pairs = (count + 1) / 2;
     // seeded state (mt19937_64 seeding recurrence)
-    std::vector<uint64_t> st(kMtN);
-    st[0] = seed;
-    for (int i = 1; i < kMtN; ++i)
-        st[i] = 6364136223846793005ull * (st[i - 1] ^ (st[i - 1] >> 62)) + (uint64_t)i;
+    const std::vector<uint64_t> st = seeded_state(seed);
     ws.state.resize(kMtN);
     CS_CUDA(cudaMemcpyAsync(ws.state.get(), st.data(), 8 * kMtN, cudaMemcpyHostToDevice, s));
     ws.pairs.resize(2 * pairs);
@@ -177,7 +216,7 @@ void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out
         ws.offsets.resize(blocks);
         {
             prof::Scope ps("mt19937_64_stream", s, 0.0, 16.0 * attempts);
-            k_mt64<<<1, kMtM, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
+            k_mt64<<<1, 32, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
             CS_LAUNCH("mt19937_64_stream");
         }
         {
@@ -210,6 +249,49 @@ void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out
         k_polar<<<std::max(blocks, 1), 256, 0, s>>>(ws.pairs.get(), count, n, ld, d_out);
         CS_LAUNCH("polar_pairs");
     }
+}
+
+void mt64_seed_device(uint64_t seed, uint64_t* d_state, cudaStream_t s) {
+    const std::vector<uint64_t> st = seeded_state(seed);
+    CS_CUDA(cudaMemcpyAsync(d_state, st.data(), 8 * kMtN, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+}
+
+void mt64_generate(uint64_t* d_state, int64_t n_out, uint64_t* d_out, cudaStream_t s) {
+    if (n_out <= 0) return;
+    prof::Scope ps("mt19937_64_stream", s, 0.0, 8.0 * n_out);
+    k_mt64<<<1, 32, 0, s>>>(d_state, n_out, d_out);
+    CS_LAUNCH("mt19937_64_stream");
+}
+
+void RademacherStream::seed(uint64_t sd, cudaStream_t s) {
+    state.resize(kMtN);
+    carry.resize(kMtM);
+    n_carry = 0;
+    mt64_seed_device(sd, state.get(), s);
+}
+
+// Draws n * cols words in order; the engine runs in whole 156-word steps, and the words of
+// the last step that this call does not use are kept for the next call.
+void RademacherStream::draw(int64_t n, int64_t cols, double* out, int64_t ld, cudaStream_t s) {
+    const int64_t need = n * cols;
+    if (need <= 0) return;
+    const int64_t fresh = std::max<int64_t>(0, need - n_carry);
+    const int64_t gen = round_up(fresh, kMtM);
+    raw.resize(n_carry + gen);
+    if (n_carry)
+        CS_CUDA(cudaMemcpyAsync(raw.get(), carry.get(), 8 * n_carry, cudaMemcpyDeviceToDevice, s));
+    mt64_generate(state.get(), gen, raw.get() + n_carry, s);
+    {
+        prof::Scope ps("rademacher_signs", s, 0.0, 16.0 * need);
+        const int blocks = (int)std::min<int64_t>((need + 255) / 256, 32LL * num_sms());
+        k_rademacher<<<std::max(blocks, 1), 256, 0, s>>>(raw.get(), n, cols, out, ld);
+        CS_LAUNCH("rademacher_signs");
+    }
+    const int64_t left = n_carry + gen - need;
+    if (left > 0)
+        CS_CUDA(cudaMemcpyAsync(carry.get(), raw.get() + need, 8 * left, cudaMemcpyDeviceToDevice, s));
+    n_carry = left;
 }
 
 }  // namespace cs

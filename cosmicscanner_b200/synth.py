@@ -104,3 +104,29 @@ def config1(seed=20261203 + 1):
 def config2(seed=20261203 + 2, n=50000, m=100000):
     return cohort(n, m, seed, maf_lo=0.05, n_pops=2, fst=0.01, missing=0.02, n_causal=1000,
                   h2=0.4, covariates="intercept+normal+bernoulli")
+
+
+def repeatability_cohort(n, m, seed, max_records=5, h2=0.3, repeatability=0.5, maf_lo=0.01,
+                         missing=0.01, n_causal=100):
+    """Record-level repeatability data: records per individual ~ U{1..max_records};
+    y = X beta + Zr (g + pe) + e with var(g) = h2, var(pe) = repeatability - h2,
+    var(e) = 1 - repeatability; fixed effects intercept, N(0,1) and a 4-level factor
+    (three indicator columns).  Returns dict(bed, n, m, rec_to_row, y, X)."""
+    base = cohort(n, m, seed, maf_lo=maf_lo, missing=missing, n_causal=n_causal, h2=1.0,
+                  covariates="intercept")
+    rng = np.random.default_rng(seed + 7)
+    g = (base["y"] - base["y"].mean()) / (base["y"].std() or 1.0) * np.sqrt(h2)
+    pe = rng.standard_normal(n) * np.sqrt(max(repeatability - h2, 0.0))
+    counts = rng.integers(1, max_records + 1, size=n)
+    rec_to_row = np.repeat(np.arange(n, dtype=np.int32), counts)
+    n_rec = len(rec_to_row)
+    level = rng.integers(0, 4, size=n_rec)
+    X = np.column_stack([np.ones(n_rec), rng.standard_normal(n_rec)] +
+                        [(level == q).astype(np.float64) for q in range(1, 4)])
+    beta = np.array([0.0, 0.5, 0.2, -0.1, 0.3])
+    y = X @ beta + g[rec_to_row] + pe[rec_to_row] + rng.standard_normal(n_rec) * np.sqrt(1 - repeatability)
+    return {"bed": base["bed"], "n": n, "m": m, "rec_to_row": rec_to_row, "y": y, "X": X}
+
+
+def config4(seed=20261203 + 4, n=100000, m=300000):
+    return repeatability_cohort(n, m, seed)

@@ -138,6 +138,68 @@ void cs_lmm_destroy(cs_lmm* lmm);
  * and copied to `out` (host, column-major, ld = n). */
 int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out);
 
+/* ---------------------------------------------------------------- PCG and AI-REML
+ * Replaces cosmic::MatrixFreePCG (libCosmicCore/src/matrix_free_pcg.h:9-75) for the mixed-
+ * model covariance V = sigma2_g K + sigma2_e I with the scalar preconditioner
+ * 1/(sigma2_g + sigma2_e) (libCosmicCore/src/stcg_vce.cpp:117-126).  B and X are device,
+ * column-major (rows() x k, leading dimensions ldb / ldx); all k right-hand sides advance
+ * together, each with its own CG recurrence, and stop when ||r|| < tol (relative = 0, the
+ * reference's absolute rule, matrix_free_pcg.h:51) or ||r|| < tol ||b|| (relative = 1), or at
+ * max_iter without an error (the reference returns silently too).  K is the operator's
+ * Z Z^T scaled by 1 / kinship_divisor (<= 0: the operator's own selected-variant count).
+ * iterations (host, k entries, may be NULL) receives each column's iteration count. */
+int cs_pcg_solve(cs_kinship* op, double kinship_divisor, double sigma2_g, double sigma2_e,
+                 const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx, double tol,
+                 int relative, int max_iter, int precision, int32_t* iterations, void* stream);
+
+/* Options of the matrix-free AI-REML (VCEConfig, libCosmicCore/src/vce.h:139-160, as
+ * src/models/repeatability_model.cpp:604-612 fills it). */
+typedef struct cs_vce_options {
+    int32_t max_iter;     /* AI-REML iterations (--reml-maxit, 50) */
+    double tol;           /* stop when the largest relative change of theta < tol (1e-6) */
+    int32_t mc_samples;   /* Rademacher probes per iteration (VCEConfig::mc_samples, 20) */
+    double pcg_tol;       /* CG threshold on ||r|| (VCEConfig::pcg_tol, 1e-10) */
+    int32_t pcg_relative; /* 0: absolute ||r|| < pcg_tol (reference); 1: ||r|| < pcg_tol ||b|| */
+    int32_t pcg_max_iter; /* VCEConfig::pcg_max_iter, 2000 */
+    int32_t slq_probes;   /* SLQ probes for the log-likelihood (30); 0 skips it */
+    int32_t slq_steps;    /* Lanczos steps per SLQ probe (15) */
+    uint64_t probe_seed;  /* mt19937_64 seed of the trace probes (20250101) */
+    int32_t precision;    /* CS_PRECISION_FP64 or CS_PRECISION_MIXED for the kinship applies */
+} cs_vce_options;
+
+typedef struct cs_vce_result {
+    double sigma2_g, sigma2_pe, sigma2_e;
+    double logl;               /* REML log-likelihood of the last iteration (NaN without SLQ) */
+    int32_t iterations, converged;
+    int64_t pcg_iterations;    /* CG iterations summed over right-hand sides */
+    int64_t operator_applies;  /* kinship applies (each carries a block of right-hand sides) */
+    int64_t operator_columns;  /* right-hand sides carried by those applies */
+    double seconds;
+} cs_vce_result;
+
+typedef struct cs_vce cs_vce;
+
+void cs_vce_default_options(cs_vce_options* opt);
+int cs_vce_create(cs_vce** out);
+/* Replaces STCG_VCE::solve() (libCosmicCore/src/stcg_vce.cpp:157-407): matrix-free AI-REML
+ * for theta = (sigma2_g, sigma2_pe, sigma2_e) with V = sg2 Zr K Zr^T + spe2 Zr Zr^T + se2 I
+ * over n_records records.  rec_to_row[i] is the operator row of record i (-1: none; NULL:
+ * record i is row i, the single-record LMM).  with_pe = 0 drops the permanent-environment
+ * component.  K = Z Z^T / kinship_divisor: STCG divides by the reader's total SNP count,
+ * monomorphic SNPs included (stcg_vce.cpp:86).  y (n_records) and X (n_records x p,
+ * column-major) are host arrays.  Starting values, trace probes (one mt19937_64 stream),
+ * EM warm-up, damped AI steps with clamps and the stopping rule follow the reference. */
+int cs_vce_solve_stcg(cs_vce* vce, cs_kinship* op, double kinship_divisor,
+                      const int32_t* rec_to_row, int64_t n_records, int with_pe, const double* y,
+                      const double* X, int64_t p, const cs_vce_options* opt, cs_vce_result* res);
+/* The final solution (stcg_vce.cpp:364-406): beta (p), genetic values a = sg2 K Zr^T P y and
+ * permanent-environment effects spe2 Zr^T P y over all operator rows (host; NULL skips). */
+int cs_vce_solution(const cs_vce* vce, double* beta, double* a_rows, double* pe_rows);
+/* Per iteration: theta after the update (3), the log-likelihood and 1 for an AI step / 0 for
+ * an EM step; 5 doubles per iteration (the reference's verbose history lines). */
+int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations);
+void cs_vce_destroy(cs_vce* vce);
+
 /* ---------------------------------------------------------------- instrumentation
  * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and
  * PlinkKinshipOperator::BlockProfile (src/kinship_operator.h:55-63): a process-wide count

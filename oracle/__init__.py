@@ -24,6 +24,22 @@ def build() -> str:
     return _LIB_PATH
 
 
+class StcgOptions(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32), ("tol", C.c_double), ("mc_samples", C.c_int32),
+        ("pcg_tol", C.c_double), ("pcg_max_iter", C.c_int32), ("slq_probes", C.c_int32),
+        ("slq_steps", C.c_int32), ("probe_seed", C.c_uint64),
+    ]
+
+
+class StcgResult(C.Structure):
+    _fields_ = [
+        ("sigma2_g", C.c_double), ("sigma2_pe", C.c_double), ("sigma2_e", C.c_double),
+        ("logl", C.c_double), ("iterations", C.c_int32), ("converged", C.c_int32),
+        ("pcg_iterations", C.c_int64),
+    ]
+
+
 class LowRankResult(C.Structure):
     _fields_ = [
         ("rank", C.c_int32), ("sketch_size", C.c_int32),
@@ -75,6 +91,9 @@ def lib():
         L.orc_pcg_solve.argtypes = [_P, _I64, _I64, _P, _P] + sel + [
             C.c_double, C.c_double, _P, C.c_double, C.c_int, _P]
         L.orc_pcg_solve.restype = C.c_int
+        L.orc_stcg_vce.argtypes = [_P, _I64, _I64, _I64, _P, _P, _P, _I64, C.c_int, _P, _P, _I64,
+                                   _P, _P, _P, _P, _P]
+        L.orc_stcg_vce.restype = C.c_int
         _lib = L
     return _lib
 
@@ -199,6 +218,30 @@ class Bed:
         it = lib().orc_pcg_solve(_ptr(self.rows), self.n, self.stride, _ptr(self.mean),
                                  _ptr(self.inv_std), *args, sg2, se2, _ptr(b), tol, max_iter, _ptr(x))
         return x, it
+
+
+def stcg_vce(bed: "Bed", y, X, rec_to_row=None, with_pe=False, max_iter=50, tol=1e-6,
+             mc_samples=20, pcg_tol=1e-10, pcg_max_iter=2000, slq_probes=30, slq_steps=15,
+             probe_seed=20250101):
+    """STCG_VCE::solve restated (libCosmicCore/src/stcg_vce.cpp:157-407); returns
+    (result dict, beta, a_rows, pe_rows)."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
+    rmap = None if rec_to_row is None else np.ascontiguousarray(rec_to_row, dtype=np.int32)
+    opt = StcgOptions(max_iter, tol, mc_samples, pcg_tol, pcg_max_iter, slq_probes, slq_steps,
+                      probe_seed)
+    res = StcgResult()
+    beta = np.zeros(X.shape[1])
+    a = np.zeros(bed.n)
+    pe = np.zeros(bed.n)
+    rc = lib().orc_stcg_vce(_ptr(bed.rows), bed.n, bed.stride, bed.m, _ptr(bed.mean),
+                            _ptr(bed.inv_std), _ptr(rmap), len(y), int(bool(with_pe)), _ptr(y),
+                            _ptr(X), X.shape[1], C.byref(opt), C.byref(res), _ptr(beta), _ptr(a),
+                            _ptr(pe))
+    if rc != 0:
+        raise RuntimeError("oracle stcg_vce failed")
+    out = {name: getattr(res, name) for name, _ in res._fields_}
+    return out, beta, a, pe
 
 
 def kinship_batch_fixture(n=37, m=1031, seed=8128, rows=None, widths=(1, 7, 41)):

@@ -833,7 +833,7 @@ int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
                                  v, kv.data(), 1);
         for (int64_t i = 0; i < n; ++i) out[i] = sg2 * kv[i] + se2 * v[i];
     };
-    const double precond = 1.0 / (sg2 + se2);
+    const double diag = sg2 + se2;
     std::vector<double> r(n), z(n), pdir(n), ap(n);
     std::fill(x, x + n, 0.0);
     mult(x, ap.data());
@@ -845,7 +845,7 @@ int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
     if (std::sqrt(rn) < 1e-20) return 0;
     double rsold = 0.0;
     for (int64_t i = 0; i < n; ++i) {
-        z[i] = r[i] * precond;
+        z[i] = r[i] / diag;
         pdir[i] = z[i];
         rsold += r[i] * z[i];
     }
@@ -863,13 +863,488 @@ int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
         if (std::sqrt(rn) < tol) return it + 1;
         double rsnew = 0.0;
         for (int64_t i = 0; i < n; ++i) {
-            z[i] = r[i] * precond;
+            z[i] = r[i] / diag;
             rsnew += r[i] * z[i];
         }
         for (int64_t i = 0; i < n; ++i) pdir[i] = z[i] + (rsnew / rsold) * pdir[i];
         rsold = rsnew;
     }
     return max_iter;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- STCG_VCE
+namespace {
+
+// libCosmicCore/src/plink_reader.cpp:355-402 (multiply_Zt_v) and :241-308 (multiply_Z_v)
+// over every SNP of the reader, one worker; then apply_G's division by the SNP count
+// (libCosmicCore/src/stcg_vce.cpp:80-87).
+struct GenoMatrix {
+    const uint8_t* bed;
+    int64_t n, m, stride;
+    const double* mean;
+    const double* inv_std;
+    void apply_G(const double* u, double* out) const {
+        std::vector<double> t(m);
+        for (int64_t j = 0; j < m; ++j) {
+            const double is = inv_std[j];
+            if (is == 0.0) { t[j] = 0.0; continue; }
+            const double mu = mean[j];
+            const uint8_t* col = bed + j * stride;
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                const int code = code_at(col, i);
+                if (code != 1) acc += (static_cast<double>(kLookup[code]) - mu) * u[i];
+            }
+            t[j] = acc * is;
+        }
+        std::fill(out, out + n, 0.0);
+        for (int64_t j = 0; j < m; ++j) {
+            const double is = inv_std[j];
+            if (is == 0.0) continue;
+            const double mu = mean[j];
+            const double w = t[j] * is;
+            const double vmap[4] = {(static_cast<double>(kLookup[0]) - mu) * w, 0.0,
+                                    (static_cast<double>(kLookup[2]) - mu) * w,
+                                    (static_cast<double>(kLookup[3]) - mu) * w};
+            const uint8_t* col = bed + j * stride;
+            for (int64_t i = 0; i < n; ++i) out[i] += vmap[code_at(col, i)];
+        }
+        const double denom = (double)std::max<int64_t>(1, m);
+        for (int64_t i = 0; i < n; ++i) out[i] /= denom;
+    }
+};
+
+double dot(const std::vector<double>& a, const std::vector<double>& b) {
+    double s = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    return s;
+}
+
+// Eigen::LDLT solve of the 3x3 AI system as the reference uses it: a zero pivot (the
+// absent permanent-environment component) contributes a zero step.
+bool solve_ai(const double AI[3][3], const double g[3], double out[3]) {
+    int idx[3], k = 0;
+    for (int i = 0; i < 3; ++i)
+        if (AI[i][i] != 0.0) idx[k++] = i;
+    out[0] = out[1] = out[2] = 0.0;
+    std::vector<double> A(k * k), L, D;
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) A[a + b * k] = AI[idx[a]][idx[b]];
+    if (!ldlt(A.data(), k, L, D)) return false;
+    std::vector<double> r(k);
+    for (int a = 0; a < k; ++a) r[a] = g[idx[a]];
+    ldlt_solve(L, D, k, r.data());
+    for (int a = 0; a < k; ++a) out[idx[a]] = r[a];
+    return true;
+}
+
+// Symmetric tridiagonal eigen-decomposition (implicit QL); returns eigenvalues and the
+// first components of the eigenvectors (all the SLQ quadrature needs).
+void tridiag_eig_first(std::vector<double> d, std::vector<double> e, std::vector<double>& evals,
+                       std::vector<double>& first) {
+    const int n = (int)d.size();
+    std::vector<double> Z(n * n, 0.0);
+    for (int i = 0; i < n; ++i) Z[i + i * n] = 1.0;
+    e.push_back(0.0);
+    for (int l = 0; l < n; ++l) {
+        int iter = 0, m;
+        do {
+            for (m = l; m < n - 1; ++m) {
+                const double dd = std::abs(d[m]) + std::abs(d[m + 1]);
+                if (std::abs(e[m]) <= 1e-15 * dd) break;
+            }
+            if (m != l) {
+                if (++iter > 200) break;
+                double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                double r = std::hypot(g, 1.0);
+                g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
+                double s = 1.0, c = 1.0, p = 0.0;
+                int i;
+                for (i = m - 1; i >= l; --i) {
+                    double f = s * e[i], b = c * e[i];
+                    r = std::hypot(f, g);
+                    e[i + 1] = r;
+                    if (r == 0.0) { d[i + 1] -= p; e[m] = 0.0; break; }
+                    s = f / r; c = g / r;
+                    g = d[i + 1] - p;
+                    r = (d[i] - g) * s + 2.0 * c * b;
+                    p = s * r;
+                    d[i + 1] = g + p;
+                    g = c * r - b;
+                    for (int k = 0; k < n; ++k) {
+                        f = Z[k + (i + 1) * n];
+                        Z[k + (i + 1) * n] = s * Z[k + i * n] + c * f;
+                        Z[k + i * n] = c * Z[k + i * n] - s * f;
+                    }
+                }
+                if (r == 0.0 && i >= l) continue;
+                d[l] -= p; e[l] = g; e[m] = 0.0;
+            }
+        } while (m != l);
+    }
+    evals = d;
+    first.resize(n);
+    for (int i = 0; i < n; ++i) first[i] = Z[0 + i * n];
+}
+
+struct Stcg {
+    GenoMatrix geno;
+    const int32_t* rec_to_ind;  // NULL: record i is genotype row i
+    int64_t n_rec, p;
+    bool with_pe;
+    const double* y;
+    const double* X;  // n_rec x p column-major
+    double vg = 0.0, vpe = 0.0, ve = 0.0;
+    double pcg_tol;
+    int pcg_max_iter;
+    int64_t pcg_iterations = 0;
+
+    int ind(int64_t i) const { return rec_to_ind ? rec_to_ind[i] : (int)i; }
+    // stcg_vce.cpp:64-78
+    void gather(const double* v, std::vector<double>& u) const {
+        u.assign(geno.n, 0.0);
+        for (int64_t i = 0; i < n_rec; ++i)
+            if (ind(i) >= 0) u[ind(i)] += v[i];
+    }
+    void scatter(const std::vector<double>& u, double* out) const {
+        for (int64_t i = 0; i < n_rec; ++i) out[i] = ind(i) >= 0 ? u[ind(i)] : 0.0;
+    }
+    // stcg_vce.cpp:89-101
+    void dV_genetic(const double* v, double* out) const {
+        std::vector<double> u, gu(geno.n);
+        gather(v, u);
+        geno.apply_G(u.data(), gu.data());
+        scatter(gu, out);
+    }
+    void dV_pe(const double* v, double* out) const {
+        std::vector<double> u;
+        gather(v, u);
+        scatter(u, out);
+    }
+    // stcg_vce.cpp:103-115
+    void apply_V(const double* v, double* out) const {
+        std::vector<double> tmp(n_rec);
+        std::fill(out, out + n_rec, 0.0);
+        dV_genetic(v, tmp.data());
+        for (int64_t i = 0; i < n_rec; ++i) out[i] += vg * tmp[i];
+        if (with_pe) {
+            dV_pe(v, tmp.data());
+            for (int64_t i = 0; i < n_rec; ++i) out[i] += vpe * tmp[i];
+        }
+        for (int64_t i = 0; i < n_rec; ++i) out[i] += ve * v[i];
+    }
+    // stcg_vce.cpp:117-126 + matrix_free_pcg.h:20-68 (x0 = 0)
+    std::vector<double> solve_V(const std::vector<double>& b) {
+        const int64_t n = n_rec;
+        std::vector<double> x(n, 0.0), r(b), z(n), pd(n), ap(n);
+        if (std::sqrt(dot(r, r)) < 1e-20) return x;
+        double diag = std::max(ve, 1e-12) + std::max(vg, 1e-12);
+        if (with_pe) diag += std::max(vpe, 1e-12);
+        for (int64_t i = 0; i < n; ++i) z[i] = r[i] / diag;
+        pd = z;
+        double rsold = dot(r, z);
+        for (int it = 0; it < pcg_max_iter; ++it) {
+            ++pcg_iterations;
+            apply_V(pd.data(), ap.data());
+            const double alpha = rsold / dot(pd, ap);
+            for (int64_t i = 0; i < n; ++i) {
+                x[i] += alpha * pd[i];
+                r[i] -= alpha * ap[i];
+            }
+            if (std::sqrt(dot(r, r)) < pcg_tol) return x;
+            for (int64_t i = 0; i < n; ++i) z[i] = r[i] / diag;
+            const double rsnew = dot(r, z);
+            for (int64_t i = 0; i < n; ++i) pd[i] = z[i] + (rsnew / rsold) * pd[i];
+            rsold = rsnew;
+        }
+        return x;
+    }
+    // stcg_vce.cpp:128-145
+    struct Null {
+        std::vector<double> Vinv_y, Vinv_X, XtVinvX, XtVinvX_inv, beta;
+    };
+    bool compute_null(Null& nl) {
+        nl.Vinv_y = solve_V(std::vector<double>(y, y + n_rec));
+        nl.Vinv_X.assign(n_rec * p, 0.0);
+        for (int64_t j = 0; j < p; ++j) {
+            std::vector<double> xs = solve_V(std::vector<double>(X + j * n_rec, X + (j + 1) * n_rec));
+            std::copy(xs.begin(), xs.end(), nl.Vinv_X.begin() + j * n_rec);
+        }
+        nl.XtVinvX.assign(p * p, 0.0);
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) {
+                double acc = 0.0;
+                for (int64_t i = 0; i < n_rec; ++i) acc += X[i + a * n_rec] * nl.Vinv_X[i + b * n_rec];
+                nl.XtVinvX[a + b * p] = acc;
+            }
+        std::vector<double> L, D;
+        nl.XtVinvX_inv.assign(p * p, 0.0);
+        nl.beta.assign(p, 0.0);
+        if (p == 0) return true;
+        if (!ldlt(nl.XtVinvX.data(), p, L, D)) return false;
+        for (int64_t c = 0; c < p; ++c) {
+            std::vector<double> e(p, 0.0);
+            e[c] = 1.0;
+            ldlt_solve(L, D, p, e.data());
+            for (int64_t r = 0; r < p; ++r) nl.XtVinvX_inv[r + c * p] = e[r];
+        }
+        std::vector<double> xty(p, 0.0);
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t i = 0; i < n_rec; ++i) xty[a] += X[i + a * n_rec] * nl.Vinv_y[i];
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) nl.beta[a] += nl.XtVinvX_inv[a + b * p] * xty[b];
+        return true;
+    }
+    // stcg_vce.cpp:147-154: P v = V^-1 v - V^-1 X (XtVinvX)^-1 X^T V^-1 v
+    std::vector<double> project(const std::vector<double>& vinv_v, const Null& nl) const {
+        std::vector<double> xtv(p, 0.0), coef(p, 0.0), out(vinv_v);
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t i = 0; i < n_rec; ++i) xtv[a] += X[i + a * n_rec] * vinv_v[i];
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) coef[a] += nl.XtVinvX_inv[a + b * p] * xtv[b];
+        for (int64_t i = 0; i < n_rec; ++i) {
+            double acc = 0.0;
+            for (int64_t a = 0; a < p; ++a) acc += nl.Vinv_X[i + a * n_rec] * coef[a];
+            out[i] -= acc;
+        }
+        return out;
+    }
+    std::vector<double> apply_P(const std::vector<double>& v, const Null& nl) {
+        return project(solve_V(v), nl);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
+                 const double* mean, const double* inv_std, const int32_t* rec_to_ind,
+                 int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
+                 const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                 double* a_ind_out, double* pe_ind_out) {
+    Stcg st{GenoMatrix{bed, n_fam, n_snps, stride, mean, inv_std}, rec_to_ind, n_rec, p,
+            with_pe != 0, y, X};
+    st.pcg_tol = opt->pcg_tol;
+    st.pcg_max_iter = opt->pcg_max_iter;
+    const int64_t n = n_rec;
+    // stcg_vce.cpp:157-214: moment-based starting values
+    int64_t n_ind = 0;
+    for (int64_t i = 0; i < n; ++i) n_ind = std::max<int64_t>(n_ind, st.ind(i) + 1);
+    double mean_y = 0.0;
+    for (int64_t i = 0; i < n; ++i) mean_y += y[i];
+    mean_y /= (double)n;
+    double var_y = 0.0;
+    for (int64_t i = 0; i < n; ++i) var_y += (y[i] - mean_y) * (y[i] - mean_y);
+    var_y /= (double)std::max<int64_t>(1, n - 1);
+    const double var_floor = std::max(1e-10, var_y * 1e-6);
+    std::vector<double> sum_y(n_ind, 0.0), sumsq_y(n_ind, 0.0);
+    std::vector<int> cnt_y(n_ind, 0);
+    for (int64_t i = 0; i < n; ++i) {
+        const int idx = st.ind(i);
+        if (idx >= 0 && idx < n_ind) {
+            sum_y[idx] += y[i];
+            sumsq_y[idx] += y[i] * y[i];
+            cnt_y[idx] += 1;
+        }
+    }
+    double within_ss = 0.0, avg_n = 0.0;
+    int within_df = 0;
+    std::vector<double> subj_means;
+    for (int64_t i = 0; i < n_ind; ++i) {
+        if (cnt_y[i] <= 0) continue;
+        const double mi = sum_y[i] / cnt_y[i];
+        subj_means.push_back(mi);
+        avg_n += cnt_y[i];
+        if (cnt_y[i] > 1) {
+            within_ss += sumsq_y[i] - cnt_y[i] * mi * mi;
+            within_df += cnt_y[i] - 1;
+        }
+    }
+    avg_n = subj_means.empty() ? 1.0 : (avg_n / subj_means.size());
+    const double within_var = within_df > 0 ? within_ss / within_df : 0.5 * var_y;
+    double subj_mean = 0.0;
+    for (double m : subj_means) subj_mean += m;
+    subj_mean /= (double)std::max<size_t>(1, subj_means.size());
+    double between_var = 0.0;
+    for (double m : subj_means) between_var += (m - subj_mean) * (m - subj_mean);
+    between_var /= (double)std::max<int>(1, (int)subj_means.size() - 1);
+    const double rep_guess = std::max(var_floor, between_var - within_var / std::max(1.0, avg_n));
+    double pe_guess = std::max(var_floor, 0.35 * within_var);
+    double ve_guess = std::max(var_floor, within_var - pe_guess);
+    double vg_guess = std::max(var_floor, rep_guess);
+    const double total_guess = vg_guess + pe_guess + ve_guess;
+    if (total_guess > 0.0 && var_y > var_floor) {
+        const double scale = var_y / total_guess;
+        vg_guess *= scale;
+        pe_guess *= scale;
+        ve_guess *= scale;
+    }
+    st.ve = ve_guess;
+    st.vg = vg_guess;
+    st.vpe = st.with_pe ? pe_guess : 0.0;
+
+    std::mt19937_64 rng(opt->probe_seed);
+    std::uniform_int_distribution<int> bit(0, 1);
+    double last[3] = {NAN, NAN, NAN};
+    const int em_warmup = 4;
+    const double min_f = 0.5, max_f = 2.0, blend = 0.35;
+    res->converged = 0;
+    res->iterations = 0;
+    res->logl = NAN;
+    for (int iter = 0; iter < opt->max_iter; ++iter) {
+        Stcg::Null nl;
+        if (!st.compute_null(nl)) return -1;
+        std::vector<double> Py(n);
+        for (int64_t i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int64_t a = 0; a < p; ++a) acc += nl.Vinv_X[i + a * n] * nl.beta[a];
+            Py[i] = nl.Vinv_y[i] - acc;
+        }
+        std::vector<double> s[3], q[3];
+        s[0].assign(n, 0.0);
+        s[1].assign(n, 0.0);
+        s[2] = Py;
+        st.dV_genetic(Py.data(), s[0].data());
+        if (st.with_pe) st.dV_pe(Py.data(), s[1].data());
+        for (int k = 0; k < 3; ++k) q[k] = st.apply_P(s[k], nl);
+        double tr[3] = {0, 0, 0};
+        for (int t = 0; t < opt->mc_samples; ++t) {
+            std::vector<double> z(n);
+            for (int64_t i = 0; i < n; ++i) z[i] = bit(rng) ? 1.0 : -1.0;
+            std::vector<double> Pz = st.apply_P(z, nl);
+            std::vector<double> dg(n), dp(n, 0.0);
+            st.dV_genetic(z.data(), dg.data());
+            if (st.with_pe) st.dV_pe(z.data(), dp.data());
+            tr[0] += dot(Pz, dg);
+            tr[1] += dot(Pz, dp);
+            tr[2] += dot(Pz, z);
+        }
+        for (double& t : tr) t /= (double)opt->mc_samples;
+        double quad[3], grad[3];
+        for (int k = 0; k < 3; ++k) {
+            quad[k] = dot(Py, s[k]);
+            grad[k] = 0.5 * (quad[k] - tr[k]);
+        }
+        double AI[3][3];
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) AI[a][b] = AI[b][a] = 0.5 * dot(s[a], q[b]);
+        const double theta[3] = {st.vg, st.with_pe ? st.vpe : 0.0, st.ve};
+        double next[3] = {theta[0], theta[1], theta[2]};
+        bool em = iter < em_warmup;
+        if (!em) {
+            double delta[3];
+            if (solve_ai(AI, grad, delta) && std::isfinite(delta[0]) && std::isfinite(delta[1]) &&
+                std::isfinite(delta[2])) {
+                for (int k = 0; k < 3; ++k) {
+                    const double lo = std::max(var_floor, theta[k] * min_f);
+                    const double hi = std::max(lo, theta[k] * max_f);
+                    next[k] = std::max(lo, std::min(hi, theta[k] + blend * delta[k]));
+                }
+            } else {
+                em = true;
+            }
+        }
+        if (em) {
+            for (int k = 0; k < 3; ++k) {
+                const double denom = std::max(tr[k], var_floor);
+                double target = quad[k] / denom;
+                if (!std::isfinite(target) || target < 0.0) target = theta[k];
+                const double lo = std::max(var_floor, theta[k] * min_f);
+                const double hi = std::max(lo, theta[k] * max_f);
+                next[k] = std::max(lo, std::min(hi, target));
+            }
+        }
+        for (double& v : next) v = std::max(var_floor, v);
+        // stcg_vce.cpp:330-348: REML log-likelihood with the SLQ log-determinant (at the
+        // current theta, before the update); the estimator's probes come from one
+        // mt19937_64(42 + iter) stream, i.e. its one-thread schedule.
+        if (opt->slq_probes > 0) {
+            const int m = (int)std::min<int64_t>(opt->slq_steps, n);
+            std::mt19937_64 srng(42ull + (uint64_t)iter);
+            std::uniform_int_distribution<int> sbit(0, 1);
+            double total = 0.0;
+            for (int sp = 0; sp < opt->slq_probes; ++sp) {
+                std::vector<double> z(n);
+                for (int64_t i = 0; i < n; ++i) z[i] = sbit(srng) ? 1.0 : -1.0;
+                std::vector<std::vector<double>> V(m + 1, std::vector<double>(n, 0.0));
+                const double nz = std::sqrt((double)n);
+                for (int64_t i = 0; i < n; ++i) V[0][i] = z[i] / nz;
+                std::vector<double> alpha(m, 0.0), beta(m, 0.0);
+                int actual = m;
+                for (int j = 0; j < m; ++j) {
+                    std::vector<double> w(n);
+                    st.apply_V(V[j].data(), w.data());
+                    if (j > 0)
+                        for (int64_t i = 0; i < n; ++i) w[i] -= beta[j - 1] * V[j - 1][i];
+                    alpha[j] = dot(w, V[j]);
+                    for (int64_t i = 0; i < n; ++i) w[i] -= alpha[j] * V[j][i];
+                    for (int k = 0; k <= j; ++k) {
+                        const double pr = dot(w, V[k]);
+                        for (int64_t i = 0; i < n; ++i) w[i] -= pr * V[k][i];
+                    }
+                    beta[j] = std::sqrt(dot(w, w));
+                    if (beta[j] < 1e-12) {
+                        actual = j + 1;
+                        break;
+                    }
+                    for (int64_t i = 0; i < n; ++i) V[j + 1][i] = w[i] / beta[j];
+                }
+                std::vector<double> d(alpha.begin(), alpha.begin() + actual);
+                std::vector<double> e(beta.begin(), beta.begin() + std::max(0, actual - 1));
+                std::vector<double> ev, first;
+                tridiag_eig_first(d, e, ev, first);
+                double ss = 0.0;
+                for (int i = 0; i < actual; ++i)
+                    ss += first[i] * first[i] * std::log(std::max(ev[i], 1e-12));
+                total += (double)n * ss;
+            }
+            const double logdetV = total / opt->slq_probes;
+            std::vector<double> L, D;
+            double logdetX = 0.0;
+            if (p > 0 && ldlt(nl.XtVinvX.data(), p, L, D))
+                for (int64_t a = 0; a < p; ++a) logdetX += std::log(D[a]);
+            const double yPy = dot(std::vector<double>(y, y + n), Py);
+            res->logl = -0.5 * (logdetV + logdetX + yPy + (double)(n - p) * std::log(2 * M_PI));
+        }
+        double rel = 0.0;
+        if (iter > 0 && std::isfinite(last[0]) && std::isfinite(last[1]) && std::isfinite(last[2]))
+            for (int k = 0; k < 3; ++k)
+                rel = std::max(rel, std::abs(next[k] - last[k]) / (std::abs(last[k]) + 1e-12));
+        for (int k = 0; k < 3; ++k) last[k] = next[k];
+        st.vg = next[0];
+        if (st.with_pe) st.vpe = next[1];
+        st.ve = next[2];
+        res->iterations = iter + 1;
+        if (iter > 0 && rel < opt->tol) {
+            res->converged = 1;
+            break;
+        }
+    }
+    // stcg_vce.cpp:371-406: final BLUE / BLUP
+    Stcg::Null nl;
+    if (!st.compute_null(nl)) return -1;
+    std::vector<double> Py(n);
+    for (int64_t i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int64_t a = 0; a < p; ++a) acc += nl.Vinv_X[i + a * n] * nl.beta[a];
+        Py[i] = nl.Vinv_y[i] - acc;
+    }
+    std::vector<double> zi, ai(n_fam);
+    st.gather(Py.data(), zi);
+    st.geno.apply_G(zi.data(), ai.data());
+    if (beta_out) std::copy(nl.beta.begin(), nl.beta.end(), beta_out);
+    for (int64_t i = 0; i < n_fam; ++i) {
+        if (a_ind_out) a_ind_out[i] = ai[i] * st.vg;
+        if (pe_ind_out) pe_ind_out[i] = st.with_pe ? st.vpe * zi[i] : 0.0;
+    }
+    res->sigma2_g = st.vg;
+    res->sigma2_pe = st.with_pe ? st.vpe : 0.0;
+    res->sigma2_e = st.ve;
+    res->pcg_iterations = st.pcg_iterations;
+    return 0;
 }
 
 }  // extern "C"

@@ -133,6 +133,38 @@ int orc_pcg_solve(const uint8_t* bed, int64_t n_fam, int64_t stride,
                   double sg2, double se2, const double* b, double tol, int max_iter,
                   double* x);
 
+/* libCosmicCore/src/stcg_vce.cpp:157-407 (STCG_VCE::solve): matrix-free AI-REML with
+ * theta = (sigma2_g, sigma2_pe, sigma2_e), V = sg2 Zr (Z Z^T / n_snps) Zr^T + spe2 Zr Zr^T
+ * + se2 I over records.  The genotype operator is PlinkReader::multiply_Zt_v/multiply_Z_v
+ * over every SNP of the reader (plink_reader.cpp:241-402), scaled by the SNP count.
+ * rec_to_ind[i] is the genotype row of record i (NULL: record i is row i).  with_pe = 0
+ * drops the permanent-environment component (the single-record LMM).  Probes: one
+ * mt19937_64(probe_seed) stream with uniform_int_distribution<int>(0, 1).  SLQ is the
+ * estimator's one-thread schedule (seed 42 + iteration).  Outputs: beta (p), the genetic
+ * BLUP a = sg2 K gather(Py) and pe = spe2 gather(Py) over all n_fam rows. */
+typedef struct {
+    int32_t max_iter;
+    double tol;
+    int32_t mc_samples;
+    double pcg_tol;
+    int32_t pcg_max_iter;
+    int32_t slq_probes;
+    int32_t slq_steps;
+    uint64_t probe_seed;
+} orc_stcg_options;
+
+typedef struct {
+    double sigma2_g, sigma2_pe, sigma2_e, logl;
+    int32_t iterations, converged;
+    int64_t pcg_iterations;
+} orc_stcg_result;
+
+int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
+                 const double* mean, const double* inv_std, const int32_t* rec_to_ind,
+                 int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
+                 const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                 double* a_ind_out, double* pe_ind_out);
+
 #ifdef __cplusplus
 }
 #endif

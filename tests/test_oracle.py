@@ -109,3 +109,35 @@ def test_prepare_marker():
     assert np.allclose(vals, np.where(np.isnan(raw), 0.0, raw - mean), atol=0)
     ok, *_ = oracle.prepare_marker(np.array([0.0, 0.0, np.nan]), 0.01)
     assert not ok                                # fewer than 3 observed / monomorphic
+
+
+def test_oracle_pcg_matches_dense_solve():
+    """matrix_free_pcg.h restated on sg2 K + se2 I agrees with a dense FP64 solve."""
+    from cosmicscanner_b200 import synth
+
+    d = synth.cohort(120, 300, 11, missing=0.02, n_causal=20)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    Z = ref.dense_z()
+    K = Z @ Z.T / d["m"]
+    b = np.random.default_rng(2).standard_normal(d["n"])
+    x, it = ref.pcg_solve(b, 0.7, 0.3, 1e-11, 1000)
+    xd = np.linalg.solve(0.7 * K + 0.3 * np.eye(d["n"]), b)
+    assert 0 < it < 1000
+    assert np.abs(x - xd).max() < 1e-9 * np.abs(xd).max()
+
+
+def test_oracle_stcg_runs_and_recovers_scale():
+    """STCG_VCE restated: two-component run on a tiny cohort gives positive components that
+    add up to roughly the phenotypic variance, with the documented iteration budget."""
+    from cosmicscanner_b200 import synth
+
+    d = synth.cohort(150, 400, 12, missing=0.01, n_causal=30, h2=0.5)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    res, beta, a, pe = oracle.stcg_vce(ref, d["y"], d["X"], max_iter=5, mc_samples=4,
+                                       slq_probes=2, slq_steps=4)
+    assert res["iterations"] == 5
+    assert res["sigma2_g"] > 0 and res["sigma2_e"] > 0 and res["sigma2_pe"] == 0
+    total = res["sigma2_g"] + res["sigma2_e"]
+    assert 0.3 < total / np.var(d["y"]) < 3.0
+    assert np.isfinite(res["logl"])
+    assert np.all(pe == 0)
