@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-out", default="")
+    ap.add_argument("--apply-only", action="store_true",
+                    help="time kinship applies alone (the profiling case), not the REML+scan job")
+    ap.add_argument("--k", type=int, default=68, help="right-hand sides for --apply-only")
     return ap.parse_args()
 
 
@@ -140,6 +143,79 @@ def fp64_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def int8_peak_tops(torch):
+    """cuBLASLt int8 GEMM 8192^3 throughput on this GPU (the int8 tensor-pipe denominator)."""
+    a = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device="cuda")
+    b = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device="cuda").t()
+    for _ in range(2):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def profile_traffic():
+    """DRAM bytes per packed byte of the tensor-core passes from the committed ncu summary
+    (profiles/kinship_tc_passes_n20000_m30000_k68.md), or None."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", "kinship_tc_passes_n20000_m30000_k68.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    out = {}
+    for name in ("rows", "samples"):
+        m = re.search(rf"traffic_per_packed_byte_{name}:\s*([0-9.]+)", text)
+        if m:
+            out[name] = float(m.group(1))
+    return out or None
+
+
+def run_apply_only(args):
+    """Kinship applies alone: the small case the ncu captures use."""
+    import torch
+
+    import cosmicscanner_b200 as cs
+    from cosmicscanner_b200 import synth
+
+    torch.cuda.set_device(0)
+    d = synth.cohort(args.n, args.m, 20261203, n_pops=2, fst=0.01, missing=0.02, n_causal=100)
+    g = cs.Genotypes.from_bed_bytes(d["bed"], args.n, args.m)
+    op = cs.KinshipOperator(g, None, None)
+    X = torch.randn(args.k, args.n, dtype=torch.float64, device="cuda")  # column-major n x k
+    Y = torch.empty_like(X)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        op.apply_device(X.data_ptr(), args.n, args.k, Y.data_ptr(), args.n, args.precision, stream)
+    torch.cuda.synchronize()
+    cs.profile_enable(True)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(args.steps):
+        op.apply_device(X.data_ptr(), args.n, args.k, Y.data_ptr(), args.n, args.precision, stream)
+    e.record()
+    torch.cuda.synchronize()
+    prof = cs.profile_summary()
+    cs.profile_enable(False)
+    ms = s.elapsed_time(e) / args.steps
+    flops = 4.0 * args.n * args.m * args.k
+    print(json.dumps({"metric": "kinship apply ms", "value": ms, "unit": "ms", "n": args.n,
+                      "m": args.m, "k": args.k, "precision": args.precision,
+                      "tflops": flops / (ms * 1e-3) / 1e12,
+                      "kernels": [(k["name"], k["launches"], k["ms"] / k["launches"])
+                                  for k in prof["kernels"]]}))
+    return 0
+
+
 def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
     """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
     (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
@@ -207,6 +283,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.apply_only:
+        return run_apply_only(args)
     import torch
 
     world, rank, local = dist_setup()
@@ -301,11 +379,32 @@ def main():
             peak = peaks["bf16_tflops"]
             roof = {"bound": "tensor", "peak_kind": f"bf16_tflops ({peak_kind})"}
         achieved = flops_per_launch / (per_launch_ms * 1e-3) / 1e12
+        bytes_per_launch = top["bytes"] / top["launches"]
+        traffic = None
+        tr = profile_traffic()
+        if tr and "_tc" in top["name"]:
+            key = "rows" if "rows" in top["name"] else "samples"
+            if key in tr:
+                traffic = tr[key] * bytes_per_launch
         roof.update({"kernel": top["name"], "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                     "algorithmic_bytes_per_launch": top["bytes"] / top["launches"],
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "traffic_note": "ncu DRAM bytes per packed byte at N=20000 M=30000 k=68, "
+                                     "scaled by this launch's packed bytes",
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
                      "ms_per_launch": per_launch_ms,
                      "share_of_step": top["ms"] / ms})
+        if "_tc" in top["name"]:
+            # the int8 datapath: 6 MMAs per useful multiply-add (3 right-hand-side pieces x
+            # {dosage, missing} tiles) on columns padded to the column tile
+            k_rhs = RANK + OVERSAMPLE
+            tiles = -(-k_rhs // 80)
+            per_tile = -(-k_rhs // tiles)
+            kc = -(-per_tile // 16) * 16
+            ops = achieved * 6 * (tiles * kc) / k_rhs
+            ipeak = int8_peak_tops(torch)
+            roof["int8_datapath"] = {"mma_tops": ops, "peak_tops": ipeak,
+                                     "peak_kind": "cuBLASLt int8 GEMM 8192^3 measured in this run",
+                                     "frac": ops / ipeak}
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             threads = os.cpu_count() or 1

@@ -37,6 +37,14 @@ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 // nothing to any product or count.
 constexpr int64_t kRowAlign = 64;
 
+// Device memory from the device's stream-ordered pool (memory.cpp).  The pool keeps freed
+// blocks reserved, so handles created per request (operators, engines, their workspaces)
+// reuse memory instead of paying cudaMalloc / cudaFree each time.  device_alloc returns
+// memory usable from any stream; device_free waits for the device before returning the
+// block (the same guarantee cudaFree gives).
+void* device_alloc(size_t bytes);
+void device_free(void* p) noexcept;
+
 // Device allocation that frees itself.
 template <typename T>
 struct DeviceBuffer {
@@ -47,7 +55,7 @@ struct DeviceBuffer {
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
     ~DeviceBuffer() { release(); }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) device_free(ptr);
         ptr = nullptr;
         count = 0;
     }
@@ -55,7 +63,7 @@ struct DeviceBuffer {
         if (n <= count) return;
         release();
         if (n == 0) return;
-        CS_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+        ptr = static_cast<T*>(device_alloc(n * sizeof(T)));
         count = n;
     }
     T* get() const { return ptr; }

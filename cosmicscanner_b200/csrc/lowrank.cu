@@ -21,6 +21,7 @@
 
 #include "cs_internal.h"
 #include "linalg_host.h"
+#include "vce_internal.h"
 
 struct cs_lmm {
     int64_t n = 0, p = 0, rank = 0;
@@ -46,7 +47,6 @@ struct cs_lmm {
     cs::DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
     cs::DeviceBuffer<uint8_t> d_pass;
     ~cs_lmm() {
-        if (blas) cublasDestroy(blas);
         cs::mixed_scan_destroy(scan_mixed);
     }
 };
@@ -55,10 +55,6 @@ namespace cs {
 
 namespace {
 
-void check_blas(cublasStatus_t st, const char* what) {
-    if (st != CUBLAS_STATUS_SUCCESS) fail(CS_ERR_CUDA, std::string(what) + ": cuBLAS status " + std::to_string((int)st));
-}
-#define CS_BLAS(call) check_blas((call), #call)
 
 // ---------------------------------------------------------------- QR
 // Thin QR of Y (n x k row-major) by Cholesky-QR2: two passes of G = Y^T Y, G = R^T R,
@@ -321,9 +317,11 @@ __global__ void k_scan_epilogue(ScanParams P) {
 cs_lmm* lmm_create() {
     prof::HostScope hs("lmm_create");
     auto* l = new cs_lmm();
-    if (cublasCreate(&l->blas) != CUBLAS_STATUS_SUCCESS) {
+    try {
+        l->blas = shared_blas();
+    } catch (...) {
         delete l;
-        fail(CS_ERR_CUDA, "cublasCreate failed");
+        throw;
     }
     return l;
 }
@@ -337,6 +335,7 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
                          int rank, int oversample, int64_t seed, double trace_threshold,
                          int min_rank, int precision, cs_lowrank_diagnostics* diag) {
     const auto start = std::chrono::steady_clock::now();
+    l->blas = shared_blas();  // the calling thread's handle
     const int64_t n = op->rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
@@ -487,6 +486,7 @@ void lmm_lowrank_basis(const cs_lmm* l, double* U, int64_t ldu, double* lambda) 
 void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
               double min_maf, int precision, double* beta, double* se, double* pvalue,
               double* log10p, double* freq, int32_t* tested) {
+    l->blas = shared_blas();  // the calling thread's handle
     if (!l->prepared) fail(CS_ERR_INVALID_ARGUMENT, "low-rank model not prepared");
     if (precision != CS_PRECISION_FP64 && precision != CS_PRECISION_MIXED)
         fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");

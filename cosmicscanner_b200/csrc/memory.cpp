@@ -1,0 +1,54 @@
+// Device memory pool and shared cuBLAS handles.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "cs_internal.h"
+
+namespace cs {
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::once_flag g_pool_once[kMaxDevices];
+
+void prepare_pool(int dev) {
+    std::call_once(g_pool_once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+        // keep freed blocks reserved for this process (released when the context ends)
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    });
+}
+}  // namespace
+
+void* device_alloc(size_t bytes) {
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < kMaxDevices) prepare_pool(dev);
+    void* p = nullptr;
+    CS_CUDA(cudaMallocAsync(&p, bytes, 0));
+    // usable from every stream once the allocation is ordered on the legacy stream
+    CS_CUDA(cudaStreamSynchronize(0));
+    return p;
+}
+
+cublasHandle_t shared_blas() {
+    thread_local cublasHandle_t handles[kMaxDevices] = {};
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
+    if (!handles[dev] && cublasCreate(&handles[dev]) != CUBLAS_STATUS_SUCCESS)
+        fail(CS_ERR_CUDA, "cublasCreate failed");
+    return handles[dev];
+}
+
+void device_free(void* p) noexcept {
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, 0);
+}
+
+}  // namespace cs

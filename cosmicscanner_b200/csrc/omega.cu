@@ -7,7 +7,7 @@
 //     n = 312, m = 156, r = 31, a = 0xB5026F5AA96619E9, tempering (29, d), (17, b), (37, c),
 //     43, seeding multiplier 6364136223846793005) is the linear recurrence
 //     x[k] = x[k - 156] ^ twist(x[k - 312], x[k - 311]), so 156 consecutive words depend only
-//     on earlier words: one warp advances the stream 156 words per step.
+//     on earlier words: one CTA advances the stream 156 words per step.
 //  2. Marsaglia's polar method as libstdc++ implements it: uniforms u = double(raw) / 2^64
 //     (clamped below 1), x = 2u - 1, y = 2u' - 1 from consecutive draws, an attempt is
 //     accepted when r2 = x^2 + y^2 is in (0, 1]; accepted attempts are compacted in order.
@@ -26,7 +26,7 @@ namespace cs {
 
 namespace {
 
-constexpr int kMtN = 312, kMtM = 156, kRing = 468;
+constexpr int kMtN = 312, kMtM = 156;
 constexpr uint64_t kMatA = 0xB5026F5AA96619E9ull;
 constexpr uint64_t kUpper = 0xFFFFFFFF80000000ull, kLower = 0x7FFFFFFFull;
 
@@ -38,55 +38,38 @@ __device__ __forceinline__ uint64_t temper(uint64_t y) {
     return y;
 }
 
-// One warp continues the sequence from the 312 words in `state` (x[K-312 .. K-1]), writes
-// n_out tempered outputs x[K ..], then stores the new last 312 words (the engine advances by
-// n_out rounded up to a multiple of 156).  Step s produces x[K + 156 s + t], t = 0..155, from x[. - 312] and x[. - 311]
-// (step s - 2, slots t and t + 1; slot 0 of step s - 1 for t = 155) and x[. - 156] (step
-// s - 1, slot t).  Lane l owns slots t = l + 32 j, j = 0..4, and keeps the words of the two
-// previous steps in registers, so a step needs shuffles only: no shared memory and no
-// block barrier on the recurrence's critical path.
-__global__ void __launch_bounds__(32, 1)
+// One CTA of 156 threads continues the sequence from the 312 words in `state`
+// (x[K-312 .. K-1]), writes n_out tempered outputs x[K ..], then stores the new last 312
+// words (the engine advances by n_out rounded up to a multiple of 156).  Step s produces
+// x[K + 156 s + t], t = 0..155, from x[. - 312] and x[. - 156] (thread t's own words of steps
+// s - 2 and s - 1, kept in registers) and x[. - 311] (slot t + 1 of step s - 2, or slot 0 of
+// step s - 1 for t = 155), exchanged through a 3-step shared ring: one barrier per step.
+__global__ void __launch_bounds__(kMtM, 1)
 k_mt64(uint64_t* __restrict__ state, int64_t n_out, uint64_t* __restrict__ out) {
-    const int lane = threadIdx.x;
-    constexpr int kSlots = 5;
-    uint64_t p2[kSlots], p1[kSlots];
-#pragma unroll
-    for (int j = 0; j < kSlots; ++j) {
-        const int t = lane + 32 * j;
-        p2[j] = t < kMtM ? state[t] : 0ull;
-        p1[j] = t < kMtM ? state[kMtM + t] : 0ull;
-    }
+    __shared__ uint64_t ring[3][kMtM];
+    const int t = threadIdx.x;
+    uint64_t p2 = state[t], p1 = state[kMtM + t];
+    ring[1][t] = p2;  // step -2
+    ring[2][t] = p1;  // step -1
+    __syncthreads();
     const int64_t steps = (n_out + kMtM - 1) / kMtM;
+    int cur = 0, older = 1, prev = 2;  // ring slots of steps s, s - 2, s - 1
     for (int64_t st = 0; st < steps; ++st) {
-        uint64_t nw[kSlots];
-        const uint64_t first_prev = __shfl_sync(0xffffffffu, p1[0], 0);  // slot 0, step s-1
-#pragma unroll
-        for (int j = 0; j < kSlots; ++j) {
-            const uint64_t down = __shfl_down_sync(0xffffffffu, p2[j], 1);
-            const uint64_t wrap = __shfl_sync(0xffffffffu, j + 1 < kSlots ? p2[j + 1] : 0ull, 0);
-            const int t = lane + 32 * j;
-            uint64_t nb = lane < 31 ? down : wrap;  // word of slot t + 1, step s - 2
-            if (t == kMtM - 1) nb = first_prev;
-            const uint64_t y = (p2[j] & kUpper) | (nb & kLower);
-            nw[j] = p1[j] ^ (y >> 1) ^ ((y & 1ull) ? kMatA : 0ull);
-        }
-        uint64_t* o = out + st * kMtM;
-#pragma unroll
-        for (int j = 0; j < kSlots; ++j) {
-            const int t = lane + 32 * j;
-            if (t < kMtM && st * kMtM + t < n_out) o[t] = temper(nw[j]);
-            p2[j] = p1[j];
-            p1[j] = nw[j];
-        }
+        const uint64_t nb = t + 1 < kMtM ? ring[older][t + 1] : ring[prev][0];
+        const uint64_t y = (p2 & kUpper) | (nb & kLower);
+        const uint64_t v = p1 ^ (y >> 1) ^ ((y & 1ull) ? kMatA : 0ull);
+        ring[cur][t] = v;
+        if (st * kMtM + t < n_out) out[st * kMtM + t] = temper(v);
+        p2 = p1;
+        p1 = v;
+        __syncthreads();
+        const int next = older;  // the slot of step s - 2 is free for step s + 1
+        older = prev;
+        prev = cur;
+        cur = next;
     }
-#pragma unroll
-    for (int j = 0; j < kSlots; ++j) {
-        const int t = lane + 32 * j;
-        if (t < kMtM) {
-            state[t] = p2[j];
-            state[kMtM + t] = p1[j];
-        }
-    }
+    state[t] = p2;
+    state[kMtM + t] = p1;
 }
 
 __device__ __forceinline__ double canonical(uint64_t r) {
@@ -216,7 +199,7 @@ void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out
         ws.offsets.resize(blocks);
         {
             prof::Scope ps("mt19937_64_stream", s, 0.0, 16.0 * attempts);
-            k_mt64<<<1, 32, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
+            k_mt64<<<1, kMtM, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
             CS_LAUNCH("mt19937_64_stream");
         }
         {
@@ -260,7 +243,7 @@ void mt64_seed_device(uint64_t seed, uint64_t* d_state, cudaStream_t s) {
 void mt64_generate(uint64_t* d_state, int64_t n_out, uint64_t* d_out, cudaStream_t s) {
     if (n_out <= 0) return;
     prof::Scope ps("mt19937_64_stream", s, 0.0, 8.0 * n_out);
-    k_mt64<<<1, 32, 0, s>>>(d_state, n_out, d_out);
+    k_mt64<<<1, kMtM, 0, s>>>(d_state, n_out, d_out);
     CS_LAUNCH("mt19937_64_stream");
 }
 

@@ -34,9 +34,6 @@ struct cs_vce {
     std::vector<double> beta, a_rows, pe_rows, hist;
     int64_t p = 0, n_rows = 0;
     bool solved = false;
-    ~cs_vce() {
-        if (blas) cublasDestroy(blas);
-    }
 };
 
 namespace cs {
@@ -192,9 +189,11 @@ void vce_default_options(cs_vce_options* o) {
 
 cs_vce* vce_create() {
     auto* v = new cs_vce();
-    if (cublasCreate(&v->blas) != CUBLAS_STATUS_SUCCESS) {
+    try {
+        v->blas = shared_blas();
+    } catch (...) {
         delete v;
-        fail(CS_ERR_CUDA, "cublasCreate failed");
+        throw;
     }
     return v;
 }
@@ -286,6 +285,7 @@ void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* re
                     int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
                     const cs_vce_options* opt_in, cs_vce_result* res) {
     const auto t_start = std::chrono::steady_clock::now();
+    v->blas = shared_blas();  // the calling thread's handle
     cs_vce_options opt;
     if (opt_in) opt = *opt_in;
     else vce_default_options(&opt);

@@ -17,6 +17,9 @@ inline void check_blas_status(cublasStatus_t st, const char* what) {
 }
 #define CS_BLAS(call) ::cs::check_blas_status((call), #call)
 
+// One cuBLAS handle per (thread, device), created on first use and kept for the process.
+cublasHandle_t shared_blas();
+
 // Records -> genotype rows (libCosmicCore/src/stcg_vce.cpp:17-38, 64-78).  Identity when
 // every record is its own genotype row, in order.
 struct RecordMap {

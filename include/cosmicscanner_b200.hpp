@@ -1,0 +1,228 @@
+// Header-only C++ facade over the C ABI of cosmicscanner_b200.h, shaped like the reference's
+// interfaces so its call sites can swap in without semantic change:
+//   cs::Genotypes        ~ cosmic::PlinkReader (libCosmicCore/src/plink_reader.h)
+//   cs::KinshipOperator  ~ cosmic::KinshipOperator (src/kinship_operator.h:18-46)
+//   cs::pcg_solve        ~ cosmic::MatrixFreePCG::solve (libCosmicCore/src/matrix_free_pcg.h)
+//   cs::StcgVce          ~ cosmic::STCG_VCE (libCosmicCore/src/stcg_vce.h:7-54)
+//   cs::LmmEngine        ~ LmmEngine::prepareLowRankMatrixFree / scan (src/lmm_engine.h)
+// Status codes come back as std::runtime_error (std::invalid_argument for bad arguments)
+// carrying the library's message, as the reference throws.  Types are Eigen-free: matrices
+// are column-major std::vector<double> with explicit row counts.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "cosmicscanner_b200.h"
+
+namespace cs {
+
+inline void check(int status) {
+    if (status == CS_OK) return;
+    const std::string msg = cs_last_error();
+    if (status == CS_ERR_INVALID_ARGUMENT) throw std::invalid_argument(msg);
+    throw std::runtime_error(msg);
+}
+
+enum class Precision { FP64 = CS_PRECISION_FP64, Mixed = CS_PRECISION_MIXED };
+
+class Genotypes {
+   public:
+    // PlinkReader::openBed on `prefix`.bed/.bim/.fam; the packed matrix becomes resident.
+    static Genotypes open(const std::string& prefix) {
+        cs_genotypes* h = nullptr;
+        check(cs_genotypes_open_plink(prefix.c_str(), &h));
+        return Genotypes(h);
+    }
+    // From the bytes of a .bed file (magic included).
+    static Genotypes from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_samples, int64_t n_snps) {
+        cs_genotypes* h = nullptr;
+        check(cs_genotypes_create(bed, n_bytes, n_samples, n_snps, &h));
+        return Genotypes(h);
+    }
+    Genotypes(Genotypes&& o) noexcept : h_(std::exchange(o.h_, nullptr)) {}
+    Genotypes& operator=(Genotypes&& o) noexcept {
+        std::swap(h_, o.h_);
+        return *this;
+    }
+    Genotypes(const Genotypes&) = delete;
+    Genotypes& operator=(const Genotypes&) = delete;
+    ~Genotypes() { cs_genotypes_destroy(h_); }
+
+    int64_t getNumSamples() const { return info().first; }
+    int64_t getNumSnps() const { return info().second; }
+    // PlinkReader::computeStats outputs (over all .fam samples).
+    void stats(std::vector<double>& mean, std::vector<double>& inv_std) const {
+        mean.resize(getNumSnps());
+        inv_std.resize(getNumSnps());
+        check(cs_genotypes_stats(h_, mean.data(), inv_std.data(), nullptr, nullptr));
+    }
+    cs_genotypes* handle() const { return h_; }
+
+   private:
+    explicit Genotypes(cs_genotypes* h) : h_(h) {}
+    std::pair<int64_t, int64_t> info() const {
+        int64_t n = 0, m = 0;
+        check(cs_genotypes_info(h_, &n, &m, nullptr));
+        return {n, m};
+    }
+    cs_genotypes* h_ = nullptr;
+};
+
+class KinshipOperator {
+   public:
+    // createKinshipOperator(reader, keep_indices, variant_indices) (kinship_operator.cpp:370-374);
+    // empty vectors mean all samples / all variants.  `g` must outlive the operator.
+    KinshipOperator(const Genotypes& g, const std::vector<int>& keep = {},
+                    const std::vector<int>& variants = {}) {
+        check(cs_kinship_create(g.handle(), keep.empty() ? nullptr : keep.data(), (int64_t)keep.size(),
+                                variants.empty() ? nullptr : variants.data(),
+                                (int64_t)variants.size(), &h_));
+        check(cs_kinship_info(h_, &rows_, &m_));
+    }
+    KinshipOperator(const KinshipOperator&) = delete;
+    KinshipOperator& operator=(const KinshipOperator&) = delete;
+    ~KinshipOperator() { cs_kinship_destroy(h_); }
+
+    int rows() const { return (int)rows_; }
+    int cols() const { return (int)rows_; }
+    int numVariants() const { return (int)m_; }
+    bool isDense() const { return false; }
+
+    // apply(const MatrixXd& X, MatrixXd& out): X is rows() x k column-major (host).
+    void apply(const std::vector<double>& X, int64_t k, std::vector<double>& out,
+               Precision p = Precision::FP64) const {
+        if ((int64_t)X.size() != rows_ * k)
+            throw std::runtime_error("PlinkKinshipOperator::apply: dimension mismatch");
+        out.resize(rows_ * k);
+        check(cs_kinship_apply_host(h_, X.data(), rows_, k, out.data(), rows_, (int)p));
+    }
+    void applyTranspose(const std::vector<double>& X, int64_t k, std::vector<double>& out,
+                        Precision p = Precision::FP64) const {
+        apply(X, k, out, p);  // K is symmetric
+    }
+    // Device form: X, Y device pointers, column-major with leading dimensions.
+    void apply_device(const double* X, int64_t ldx, int64_t k, double* Y, int64_t ldy,
+                      Precision p = Precision::FP64, void* stream = nullptr) const {
+        check(cs_kinship_apply(h_, X, ldx, k, Y, ldy, (int)p, stream));
+    }
+    double trace() const {
+        double t = 0.0;
+        check(cs_kinship_trace(h_, &t));
+        return t;
+    }
+    void getDiagonal(std::vector<double>& d) const {
+        d.resize(rows_);
+        check(cs_kinship_diagonal(h_, d.data()));
+    }
+    cs_kinship* handle() const { return h_; }
+
+   private:
+    cs_kinship* h_ = nullptr;
+    int64_t rows_ = 0, m_ = 0;
+};
+
+// MatrixFreePCG::solve on (sigma2_g K + sigma2_e I) X = B, device column-major blocks.
+inline std::vector<int32_t> pcg_solve(const KinshipOperator& op, double sigma2_g, double sigma2_e,
+                                      const double* B, int64_t ldb, int64_t k, double* X,
+                                      int64_t ldx, double tol = 1e-8, int max_iter = 1000,
+                                      bool relative = false, Precision p = Precision::FP64,
+                                      double kinship_divisor = 0.0, void* stream = nullptr) {
+    std::vector<int32_t> it(k > 0 ? k : 1);
+    check(cs_pcg_solve(op.handle(), kinship_divisor, sigma2_g, sigma2_e, B, ldb, k, X, ldx, tol,
+                       relative ? 1 : 0, max_iter, (int)p, it.data(), stream));
+    it.resize(k);
+    return it;
+}
+
+class StcgVce {
+   public:
+    StcgVce() { check(cs_vce_create(&h_)); }
+    StcgVce(const StcgVce&) = delete;
+    StcgVce& operator=(const StcgVce&) = delete;
+    ~StcgVce() { cs_vce_destroy(h_); }
+
+    static cs_vce_options default_options() {
+        cs_vce_options o;
+        cs_vce_default_options(&o);
+        return o;
+    }
+    // STCG_VCE::solve(); X is n_records x p column-major; rec_to_row empty = one record per row.
+    cs_vce_result solve(const KinshipOperator& op, const std::vector<double>& y,
+                        const std::vector<double>& X, int64_t p,
+                        const std::vector<int32_t>& rec_to_row = {}, bool with_pe = false,
+                        double kinship_divisor = 0.0, const cs_vce_options& opt = default_options()) {
+        cs_vce_result r{};
+        check(cs_vce_solve_stcg(h_, op.handle(), kinship_divisor,
+                                rec_to_row.empty() ? nullptr : rec_to_row.data(), (int64_t)y.size(),
+                                with_pe ? 1 : 0, y.data(), X.empty() ? nullptr : X.data(), p, &opt,
+                                &r));
+        last_ = r;
+        rows_ = op.rows();
+        p_ = p;
+        return r;
+    }
+    double getVarE() const { return last_.sigma2_e; }
+    std::vector<double> getVarsU() const { return {last_.sigma2_g, last_.sigma2_pe}; }
+    // final_solution pieces: beta (p), genetic values and pe effects over operator rows
+    void solution(std::vector<double>& beta, std::vector<double>& a, std::vector<double>& pe) const {
+        beta.resize(p_);
+        a.resize(rows_);
+        pe.resize(rows_);
+        check(cs_vce_solution(h_, beta.data(), a.data(), pe.data()));
+    }
+
+   private:
+    cs_vce* h_ = nullptr;
+    cs_vce_result last_{};
+    int64_t rows_ = 0, p_ = 0;
+};
+
+class LmmEngine {
+   public:
+    LmmEngine() { check(cs_lmm_create(&h_)); }
+    LmmEngine(const LmmEngine&) = delete;
+    LmmEngine& operator=(const LmmEngine&) = delete;
+    ~LmmEngine() { cs_lmm_destroy(h_); }
+
+    // prepareLowRankMatrixFree(y, X, op, rank, ...): X column-major n x p, already FP32-rounded
+    // where the caller mirrors the reference's MatrixXf covariates.
+    cs_lowrank_diagnostics prepareLowRankMatrixFree(const std::vector<double>& y,
+                                                    const std::vector<double>& X, int64_t p,
+                                                    KinshipOperator& op, int rank = 256,
+                                                    int oversample = 10, int64_t seed = 42,
+                                                    double trace_threshold = 0.95, int min_rank = 1,
+                                                    Precision prec = Precision::FP64) {
+        cs_lowrank_diagnostics d{};
+        check(cs_lmm_prepare_lowrank_matrix_free(h_, op.handle(), y.data(),
+                                                 X.empty() ? nullptr : X.data(), p, rank,
+                                                 oversample, seed, trace_threshold, min_rank,
+                                                 (int)prec, &d));
+        return d;
+    }
+
+    struct ScanResult {
+        std::vector<double> beta, se, p, log10p, freq;
+        std::vector<int32_t> tested;
+    };
+    // scan(PlinkReader, ...) -> scanLowRank for every SNP, keep = analysed samples in y order.
+    ScanResult scan(const Genotypes& g, const std::vector<int32_t>& keep, double min_maf = 0.01,
+                    Precision prec = Precision::FP64) {
+        const int64_t m = g.getNumSnps();
+        ScanResult r;
+        for (auto* v : {&r.beta, &r.se, &r.p, &r.log10p, &r.freq}) v->resize(m);
+        r.tested.resize(m);
+        check(cs_lmm_scan(h_, g.handle(), keep.data(), (int64_t)keep.size(), min_maf, (int)prec,
+                          r.beta.data(), r.se.data(), r.p.data(), r.log10p.data(), r.freq.data(),
+                          r.tested.data()));
+        return r;
+    }
+
+   private:
+    cs_lmm* h_ = nullptr;
+};
+
+}  // namespace cs

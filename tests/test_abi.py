@@ -48,3 +48,39 @@ def test_package_fails_loudly_without_library(tmp_path):
         assert "no CPU fallback" in str(e)
     else:
         raise AssertionError("load of a missing library must raise")
+
+
+def test_cpp_facade_compiles_links_and_reports_errors(tmp_path):
+    """include/cosmicscanner_b200.hpp compiles against the header, links against the library
+    and turns a status code into the reference's exception types (no device work)."""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "facade.cpp"
+    src.write_text(r'''
+#include "cosmicscanner_b200.hpp"
+#include <cstdio>
+int main() {
+    unsigned char bad[4] = {0x6C, 0x1B, 0x00, 0};
+    try {
+        cs::Genotypes::from_bed(bad, 4, 4, 1);
+        return 1;
+    } catch (const std::runtime_error& e) {
+        std::printf("%s\n", e.what());
+    }
+    try {
+        cs::Genotypes::from_bed(bad, 4, 0, 1);
+        return 2;
+    } catch (const std::invalid_argument& e) {
+        std::printf("invalid: %s\n", e.what());
+    }
+    cs_vce_options o = cs::StcgVce::default_options();
+    return (o.mc_samples == 20 && o.pcg_tol == 1e-10 && o.probe_seed == 20250101ull) ? 0 : 3;
+}
+''')
+    exe = tmp_path / "facade"
+    lib_dir = os.path.dirname(_abi.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(root, "include"), str(src),
+                    "-o", str(exe), "-L", lib_dir, "-lcosmicscanner_b200",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "SNP-major" in out.stdout and "invalid:" in out.stdout
