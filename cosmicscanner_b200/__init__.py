@@ -410,6 +410,19 @@ class StcgVce:
             pass
 
 
+def write_assoc_txt(path: str, bim_path: str, results: dict, n_obs: int, stcg_columns=False):
+    """Writes `.assoc.txt` (src/gwas_output.cpp:123-183) from a scan result dict."""
+    m = len(results["p"])
+    arr = {k: np.ascontiguousarray(results[k], dtype=np.float64)
+           for k in ("freq", "beta", "se", "p", "log10p")}
+    tested = results.get("tested")
+    tested = None if tested is None else np.ascontiguousarray(tested, dtype=np.int32)
+    _check(_abi.lib().cs_write_assoc_txt(path.encode(), bim_path.encode(), m, int(n_obs),
+                                         _ptr(arr["freq"]), _ptr(arr["beta"]), _ptr(arr["se"]),
+                                         _ptr(arr["p"]), _ptr(arr["log10p"]), _ptr(tested),
+                                         int(bool(stcg_columns))))
+
+
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
     MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""

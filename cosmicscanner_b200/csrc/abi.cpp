@@ -38,6 +38,9 @@ void vce_history(const cs_vce* v, double* out, int64_t* n_iter);
 void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, const double* B,
                       int64_t ldb, int64_t k, double* X, int64_t ldx, double tol, int relative,
                       int max_iter, int precision, int32_t* iterations, cudaStream_t s);
+void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                     const double* freq, const double* beta, const double* se, const double* p,
+                     const double* log10p, const int32_t* tested, int stcg_columns);
 }  // namespace cs
 
 namespace {
@@ -272,6 +275,16 @@ int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations) {
 }
 
 void cs_vce_destroy(cs_vce* vce) { cs::vce_destroy(vce); }
+
+int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                       const double* freq, const double* beta, const double* se,
+                       const double* pvalue, const double* log10p, const int32_t* tested,
+                       int stcg_columns) {
+    return guarded([&] {
+        cs::write_assoc_txt(out_path, bim_path, n_snps, n_obs, freq, beta, se, pvalue, log10p,
+                            tested, stcg_columns);
+    });
+}
 
 int cs_profile_enable(int on) {
     return guarded([&] { cs::prof::set_enabled(on != 0); });

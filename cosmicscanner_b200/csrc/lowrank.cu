@@ -58,24 +58,27 @@ namespace {
 
 // ---------------------------------------------------------------- QR
 // Thin QR of Y (n x k row-major) by Cholesky-QR2: two passes of G = Y^T Y, G = R^T R,
-// Y <- Y R^{-1} (a triangular solve on the device); a first pass whose Gram matrix is not
-// numerically positive definite is shifted (shifted Cholesky-QR) and a third pass added.
-// Any orthonormal basis of span(Y) gives the same subspace iteration as the reference's
-// HouseholderQR (lmm_engine.cpp:931-941): Q is unique up to column signs, which cancel
-// in Q^T K Q and in U = Q W.  Y is left unchanged; the result is written to Q.
+// Y <- Y R^{-1}, with the k x k triangular inverse formed on the host and applied as one
+// DGEMM (a device triangular solve of this shape runs several times slower than the GEMM).
+// A first pass whose Gram matrix is not numerically positive definite is shifted (shifted
+// Cholesky-QR) and a third pass added.  Any orthonormal basis of span(Y) gives the same
+// subspace iteration as the reference's HouseholderQR (lmm_engine.cpp:931-941): Q is unique
+// up to column signs, which cancel in Q^T K Q and in U = Q W.  Y is used as scratch; the
+// result is written to Q.
 void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q,
                  DeviceBuffer<double>& d_gram, cudaStream_t s) {
     const double one = 1.0, zero = 0.0;
     d_gram.resize(2 * k * k);
     double* G = d_gram.get();
-    double* Rd = G + k * k;
+    double* Rinv_d = G + k * k;
     std::vector<double> g(k * k), R;
-    CS_CUDA(cudaMemcpyAsync(Q, Y, 8 * n * k, cudaMemcpyDeviceToDevice, s));
     CS_BLAS(cublasSetStream(blas, s));
     int passes = 2;
+    double* src = Y;
+    double* dst = Q;
     for (int pass = 0; pass < passes; ++pass) {
-        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, Q,
-                            (int)k, Q, (int)k, &zero, G, (int)k));
+        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, src,
+                            (int)k, src, (int)k, &zero, G, (int)k));
         CS_CUDA(cudaMemcpyAsync(g.data(), G, 8 * k * k, cudaMemcpyDeviceToHost, s));
         CS_CUDA(cudaStreamSynchronize(s));
         if (!la::cholesky_upper(g, (int)k, R)) {
@@ -88,10 +91,19 @@ void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q
                 fail(CS_ERR_NUMERIC, "QR of the sketch failed (rank-deficient sketch)");
             passes = std::min(passes + 1, 4);
         }
-        CS_CUDA(cudaMemcpyAsync(Rd, R.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
-        // row-major Q = Q R^{-1}  <=>  column-major Q^c = R^{-T} Q^c: solve R^T X = Q^c
-        CS_BLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T,
-                            CUBLAS_DIAG_NON_UNIT, (int)k, (int)n, &one, Rd, (int)k, Q, (int)k));
+        const std::vector<double> Rinv = la::upper_inverse(R, (int)k);
+        CS_CUDA(cudaMemcpyAsync(Rinv_d, Rinv.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
+        // row-major dst = src R^{-1}  <=>  column-major dst^c = R^{-T} src^c
+        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)k, (int)n, (int)k, &one, Rinv_d,
+                            (int)k, src, (int)k, &zero, dst, (int)k));
+        // the last pass must land in Q
+        const bool last = pass + 1 == passes;
+        if (!last) {
+            src = dst;
+            dst = dst == Q ? Y : Q;
+        } else if (dst != Q) {
+            CS_CUDA(cudaMemcpyAsync(Q, dst, 8 * n * k, cudaMemcpyDeviceToDevice, s));
+        }
     }
     CS_CUDA(cudaStreamSynchronize(s));
 }

@@ -1,0 +1,81 @@
+// Association result files, column for column as the reference writes them.
+//
+// `.assoc.txt`: src/gwas_output_schema.h:14-37 (kUnifiedHeader, writeAdditiveRow) through
+// GwasScanner::flushAssocResults (src/gwas_output.cpp:123-183): rows whose P is NaN are
+// skipped; numbers use the stream's default formatting (6 significant digits); the additive
+// row carries NA for the six dominance / joint fields.  CHR, SNP, BP, A1 (.bim column 5) and
+// A2 (.bim column 6) come from the .bim as PlinkReader::readBim parses it
+// (libCosmicCore/src/plink_reader.cpp:52-65); FREQ is the A1 frequency over the analysed
+// samples, N the analysed sample count (src/lmm_engine.cpp:1315-1326).
+// `.stcg.assoc.txt`: src/models/repeatability_scan_stcg.cpp:190-193 header and :138-140 rows
+// (FREQ there is the folded minor-allele frequency, N the subject count).
+#include <cmath>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "cs_internal.h"
+
+namespace cs {
+
+namespace {
+
+struct BimRow {
+    std::string chrom, id, a1, a2;
+    long long bp = 0;
+};
+
+std::vector<BimRow> read_bim(const std::string& path) {
+    std::ifstream ifs(path);
+    if (!ifs) fail(CS_ERR_IO, "Cannot open .bim file: " + path);
+    std::vector<BimRow> rows;
+    std::string line;
+    while (std::getline(ifs, line)) {
+        if (line.empty()) continue;
+        std::stringstream ss(line);
+        BimRow r;
+        double cm = 0.0;
+        ss >> r.chrom >> r.id >> cm >> r.bp >> r.a1 >> r.a2;
+        rows.push_back(std::move(r));
+    }
+    return rows;
+}
+
+}  // namespace
+
+void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                     const double* freq, const double* beta, const double* se, const double* p,
+                     const double* log10p, const int32_t* tested, int stcg_columns) {
+    if (!out_path || !bim_path || n_snps < 0 || !freq || !beta || !se || !p || !log10p)
+        fail(CS_ERR_INVALID_ARGUMENT, "write_assoc_txt: null argument");
+    const std::vector<BimRow> bim = read_bim(bim_path);
+    if ((int64_t)bim.size() != n_snps)
+        fail(CS_ERR_INVALID_ARGUMENT, "write_assoc_txt: .bim has " + std::to_string(bim.size()) +
+                                          " variants, results have " + std::to_string(n_snps));
+    std::ofstream ofs(out_path);
+    if (!ofs) fail(CS_ERR_IO, "Cannot open output file: " + std::string(out_path));
+    if (stcg_columns)
+        ofs << "CHR\tSNP\tBP\tA1\tA2\tFREQ\tN\tBETA\tSE\tP\tLOG10P\n";
+    else
+        ofs << "CHR\tSNP\tBP\tA1\tA2\tFREQ\tN"
+               "\tBETA_A\tSE_A\tP_A\tLOG10P_A"
+               "\tBETA_D\tSE_D\tP_D\tLOG10P_D"
+               "\tP_JOINT\tLOG10P_JOINT\n";
+    for (int64_t j = 0; j < n_snps; ++j) {
+        if (tested && !tested[j]) continue;
+        if (std::isnan(p[j])) continue;
+        const BimRow& b = bim[j];
+        ofs << b.chrom << '\t' << b.id << '\t' << b.bp << '\t' << b.a1 << '\t' << b.a2 << '\t'
+            << freq[j] << '\t' << n_obs << '\t' << beta[j] << '\t' << se[j] << '\t' << p[j]
+            << '\t' << log10p[j];
+        if (stcg_columns)
+            ofs << '\n';
+        else
+            ofs << "\tNA\tNA\tNA\tNA\tNA\tNA\n";
+    }
+    ofs.flush();
+    if (!ofs) fail(CS_ERR_IO, "Error writing output file: " + std::string(out_path));
+}
+
+}  // namespace cs

@@ -200,6 +200,20 @@ int cs_vce_solution(const cs_vce* vce, double* beta, double* a_rows, double* pe_
 int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations);
 void cs_vce_destroy(cs_vce* vce);
 
+/* ---------------------------------------------------------------- result files
+ * Writes association results the way GwasScanner::flushAssocResults writes `.assoc.txt`
+ * (src/gwas_output.cpp:123-183, columns of src/gwas_output_schema.h:14-37): the unified
+ * header, one additive row per SNP with a non-NaN P (and tested[j] != 0 when tested is not
+ * NULL), NA in the six dominance / joint fields, numbers at the stream's default 6
+ * significant digits.  CHR / SNP / BP / A1 / A2 come from bim_path (one line per SNP, in
+ * the order of the result arrays); n_obs fills N.  stcg_columns = 1 writes the
+ * `.stcg.assoc.txt` layout instead (CHR SNP BP A1 A2 FREQ N BETA SE P LOG10P,
+ * src/models/repeatability_scan_stcg.cpp:190-193). */
+int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                       const double* freq, const double* beta, const double* se,
+                       const double* pvalue, const double* log10p, const int32_t* tested,
+                       int stcg_columns);
+
 /* ---------------------------------------------------------------- instrumentation
  * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and
  * PlinkKinshipOperator::BlockProfile (src/kinship_operator.h:55-63): a process-wide count

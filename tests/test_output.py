@@ -1,0 +1,64 @@
+"""`.assoc.txt` writer: the reference's header, row layout and default 6-digit formatting
+(src/gwas_output_schema.h:14-37, src/gwas_output.cpp:123-183).  Host-only: no GPU."""
+import numpy as np
+import pytest
+
+import cosmicscanner_b200 as cs
+
+HEADER = ("CHR\tSNP\tBP\tA1\tA2\tFREQ\tN\tBETA_A\tSE_A\tP_A\tLOG10P_A\tBETA_D\tSE_D\tP_D"
+          "\tLOG10P_D\tP_JOINT\tLOG10P_JOINT")
+
+
+def fmt(x):
+    # std::ostream's default floating-point output: %g with precision 6
+    return "%g" % x
+
+
+def test_assoc_txt_rows_and_formatting(tmp_path):
+    bim = tmp_path / "c.bim"
+    bim.write_text("1\trs1\t0\t1000\tA\tG\n1\trs2\t0\t2000\tC\tT\n\n2\trs3\t0.5\t123456789\tG\tA\n")
+    res = {
+        "freq": np.array([0.123456789, 0.5, 0.0123]),
+        "beta": np.array([1.23456789e-5, -2.0, 3.3]),
+        "se": np.array([0.000123456789, 1.0 / 3.0, 12345678.9]),
+        "p": np.array([1e-300, np.nan, 0.999999999]),
+        "log10p": np.array([300.0, np.nan, 4.34e-10]),
+        "tested": np.array([1, 1, 1], dtype=np.int32),
+    }
+    out = tmp_path / "r.assoc.txt"
+    cs.write_assoc_txt(str(out), str(bim), res, 4321)
+    lines = out.read_text().split("\n")
+    assert lines[0] == HEADER
+    assert lines[-1] == ""
+    rows = lines[1:-1]
+    assert len(rows) == 2  # the NaN-P row is skipped
+    want0 = ["1", "rs1", "1000", "A", "G", fmt(0.123456789), "4321", fmt(1.23456789e-5),
+             fmt(0.000123456789), fmt(1e-300), fmt(300.0)] + ["NA"] * 6
+    assert rows[0].split("\t") == want0
+    f = rows[1].split("\t")
+    assert f[:5] == ["2", "rs3", "123456789", "G", "A"]
+    assert f[7] == fmt(3.3) and f[8] == fmt(12345678.9) == "1.23457e+07"
+    assert f[9] == "1" and f[10] == fmt(4.34e-10)
+
+
+def test_stcg_layout_and_untested_rows(tmp_path):
+    bim = tmp_path / "c.bim"
+    bim.write_text("1 a 0 10 A C\n1 b 0 20 G T\n")
+    res = {k: np.array([0.25, 0.5]) for k in ("freq", "beta", "se", "p", "log10p")}
+    res["tested"] = np.array([0, 1], dtype=np.int32)
+    out = tmp_path / "r.stcg.assoc.txt"
+    cs.write_assoc_txt(str(out), str(bim), res, 10, stcg_columns=True)
+    lines = out.read_text().strip().split("\n")
+    assert lines[0] == "CHR\tSNP\tBP\tA1\tA2\tFREQ\tN\tBETA\tSE\tP\tLOG10P"
+    assert lines[1].split("\t") == ["1", "b", "20", "G", "T", "0.5", "10", "0.5", "0.5", "0.5", "0.5"]
+    assert len(lines) == 2
+
+
+def test_writer_errors(tmp_path):
+    res = {k: np.zeros(1) for k in ("freq", "beta", "se", "p", "log10p")}
+    with pytest.raises(cs.CosmicError):
+        cs.write_assoc_txt(str(tmp_path / "x"), str(tmp_path / "missing.bim"), res, 1)
+    bim = tmp_path / "c.bim"
+    bim.write_text("1 a 0 10 A C\n1 b 0 20 G T\n")
+    with pytest.raises(cs.InvalidArgument):
+        cs.write_assoc_txt(str(tmp_path / "x"), str(bim), res, 1)
