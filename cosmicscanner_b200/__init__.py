@@ -10,6 +10,7 @@ Python mirror of the reference's C++ interfaces over the library's C ABI
                               (src/lmm_engine.h:108-131)
 * :class:`MatrixFreePCG`    — ``MatrixFreePCG`` (libCosmicCore/src/matrix_free_pcg.h:9-75)
 * :class:`StcgVce`          — ``STCG_VCE`` (libCosmicCore/src/stcg_vce.h:7-54)
+* :class:`Server`           — resident-genotype request loop (no reference counterpart)
 
 Every compute call runs the CUDA kernels in ``libcosmicscanner_b200.so``; there is
 no CPU fallback.  A missing library or CUDA device raises immediately.
@@ -421,6 +422,110 @@ def write_assoc_txt(path: str, bim_path: str, results: dict, n_obs: int, stcg_co
                                          _ptr(arr["freq"]), _ptr(arr["beta"]), _ptr(arr["se"]),
                                          _ptr(arr["p"]), _ptr(arr["log10p"]), _ptr(tested),
                                          int(bool(stcg_columns))))
+
+
+# ---------------------------------------------------------------- serving loop
+
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("rank", C.c_int32), ("oversample", C.c_int32), ("trace_threshold", C.c_double),
+        ("min_rank", C.c_int32), ("min_maf", C.c_double), ("precision", C.c_int32),
+        ("max_batch_columns", C.c_int64), ("memory_budget_gb", C.c_double),
+        ("max_active", C.c_int32),
+    ]
+
+
+class ServeRequest(C.Structure):
+    _fields_ = [
+        ("samples", C.c_void_p), ("n_samples", C.c_int64), ("Y", C.c_void_p),
+        ("n_traits", C.c_int32), ("X", C.c_void_p), ("p", C.c_int32),
+        ("snp_begin", C.c_int64), ("snp_end", C.c_int64), ("seed", C.c_uint64),
+    ]
+
+
+class ServeStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("latency_s", C.c_double), ("queue_s", C.c_double),
+                ("effective_rank", C.c_int32)]
+
+
+class ServerStatistics(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+        ("p50_s", C.c_double), ("p99_s", C.c_double), ("mean_s", C.c_double),
+        ("throughput_rps", C.c_double), ("wall_s", C.c_double), ("applies", C.c_int64),
+        ("apply_columns", C.c_int64), ("max_requests_per_apply", C.c_int64),
+        ("max_concurrent", C.c_int64),
+    ]
+
+
+class Server:
+    """Resident-genotype association server with continuous batching of kinship applies
+    across requests (no reference counterpart; each request is the matrix-free LMM job of
+    src/gwas_scanner.cpp on a cohort subset and a SNP window)."""
+
+    def __init__(self, genotypes: Genotypes, variants=None, **options):
+        o = ServerOptions()
+        _abi.lib().cs_server_default_options(C.byref(o))
+        for k, v in options.items():
+            setattr(o, k, _prec(v) if k == "precision" else v)
+        self._g = genotypes
+        var = None if variants is None else np.ascontiguousarray(variants, dtype=np.int32)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_server_create(genotypes._h, _ptr(var),
+                                           0 if var is None else len(var), C.byref(o),
+                                           C.byref(h)))
+        self._h = h
+        self._windows = {}
+
+    def submit(self, samples, Y, X, snp_begin=0, snp_end=None, seed=42) -> int:
+        samples = np.ascontiguousarray(samples, dtype=np.int32)
+        Y = np.asfortranarray(np.asarray(Y, dtype=np.float64).reshape(len(samples), -1))
+        X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(samples), -1))
+        end = self._g.n_snps if snp_end is None else int(snp_end)
+        q = ServeRequest(samples.ctypes.data, len(samples), Y.ctypes.data, Y.shape[1],
+                         X.ctypes.data if X.shape[1] else None, X.shape[1], int(snp_begin), end,
+                         int(seed))
+        rid = C.c_int64()
+        _check(_abi.lib().cs_server_submit(self._h, C.byref(q), C.byref(rid)))
+        self._windows[rid.value] = (end - int(snp_begin), Y.shape[1])
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> dict:
+        st = ServeStatus()
+        _check(_abi.lib().cs_server_wait(self._h, rid, float(timeout), C.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def result(self, rid: int, trait: int = 0) -> dict:
+        w, _ = self._windows[rid]
+        out = {k: np.zeros(w) for k in ("beta", "se", "p", "log10p", "freq")}
+        tested = np.zeros(w, dtype=np.int32)
+        s2 = np.zeros(2)
+        _check(_abi.lib().cs_server_result(self._h, rid, trait, _ptr(s2), _ptr(out["beta"]),
+                                           _ptr(out["se"]), _ptr(out["p"]), _ptr(out["log10p"]),
+                                           _ptr(out["freq"]), _ptr(tested)))
+        out["tested"] = tested.astype(bool)
+        out["sigma2_g"], out["sigma2_e"] = float(s2[0]), float(s2[1])
+        return out
+
+    def release(self, rid: int):
+        _check(_abi.lib().cs_server_release(self._h, rid))
+        self._windows.pop(rid, None)
+
+    def stats(self) -> dict:
+        st = ServerStatistics()
+        _check(_abi.lib().cs_server_stats(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in st._fields_}
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:

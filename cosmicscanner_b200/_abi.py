@@ -53,6 +53,14 @@ _SIGNATURES = {
     "cs_vce_solution": ([_P, _P, _P, _P], _I),
     "cs_vce_history": ([_P, _P, _P], _I),
     "cs_vce_destroy": ([_P], None),
+    "cs_server_default_options": ([_P], None),
+    "cs_server_create": ([_P, _P, _I64, _P, _P], _I),
+    "cs_server_submit": ([_P, _P, _P], _I),
+    "cs_server_wait": ([_P, _I64, _D, _P], _I),
+    "cs_server_result": ([_P, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _P], _I),
+    "cs_server_release": ([_P, _I64], _I),
+    "cs_server_stats": ([_P, _P], _I),
+    "cs_server_destroy": ([_P], None),
     "cs_write_assoc_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _I], _I),
     "cs_profile_enable": ([_I], _I),
     "cs_profile_summary": ([C.c_char_p, C.c_size_t, _P], _I),

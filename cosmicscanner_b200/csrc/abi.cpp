@@ -38,6 +38,16 @@ void vce_history(const cs_vce* v, double* out, int64_t* n_iter);
 void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, const double* B,
                       int64_t ldb, int64_t k, double* X, int64_t ldx, double tol, int relative,
                       int max_iter, int precision, int32_t* iterations, cudaStream_t s);
+void server_default_options(cs_server_options* o);
+cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_var,
+                         const cs_server_options* opt);
+int64_t server_submit(cs_server* sv, const cs_serve_request* q);
+void server_wait(cs_server* sv, int64_t id, double timeout_s, cs_serve_status* out);
+void server_result(cs_server* sv, int64_t id, int32_t trait, double* sigma2, double* beta,
+                   double* se, double* pval, double* log10p, double* freq, int32_t* tested);
+void server_release(cs_server* sv, int64_t id);
+void server_stats(cs_server* sv, cs_server_statistics* out);
+void server_destroy(cs_server* sv);
 void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                      const double* freq, const double* beta, const double* se, const double* p,
                      const double* log10p, const int32_t* tested, int stcg_columns);
@@ -275,6 +285,56 @@ int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations) {
 }
 
 void cs_vce_destroy(cs_vce* vce) { cs::vce_destroy(vce); }
+
+void cs_server_default_options(cs_server_options* opt) {
+    if (opt) cs::server_default_options(opt);
+}
+
+int cs_server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
+                     const cs_server_options* opt, cs_server** out) {
+    return guarded([&] {
+        require(out != nullptr, "null output handle");
+        *out = cs::server_create(g, variants, n_variants, opt);
+    });
+}
+
+int cs_server_submit(cs_server* server, const cs_serve_request* request, int64_t* id) {
+    return guarded([&] {
+        require(server != nullptr && id != nullptr, "null argument");
+        *id = cs::server_submit(server, request);
+    });
+}
+
+int cs_server_wait(cs_server* server, int64_t id, double timeout_s, cs_serve_status* status) {
+    return guarded([&] {
+        require(server != nullptr, "null server handle");
+        cs::server_wait(server, id, timeout_s, status);
+    });
+}
+
+int cs_server_result(cs_server* server, int64_t id, int32_t trait, double* sigma2, double* beta,
+                     double* se, double* pvalue, double* log10p, double* freq, int32_t* tested) {
+    return guarded([&] {
+        require(server != nullptr, "null server handle");
+        cs::server_result(server, id, trait, sigma2, beta, se, pvalue, log10p, freq, tested);
+    });
+}
+
+int cs_server_release(cs_server* server, int64_t id) {
+    return guarded([&] {
+        require(server != nullptr, "null server handle");
+        cs::server_release(server, id);
+    });
+}
+
+int cs_server_stats(cs_server* server, cs_server_statistics* stats) {
+    return guarded([&] {
+        require(server != nullptr && stats != nullptr, "null argument");
+        cs::server_stats(server, stats);
+    });
+}
+
+void cs_server_destroy(cs_server* server) { cs::server_destroy(server); }
 
 int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                        const double* freq, const double* beta, const double* se,

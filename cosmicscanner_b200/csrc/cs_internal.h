@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -44,6 +45,9 @@ constexpr int64_t kRowAlign = 64;
 // block (the same guarantee cudaFree gives).
 void* device_alloc(size_t bytes);
 void device_free(void* p) noexcept;
+// For threads that synchronise their own streams before any buffer is released (the request
+// workers of the serving loop): frees then skip the device-wide synchronisation.
+void set_thread_owns_its_streams(bool on);
 
 // Device allocation that frees itself.
 template <typename T>
@@ -179,6 +183,29 @@ void rowmajor_to_colmajor(const double* src, int64_t kp, int64_t n, int64_t k, d
                           int64_t ld, cudaStream_t s);
 
 int num_sms();
+
+// The low-rank engine's view of the kinship operator: its row count, trace and an apply
+// Y = K X on row-major device blocks (lowrank.cu).
+struct LowRankTarget {
+    int64_t rows = 0;
+    double trace = 0.0;
+    std::function<void(const double* X, int64_t ldx, int64_t k, double* Y, int64_t ldy,
+                       cudaStream_t s)>
+        apply;
+};
+cs_lmm* lmm_create();
+void lmm_destroy(cs_lmm* l);
+void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const double* y,
+                                const double* X, int64_t p, int rank, int oversample,
+                                int64_t seed, double trace_threshold, int min_rank,
+                                cs_lowrank_diagnostics* diag, cudaStream_t s);
+void lmm_fit_reml(cs_lmm* l, const double* y, const double* X, int64_t p,
+                  cs_lowrank_diagnostics* diag, cudaStream_t s);
+// Scan of SNPs [snp_begin, snp_end) of g; per-SNP outputs have snp_end - snp_begin entries.
+void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                     int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
+                     double* beta, double* se, double* pvalue, double* log10p, double* freq,
+                     int32_t* tested, cudaStream_t s);
 
 namespace prof {
 // Counts one kernel launch; with profiling enabled, times it with events on stream s.

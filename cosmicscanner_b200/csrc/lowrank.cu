@@ -26,6 +26,8 @@
 struct cs_lmm {
     int64_t n = 0, p = 0, rank = 0;
     bool prepared = false;
+    bool sketched = false;
+    cs_lowrank_diagnostics sketch_diag{};
     std::vector<double> lambda;
     double r0 = 0.0, sigma2_g = 0.0, sigma2_e = 0.0, delta = 0.0;
     std::vector<double> y, X;  // host, X column-major n x p
@@ -38,6 +40,7 @@ struct cs_lmm {
     // scan: analysed-sample view of the genotypes and its tensor-core context, cached
     // for repeated scans of the same (genotypes, keep) pair
     uint64_t scan_g_uid = 0;
+    int64_t scan_begin = -1, scan_end = -1;
     std::vector<int32_t> scan_keep;
     cs::DeviceBuffer<uint8_t> scan_own;
     cs_packed_view scan_view;
@@ -346,15 +349,29 @@ void lmm_destroy(cs_lmm* l) {
 void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const double* X, int64_t p,
                          int rank, int oversample, int64_t seed, double trace_threshold,
                          int min_rank, int precision, cs_lowrank_diagnostics* diag) {
+    LowRankTarget t;
+    t.rows = op->rows;
+    t.trace = op->trace;
+    t.apply = [op, precision](const double* X_, int64_t ldx, int64_t k, double* Y_, int64_t ldy,
+                              cudaStream_t st) {
+        kinship_apply_rowmajor(op, X_, ldx, k, Y_, ldy, precision, st);
+    };
+    lmm_prepare_lowrank_target(l, t, y, X, p, rank, oversample, seed, trace_threshold, min_rank,
+                               diag, 0);
+}
+
+void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const double* y,
+                                const double* X, int64_t p, int rank, int oversample,
+                                int64_t seed, double trace_threshold, int min_rank,
+                                cs_lowrank_diagnostics* diag, cudaStream_t s) {
     const auto start = std::chrono::steady_clock::now();
     l->blas = shared_blas();  // the calling thread's handle
-    const int64_t n = op->rows;
+    const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
              "Low-rank LMM requires valid dimensions and 0 < rank < sample count");
     if (p > 16) fail(CS_ERR_UNSUPPORTED, "at most 16 covariate columns are supported");
     const int64_t sk = std::min<int64_t>(n, rank + std::max(0, oversample));
-    cudaStream_t s = 0;
     CS_BLAS(cublasSetStream(l->blas, s));
     DeviceBuffer<double>&omega = l->omega, &sample = l->sample, &q = l->q, &scratch = l->scratch,
                          &gram = l->gram, &small = l->small;
@@ -367,13 +384,13 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     }
     {
         prof::HostScope hs("lowrank_subspace_iteration");
-        kinship_apply_rowmajor(op, omega.get(), sk, sk, sample.get(), sk, precision, s);
+        target.apply(omega.get(), sk, sk, sample.get(), sk, s);
         for (int it = 0; it < 2; ++it) {
             cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
-            kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
+            target.apply(q.get(), sk, sk, sample.get(), sk, s);
         }
         cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
-        kinship_apply_rowmajor(op, q.get(), sk, sk, sample.get(), sk, precision, s);
+        target.apply(q.get(), sk, sk, sample.get(), sk, s);
         CS_CUDA(cudaStreamSynchronize(s));
     }
     std::optional<prof::HostScope> hs_stage;
@@ -391,7 +408,7 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     std::vector<double> lead(rank);
     for (int j = 0; j < rank; ++j) lead[j] = std::max(0.0, evals[sk - 1 - j]);
     // trace-fraction rank selection (lmm_engine.cpp:958-973)
-    const double total_trace = op->trace;
+    const double total_trace = target.trace;
     int selected = rank;
     bool met = trace_threshold <= 0.0;
     if (trace_threshold > 0.0 && total_trace > 0.0) {
@@ -418,7 +435,6 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_T, CUBLAS_OP_N, selected, (int)n, (int)sk, &one,
                         gram.get(), (int)sk, q.get(), (int)sk, &zero, l->d_U.get(), selected));
     l->n = n;
-    l->p = p;
     l->rank = selected;
     l->lambda.assign(lead.begin(), lead.begin() + selected);
     double lam_sum = 0.0, lam_sq = 0.0;
@@ -432,6 +448,36 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     for (double v : l->lambda) cross += (v - l->r0) * v;
     const double resid_sq = std::max(0.0, total_trace * total_trace + approx_sq - 2.0 * cross);
     const double rel_err = std::sqrt(resid_sq) / std::max(total_trace, std::numeric_limits<double>::min());
+    l->n = n;
+    l->sketch_diag = cs_lowrank_diagnostics{};
+    l->sketch_diag.requested_rank = rank;
+    l->sketch_diag.effective_rank = selected;
+    l->sketch_diag.sketch_size = (int32_t)sk;
+    l->sketch_diag.trace_threshold_met = met;
+    l->sketch_diag.residual_eigenvalue = l->r0;
+    l->sketch_diag.relative_frobenius_error = rel_err;
+    l->sketch_diag.trace = total_trace;
+    l->sketch_diag.trace_fraction = total_trace > 0.0 ? lam_sum / total_trace : 0.0;
+    l->sketched = true;
+    hs_stage.reset();
+    lmm_fit_reml(l, y, X, p, diag, s);
+    if (diag)
+        diag->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+}
+
+// REML of one trait in the basis of the last sketch (lmm_engine.cpp:1010-1073).
+void lmm_fit_reml(cs_lmm* l, const double* y, const double* X, int64_t p,
+                  cs_lowrank_diagnostics* diag, cudaStream_t s) {
+    const auto start = std::chrono::steady_clock::now();
+    prof::HostScope hs("lowrank_reml");
+    if (!l->sketched) fail(CS_ERR_INVALID_ARGUMENT, "low-rank basis not computed");
+    if (p < 0 || (p > 0 && X == nullptr) || y == nullptr)
+        fail(CS_ERR_INVALID_ARGUMENT, "Low-rank LMM requires valid dimensions");
+    if (p > 16) fail(CS_ERR_UNSUPPORTED, "at most 16 covariate columns are supported");
+    l->blas = shared_blas();
+    const int64_t n = l->n;
+    const int selected = l->rank;
+    l->p = p;
     // REML in the basis
     l->y.assign(y, y + n);
     l->X.assign(X, X + n * p);
@@ -466,14 +512,7 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     l->sigma2_g = std::exp(ble) * l->sigma2_e;
     l->prepared = true;
     if (diag) {
-        diag->requested_rank = rank;
-        diag->effective_rank = selected;
-        diag->sketch_size = (int32_t)sk;
-        diag->trace_threshold_met = met;
-        diag->residual_eigenvalue = l->r0;
-        diag->relative_frobenius_error = rel_err;
-        diag->trace = total_trace;
-        diag->trace_fraction = total_trace > 0.0 ? lam_sum / total_trace : 0.0;
+        *diag = l->sketch_diag;
         diag->sigma2_g = l->sigma2_g;
         diag->sigma2_e = l->sigma2_e;
         diag->delta = l->delta;
@@ -498,17 +537,26 @@ void lmm_lowrank_basis(const cs_lmm* l, double* U, int64_t ldu, double* lambda) 
 void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
               double min_maf, int precision, double* beta, double* se, double* pvalue,
               double* log10p, double* freq, int32_t* tested) {
+    lmm_scan_window(l, g, keep, n_keep, 0, g ? g->n_snps : 0, min_maf, precision, beta, se,
+                    pvalue, log10p, freq, tested, 0);
+}
+
+void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                     int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
+                     double* beta, double* se, double* pvalue, double* log10p, double* freq,
+                     int32_t* tested, cudaStream_t s) {
     l->blas = shared_blas();  // the calling thread's handle
     if (!l->prepared) fail(CS_ERR_INVALID_ARGUMENT, "low-rank model not prepared");
     if (precision != CS_PRECISION_FP64 && precision != CS_PRECISION_MIXED)
         fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
-    const int64_t n = l->n, p = l->p, r = l->rank, M = g->n_snps;
+    if (snp_begin < 0 || snp_end > g->n_snps || snp_begin > snp_end)
+        fail(CS_ERR_INVALID_ARGUMENT, "scan: SNP window out of range");
+    const int64_t n = l->n, p = l->p, r = l->rank, M = snp_end - snp_begin;
     if (keep == nullptr || n_keep != n)
         fail(CS_ERR_INVALID_ARGUMENT, "Sample size mismatch in scan");
     for (int64_t i = 0; i < n_keep; ++i)
         if (keep[i] < 0 || keep[i] >= g->n_samples)
             fail(CS_ERR_INVALID_ARGUMENT, "scan: sample index out of range");
-    cudaStream_t s = 0;
     CS_BLAS(cublasSetStream(l->blas, s));
     // ---- null quantities (lmm_engine.cpp:1273-1287) in the basis
     const double base = 1.0 / std::max(1e-12, l->sigma2_g * l->r0 + l->sigma2_e);
@@ -580,20 +628,22 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
     // ---- packed view of the analysed samples over every SNP (cached per genotypes + keep)
     prof::HostScope hs_scan("scan_host_setup");
     const bool cached = l->scan_g_uid == g->uid && (int64_t)l->scan_keep.size() == n_keep &&
+                        l->scan_begin == snp_begin && l->scan_end == snp_end &&
                         std::memcmp(l->scan_keep.data(), keep, 4 * n_keep) == 0;
     if (!cached) {
         mixed_scan_destroy(l->scan_mixed);
         l->scan_mixed = nullptr;
         bool identity = n_keep == g->n_samples;
         for (int64_t i = 0; identity && i < n_keep; ++i) identity = keep[i] == i;
-        l->scan_view = cs_packed_view{g->packed.get(), M, g->n_samples, g->stride};
+        const uint8_t* first_row = g->packed.get() + snp_begin * g->stride;
+        l->scan_view = cs_packed_view{first_row, M, g->n_samples, g->stride};
         if (!identity) {
             const int64_t stride = round_up((n + 3) / 4, kRowAlign);
             l->scan_own.resize(std::max<int64_t>(1, M * stride));
             DeviceBuffer<int32_t> d_keep;
             d_keep.resize(n);
             CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, 4 * n, cudaMemcpyHostToDevice, s));
-            repack(g->packed.get(), g->stride, nullptr, M, d_keep.get(), n, l->scan_own.get(),
+            repack(first_row, g->stride, nullptr, M, d_keep.get(), n, l->scan_own.get(),
                    stride, s);
             CS_CUDA(cudaStreamSynchronize(s));
             l->scan_view = cs_packed_view{l->scan_own.get(), M, n, stride};
@@ -607,6 +657,8 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
             CS_CUDA(cudaStreamSynchronize(s));
         }
         l->scan_g_uid = g->uid;
+        l->scan_begin = snp_begin;
+        l->scan_end = snp_end;
         l->scan_keep.assign(keep, keep + n_keep);
     }
     const cs_packed_view& v = l->scan_view;

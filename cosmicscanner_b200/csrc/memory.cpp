@@ -45,9 +45,17 @@ cublasHandle_t shared_blas() {
     return handles[dev];
 }
 
+namespace {
+thread_local bool g_free_without_device_sync = false;
+}
+
+void set_thread_owns_its_streams(bool on) { g_free_without_device_sync = on; }
+
 void device_free(void* p) noexcept {
     if (!p) return;
-    cudaDeviceSynchronize();
+    // A thread that synchronises its own (non-blocking) streams before releasing buffers
+    // frees without stalling the other threads' work on the device.
+    if (!g_free_without_device_sync) cudaDeviceSynchronize();
     cudaFreeAsync(p, 0);
 }
 

@@ -200,6 +200,73 @@ int cs_vce_solution(const cs_vce* vce, double* beta, double* a_rows, double* pe_
 int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations);
 void cs_vce_destroy(cs_vce* vce);
 
+/* ---------------------------------------------------------------- serving loop
+ * No reference counterpart (the reference runs one job per process).  A server keeps the
+ * packed genotypes resident and answers requests, each the matrix-free LMM job of
+ * cs_lmm_prepare_lowrank_matrix_free + cs_lmm_scan on a cohort subset: low-rank sketch of the
+ * subset's kinship, REML per trait, scan of a SNP window.  Kinship applies of all running
+ * requests are stacked into one multi-right-hand-side apply whenever the GPU is free
+ * (continuous batching; requests of different subset sizes share an apply through the full
+ * sample space); requests are admitted FIFO as worker slots and the memory budget allow. */
+typedef struct cs_server_options {
+    int32_t rank;              /* low-rank basis size (--fastlmm-max-rank, 256) */
+    int32_t oversample;        /* sketch oversampling (10) */
+    double trace_threshold;    /* trace fraction for rank selection (0.95) */
+    int32_t min_rank;          /* (1) */
+    double min_maf;            /* scan MAF filter (0.01) */
+    int32_t precision;         /* kinship applies and scan projection (CS_PRECISION_MIXED) */
+    int64_t max_batch_columns; /* right-hand sides per stacked apply (4096) */
+    double memory_budget_gb;   /* admission budget for request working sets (64) */
+    int32_t max_active;        /* requests running at once (8) */
+} cs_server_options;
+
+typedef struct cs_serve_request {
+    const int32_t* samples;  /* operator rows of the cohort subset (distinct), in y's order */
+    int64_t n_samples;
+    const double* Y;         /* n_samples x n_traits, column-major (host, copied) */
+    int32_t n_traits;
+    const double* X;         /* n_samples x p covariates, column-major (host, copied) */
+    int32_t p;
+    int64_t snp_begin, snp_end; /* scan window [begin, end) */
+    uint64_t seed;           /* sketch seed (42) */
+} cs_serve_request;
+
+typedef struct cs_serve_status {
+    int32_t state;           /* 0 queued, 1 running, 2 done, -1 failed */
+    double latency_s;        /* submit -> done (-1 while not done) */
+    double queue_s;          /* submit -> admitted (-1 while queued) */
+    int32_t effective_rank;
+} cs_serve_status;
+
+typedef struct cs_server_statistics {
+    int64_t submitted, completed, failed;
+    double p50_s, p99_s, mean_s;   /* latency of completed requests */
+    double throughput_rps, wall_s; /* completed / (last completion - first submit) */
+    int64_t applies, apply_columns;
+    int64_t max_requests_per_apply, max_concurrent;
+} cs_server_statistics;
+
+typedef struct cs_server cs_server;
+
+void cs_server_default_options(cs_server_options* opt);
+/* variants: the GRM variant selection (as for cs_kinship_create over all samples). */
+int cs_server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
+                     const cs_server_options* opt, cs_server** out);
+/* Copies the request's inputs and returns at once with its id. */
+int cs_server_submit(cs_server* server, const cs_serve_request* request, int64_t* id);
+/* Waits for a request (timeout_s < 0: without limit); a failed request returns CS_ERR_CUDA
+ * with its message. */
+int cs_server_wait(cs_server* server, int64_t id, double timeout_s, cs_serve_status* status);
+/* One trait's results: sigma2 = (sigma2_g, sigma2_e); per-SNP arrays of the window length
+ * (NaN where tested = 0, as cs_lmm_scan).  Any output may be NULL. */
+int cs_server_result(cs_server* server, int64_t id, int32_t trait, double* sigma2, double* beta,
+                     double* se, double* pvalue, double* log10p, double* freq, int32_t* tested);
+/* Drops a finished request's results. */
+int cs_server_release(cs_server* server, int64_t id);
+int cs_server_stats(cs_server* server, cs_server_statistics* stats);
+/* Finishes running requests, drops queued ones, frees the server. */
+void cs_server_destroy(cs_server* server);
+
 /* ---------------------------------------------------------------- result files
  * Writes association results the way GwasScanner::flushAssocResults writes `.assoc.txt`
  * (src/gwas_output.cpp:123-183, columns of src/gwas_output_schema.h:14-37): the unified
