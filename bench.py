@@ -49,6 +49,10 @@ def parse():
     ap.add_argument("--apply-only", action="store_true",
                     help="time kinship applies alone (the profiling case), not the REML+scan job")
     ap.add_argument("--k", type=int, default=68, help="right-hand sides for --apply-only")
+    ap.add_argument("--serve-requests", type=int, default=32,
+                    help="requests in the serving stream measured after the job (0 skips)")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="skip the one-step timing of the plain FP64 GPU form")
     return ap.parse_args()
 
 
@@ -216,6 +220,62 @@ def run_apply_only(args):
     return 0
 
 
+def run_serve(cs, g, variants, d, args):
+    """A Poisson stream of association requests against the resident genotypes: subsets of
+    log-uniform size 5,000..N, 1..16 traits, an intercept and 2..5 N(0,1) covariates, full
+    low-rank REML on all SNPs and a scan of a random contiguous window of M/2 SNPs (the
+    serving configuration's shapes, scaled to the resident matrix).  Arrivals at 80 % of the
+    single-request service rate.  Returns the server's latency / throughput statistics."""
+    n, m = d["n"], d["m"]
+    rng = np.random.default_rng(20261208)
+    base = (d["y"] - d["y"].mean()) / d["y"].std()
+    window = max(1, m // 2)
+
+    def request():
+        n_sub = int(np.exp(rng.uniform(np.log(min(5000, n // 2)), np.log(n))))
+        S = np.sort(rng.choice(n, n_sub, replace=False)).astype(np.int32)
+        t = int(rng.integers(1, 17))
+        h2 = rng.uniform(0.1, 0.7, size=t)
+        Y = np.column_stack([np.sqrt(h2[j]) * base[S] + np.sqrt(1 - h2[j]) *
+                             rng.standard_normal(n_sub) for j in range(t)])
+        p = int(rng.integers(2, 6))
+        X = np.column_stack([np.ones(n_sub)] + [rng.standard_normal(n_sub) for _ in range(p)])
+        b = int(rng.integers(0, m - window + 1))
+        return S, Y, X.astype(np.float32).astype(np.float64), b, b + window
+
+    reqs = [request() for _ in range(args.serve_requests)]
+    # service time of one request alone (calibrates the arrival rate)
+    cal = cs.Server(g, variants, precision=args.precision, max_active=8)
+    rid = cal.submit(*reqs[0])
+    single = cal.wait(rid)["latency_s"]
+    cal.close()
+    rate = 0.8 / single
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    srv = cs.Server(g, variants, precision=args.precision, max_active=8)
+    t0 = time.perf_counter()
+    ids = []
+    for (S, Y, X, b, e), at in zip(reqs, arrivals):
+        delay = at - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(S, Y, X, b, e))
+    for rid in ids:
+        srv.wait(rid)
+    st = srv.stats()
+    srv.close()
+    return {
+        "requests": len(reqs), "req_per_s": st["throughput_rps"],
+        "p50_ms": st["p50_s"] * 1e3, "p99_ms": st["p99_s"] * 1e3, "mean_ms": st["mean_s"] * 1e3,
+        "single_request_ms": single * 1e3, "arrival_rate_per_s": rate,
+        "applies": st["applies"], "mean_columns_per_apply": st["apply_columns"] / max(1, st["applies"]),
+        "max_requests_per_apply": st["max_requests_per_apply"],
+        "max_concurrent": st["max_concurrent"], "failed": st["failed"],
+        "config": f"resident N={n} M={m}; subsets log-U[5000,{n}], traits U{{1..16}}, "
+                  f"intercept + U{{2..5}} N(0,1) covariates, window {window} SNPs, "
+                  f"Poisson arrivals at 80% of the single-request rate, {args.precision}",
+    }
+
+
 def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
     """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
     (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
@@ -366,6 +426,19 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # ---- the plain FP64 GPU form of the same job, one step (the north-star comparison)
+    fp64_s = None
+    if not args.no_fp64_compare and args.precision != "fp64":
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        eng.prepareLowRankMatrixFree(y, X, op, rank=RANK, oversample=OVERSAMPLE, precision="fp64")
+        eng.scan(g, keep, min_maf=0.01, precision="fp64")
+        a1.record()
+        torch.cuda.synchronize()
+        fp64_s = a0.elapsed_time(a1) / 1e3
+    serve = run_serve(cs, g, variants, d, args) if args.serve_requests > 0 and world == 1 else None
+
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         kernels = [k for k in prof["kernels"]]
@@ -429,6 +502,11 @@ def main():
             "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "pinned_host": bool(pinned),
                     "ms_each": e2e_ms, "host_stages": e2e_prof.get("host", [])},
+            "fp64_gpu": None if fp64_s is None else {
+                "value": fp64_s, "unit": "s",
+                "speedup_mixed_over_fp64": fp64_s / sec_per_step,
+                "note": "the same REML+scan step with FP64 kinship applies and scan projection"},
+            "serve": serve,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,

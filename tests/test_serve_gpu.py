@@ -2,7 +2,8 @@
 
 Each request is the matrix-free LMM job on its subset (low-rank sketch of the subset's
 kinship, REML per trait, scan of a SNP window).  Checks: one request against the CPU oracle
-of the same job (src/lmm_engine.cpp:897-1361 restated); every request of a concurrent mix
+of the same job (src/lmm_engine.cpp:897-1361 restated; variance components 1e-5 relative, BETA 1e-5, -log10 P
+1e-4); every request of a concurrent mix
 against the same request run alone (the stacked applies keep columns independent, so the
 results agree to FP64 rounding: 1e-9); the batcher really stacked requests; bad requests
 fail before any work.
@@ -52,8 +53,8 @@ def test_request_matches_oracle(data):
     for t in range(2):
         U, lam, res = ref.lowrank_prepare(Y[:, t], X, 40, keep=S, variants=variants, n_threads=8)
         out = srv.result(rid, t)
-        assert abs(out["sigma2_g"] - res.sigma2_g) <= 1e-6 * res.sigma2_g
-        assert abs(out["sigma2_e"] - res.sigma2_e) <= 1e-6 * res.sigma2_e
+        assert abs(out["sigma2_g"] - res.sigma2_g) <= 1e-5 * res.sigma2_g
+        assert abs(out["sigma2_e"] - res.sigma2_e) <= 1e-5 * res.sigma2_e
         o = wbed.scan_lowrank(S, U, lam, res.residual_eigenvalue, res.sigma2_g, res.sigma2_e,
                               Y[:, t], X)
         assert np.array_equal(out["tested"], o["tested"])
