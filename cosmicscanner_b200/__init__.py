@@ -265,6 +265,21 @@ class LmmEngine:
         out["tested"] = tested.astype(bool)
         return out
 
+    def scan_window(self, reader: Genotypes, keep_indices, snp_begin: int, snp_end: int,
+                    min_maf=0.01, precision="fp64"):
+        """scan() over SNPs [snp_begin, snp_end) only (a LOCO chromosome)."""
+        keep = np.ascontiguousarray(keep_indices, dtype=np.int32)
+        w = int(snp_end) - int(snp_begin)
+        out = {k: np.zeros(max(w, 0)) for k in ("beta", "se", "p", "log10p", "freq")}
+        tested = np.zeros(max(w, 0), dtype=np.int32)
+        _check(_abi.lib().cs_lmm_scan_window(self._h, reader._h, _ptr(keep), len(keep),
+                                             int(snp_begin), int(snp_end), min_maf,
+                                             _prec(precision), _ptr(out["beta"]), _ptr(out["se"]),
+                                             _ptr(out["p"]), _ptr(out["log10p"]),
+                                             _ptr(out["freq"]), _ptr(tested)))
+        out["tested"] = tested.astype(bool)
+        return out
+
     def close(self):
         if self._h:
             _abi.lib().cs_lmm_destroy(self._h)
@@ -537,19 +552,74 @@ def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     return np.nonzero(ok)[0].astype(np.int32)
 
 
+def read_bim(path: str) -> dict:
+    """A .bim file as PlinkReader::readBim parses it (libCosmicCore/src/plink_reader.cpp:52-65):
+    chrom, id, cm, bp, A1 (column 5), A2 (column 6) per non-empty line."""
+    cols = {k: [] for k in ("chrom", "id", "cm", "bp", "a1", "a2")}
+    with open(path) as f:
+        for line in f:
+            if not line.strip():
+                continue
+            t = line.split()
+            cols["chrom"].append(t[0])
+            cols["id"].append(t[1])
+            cols["cm"].append(float(t[2]))
+            cols["bp"].append(int(t[3]))
+            cols["a1"].append(t[4])
+            cols["a2"].append(t[5])
+    cols["chrom"] = np.asarray(cols["chrom"], dtype=object)
+    cols["bp"] = np.asarray(cols["bp"], dtype=np.int64)
+    return cols
+
+
+def _stoi(text: str):
+    """std::stoi: optional sign and leading digits after whitespace; None when it throws."""
+    t = text.lstrip()
+    i = 1 if t[:1] in "+-" else 0
+    j = i
+    while j < len(t) and t[j].isdigit():
+        j += 1
+    return int(t[:j]) if j > i else None
+
+
+def sort_chrom_labels(labels) -> list:
+    """The LOCO chromosome order of src/gwas_scanner.cpp:62-72: numeric labels compare as
+    integers (std::stoi), anything else as strings, over the distinct labels."""
+    import functools
+
+    def before(a, b):
+        ia, ib = _stoi(a), _stoi(b)
+        if ia is not None and ib is not None:
+            return -1 if ia < ib else (1 if ib < ia else 0)
+        return -1 if a < b else (1 if b < a else 0)
+
+    return sorted(set(str(x) for x in labels), key=functools.cmp_to_key(before))
+
+
 def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=256,
                         oversample=10, seed=42, trace_threshold=0.95, min_rank=1,
-                        min_maf=0.01, precision="fp64", genotypes: Genotypes | None = None):
+                        min_maf=0.01, precision="fp64", genotypes: Genotypes | None = None,
+                        chrom=None, loco=True):
     """The `gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback --no-loco`
     path (src/gwas_scanner.cpp:121-129, 254-346, 447) from host buffers: upload + stats,
-    GRM variant selection, operator, low-rank REML null model, scan of every SNP.
-    Returns (results dict, diagnostics dict)."""
+    GRM variant selection, operator, low-rank REML null model, scan of every SNP.  With
+    per-SNP chromosome labels spanning more than one chromosome (and loco=True) it runs the
+    reference's default leave-one-chromosome-out loop (src/gwas_scanner.cpp:299-314,
+    464-472): per chromosome, an operator without that chromosome's GRM variants, its own
+    null model, and the scan of that chromosome's SNPs.  Returns (results dict, diagnostics
+    dict; per chromosome under LOCO)."""
     g = genotypes if genotypes is not None else Genotypes.from_bed_bytes(bed, n_samples, n_snps)
     keep_arr = np.arange(n_samples, dtype=np.int32) if keep is None else np.asarray(keep, np.int32)
     variants = grm_variant_selection(g.stats(), min_maf)
     if len(variants) == 0:
         raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
                               "Matrix-free GRM selection produced no variants")
+    if chrom is not None and loco and len(set(str(c) for c in chrom)) > 1:
+        res, diag = _run_loco(g, keep, keep_arr, variants, np.asarray(chrom).astype(str), y, X,
+                              rank, oversample, seed, trace_threshold, min_rank, min_maf, precision)
+        if genotypes is None:
+            g.close()
+        return res, diag
     op = KinshipOperator(g, None if keep is None else keep_arr, variants)
     rank_eff = max(1, min(rank, op.rows() - 1))
     eng = LmmEngine()
@@ -562,3 +632,35 @@ def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=
     if genotypes is None:
         g.close()
     return res, diag
+
+
+def _run_loco(g, keep, keep_arr, variants, chrom, y, X, rank, oversample, seed,
+              trace_threshold, min_rank, min_maf, precision):
+    m = g.n_snps
+    out = {k: np.full(m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
+    out["tested"] = np.zeros(m, dtype=bool)
+    diags = {}
+    var_chrom = chrom[variants]
+    for c in sort_chrom_labels(chrom):
+        loco_variants = variants[var_chrom != c]
+        if len(loco_variants) == 0:
+            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
+                                  "Matrix-free LOCO left no GRM variants for chromosome " + c)
+        op = KinshipOperator(g, None if keep is None else keep_arr, loco_variants)
+        eng = LmmEngine()
+        rank_eff = max(1, min(rank, op.rows() - 1))
+        diags[c] = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
+                                                seed=seed, trace_threshold=trace_threshold,
+                                                min_rank=min_rank, precision=precision)
+        idx = np.flatnonzero(chrom == c)
+        # the chromosome's SNPs as contiguous runs of the .bim order
+        breaks = np.flatnonzero(np.diff(idx) != 1)
+        starts = np.r_[idx[0], idx[breaks + 1]]
+        ends = np.r_[idx[breaks] + 1, idx[-1] + 1]
+        for b, e in zip(starts, ends):
+            r = eng.scan_window(g, keep_arr, int(b), int(e), min_maf=min_maf, precision=precision)
+            for k in ("beta", "se", "p", "log10p", "freq", "tested"):
+                out[k][b:e] = r[k]
+        op.close()
+        eng.close()
+    return out, diags

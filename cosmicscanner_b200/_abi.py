@@ -44,6 +44,7 @@ _SIGNATURES = {
         [_P, _P, _P, _P, _I64, _I, _I, _I64, _D, _I, _I, _P], _I),
     "cs_lmm_lowrank_basis": ([_P, _P, _I64, _P], _I),
     "cs_lmm_scan": ([_P, _P, _P, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
+    "cs_lmm_scan_window": ([_P, _P, _P, _I64, _I64, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_lmm_destroy": ([_P], None),
     "cs_normal_matrix": ([C.c_uint64, _I64, _I64, _P], _I),
     "cs_pcg_solve": ([_P, _D, _D, _D, _P, _I64, _I64, _P, _I64, _D, _I, _I, _I, _P, _P], _I),

@@ -222,6 +222,17 @@ int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t
     });
 }
 
+int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                       int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
+                       double* beta, double* se, double* pvalue, double* log10p, double* freq,
+                       int32_t* tested) {
+    return guarded([&] {
+        require(lmm != nullptr && g != nullptr, "null argument");
+        cs::lmm_scan_window(lmm, g, keep, n_keep, snp_begin, snp_end, min_maf, precision, beta,
+                            se, pvalue, log10p, freq, tested, 0);
+    });
+}
+
 void cs_lmm_destroy(cs_lmm* lmm) { cs::lmm_destroy(lmm); }
 
 int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out) {

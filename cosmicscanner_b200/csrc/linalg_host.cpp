@@ -32,12 +32,17 @@ bool cholesky_upper(const std::vector<double>& G, int n, std::vector<double>& R)
 
 std::vector<double> upper_inverse(const std::vector<double>& R, int n) {
     std::vector<double> X((size_t)n * n, 0.0);
+    // column j of the inverse solves R x = e_j: back substitution in axpy form, which walks
+    // the columns of R contiguously; the columns are independent
+#pragma omp parallel for schedule(dynamic, 4) if (n > 96)
     for (int j = 0; j < n; ++j) {
-        X[j + (size_t)j * n] = 1.0 / R[j + (size_t)j * n];
-        for (int i = j - 1; i >= 0; --i) {
-            double s = 0.0;
-            for (int k = i + 1; k <= j; ++k) s += R[i + (size_t)k * n] * X[k + (size_t)j * n];
-            X[i + (size_t)j * n] = -s / R[i + (size_t)i * n];
+        double* x = X.data() + (size_t)j * n;
+        x[j] = 1.0;
+        for (int k = j; k >= 0; --k) {
+            const double* rk = R.data() + (size_t)k * n;
+            const double xk = x[k] / rk[k];
+            x[k] = xk;
+            for (int i = 0; i < k; ++i) x[i] -= xk * rk[i];
         }
     }
     return X;

@@ -130,6 +130,13 @@ int cs_lmm_lowrank_basis(const cs_lmm* lmm, double* U, int64_t ldu, double* lamb
 int cs_lmm_scan(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
                 double min_maf, int precision, double* beta, double* se, double* pvalue,
                 double* log10p, double* freq, int32_t* tested);
+/* The same scan restricted to SNPs [snp_begin, snp_end) of g (a chromosome of a LOCO run,
+ * src/gwas_scanner.cpp:447 with chrom_filter; or a --scan-from/to-bp window); the outputs
+ * have snp_end - snp_begin entries. */
+int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                       int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
+                       double* beta, double* se, double* pvalue, double* log10p, double* freq,
+                       int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
 
 /* The test matrix of src/lmm_engine.cpp:917-922 (also libCosmicCore/src/rng.h:27-33):

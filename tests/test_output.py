@@ -62,3 +62,15 @@ def test_writer_errors(tmp_path):
     bim.write_text("1 a 0 10 A C\n1 b 0 20 G T\n")
     with pytest.raises(cs.InvalidArgument):
         cs.write_assoc_txt(str(tmp_path / "x"), str(bim), res, 1)
+
+
+def test_chromosome_order_and_bim_reader(tmp_path):
+    """LOCO chromosome order (src/gwas_scanner.cpp:62-72: std::stoi comparison, else string)
+    and the .bim columns of PlinkReader::readBim."""
+    assert cs.sort_chrom_labels(["10", "2", "X", "1", "MT", "2", "22", "Y"]) == \
+        ["1", "2", "10", "22", "MT", "X", "Y"]
+    bim = tmp_path / "x.bim"
+    bim.write_text("1 rs1 0.0 100 A G\n\n2 rs2 0.5 200 C T\n")
+    b = cs.read_bim(str(bim))
+    assert list(b["chrom"]) == ["1", "2"] and list(b["bp"]) == [100, 200]
+    assert b["a1"] == ["A", "C"] and b["a2"] == ["G", "T"]
