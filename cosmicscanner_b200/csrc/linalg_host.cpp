@@ -48,77 +48,97 @@ std::vector<double> upper_inverse(const std::vector<double>& R, int n) {
     return X;
 }
 
-bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
-          std::vector<double>& V) {
-    // A (row-major == column-major for a symmetric matrix) from the lower triangle
+bool tridiag_ql(const std::vector<double>& A_in, int n, std::vector<double>& d,
+                std::vector<double>& Q, std::vector<PlaneRotation>& rots) {
+    // Householder reduction of the lower triangle to tridiagonal form, updating only the
+    // trailing block; the reflectors are kept for the backward accumulation of Q.
     std::vector<double> A((size_t)n * n);
     for (int c = 0; c < n; ++c)
         for (int r = 0; r < n; ++r) {
             const int lo_r = std::max(r, c), lo_c = std::min(r, c);
             A[r + (size_t)c * n] = A_in[lo_r + (size_t)lo_c * n];
         }
-    // Qt: transpose of the accumulated orthogonal factor, row-major: Qt[j][k] = Q[k][j]
-    std::vector<double> Qt((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) Qt[(size_t)i * n + i] = 1.0;
-    std::vector<double> v(n), p(n), w(n), qv(n);
-    // Householder reduction to tridiagonal form: A <- H A H, Q <- Q H
+    d.assign(n, 0.0);
+    std::vector<double> e(n, 0.0);
+    std::vector<double> refl((size_t)n * n, 0.0);  // column k: reflector v_k (rows k+1..n-1)
+    std::vector<char> has_refl(n, 0);
+    std::vector<double> p(n), w(n);
     for (int k = 0; k + 2 < n; ++k) {
+        const int m0 = k + 1, len = n - m0;
+        const double* col = A.data() + (size_t)k * n;
         double norm2 = 0.0;
-        for (int i = k + 1; i < n; ++i) norm2 += A[i + (size_t)k * n] * A[i + (size_t)k * n];
-        const double x0 = A[k + 1 + (size_t)k * n];
+        for (int i = m0; i < n; ++i) norm2 += col[i] * col[i];
         const double norm = std::sqrt(norm2);
-        if (norm == 0.0) continue;
+        const double x0 = col[m0];
+        d[k] = col[k];
+        if (norm == 0.0) {
+            e[k] = 0.0;
+            continue;
+        }
         const double alpha = x0 > 0 ? -norm : norm;
-        std::fill(v.begin(), v.end(), 0.0);
-        for (int i = k + 1; i < n; ++i) v[i] = A[i + (size_t)k * n];
-        v[k + 1] -= alpha;
+        double* v = refl.data() + (size_t)k * n;
+        for (int i = m0; i < n; ++i) v[i] = col[i];
+        v[m0] -= alpha;
         double vn = 0.0;
-        for (int i = k + 1; i < n; ++i) vn += v[i] * v[i];
+        for (int i = m0; i < n; ++i) vn += v[i] * v[i];
         vn = std::sqrt(vn);
+        e[k] = alpha;
         if (vn == 0.0) continue;
-        for (int i = k + 1; i < n; ++i) v[i] /= vn;
-        // p = A v (A symmetric: column c of A dotted with v)
-#pragma omp parallel for schedule(static) if (n > 96)
-        for (int c = 0; c < n; ++c) {
-            const double* col = A.data() + (size_t)c * n;
-            double s = 0.0;
-            for (int j = k + 1; j < n; ++j) s += col[j] * v[j];
-            p[c] = s;
+        for (int i = m0; i < n; ++i) v[i] /= vn;
+        has_refl[k] = 1;
+        // p = A_sub v over the trailing block (symmetric: column dots)
+        for (int c = m0; c < n; ++c) {
+            const double* __restrict__ ac = A.data() + (size_t)c * n;
+            const double* __restrict__ vv = v;
+            double sacc = 0.0;
+#pragma omp simd reduction(+ : sacc)
+            for (int j = m0; j < n; ++j) sacc += ac[j] * vv[j];
+            p[c] = sacc;
         }
         double kappa = 0.0;
-        for (int i = k + 1; i < n; ++i) kappa += v[i] * p[i];
-        for (int i = 0; i < n; ++i) w[i] = p[i] - kappa * v[i];
-        // A' = A - 2 (v w^T + w v^T)
-#pragma omp parallel for schedule(static) if (n > 96)
-        for (int c = 0; c < n; ++c) {
-            double* col = A.data() + (size_t)c * n;
-            const double vc = v[c], wc = w[c];
-            for (int r = 0; r < n; ++r) col[r] -= 2.0 * (v[r] * wc + w[r] * vc);
+        for (int i = m0; i < n; ++i) kappa += v[i] * p[i];
+        for (int i = m0; i < n; ++i) w[i] = p[i] - kappa * v[i];
+        // A_sub -= 2 (v w^T + w v^T)
+        for (int c = m0; c < n; ++c) {
+            double* __restrict__ ac = A.data() + (size_t)c * n;
+            const double* __restrict__ vv = v;
+            const double* __restrict__ ww = w.data();
+            const double vc = 2.0 * v[c], wc = 2.0 * w[c];
+#pragma omp simd
+            for (int r = m0; r < n; ++r) ac[r] -= vv[r] * wc + ww[r] * vc;
         }
-        // Q <- Q H: Q[r][j] -= 2 (Q v)_r v_j, i.e. Qt[j][r] -= 2 v_j qv_r
-        for (int r = 0; r < n; ++r) qv[r] = 0.0;
-        for (int j = k + 1; j < n; ++j) {
-            const double vj = v[j];
-            const double* row = Qt.data() + (size_t)j * n;
-            for (int r = 0; r < n; ++r) qv[r] += row[r] * vj;
+        (void)len;
+    }
+    if (n >= 2) {
+        d[n - 2] = A[(n - 2) + (size_t)(n - 2) * n];
+        e[n - 2] = A[(n - 1) + (size_t)(n - 2) * n];
+    }
+    d[n - 1] = A[(n - 1) + (size_t)(n - 1) * n];
+    // Q = H_0 H_1 ... H_{n-3}, accumulated backwards on the trailing blocks (column-major)
+    Q.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) Q[i + (size_t)i * n] = 1.0;
+    std::vector<double> t(n);
+    for (int k = n - 3; k >= 0; --k) {
+        if (!has_refl[k]) continue;
+        const int m0 = k + 1;
+        const double* v = refl.data() + (size_t)k * n;
+        for (int c = m0; c < n; ++c) {
+            const double* __restrict__ qc = Q.data() + (size_t)c * n;
+            double sacc = 0.0;
+#pragma omp simd reduction(+ : sacc)
+            for (int i = m0; i < n; ++i) sacc += v[i] * qc[i];
+            t[c] = 2.0 * sacc;
         }
-#pragma omp parallel for schedule(static) if (n > 96)
-        for (int j = k + 1; j < n; ++j) {
-            double* row = Qt.data() + (size_t)j * n;
-            const double vj = 2.0 * v[j];
-            for (int r = 0; r < n; ++r) row[r] -= vj * qv[r];
+        for (int c = m0; c < n; ++c) {
+            double* __restrict__ qc = Q.data() + (size_t)c * n;
+            const double tc = t[c];
+#pragma omp simd
+            for (int i = m0; i < n; ++i) qc[i] -= v[i] * tc;
         }
     }
-    std::vector<double> d(n), e(n, 0.0);
-    for (int i = 0; i < n; ++i) d[i] = A[i + (size_t)i * n];
-    for (int i = 0; i + 1 < n; ++i) e[i] = A[i + 1 + (size_t)i * n];
-    // Implicit QL with shifts on (d, e); the plane rotations are recorded and applied to
-    // the eigenvector rows afterwards, in parallel (e[i] couples d[i] and d[i+1]).
-    struct Rot {
-        int i;
-        double c, s;
-    };
-    std::vector<Rot> rots;
+    // Implicit QL with shifts on (d, e); the plane rotations are recorded so that they can be
+    // applied to the columns of Q afterwards (in order).
+    rots.clear();
     rots.reserve((size_t)n * 8);
     for (int l = 0; l < n; ++l) {
         int iter = 0;
@@ -131,14 +151,14 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
             if (m != l) {
                 if (++iter > 200) return false;
                 double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-                double r = std::hypot(g, 1.0);
+                double r = std::sqrt(g * g + 1.0);
                 g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
                 double s = 1.0, c = 1.0, pp = 0.0;
                 int i;
                 for (i = m - 1; i >= l; --i) {
                     const double f = s * e[i];
                     const double b = c * e[i];
-                    r = std::hypot(f, g);
+                    r = std::sqrt(f * f + g * g);
                     e[i + 1] = r;
                     if (r == 0.0) {
                         d[i + 1] -= pp;
@@ -152,7 +172,7 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
                     pp = s * r;
                     d[i + 1] = g + pp;
                     g = c * r - b;
-                    rots.push_back(Rot{i, c, s});
+                    rots.push_back(PlaneRotation{i, c, s});
                 }
                 if (r == 0.0 && i >= l) continue;
                 d[l] -= pp;
@@ -161,25 +181,30 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
             }
         } while (m != l);
     }
-    // eigenvectors: rows of Q (= columns of Qt) rotated in sequence; each row independently
-    std::vector<double> Vr((size_t)n * n);  // row-major: Vr[r][j] = Q[r][j]
-    for (int j = 0; j < n; ++j)
-        for (int r = 0; r < n; ++r) Vr[(size_t)r * n + j] = Qt[(size_t)j * n + r];
-#pragma omp parallel
-    {
-#ifdef _OPENMP
-        const int nt = omp_get_num_threads(), tid = omp_get_thread_num();
-#else
-        const int nt = 1, tid = 0;
-#endif
-        const int r0 = (int)((int64_t)n * tid / nt), r1 = (int)((int64_t)n * (tid + 1) / nt);
-        for (const Rot& rt : rots)
+    return true;
+}
+
+bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
+          std::vector<double>& V) {
+    std::vector<double> d, Q;
+    std::vector<PlaneRotation> rots;
+    if (!tridiag_ql(A_in, n, d, Q, rots)) return false;
+    // rotations on the columns of Q, each thread on its own block of rows
+    constexpr int kRowBlock = 64;
+    const int blocks = (n + kRowBlock - 1) / kRowBlock;
+#pragma omp parallel for schedule(static) if (n > 96)
+    for (int bidx = 0; bidx < blocks; ++bidx) {
+        const int r0 = bidx * kRowBlock, r1 = std::min(n, r0 + kRowBlock);
+        for (const PlaneRotation& rt : rots) {
+            double* __restrict__ qa = Q.data() + (size_t)rt.i * n;
+            double* __restrict__ qb = qa + n;
+#pragma omp simd
             for (int r = r0; r < r1; ++r) {
-                double* row = Vr.data() + (size_t)r * n;
-                const double f = row[rt.i + 1];
-                row[rt.i + 1] = rt.s * row[rt.i] + rt.c * f;
-                row[rt.i] = rt.c * row[rt.i] - rt.s * f;
+                const double f = qb[r];
+                qb[r] = rt.s * qa[r] + rt.c * f;
+                qa[r] = rt.c * qa[r] - rt.s * f;
             }
+        }
     }
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
@@ -188,7 +213,8 @@ bool eigh(const std::vector<double>& A_in, int n, std::vector<double>& evals,
     V.assign((size_t)n * n, 0.0);
     for (int c = 0; c < n; ++c) {
         evals[c] = d[order[c]];
-        for (int r = 0; r < n; ++r) V[r + (size_t)c * n] = Vr[(size_t)r * n + order[c]];
+        std::copy(Q.begin() + (size_t)order[c] * n, Q.begin() + (size_t)(order[c] + 1) * n,
+                  V.begin() + (size_t)c * n);
     }
     return true;
 }

@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <numeric>
+#include <mutex>
 #include <optional>
 #include <random>
 
@@ -49,6 +51,9 @@ struct cs_lmm {
     cs::DeviceBuffer<int32_t> d_counts, d_tested;
     cs::DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
     cs::DeviceBuffer<uint8_t> d_pass;
+    // sketch eigenvectors: the rotated Q, the QL rotations, the selected columns
+    cs::DeviceBuffer<double> d_eig, d_rot_cs;
+    cs::DeviceBuffer<int32_t> d_rot_i, d_cols;
     ~cs_lmm() {
         cs::mixed_scan_destroy(scan_mixed);
     }
@@ -109,6 +114,50 @@ void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q
         }
     }
     CS_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------- eigenvectors
+// Applies the recorded QL rotations to the columns of Q (n x n, column-major): block b owns
+// rows 32 b .. 32 b + 31 in shared memory (one lane per row, bank-conflict free), a warp loads
+// 32 rotations at a time and broadcasts them with shuffles, and the rotations are applied in
+// order (each updates columns i and i + 1 of the lane's row).
+__global__ void __launch_bounds__(32, 1)
+k_rotate_rows(double* __restrict__ Q, int n, const int32_t* __restrict__ ri,
+              const double2* __restrict__ rcs, int64_t nrot) {
+    extern __shared__ double rows_s[];  // rows_s[c * 32 + lane]
+    const int lane = threadIdx.x;
+    const int r = blockIdx.x * 32 + lane;
+    const bool live = r < n;
+    for (int c = 0; c < n; ++c) rows_s[c * 32 + lane] = live ? Q[r + (int64_t)c * n] : 0.0;
+    __syncwarp();
+    for (int64_t base = 0; base < nrot; base += 32) {
+        const int64_t q = base + lane;
+        const int my_i = q < nrot ? ri[q] : 0;
+        const double2 my_cs = q < nrot ? rcs[q] : make_double2(1.0, 0.0);
+        const int cnt = nrot - base < 32 ? (int)(nrot - base) : 32;
+        for (int j = 0; j < cnt; ++j) {
+            const int i = __shfl_sync(0xffffffffu, my_i, j);
+            const double c = __shfl_sync(0xffffffffu, my_cs.x, j);
+            const double sn = __shfl_sync(0xffffffffu, my_cs.y, j);
+            const double a = rows_s[i * 32 + lane], b = rows_s[(i + 1) * 32 + lane];
+            rows_s[(i + 1) * 32 + lane] = sn * a + c * b;
+            rows_s[i * 32 + lane] = c * a - sn * b;
+        }
+    }
+    __syncwarp();
+    if (live)
+        for (int c = 0; c < n; ++c) Q[r + (int64_t)c * n] = rows_s[c * 32 + lane];
+}
+
+// out[:, j] = Q[:, cols[j]] (column-major, n rows)
+__global__ void k_gather_columns(const double* __restrict__ Q, int64_t n,
+                                 const int32_t* __restrict__ cols, int64_t k, double* __restrict__ out) {
+    const int64_t total = n * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = e / n, a = e - j * n;
+        out[e] = Q[a + (int64_t)cols[j] * n];
+    }
 }
 
 // ---------------------------------------------------------------- REML (host)
@@ -329,6 +378,38 @@ __global__ void k_scan_epilogue(ScanParams P) {
 
 }  // namespace
 
+// Q (host, the tridiagonalising factor) and the QL rotations -> eigenvector matrix in l->d_eig.
+static void rotate_eigenvectors(cs_lmm* l, const std::vector<double>& Qh,
+                                const std::vector<la::PlaneRotation>& rots, int n, cudaStream_t s) {
+    prof::HostScope hs("lowrank_eigvec_rotations");
+    const int64_t nr = (int64_t)rots.size();
+    std::vector<int32_t> ri(std::max<int64_t>(nr, 1));
+    std::vector<double2> rcs(std::max<int64_t>(nr, 1));
+    for (int64_t q = 0; q < nr; ++q) {
+        ri[q] = rots[q].i;
+        rcs[q] = make_double2(rots[q].c, rots[q].s);
+    }
+    l->d_eig.resize((int64_t)n * n);
+    l->d_rot_i.resize(ri.size());
+    l->d_rot_cs.resize(2 * rcs.size());
+    CS_CUDA(cudaMemcpyAsync(l->d_eig.get(), Qh.data(), 8 * (size_t)n * n, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_rot_i.get(), ri.data(), 4 * ri.size(), cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_rot_cs.get(), rcs.data(), 16 * rcs.size(), cudaMemcpyHostToDevice, s));
+    const size_t smem = (size_t)n * 32 * sizeof(double);
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(k_rotate_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    200 * 1024);
+    });
+    check_cuda(attr, "configure eigenvector rotation kernel");
+    if (smem > 200 * 1024) fail(CS_ERR_UNSUPPORTED, "sketch too wide for the rotation kernel");
+    prof::Scope ps("eigvec_rotations", s, 6.0 * (double)nr * n, 0.0);
+    k_rotate_rows<<<(unsigned)((n + 31) / 32), 32, smem, s>>>(
+        l->d_eig.get(), n, l->d_rot_i.get(), reinterpret_cast<const double2*>(l->d_rot_cs.get()), nr);
+    CS_LAUNCH("eigvec_rotations");
+}
+
 cs_lmm* lmm_create() {
     prof::HostScope hs("lmm_create");
     auto* l = new cs_lmm();
@@ -403,8 +484,18 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     std::vector<double> B(sk * sk);
     CS_CUDA(cudaMemcpyAsync(B.data(), small.get(), 8 * sk * sk, cudaMemcpyDeviceToHost, s));
     CS_CUDA(cudaStreamSynchronize(s));
-    std::vector<double> evals, evecs;
-    if (!la::eigh(B, (int)sk, evals, evecs)) fail(CS_ERR_NUMERIC, "Low-rank GRM eigensolver failed");
+    // eigendecomposition of B: tridiagonalisation and QL on the host, the QL rotations
+    // applied to the eigenvector matrix on the device
+    std::vector<double> dvals, Qh;
+    std::vector<la::PlaneRotation> rots;
+    if (!la::tridiag_ql(B, (int)sk, dvals, Qh, rots))
+        fail(CS_ERR_NUMERIC, "Low-rank GRM eigensolver failed");
+    std::vector<int> order(sk);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return dvals[a] < dvals[b]; });
+    std::vector<double> evals(sk);
+    for (int64_t j = 0; j < sk; ++j) evals[j] = dvals[order[j]];
+    rotate_eigenvectors(l, Qh, rots, (int)sk, s);
     std::vector<double> lead(rank);
     for (int j = 0; j < rank; ++j) lead[j] = std::max(0.0, evals[sk - 1 - j]);
     // trace-fraction rank selection (lmm_engine.cpp:958-973)
@@ -425,12 +516,18 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     }
     hs_stage.reset();
     hs_stage.emplace("lowrank_basis_reml");
-    // U = Q W_top (n x selected, row-major): U^c = W_top^T Q^c
-    std::vector<double> wtop(sk * selected);
-    for (int j = 0; j < selected; ++j)
-        for (int64_t a = 0; a < sk; ++a) wtop[a + j * sk] = evecs[a + (sk - 1 - j) * sk];
+    // U = Q W_top (n x selected, row-major): U^c = W_top^T Q^c, W_top = the eigenvectors of
+    // the `selected` largest eigenvalues, largest first
     gram.resize(sk * selected);
-    CS_CUDA(cudaMemcpyAsync(gram.get(), wtop.data(), 8 * sk * selected, cudaMemcpyHostToDevice, s));
+    {
+        std::vector<int32_t> cols(selected);
+        for (int j = 0; j < selected; ++j) cols[j] = order[sk - 1 - j];
+        l->d_cols.resize(selected);
+        CS_CUDA(cudaMemcpyAsync(l->d_cols.get(), cols.data(), 4 * selected, cudaMemcpyHostToDevice, s));
+        k_gather_columns<<<(unsigned)std::max<int64_t>(1, (sk * selected + 255) / 256), 256, 0, s>>>(
+            l->d_eig.get(), sk, l->d_cols.get(), selected, gram.get());
+        CS_LAUNCH("gather_eigenvectors");
+    }
     l->d_U.resize(n * selected);
     CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_T, CUBLAS_OP_N, selected, (int)n, (int)sk, &one,
                         gram.get(), (int)sk, q.get(), (int)sk, &zero, l->d_U.get(), selected));
