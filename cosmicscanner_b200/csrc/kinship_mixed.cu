@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -321,6 +322,235 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
     }
 }
 
+// ---------------------------------------------------------------- samples pass on CTA pairs
+// The samples pass with a two-CTA MMA (cta_group::2, a cluster of two CTAs): each CTA decodes
+// its own 128-sample tile of the packed K-block, and loads only half of the right-hand-side
+// pieces (rows [1.5 kc r, 1.5 kc (r + 1)) of each 3 kc-row part, r = CTA rank).  The leader
+// (rank 0) issues M = 256 MMAs that read both CTAs' tiles and halves, so every B byte
+// crosses from L2 once per 256 samples instead of once per 128, and the smaller B stage
+// leaves room for four TMA stages.  Each CTA's TMEM receives its own 128 rows.
+//   decoders (both CTAs) -> leader's full_d (cluster-scope arrive), after their own TMA
+//   stage landed, so a completed full_d also covers both B halves;
+//   leader's MMAs -> commit multicast to both CTAs' empty_t / empty_d / acc_full;
+//   epilogues (both) -> leader's acc_empty.
+struct PairLayout {
+    static constexpr int kTmaStages = 4;
+    static constexpr int kBBytes = 3 * kMaxKc * 128;  // two 1.5 kc-row halves (W, mu o W)
+    static constexpr int kTmaBytes = kBBytes + kPackedBytes;
+    static constexpr int kDecBytes = 2 * kATileBytes;
+    static constexpr int kSmem = kDecStages * kDecBytes + kTmaStages * kTmaBytes + 1024 + 256;
+    static __host__ __device__ constexpr int a(int d) { return d * kDecBytes; }
+    static __host__ __device__ constexpr int am(int d) { return d * kDecBytes + kATileBytes; }
+    static __host__ __device__ constexpr int b(int s) { return kDecStages * kDecBytes + s * kTmaBytes; }
+    static __host__ __device__ constexpr int p(int s) { return b(s) + kBBytes; }
+    static __host__ __device__ constexpr int bars() { return kDecStages * kDecBytes + kTmaStages * kTmaBytes; }
+};
+static_assert(PairLayout::kSmem <= 227 * 1024, "paired samples pass exceeds shared memory");
+static_assert(PairLayout::kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
+
+__global__ void __launch_bounds__(kThreads, 1)
+k_samples_pass_pair(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+                    PassArgs P) {
+    using L = PairLayout;
+    constexpr int ST = L::kTmaStages, SD = kDecStages, NB = 2;
+    constexpr uint32_t kAccStride = 256;
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bars());
+    uint64_t* full_t = bars;
+    uint64_t* empty_t = full_t + ST;
+    uint64_t* full_d = empty_t + ST;      // leader: both CTAs' decoders
+    uint64_t* empty_d = full_d + SD;
+    uint64_t* acc_full = empty_d + SD;
+    uint64_t* acc_empty = acc_full + NB;  // leader: both CTAs' epilogue warps
+    uint64_t* drained = acc_empty + NB;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int kc = P.kc, kp = P.kp, half = kc / 2;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < ST; ++q) {
+            mbar_init(&full_t[q], 1);
+            mbar_init(&empty_t[q], 1);
+        }
+        for (int d = 0; d < SD; ++d) {
+            mbar_init(&full_d[d], 2 * kDecodeWarps);
+            mbar_init(&empty_d[d], 1);
+        }
+        for (int b = 0; b < NB; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 8);
+        }
+        mbar_init(drained, 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc_pair(tmem_slot, kTmemCols);
+    tc_fence_before();
+    cluster_sync_all();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    const int pairs = P.n_tiles;  // tile pairs (n_tiles of this kernel counts pairs)
+    const int units = pairs * P.n_ctiles * P.n_splits;
+    const int cluster = (int)cluster_id_x(), clusters = (int)cluster_count_x();
+    auto unit_coords = [&](int u, int& tile, int& ct, int& split, int& kb0, int& kb1) {
+        const int pr = u % pairs;
+        const int rest = u / pairs;
+        tile = 2 * pr + (int)rank;
+        ct = rest % P.n_ctiles;
+        split = rest / P.n_ctiles;
+        kb0 = split * P.kb_per_split;
+        kb1 = min(P.kb_total, kb0 + P.kb_per_split);
+    };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ TMA producer (both)
+        if (elect_one()) {
+            prefetch_tensormap(&tm_a);
+            prefetch_tensormap(&tm_b);
+            const uint32_t bytes = (uint32_t)(kPackedBytes + 6 * half * 128);
+            uint32_t j = 0;
+            bool ok = true;
+            for (int u = cluster; u < units && ok; u += clusters) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int sg = j % ST;
+                    if (!(ok = mbar_wait(&empty_t[sg], ((j / ST) & 1) ^ 1, P.status, kTimeoutTma))) break;
+                    mbar_arrive_expect_tx(&full_t[sg], bytes);
+                    tma_load_2d(smem + L::p(sg), &tm_a, tile * 32, kb * kKBlock, &full_t[sg]);
+                    // this CTA's half of each part: half-pieces 3 rank .. 3 rank + 2 of
+                    // [p0a p0b p1a p1b p2a p2b] (kc / 2 rows each)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int h = 3 * (int)rank + c, q = h >> 1;
+                        const int row = q * kp + ct * kc + (h & 1) * half;
+                        tma_load_2d(smem + L::b(sg) + c * half * 128, &tm_b, kb * kKBlock, row,
+                                    &full_t[sg]);
+                        tma_load_2d(smem + L::b(sg) + (3 + c) * half * 128, &tm_b, kb * kKBlock,
+                                    row + 3 * kp, &full_t[sg]);
+                    }
+                }
+            }
+            for (uint32_t q = (j >= (uint32_t)ST ? j - ST : 0); q < j; ++q)
+                mbar_wait(&full_t[q % ST], (q / ST) & 1, P.status, kTimeoutTma, 1u << 20);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (leader)
+        if (rank == 0 && elect_one()) {
+            // s8 x s8 -> s32, MN-major A (samples x SNPs), M = 256 over the pair
+            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) |
+                                   ((uint32_t)((3 * kc) >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+            uint32_t j = 0;
+            int ui = 0;
+            bool ok = true;
+            for (int u = cluster; u < units && ok; u += clusters, ++ui) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                const int buf = ui % NB;
+                if (!(ok = mbar_wait_cluster(&acc_empty[buf], ((ui / NB) & 1) ^ 1, P.status, kTimeoutMma)))
+                    break;
+                tc_fence_after();
+                const uint32_t acc = tmem_base + buf * kAccStride;
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int sg = j % ST, d = j % SD;
+                    if (!(ok = mbar_wait_cluster(&full_d[d], (j / SD) & 1, P.status, kTimeoutMma))) break;
+                    tc_fence_after();
+                    const uint32_t a = smem_addr(smem + L::a(d));
+                    const uint32_t am = smem_addr(smem + L::am(d));
+                    const uint32_t b = smem_addr(smem + L::b(sg));
+                    const uint32_t bm = b + 3 * half * 128;
+#pragma unroll
+                    for (int ks = 0; ks < kKBlock / 32; ++ks) {
+                        const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
+                        const uint64_t da = smem_desc_sw128(a + ks * 4096, 16, 1024);
+                        const uint64_t dm = smem_desc_sw128(am + ks * 4096, 16, 1024);
+                        const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
+                        const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
+                        mma_i8_pair(acc, da, db, idesc, first);
+                        mma_i8_pair(acc, dm, dbm, idesc, 1u);
+                    }
+                    mma_commit_pair(&empty_t[sg], 3);
+                    mma_commit_pair(&empty_d[d], 3);
+                }
+                if (ok) mma_commit_pair(&acc_full[buf], 3);
+            }
+            mma_commit_pair(drained, 1);
+            mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
+        }
+    } else if (warp < kEpiWarp0) {
+        // ------------------------------------------------------------ decoders (both)
+        const int dt = threadIdx.x - kDecodeWarp0 * 32;
+        const int r = dt & 127, h = dt >> 7;
+        const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
+        uint32_t j = 0;
+        bool ok = true;
+        for (int u = cluster; u < units && ok; u += clusters) {
+            int tile, ct, split, kb0, kb1;
+            unit_coords(u, tile, ct, split, kb0, kb1);
+            for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                const int sg = j % ST, d = j % SD;
+                if (!(ok = mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode))) break;
+                if (!(ok = mbar_wait(&full_t[sg], (j / ST) & 1, P.status, kTimeoutDecode))) break;
+                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sg) + r * 32 + h * 16);
+                unsigned char* a = smem + L::a(d);
+                unsigned char* am = smem + L::am(d);
+                const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
+#pragma unroll
+                for (int cj = 0; cj < 4; ++cj) {
+                    uint4 dos, mis;
+                    decode_word(words[cj], dos, mis);
+                    const int chunk = 4 * h + cj;
+                    const int off = rbase + ((chunk ^ (r & 7)) << 4);
+                    *reinterpret_cast<uint4*>(a + off) = dos;
+                    *reinterpret_cast<uint4*>(am + off) = mis;
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_remote(mapa_shared(&full_d[d], 0));
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (both)
+        const int q = warp & 3;
+        int ui = 0;
+        bool ok = true;
+        const double ib = 1.0 / kBase, ib2 = 1.0 / (kBase * kBase);
+        for (int u = cluster; u < units && ok; u += clusters, ++ui) {
+            int tile, ct, split, kb0, kb1;
+            unit_coords(u, tile, ct, split, kb0, kb1);
+            const int buf = ui % NB;
+            if (!(ok = mbar_wait(&acc_full[buf], (ui / NB) & 1, P.status, kTimeoutEpilogue))) break;
+            tc_fence_after();
+            const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
+            const uint32_t tb = tmem_base + buf * kAccStride + ((uint32_t)(32 * q) << 16);
+            double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
+            for (int c0 = 0; c0 < kc; c0 += 16) {
+                int32_t m1[16], m2[16], m3[16];
+                tmem_ld16i(tb + c0, m1);
+                tmem_ld16i(tb + kc + c0, m2);
+                tmem_ld16i(tb + 2 * kc + c0, m3);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                    dst[(int64_t)(c0 + i) * P.ld] = mv * P.inv_f[ct * kc + c0 + i];
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_remote(mapa_shared(&acc_empty[buf], 0));
+        }
+    }
+    tc_fence_before();
+    cluster_sync_all();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem_base, kTmemCols);
+    }
+}
+
 // ---------------------------------------------------------------- operand preparation
 // All reductions here are deterministic: block-level trees in a fixed order, per-block
 // partials summed in block order, and maxima through atomicMax on non-negative doubles
@@ -586,6 +816,19 @@ CUtensorMap make_map_u8(const void* base, uint64_t inner, uint64_t outer, uint64
     return m;
 }
 
+// The samples pass runs on single CTAs; CS_B200_SAMPLES_PASS=pair selects the CTA-pair
+// kernel.  Measured on B200 at N=50k, M=100k, k=266: 10.9 ms paired vs 9.6 ms single —
+// halving the L2->SM bytes of the right-hand-side pieces did not pay for the per-K-block
+// cross-CTA handshake (ncu: tensor pipe 38 % active, membar stalls from the cluster-scope
+// release arrives).  Kept for comparison.
+bool samples_pass_on_pairs() {
+    static const bool pairs = [] {
+        const char* v = std::getenv("CS_B200_SAMPLES_PASS");
+        return v && std::strcmp(v, "pair") == 0;
+    }();
+    return pairs;
+}
+
 int blocks_for(int64_t work) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 16LL * num_sms()));
 }
@@ -610,10 +853,11 @@ struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
     DeviceBuffer<unsigned long long> max1, max_w, max_muw;
-    CUtensorMap tm_b1{}, tm_b2{};
+    CUtensorMap tm_b1{}, tm_b2{}, tm_b2h{};
     const void* tm_b1_base = nullptr;
     const void* tm_b2_base = nullptr;
-    int64_t tm_b1_key = -1, tm_b2_key = -1;
+    const void* tm_b2h_base = nullptr;
+    int64_t tm_b1_key = -1, tm_b2_key = -1, tm_b2h_key = -1;
     DeviceBuffer<int> status;
 };
 
@@ -636,6 +880,10 @@ void configure_kernels() {
             err = cudaFuncSetAttribute(k_mixed_pass<false>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        Layout<false>::kSmem);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(k_samples_pass_pair,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       PairLayout::kSmem);
     });
     check_cuda(err, "configure tensor-core kernels");
 }
@@ -648,7 +896,9 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     r.R = v.n_rows;
     r.n = v.n_samples;
     r.r_pad = round_up(std::max<int64_t>(r.R, 1), kTile);
-    r.n_pad = round_up(std::max<int64_t>(r.n, 1), kTile);
+    // samples padded to 256: the samples pass runs on pairs of 128-sample tiles (packed rows
+    // hold a multiple of 256 samples, so the padding tiles read missing codes)
+    r.n_pad = round_up(std::max<int64_t>(r.n, 1), 2 * kTile);
     std::vector<double> mu(r.r_pad, 0.0), ex(r.r_pad, 0.0), sv(r.r_pad, 0.0);
     for (int64_t t = 0; t < r.R; ++t) {
         const double mt = mean[t];
@@ -821,7 +1071,32 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2, P);
+        if (samples_pass_on_pairs() && tiles % 2 == 0 && num_sms() >= 2) {
+            // CTA pairs: box of kc / 2 rows for the B halves
+            const int64_t hkey = (kp * 1000003 + r_pad) * 131 + tl.kc;
+            if (ws.tm_b2h_base != ws.b2.get() || ws.tm_b2h_key != hkey) {
+                ws.tm_b2h = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc / 2, true);
+                ws.tm_b2h_base = ws.b2.get();
+                ws.tm_b2h_key = hkey;
+            }
+            PassArgs Pp = P;
+            Pp.n_tiles = (int)(tiles / 2);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)(num_sms() & ~1));
+            cfg.blockDim = dim3(kThreads);
+            cfg.dynamicSmemBytes = PairLayout::kSmem;
+            cfg.stream = s;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = 2;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            CS_CUDA(cudaLaunchKernelEx(&cfg, k_samples_pass_pair, r.tm, ws.tm_b2h, Pp));
+        } else {
+            k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2, P);
+        }
         CS_LAUNCH("kinship_samples_tc");
     }
     {

@@ -130,6 +130,10 @@ k_rotate_rows(double* __restrict__ Q, int n, const int32_t* __restrict__ ri,
     const bool live = r < n;
     for (int c = 0; c < n; ++c) rows_s[c * 32 + lane] = live ? Q[r + (int64_t)c * n] : 0.0;
     __syncwarp();
+    // A QL sweep runs i downwards, so rotation (i - 1, i) usually follows (i, i + 1): the new
+    // column i stays in a register for it instead of a store-load round trip.
+    int prev_i = -2;
+    double carry = 0.0;
     for (int64_t base = 0; base < nrot; base += 32) {
         const int64_t q = base + lane;
         const int my_i = q < nrot ? ri[q] : 0;
@@ -139,9 +143,13 @@ k_rotate_rows(double* __restrict__ Q, int n, const int32_t* __restrict__ ri,
             const int i = __shfl_sync(0xffffffffu, my_i, j);
             const double c = __shfl_sync(0xffffffffu, my_cs.x, j);
             const double sn = __shfl_sync(0xffffffffu, my_cs.y, j);
-            const double a = rows_s[i * 32 + lane], b = rows_s[(i + 1) * 32 + lane];
+            const double a = rows_s[i * 32 + lane];
+            const double b = (i + 1 == prev_i) ? carry : rows_s[(i + 1) * 32 + lane];
+            const double na = c * a - sn * b;
             rows_s[(i + 1) * 32 + lane] = sn * a + c * b;
-            rows_s[i * 32 + lane] = c * a - sn * b;
+            rows_s[i * 32 + lane] = na;
+            carry = na;
+            prev_i = i;
         }
     }
     __syncwarp();
