@@ -53,6 +53,8 @@ def parse():
                     help="requests in the serving stream measured after the job (0 skips)")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the one-step timing of the plain FP64 GPU form")
+    ap.add_argument("--aireml-iters", type=int, default=2,
+                    help="AI-REML (PCG + Hutchinson) iterations timed per precision (0 skips)")
     return ap.parse_args()
 
 
@@ -276,6 +278,34 @@ def run_serve(cs, g, variants, d, args):
     }
 
 
+def run_aireml(cs, op, d, args, iters=4, probes=64):
+    """The PCG + Hutchinson AI-REML route (STCG_VCE with the single-record design, the
+    configuration's 64 Rademacher probes and 1 + p right-hand sides, absolute CG tolerance
+    1e-10): `iters` AI-REML iterations in the mixed form and in the FP64 form, seconds per
+    iteration each (the same probes, so the same CG systems)."""
+    import torch
+
+    out = {}
+    for prec in (args.precision, "fp64") if args.precision != "fp64" else ("fp64",):
+        vce = cs.StcgVce()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = vce.solve(op, d["y"], d["X"], kinship_divisor=float(d["m"]), max_iter=iters,
+                      mc_samples=probes, slq_probes=0, precision=prec)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[prec] = {"s_per_iteration": dt / max(1, r["iterations"]), "iterations": r["iterations"],
+                     "sigma2_g": r["sigma2_g"], "sigma2_e": r["sigma2_e"],
+                     "kinship_applies": r["operator_applies"],
+                     "rhs_per_apply": r["operator_columns"] / max(1, r["operator_applies"])}
+        vce.close()
+    if len(out) == 2:
+        out["speedup_mixed_over_fp64"] = out["fp64"]["s_per_iteration"] / out[args.precision]["s_per_iteration"]
+    out["config"] = (f"N={d['n']} M={d['m']}, {probes} probes + y + {d['X'].shape[1]} covariates, "
+                     f"pcg_tol 1e-10 absolute, {iters} iterations (EM warm-up steps)")
+    return out
+
+
 def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
     """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
     (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
@@ -438,6 +468,11 @@ def main():
         torch.cuda.synchronize()
         fp64_s = a0.elapsed_time(a1) / 1e3
     serve = run_serve(cs, g, variants, d, args) if args.serve_requests > 0 and world == 1 else None
+    aireml = None
+    if args.aireml_iters > 0 and world == 1:
+        op_all = cs.KinshipOperator(g, None, None)
+        aireml = run_aireml(cs, op_all, d, args, iters=args.aireml_iters)
+        op_all.close()
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
@@ -507,6 +542,7 @@ def main():
                 "speedup_mixed_over_fp64": fp64_s / sec_per_step,
                 "note": "the same REML+scan step with FP64 kinship applies and scan projection"},
             "serve": serve,
+            "aireml": aireml,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,

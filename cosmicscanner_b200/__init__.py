@@ -543,6 +543,30 @@ class Server:
             pass
 
 
+def stcg_scan(genotypes: Genotypes, G, subject_rows, obs_to_subject, y, X, vg, vpe, ve,
+              min_maf=0.01, snp_begin=0, snp_end=None) -> dict:
+    """RepeatabilityModel::scanSTCG's scan with a given subject GRM
+    (src/models/repeatability_scan_stcg.cpp:42-140) on the GPU; per-SNP dict for
+    [snp_begin, snp_end): beta, se, p, log10p, maf (folded, the FREQ column), tested."""
+    G = np.asfortranarray(G, dtype=np.float64)
+    q = G.shape[0]
+    subj = np.ascontiguousarray(subject_rows, dtype=np.int32)
+    o2s = np.ascontiguousarray(obs_to_subject, dtype=np.int32)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
+    end = genotypes.n_snps if snp_end is None else int(snp_end)
+    w = end - int(snp_begin)
+    out = {k: np.zeros(max(w, 0)) for k in ("beta", "se", "p", "log10p", "maf")}
+    tested = np.zeros(max(w, 0), dtype=np.int32)
+    _check(_abi.lib().cs_stcg_scan(genotypes._h, _ptr(G), q, _ptr(subj), _ptr(o2s), len(y),
+                                   _ptr(y), _ptr(X), X.shape[1], float(vg), float(vpe), float(ve),
+                                   float(min_maf), int(snp_begin), end, _ptr(out["beta"]),
+                                   _ptr(out["se"]), _ptr(out["p"]), _ptr(out["log10p"]),
+                                   _ptr(out["maf"]), _ptr(tested)))
+    out["tested"] = tested.astype(bool)
+    return out
+
+
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
     MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""

@@ -38,6 +38,11 @@ void vce_history(const cs_vce* v, double* out, int64_t* n_iter);
 void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, const double* B,
                       int64_t ldb, int64_t k, double* X, int64_t ldx, double tol, int relative,
                       int max_iter, int precision, int32_t* iterations, cudaStream_t s);
+void stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_t* subject_rows,
+               const int32_t* obs_to_subject, int64_t n_obs, const double* y, const double* X,
+               int64_t p, double vg, double vpe, double ve, double min_maf, int64_t snp_begin,
+               int64_t snp_end, double* beta, double* se, double* pvalue, double* log10p,
+               double* maf, int32_t* tested);
 void server_default_options(cs_server_options* o);
 cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_var,
                          const cs_server_options* opt);
@@ -296,6 +301,17 @@ int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations) {
 }
 
 void cs_vce_destroy(cs_vce* vce) { cs::vce_destroy(vce); }
+
+int cs_stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_t* subject_rows,
+                 const int32_t* obs_to_subject, int64_t n_obs, const double* y, const double* X,
+                 int64_t p, double vg, double vpe, double ve, double min_maf, int64_t snp_begin,
+                 int64_t snp_end, double* beta, double* se, double* pvalue, double* log10p,
+                 double* maf, int32_t* tested) {
+    return guarded([&] {
+        cs::stcg_scan(g, G, q, subject_rows, obs_to_subject, n_obs, y, X, p, vg, vpe, ve, min_maf,
+                      snp_begin, snp_end, beta, se, pvalue, log10p, maf, tested);
+    });
+}
 
 void cs_server_default_options(cs_server_options* opt) {
     if (opt) cs::server_default_options(opt);

@@ -207,6 +207,22 @@ int cs_vce_solution(const cs_vce* vce, double* beta, double* a_rows, double* pe_
 int cs_vce_history(const cs_vce* vce, double* out, int64_t* n_iterations);
 void cs_vce_destroy(cs_vce* vce);
 
+/* Replaces the repeatability scan after the STCG null model (RepeatabilityModel::scanSTCG,
+ * scan_stcg_with_grm, src/models/repeatability_scan_stcg.cpp:42-140) for SNPs
+ * [snp_begin, snp_end) of g.  G: the q x q subject GRM (host, column-major; the reference's
+ * G_subject_ or a LOCO G_loco), subject s is operator row subject_rows[s]; record i belongs to
+ * subject obs_to_subject[i]; y (n_obs) and X (n_obs x p, column-major, host) are the records'
+ * phenotype and fixed effects; vg / vpe / ve the null variance components.  Per SNP: the
+ * record dosages centred on their mean (missing calls at -mean), skip when fewer than 10
+ * records carry a call or the folded MAF < min_maf, score = g' P y, var = g' P g (skip below
+ * 1e-15), P = erfc(|z| / sqrt 2), LOG10P as the reference.  maf receives the folded MAF (the
+ * file's FREQ column).  Outputs have snp_end - snp_begin entries (NaN where tested = 0). */
+int cs_stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_t* subject_rows,
+                 const int32_t* obs_to_subject, int64_t n_obs, const double* y, const double* X,
+                 int64_t p, double vg, double vpe, double ve, double min_maf, int64_t snp_begin,
+                 int64_t snp_end, double* beta, double* se, double* pvalue, double* log10p,
+                 double* maf, int32_t* tested);
+
 /* ---------------------------------------------------------------- serving loop
  * No reference counterpart (the reference runs one job per process).  A server keeps the
  * packed genotypes resident and answers requests, each the matrix-free LMM job of

@@ -94,6 +94,10 @@ def lib():
         L.orc_stcg_vce.argtypes = [_P, _I64, _I64, _I64, _P, _P, _P, _I64, C.c_int, _P, _P, _I64,
                                    _P, _P, _P, _P, _P]
         L.orc_stcg_vce.restype = C.c_int
+        L.orc_stcg_scan.argtypes = [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P, _I64,
+                                    C.c_double, C.c_double, C.c_double, C.c_double, _I64, _I64,
+                                    _P, _P, _P, _P, _P, _P]
+        L.orc_stcg_scan.restype = C.c_int
         _lib = L
     return _lib
 
@@ -242,6 +246,28 @@ def stcg_vce(bed: "Bed", y, X, rec_to_row=None, with_pe=False, max_iter=50, tol=
         raise RuntimeError("oracle stcg_vce failed")
     out = {name: getattr(res, name) for name, _ in res._fields_}
     return out, beta, a, pe
+
+
+def stcg_scan(bed: "Bed", G, subject_rows, obs_to_subject, y, X, vg, vpe, ve, min_maf=0.01,
+              snp_begin=0, snp_end=None):
+    """scan_stcg_with_grm restated (src/models/repeatability_scan_stcg.cpp:42-140)."""
+    G = np.asfortranarray(G, dtype=np.float64)
+    subj = np.ascontiguousarray(subject_rows, dtype=np.int32)
+    o2s = np.ascontiguousarray(obs_to_subject, dtype=np.int32)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
+    end = bed.m if snp_end is None else int(snp_end)
+    w = end - int(snp_begin)
+    out = {k: np.zeros(w) for k in ("beta", "se", "p", "log10p", "maf")}
+    tested = np.zeros(w, dtype=np.int32)
+    rc = lib().orc_stcg_scan(_ptr(bed.rows), bed.n, bed.stride, _ptr(G), G.shape[0], _ptr(subj),
+                             _ptr(o2s), len(y), _ptr(y), _ptr(X), X.shape[1], vg, vpe, ve,
+                             min_maf, int(snp_begin), end, _ptr(out["beta"]), _ptr(out["se"]),
+                             _ptr(out["p"]), _ptr(out["log10p"]), _ptr(out["maf"]), _ptr(tested))
+    if rc != 0:
+        raise RuntimeError(f"oracle stcg_scan failed ({rc})")
+    out["tested"] = tested.astype(bool)
+    return out
 
 
 def kinship_batch_fixture(n=37, m=1031, seed=8128, rows=None, widths=(1, 7, 41)):

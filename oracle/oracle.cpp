@@ -1348,3 +1348,108 @@ int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_sn
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- scanSTCG
+extern "C" {
+
+// src/models/repeatability_scan_stcg.cpp:42-140 (scan_stcg_with_grm) over SNPs
+// [snp_begin, snp_end) of the packed rows; dense FP64, one LDLT solve per SNP as written.
+int orc_stcg_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const double* G, int64_t q,
+                  const int32_t* subject_rows, const int32_t* obs_to_subject, int64_t n_obs,
+                  const double* y, const double* X, int64_t p, double vg, double vpe, double ve,
+                  double min_maf, int64_t snp_begin, int64_t snp_end, double* beta, double* se,
+                  double* pval, double* log10p, double* maf_out, int32_t* tested) {
+    (void)n_fam;
+    std::vector<double> D(q, 0.0), K(q * q);
+    for (int64_t i = 0; i < n_obs; ++i) D[obs_to_subject[i]] += 1.0;
+    for (int64_t c = 0; c < q; ++c)
+        for (int64_t r = 0; r < q; ++r) K[r + c * q] = vg * G[r + c * q] + (r == c ? vpe : 0.0);
+    std::vector<double> L, Dl;
+    if (!ldlt(K.data(), q, L, Dl)) return -1;
+    std::vector<double> M(q * q, 0.0);
+    for (int64_t c = 0; c < q; ++c) {
+        M[c + c * q] = 1.0;
+        ldlt_solve(L, Dl, q, M.data() + c * q);
+    }
+    for (int64_t s2 = 0; s2 < q; ++s2) M[s2 + s2 * q] += D[s2] / ve;
+    std::vector<double> LM, DM;
+    if (!ldlt(M.data(), q, LM, DM)) return -2;
+    auto woodbury = [&](const double* v, double* out) {
+        std::vector<double> z(q, 0.0);
+        for (int64_t i = 0; i < n_obs; ++i) z[obs_to_subject[i]] += v[i];
+        ldlt_solve(LM, DM, q, z.data());
+        for (int64_t i = 0; i < n_obs; ++i) out[i] = v[i] / ve - z[obs_to_subject[i]] / (ve * ve);
+    };
+    std::vector<double> Vy(n_obs), VX(n_obs * p);
+    woodbury(y, Vy.data());
+    for (int64_t a = 0; a < p; ++a) woodbury(X + a * n_obs, VX.data() + a * n_obs);
+    std::vector<double> XtVX(p * p, 0.0), Xty(p, 0.0);
+    for (int64_t a = 0; a < p; ++a) {
+        for (int64_t b = 0; b < p; ++b)
+            for (int64_t i = 0; i < n_obs; ++i) XtVX[a + b * p] += X[i + a * n_obs] * VX[i + b * n_obs];
+        for (int64_t i = 0; i < n_obs; ++i) Xty[a] += X[i + a * n_obs] * Vy[i];
+    }
+    std::vector<double> LX, DX;
+    if (p > 0 && !ldlt(XtVX.data(), p, LX, DX)) return -3;
+    std::vector<double> bh(Xty);
+    if (p > 0) ldlt_solve(LX, DX, p, bh.data());
+    std::vector<double> resid(n_obs), Py(n_obs);
+    for (int64_t i = 0; i < n_obs; ++i) {
+        double fit = 0.0;
+        for (int64_t a = 0; a < p; ++a) fit += X[i + a * n_obs] * bh[a];
+        resid[i] = y[i] - fit;
+    }
+    woodbury(resid.data(), Py.data());
+    std::vector<double> g(n_obs), Vg(n_obs), t(p);
+    for (int64_t j = snp_begin; j < snp_end; ++j) {
+        const int64_t o = j - snp_begin;
+        const uint8_t* row = bed + j * stride;
+        double sum_g = 0.0;
+        int valid_n = 0;
+        for (int64_t i = 0; i < n_obs; ++i) {
+            const int code = code_at(row, subject_rows[obs_to_subject[i]]);
+            const float val = kLookup[code];
+            g[i] = val;
+            if (!std::isnan(val)) {
+                sum_g += val;
+                ++valid_n;
+            } else {
+                g[i] = 0.0;
+            }
+        }
+        tested[o] = 0;
+        beta[o] = se[o] = pval[o] = log10p[o] = NAN;
+        double maf = valid_n > 0 ? sum_g / (2.0 * valid_n) : 0.0;
+        if (maf > 0.5) maf = 1.0 - maf;
+        maf_out[o] = maf;
+        if (valid_n < 10) continue;
+        if (maf < min_maf) continue;
+        const double gm = sum_g / valid_n;
+        for (int64_t i = 0; i < n_obs; ++i) g[i] -= gm;
+        double score = 0.0;
+        for (int64_t i = 0; i < n_obs; ++i) score += g[i] * Py[i];
+        woodbury(g.data(), Vg.data());
+        for (int64_t a = 0; a < p; ++a) {
+            t[a] = 0.0;
+            for (int64_t i = 0; i < n_obs; ++i) t[a] += X[i + a * n_obs] * Vg[i];
+        }
+        if (p > 0) ldlt_solve(LX, DX, p, t.data());
+        double var = 0.0;
+        for (int64_t i = 0; i < n_obs; ++i) {
+            double pg = Vg[i];
+            for (int64_t a = 0; a < p; ++a) pg -= VX[i + a * n_obs] * t[a];
+            var += g[i] * pg;
+        }
+        if (var < 1e-15) continue;
+        const double z = score / std::sqrt(var);
+        const double pv = std::erfc(std::abs(z) / std::sqrt(2.0));
+        tested[o] = 1;
+        beta[o] = score / var;
+        se[o] = 1.0 / std::sqrt(var);
+        pval[o] = pv;
+        log10p[o] = (pv > 0.0 && pv <= 1.0) ? -std::log10(pv) : (pv > 1.0 ? 0.0 : 300.0);
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -165,6 +165,14 @@ int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_sn
                  const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
                  double* a_ind_out, double* pe_ind_out);
 
+/* src/models/repeatability_scan_stcg.cpp:42-140 (scan_stcg_with_grm) with a given q x q
+ * subject GRM G (column-major) for SNPs [snp_begin, snp_end); maf_out = folded MAF. */
+int orc_stcg_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const double* G, int64_t q,
+                  const int32_t* subject_rows, const int32_t* obs_to_subject, int64_t n_obs,
+                  const double* y, const double* X, int64_t p, double vg, double vpe, double ve,
+                  double min_maf, int64_t snp_begin, int64_t snp_end, double* beta, double* se,
+                  double* pval, double* log10p, double* maf_out, int32_t* tested);
+
 #ifdef __cplusplus
 }
 #endif

@@ -141,3 +141,35 @@ def test_oracle_stcg_runs_and_recovers_scale():
     assert 0.3 < total / np.var(d["y"]) < 3.0
     assert np.isfinite(res["logl"])
     assert np.all(pe == 0)
+
+
+def test_oracle_stcg_scan_matches_dense_formula():
+    """scan_stcg_with_grm restated (Woodbury through M = K^-1 + D / ve) equals the same test
+    computed with the dense record-level V = Zr K Zr^T + ve I."""
+    from cosmicscanner_b200 import synth
+
+    d = synth.repeatability_cohort(80, 60, 17, max_records=3)
+    n, m = d["n"], d["m"]
+    ref = oracle.Bed(d["bed"][3:].reshape(m, -1), n)
+    subj = np.arange(n, dtype=np.int32)
+    o2s = d["rec_to_row"]
+    y, X = d["y"], d["X"]
+    Zs = ref.dense_z(None, None)
+    G = Zs @ Zs.T / m
+    vg, vpe, ve = 0.4, 0.25, 0.6
+    o = oracle.stcg_scan(ref, G, subj, o2s, y, X, vg, vpe, ve, 0.01)
+    Zr = np.zeros((len(y), n))
+    Zr[np.arange(len(y)), o2s] = 1.0
+    V = Zr @ (vg * G + vpe * np.eye(n)) @ Zr.T + ve * np.eye(len(y))
+    Vi = np.linalg.inv(V)
+    P = Vi - Vi @ X @ np.linalg.solve(X.T @ Vi @ X, X.T @ Vi)
+    rows = d["bed"][3:].reshape(m, -1)
+    for j in np.flatnonzero(o["tested"])[:20]:
+        codes = (rows[j][o2s // 4] >> (2 * (o2s % 4))) & 3
+        val = np.where(codes == 0, 2.0, np.where(codes == 2, 1.0, 0.0))
+        obs = codes != 1
+        gv = np.where(obs, val, 0.0)
+        gv = gv - gv[obs].sum() / obs.sum()
+        score, var = gv @ P @ y, gv @ P @ gv
+        assert abs(o["beta"][j] - score / var) <= 1e-9 * abs(score / var) + 1e-12
+        assert abs(o["se"][j] - 1 / np.sqrt(var)) <= 1e-9 / np.sqrt(var)
