@@ -567,6 +567,33 @@ def stcg_scan(genotypes: Genotypes, G, subject_rows, obs_to_subject, y, X, vg, v
     return out
 
 
+def mvlmm_scan(genotypes: Genotypes, keep, W, D, Uty, UtX, Vg, Ve, snp_begin=0, snp_end=None,
+               precision="fp64") -> dict:
+    """MvLmmEngine::scan(PlinkReader) (src/mvlmm_engine.cpp:756-931) on the GPU with a given
+    null (W: n x r eigenbasis, D: r, U'y: r x d, U'X: r x p, Vg, Ve: d x d).  Per SNP: beta
+    (d), cov (d x d), wald, p, freq, status (0 OK, 1 roundoff, 2 boundary, 3 singular)."""
+    keep = np.ascontiguousarray(keep, dtype=np.int32)
+    W = np.asfortranarray(W, dtype=np.float64)
+    n, r = W.shape
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    Uty = np.asfortranarray(np.asarray(Uty, dtype=np.float64).reshape(r, -1))
+    d = Uty.shape[1]
+    UtX = np.asfortranarray(np.asarray(UtX, dtype=np.float64).reshape(r, -1))
+    Vg = np.asfortranarray(Vg, dtype=np.float64)
+    Ve = np.asfortranarray(Ve, dtype=np.float64)
+    end = genotypes.n_snps if snp_end is None else int(snp_end)
+    m = end - int(snp_begin)
+    beta = np.zeros((m, d))
+    cov = np.zeros((m, d, d))
+    wald, pv, fr = np.zeros(m), np.zeros(m), np.zeros(m)
+    st = np.zeros(m, dtype=np.int32)
+    _check(_abi.lib().cs_mvlmm_scan(genotypes._h, _ptr(keep), n, _ptr(W), r, _ptr(D), _ptr(Uty), d,
+                                    _ptr(UtX), UtX.shape[1], _ptr(Vg), _ptr(Ve), int(snp_begin), end,
+                                    _prec(precision), _ptr(beta), _ptr(cov), _ptr(wald), _ptr(pv),
+                                    _ptr(fr), _ptr(st)))
+    return {"beta": beta, "cov": cov, "wald": wald, "p": pv, "freq": fr, "status": st}
+
+
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
     MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""

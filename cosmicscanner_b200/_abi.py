@@ -56,6 +56,8 @@ _SIGNATURES = {
     "cs_vce_destroy": ([_P], None),
     "cs_stcg_scan": ([_P, _P, _I64, _P, _P, _I64, _P, _P, _I64, _D, _D, _D, _D, _I64, _I64,
                       _P, _P, _P, _P, _P, _P], _I),
+    "cs_mvlmm_scan": ([_P, _P, _I64, _P, _I64, _P, _P, _I64, _P, _I64, _P, _P, _I64, _I64, _I,
+                       _P, _P, _P, _P, _P, _P], _I),
     "cs_server_default_options": ([_P], None),
     "cs_server_create": ([_P, _P, _I64, _P, _P], _I),
     "cs_server_submit": ([_P, _P, _P], _I),

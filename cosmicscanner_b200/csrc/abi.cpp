@@ -43,6 +43,11 @@ void stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_t*
                int64_t p, double vg, double vpe, double ve, double min_maf, int64_t snp_begin,
                int64_t snp_end, double* beta, double* se, double* pvalue, double* log10p,
                double* maf, int32_t* tested);
+void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* Wp, int64_t r,
+                const double* Dv, const double* Uty, int64_t d, const double* UtX, int64_t p,
+                const double* Vg, const double* Ve, int64_t snp_begin, int64_t snp_end,
+                int precision, double* beta, double* cov, double* wald, double* pvalue,
+                double* freq, int32_t* status);
 void server_default_options(cs_server_options* o);
 cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_var,
                          const cs_server_options* opt);
@@ -310,6 +315,18 @@ int cs_stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_
     return guarded([&] {
         cs::stcg_scan(g, G, q, subject_rows, obs_to_subject, n_obs, y, X, p, vg, vpe, ve, min_maf,
                       snp_begin, snp_end, beta, se, pvalue, log10p, maf, tested);
+    });
+}
+
+int cs_mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* W,
+                  int64_t r, const double* D, const double* Uty, int64_t d, const double* UtX,
+                  int64_t p, const double* Vg, const double* Ve, int64_t snp_begin,
+                  int64_t snp_end, int precision, double* beta, double* cov, double* wald,
+                  double* pvalue, double* freq, int32_t* status) {
+    return guarded([&] {
+        require(beta && wald && pvalue && freq && status, "null output");
+        cs::mvlmm_scan(g, keep, n, W, r, D, Uty, d, UtX, p, Vg, Ve, snp_begin, snp_end, precision,
+                       beta, cov, wald, pvalue, freq, status);
     });
 }
 

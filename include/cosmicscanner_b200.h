@@ -223,6 +223,22 @@ int cs_stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_
                  int64_t snp_end, double* beta, double* se, double* pvalue, double* log10p,
                  double* maf, int32_t* tested);
 
+/* Replaces MvLmmEngine::scan(PlinkReader, ...) (src/mvlmm_engine.cpp:756-931, processBlock
+ * :210-396) for SNPs [snp_begin, snp_end) of g, with the null model of prepareFromVce
+ * (:195-207): W (n x r eigenbasis, column-major), D (r), U'y (r x d), U'X (r x p), Vg and Ve
+ * (d x d), all host arrays; keep lists the n analysed samples (rows of W).  Default options of
+ * the reference (centred genotypes, LLT-based Sigma inverses, Wald = b' Schur b, df = d).
+ * Per SNP o: beta[o*d ..] (d), cov[o*d*d ..] (the d x d Var(beta), may be NULL), wald,
+ * pvalue, freq (mean dosage / 2 over observed kept samples), status = 0 OK,
+ * 1 NUMERICAL_ROUNDOFF (covariance clipped), 2 BOUNDARY_SOLUTION, 3 TRUE_SINGULARITY (no
+ * row written by the reference; outputs NaN).  precision selects the genotype rotation:
+ * FP64 decode-GEMM or the int8 tensor-core projection. */
+int cs_mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* W,
+                  int64_t r, const double* D, const double* Uty, int64_t d, const double* UtX,
+                  int64_t p, const double* Vg, const double* Ve, int64_t snp_begin,
+                  int64_t snp_end, int precision, double* beta, double* cov, double* wald,
+                  double* pvalue, double* freq, int32_t* status);
+
 /* ---------------------------------------------------------------- serving loop
  * No reference counterpart (the reference runs one job per process).  A server keeps the
  * packed genotypes resident and answers requests, each the matrix-free LMM job of

@@ -98,6 +98,9 @@ def lib():
                                     C.c_double, C.c_double, C.c_double, C.c_double, _I64, _I64,
                                     _P, _P, _P, _P, _P, _P]
         L.orc_stcg_scan.restype = C.c_int
+        L.orc_mvlmm_scan.argtypes = [_P, _I64, _I64, _P, _I64, _P, _I64, _P, _P, _I64, _P, _I64,
+                                     _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P]
+        L.orc_mvlmm_scan.restype = C.c_int
         _lib = L
     return _lib
 
@@ -268,6 +271,29 @@ def stcg_scan(bed: "Bed", G, subject_rows, obs_to_subject, y, X, vg, vpe, ve, mi
         raise RuntimeError(f"oracle stcg_scan failed ({rc})")
     out["tested"] = tested.astype(bool)
     return out
+
+
+def mvlmm_scan(bed: "Bed", keep, W, D, Uty, UtX, Vg, Ve, snp_begin=0, snp_end=None):
+    """MvLmmEngine::scan(PlinkReader) restated (src/mvlmm_engine.cpp:756-931)."""
+    keep = np.ascontiguousarray(keep, dtype=np.int32)
+    W = np.asfortranarray(W, dtype=np.float64)
+    n, r = W.shape
+    D = np.ascontiguousarray(D, dtype=np.float64)
+    Uty = np.asfortranarray(np.asarray(Uty, dtype=np.float64).reshape(r, -1))
+    d = Uty.shape[1]
+    UtX = np.asfortranarray(np.asarray(UtX, dtype=np.float64).reshape(r, -1))
+    Vg = np.asfortranarray(Vg, dtype=np.float64)
+    Ve = np.asfortranarray(Ve, dtype=np.float64)
+    end = bed.m if snp_end is None else int(snp_end)
+    m = end - int(snp_begin)
+    beta, cov = np.zeros((m, d)), np.zeros((m, d, d))
+    wald, pv, fr = np.zeros(m), np.zeros(m), np.zeros(m)
+    st = np.zeros(m, dtype=np.int32)
+    lib().orc_mvlmm_scan(_ptr(bed.rows), bed.n, bed.stride, _ptr(keep), n, _ptr(W), r, _ptr(D),
+                         _ptr(Uty), d, _ptr(UtX), UtX.shape[1], _ptr(Vg), _ptr(Ve),
+                         int(snp_begin), end, _ptr(beta), _ptr(cov), _ptr(wald), _ptr(pv),
+                         _ptr(fr), _ptr(st))
+    return {"beta": beta, "cov": cov, "wald": wald, "p": pv, "freq": fr, "status": st}
 
 
 def kinship_batch_fixture(n=37, m=1031, seed=8128, rows=None, widths=(1, 7, 41)):

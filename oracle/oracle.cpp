@@ -1453,3 +1453,172 @@ int orc_stcg_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const doubl
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- MvLMM scan
+namespace {
+
+// mvlmm_numerics.h:27-45 / :47-69 with the Jacobi eigensolver: 0 OK, 1 roundoff,
+// 2 boundary, 3 singular.
+int mv_invert(const std::vector<double>& info, int64_t d, std::vector<double>& cov) {
+    for (double v : info)
+        if (!std::isfinite(v)) return 3;
+    std::vector<double> sym(d * d), ev(d), V(d * d);
+    for (int64_t a = 0; a < d; ++a)
+        for (int64_t b = 0; b < d; ++b) sym[a + b * d] = 0.5 * (info[a + b * d] + info[b + a * d]);
+    jacobi_eigh(sym.data(), d, ev.data(), V.data());
+    double mn = ev[0], mx = 0.0;
+    for (double v : ev) {
+        mn = std::min(mn, v);
+        mx = std::max(mx, std::abs(v));
+    }
+    const double tol = 128.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, mx) * d;
+    if (!(mn > tol)) return 3;
+    cov.assign(d * d, 0.0);
+    for (int64_t a = 0; a < d; ++a)
+        for (int64_t b = 0; b < d; ++b)
+            for (int64_t l = 0; l < d; ++l) cov[a + b * d] += V[a + l * d] * V[b + l * d] / ev[l];
+    for (int64_t a = 0; a < d; ++a)
+        for (int64_t b = a + 1; b < d; ++b) cov[a + b * d] = cov[b + a * d] = 0.5 * (cov[a + b * d] + cov[b + a * d]);
+    return 0;
+}
+
+int mv_condition(std::vector<double>& cov, int64_t d) {
+    for (int64_t a = 0; a < d; ++a)
+        for (int64_t b = a + 1; b < d; ++b) cov[a + b * d] = cov[b + a * d] = 0.5 * (cov[a + b * d] + cov[b + a * d]);
+    std::vector<double> ev(d), V(d * d);
+    jacobi_eigh(cov.data(), d, ev.data(), V.data());
+    double mn = ev[0], mx = 0.0;
+    for (double v : ev) {
+        mn = std::min(mn, v);
+        mx = std::max(mx, std::abs(v));
+    }
+    const double tol = 128.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, mx) * d;
+    if (mn < -tol) return 3;
+    if (mn < 0.0) {
+        std::fill(cov.begin(), cov.end(), 0.0);
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = 0; b < d; ++b)
+                for (int64_t l = 0; l < d; ++l) cov[a + b * d] += V[a + l * d] * V[b + l * d] * std::max(ev[l], 0.0);
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = a + 1; b < d; ++b) cov[a + b * d] = cov[b + a * d] = 0.5 * (cov[a + b * d] + cov[b + a * d]);
+        return 1;
+    }
+    return mn <= tol ? 2 : 0;
+}
+
+// (d x d) inverse of an SPD matrix through LDL^T (Sigma.llt().solve(I) in the reference)
+std::vector<double> spd_inv(const std::vector<double>& A, int64_t d) {
+    std::vector<double> L, D, X(d * d, 0.0);
+    ldlt(A.data(), d, L, D);
+    for (int64_t c = 0; c < d; ++c) {
+        X[c + c * d] = 1.0;
+        ldlt_solve(L, D, d, X.data() + c * d);
+    }
+    return X;
+}
+
+}  // namespace
+
+extern "C" {
+
+// src/mvlmm_engine.cpp:756-931 + processBlock :210-396, default options
+int orc_mvlmm_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const int32_t* keep,
+                   int64_t n, const double* W, int64_t r, const double* Dv, const double* Uty,
+                   int64_t d, const double* UtX, int64_t p, const double* Vg, const double* Ve,
+                   int64_t snp_begin, int64_t snp_end, double* beta, double* cov, double* wald,
+                   double* pvalue, double* freq, int32_t* status) {
+    (void)n_fam;
+    std::vector<std::vector<double>> Si(r);
+    for (int64_t i = 0; i < r; ++i) {
+        std::vector<double> S(d * d);
+        for (int64_t a = 0; a < d * d; ++a) S[a] = Dv[i] * Vg[a] + Ve[a];
+        Si[i] = spd_inv(S, d);
+    }
+    const int64_t pd = p * d;
+    std::vector<double> HXX(pd * pd, 0.0), RHSX(pd, 0.0);
+    for (int64_t i = 0; i < r; ++i) {
+        std::vector<double> siy(d, 0.0);
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = 0; b < d; ++b) siy[a] += Si[i][a + b * d] * Uty[i + b * r];
+        for (int64_t j = 0; j < p; ++j) {
+            for (int64_t k = 0; k < p; ++k)
+                for (int64_t a = 0; a < d; ++a)
+                    for (int64_t b = 0; b < d; ++b)
+                        HXX[(j * d + a) + (k * d + b) * pd] += UtX[i + j * r] * UtX[i + k * r] * Si[i][a + b * d];
+            for (int64_t a = 0; a < d; ++a) RHSX[j * d + a] += UtX[i + j * r] * siy[a];
+        }
+    }
+    std::vector<double> HXXi = pd > 0 ? spd_inv(HXX, pd) : std::vector<double>();
+    std::vector<double> s(n), srot(r);
+    for (int64_t snp = snp_begin; snp < snp_end; ++snp) {
+        const int64_t o = snp - snp_begin;
+        const uint8_t* row = bed + snp * stride;
+        double sum = 0.0;
+        int count = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const float v = kLookup[code_at(row, keep[i])];
+            s[i] = v;
+            if (!std::isnan(v)) {
+                sum += v;
+                ++count;
+            }
+        }
+        const double mean = count > 0 ? sum / count : 0.0;
+        for (int64_t i = 0; i < n; ++i) s[i] = std::isnan(s[i]) ? 0.0 : s[i] - mean;
+        for (int64_t c = 0; c < r; ++c) {
+            double acc = 0.0;
+            for (int64_t i = 0; i < n; ++i) acc += W[i + c * n] * s[i];
+            srot[c] = acc;
+        }
+        std::vector<double> HSS(d * d, 0.0), RHSS(d, 0.0), HXS(pd * d, 0.0);
+        for (int64_t i = 0; i < r; ++i) {
+            const double si = srot[i];
+            std::vector<double> siy(d, 0.0);
+            for (int64_t a = 0; a < d; ++a)
+                for (int64_t b = 0; b < d; ++b) siy[a] += Si[i][a + b * d] * Uty[i + b * r];
+            for (int64_t a = 0; a < d * d; ++a) HSS[a] += si * si * Si[i][a];
+            for (int64_t a = 0; a < d; ++a) RHSS[a] += si * siy[a];
+            for (int64_t j = 0; j < p; ++j)
+                for (int64_t a = 0; a < d; ++a)
+                    for (int64_t b = 0; b < d; ++b)
+                        HXS[(j * d + a) + b * pd] += UtX[i + j * r] * si * Si[i][a + b * d];
+        }
+        std::vector<double> schur(HSS), adj(RHSS);
+        for (int64_t a = 0; a < d; ++a) {
+            for (int64_t b = 0; b < d; ++b) {
+                double acc = 0.0;
+                for (int64_t u = 0; u < pd; ++u)
+                    for (int64_t v = 0; v < pd; ++v) acc += HXS[u + a * pd] * HXXi[u + v * pd] * HXS[v + b * pd];
+                schur[a + b * d] -= acc;
+            }
+            double acc = 0.0;
+            for (int64_t u = 0; u < pd; ++u)
+                for (int64_t v = 0; v < pd; ++v) acc += HXS[u + a * pd] * HXXi[u + v * pd] * RHSX[v];
+            adj[a] -= acc;
+        }
+        freq[o] = mean / 2.0;
+        wald[o] = pvalue[o] = NAN;
+        status[o] = 3;
+        std::vector<double> sinv;
+        if (mv_invert(schur, d, sinv) != 0) continue;
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = a + 1; b < d; ++b) schur[a + b * d] = schur[b + a * d] = 0.5 * (schur[a + b * d] + schur[b + a * d]);
+        std::vector<double> bt(d, 0.0);
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = 0; b < d; ++b) bt[a] += sinv[a + b * d] * adj[b];
+        double w2 = 0.0;
+        for (int64_t a = 0; a < d; ++a)
+            for (int64_t b = 0; b < d; ++b) w2 += bt[a] * schur[a + b * d] * bt[b];
+        if (!std::isfinite(w2) || w2 < 0.0) continue;
+        const int cst = mv_condition(sinv, d);
+        if (cst == 3) continue;
+        status[o] = cst;
+        wald[o] = w2;
+        pvalue[o] = orc_chisq_prob(w2, (int)d);
+        for (int64_t a = 0; a < d; ++a) beta[o * d + a] = bt[a];
+        for (int64_t a = 0; a < d * d; ++a) cov[o * d * d + a] = sinv[a];
+    }
+    return 0;
+}
+
+}  // extern "C"

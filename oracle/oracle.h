@@ -173,6 +173,14 @@ int orc_stcg_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const doubl
                   double min_maf, int64_t snp_begin, int64_t snp_end, double* beta, double* se,
                   double* pval, double* log10p, double* maf_out, int32_t* tested);
 
+/* src/mvlmm_engine.cpp:756-931 (MvLmmEngine::scan(PlinkReader)) with processBlock :210-396
+ * and the checks of src/mvlmm_numerics.h, default options, for SNPs [snp_begin, snp_end). */
+int orc_mvlmm_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const int32_t* keep,
+                   int64_t n, const double* W, int64_t r, const double* Dv, const double* Uty,
+                   int64_t d, const double* UtX, int64_t p, const double* Vg, const double* Ve,
+                   int64_t snp_begin, int64_t snp_end, double* beta, double* cov, double* wald,
+                   double* pvalue, double* freq, int32_t* status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,3 +173,43 @@ def test_oracle_stcg_scan_matches_dense_formula():
         score, var = gv @ P @ y, gv @ P @ gv
         assert abs(o["beta"][j] - score / var) <= 1e-9 * abs(score / var) + 1e-12
         assert abs(o["se"][j] - 1 / np.sqrt(var)) <= 1e-9 / np.sqrt(var)
+
+
+def test_oracle_mvlmm_matches_dense_gls():
+    """MvLmmEngine::scan restated (rotated per-sample Sigma_i^-1 accumulations, Schur
+    complement, Wald = b' Schur b) equals dense multivariate GLS with
+    V = K (x) Vg + I (x) Ve when the eigenbasis is complete."""
+    from cosmicscanner_b200 import synth
+
+    d = synth.cohort(60, 40, 23, missing=0.02, n_causal=10)
+    n, m = d["n"], d["m"]
+    ref = oracle.Bed(d["bed"][3:].reshape(m, -1), n)
+    Zs = ref.dense_z()
+    K = Zs @ Zs.T / m
+    D, W = np.linalg.eigh(K)
+    rng = np.random.default_rng(4)
+    t = 2
+    Y = np.column_stack([d["y"] + 0.5 * rng.standard_normal(n) for _ in range(t)])
+    X = d["X"]
+    Vg = np.array([[0.6, 0.2], [0.2, 0.4]])
+    Ve = np.array([[0.5, 0.1], [0.1, 0.7]])
+    o = oracle.mvlmm_scan(ref, np.arange(n), W, D, W.T @ Y, W.T @ X, Vg, Ve)
+    V = np.kron(K, Vg) + np.kron(np.eye(n), Ve)
+    Vi = np.linalg.inv(V)
+    yv = Y.reshape(-1)  # sample-major, traits inner
+    rows = d["bed"][3:].reshape(m, -1)
+    for j in range(0, m, 7):
+        if o["status"][j] == 3:
+            continue
+        codes = (rows[j][np.arange(n) // 4] >> (2 * (np.arange(n) % 4))) & 3
+        val = np.where(codes == 0, 2.0, np.where(codes == 2, 1.0, 0.0))
+        obs = codes != 1
+        s = np.where(obs, val - val[obs].mean(), 0.0)
+        Xf = np.hstack([np.kron(X, np.eye(t)), np.kron(s[:, None], np.eye(t))])
+        info = Xf.T @ Vi @ Xf
+        bfull = np.linalg.solve(info, Xf.T @ Vi @ yv)
+        cov = np.linalg.inv(info)[-t:, -t:]
+        b = bfull[-t:]
+        assert np.abs(o["beta"][j] - b).max() <= 1e-8 * max(1.0, np.abs(b).max())
+        assert np.abs(o["cov"][j] - cov).max() <= 1e-8 * np.abs(cov).max()
+        assert abs(o["wald"][j] - b @ np.linalg.solve(cov, b)) <= 1e-7 * max(1.0, o["wald"][j])
