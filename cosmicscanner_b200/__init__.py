@@ -594,6 +594,15 @@ def mvlmm_scan(genotypes: Genotypes, keep, W, D, Uty, UtX, Vg, Ve, snp_begin=0, 
     return {"beta": beta, "cov": cov, "wald": wald, "p": pv, "freq": fr, "status": st}
 
 
+def write_assoc_mv_txt(path: str, bim_path: str, results: dict):
+    """Writes `.assoc.mv.txt` (src/models/multivariate_output.cpp:40-70) from mvlmm_scan()."""
+    m, d = results["beta"].shape
+    arr = {k: np.ascontiguousarray(results[k], dtype=np.float64) for k in ("freq", "wald", "p", "beta", "cov")}
+    _check(_abi.lib().cs_write_assoc_mv_txt(path.encode(), bim_path.encode(), m, d,
+                                            _ptr(arr["freq"]), _ptr(arr["wald"]), _ptr(arr["p"]),
+                                            _ptr(arr["beta"]), _ptr(arr["cov"])))
+
+
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
     MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""

@@ -67,6 +67,7 @@ _SIGNATURES = {
     "cs_server_stats": ([_P, _P], _I),
     "cs_server_destroy": ([_P], None),
     "cs_write_assoc_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _I], _I),
+    "cs_write_assoc_mv_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P], _I),
     "cs_profile_enable": ([_I], _I),
     "cs_profile_summary": ([C.c_char_p, C.c_size_t, _P], _I),
     "cs_launch_count": ([_P], _I),

@@ -58,6 +58,9 @@ void server_result(cs_server* sv, int64_t id, int32_t trait, double* sigma2, dou
 void server_release(cs_server* sv, int64_t id);
 void server_stats(cs_server* sv, cs_server_statistics* out);
 void server_destroy(cs_server* sv);
+void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
+                        const double* freq, const double* wald, const double* p, const double* beta,
+                        const double* cov);
 void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                      const double* freq, const double* beta, const double* se, const double* p,
                      const double* log10p, const int32_t* tested, int stcg_columns);
@@ -387,6 +390,14 @@ int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snp
     return guarded([&] {
         cs::write_assoc_txt(out_path, bim_path, n_snps, n_obs, freq, beta, se, pvalue, log10p,
                             tested, stcg_columns);
+    });
+}
+
+int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
+                          const double* freq, const double* wald, const double* pvalue,
+                          const double* beta, const double* cov) {
+    return guarded([&] {
+        cs::write_assoc_mv_txt(out_path, bim_path, n_snps, d, freq, wald, pvalue, beta, cov);
     });
 }
 

@@ -9,6 +9,9 @@
 // samples, N the analysed sample count (src/lmm_engine.cpp:1315-1326).
 // `.stcg.assoc.txt`: src/models/repeatability_scan_stcg.cpp:190-193 header and :138-140 rows
 // (FREQ there is the folded minor-allele frequency, N the subject count).
+// `.assoc.mv.txt`: src/models/multivariate_model.cpp:943-951 header and
+// src/models/multivariate_output.cpp:40-70 rows (WALD_STAT, P, then BETA_t / SE_t per trait,
+// SE = sqrt of the Var(beta) diagonal; a negative or non-finite variance is an error).
 #include <cmath>
 #include <fstream>
 #include <sstream>
@@ -73,6 +76,38 @@ void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps,
             ofs << '\n';
         else
             ofs << "\tNA\tNA\tNA\tNA\tNA\tNA\n";
+    }
+    ofs.flush();
+    if (!ofs) fail(CS_ERR_IO, "Error writing output file: " + std::string(out_path));
+}
+
+void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
+                        const double* freq, const double* wald, const double* p, const double* beta,
+                        const double* cov) {
+    if (!out_path || !bim_path || n_snps < 0 || d < 1 || !freq || !wald || !p || !beta || !cov)
+        fail(CS_ERR_INVALID_ARGUMENT, "write_assoc_mv_txt: null argument");
+    const std::vector<BimRow> bim = read_bim(bim_path);
+    if ((int64_t)bim.size() != n_snps)
+        fail(CS_ERR_INVALID_ARGUMENT, "write_assoc_mv_txt: .bim has " + std::to_string(bim.size()) +
+                                          " variants, results have " + std::to_string(n_snps));
+    std::ofstream ofs(out_path);
+    if (!ofs) fail(CS_ERR_IO, "Cannot open output file: " + std::string(out_path));
+    ofs << "CHR\tSNP\tBP\tA1\tA2\tFREQ\tWALD_STAT\tP";
+    for (int t = 0; t < d; ++t) ofs << "\tBETA_" << (t + 1) << "\tSE_" << (t + 1);
+    ofs << "\n";
+    for (int64_t j = 0; j < n_snps; ++j) {
+        if (std::isnan(p[j])) continue;
+        const BimRow& b = bim[j];
+        ofs << b.chrom << '\t' << b.id << '\t' << b.bp << '\t' << b.a1 << '\t' << b.a2 << '\t'
+            << freq[j] << '\t' << wald[j] << '\t' << p[j];
+        for (int t = 0; t < d; ++t) {
+            const double var = cov[j * d * d + t + (int64_t)t * d];
+            if (!std::isfinite(var) || var < 0.0)
+                fail(CS_ERR_NUMERIC, "mvLMM covariance TRUE_SINGULARITY for SNP " + b.id +
+                                         ": invalid trait variance");
+            ofs << '\t' << beta[j * d + t] << '\t' << std::sqrt(var);
+        }
+        ofs << '\n';
     }
     ofs.flush();
     if (!ofs) fail(CS_ERR_IO, "Error writing output file: " + std::string(out_path));

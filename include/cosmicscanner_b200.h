@@ -320,6 +320,13 @@ int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snp
                        const double* pvalue, const double* log10p, const int32_t* tested,
                        int stcg_columns);
 
+/* `.assoc.mv.txt` of the multivariate model (src/models/multivariate_model.cpp:943-951,
+ * src/models/multivariate_output.cpp:40-70) from cs_mvlmm_scan outputs: per SNP freq, wald,
+ * p, beta (d), cov (d x d); rows with NaN P are skipped; SE_t = sqrt(cov[t][t]). */
+int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
+                          const double* freq, const double* wald, const double* pvalue,
+                          const double* beta, const double* cov);
+
 /* ---------------------------------------------------------------- instrumentation
  * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and
  * PlinkKinshipOperator::BlockProfile (src/kinship_operator.h:55-63): a process-wide count

@@ -74,3 +74,23 @@ def test_chromosome_order_and_bim_reader(tmp_path):
     b = cs.read_bim(str(bim))
     assert list(b["chrom"]) == ["1", "2"] and list(b["bp"]) == [100, 200]
     assert b["a1"] == ["A", "C"] and b["a2"] == ["G", "T"]
+
+
+def test_assoc_mv_txt(tmp_path):
+    """`.assoc.mv.txt` columns (src/models/multivariate_model.cpp:943-951, multivariate_output.cpp:
+    40-70): WALD_STAT, P, then BETA_t / SE_t with SE = sqrt(Var diagonal); NaN-P rows skipped."""
+    bim = tmp_path / "c.bim"
+    bim.write_text("1 a 0 10 A C\n1 b 0 20 G T\n")
+    res = {"freq": np.array([0.25, 0.5]), "wald": np.array([3.5, np.nan]),
+           "p": np.array([0.17, np.nan]), "beta": np.array([[0.1, -0.2], [0, 0]]),
+           "cov": np.array([[[0.04, 0.01], [0.01, 0.09]], [[1, 0], [0, 1]]])}
+    out = tmp_path / "r.assoc.mv.txt"
+    cs.write_assoc_mv_txt(str(out), str(bim), res)
+    lines = out.read_text().strip().split("\n")
+    assert lines[0] == "CHR\tSNP\tBP\tA1\tA2\tFREQ\tWALD_STAT\tP\tBETA_1\tSE_1\tBETA_2\tSE_2"
+    assert lines[1].split("\t") == ["1", "a", "10", "A", "C", "0.25", "3.5", "0.17", "0.1", "0.2",
+                                    "-0.2", "0.3"]
+    assert len(lines) == 2
+    res["cov"][0, 1, 1] = -1.0
+    with pytest.raises(cs.CosmicError):
+        cs.write_assoc_mv_txt(str(out), str(bim), res)
