@@ -145,9 +145,30 @@ struct OmegaWorkspace {
     DeviceBuffer<int32_t> counts;
     DeviceBuffer<int64_t> offsets;
     DeviceBuffer<double> pairs;
+    int64_t total_pairs = 0, have = 0;  // accepted polar pairs: needed in all, drawn so far
+    // the draw in flight: its attempts, count blocks and pair target; the per-block counts
+    // come back to pinned host memory, signalled by `counted`
+    int64_t pending_attempts = 0, pending_blocks = 0, pending_target = 0;
+    int32_t* h_counts = nullptr;
+    int64_t h_counts_cap = 0;
+    cudaEvent_t counted = nullptr;
+    OmegaWorkspace() = default;
+    OmegaWorkspace(const OmegaWorkspace&) = delete;
+    OmegaWorkspace& operator=(const OmegaWorkspace&) = delete;
+    ~OmegaWorkspace();
 };
 void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out, int64_t ld,
                            OmegaWorkspace& ws, cudaStream_t s);
+// The same stream in pieces: seed for total_count normals, draw until pairs_needed pairs are
+// accepted, transform columns [c0, c1) (normals c0 n .. c1 n - 1).
+void omega_begin(uint64_t seed, int64_t total_count, OmegaWorkspace& ws, cudaStream_t s);
+void omega_ensure(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s);
+// omega_ensure in two halves: omega_draw launches the engine and the acceptance count without
+// waiting; omega_accept waits for the count, writes the accepted pairs and tops up if short.
+void omega_draw(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s);
+void omega_accept(OmegaWorkspace& ws, cudaStream_t s);
+void omega_emit(OmegaWorkspace& ws, int64_t n, int64_t c0, int64_t c1, double* d_out, int64_t ld,
+                cudaStream_t s);
 
 // Tensor-core projection for the scan: T[t][c] = sum_i (g_ti - m_t)[observed] B[i][c] over
 // every row of a packed view, m_t = row_mean[t] (kinship_mixed.cu).

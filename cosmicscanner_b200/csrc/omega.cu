@@ -138,11 +138,13 @@ __global__ void k_accept_write(const uint64_t* __restrict__ raw, int64_t attempt
     }
 }
 
-// draw idx of the column-by-column stream -> out[row * ld + col], row = idx % n, col = idx / n
-__global__ void k_polar(const double* __restrict__ pairs, int64_t count, int64_t n, int64_t ld,
-                        double* __restrict__ out) {
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < count;
-         idx += (int64_t)gridDim.x * blockDim.x) {
+// draw idx (first <= idx < first + count) of the column-by-column stream ->
+// out[row * ld + col], row = idx % n, col = idx / n
+__global__ void k_polar(const double* __restrict__ pairs, int64_t first, int64_t count, int64_t n,
+                        int64_t ld, double* __restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t idx = first + e;
         const int64_t p = idx >> 1;
         const double x = pairs[2 * p], y = pairs[2 * p + 1];
         const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
@@ -175,63 +177,114 @@ std::vector<uint64_t> seeded_state(uint64_t seed) {
 
 }  // namespace
 
+// Incremental generation: the stream is seeded once, pairs are accepted in order as the
+// caller asks for them, and column ranges are transformed as soon as their pairs exist, so a
+// caller can start using the first columns while later ones are still being drawn.
+void omega_begin(uint64_t seed, int64_t total_count, OmegaWorkspace& ws, cudaStream_t s) {
+    const std::vector<uint64_t> st = seeded_state(seed);
+    // earlier work on s may still read the buffers that grow here
+    if ((int64_t)ws.pairs.count < 2 * ((total_count + 1) / 2)) CS_CUDA(cudaStreamSynchronize(s));
+    ws.state.resize(kMtN);
+    CS_CUDA(cudaMemcpyAsync(ws.state.get(), st.data(), 8 * kMtN, cudaMemcpyHostToDevice, s));
+    ws.total_pairs = (total_count + 1) / 2;
+    ws.pairs.resize(std::max<int64_t>(2, 2 * ws.total_pairs));
+    ws.have = 0;
+}
+
+OmegaWorkspace::~OmegaWorkspace() {
+    if (counted) cudaEventSynchronize(counted);
+    if (h_counts) cudaFreeHost(h_counts);
+    if (counted) cudaEventDestroy(counted);
+}
+
+void omega_draw(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s) {
+    pairs_needed = std::min(pairs_needed, ws.total_pairs);
+    ws.pending_blocks = 0;
+    if (ws.have >= pairs_needed) return;
+    // acceptance is pi/4 per attempt: draw for 1.3x the missing pairs (a top-up follows in the
+    // rare case that is short).  An even number of draws that is a multiple of 156 keeps the
+    // stream contiguous across calls: each call advances the engine by exactly its outputs.
+    const int64_t want = (int64_t)((pairs_needed - ws.have) * 1.3) + 8192;
+    const int64_t attempts = round_up(want, kMtM / 2);
+    const int64_t blocks = (attempts + kAttemptsPerBlock - 1) / kAttemptsPerBlock;
+    if ((int64_t)ws.raw.count < 2 * attempts || (int64_t)ws.counts.count < blocks ||
+        ws.h_counts_cap < blocks) {
+        CS_CUDA(cudaStreamSynchronize(s));  // earlier draws' kernels may still read them
+        ws.raw.resize(2 * attempts);
+        ws.counts.resize(blocks);
+        ws.offsets.resize(blocks);
+        if (ws.h_counts_cap < blocks) {
+            if (ws.h_counts) CS_CUDA(cudaFreeHost(ws.h_counts));
+            ws.h_counts = nullptr;
+            ws.h_counts_cap = 0;
+            CS_CUDA(cudaMallocHost(&ws.h_counts, 4 * blocks));
+            ws.h_counts_cap = blocks;
+        }
+    }
+    if (!ws.counted) CS_CUDA(cudaEventCreateWithFlags(&ws.counted, cudaEventDisableTiming));
+    {
+        prof::Scope ps("mt19937_64_stream", s, 0.0, 16.0 * attempts);
+        k_mt64<<<1, kMtM, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
+        CS_LAUNCH("mt19937_64_stream");
+    }
+    {
+        prof::Scope ps("polar_accept_count", s, 0.0, 16.0 * attempts);
+        k_accept_count<<<(unsigned)blocks, 256, 0, s>>>(ws.raw.get(), attempts, ws.counts.get());
+        CS_LAUNCH("polar_accept_count");
+    }
+    CS_CUDA(cudaMemcpyAsync(ws.h_counts, ws.counts.get(), 4 * blocks, cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaEventRecord(ws.counted, s));
+    ws.pending_attempts = attempts;
+    ws.pending_blocks = blocks;
+    ws.pending_target = pairs_needed;
+}
+
+void omega_accept(OmegaWorkspace& ws, cudaStream_t s) {
+    while (ws.pending_blocks > 0) {
+        const int64_t blocks = ws.pending_blocks, attempts = ws.pending_attempts;
+        CS_CUDA(cudaEventSynchronize(ws.counted));
+        std::vector<int64_t> off(blocks);
+        int64_t run = ws.have;
+        for (int64_t b = 0; b < blocks; ++b) {
+            off[b] = run;
+            run += ws.h_counts[b];
+        }
+        CS_CUDA(cudaMemcpyAsync(ws.offsets.get(), off.data(), 8 * blocks, cudaMemcpyHostToDevice, s));
+        {
+            prof::Scope ps("polar_accept_write", s, 0.0, 16.0 * attempts);
+            k_accept_write<<<(unsigned)blocks, 256, 0, s>>>(ws.raw.get(), attempts, ws.offsets.get(),
+                                                            ws.total_pairs, ws.pairs.get());
+            CS_LAUNCH("polar_accept_write");
+        }
+        ws.have = run;
+        omega_draw(ws, ws.pending_target, s);  // a top-up when this draw fell short
+    }
+}
+
+void omega_ensure(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s) {
+    omega_draw(ws, pairs_needed, s);
+    omega_accept(ws, s);
+}
+
+// Normals [c0 n, c1 n) of the column-by-column stream -> columns c0 .. c1 - 1 of d_out.
+void omega_emit(OmegaWorkspace& ws, int64_t n, int64_t c0, int64_t c1, double* d_out, int64_t ld,
+                cudaStream_t s) {
+    const int64_t first = c0 * n, count = (c1 - c0) * n;
+    if (count <= 0) return;
+    prof::Scope ps("polar_pairs", s, 0.0, 16.0 * count);
+    const int blocks = (int)std::min<int64_t>((count + 255) / 256, 32LL * num_sms());
+    k_polar<<<std::max(blocks, 1), 256, 0, s>>>(ws.pairs.get(), first, count, n, ld, d_out);
+    CS_LAUNCH("polar_pairs");
+}
+
 // Omega (n x cols, written row-major with leading dimension ld) on the device.
 void generate_omega_device(uint64_t seed, int64_t n, int64_t cols, double* d_out, int64_t ld,
                            OmegaWorkspace& ws, cudaStream_t s) {
     const int64_t count = n * cols;
     if (count == 0) return;
-    const int64_t pairs = (count + 1) / 2;
-    // seeded state (mt19937_64 seeding recurrence)
-    const std::vector<uint64_t> st = seeded_state(seed);
-    ws.state.resize(kMtN);
-    CS_CUDA(cudaMemcpyAsync(ws.state.get(), st.data(), 8 * kMtN, cudaMemcpyHostToDevice, s));
-    ws.pairs.resize(2 * pairs);
-    int64_t have = 0;
-    // acceptance is pi/4 per attempt: draw for 1.3x the needed attempts, then top up
-    int64_t want_attempts = (int64_t)(pairs * 1.3) + 8192;
-    while (have < pairs) {
-        // an even number of draws that is a multiple of 156 keeps the stream contiguous
-        // across top-ups (each call advances the engine by exactly its outputs)
-        const int64_t attempts = round_up(want_attempts, kMtM / 2);
-        const int64_t blocks = (attempts + kAttemptsPerBlock - 1) / kAttemptsPerBlock;
-        ws.raw.resize(2 * attempts);
-        ws.counts.resize(blocks);
-        ws.offsets.resize(blocks);
-        {
-            prof::Scope ps("mt19937_64_stream", s, 0.0, 16.0 * attempts);
-            k_mt64<<<1, kMtM, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
-            CS_LAUNCH("mt19937_64_stream");
-        }
-        {
-            prof::Scope ps("polar_accept_count", s, 0.0, 16.0 * attempts);
-            k_accept_count<<<(unsigned)blocks, 256, 0, s>>>(ws.raw.get(), attempts, ws.counts.get());
-            CS_LAUNCH("polar_accept_count");
-        }
-        std::vector<int32_t> c(blocks);
-        CS_CUDA(cudaMemcpyAsync(c.data(), ws.counts.get(), 4 * blocks, cudaMemcpyDeviceToHost, s));
-        CS_CUDA(cudaStreamSynchronize(s));
-        std::vector<int64_t> off(blocks);
-        int64_t run = have;
-        for (int64_t b = 0; b < blocks; ++b) {
-            off[b] = run;
-            run += c[b];
-        }
-        CS_CUDA(cudaMemcpyAsync(ws.offsets.get(), off.data(), 8 * blocks, cudaMemcpyHostToDevice, s));
-        {
-            prof::Scope ps("polar_accept_write", s, 0.0, 16.0 * attempts);
-            k_accept_write<<<(unsigned)blocks, 256, 0, s>>>(ws.raw.get(), attempts,
-                                                            ws.offsets.get(), pairs, ws.pairs.get());
-            CS_LAUNCH("polar_accept_write");
-        }
-        have = run;
-        want_attempts = (int64_t)((pairs - std::min(have, pairs)) * 1.3) + 8192;
-    }
-    {
-        prof::Scope ps("polar_pairs", s, 0.0, 16.0 * count);
-        const int blocks = (int)std::min<int64_t>((count + 255) / 256, 32LL * num_sms());
-        k_polar<<<std::max(blocks, 1), 256, 0, s>>>(ws.pairs.get(), count, n, ld, d_out);
-        CS_LAUNCH("polar_pairs");
-    }
+    omega_begin(seed, count, ws, s);
+    omega_ensure(ws, ws.total_pairs, s);
+    omega_emit(ws, n, 0, cols, d_out, ld, s);
 }
 
 void mt64_seed_device(uint64_t seed, uint64_t* d_state, cudaStream_t s) {
