@@ -84,6 +84,7 @@ struct PassArgs {
     int n_tiles, n_ctiles, n_splits;
     int kb_total, kb_per_split;  // K-blocks of the contraction, per slice
     int kc, kp;                  // column tile width, padded column count
+    int kc_last;                 // width of the last column tile (a multiple of 16, <= kc)
     const double* mu;            // rows pass: mu_t per SNP row (epilogue)
     const double* inv_f;         // samples pass: 1 / quantisation factor per column
     double* part;                // [n_splits][kp][ld] FP64 slice partials
@@ -110,7 +111,7 @@ __device__ __forceinline__ void decode_word(uint32_t w, uint4& dos, uint4& mis) 
 template <bool ROWS>
 __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
-             PassArgs P) {
+             const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
     using L = Layout<ROWS>;
     constexpr int ST = L::kTmaStages, SD = kDecStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
@@ -159,18 +160,24 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         kb0 = split * P.kb_per_split;
         kb1 = min(P.kb_total, kb0 + P.kb_per_split);
     };
+    // columns [ct kc, ct kc + w) of the padded kp; only the last tile may be narrower
+    auto width = [&](int ct) { return ct == P.n_ctiles - 1 ? P.kc_last : kc; };
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (elect_one()) {
             prefetch_tensormap(&tm_a);
             prefetch_tensormap(&tm_b);
-            const uint32_t bytes = (uint32_t)(kPackedBytes + L::kPieces * kc * 128);
+            prefetch_tensormap(&tm_bt);
             uint32_t j = 0;
             bool ok = true;
             for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
+                const int w = width(ct);
+                // the narrower last tile has its own map (box of kc_last rows)
+                const CUtensorMap* mb = ct == P.n_ctiles - 1 ? &tm_bt : &tm_b;
+                const uint32_t bytes = (uint32_t)(kPackedBytes + L::kPieces * w * 128);
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST;
                     if (!(ok = mbar_wait(&empty_t[s], ((j / ST) & 1) ^ 1, P.status, kTimeoutTma))) break;
@@ -181,7 +188,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                     else
                         tma_load_2d(smem + L::p(s), &tm_a, tile * 32, kb * kKBlock, &full_t[s]);
                     for (int q = 0; q < L::kPieces; ++q)
-                        tma_load_2d(smem + L::b(s) + q * kc * 128, &tm_b, kb * kKBlock,
+                        tma_load_2d(smem + L::b(s) + q * w * 128, mb, kb * kKBlock,
                                     q * kp + ct * kc, &full_t[s]);
                 }
             }
@@ -194,19 +201,22 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         if (elect_one()) {
             // s8 x s8 -> s32; rows pass: K-major A (SNP rows x samples); samples pass:
             // MN-major A (the same tile read as samples x SNPs)
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
-                                   ((uint32_t)((3 * kc) >> 3) << 17) | ((uint32_t)(kTile >> 4) << 24);
+            // (N = 3 w: the three pieces of a column tile side by side)
+            const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
+                                    ((uint32_t)(kTile >> 4) << 24);
             uint32_t j = 0;
             int ui = 0;
             bool ok = true;
             for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
+                const int w = width(ct);
+                const uint32_t idesc = idesc0 | ((uint32_t)((3 * w) >> 3) << 17);
                 const int buf = ui % NB;
                 if (!(ok = mbar_wait(&acc_empty[buf], ((ui / NB) & 1) ^ 1, P.status, kTimeoutMma))) break;
                 tc_fence_after();
                 const uint32_t acc_main = tmem_base + buf * L::kAccStride;
-                const uint32_t acc_miss = ROWS ? acc_main + 3 * kc : acc_main;
+                const uint32_t acc_miss = ROWS ? acc_main + 3 * w : acc_main;
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST, d = j % SD;
                     if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutMma))) break;
@@ -215,7 +225,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                     const uint32_t a = smem_addr(smem + L::a(d));
                     const uint32_t am = smem_addr(smem + L::am(d));
                     const uint32_t b = smem_addr(smem + L::b(s));
-                    const uint32_t bm = ROWS ? b : b + 3 * kc * 128;
+                    const uint32_t bm = ROWS ? b : b + 3 * w * 128;
 #pragma unroll
                     for (int ks = 0; ks < kKBlock / 32; ++ks) {
                         const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
@@ -284,17 +294,18 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
             const uint32_t tb = tmem_base + buf * L::kAccStride + ((uint32_t)(32 * q) << 16);
             const double mu = ROWS ? P.mu[row] : 0.0;
+            const int w = width(ct);
             double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
-            for (int c0 = 0; c0 < kc; c0 += 16) {
+            for (int c0 = 0; c0 < w; c0 += 16) {
                 int32_t m1[16], m2[16], m3[16];
                 tmem_ld16i(tb + c0, m1);
-                tmem_ld16i(tb + kc + c0, m2);
-                tmem_ld16i(tb + 2 * kc + c0, m3);
+                tmem_ld16i(tb + w + c0, m2);
+                tmem_ld16i(tb + 2 * w + c0, m3);
                 if (ROWS) {
                     int32_t x1[16], x2[16], x3[16];
-                    tmem_ld16i(tb + 3 * kc + c0, x1);
-                    tmem_ld16i(tb + 4 * kc + c0, x2);
-                    tmem_ld16i(tb + 5 * kc + c0, x3);
+                    tmem_ld16i(tb + 3 * w + c0, x1);
+                    tmem_ld16i(tb + 4 * w + c0, x2);
+                    tmem_ld16i(tb + 5 * w + c0, x3);
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
@@ -854,6 +865,7 @@ struct MixedWorkspace {
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
     DeviceBuffer<unsigned long long> max1, max_w, max_muw;
     CUtensorMap tm_b1{}, tm_b2{}, tm_b2h{};
+    CUtensorMap tm_b1t{}, tm_b2t{};  // boxes of the last column tile's width
     const void* tm_b1_base = nullptr;
     const void* tm_b2_base = nullptr;
     const void* tm_b2h_base = nullptr;
@@ -919,15 +931,24 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
 }
 
 struct Tiling {
-    int n_ctiles, kc;
+    int n_ctiles, kc, kc_last;
     int64_t kp;
 };
 
-Tiling tiling_for(int64_t k) {
+// Column tiles of kMaxKc columns and a last tile of the remainder rounded up to 16 (the MMA's
+// N granularity), so that k = 266 runs 80 + 80 + 80 + 32 columns.  `uniform` (the CTA-pair
+// kernel) gives every tile the same width instead.
+Tiling tiling_for(int64_t k, bool uniform = false) {
     Tiling t;
     t.n_ctiles = (int)((k + kMaxKc - 1) / kMaxKc);
-    t.kc = (int)round_up((k + t.n_ctiles - 1) / t.n_ctiles, 16);
-    t.kp = (int64_t)t.kc * t.n_ctiles;
+    if (uniform || t.n_ctiles == 1) {
+        t.kc = (int)round_up((k + t.n_ctiles - 1) / t.n_ctiles, 16);
+        t.kc_last = t.kc;
+    } else {
+        t.kc = kMaxKc;
+        t.kc_last = (int)round_up(k - (int64_t)(t.n_ctiles - 1) * kMaxKc, 16);
+    }
+    t.kp = (int64_t)t.kc * (t.n_ctiles - 1) + t.kc_last;
     return t;
 }
 
@@ -971,9 +992,10 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
         ws.status.resize(1);
         CS_CUDA(cudaMemset(ws.status.get(), 0, sizeof(int)));
     }
-    const int64_t key = kp * 1000003 + n_pad;
+    const int64_t key = (kp * 1000003 + n_pad) * 131 + tl.kc_last;
     if (ws.tm_b1_base != ws.b1.get() || ws.tm_b1_key != key) {
         ws.tm_b1 = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, tl.kc, true);
+        ws.tm_b1t = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, tl.kc_last, true);
         ws.tm_b1_base = ws.b1.get();
         ws.tm_b1_key = key;
     }
@@ -997,6 +1019,7 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
     P.kb_total = kb;
     P.kb_per_split = kbs;
     P.kc = tl.kc;
+    P.kc_last = tl.kc_last;
     P.kp = (int)kp;
     P.mu = r.mu.get();
     P.part = ws.part.get();
@@ -1006,7 +1029,8 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        k_mixed_pass<true><<<num_sms(), kThreads, Layout<true>::kSmem, s>>>(r.tm, ws.tm_b1, P);
+        k_mixed_pass<true><<<num_sms(), kThreads, Layout<true>::kSmem, s>>>(r.tm, ws.tm_b1,
+                                                                             ws.tm_b1t, P);
         CS_LAUNCH("kinship_rows_tc");
     }
     if (want_max) {
@@ -1029,10 +1053,11 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
 // per-column maxima computed by rows_pass(want_max).
 void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
                   double* Y, int64_t ldy, cudaStream_t s) {
-    const Tiling tl = tiling_for(k);
+    const int64_t tiles = r.n_pad / kTile;
+    const bool pairs = samples_pass_on_pairs() && tiles % 2 == 0 && num_sms() >= 2;
+    const Tiling tl = tiling_for(k, pairs);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(r_pad / kKBlock);
-    const int64_t tiles = n_pad / kTile;
     const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
     const int kbs = (kb + splits - 1) / splits;
     const int nrb = (int)((r_pad + 2047) / 2048);
@@ -1041,9 +1066,10 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     ws.colpart.resize((int64_t)nrb * k);
     ws.inv_f.resize(kp);
     ws.c0.resize(k);
-    const int64_t key = kp * 1000003 + r_pad;
+    const int64_t key = (kp * 1000003 + r_pad) * 131 + tl.kc_last;
     if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
         ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc, true);
+        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc_last, true);
         ws.tm_b2_base = ws.b2.get();
         ws.tm_b2_key = key;
     }
@@ -1063,6 +1089,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     P.kb_total = kb;
     P.kb_per_split = kbs;
     P.kc = tl.kc;
+    P.kc_last = tl.kc_last;
     P.kp = (int)kp;
     P.inv_f = ws.inv_f.get();
     P.part = ws.part.get();
@@ -1071,7 +1098,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        if (samples_pass_on_pairs() && tiles % 2 == 0 && num_sms() >= 2) {
+        if (pairs) {
             // CTA pairs: box of kc / 2 rows for the B halves
             const int64_t hkey = (kp * 1000003 + r_pad) * 131 + tl.kc;
             if (ws.tm_b2h_base != ws.b2.get() || ws.tm_b2h_key != hkey) {
@@ -1095,7 +1122,8 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
             cfg.numAttrs = 1;
             CS_CUDA(cudaLaunchKernelEx(&cfg, k_samples_pass_pair, r.tm, ws.tm_b2h, Pp));
         } else {
-            k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2, P);
+            k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2,
+                                                                                  ws.tm_b2t, P);
         }
         CS_LAUNCH("kinship_samples_tc");
     }

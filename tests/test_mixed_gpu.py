@@ -42,7 +42,7 @@ def test_batch_fixture_mixed():
             assert np.array_equal(again, Y), "mixed apply is not bitwise repeatable"
 
 
-@pytest.mark.parametrize("k", [1, 5, 16, 65, 68, 81, 266])
+@pytest.mark.parametrize("k", [1, 5, 16, 65, 68, 81, 170, 240, 266])
 def test_operator_mixed_random(k):
     d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
     ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
