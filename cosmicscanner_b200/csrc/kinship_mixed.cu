@@ -46,6 +46,10 @@ using namespace sm100;
 constexpr int kTile = 128;        // MMA M, and SNP rows / samples per decoded tile
 constexpr int kKBlock = 128;      // K elements (int8) per stage: one 128-byte swizzle row
 constexpr int kMaxKc = 80;        // column-tile width cap (TMEM: rows pass 6 x 80 columns)
+// samples-pass column-tile cap: 6 B pieces of 48 columns keep a TMA stage at 40 KB, so that
+// four stages fit beside the decode ring (two 65 KB stages at 80 columns left the MMA
+// waiting on L2 latency)
+constexpr int kMaxKcSamples = 48;
 constexpr int kWarps = 14;
 constexpr int kThreads = kWarps * 32;
 constexpr int kDecodeWarp0 = 2, kDecodeWarps = 8;
@@ -59,17 +63,19 @@ constexpr int kPackedBytes = kTile * 32;         // 128 rows x 32 B
 
 // Shared memory: a ring of decoded tiles {dosages, missing indicators} and a deeper ring of
 // TMA stages {packed tile, B pieces}, so that TMA latency is covered independently of the
-// decode buffers.  Rows pass: 3 B pieces, 4 TMA stages, accumulator = 6 kc TMEM columns
-// (main and missing sums kept apart).  Samples pass: 6 B pieces (W and mu o W with one
-// scale), 2 TMA stages, accumulator = 3 kc columns, double-buffered.
+// decode buffers.  Rows pass: 3 B pieces of up to 80 columns, 4 TMA stages, accumulator =
+// 6 kc TMEM columns (main and missing sums kept apart).  Samples pass: 6 B pieces (W and
+// mu o W with one scale) of up to 48 columns, 4 TMA stages, accumulator = 3 kc columns,
+// double-buffered.
 template <bool ROWS>
 struct Layout {
     static constexpr int kPieces = ROWS ? 3 : 6;
-    static constexpr int kTmaStages = ROWS ? 4 : 2;
-    static constexpr int kAccCols = ROWS ? 6 * kMaxKc : 3 * kMaxKc;
+    static constexpr int kMaxW = ROWS ? kMaxKc : kMaxKcSamples;
+    static constexpr int kTmaStages = 4;
+    static constexpr int kAccCols = ROWS ? 6 * kMaxW : 3 * kMaxW;
     static constexpr int kAccBufs = ROWS ? 1 : 2;
     static constexpr uint32_t kAccStride = 256;
-    static constexpr int kBBytes = kPieces * kMaxKc * 128;
+    static constexpr int kBBytes = kPieces * kMaxW * 128;
     static constexpr int kTmaBytes = kBBytes + kPackedBytes;
     static constexpr int kDecBytes = 2 * kATileBytes;
     static constexpr int kSmem = kDecStages * kDecBytes + kTmaStages * kTmaBytes + 1024 + 256;
@@ -79,6 +85,14 @@ struct Layout {
     static __host__ __device__ constexpr int p(int s) { return b(s) + kBBytes; }
     static __host__ __device__ constexpr int bars() { return kDecStages * kDecBytes + kTmaStages * kTmaBytes; }
 };
+
+static_assert(Layout<true>::kSmem <= 227 * 1024 && Layout<false>::kSmem <= 227 * 1024,
+              "mixed pass exceeds shared memory");
+static_assert(Layout<true>::kTmaBytes % 1024 == 0 && Layout<false>::kTmaBytes % 1024 == 0,
+              "TMA stages must keep 1024-byte alignment");
+static_assert(Layout<true>::kAccCols <= (int)kTmemCols &&
+                  Layout<false>::kAccCols <= (int)Layout<false>::kAccStride,
+              "accumulators exceed TMEM");
 
 struct PassArgs {
     int n_tiles, n_ctiles, n_splits;
@@ -935,18 +949,18 @@ struct Tiling {
     int64_t kp;
 };
 
-// Column tiles of kMaxKc columns and a last tile of the remainder rounded up to 16 (the MMA's
-// N granularity), so that k = 266 runs 80 + 80 + 80 + 32 columns.  `uniform` (the CTA-pair
-// kernel) gives every tile the same width instead.
-Tiling tiling_for(int64_t k, bool uniform = false) {
+// Column tiles of max_w columns and a last tile of the remainder rounded up to 16 (the MMA's
+// N granularity), so that k = 266 runs 80 + 80 + 80 + 32 columns in the rows pass.  `uniform`
+// (the CTA-pair kernel) gives every tile the same width instead.
+Tiling tiling_for(int64_t k, int max_w, bool uniform = false) {
     Tiling t;
-    t.n_ctiles = (int)((k + kMaxKc - 1) / kMaxKc);
+    t.n_ctiles = (int)((k + max_w - 1) / max_w);
     if (uniform || t.n_ctiles == 1) {
         t.kc = (int)round_up((k + t.n_ctiles - 1) / t.n_ctiles, 16);
         t.kc_last = t.kc;
     } else {
-        t.kc = kMaxKc;
-        t.kc_last = (int)round_up(k - (int64_t)(t.n_ctiles - 1) * kMaxKc, 16);
+        t.kc = max_w;
+        t.kc_last = (int)round_up(k - (int64_t)(t.n_ctiles - 1) * max_w, 16);
     }
     t.kp = (int64_t)t.kc * (t.n_ctiles - 1) + t.kc_last;
     return t;
@@ -970,7 +984,7 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, int64_t k,
                double* out, int64_t out_ld, bool colmajor, int spow, bool want_max,
                cudaStream_t s) {
-    const Tiling tl = tiling_for(k);
+    const Tiling tl = tiling_for(k, kMaxKc);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(n_pad / kKBlock);
     const int64_t tiles = r_pad / kTile;
@@ -1055,7 +1069,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
                   double* Y, int64_t ldy, cudaStream_t s) {
     const int64_t tiles = r.n_pad / kTile;
     const bool pairs = samples_pass_on_pairs() && tiles % 2 == 0 && num_sms() >= 2;
-    const Tiling tl = tiling_for(k, pairs);
+    const Tiling tl = tiling_for(k, pairs ? kMaxKc : kMaxKcSamples, pairs);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(r_pad / kKBlock);
     const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
