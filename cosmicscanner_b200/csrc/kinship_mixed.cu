@@ -18,10 +18,10 @@
 // against the pieces plus one of the missing-indicator tile (same pieces in the rows pass,
 // the (mu o W) pieces in the samples pass).
 //
-// Kernel structure (one CTA per SM, 14 warps): warp 0 issues TMA loads of the packed tile
-// and of the quantised pieces into a ring of stages; warps 2-9 decode; warp 1 issues the
-// MMAs from one thread into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and
-// write FP64 slice partials.  The decoded tile (SNP rows x samples) serves as a K-major A
+// Kernel structure (one CTA per SM, 15 warps): warp 14 issues TMA loads of the packed
+// tiles (from HBM) into a deep ring of their own, warp 0 those of the quantised pieces (L2
+// resident) into a ring of stages; warps 2-9 decode; warp 1 issues the MMAs from one thread
+// into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.  The decoded tile (SNP rows x samples) serves as a K-major A
 // operand in the rows pass and as an MN-major A operand in the samples pass.  Every wait
 // is bounded; a timeout leaves a status code that the host reports as an error.
 #include <cuda.h>
@@ -46,53 +46,72 @@ using namespace sm100;
 constexpr int kTile = 128;        // MMA M, and SNP rows / samples per decoded tile
 constexpr int kKBlock = 128;      // K elements (int8) per stage: one 128-byte swizzle row
 constexpr int kMaxKc = 80;        // column-tile width cap (TMEM: rows pass 6 x 80 columns)
-// samples-pass column-tile cap: 6 B pieces of 48 columns keep a TMA stage at 40 KB, so that
-// four stages fit beside the decode ring (two 65 KB stages at 80 columns left the MMA
-// waiting on L2 latency)
-constexpr int kMaxKcSamples = 48;
-constexpr int kWarps = 14;
+constexpr int kWarps = 15;
 constexpr int kThreads = kWarps * 32;
 constexpr int kDecodeWarp0 = 2, kDecodeWarps = 8;
 constexpr int kEpiWarp0 = 10;
+constexpr int kPackedWarp = 14;
 constexpr uint32_t kTmemCols = 512;
 constexpr double kBase = 254.0;
-constexpr int kDecStages = 2;
 
 constexpr int kATileBytes = kTile * kKBlock;     // 16 KB
 constexpr int kPackedBytes = kTile * 32;         // 128 rows x 32 B
 
-// Shared memory: a ring of decoded tiles {dosages, missing indicators} and a deeper ring of
-// TMA stages {packed tile, B pieces}, so that TMA latency is covered independently of the
-// decode buffers.  Rows pass: 3 B pieces of up to 80 columns, 4 TMA stages, accumulator =
-// 6 kc TMEM columns (main and missing sums kept apart).  Samples pass: 6 B pieces (W and
-// mu o W with one scale) of up to 48 columns, 4 TMA stages, accumulator = 3 kc columns,
-// double-buffered.
-template <bool ROWS>
+// Shared memory: a ring of decoded tiles {dosages, missing indicators}, a deep ring of
+// packed tiles (HBM latency is the longest, so they are requested furthest ahead) and a ring
+// of B stages (the quantised pieces, re-read by every CTA from L2).  The rows pass has 3 B
+// pieces and two accumulators of 3 kc TMEM columns (main and missing-call sums kept apart);
+// the samples pass has 6 B pieces (W and mu o W with one scale) and one accumulator of 3 kc
+// columns, double-buffered.
+//
+// CTA pairs (cta_group::2): a cluster of two CTAs shares each MMA, M = 256 rows (128 from
+// each CTA's decoded tile) by N = 3 kc, and each CTA holds only half of the B pieces (rows
+// [1.5 kc r, 1.5 kc (r + 1)) of every 3 kc-row set, r = CTA rank).  The tensor core then
+// reads half the B bytes per MAC from each SM's shared memory, which is what bounds the
+// single-CTA MMAs (about 68 bytes of operands per clock per SM); the smaller B stages leave
+// room for wider column tiles and a deeper decode ring, which covers the extra hop of the
+// cross-CTA handshakes.
+// Pipeline depths {column-tile width cap, B stages, packed stages, decode stages}:
+constexpr int kRowsW = 80, kRowsST = 4, kRowsSP = 8, kRowsSD = 2;
+constexpr int kSamplesW = 48, kSamplesST = 3, kSamplesSP = 12, kSamplesSD = 2;
+constexpr int kPairRowsW = 80, kPairRowsST = 4, kPairRowsSP = 8, kPairRowsSD = 4;
+constexpr int kPairSamplesW = 80, kPairSamplesST = 3, kPairSamplesSP = 6, kPairSamplesSD = 3;
+
+template <bool ROWS, bool PAIR>
 struct Layout {
-    static constexpr int kPieces = ROWS ? 3 : 6;
-    static constexpr int kMaxW = ROWS ? kMaxKc : kMaxKcSamples;
-    static constexpr int kTmaStages = 4;
+    static constexpr int kPieces = ROWS ? 3 : 6;  // per column tile, over the pair
+    static constexpr int kMaxW = PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
+    static constexpr int kTmaStages = PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
+    static constexpr int kPackedStages = PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
+    static constexpr int kDecodeStages = PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
     static constexpr int kAccCols = ROWS ? 6 * kMaxW : 3 * kMaxW;
     static constexpr int kAccBufs = ROWS ? 1 : 2;
     static constexpr uint32_t kAccStride = 256;
-    static constexpr int kBBytes = kPieces * kMaxW * 128;
-    static constexpr int kTmaBytes = kBBytes + kPackedBytes;
+    static constexpr int kBBytes = kPieces * kMaxW * 128 / (PAIR ? 2 : 1);  // this CTA's share
+    static constexpr int kTmaBytes = kBBytes;
     static constexpr int kDecBytes = 2 * kATileBytes;
-    static constexpr int kSmem = kDecStages * kDecBytes + kTmaStages * kTmaBytes + 1024 + 256;
+    static constexpr int kDecodeRegion = kDecodeStages * kDecBytes;
+    // barriers: full / empty per B, packed and decode stage, full / empty per accumulator,
+    // `drained`, then the TMEM slot
+    static constexpr int kBarBytes =
+        (2 * (kTmaStages + kPackedStages + kDecodeStages + kAccBufs) + 1) * 8 + 8;
+    static constexpr int kSmem = kDecodeRegion + kTmaStages * kTmaBytes +
+                                 kPackedStages * kPackedBytes + 1024 + kBarBytes;
     static __host__ __device__ constexpr int a(int d) { return d * kDecBytes; }
     static __host__ __device__ constexpr int am(int d) { return d * kDecBytes + kATileBytes; }
-    static __host__ __device__ constexpr int b(int s) { return kDecStages * kDecBytes + s * kTmaBytes; }
-    static __host__ __device__ constexpr int p(int s) { return b(s) + kBBytes; }
-    static __host__ __device__ constexpr int bars() { return kDecStages * kDecBytes + kTmaStages * kTmaBytes; }
+    static __host__ __device__ constexpr int b(int s) { return kDecodeRegion + s * kTmaBytes; }
+    static __host__ __device__ constexpr int p(int s) {
+        return kDecodeRegion + kTmaStages * kTmaBytes + s * kPackedBytes;
+    }
+    static __host__ __device__ constexpr int bars() {
+        return kDecodeRegion + kTmaStages * kTmaBytes + kPackedStages * kPackedBytes;
+    }
+    static_assert(kSmem <= 227 * 1024, "mixed pass exceeds shared memory");
+    static_assert(kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
+    static_assert(ROWS ? kAccCols <= (int)kTmemCols : kAccCols <= (int)kAccStride,
+                  "accumulators exceed TMEM");
+    static_assert(kMaxW % 16 == 0 && kMaxW <= kMaxKc, "column tiles are multiples of 16, at most 80");
 };
-
-static_assert(Layout<true>::kSmem <= 227 * 1024 && Layout<false>::kSmem <= 227 * 1024,
-              "mixed pass exceeds shared memory");
-static_assert(Layout<true>::kTmaBytes % 1024 == 0 && Layout<false>::kTmaBytes % 1024 == 0,
-              "TMA stages must keep 1024-byte alignment");
-static_assert(Layout<true>::kAccCols <= (int)kTmemCols &&
-                  Layout<false>::kAccCols <= (int)Layout<false>::kAccStride,
-              "accumulators exceed TMEM");
 
 struct PassArgs {
     int n_tiles, n_ctiles, n_splits;
@@ -106,35 +125,41 @@ struct PassArgs {
     int* status;
 };
 
-// One packed byte (4 codes) -> 4 int8 dosages and 4 missing indicators via byte permutes
-// of the tables {2, 0, 1, 0} and {0, 1, 0, 0} indexed by the codes.
-__device__ __forceinline__ void decode_byte(uint32_t x, uint32_t& dos, uint32_t& mis) {
-    const uint32_t sel = (x & 3u) | ((x & 0xCu) << 2) | ((x & 0x30u) << 4) | ((x & 0xC0u) << 6);
-    dos = __byte_perm(0x00010002u, 0u, sel);
-    mis = __byte_perm(0x00000100u, 0u, sel);
+// 16 codes (one 32-bit word, code j in bits 2j..2j+1) -> 16 int8 dosages and 16 missing
+// indicators in the interleaved sample order 0 2 4 .. 14 1 3 .. 15 within the group: the
+// even codes, masked in place, are already byte-permute selectors (one nibble each), and
+// so are the odd codes after one shift.  sample_at(p) / position_of(s) convert.
+__device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint4& dos, uint4& mis) {
+    const uint32_t se = w & 0x33333333u, so = (w >> 2) & 0x33333333u;
+    dos.x = __byte_perm(0x00010002u, 0u, se);
+    dos.y = __byte_perm(0x00010002u, 0u, se >> 16);
+    dos.z = __byte_perm(0x00010002u, 0u, so);
+    dos.w = __byte_perm(0x00010002u, 0u, so >> 16);
+    mis.x = __byte_perm(0x00000100u, 0u, se);
+    mis.y = __byte_perm(0x00000100u, 0u, se >> 16);
+    mis.z = __byte_perm(0x00000100u, 0u, so);
+    mis.w = __byte_perm(0x00000100u, 0u, so >> 16);
 }
+// position p (0..15) of the interleaved order -> sample offset in the group, and back
+__host__ __device__ __forceinline__ int sample_at(int p) { return p < 8 ? 2 * p : 2 * (p - 8) + 1; }
+__host__ __device__ __forceinline__ int position_of(int s) { return (s & 1) ? 8 + (s >> 1) : s >> 1; }
 
-// 16 codes (one 32-bit word) -> 16 int8 dosages and 16 indicators.
-__device__ __forceinline__ void decode_word(uint32_t w, uint4& dos, uint4& mis) {
-    decode_byte(w & 0xFFu, dos.x, mis.x);
-    decode_byte((w >> 8) & 0xFFu, dos.y, mis.y);
-    decode_byte((w >> 16) & 0xFFu, dos.z, mis.z);
-    decode_byte(w >> 24, dos.w, mis.w);
-}
-
-template <bool ROWS>
+template <bool ROWS, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
-    using L = Layout<ROWS>;
-    constexpr int ST = L::kTmaStages, SD = kDecStages, NB = L::kAccBufs;
+    using L = Layout<ROWS, PAIR>;
+    constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bars());
-    uint64_t* full_t = bars;              // TMA landed (1 arrival + tx bytes)
-    uint64_t* empty_t = full_t + ST;      // MMAs reading the stage done (commit)
-    uint64_t* full_d = empty_t + ST;      // decoded (one arrival per decode warp)
+    uint64_t* full_t = bars;              // B stage landed (1 arrival + tx bytes)
+    uint64_t* empty_t = full_t + ST;      // MMAs reading the B stage done (commit)
+    uint64_t* full_p = empty_t + ST;      // packed tile landed (1 arrival + tx bytes)
+    uint64_t* empty_p = full_p + SP;      // packed tile decoded (one arrival per decode warp)
+    uint64_t* full_d = empty_p + SP;      // decoded (one arrival per decode warp; pair: the
+                                          // leader's counts both CTAs' warps)
     uint64_t* empty_d = full_d + SD;      // MMAs reading the decoded tile done (commit)
     uint64_t* acc_full = empty_d + SD;    // accumulator ready for the epilogue (commit)
     uint64_t* acc_empty = acc_full + NB;  // accumulator drained (one arrival per epilogue warp)
@@ -143,32 +168,51 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kc = P.kc, kp = P.kp;
+    const uint32_t rank = PAIR ? cluster_ctarank() : 0u;
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
             mbar_init(&full_t[s], 1);
             mbar_init(&empty_t[s], 1);
         }
+        for (int s = 0; s < SP; ++s) {
+            mbar_init(&full_p[s], 1);
+            mbar_init(&empty_p[s], kDecodeWarps);
+        }
         for (int d = 0; d < SD; ++d) {
-            mbar_init(&full_d[d], kDecodeWarps);
+            mbar_init(&full_d[d], (PAIR ? 2 : 1) * kDecodeWarps);
             mbar_init(&empty_d[d], 1);
         }
         for (int b = 0; b < NB; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 4);
+            mbar_init(&acc_empty[b], PAIR ? 8 : 4);
         }
         mbar_init(drained, 1);
         fence_mbar_init();
     }
-    if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
+    if (warp == 1) {
+        if (PAIR)
+            tmem_alloc_pair(tmem_slot, kTmemCols);
+        else
+            tmem_alloc(tmem_slot, kTmemCols);
+    }
     tc_fence_before();
-    __syncthreads();
+    if (PAIR)
+        cluster_sync_all();
+    else
+        __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int units = P.n_tiles * P.n_ctiles * P.n_splits;
+    // A unit is one M tile (pair: two, one per CTA) x one column tile x one K slice; both
+    // CTAs of a pair walk the same units.
+    const int groups = PAIR ? P.n_tiles / 2 : P.n_tiles;
+    const int units = groups * P.n_ctiles * P.n_splits;
+    const int u0 = PAIR ? (int)cluster_id_x() : (int)blockIdx.x;
+    const int ustep = PAIR ? (int)cluster_count_x() : (int)gridDim.x;
     auto unit_coords = [&](int u, int& tile, int& ct, int& split, int& kb0, int& kb1) {
-        tile = u % P.n_tiles;
-        const int rest = u / P.n_tiles;
+        const int g = u % groups;
+        tile = PAIR ? 2 * g + (int)rank : g;
+        const int rest = u / groups;
         ct = rest % P.n_ctiles;
         split = rest / P.n_ctiles;
         kb0 = split * P.kb_per_split;
@@ -176,34 +220,52 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
     };
     // columns [ct kc, ct kc + w) of the padded kp; only the last tile may be narrower
     auto width = [&](int ct) { return ct == P.n_ctiles - 1 ? P.kc_last : kc; };
+    // Waits on barriers that the MMA commits arrive on (pair: multicast from the leader) or
+    // that the other CTA arrives on: pairs poll without suspending (see mbar_poll); the
+    // cluster form also acquires what the other CTA released.
+    auto wait_commit = [&](uint64_t* bar, uint32_t parity, int code) {
+        return PAIR ? mbar_poll(bar, parity, P.status, code) : mbar_wait(bar, parity, P.status, code);
+    };
+    auto wait_peer = [&](uint64_t* bar, uint32_t parity, int code) {
+        return PAIR ? mbar_poll_cluster(bar, parity, P.status, code)
+                    : mbar_wait(bar, parity, P.status, code);
+    };
 
     if (warp == 0) {
-        // ------------------------------------------------------------ TMA producer
+        // ------------------------------------------------------------ TMA producer (B)
         if (elect_one()) {
-            prefetch_tensormap(&tm_a);
             prefetch_tensormap(&tm_b);
             prefetch_tensormap(&tm_bt);
             uint32_t j = 0;
             bool ok = true;
-            for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+            for (int u = u0; u < units && ok; u += ustep) {
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 const int w = width(ct);
-                // the narrower last tile has its own map (box of kc_last rows)
+                // the narrower last tile has its own map (box of kc_last rows, pair: half)
                 const CUtensorMap* mb = ct == P.n_ctiles - 1 ? &tm_bt : &tm_b;
-                const uint32_t bytes = (uint32_t)(kPackedBytes + L::kPieces * w * 128);
+                const uint32_t bytes = (uint32_t)(L::kPieces * w * 128 / (PAIR ? 2 : 1));
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST;
-                    if (!(ok = mbar_wait(&empty_t[s], ((j / ST) & 1) ^ 1, P.status, kTimeoutTma))) break;
+                    if (!(ok = wait_commit(&empty_t[s], ((j / ST) & 1) ^ 1, kTimeoutTma))) break;
                     mbar_arrive_expect_tx(&full_t[s], bytes);
-                    // packed tile: 128 SNP rows x 32 bytes (128 samples)
-                    if (ROWS)
-                        tma_load_2d(smem + L::p(s), &tm_a, kb * 32, tile * kTile, &full_t[s]);
-                    else
-                        tma_load_2d(smem + L::p(s), &tm_a, tile * 32, kb * kKBlock, &full_t[s]);
-                    for (int q = 0; q < L::kPieces; ++q)
-                        tma_load_2d(smem + L::b(s) + q * w * 128, mb, kb * kKBlock,
-                                    q * kp + ct * kc, &full_t[s]);
+                    if (PAIR) {
+                        // half-pieces [p0a p0b p1a p1b p2a p2b] of each set (w / 2 rows each):
+                        // this CTA loads 3 r .. 3 r + 2
+                        const int hw = w / 2;
+#pragma unroll
+                        for (int set = 0; set < L::kPieces / 3; ++set)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const int h = 3 * (int)rank + c, q = h >> 1;
+                                tma_load_2d(smem + L::b(s) + (set * 3 + c) * hw * 128, mb, kb * kKBlock,
+                                            (set * 3 + q) * kp + ct * kc + (h & 1) * hw, &full_t[s]);
+                            }
+                    } else {
+                        for (int q = 0; q < L::kPieces; ++q)
+                            tma_load_2d(smem + L::b(s) + q * w * 128, mb, kb * kKBlock,
+                                        q * kp + ct * kc, &full_t[s]);
+                    }
                 }
             }
             // leave no copy in flight
@@ -211,35 +273,36 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 mbar_wait(&full_t[q % ST], (q / ST) & 1, P.status, kTimeoutTma, 1u << 20);
         }
     } else if (warp == 1) {
-        // ------------------------------------------------------------ MMA issuer
-        if (elect_one()) {
+        // ------------------------------------------------------------ MMA issuer (pair: leader)
+        if ((!PAIR || rank == 0) && elect_one()) {
             // s8 x s8 -> s32; rows pass: K-major A (SNP rows x samples); samples pass:
-            // MN-major A (the same tile read as samples x SNPs)
-            // (N = 3 w: the three pieces of a column tile side by side)
+            // MN-major A (the same tile read as samples x SNPs); N = 3 w (the three pieces
+            // of a column tile side by side), M = 128 (pair: 256)
             const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
-                                    ((uint32_t)(kTile >> 4) << 24);
+                                    ((uint32_t)((PAIR ? 2 : 1) * kTile >> 4) << 24);
             uint32_t j = 0;
             int ui = 0;
             bool ok = true;
-            for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
+            for (int u = u0; u < units && ok; u += ustep, ++ui) {
                 int tile, ct, split, kb0, kb1;
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 const int w = width(ct);
                 const uint32_t idesc = idesc0 | ((uint32_t)((3 * w) >> 3) << 17);
                 const int buf = ui % NB;
-                if (!(ok = mbar_wait(&acc_empty[buf], ((ui / NB) & 1) ^ 1, P.status, kTimeoutMma))) break;
+                if (!(ok = wait_peer(&acc_empty[buf], ((ui / NB) & 1) ^ 1, kTimeoutMma))) break;
                 tc_fence_after();
                 const uint32_t acc_main = tmem_base + buf * L::kAccStride;
                 const uint32_t acc_miss = ROWS ? acc_main + 3 * w : acc_main;
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST, d = j % SD;
                     if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutMma))) break;
-                    if (!(ok = mbar_wait(&full_d[d], (j / SD) & 1, P.status, kTimeoutMma))) break;
+                    if (!(ok = wait_peer(&full_d[d], (j / SD) & 1, kTimeoutMma))) break;
                     tc_fence_after();
                     const uint32_t a = smem_addr(smem + L::a(d));
                     const uint32_t am = smem_addr(smem + L::am(d));
                     const uint32_t b = smem_addr(smem + L::b(s));
-                    const uint32_t bm = ROWS ? b : b + 3 * w * 128;
+                    // samples pass: the (mu o W) set follows the W set (this CTA's share)
+                    const uint32_t bm = ROWS ? b : b + 3 * w * 128 / (PAIR ? 2 : 1);
 #pragma unroll
                     for (int ks = 0; ks < kKBlock / 32; ++ks) {
                         const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
@@ -248,16 +311,34 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                         const uint64_t dm = smem_desc_sw128(am + aoff, 16, 1024);
                         const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
                         const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
-                        mma_i8(acc_main, da, db, idesc, first);
                         // rows pass: separate missing-call sums; samples pass: same columns
-                        mma_i8(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
+                        if (PAIR) {
+                            mma_i8_pair(acc_main, da, db, idesc, first);
+                            mma_i8_pair(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
+                        } else {
+                            mma_i8(acc_main, da, db, idesc, first);
+                            mma_i8(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
+                        }
                     }
-                    mma_commit(&empty_t[s]);
-                    mma_commit(&empty_d[d]);
+                    if (PAIR) {
+                        mma_commit_pair(&empty_t[s], 3);
+                        mma_commit_pair(&empty_d[d], 3);
+                    } else {
+                        mma_commit(&empty_t[s]);
+                        mma_commit(&empty_d[d]);
+                    }
                 }
-                if (ok) mma_commit(&acc_full[buf]);
+                if (ok) {
+                    if (PAIR)
+                        mma_commit_pair(&acc_full[buf], 3);
+                    else
+                        mma_commit(&acc_full[buf]);
+                }
             }
-            mma_commit(drained);
+            if (PAIR)
+                mma_commit_pair(drained, 1);
+            else
+                mma_commit(drained);
             mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
         }
     } else if (warp < kEpiWarp0) {
@@ -268,21 +349,21 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
         uint32_t j = 0;
         bool ok = true;
-        for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+        for (int u = u0; u < units && ok; u += ustep) {
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                const int s = j % ST, d = j % SD;
-                if (!(ok = mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode))) break;
-                if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
-                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(s) + r * 32 + h * 16);
+                const int sp = j % SP, d = j % SD;
+                if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
+                if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
+                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
                 unsigned char* a = smem + L::a(d);
                 unsigned char* am = smem + L::am(d);
                 const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
 #pragma unroll
                 for (int cj = 0; cj < 4; ++cj) {
                     uint4 dos, mis;
-                    decode_word(words[cj], dos, mis);
+                    decode_word_interleaved(words[cj], dos, mis);
                     const int chunk = 4 * h + cj;  // 16 samples per 16-byte chunk
                     const int off = rbase + ((chunk ^ (r & 7)) << 4);
                     *reinterpret_cast<uint4*>(a + off) = dos;
@@ -290,8 +371,44 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&full_d[d]);
+                if (PAIR) {
+                    // the leader's MMA also reads this CTA's half of B: its stage must have
+                    // landed before the arrival below completes the leader's full_d
+                    const int s = j % ST;
+                    if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
+                }
+                if (lane == 0) {
+                    if (PAIR)
+                        mbar_arrive_remote(mapa_shared(&full_d[d], 0));
+                    else
+                        mbar_arrive(&full_d[d]);
+                    mbar_arrive(&empty_p[sp]);  // the packed tile has been read
+                }
             }
+        }
+    } else if (warp == kPackedWarp) {
+        // ------------------------------------------------------------ TMA producer (packed)
+        if (elect_one()) {
+            prefetch_tensormap(&tm_a);
+            uint32_t j = 0;
+            bool ok = true;
+            for (int u = u0; u < units && ok; u += ustep) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int sp = j % SP;
+                    if (!(ok = mbar_wait(&empty_p[sp], ((j / SP) & 1) ^ 1, P.status, kTimeoutTma))) break;
+                    mbar_arrive_expect_tx(&full_p[sp], (uint32_t)kPackedBytes);
+                    // packed tile: 128 SNP rows x 32 bytes (128 samples)
+                    if (ROWS)
+                        tma_load_2d(smem + L::p(sp), &tm_a, kb * 32, tile * kTile, &full_p[sp]);
+                    else
+                        tma_load_2d(smem + L::p(sp), &tm_a, tile * 32, kb * kKBlock, &full_p[sp]);
+                }
+            }
+            // leave no copy in flight
+            for (uint32_t q = (j >= (uint32_t)SP ? j - SP : 0); q < j; ++q)
+                mbar_wait(&full_p[q % SP], (q / SP) & 1, P.status, kTimeoutTma, 1u << 20);
         }
     } else {
         // ------------------------------------------------------------ epilogue
@@ -299,13 +416,16 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         int ui = 0;
         bool ok = true;
         const double ib = 1.0 / kBase, ib2 = 1.0 / (kBase * kBase);
-        for (int u = blockIdx.x; u < units && ok; u += gridDim.x, ++ui) {
+        for (int u = u0; u < units && ok; u += ustep, ++ui) {
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
             const int buf = ui % NB;
-            if (!(ok = mbar_wait(&acc_full[buf], (ui / NB) & 1, P.status, kTimeoutEpilogue))) break;
+            if (!(ok = wait_commit(&acc_full[buf], (ui / NB) & 1, kTimeoutEpilogue))) break;
             tc_fence_after();
-            const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
+            // rows pass: TMEM lane = SNP row; samples pass: lane = position in the decoded
+            // tile, whose samples are interleaved within each group of 16
+            const int lp = 32 * q + lane;
+            const int64_t row = (int64_t)tile * kTile + (ROWS ? lp : (lp & ~15) + sample_at(lp & 15));
             const uint32_t tb = tmem_base + buf * L::kAccStride + ((uint32_t)(32 * q) << 16);
             const double mu = ROWS ? P.mu[row] : 0.0;
             const int w = width(ct);
@@ -316,15 +436,18 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 tmem_ld16i(tb + w + c0, m2);
                 tmem_ld16i(tb + 2 * w + c0, m3);
                 if (ROWS) {
-                    int32_t x1[16], x2[16], x3[16];
-                    tmem_ld16i(tb + 3 * w + c0, x1);
-                    tmem_ld16i(tb + 4 * w + c0, x2);
-                    tmem_ld16i(tb + 5 * w + c0, x3);
+                    // main sums first, then the missing-call sums (fewer live registers)
+                    double mv[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        mv[i] = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                    tmem_ld16i(tb + 3 * w + c0, m1);
+                    tmem_ld16i(tb + 4 * w + c0, m2);
+                    tmem_ld16i(tb + 5 * w + c0, m3);
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
-                        const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
-                        const double xv = (double)x1[i] + (double)x2[i] * ib + (double)x3[i] * ib2;
-                        dst[(int64_t)(c0 + i) * P.ld] = mv + mu * xv;
+                        const double xv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
+                        dst[(int64_t)(c0 + i) * P.ld] = mv[i] + mu * xv;
                     }
                 } else {
 #pragma unroll
@@ -336,243 +459,25 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[buf]);
+            if (lane == 0) {
+                if (PAIR)
+                    mbar_arrive_remote(mapa_shared(&acc_empty[buf], 0));
+                else
+                    mbar_arrive(&acc_empty[buf]);
+            }
         }
     }
     tc_fence_before();
-    __syncthreads();
+    if (PAIR)
+        cluster_sync_all();
+    else
+        __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, kTmemCols);
-    }
-}
-
-// ---------------------------------------------------------------- samples pass on CTA pairs
-// The samples pass with a two-CTA MMA (cta_group::2, a cluster of two CTAs): each CTA decodes
-// its own 128-sample tile of the packed K-block, and loads only half of the right-hand-side
-// pieces (rows [1.5 kc r, 1.5 kc (r + 1)) of each 3 kc-row part, r = CTA rank).  The leader
-// (rank 0) issues M = 256 MMAs that read both CTAs' tiles and halves, so every B byte
-// crosses from L2 once per 256 samples instead of once per 128, and the smaller B stage
-// leaves room for four TMA stages.  Each CTA's TMEM receives its own 128 rows.
-//   decoders (both CTAs) -> leader's full_d (cluster-scope arrive), after their own TMA
-//   stage landed, so a completed full_d also covers both B halves;
-//   leader's MMAs -> commit multicast to both CTAs' empty_t / empty_d / acc_full;
-//   epilogues (both) -> leader's acc_empty.
-struct PairLayout {
-    static constexpr int kTmaStages = 4;
-    static constexpr int kBBytes = 3 * kMaxKc * 128;  // two 1.5 kc-row halves (W, mu o W)
-    static constexpr int kTmaBytes = kBBytes + kPackedBytes;
-    static constexpr int kDecBytes = 2 * kATileBytes;
-    static constexpr int kSmem = kDecStages * kDecBytes + kTmaStages * kTmaBytes + 1024 + 256;
-    static __host__ __device__ constexpr int a(int d) { return d * kDecBytes; }
-    static __host__ __device__ constexpr int am(int d) { return d * kDecBytes + kATileBytes; }
-    static __host__ __device__ constexpr int b(int s) { return kDecStages * kDecBytes + s * kTmaBytes; }
-    static __host__ __device__ constexpr int p(int s) { return b(s) + kBBytes; }
-    static __host__ __device__ constexpr int bars() { return kDecStages * kDecBytes + kTmaStages * kTmaBytes; }
-};
-static_assert(PairLayout::kSmem <= 227 * 1024, "paired samples pass exceeds shared memory");
-static_assert(PairLayout::kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
-
-__global__ void __launch_bounds__(kThreads, 1)
-k_samples_pass_pair(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
-                    PassArgs P) {
-    using L = PairLayout;
-    constexpr int ST = L::kTmaStages, SD = kDecStages, NB = 2;
-    constexpr uint32_t kAccStride = 256;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char* smem = reinterpret_cast<unsigned char*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bars());
-    uint64_t* full_t = bars;
-    uint64_t* empty_t = full_t + ST;
-    uint64_t* full_d = empty_t + ST;      // leader: both CTAs' decoders
-    uint64_t* empty_d = full_d + SD;
-    uint64_t* acc_full = empty_d + SD;
-    uint64_t* acc_empty = acc_full + NB;  // leader: both CTAs' epilogue warps
-    uint64_t* drained = acc_empty + NB;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drained + 1);
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t rank = cluster_ctarank();
-    const int kc = P.kc, kp = P.kp, half = kc / 2;
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < ST; ++q) {
-            mbar_init(&full_t[q], 1);
-            mbar_init(&empty_t[q], 1);
-        }
-        for (int d = 0; d < SD; ++d) {
-            mbar_init(&full_d[d], 2 * kDecodeWarps);
-            mbar_init(&empty_d[d], 1);
-        }
-        for (int b = 0; b < NB; ++b) {
-            mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 8);
-        }
-        mbar_init(drained, 1);
-        fence_mbar_init();
-    }
-    if (warp == 1) tmem_alloc_pair(tmem_slot, kTmemCols);
-    tc_fence_before();
-    cluster_sync_all();
-    tc_fence_after();
-    const uint32_t tmem_base = *tmem_slot;
-
-    const int pairs = P.n_tiles;  // tile pairs (n_tiles of this kernel counts pairs)
-    const int units = pairs * P.n_ctiles * P.n_splits;
-    const int cluster = (int)cluster_id_x(), clusters = (int)cluster_count_x();
-    auto unit_coords = [&](int u, int& tile, int& ct, int& split, int& kb0, int& kb1) {
-        const int pr = u % pairs;
-        const int rest = u / pairs;
-        tile = 2 * pr + (int)rank;
-        ct = rest % P.n_ctiles;
-        split = rest / P.n_ctiles;
-        kb0 = split * P.kb_per_split;
-        kb1 = min(P.kb_total, kb0 + P.kb_per_split);
-    };
-
-    if (warp == 0) {
-        // ------------------------------------------------------------ TMA producer (both)
-        if (elect_one()) {
-            prefetch_tensormap(&tm_a);
-            prefetch_tensormap(&tm_b);
-            const uint32_t bytes = (uint32_t)(kPackedBytes + 6 * half * 128);
-            uint32_t j = 0;
-            bool ok = true;
-            for (int u = cluster; u < units && ok; u += clusters) {
-                int tile, ct, split, kb0, kb1;
-                unit_coords(u, tile, ct, split, kb0, kb1);
-                for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                    const int sg = j % ST;
-                    if (!(ok = mbar_wait(&empty_t[sg], ((j / ST) & 1) ^ 1, P.status, kTimeoutTma))) break;
-                    mbar_arrive_expect_tx(&full_t[sg], bytes);
-                    tma_load_2d(smem + L::p(sg), &tm_a, tile * 32, kb * kKBlock, &full_t[sg]);
-                    // this CTA's half of each part: half-pieces 3 rank .. 3 rank + 2 of
-                    // [p0a p0b p1a p1b p2a p2b] (kc / 2 rows each)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const int h = 3 * (int)rank + c, q = h >> 1;
-                        const int row = q * kp + ct * kc + (h & 1) * half;
-                        tma_load_2d(smem + L::b(sg) + c * half * 128, &tm_b, kb * kKBlock, row,
-                                    &full_t[sg]);
-                        tma_load_2d(smem + L::b(sg) + (3 + c) * half * 128, &tm_b, kb * kKBlock,
-                                    row + 3 * kp, &full_t[sg]);
-                    }
-                }
-            }
-            for (uint32_t q = (j >= (uint32_t)ST ? j - ST : 0); q < j; ++q)
-                mbar_wait(&full_t[q % ST], (q / ST) & 1, P.status, kTimeoutTma, 1u << 20);
-        }
-    } else if (warp == 1) {
-        // ------------------------------------------------------------ MMA issuer (leader)
-        if (rank == 0 && elect_one()) {
-            // s8 x s8 -> s32, MN-major A (samples x SNPs), M = 256 over the pair
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) |
-                                   ((uint32_t)((3 * kc) >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
-            uint32_t j = 0;
-            int ui = 0;
-            bool ok = true;
-            for (int u = cluster; u < units && ok; u += clusters, ++ui) {
-                int tile, ct, split, kb0, kb1;
-                unit_coords(u, tile, ct, split, kb0, kb1);
-                const int buf = ui % NB;
-                if (!(ok = mbar_wait_cluster(&acc_empty[buf], ((ui / NB) & 1) ^ 1, P.status, kTimeoutMma)))
-                    break;
-                tc_fence_after();
-                const uint32_t acc = tmem_base + buf * kAccStride;
-                for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                    const int sg = j % ST, d = j % SD;
-                    if (!(ok = mbar_wait_cluster(&full_d[d], (j / SD) & 1, P.status, kTimeoutMma))) break;
-                    tc_fence_after();
-                    const uint32_t a = smem_addr(smem + L::a(d));
-                    const uint32_t am = smem_addr(smem + L::am(d));
-                    const uint32_t b = smem_addr(smem + L::b(sg));
-                    const uint32_t bm = b + 3 * half * 128;
-#pragma unroll
-                    for (int ks = 0; ks < kKBlock / 32; ++ks) {
-                        const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
-                        const uint64_t da = smem_desc_sw128(a + ks * 4096, 16, 1024);
-                        const uint64_t dm = smem_desc_sw128(am + ks * 4096, 16, 1024);
-                        const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
-                        const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
-                        mma_i8_pair(acc, da, db, idesc, first);
-                        mma_i8_pair(acc, dm, dbm, idesc, 1u);
-                    }
-                    mma_commit_pair(&empty_t[sg], 3);
-                    mma_commit_pair(&empty_d[d], 3);
-                }
-                if (ok) mma_commit_pair(&acc_full[buf], 3);
-            }
-            mma_commit_pair(drained, 1);
-            mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
-        }
-    } else if (warp < kEpiWarp0) {
-        // ------------------------------------------------------------ decoders (both)
-        const int dt = threadIdx.x - kDecodeWarp0 * 32;
-        const int r = dt & 127, h = dt >> 7;
-        const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
-        uint32_t j = 0;
-        bool ok = true;
-        for (int u = cluster; u < units && ok; u += clusters) {
-            int tile, ct, split, kb0, kb1;
-            unit_coords(u, tile, ct, split, kb0, kb1);
-            for (int kb = kb0; kb < kb1; ++kb, ++j) {
-                const int sg = j % ST, d = j % SD;
-                if (!(ok = mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode))) break;
-                if (!(ok = mbar_wait(&full_t[sg], (j / ST) & 1, P.status, kTimeoutDecode))) break;
-                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sg) + r * 32 + h * 16);
-                unsigned char* a = smem + L::a(d);
-                unsigned char* am = smem + L::am(d);
-                const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
-#pragma unroll
-                for (int cj = 0; cj < 4; ++cj) {
-                    uint4 dos, mis;
-                    decode_word(words[cj], dos, mis);
-                    const int chunk = 4 * h + cj;
-                    const int off = rbase + ((chunk ^ (r & 7)) << 4);
-                    *reinterpret_cast<uint4*>(a + off) = dos;
-                    *reinterpret_cast<uint4*>(am + off) = mis;
-                }
-                fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) mbar_arrive_remote(mapa_shared(&full_d[d], 0));
-            }
-        }
-    } else {
-        // ------------------------------------------------------------ epilogue (both)
-        const int q = warp & 3;
-        int ui = 0;
-        bool ok = true;
-        const double ib = 1.0 / kBase, ib2 = 1.0 / (kBase * kBase);
-        for (int u = cluster; u < units && ok; u += clusters, ++ui) {
-            int tile, ct, split, kb0, kb1;
-            unit_coords(u, tile, ct, split, kb0, kb1);
-            const int buf = ui % NB;
-            if (!(ok = mbar_wait(&acc_full[buf], (ui / NB) & 1, P.status, kTimeoutEpilogue))) break;
-            tc_fence_after();
-            const int64_t row = (int64_t)tile * kTile + 32 * q + lane;
-            const uint32_t tb = tmem_base + buf * kAccStride + ((uint32_t)(32 * q) << 16);
-            double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
-            for (int c0 = 0; c0 < kc; c0 += 16) {
-                int32_t m1[16], m2[16], m3[16];
-                tmem_ld16i(tb + c0, m1);
-                tmem_ld16i(tb + kc + c0, m2);
-                tmem_ld16i(tb + 2 * kc + c0, m3);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
-                    dst[(int64_t)(c0 + i) * P.ld] = mv * P.inv_f[ct * kc + c0 + i];
-                }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive_remote(mapa_shared(&acc_empty[buf], 0));
-        }
-    }
-    tc_fence_before();
-    cluster_sync_all();
-    if (warp == 1) {
-        tc_fence_after();
-        tmem_dealloc_pair(tmem_base, kTmemCols);
+        if (PAIR)
+            tmem_dealloc_pair(tmem_base, kTmemCols);
+        else
+            tmem_dealloc(tmem_base, kTmemCols);
     }
 }
 
@@ -648,8 +553,9 @@ k_col_absmax(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
     }
 }
 
-// Rows-pass operand: B1[q*kp + c][i] (int8 pieces of (x_ic - mean_c) 127 / max_c, i < n_pad)
-// and per-tile sums of the represented values qpart[blockIdx.x][c].
+// Rows-pass operand: B1[q*kp + c][pos(i)] (int8 pieces of (x_ic - mean_c) 127 / max_c, i < n_pad;
+// pos interleaves each group of 16 samples as the decoded tiles do) and per-tile sums of the
+// represented values qpart[blockIdx.x][c].
 __global__ void __launch_bounds__(256)
 k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k, int64_t kp,
                      int64_t n_pad, const double* __restrict__ mean,
@@ -677,9 +583,11 @@ k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n, int64_
             if (i >= n_pad) continue;
             int8_t q1 = 0, q2 = 0, q3 = 0;
             if (c < k && i < n) qs[cc] += quantise3((tile[rr][col] - mc) * f, q1, q2, q3);
-            B[c * n_pad + i] = q1;
-            B[(kp + c) * n_pad + i] = q2;
-            B[(2 * kp + c) * n_pad + i] = q3;
+            // K position of sample i: the decoded tiles interleave each group of 16 samples
+            const int64_t pos = (i & ~(int64_t)15) + position_of((int)(i & 15));
+            B[c * n_pad + pos] = q1;
+            B[(kp + c) * n_pad + pos] = q2;
+            B[(2 * kp + c) * n_pad + pos] = q3;
         }
     }
     for (int cc = 0; cc < 4; ++cc) {
@@ -846,12 +754,14 @@ CUtensorMap make_map_u8(const void* base, uint64_t inner, uint64_t outer, uint64
 // halving the L2->SM bytes of the right-hand-side pieces did not pay for the per-K-block
 // cross-CTA handshake (ncu: tensor pipe 38 % active, membar stalls from the cluster-scope
 // release arrives).  Kept for comparison.
-bool samples_pass_on_pairs() {
+// Both passes run on CTA pairs (cta_group::2) unless CS_B200_CTA_PAIRS=0 selects the
+// single-CTA kernels.
+bool use_cta_pairs() {
     static const bool pairs = [] {
-        const char* v = std::getenv("CS_B200_SAMPLES_PASS");
-        return v && std::strcmp(v, "pair") == 0;
+        const char* v = std::getenv("CS_B200_CTA_PAIRS");
+        return !(v && std::strcmp(v, "0") == 0);
     }();
-    return pairs;
+    return pairs && num_sms() >= 2;
 }
 
 int blocks_for(int64_t work) {
@@ -878,12 +788,11 @@ struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
     DeviceBuffer<unsigned long long> max1, max_w, max_muw;
-    CUtensorMap tm_b1{}, tm_b2{}, tm_b2h{};
+    CUtensorMap tm_b1{}, tm_b2{};
     CUtensorMap tm_b1t{}, tm_b2t{};  // boxes of the last column tile's width
     const void* tm_b1_base = nullptr;
     const void* tm_b2_base = nullptr;
-    const void* tm_b2h_base = nullptr;
-    int64_t tm_b1_key = -1, tm_b2_key = -1, tm_b2h_key = -1;
+    int64_t tm_b1_key = -1, tm_b2_key = -1;
     DeviceBuffer<int> status;
 };
 
@@ -896,22 +805,73 @@ void destroy_mixed(MixedOperator* m) { delete m; }
 
 namespace {
 
+template <bool ROWS, bool PAIR>
+cudaError_t allow_smem() {
+    return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Layout<ROWS, PAIR>::kSmem);
+}
+
 void configure_kernels() {
     static std::once_flag once;
     static cudaError_t err = cudaSuccess;
     std::call_once(once, [] {
-        err = cudaFuncSetAttribute(k_mixed_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   Layout<true>::kSmem);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_mixed_pass<false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       Layout<false>::kSmem);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(k_samples_pass_pair,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       PairLayout::kSmem);
+        err = allow_smem<true, false>();
+        if (err == cudaSuccess) err = allow_smem<false, false>();
+        if (err == cudaSuccess) err = allow_smem<true, true>();
+        if (err == cudaSuccess) err = allow_smem<false, true>();
     });
     check_cuda(err, "configure tensor-core kernels");
+}
+
+// Clusters of two CTAs that can be resident at once (an SM without a partner in its GPC
+// stays idle): the persistent pair kernels launch exactly that many, since clusters beyond
+// it would run as a second wave after the first has finished all its units.
+template <bool ROWS>
+int resident_pairs() {
+    static int cached[64] = {};  // per device ordinal
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    int& n = cached[dev < 64 ? dev : 0];
+    if (n == 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(num_sms() & ~1));
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = Layout<ROWS, true>::kSmem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true>, &cfg));
+        n = std::max(1, std::min(clusters, num_sms() / 2));
+    }
+    return n;
+}
+
+// One CTA per SM, or (PAIR) as many clusters of two CTAs as are resident together.
+template <bool ROWS, bool PAIR>
+void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
+                 const PassArgs& P, cudaStream_t s) {
+    if (PAIR) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * resident_pairs<ROWS>()));
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = Layout<ROWS, true>::kSmem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true>, ta, tb, tbt, P));
+    } else {
+        k_mixed_pass<ROWS, false><<<num_sms(), kThreads, Layout<ROWS, false>::kSmem, s>>>(ta, tb, tbt, P);
+    }
 }
 
 // Per-row statistics: mu_t, exc_t = S_t - mu_t n_t (from code counts c00, c01, c10, c11),
@@ -921,7 +881,8 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     configure_kernels();
     r.R = v.n_rows;
     r.n = v.n_samples;
-    r.r_pad = round_up(std::max<int64_t>(r.R, 1), kTile);
+    // SNP rows padded to 256 as well: the rows pass runs on pairs of 128-row tiles
+    r.r_pad = round_up(std::max<int64_t>(r.R, 1), 2 * kTile);
     // samples padded to 256: the samples pass runs on pairs of 128-sample tiles (packed rows
     // hold a multiple of 256 samples, so the padding tiles read missing codes)
     r.n_pad = round_up(std::max<int64_t>(r.n, 1), 2 * kTile);
@@ -984,11 +945,14 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, int64_t k,
                double* out, int64_t out_ld, bool colmajor, int spow, bool want_max,
                cudaStream_t s) {
-    const Tiling tl = tiling_for(k, kMaxKc);
+    const int64_t tiles = r.r_pad / kTile;
+    const bool pairs = use_cta_pairs() && tiles % 2 == 0;
+    const Tiling tl = tiling_for(k, pairs ? kPairRowsW : kRowsW);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(n_pad / kKBlock);
-    const int64_t tiles = r_pad / kTile;
-    const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    // about 8 units per CTA (pairs: per cluster of two)
+    const int splits = pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
+                             : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
     const int kbs = (kb + splits - 1) / splits;
     const int rt = (int)((n_pad + kPrepRows - 1) / kPrepRows);
     const int nbs = (int)std::min<int64_t>(512, std::max<int64_t>(1, n / 128));
@@ -1006,10 +970,12 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
         ws.status.resize(1);
         CS_CUDA(cudaMemset(ws.status.get(), 0, sizeof(int)));
     }
-    const int64_t key = (kp * 1000003 + n_pad) * 131 + tl.kc_last;
+    // boxes of one column tile's rows (pairs: half of them)
+    const int box = pairs ? tl.kc / 2 : tl.kc, box_last = pairs ? tl.kc_last / 2 : tl.kc_last;
+    const int64_t key = ((kp * 1000003 + n_pad) * 131 + box_last) * 131 + box;
     if (ws.tm_b1_base != ws.b1.get() || ws.tm_b1_key != key) {
-        ws.tm_b1 = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, tl.kc, true);
-        ws.tm_b1t = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, tl.kc_last, true);
+        ws.tm_b1 = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, box, true);
+        ws.tm_b1t = make_map_u8(ws.b1.get(), n_pad, 3 * kp, n_pad, kKBlock, box_last, true);
         ws.tm_b1_base = ws.b1.get();
         ws.tm_b1_key = key;
     }
@@ -1043,8 +1009,10 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        k_mixed_pass<true><<<num_sms(), kThreads, Layout<true>::kSmem, s>>>(r.tm, ws.tm_b1,
-                                                                             ws.tm_b1t, P);
+        if (pairs)
+            launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+        else
+            launch_pass<true, false>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         CS_LAUNCH("kinship_rows_tc");
     }
     if (want_max) {
@@ -1068,11 +1036,12 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
 void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
                   double* Y, int64_t ldy, cudaStream_t s) {
     const int64_t tiles = r.n_pad / kTile;
-    const bool pairs = samples_pass_on_pairs() && tiles % 2 == 0 && num_sms() >= 2;
-    const Tiling tl = tiling_for(k, pairs ? kMaxKc : kMaxKcSamples, pairs);
+    const bool pairs = use_cta_pairs() && tiles % 2 == 0;
+    const Tiling tl = tiling_for(k, pairs ? kPairSamplesW : kSamplesW);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(r_pad / kKBlock);
-    const int splits = choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    const int splits = pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
+                             : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
     const int kbs = (kb + splits - 1) / splits;
     const int nrb = (int)((r_pad + 2047) / 2048);
     ws.b2.resize(6 * kp * r_pad);
@@ -1080,10 +1049,12 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     ws.colpart.resize((int64_t)nrb * k);
     ws.inv_f.resize(kp);
     ws.c0.resize(k);
-    const int64_t key = (kp * 1000003 + r_pad) * 131 + tl.kc_last;
+    // boxes of one column tile's rows (pairs: half of them)
+    const int box = pairs ? tl.kc / 2 : tl.kc, box_last = pairs ? tl.kc_last / 2 : tl.kc_last;
+    const int64_t key = ((kp * 1000003 + r_pad) * 131 + box_last) * 131 + box;
     if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
-        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc, true);
-        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc_last, true);
+        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, box, true);
+        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, box_last, true);
         ws.tm_b2_base = ws.b2.get();
         ws.tm_b2_key = key;
     }
@@ -1112,33 +1083,10 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        if (pairs) {
-            // CTA pairs: box of kc / 2 rows for the B halves
-            const int64_t hkey = (kp * 1000003 + r_pad) * 131 + tl.kc;
-            if (ws.tm_b2h_base != ws.b2.get() || ws.tm_b2h_key != hkey) {
-                ws.tm_b2h = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, tl.kc / 2, true);
-                ws.tm_b2h_base = ws.b2.get();
-                ws.tm_b2h_key = hkey;
-            }
-            PassArgs Pp = P;
-            Pp.n_tiles = (int)(tiles / 2);
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3((unsigned)(num_sms() & ~1));
-            cfg.blockDim = dim3(kThreads);
-            cfg.dynamicSmemBytes = PairLayout::kSmem;
-            cfg.stream = s;
-            cudaLaunchAttribute attr[1];
-            attr[0].id = cudaLaunchAttributeClusterDimension;
-            attr[0].val.clusterDim.x = 2;
-            attr[0].val.clusterDim.y = 1;
-            attr[0].val.clusterDim.z = 1;
-            cfg.attrs = attr;
-            cfg.numAttrs = 1;
-            CS_CUDA(cudaLaunchKernelEx(&cfg, k_samples_pass_pair, r.tm, ws.tm_b2h, Pp));
-        } else {
-            k_mixed_pass<false><<<num_sms(), kThreads, Layout<false>::kSmem, s>>>(r.tm, ws.tm_b2,
-                                                                                  ws.tm_b2t, P);
-        }
+        if (pairs)
+            launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
+        else
+            launch_pass<false, false>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         CS_LAUNCH("kinship_samples_tc");
     }
     {

@@ -197,10 +197,14 @@ __device__ __forceinline__ uint32_t mapa_shared(const void* p, uint32_t rank) {
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_addr(p)), "r"(rank));
     return r;
 }
-// Arrive (release, cluster scope) on an mbarrier given by its shared::cluster address.
+// Arrive on an mbarrier given by its shared::cluster address (the other CTA of a pair), with
+// the arrive's default release semantics.  A cluster-scope release costs the arriving thread
+// some two thousand cycles under load (it waits for the thread's memory operations to be
+// visible cluster-wide); what the pair pipelines hand over is shared memory that only the
+// tensor core reads, which the writer's proxy fence has already ordered, as in the usual
+// cluster pipelines.
 __device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
-                 : "memory");
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
@@ -219,6 +223,50 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity
                                                   int code, uint32_t limit = (1u << 24)) {
     for (uint32_t i = 0; i < limit; ++i) {
         if (mbar_try_wait_cluster(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && *(volatile int*)status != kOk) return false;
+    }
+    atomicCAS(status, kOk, code);
+    return false;
+}
+// Non-suspending forms for barriers that the other CTA of a pair arrives on (a remote arrive
+// or a multicast commit): try_wait may sleep through such an arrival for its whole
+// hardware-defined interval, so these poll with test_wait instead.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_test_wait_cluster(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded polls (as mbar_wait: `limit` polls, then `code` in *status and false).
+__device__ __forceinline__ bool mbar_poll(uint64_t* bar, uint32_t parity, int* status, int code,
+                                          uint32_t limit = (1u << 26)) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        if (mbar_test_wait(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && *(volatile int*)status != kOk) return false;
+    }
+    atomicCAS(status, kOk, code);
+    return false;
+}
+__device__ __forceinline__ bool mbar_poll_cluster(uint64_t* bar, uint32_t parity, int* status,
+                                                  int code, uint32_t limit = (1u << 26)) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        if (mbar_test_wait_cluster(bar, parity)) return true;
         if ((i & 1023u) == 1023u && *(volatile int*)status != kOk) return false;
     }
     atomicCAS(status, kOk, code);
