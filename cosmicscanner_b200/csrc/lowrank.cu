@@ -26,6 +26,17 @@
 #include "linalg_host.h"
 #include "vce_internal.h"
 
+namespace cs {
+// Workspace of the device Cholesky-QR: cuSOLVER buffers and the factorisation status.
+struct QrWorkspace {
+    DeviceBuffer<double> potrf_work;
+    DeviceBuffer<char> trtri_work;
+    std::vector<char> trtri_host;
+    DeviceBuffer<int> info;
+    int64_t k = -1;
+};
+}  // namespace cs
+
 struct cs_lmm {
     int64_t n = 0, p = 0, rank = 0;
     bool prepared = false;
@@ -40,6 +51,7 @@ struct cs_lmm {
     // persistent work buffers (grown on demand, never freed between calls)
     cs::DeviceBuffer<double> omega, sample, q, scratch, gram, small;
     cs::OmegaWorkspace omega_ws;
+    cs::QrWorkspace qr_ws;
     // scan: analysed-sample view of the genotypes and its tensor-core context, cached
     // for repeated scans of the same (genotypes, keep) pair
     uint64_t scan_g_uid = 0;
@@ -76,43 +88,95 @@ namespace {
 
 // ---------------------------------------------------------------- QR
 // Thin QR of Y (n x k row-major) by Cholesky-QR2: two passes of G = Y^T Y, G = R^T R,
-// Y <- Y R^{-1}, with the k x k triangular inverse formed on the host and applied as one
-// DGEMM (a device triangular solve of this shape runs several times slower than the GEMM).
-// A first pass whose Gram matrix is not numerically positive definite is shifted (shifted
-// Cholesky-QR) and a third pass added.  Any orthonormal basis of span(Y) gives the same
+// Y <- Y R^{-1}, with the k x k factor and its triangular inverse formed on the device
+// (cuSOLVER potrf + trtri) and applied as one DGEMM (a device triangular solve of this shape
+// runs several times slower than the GEMM).  A pass whose Gram matrix is not numerically
+// positive definite is factored on the host with a shift (shifted Cholesky-QR) and a third
+// pass added.  Any orthonormal basis of span(Y) gives the same
 // subspace iteration as the reference's HouseholderQR (lmm_engine.cpp:931-941): Q is unique
 // up to column signs, which cancel in Q^T K Q and in U = Q W.  Y is used as scratch; the
 // result is written to Q.
-void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q,
-                 DeviceBuffer<double>& d_gram, cudaStream_t s) {
-    const double one = 1.0, zero = 0.0;
-    d_gram.resize(2 * k * k);
-    double* G = d_gram.get();
-    double* Rinv_d = G + k * k;
+// Strictly lower triangle of a k x k column-major matrix -> 0 (cuSOLVER leaves the Gram's
+// lower half under the factor).
+__global__ void k_zero_lower(double* __restrict__ A, int64_t k) {
+    const int64_t total = k * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x)
+        if (e % k > e / k) A[e] = 0.0;
+}
+
+// One pass with the factor on the host (shifted when the Gram is not numerically positive
+// definite): R^{-1} -> Rinv_d.  Returns false when even the shifted Gram fails.
+bool host_factor_pass(const double* G, int64_t n, int64_t k, double* Rinv_d, bool& shifted,
+                      cudaStream_t s) {
     std::vector<double> g(k * k), R;
+    CS_CUDA(cudaMemcpyAsync(g.data(), G, 8 * k * k, cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    shifted = false;
+    if (!la::cholesky_upper(g, (int)k, R)) {
+        // shifted Cholesky-QR: G + sigma I is safely positive definite
+        double tr = 0.0;
+        for (int64_t j = 0; j < k; ++j) tr += g[j + j * k];
+        const double shift = 11.0 * (double)(n * k + k * (k + 1)) * 2.2e-16 * tr;
+        for (int64_t j = 0; j < k; ++j) g[j + j * k] += shift;
+        if (!la::cholesky_upper(g, (int)k, R)) return false;
+        shifted = true;
+    }
+    const std::vector<double> Rinv = la::upper_inverse(R, (int)k);
+    CS_CUDA(cudaMemcpyAsync(Rinv_d, Rinv.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
+void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q,
+                 DeviceBuffer<double>& d_gram, QrWorkspace& ws, cudaStream_t s) {
+    const double one = 1.0, zero = 0.0;
+    d_gram.resize(k * k);
+    double* G = d_gram.get();
     CS_BLAS(cublasSetStream(blas, s));
+    cusolverDnHandle_t sol = shared_solver();
+    CS_SOLVER(cusolverDnSetStream(sol, s));
+    if (ws.k != k) {
+        int lw = 0;
+        CS_SOLVER(cusolverDnDpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, (int)k, G, (int)k, &lw));
+        ws.potrf_work.resize(std::max(lw, 1));
+        size_t dbytes = 0, hbytes = 0;
+        CS_SOLVER(cusolverDnXtrtri_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, k,
+                                              CUDA_R_64F, G, k, &dbytes, &hbytes));
+        ws.trtri_work.resize(std::max<size_t>(dbytes, 1));
+        ws.trtri_host.resize(std::max<size_t>(hbytes, 1));
+        ws.info.resize(2);
+        ws.k = k;
+    }
     int passes = 2;
     double* src = Y;
     double* dst = Q;
     for (int pass = 0; pass < passes; ++pass) {
         CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, src,
                             (int)k, src, (int)k, &zero, G, (int)k));
-        CS_CUDA(cudaMemcpyAsync(g.data(), G, 8 * k * k, cudaMemcpyDeviceToHost, s));
+        // G = R^T R on the device, then R^{-1} in place (upper triangle)
+        CS_SOLVER(cusolverDnDpotrf(sol, CUBLAS_FILL_MODE_UPPER, (int)k, G, (int)k,
+                                   ws.potrf_work.get(), (int)ws.potrf_work.count, ws.info.get()));
+        int info = 0;
+        CS_CUDA(cudaMemcpyAsync(&info, ws.info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
         CS_CUDA(cudaStreamSynchronize(s));
-        if (!la::cholesky_upper(g, (int)k, R)) {
-            // shifted Cholesky-QR: G + sigma I is safely positive definite
-            double tr = 0.0;
-            for (int64_t j = 0; j < k; ++j) tr += g[j + j * k];
-            const double shift = 11.0 * (double)(n * k + k * (k + 1)) * 2.2e-16 * tr;
-            for (int64_t j = 0; j < k; ++j) g[j + j * k] += shift;
-            if (!la::cholesky_upper(g, (int)k, R))
+        if (info == 0) {
+            CS_SOLVER(cusolverDnXtrtri(sol, CUBLAS_FILL_MODE_UPPER, CUBLAS_DIAG_NON_UNIT, k, CUDA_R_64F,
+                                       G, k, ws.trtri_work.get(), ws.trtri_work.count,
+                                       ws.trtri_host.data(), ws.trtri_host.size(), ws.info.get() + 1));
+            k_zero_lower<<<(unsigned)std::min<int64_t>((k * k + 255) / 256, 1024), 256, 0, s>>>(G, k);
+            CS_LAUNCH("zero_lower");
+        } else {
+            // not numerically positive definite: recompute the Gram and factor it on the host
+            CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)k, (int)n, &one, src,
+                                (int)k, src, (int)k, &zero, G, (int)k));
+            bool shifted = false;
+            if (!host_factor_pass(G, n, k, G, shifted, s))
                 fail(CS_ERR_NUMERIC, "QR of the sketch failed (rank-deficient sketch)");
-            passes = std::min(passes + 1, 4);
+            if (shifted) passes = std::min(passes + 1, 4);
         }
-        const std::vector<double> Rinv = la::upper_inverse(R, (int)k);
-        CS_CUDA(cudaMemcpyAsync(Rinv_d, Rinv.data(), 8 * k * k, cudaMemcpyHostToDevice, s));
         // row-major dst = src R^{-1}  <=>  column-major dst^c = R^{-T} src^c
-        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)k, (int)n, (int)k, &one, Rinv_d,
+        CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)k, (int)n, (int)k, &one, G,
                             (int)k, src, (int)k, &zero, dst, (int)k));
         // the last pass must land in Q
         const bool last = pass + 1 == passes;
@@ -123,7 +187,10 @@ void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q
             CS_CUDA(cudaMemcpyAsync(Q, dst, 8 * n * k, cudaMemcpyDeviceToDevice, s));
         }
     }
+    int tinfo[2] = {0, 0};
+    CS_CUDA(cudaMemcpyAsync(tinfo, ws.info.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CS_CUDA(cudaStreamSynchronize(s));
+    if (tinfo[1] != 0) fail(CS_ERR_NUMERIC, "QR of the sketch failed (singular triangular factor)");
 }
 
 // ---------------------------------------------------------------- eigenvectors
@@ -511,10 +578,10 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     {
         prof::HostScope hs("lowrank_subspace_iteration");
         for (int it = 0; it < 2; ++it) {
-            cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
+            cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s);
             target.apply(q.get(), sk, sk, sample.get(), sk, s);
         }
-        cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, s);
+        cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s);
         target.apply(q.get(), sk, sk, sample.get(), sk, s);
         CS_CUDA(cudaStreamSynchronize(s));
     }

@@ -1,6 +1,7 @@
 // Device memory pool and shared cuBLAS handles.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <cstdint>
 #include <mutex>
@@ -42,6 +43,16 @@ cublasHandle_t shared_blas() {
     if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
     if (!handles[dev] && cublasCreate(&handles[dev]) != CUBLAS_STATUS_SUCCESS)
         fail(CS_ERR_CUDA, "cublasCreate failed");
+    return handles[dev];
+}
+
+cusolverDnHandle_t shared_solver() {
+    thread_local cusolverDnHandle_t handles[kMaxDevices] = {};
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
+    if (!handles[dev] && cusolverDnCreate(&handles[dev]) != CUSOLVER_STATUS_SUCCESS)
+        fail(CS_ERR_CUDA, "cusolverDnCreate failed");
     return handles[dev];
 }
 

@@ -29,20 +29,6 @@ namespace cs {
 
 namespace {
 
-void check_solver(cusolverStatus_t st, const char* what) {
-    if (st != CUSOLVER_STATUS_SUCCESS)
-        fail(CS_ERR_CUDA, std::string(what) + ": cuSOLVER status " + std::to_string((int)st));
-}
-#define CS_SOLVER(call) check_solver((call), #call)
-
-cusolverDnHandle_t shared_solver() {
-    thread_local cusolverDnHandle_t handles[64] = {};
-    int dev = 0;
-    CS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) fail(CS_ERR_CUDA, "device ordinal out of range");
-    if (!handles[dev]) CS_SOLVER(cusolverDnCreate(&handles[dev]));
-    return handles[dev];
-}
 
 unsigned grid_for(int64_t total) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 32LL * num_sms()));

@@ -4,6 +4,7 @@
 // sample (or record) i, so the kinship operator consumes them without a transpose.
 #pragma once
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 
 #include <vector>
 
@@ -17,8 +18,16 @@ inline void check_blas_status(cublasStatus_t st, const char* what) {
 }
 #define CS_BLAS(call) ::cs::check_blas_status((call), #call)
 
-// One cuBLAS handle per (thread, device), created on first use and kept for the process.
+inline void check_solver_status(cusolverStatus_t st, const char* what) {
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        fail(CS_ERR_CUDA, std::string(what) + ": cuSOLVER status " + std::to_string((int)st));
+}
+#define CS_SOLVER(call) ::cs::check_solver_status((call), #call)
+
+// One cuBLAS and one cuSOLVER handle per (thread, device), created on first use and kept for
+// the process.
 cublasHandle_t shared_blas();
+cusolverDnHandle_t shared_solver();
 
 // Records -> genotype rows (libCosmicCore/src/stcg_vce.cpp:17-38, 64-78).  Identity when
 // every record is its own genotype row, in order.
