@@ -15,6 +15,7 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <numeric>
@@ -52,6 +53,9 @@ struct cs_lmm {
     cs::DeviceBuffer<double> omega, sample, q, scratch, gram, small;
     cs::OmegaWorkspace omega_ws;
     cs::QrWorkspace qr_ws;
+    // device eigensolver of the sketch's projected matrix: eigenvalues, workspace, status
+    cs::DeviceBuffer<double> eig_w, eig_work;
+    cs::DeviceBuffer<int> eig_info;
     // scan: analysed-sample view of the genotypes and its tensor-core context, cached
     // for repeated scans of the same (genotypes, keep) pair
     uint64_t scan_g_uid = 0;
@@ -495,6 +499,55 @@ static void rotate_eigenvectors(cs_lmm* l, const std::vector<double>& Qh,
     CS_LAUNCH("eigvec_rotations");
 }
 
+// Symmetric eigendecomposition of the k x k matrix at d_B (lower triangle) on the device:
+// eigenvectors (columns, ascending eigenvalues) -> l->d_eig, eigenvalues -> w.  cuSOLVER
+// syevd (divide and conquer) by default, syevj (Jacobi) with CS_B200_EIGH=syevj; false when
+// CS_B200_EIGH=host or the solver reports a failure.
+static bool device_eigh(cs_lmm* l, const double* d_B, int64_t k, std::vector<double>& w,
+                        cudaStream_t s) {
+    static const int mode = [] {
+        const char* v = std::getenv("CS_B200_EIGH");
+        if (v && std::strcmp(v, "host") == 0) return 0;
+        if (v && std::strcmp(v, "syevj") == 0) return 2;
+        return 1;
+    }();
+    if (mode == 0) return false;
+    cusolverDnHandle_t sol = shared_solver();
+    CS_SOLVER(cusolverDnSetStream(sol, s));
+    l->d_eig.resize(k * k);
+    l->eig_w.resize(k);
+    l->eig_info.resize(1);
+    CS_CUDA(cudaMemcpyAsync(l->d_eig.get(), d_B, 8 * k * k, cudaMemcpyDeviceToDevice, s));
+    int lwork = 0;
+    if (mode == 1) {
+        CS_SOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                              (int)k, l->d_eig.get(), (int)k, l->eig_w.get(), &lwork));
+        l->eig_work.resize(std::max(lwork, 1));
+        CS_SOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)k,
+                                   l->d_eig.get(), (int)k, l->eig_w.get(), l->eig_work.get(), lwork,
+                                   l->eig_info.get()));
+    } else {
+        syevjInfo_t params = nullptr;
+        CS_SOLVER(cusolverDnCreateSyevjInfo(&params));
+        CS_SOLVER(cusolverDnDsyevj_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                              (int)k, l->d_eig.get(), (int)k, l->eig_w.get(), &lwork,
+                                              params));
+        l->eig_work.resize(std::max(lwork, 1));
+        const cusolverStatus_t st =
+            cusolverDnDsyevj(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)k,
+                             l->d_eig.get(), (int)k, l->eig_w.get(), l->eig_work.get(), lwork,
+                             l->eig_info.get(), params);
+        cusolverDnDestroySyevjInfo(params);
+        CS_SOLVER(st);
+    }
+    int info = 0;
+    w.resize(k);
+    CS_CUDA(cudaMemcpyAsync(w.data(), l->eig_w.get(), 8 * k, cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaMemcpyAsync(&info, l->eig_info.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    return info == 0;
+}
+
 cs_lmm* lmm_create() {
     prof::HostScope hs("lmm_create");
     auto* l = new cs_lmm();
@@ -592,21 +645,25 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     const double one = 1.0, zero = 0.0;
     CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)sk, (int)sk, (int)n, &one, q.get(),
                         (int)sk, sample.get(), (int)sk, &zero, small.get(), (int)sk));
-    std::vector<double> B(sk * sk);
-    CS_CUDA(cudaMemcpyAsync(B.data(), small.get(), 8 * sk * sk, cudaMemcpyDeviceToHost, s));
-    CS_CUDA(cudaStreamSynchronize(s));
-    // eigendecomposition of B: tridiagonalisation and QL on the host, the QL rotations
-    // applied to the eigenvector matrix on the device
-    std::vector<double> dvals, Qh;
-    std::vector<la::PlaneRotation> rots;
-    if (!la::tridiag_ql(B, (int)sk, dvals, Qh, rots))
-        fail(CS_ERR_NUMERIC, "Low-rank GRM eigensolver failed");
+    // eigendecomposition of B (its lower triangle): on the device by cuSOLVER, or on the host
+    // (tridiagonalisation and QL, the QL rotations applied to the eigenvector matrix on the
+    // device) when the device solver reports a failure or CS_B200_EIGH=host asks for it
+    std::vector<double> dvals;
+    if (!device_eigh(l, small.get(), sk, dvals, s)) {
+        std::vector<double> B(sk * sk);
+        CS_CUDA(cudaMemcpyAsync(B.data(), small.get(), 8 * sk * sk, cudaMemcpyDeviceToHost, s));
+        CS_CUDA(cudaStreamSynchronize(s));
+        std::vector<double> Qh;
+        std::vector<la::PlaneRotation> rots;
+        if (!la::tridiag_ql(B, (int)sk, dvals, Qh, rots))
+            fail(CS_ERR_NUMERIC, "Low-rank GRM eigensolver failed");
+        rotate_eigenvectors(l, Qh, rots, (int)sk, s);
+    }
     std::vector<int> order(sk);
     std::iota(order.begin(), order.end(), 0);
     std::sort(order.begin(), order.end(), [&](int a, int b) { return dvals[a] < dvals[b]; });
     std::vector<double> evals(sk);
     for (int64_t j = 0; j < sk; ++j) evals[j] = dvals[order[j]];
-    rotate_eigenvectors(l, Qh, rots, (int)sk, s);
     std::vector<double> lead(rank);
     for (int j = 0; j < rank; ++j) lead[j] = std::max(0.0, evals[sk - 1 - j]);
     // trace-fraction rank selection (lmm_engine.cpp:958-973)
