@@ -35,6 +35,27 @@ def _host_cxx() -> str:
     return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 
+GEN_SRC = os.path.join(HERE, "gen_mt64_jump.cpp")
+GEN_INC = os.path.join(BUILD, "mt64_jump_table.inc")
+
+
+def _jump_table() -> None:
+    """The mt19937_64 jump table (X^(c J) mod p(X)) that omega.cu compiles in: computed at
+    build time by gen_mt64_jump.cpp, which checks a jump against direct generation."""
+    if os.path.exists(GEN_INC) and os.path.getmtime(GEN_INC) >= os.path.getmtime(GEN_SRC):
+        return
+    exe = os.path.join(BUILD, "gen_mt64_jump")
+    res = subprocess.run([_host_cxx(), "-O2", "-std=c++17", GEN_SRC, "-o", exe],
+                         capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"g++ failed on gen_mt64_jump.cpp:\n{res.stdout}\n{res.stderr}")
+    tmp = GEN_INC + ".tmp"
+    res = subprocess.run([exe, tmp], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"gen_mt64_jump failed:\n{res.stdout}\n{res.stderr}")
+    os.replace(tmp, GEN_INC)
+
+
 def _sources():
     return sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
@@ -48,8 +69,10 @@ def _headers_mtime() -> float:
 def _compile(src: str, force: bool, verbose: bool) -> str:
     obj = os.path.join(BUILD, src + ".o")
     path = os.path.join(CSRC, src)
-    if (not force and os.path.exists(obj)
-            and os.path.getmtime(obj) >= max(os.path.getmtime(path), _headers_mtime())):
+    deps = [os.path.getmtime(path), _headers_mtime()]
+    if src == "omega.cu":
+        deps.append(os.path.getmtime(GEN_INC))
+    if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(deps)):
         return obj
     if src.endswith(".cpp"):
         # host-only translation units: the system g++ with OpenMP (small dense algebra)
@@ -59,7 +82,7 @@ def _compile(src: str, force: bool, verbose: bool) -> str:
     else:
         cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-lineinfo", "-O3", "-std=c++17",
                "-Xcompiler", "-fPIC,-O2,-Wall,-Wno-unused-function", "--expt-relaxed-constexpr",
-               "-I", INCLUDE, "-c", path, "-o", obj]
+               "-I", INCLUDE, "-I", BUILD, "-c", path, "-o", obj]
     if src.endswith(".cu") and verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -72,6 +95,7 @@ def _compile(src: str, force: bool, verbose: bool) -> str:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    _jump_table()
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))

@@ -146,6 +146,8 @@ struct OmegaWorkspace {
     DeviceBuffer<int64_t> offsets;
     DeviceBuffer<double> pairs;
     int64_t total_pairs = 0, have = 0;  // accepted polar pairs: needed in all, drawn so far
+    int64_t position = 0;               // draws taken from the engine since seeding
+    DeviceBuffer<uint64_t> prefix, windows;  // parallel draws: stream prefix, chunk windows
     // the draw in flight: its attempts, count blocks and pair target; the per-block counts
     // come back to pinned host memory, signalled by `counted`
     int64_t pending_attempts = 0, pending_blocks = 0, pending_target = 0;

@@ -71,18 +71,7 @@ struct cs_lmm {
     // sketch eigenvectors: the rotated Q, the QL rotations, the selected columns
     cs::DeviceBuffer<double> d_eig, d_rot_cs;
     cs::DeviceBuffer<int32_t> d_rot_i, d_cols;
-    // second stream and events for drawing Omega under the first apply
-    cudaStream_t gen_stream = nullptr;
-    std::array<cudaEvent_t, 8> chunk_events{};
-    ~cs_lmm() {
-        cs::mixed_scan_destroy(scan_mixed);
-        if (gen_stream) {
-            cudaStreamSynchronize(gen_stream);
-            cudaStreamDestroy(gen_stream);
-        }
-        for (cudaEvent_t e : chunk_events)
-            if (e) cudaEventDestroy(e);
-    }
+    ~cs_lmm() { cs::mixed_scan_destroy(scan_mixed); }
 };
 
 namespace cs {
@@ -598,35 +587,11 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     sample.resize(n * sk);
     q.resize(n * sk);
     {
-        // Omega and the first apply overlap: Omega is drawn in chunks of 80 columns (one
-        // column tile of the apply) on a second stream, where one CTA runs the Mersenne
-        // Twister beside the persistent apply kernel; chunk c + 1 is drawn while chunk c is
-        // applied.
+        // Omega on the device (the engine's chunks drawn in parallel from jumped windows),
+        // then the first apply
         prof::HostScope hs("lowrank_omega_first_apply");
-        if (!l->gen_stream) {
-            CS_CUDA(cudaStreamCreateWithFlags(&l->gen_stream, cudaStreamNonBlocking));
-            for (auto& e : l->chunk_events) CS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        }
-        cudaStream_t g = l->gen_stream;
-        // the generator stream must not run ahead of earlier work on s (buffer reuse)
-        CS_CUDA(cudaEventRecord(l->chunk_events[0], s));
-        CS_CUDA(cudaStreamWaitEvent(g, l->chunk_events[0], 0));
-        constexpr int64_t kChunk = 80;
-        const int64_t n_chunks = (sk + kChunk - 1) / kChunk;
-        auto chunk_end = [&](int64_t c) { return std::min<int64_t>(sk, (c + 1) * kChunk); };
-        auto pairs_for = [&](int64_t c) { return (chunk_end(c) * n + 1) / 2; };
-        omega_begin((uint64_t)seed, n * sk, l->omega_ws, g);
-        omega_ensure(l->omega_ws, pairs_for(0), g);
-        for (int64_t c = 0; c < n_chunks; ++c) {
-            const int64_t c0 = c * kChunk, c1 = chunk_end(c);
-            omega_emit(l->omega_ws, n, c0, c1, omega.get(), sk, g);
-            cudaEvent_t e = l->chunk_events[1 + c % (l->chunk_events.size() - 1)];
-            CS_CUDA(cudaEventRecord(e, g));
-            if (c + 1 < n_chunks) omega_draw(l->omega_ws, pairs_for(c + 1), g);
-            CS_CUDA(cudaStreamWaitEvent(s, e, 0));
-            target.apply(omega.get() + c0, sk, c1 - c0, sample.get() + c0, sk, s);
-            if (c + 1 < n_chunks) omega_accept(l->omega_ws, g);
-        }
+        generate_omega_device((uint64_t)seed, n, sk, omega.get(), sk, l->omega_ws, s);
+        target.apply(omega.get(), sk, sk, sample.get(), sk, s);
     }
     {
         prof::HostScope hs("lowrank_subspace_iteration");

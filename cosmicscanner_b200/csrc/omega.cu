@@ -23,6 +23,14 @@
 #include "vce_internal.h"
 
 namespace cs {
+namespace {
+// X^(c J) mod p(X) for the stream's characteristic polynomial p, generated at build time by
+// gen_mt64_jump.cpp (which checks a jump against direct generation)
+#include "mt64_jump_table.inc"
+}  // namespace
+}  // namespace cs
+
+namespace cs {
 
 namespace {
 
@@ -38,17 +46,26 @@ __device__ __forceinline__ uint64_t temper(uint64_t y) {
     return y;
 }
 
-// One CTA of 156 threads continues the sequence from the 312 words in `state`
-// (x[K-312 .. K-1]), writes n_out tempered outputs x[K ..], then stores the new last 312
-// words (the engine advances by n_out rounded up to a multiple of 156).  Step s produces
-// x[K + 156 s + t], t = 0..155, from x[. - 312] and x[. - 156] (thread t's own words of steps
-// s - 2 and s - 1, kept in registers) and x[. - 311] (slot t + 1 of step s - 2, or slot 0 of
-// step s - 1 for t = 155), exchanged through a 3-step shared ring: one barrier per step.
+// One CTA of 156 threads per chunk: CTA c continues the sequence from the 312-word window
+// windows[c] (x[K-312 .. K-1]) and writes its n_out words (n_out = chunk, the last CTA:
+// total - c chunk) to out[c chunk ..], tempered or not; the last CTA stores its final window
+// in final_window when given (the engine advances by n_out rounded up to a multiple of 156).
+// Step s produces x[K + 156 s + t], t = 0..155, from x[. - 312] and x[. - 156] (thread t's own
+// words of steps s - 2 and s - 1, kept in registers) and x[. - 311] (slot t + 1 of step s - 2,
+// or slot 0 of step s - 1 for t = 155), exchanged through a 3-step shared ring: one barrier
+// per step.
+template <bool TEMPER>
 __global__ void __launch_bounds__(kMtM, 1)
-k_mt64(uint64_t* __restrict__ state, int64_t n_out, uint64_t* __restrict__ out) {
+k_mt64(const uint64_t* windows, int64_t chunk, int64_t total, uint64_t* __restrict__ out,
+       uint64_t* final_window) {
     __shared__ uint64_t ring[3][kMtM];
     const int t = threadIdx.x;
+    const int64_t begin = (int64_t)blockIdx.x * chunk;
+    const bool last = blockIdx.x + 1 == gridDim.x;
+    const int64_t n_out = last ? total - begin : chunk;
+    const uint64_t* state = windows + (int64_t)blockIdx.x * kMtN;
     uint64_t p2 = state[t], p1 = state[kMtM + t];
+    out += begin;
     ring[1][t] = p2;  // step -2
     ring[2][t] = p1;  // step -1
     __syncthreads();
@@ -59,7 +76,7 @@ k_mt64(uint64_t* __restrict__ state, int64_t n_out, uint64_t* __restrict__ out) 
         const uint64_t y = (p2 & kUpper) | (nb & kLower);
         const uint64_t v = p1 ^ (y >> 1) ^ ((y & 1ull) ? kMatA : 0ull);
         ring[cur][t] = v;
-        if (st * kMtM + t < n_out) out[st * kMtM + t] = temper(v);
+        if (st * kMtM + t < n_out) out[st * kMtM + t] = TEMPER ? temper(v) : v;
         p2 = p1;
         p1 = v;
         __syncthreads();
@@ -68,8 +85,31 @@ k_mt64(uint64_t* __restrict__ state, int64_t n_out, uint64_t* __restrict__ out) 
         prev = cur;
         cur = next;
     }
-    state[t] = p2;
-    state[kMtM + t] = p1;
+    if (last && final_window) {
+        final_window[t] = p2;
+        final_window[kMtM + t] = p1;
+    }
+}
+
+// Windows of the chunks c = 1 .. gridDim.x (J words apart) from the untempered stream x
+// (x[0..311] = the seeded window, then 19936 further words): word k of window c is the XOR of
+// x[i + k] over the set bits i of X^(c J) mod p(X).  One CTA per chunk, one thread per word;
+// the polynomial's words are read by every thread at once (broadcast) and x coalesced.
+__global__ void __launch_bounds__(kMtN)
+k_mt64_jump(const uint64_t* __restrict__ x, uint64_t* __restrict__ windows) {
+    const int c = blockIdx.x + 1, k = threadIdx.x;
+    const unsigned long long* g = kMt64Jump[c];
+    uint64_t acc = 0;
+    for (int wi = 0; wi < kMtN; ++wi) {
+        unsigned long long word = g[wi];
+        const uint64_t* xb = x + wi * 64 + k;
+        while (word) {
+            const int b = __ffsll((long long)word) - 1;
+            word &= word - 1;
+            acc ^= xb[b];
+        }
+    }
+    windows[(int64_t)c * kMtN + k] = acc;
 }
 
 __device__ __forceinline__ double canonical(uint64_t r) {
@@ -189,6 +229,7 @@ void omega_begin(uint64_t seed, int64_t total_count, OmegaWorkspace& ws, cudaStr
     ws.total_pairs = (total_count + 1) / 2;
     ws.pairs.resize(std::max<int64_t>(2, 2 * ws.total_pairs));
     ws.have = 0;
+    ws.position = 0;
 }
 
 OmegaWorkspace::~OmegaWorkspace() {
@@ -222,11 +263,38 @@ void omega_draw(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s) {
         }
     }
     if (!ws.counted) CS_CUDA(cudaEventCreateWithFlags(&ws.counted, cudaEventDisableTiming));
-    {
-        prof::Scope ps("mt19937_64_stream", s, 0.0, 16.0 * attempts);
-        k_mt64<<<1, kMtM, 0, s>>>(ws.state.get(), 2 * attempts, ws.raw.get());
+    const int64_t draws = 2 * attempts;
+    if (ws.position == 0 && draws > kMt64JumpWords) {
+        // from the seeded window: chunks of J draws in parallel from jumped windows
+        constexpr int64_t kPrefix = kMt64JumpWords > 0 ? 19936 : 0;  // x[312 .. 20247]
+        const int chunks = (int)std::min<int64_t>(kMt64JumpChunks, (draws + kMt64JumpWords - 1) / kMt64JumpWords);
+        ws.prefix.resize(kMtN + kPrefix);
+        ws.windows.resize((int64_t)chunks * kMtN);
+        CS_CUDA(cudaMemcpyAsync(ws.prefix.get(), ws.state.get(), 8 * kMtN, cudaMemcpyDeviceToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(ws.windows.get(), ws.state.get(), 8 * kMtN, cudaMemcpyDeviceToDevice, s));
+        {
+            prof::Scope ps("mt19937_64_prefix", s, 0.0, 8.0 * kPrefix);
+            k_mt64<false><<<1, kMtM, 0, s>>>(ws.state.get(), kPrefix, kPrefix, ws.prefix.get() + kMtN,
+                                             nullptr);
+            CS_LAUNCH("mt19937_64_prefix");
+        }
+        {
+            prof::Scope ps("mt19937_64_jump", s, 0.0, 8.0 * kMtN * (chunks - 1));
+            if (chunks > 1) k_mt64_jump<<<chunks - 1, kMtN, 0, s>>>(ws.prefix.get(), ws.windows.get());
+            CS_LAUNCH("mt19937_64_jump");
+        }
+        {
+            prof::Scope ps("mt19937_64_stream", s, 0.0, 8.0 * draws);
+            k_mt64<true><<<chunks, kMtM, 0, s>>>(ws.windows.get(), kMt64JumpWords, draws, ws.raw.get(),
+                                                 ws.state.get());
+            CS_LAUNCH("mt19937_64_stream");
+        }
+    } else {
+        prof::Scope ps("mt19937_64_stream", s, 0.0, 8.0 * draws);
+        k_mt64<true><<<1, kMtM, 0, s>>>(ws.state.get(), draws, draws, ws.raw.get(), ws.state.get());
         CS_LAUNCH("mt19937_64_stream");
     }
+    ws.position += draws;
     {
         prof::Scope ps("polar_accept_count", s, 0.0, 16.0 * attempts);
         k_accept_count<<<(unsigned)blocks, 256, 0, s>>>(ws.raw.get(), attempts, ws.counts.get());
@@ -296,7 +364,7 @@ void mt64_seed_device(uint64_t seed, uint64_t* d_state, cudaStream_t s) {
 void mt64_generate(uint64_t* d_state, int64_t n_out, uint64_t* d_out, cudaStream_t s) {
     if (n_out <= 0) return;
     prof::Scope ps("mt19937_64_stream", s, 0.0, 8.0 * n_out);
-    k_mt64<<<1, kMtM, 0, s>>>(d_state, n_out, d_out);
+    k_mt64<true><<<1, kMtM, 0, s>>>(d_state, n_out, n_out, d_out, d_state);
     CS_LAUNCH("mt19937_64_stream");
 }
 

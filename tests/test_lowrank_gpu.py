@@ -91,3 +91,13 @@ def test_device_normal_stream_matches_libstdcxx(n, cols):
         got = cs.normal_matrix(seed, n, cols)
         ref = oracle.normal_matrix(seed, n, cols)
         assert np.abs(got - ref).max() <= 4e-16 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n,cols,seed", [(50000, 40, 42), (100000, 266, 8128), (200000, 266, 42)])
+def test_device_normal_stream_parallel_chunks(n, cols, seed):
+    """Streams longer than one chunk of the engine (1,048,320 draws) are drawn in parallel from
+    jumped windows: 3, 33 and 66 chunks (the last beyond the 64-chunk table, finished
+    sequentially) must still equal std::normal_distribution over std::mt19937_64."""
+    got = cs.normal_matrix(seed, n, cols)
+    ref = oracle.normal_matrix(seed, n, cols)
+    assert np.abs(got - ref).max() <= 4e-16 * np.abs(ref).max()
