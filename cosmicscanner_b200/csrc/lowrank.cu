@@ -80,15 +80,6 @@ namespace {
 
 
 // ---------------------------------------------------------------- QR
-// Thin QR of Y (n x k row-major) by Cholesky-QR2: two passes of G = Y^T Y, G = R^T R,
-// Y <- Y R^{-1}, with the k x k factor and its triangular inverse formed on the device
-// (cuSOLVER potrf + trtri) and applied as one DGEMM (a device triangular solve of this shape
-// runs several times slower than the GEMM).  A pass whose Gram matrix is not numerically
-// positive definite is factored on the host with a shift (shifted Cholesky-QR) and a third
-// pass added.  Any orthonormal basis of span(Y) gives the same
-// subspace iteration as the reference's HouseholderQR (lmm_engine.cpp:931-941): Q is unique
-// up to column signs, which cancel in Q^T K Q and in U = Q W.  Y is used as scratch; the
-// result is written to Q.
 // Strictly lower triangle of a k x k column-major matrix -> 0 (cuSOLVER leaves the Gram's
 // lower half under the factor).
 __global__ void k_zero_lower(double* __restrict__ A, int64_t k) {
@@ -121,8 +112,17 @@ bool host_factor_pass(const double* G, int64_t n, int64_t k, double* Rinv_d, boo
     return true;
 }
 
+// Thin QR of Y (n x k row-major) by Cholesky-QR (`passes` passes, 2 = Cholesky-QR2) of
+// G = Y^T Y, G = R^T R, Y <- Y R^{-1}, with the k x k factor and its triangular inverse
+// formed on the device (cuSOLVER potrf + trtri) and applied as one DGEMM (a device
+// triangular solve of this shape runs several times slower than the GEMM).  A pass whose
+// Gram matrix is not numerically positive definite is factored on the host with a shift
+// (shifted Cholesky-QR) and one more pass added.  Any orthonormal basis of span(Y) gives the
+// same subspace iteration as the reference's HouseholderQR (lmm_engine.cpp:931-941): Q is
+// unique up to column signs, which cancel in Q^T K Q and in U = Q W.  Y is used as scratch;
+// the result is written to Q.
 void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q,
-                 DeviceBuffer<double>& d_gram, QrWorkspace& ws, cudaStream_t s) {
+                 DeviceBuffer<double>& d_gram, QrWorkspace& ws, cudaStream_t s, int passes = 2) {
     const double one = 1.0, zero = 0.0;
     d_gram.resize(k * k);
     double* G = d_gram.get();
@@ -141,7 +141,6 @@ void cholesky_qr(cublasHandle_t blas, double* Y, int64_t n, int64_t k, double* Q
         ws.info.resize(2);
         ws.k = k;
     }
-    int passes = 2;
     double* src = Y;
     double* dst = Q;
     for (int pass = 0; pass < passes; ++pass) {
@@ -595,8 +594,11 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     }
     {
         prof::HostScope hs("lowrank_subspace_iteration");
+        // The iterations only need a well-conditioned basis of the same span (Q = Y R^{-1}
+        // spans span(Y) whatever its loss of orthogonality): one Cholesky-QR pass each; the
+        // basis that B = Q^T K Q is formed in takes both passes.
         for (int it = 0; it < 2; ++it) {
-            cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s);
+            cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s, 1);
             target.apply(q.get(), sk, sk, sample.get(), sk, s);
         }
         cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s);

@@ -93,14 +93,17 @@ k_mt64(const uint64_t* windows, int64_t chunk, int64_t total, uint64_t* __restri
 
 // Windows of the chunks c = 1 .. gridDim.x (J words apart) from the untempered stream x
 // (x[0..311] = the seeded window, then 19936 further words): word k of window c is the XOR of
-// x[i + k] over the set bits i of X^(c J) mod p(X).  One CTA per chunk, one thread per word;
-// the polynomial's words are read by every thread at once (broadcast) and x coalesced.
+// x[i + k] over the set bits i of X^(c J) mod p(X).  CTA (c, part) takes 1 / gridDim.y of the
+// polynomial's words, one thread per window word, and XORs its partial into the zeroed
+// window; the polynomial's words are read by every thread at once (broadcast), x coalesced.
+constexpr int kJumpParts = 8;
 __global__ void __launch_bounds__(kMtN)
-k_mt64_jump(const uint64_t* __restrict__ x, uint64_t* __restrict__ windows) {
+k_mt64_jump(const uint64_t* __restrict__ x, unsigned long long* __restrict__ windows) {
     const int c = blockIdx.x + 1, k = threadIdx.x;
     const unsigned long long* g = kMt64Jump[c];
+    const int w0 = blockIdx.y * kMtN / gridDim.y, w1 = (blockIdx.y + 1) * kMtN / gridDim.y;
     uint64_t acc = 0;
-    for (int wi = 0; wi < kMtN; ++wi) {
+    for (int wi = w0; wi < w1; ++wi) {
         unsigned long long word = g[wi];
         const uint64_t* xb = x + wi * 64 + k;
         while (word) {
@@ -109,7 +112,7 @@ k_mt64_jump(const uint64_t* __restrict__ x, uint64_t* __restrict__ windows) {
             acc ^= xb[b];
         }
     }
-    windows[(int64_t)c * kMtN + k] = acc;
+    atomicXor(windows + (int64_t)c * kMtN + k, (unsigned long long)acc);
 }
 
 __device__ __forceinline__ double canonical(uint64_t r) {
@@ -280,7 +283,11 @@ void omega_draw(OmegaWorkspace& ws, int64_t pairs_needed, cudaStream_t s) {
         }
         {
             prof::Scope ps("mt19937_64_jump", s, 0.0, 8.0 * kMtN * (chunks - 1));
-            if (chunks > 1) k_mt64_jump<<<chunks - 1, kMtN, 0, s>>>(ws.prefix.get(), ws.windows.get());
+            if (chunks > 1) {
+                CS_CUDA(cudaMemsetAsync(ws.windows.get() + kMtN, 0, 8 * (int64_t)(chunks - 1) * kMtN, s));
+                k_mt64_jump<<<dim3(chunks - 1, kJumpParts), kMtN, 0, s>>>(
+                    ws.prefix.get(), reinterpret_cast<unsigned long long*>(ws.windows.get()));
+            }
             CS_LAUNCH("mt19937_64_jump");
         }
         {
