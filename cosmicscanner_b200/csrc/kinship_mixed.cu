@@ -507,50 +507,80 @@ __device__ __forceinline__ double quant_factor(unsigned long long bits) {
     return m > 0.0 ? 127.0 / m : 0.0;
 }
 
-// Per-column sums of a row-major FP64 matrix over row blocks: part[b][c].
-__global__ void k_col_partial_sums(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
-                                   int64_t rows_per_block, double* __restrict__ part) {
-    const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
-    const int64_t r1 = min(n, r0 + rows_per_block);
-    for (int64_t c = threadIdx.x; c < k; c += blockDim.x) {
-        double s = 0.0;
-        for (int64_t r = r0; r < r1; ++r) s += X[r * ld + c];
-        part[(int64_t)blockIdx.x * k + c] = s;
-    }
-}
-
-// out[c] = scale * sum_b part[b][c] (fixed order); resets maxbits[c] when given.
-__global__ void k_sum_partials(const double* __restrict__ part, int nb, int64_t k, double scale,
-                               double* __restrict__ out, unsigned long long* __restrict__ maxbits) {
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < k;
-         c += (int64_t)gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int b = 0; b < nb; ++b) s += part[(int64_t)b * k + c];
-        out[c] = s * scale;
-        if (maxbits) maxbits[c] = 0ull;
-    }
-}
-
-// Tile (blockIdx.x: 64 rows, blockIdx.y: 32 columns) of |X - mean| maxima: one atomicMax
-// per column per block.
+// Per-column sums, minima and maxima of a row-major FP64 matrix over tiles of 64 rows x 32
+// columns (blockIdx.x, blockIdx.y): part[b][c], part[nb + b][c], part[2 nb + b][c], b the row
+// tile, nb = gridDim.x.  Warps read 32 consecutive columns of a row (256-byte segments).
 __global__ void __launch_bounds__(256)
-k_col_absmax(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k,
-             const double* __restrict__ mean, unsigned long long* __restrict__ maxbits) {
-    __shared__ double red[8][kPrepCols];
+k_col_stats(const double* __restrict__ X, int64_t ld, int64_t n, int64_t k, double* __restrict__ part) {
+    __shared__ double red[3][8][kPrepCols];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const int64_t c = (int64_t)blockIdx.y * kPrepCols + tx;
     const int64_t r0 = (int64_t)blockIdx.x * kPrepRows;
-    double m = 0.0;
-    if (c < k) {
-        const double mc = mean[c];
-        for (int64_t r = r0 + ty; r < min(n, r0 + kPrepRows); r += 8) m = fmax(m, fabs(X[r * ld + c] - mc));
-    }
-    red[ty][tx] = m;
+    double sm = 0.0, mn = INFINITY, mx = -INFINITY;
+    if (c < k)
+        for (int64_t r = r0 + ty; r < min(n, r0 + kPrepRows); r += 8) {
+            const double v = X[r * ld + c];
+            sm += v;
+            mn = fmin(mn, v);
+            mx = fmax(mx, v);
+        }
+    red[0][ty][tx] = sm;
+    red[1][ty][tx] = mn;
+    red[2][ty][tx] = mx;
     __syncthreads();
     if (ty == 0 && c < k) {
-        for (int j = 1; j < 8; ++j) m = fmax(m, red[j][tx]);
-        atomicMax(maxbits + c, (unsigned long long)__double_as_longlong(m));
+        for (int j = 1; j < 8; ++j) {
+            sm += red[0][j][tx];
+            mn = fmin(mn, red[1][j][tx]);
+            mx = fmax(mx, red[2][j][tx]);
+        }
+        const int64_t nb = gridDim.x;
+        part[(int64_t)blockIdx.x * k + c] = sm;
+        part[(nb + blockIdx.x) * k + c] = mn;
+        part[(2 * nb + blockIdx.x) * k + c] = mx;
     }
+}
+
+// mean[c] = (sum over row tiles) / n and maxbits[c] = the bits of max |x - mean[c]| =
+// max(max x - mean, mean - min x) (rounding is monotonic, so this equals the maximum of the
+// rounded differences).  One warp per column: lane l takes tiles l, l + 32, ..., then a fixed
+// shuffle tree (deterministic).
+__global__ void __launch_bounds__(256)
+k_col_finalize(const double* __restrict__ part, int nb, int64_t k, int64_t n,
+               double* __restrict__ mean, unsigned long long* __restrict__ maxbits) {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c >= k) return;
+    double sm = 0.0, mn = INFINITY, mx = -INFINITY;
+    for (int b = lane; b < nb; b += 32) {
+        sm += part[(int64_t)b * k + c];
+        mn = fmin(mn, part[(int64_t)(nb + b) * k + c]);
+        mx = fmax(mx, part[(int64_t)(2 * nb + b) * k + c]);
+    }
+    for (int off = 16; off; off >>= 1) {
+        sm += __shfl_xor_sync(0xffffffffu, sm, off);
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    if (lane == 0) {
+        const double m = sm / (double)n;
+        mean[c] = m;
+        const double a = fmax(fmax(mx - m, m - mn), 0.0);
+        maxbits[c] = (unsigned long long)__double_as_longlong(a);
+    }
+}
+
+// out[c] = scale * sum_b part[b][c]: one warp per column, lane l takes b = l, l + 32, ...,
+// then a fixed shuffle tree (deterministic).  Launch with (k + 7) / 8 blocks of 256 threads.
+__global__ void __launch_bounds__(256)
+k_sum_partials(const double* __restrict__ part, int nb, int64_t k, double scale, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t c = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c >= k) return;
+    double sm = 0.0;
+    for (int b = lane; b < nb; b += 32) sm += part[(int64_t)b * k + c];
+    for (int off = 16; off; off >>= 1) sm += __shfl_xor_sync(0xffffffffu, sm, off);
+    if (lane == 0) out[c] = sm * scale;
 }
 
 // Rows-pass operand: B1[q*kp + c][pos(i)] (int8 pieces of (x_ic - mean_c) 127 / max_c, i < n_pad;
@@ -951,12 +981,10 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
                              : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
     const int kbs = (kb + splits - 1) / splits;
     const int rt = (int)((n_pad + kPrepRows - 1) / kPrepRows);
-    const int nbs = (int)std::min<int64_t>(512, std::max<int64_t>(1, n / 128));
-    const int64_t rpb = (n + nbs - 1) / nbs;
-    const int nbu = (int)((n + rpb - 1) / rpb);
+    const int nst = (int)((n + kPrepRows - 1) / kPrepRows);  // row tiles of the column stats
     ws.b1.resize(3 * kp * n_pad);
     ws.part.resize((int64_t)splits * kp * r_pad);
-    ws.colpart.resize((int64_t)std::max(rt, nbu) * k);
+    ws.colpart.resize((int64_t)std::max(rt, 3 * nst) * k);
     ws.mean1.resize(k);
     ws.qsum.resize(k);
     ws.max1.resize(k);
@@ -977,15 +1005,14 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
     }
     {
         prof::Scope ps("mixed_prep_rows_operand", s, 0.0, 24.0 * n * k + 3.0 * kp * n_pad);
-        k_col_partial_sums<<<nbu, 128, 0, s>>>(X, ldx, n, k, rpb, ws.colpart.get());
-        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), nbu, k, 1.0 / (double)n,
-                                         ws.mean1.get(), ws.max1.get());
-        dim3 g1((unsigned)((n + kPrepRows - 1) / kPrepRows), (unsigned)((k + kPrepCols - 1) / kPrepCols));
-        k_col_absmax<<<g1, 256, 0, s>>>(X, ldx, n, k, ws.mean1.get(), ws.max1.get());
+        dim3 g1((unsigned)nst, (unsigned)((k + kPrepCols - 1) / kPrepCols));
+        k_col_stats<<<g1, 256, 0, s>>>(X, ldx, n, k, ws.colpart.get());
+        k_col_finalize<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), nst, k, n,
+                                                               ws.mean1.get(), ws.max1.get());
         dim3 g2((unsigned)rt, (unsigned)((kp + kPrepCols - 1) / kPrepCols));
         k_split_rows_operand<<<g2, 256, 0, s>>>(X, ldx, n, k, kp, n_pad, ws.mean1.get(),
                                                 ws.max1.get(), ws.b1.get(), ws.colpart.get());
-        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), rt, k, 1.0, ws.qsum.get(), nullptr);
+        k_sum_partials<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), rt, k, 1.0, ws.qsum.get());
         CS_LAUNCH("mixed rows operand");
     }
     PassArgs P{};
@@ -1060,7 +1087,7 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
         k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), ws.max_w.get(),
                                                   ws.max_muw.get(), ws.b2.get(), ws.inv_f.get(),
                                                   ws.colpart.get());
-        k_sum_partials<<<1, 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get(), nullptr);
+        k_sum_partials<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get());
         CS_LAUNCH("mixed samples operand");
     }
     PassArgs P{};

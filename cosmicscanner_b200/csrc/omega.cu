@@ -181,20 +181,25 @@ __global__ void k_accept_write(const uint64_t* __restrict__ raw, int64_t attempt
     }
 }
 
-// draw idx (first <= idx < first + count) of the column-by-column stream ->
-// out[row * ld + col], row = idx % n, col = idx / n
+// draws idx (first <= idx < first + count) of the column-by-column stream ->
+// out[row * ld + col], row = idx % n, col = idx / n.  One thread per accepted pair: its
+// multiplier serves both draws (2 p and 2 p + 1).
 __global__ void k_polar(const double* __restrict__ pairs, int64_t first, int64_t count, int64_t n,
                         int64_t ld, double* __restrict__ out) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t idx = first + e;
-        const int64_t p = idx >> 1;
+    const int64_t p0 = first >> 1, p1 = (first + count - 1) >> 1;
+    for (int64_t p = p0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p <= p1;
+         p += (int64_t)gridDim.x * blockDim.x) {
         const double x = pairs[2 * p], y = pairs[2 * p + 1];
         const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
         const double mult = sqrt(__ddiv_rn(__dmul_rn(-2.0, log(r2)), r2));
-        const double v = (idx & 1) ? __dmul_rn(x, mult) : __dmul_rn(y, mult);
-        const int64_t col = idx / n, row = idx - col * n;
-        out[row * ld + col] = v;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t idx = 2 * p + h;
+            if (idx < first || idx >= first + count) continue;
+            const double v = h ? __dmul_rn(x, mult) : __dmul_rn(y, mult);
+            const int64_t col = idx / n, row = idx - col * n;
+            out[row * ld + col] = v;
+        }
     }
 }
 
@@ -347,7 +352,7 @@ void omega_emit(OmegaWorkspace& ws, int64_t n, int64_t c0, int64_t c1, double* d
     const int64_t first = c0 * n, count = (c1 - c0) * n;
     if (count <= 0) return;
     prof::Scope ps("polar_pairs", s, 0.0, 16.0 * count);
-    const int blocks = (int)std::min<int64_t>((count + 255) / 256, 32LL * num_sms());
+    const int blocks = (int)std::min<int64_t>((count / 2 + 256) / 256, 32LL * num_sms());
     k_polar<<<std::max(blocks, 1), 256, 0, s>>>(ws.pairs.get(), first, count, n, ld, d_out);
     CS_LAUNCH("polar_pairs");
 }
