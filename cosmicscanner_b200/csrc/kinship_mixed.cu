@@ -204,17 +204,19 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
     const uint32_t tmem_base = *tmem_slot;
 
     // A unit is one M tile (pair: two, one per CTA) x one column tile x one K slice; both
-    // CTAs of a pair walk the same units.
+    // CTAs of a pair walk the same units.  The column tile varies fastest, so the CTAs that
+    // run at the same time share each packed tile through L2 instead of re-reading the packed
+    // matrix from HBM once per column tile.
     const int groups = PAIR ? P.n_tiles / 2 : P.n_tiles;
     const int units = groups * P.n_ctiles * P.n_splits;
     const int u0 = PAIR ? (int)cluster_id_x() : (int)blockIdx.x;
     const int ustep = PAIR ? (int)cluster_count_x() : (int)gridDim.x;
     auto unit_coords = [&](int u, int& tile, int& ct, int& split, int& kb0, int& kb1) {
-        const int g = u % groups;
+        ct = u % P.n_ctiles;
+        const int rest = u / P.n_ctiles;
+        const int g = rest % groups;
         tile = PAIR ? 2 * g + (int)rank : g;
-        const int rest = u / groups;
-        ct = rest % P.n_ctiles;
-        split = rest / P.n_ctiles;
+        split = rest / groups;
         kb0 = split * P.kb_per_split;
         kb1 = min(P.kb_total, kb0 + P.kb_per_split);
     };
