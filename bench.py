@@ -170,10 +170,10 @@ def int8_peak_tops(torch):
 
 def profile_traffic():
     """DRAM bytes per packed byte of the tensor-core passes from the committed ncu summary
-    (profiles/kinship_tc_passes_n20000_m30000_k68.md), or None."""
+    (profiles/kinship_tc_pair_passes_n20000_m30000_k266.md), or None."""
     import re
 
-    path = os.path.join(ROOT, "profiles", "kinship_tc_passes_n20000_m30000_k68.md")
+    path = os.path.join(ROOT, "profiles", "kinship_tc_pair_passes_n20000_m30000_k266.md")
     try:
         text = open(path).read()
     except OSError:
@@ -500,7 +500,7 @@ def main():
                 traffic = tr[key] * bytes_per_launch
         roof.update({"kernel": top["name"], "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                     "traffic_note": "ncu DRAM bytes per packed byte at N=20000 M=30000 k=68, "
+                     "traffic_note": "ncu DRAM bytes per packed byte at N=20000 M=30000 k=266, "
                                      "scaled by this launch's packed bytes",
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "ms_per_launch": per_launch_ms,
