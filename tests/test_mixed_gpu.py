@@ -101,3 +101,42 @@ def test_lowrank_mixed_matches_oracle():
         err = np.abs(out[key][t] - exp[key][t]).max() / np.abs(exp[key][t]).max()
         assert err < 1e-5, (key, err)
     assert np.abs(out["log10p"][t] - exp["log10p"][t]).max() < 1e-3
+
+
+@pytest.mark.parametrize("mode", ["0", "1"])
+def test_operator_mixed_forced_cta_mode(mode):
+    """CS_B200_CTA_PAIRS=0 (single CTAs for every width) and =1 (CTA pairs for every width)
+    give the same operator as the default width-based choice, within the mixed tolerance;
+    the mode is read once per process, so each runs in a child interpreter."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    code = r'''
+import json, sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import cosmicscanner_b200 as cs
+from cosmicscanner_b200 import synth
+d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
+g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+op = cs.createKinshipOperator(g)
+out = {}
+for k in (16, 68):
+    X = np.random.default_rng(k).standard_normal((d["n"], k))
+    out[k] = op.apply(X, precision="mixed").tolist()
+print(json.dumps(out))
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CS_B200_CTA_PAIRS=mode)
+    res = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True,
+                         text=True, timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    forced = json.loads(res.stdout.strip().splitlines()[-1])
+    d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    for k in (16, 68):
+        X = np.random.default_rng(k).standard_normal((d["n"], k))
+        E = ref.apply_block(X, n_threads=8)
+        Y = np.array(forced[str(k)])
+        assert colwise_rel(Y, E).max() < 1e-6
