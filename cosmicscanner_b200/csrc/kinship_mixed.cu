@@ -121,8 +121,6 @@ struct PassArgs {
     const double* mu;            // rows pass: mu_t per SNP row (epilogue)
     const double* inv_f;         // samples pass: 1 / quantisation factor per column
     double* part;                // [n_splits][kp][ld] FP64 slice partials
-    const uint8_t* tiled;        // packed genotypes as contiguous 4 KB tiles, [SNP tile][sample tile]
-    int n_sample_tiles;          // sample tiles per SNP tile (n_pad / 128)
     int64_t ld;                  // padded output rows
     int* status;
 };
@@ -148,8 +146,8 @@ __host__ __device__ __forceinline__ int position_of(int s) { return (s & 1) ? 8 
 
 template <bool ROWS, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1)
-k_mixed_pass(const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ CUtensorMap tm_bt,
-             PassArgs P) {
+k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
+             const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
     using L = Layout<ROWS, PAIR>;
     constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
@@ -393,6 +391,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ C
     } else if (warp == kPackedWarp) {
         // ------------------------------------------------------------ TMA producer (packed)
         if (elect_one()) {
+            prefetch_tensormap(&tm_a);
             uint32_t j = 0;
             bool ok = true;
             for (int u = u0; u < units && ok; u += ustep) {
@@ -402,13 +401,11 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ C
                     const int sp = j % SP;
                     if (!(ok = mbar_wait(&empty_p[sp], ((j / SP) & 1) ^ 1, P.status, kTimeoutTma))) break;
                     mbar_arrive_expect_tx(&full_p[sp], (uint32_t)kPackedBytes);
-                    // packed tile: 128 SNP rows x 32 bytes (128 samples), one contiguous 4 KB
-                    // block of the tiled copy (rows pass: SNP tile `tile`, sample tile kb;
-                    // samples pass: SNP tile kb, sample tile `tile`)
-                    const int64_t t = ROWS ? (int64_t)tile * P.n_sample_tiles + kb
-                                           : (int64_t)kb * P.n_sample_tiles + tile;
-                    bulk_load(smem + L::p(sp), P.tiled + t * kPackedBytes, (uint32_t)kPackedBytes,
-                              &full_p[sp]);
+                    // packed tile: 128 SNP rows x 32 bytes (128 samples)
+                    if (ROWS)
+                        tma_load_2d(smem + L::p(sp), &tm_a, kb * 32, tile * kTile, &full_p[sp]);
+                    else
+                        tma_load_2d(smem + L::p(sp), &tm_a, tile * 32, kb * kKBlock, &full_p[sp]);
                 }
             }
             // leave no copy in flight
@@ -483,29 +480,6 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_b, const __grid_constant__ C
             tmem_dealloc_pair(tmem_base, kTmemCols);
         else
             tmem_dealloc(tmem_base, kTmemCols);
-    }
-}
-
-// ---------------------------------------------------------------- tiled packed copy
-// Packed rows (stride bytes apart; bytes [0, row_bytes) used, row_bytes = n_pad / 4, a
-// multiple of 32) -> 4 KB tiles of 128 rows x 32 bytes, tile (T, S) at (T n_st + S) 4096,
-// n_st = row_bytes / 32; rows at or past R become zero bytes.  One CTA per 8 rows: each row
-// is read in coalesced 16-byte chunks, and the two chunks of a tile row land side by side.
-constexpr int kTileRows = 8;
-__global__ void __launch_bounds__(256)
-k_tile_packed(const uint8_t* __restrict__ rows, int64_t stride, int64_t R, int64_t row_bytes,
-              uint8_t* __restrict__ tiled) {
-    const int64_t n_st = row_bytes / 32;
-    const int64_t chunks = row_bytes / 16;
-    for (int rr = 0; rr < kTileRows; ++rr) {
-        const int64_t row = (int64_t)blockIdx.x * kTileRows + rr;
-        const int64_t T = row >> 7, r = row & 127;
-        for (int64_t c = threadIdx.x; c < chunks; c += blockDim.x) {
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (row < R) v = *reinterpret_cast<const uint4*>(rows + row * stride + 16 * c);
-            const int64_t S = c >> 1;
-            *reinterpret_cast<uint4*>(tiled + (T * n_st + S) * 4096 + r * 32 + (c & 1) * 16) = v;
-        }
     }
 }
 
@@ -841,12 +815,10 @@ int choose_splits(int64_t units_per_split, int kb_total, int64_t target) {
 }  // namespace
 
 struct MixedRows {
-    // a packed view with per-row centring statistics, ready for the rows pass, and its
-    // tiled copy: tile (T, S) = SNP rows 128 T.., samples 128 S.. as 4 KB of 128 rows x 32
-    // bytes at offset (T (n_pad / 128) + S) 4096 (rows past R are zero bytes)
+    // a packed view with per-row centring statistics, ready for the rows pass
     int64_t R = 0, n = 0, r_pad = 0, n_pad = 0;
     DeviceBuffer<double> mu, exc, s;
-    DeviceBuffer<uint8_t> tiled;
+    CUtensorMap tm{};
 };
 
 struct MixedWorkspace {
@@ -918,7 +890,8 @@ int resident_pairs() {
 
 // One CTA per SM, or (PAIR) as many clusters of two CTAs as are resident together.
 template <bool ROWS, bool PAIR>
-void launch_pass(const CUtensorMap& tb, const CUtensorMap& tbt, const PassArgs& P, cudaStream_t s) {
+void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
+                 const PassArgs& P, cudaStream_t s) {
     if (PAIR) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(2 * resident_pairs<ROWS>()));
@@ -932,9 +905,9 @@ void launch_pass(const CUtensorMap& tb, const CUtensorMap& tbt, const PassArgs& 
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true>, tb, tbt, P));
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true>, ta, tb, tbt, P));
     } else {
-        k_mixed_pass<ROWS, false><<<num_sms(), kThreads, Layout<ROWS, false>::kSmem, s>>>(tb, tbt, P);
+        k_mixed_pass<ROWS, false><<<num_sms(), kThreads, Layout<ROWS, false>::kSmem, s>>>(ta, tb, tbt, P);
     }
 }
 
@@ -966,16 +939,7 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     CS_CUDA(cudaMemcpy(r.s.get(), sv.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     // packed tiles: 32 bytes (128 samples) x 128 SNP rows; rows past R read as zeros and
     // either land in discarded output rows (rows pass) or meet zero B rows (samples pass)
-    if (r.n_pad / 4 > v.stride || v.stride % 16 != 0)
-        fail(CS_ERR_UNSUPPORTED, "packed rows are narrower than the padded sample count");
-    r.tiled.resize(r.r_pad * (r.n_pad / 4));
-    {
-        prof::Scope ps("mixed_tile_packed", nullptr, 0.0, 2.0 * (double)r.r_pad * (double)(r.n_pad / 4));
-        const int64_t groups = r.r_pad / kTileRows;
-        k_tile_packed<<<(unsigned)groups, 256>>>(v.rows, v.stride, r.R, r.n_pad / 4, r.tiled.get());
-        CS_LAUNCH("mixed_tile_packed");
-        CS_CUDA(cudaStreamSynchronize(0));
-    }
+    r.tm = make_map_u8(v.rows, v.stride, std::max<int64_t>(r.R, 1), v.stride, 32, kTile, false);
 }
 
 struct Tiling {
@@ -1074,17 +1038,15 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
     P.mu = r.mu.get();
     P.part = ws.part.get();
     P.ld = r_pad;
-    P.tiled = r.tiled.get();
-    P.n_sample_tiles = (int)(n_pad / kTile);
     P.status = ws.status.get();
     {
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
-            launch_pass<true, true>(ws.tm_b1, ws.tm_b1t, P, s);
+            launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else
-            launch_pass<true, false>(ws.tm_b1, ws.tm_b1t, P, s);
+            launch_pass<true, false>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         CS_LAUNCH("kinship_rows_tc");
     }
     if (want_max) {
@@ -1151,16 +1113,14 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     P.inv_f = ws.inv_f.get();
     P.part = ws.part.get();
     P.ld = n_pad;
-    P.tiled = r.tiled.get();
-    P.n_sample_tiles = (int)(n_pad / kTile);
     P.status = ws.status.get();
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
-            launch_pass<false, true>(ws.tm_b2, ws.tm_b2t, P, s);
+            launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         else
-            launch_pass<false, false>(ws.tm_b2, ws.tm_b2t, P, s);
+            launch_pass<false, false>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         CS_LAUNCH("kinship_samples_tc");
     }
     {
