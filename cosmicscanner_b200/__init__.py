@@ -446,7 +446,7 @@ class ServerOptions(C.Structure):
         ("rank", C.c_int32), ("oversample", C.c_int32), ("trace_threshold", C.c_double),
         ("min_rank", C.c_int32), ("min_maf", C.c_double), ("precision", C.c_int32),
         ("max_batch_columns", C.c_int64), ("memory_budget_gb", C.c_double),
-        ("max_active", C.c_int32),
+        ("max_active", C.c_int32), ("batch_window_ms", C.c_double),
     ]
 
 
@@ -603,6 +603,186 @@ def write_assoc_mv_txt(path: str, bim_path: str, results: dict):
                                             _ptr(arr["beta"]), _ptr(arr["cov"])))
 
 
+class Samples:
+    """The .fam sample list (PlinkReader::readFam, libCosmicCore/src/plink_reader.cpp:34-48):
+    FID / IID keys in file order and the .fam phenotype column."""
+
+    def __init__(self, fam_path: str):
+        self._h = C.c_void_p()
+        _check(_abi.lib().cs_fam_read(fam_path.encode(), C.byref(self._h)))
+        n = C.c_int64()
+        _check(_abi.lib().cs_samples_count(self._h, C.byref(n)))
+        self.n = n.value
+
+    def __len__(self):
+        return self.n
+
+    def ids(self):
+        fid, iid = C.create_string_buffer(4096), C.create_string_buffer(4096)
+        out = []
+        for i in range(self.n):
+            _check(_abi.lib().cs_samples_id(self._h, i, fid, 4096, iid, 4096))
+            out.append((fid.value.decode(), iid.value.decode()))
+        return out
+
+    def fam_phenotype(self) -> np.ndarray:
+        y = np.empty(self.n)
+        _check(_abi.lib().cs_samples_fam_phenotype(self._h, _ptr(y)))
+        return y
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _abi.lib().cs_samples_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PhenoReader:
+    """PhenoReader (libCosmicCore/src/pheno_reader.cpp): load(path, col_idx) / align(samples)
+    for one trait, loadMatrix(path, cols) / alignMatrix(samples) for several."""
+
+    def __init__(self):
+        self._h = None
+
+    def _reset(self):
+        if self._h:
+            _abi.lib().cs_pheno_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def load(self, path: str, col_idx: int = 1, missing_val: float = -9.0):
+        self._reset()
+        _check(_abi.lib().cs_pheno_load(path.encode(), int(col_idx), float(missing_val),
+                                        C.byref(self._h)))
+
+    def loadMatrix(self, path: str, cols=(), missing_val: float = -9.0):
+        self._reset()
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        _check(_abi.lib().cs_pheno_load_matrix(path.encode(), _ptr(c) if len(c) else None,
+                                               len(c), float(missing_val), C.byref(self._h)))
+
+    def num_traits(self) -> int:
+        t = C.c_int32()
+        _check(_abi.lib().cs_pheno_traits(self._h, C.byref(t)))
+        return t.value
+
+    def align(self, samples: Samples):
+        """y in .fam order (NaN where unmatched or missing) and the matched count."""
+        y = np.empty(samples.n)
+        m = C.c_int64()
+        _check(_abi.lib().cs_pheno_align(self._h, samples._h, _ptr(y), C.byref(m)))
+        return y, m.value
+
+    def alignMatrix(self, samples: Samples):
+        t = self.num_traits()
+        Y = np.empty((t, samples.n))  # column-major n x t
+        m = C.c_int64()
+        _check(_abi.lib().cs_pheno_align_matrix(self._h, samples._h, _ptr(Y), samples.n, C.byref(m)))
+        return Y.T.copy(), m.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                _abi.lib().cs_pheno_destroy(self._h)
+        except Exception:
+            pass
+
+
+class CovarReader:
+    """CovarReader (libCosmicCore/src/covar_reader.cpp): load (quantitative, float) or
+    loadCategorical (k levels -> k - 1 dummies), then align(samples) -> float32 n x p."""
+
+    def __init__(self):
+        self._h = None
+
+    def _reset(self):
+        if self._h:
+            _abi.lib().cs_covar_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def load(self, path: str, missing_val: float = -9.0):
+        self._reset()
+        _check(_abi.lib().cs_covar_load(path.encode(), float(missing_val), C.byref(self._h)))
+
+    def loadCategorical(self, path: str, missing_val: str = "-9"):
+        self._reset()
+        _check(_abi.lib().cs_covar_load_categorical(path.encode(), missing_val.encode(),
+                                                    C.byref(self._h)))
+
+    def num_covars(self) -> int:
+        p = C.c_int32()
+        _check(_abi.lib().cs_covar_columns(self._h, C.byref(p)))
+        return p.value
+
+    def align(self, samples: Samples):
+        p = self.num_covars()
+        X = np.empty((p, samples.n), dtype=np.float32)  # column-major n x p
+        m = C.c_int64()
+        _check(_abi.lib().cs_covar_align(self._h, samples._h, _ptr(X) if p else None, samples.n,
+                                         C.byref(m)))
+        return X.T.copy(), m.value
+
+    def __del__(self):
+        try:
+            if self._h:
+                _abi.lib().cs_covar_destroy(self._h)
+        except Exception:
+            pass
+
+
+class DataFilter:
+    """DataFilter::filterSamples (libCosmicCore/src/data_filter.h:21-41)."""
+
+    @staticmethod
+    def filterSamples(y, X) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asarray(X, dtype=np.float32)
+        if X.ndim != 2 or X.shape[0] != y.shape[0]:
+            raise InvalidArgument(-1, "DataFilter: X and y dimension mismatch")
+        Xc = np.asfortranarray(X)
+        keep = np.empty(len(y), dtype=np.int32)
+        nk = C.c_int64()
+        _check(_abi.lib().cs_filter_samples(_ptr(y), len(y), _ptr(Xc) if X.shape[1] else None,
+                                            len(y), X.shape[1], _ptr(keep), C.byref(nk)))
+        return keep[:nk.value].copy()
+
+
+def load_association_inputs(bfile: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
+                            covar: str = None, missing_val: float = -9.0) -> dict:
+    """What the reference's standard LMM prepares before the engines run
+    (UnivariateModel::prepare, src/models/univariate_model.cpp:389-426, with
+    DataLoader::loadPhenotype / loadCovariates, src/data_loader.h:219-285): y from the
+    phenotype file (or the .fam column), X = [1 | quantitative | categorical dummies] as
+    float, the keep list of complete samples, and y / X restricted to it (X as float64
+    holding the float32 values).  Fewer than 10 kept samples is an error, as there."""
+    samples = Samples(bfile + ".fam")
+    if pheno:
+        pr = PhenoReader()
+        pr.load(pheno, mpheno, missing_val)
+        y, _ = pr.align(samples)
+    else:
+        y = samples.fam_phenotype()
+    cols = [np.ones((samples.n, 1), dtype=np.float32)]
+    if qcovar:
+        cr = CovarReader()
+        cr.load(qcovar, missing_val)
+        cols.append(cr.align(samples)[0])
+    if covar:
+        cr = CovarReader()
+        cr.loadCategorical(covar)
+        cols.append(cr.align(samples)[0])
+    X = np.concatenate(cols, axis=1)
+    keep = DataFilter.filterSamples(y, X)
+    if len(keep) < 10:
+        raise CosmicError(-1, "Too few valid samples.")
+    return {"samples": samples, "keep": keep, "y": y[keep].copy(),
+            "X": X[keep].astype(np.float64), "y_all": y, "X_all": X}
+
+
 def grm_variant_selection(stats: dict, min_maf: float = 0.01) -> np.ndarray:
     """Variants of the matrix-free GRM (src/gwas_scanner.cpp:258-277): 1/sd != 0 and
     MAF (from the all-sample mean) >= min_maf; extract/exclude lists are not modelled."""
@@ -692,6 +872,35 @@ def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=
     if genotypes is None:
         g.close()
     return res, diag
+
+
+def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
+                 covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
+                 min_rank=1, min_maf=0.01, precision="mixed", loco=True):
+    """`cosmicscanner gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback
+    --bfile BFILE --pheno PHENO --mpheno N [--qcovar Q] [--covar C] --out OUT` end to end:
+    the samples, phenotype, covariates and keep list as the reference prepares them
+    (load_association_inputs), the .bed resident on the device, the low-rank matrix-free
+    null model and scan (leave-one-chromosome-out when the .bim has more than one chromosome
+    and loco is set, as the reference's default), and OUT.assoc.txt (N = kept samples).
+    Returns (results, diagnostics, inputs)."""
+    inputs = load_association_inputs(bfile, pheno=pheno, mpheno=mpheno, qcovar=qcovar, covar=covar)
+    g = Genotypes.open_plink(bfile)
+    try:
+        if g.n_samples != len(inputs["samples"]):
+            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
+                                  ".fam and .bed sample counts differ")
+        bim = read_bim(bfile + ".bim")
+        res, diag = run_lmm_matrix_free(None, g.n_samples, g.n_snps, inputs["y"], inputs["X"],
+                                        keep=inputs["keep"], rank=rank, oversample=oversample,
+                                        seed=seed, trace_threshold=trace_threshold,
+                                        min_rank=min_rank, min_maf=min_maf, precision=precision,
+                                        genotypes=g, chrom=bim["chrom"] if loco else None,
+                                        loco=loco)
+        write_assoc_txt(out + ".assoc.txt", bfile + ".bim", res, n_obs=len(inputs["keep"]))
+    finally:
+        g.close()
+    return res, diag, inputs
 
 
 def _run_loco(g, keep, keep_arr, variants, chrom, y, X, rank, oversample, seed,

@@ -68,6 +68,23 @@ _SIGNATURES = {
     "cs_server_destroy": ([_P], None),
     "cs_write_assoc_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _I], _I),
     "cs_write_assoc_mv_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P], _I),
+    "cs_fam_read": ([C.c_char_p, _P], _I),
+    "cs_samples_count": ([_P, _P], _I),
+    "cs_samples_id": ([_P, _I64, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t], _I),
+    "cs_samples_fam_phenotype": ([_P, _P], _I),
+    "cs_samples_destroy": ([_P], None),
+    "cs_pheno_load": ([C.c_char_p, C.c_int32, _D, _P], _I),
+    "cs_pheno_load_matrix": ([C.c_char_p, _P, C.c_int32, _D, _P], _I),
+    "cs_pheno_traits": ([_P, _P], _I),
+    "cs_pheno_align": ([_P, _P, _P, _P], _I),
+    "cs_pheno_align_matrix": ([_P, _P, _P, _I64, _P], _I),
+    "cs_pheno_destroy": ([_P], None),
+    "cs_covar_load": ([C.c_char_p, _D, _P], _I),
+    "cs_covar_load_categorical": ([C.c_char_p, C.c_char_p, _P], _I),
+    "cs_covar_columns": ([_P, _P], _I),
+    "cs_covar_align": ([_P, _P, _P, _I64, _P], _I),
+    "cs_covar_destroy": ([_P], None),
+    "cs_filter_samples": ([_P, _I64, _P, _I64, C.c_int32, _P, _P], _I),
     "cs_profile_enable": ([_I], _I),
     "cs_profile_summary": ([C.c_char_p, C.c_size_t, _P], _I),
     "cs_launch_count": ([_P], _I),

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "cs_internal.h"
+#include "input_internal.h"
 
 namespace cs {
 cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_samples,
@@ -398,6 +399,164 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
                           const double* beta, const double* cov) {
     return guarded([&] {
         cs::write_assoc_mv_txt(out_path, bim_path, n_snps, d, freq, wald, pvalue, beta, cov);
+    });
+}
+
+int cs_fam_read(const char* fam_path, cs_samples** out) {
+    return guarded([&] {
+        if (!fam_path || !out) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_fam_read: null argument");
+        auto* s = new cs_samples();
+        try {
+            s->fam = cs::read_fam(fam_path);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int cs_samples_count(const cs_samples* s, int64_t* n) {
+    return guarded([&] {
+        if (!s || !n) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_samples_count: null argument");
+        *n = (int64_t)s->fam.size();
+    });
+}
+
+int cs_samples_id(const cs_samples* s, int64_t i, char* fid, size_t fid_len, char* iid, size_t iid_len) {
+    return guarded([&] {
+        if (!s || i < 0 || i >= (int64_t)s->fam.size())
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_samples_id: sample index out of range");
+        auto put = [](const std::string& v, char* buf, size_t len) {
+            if (!buf || len == 0) return;
+            const size_t k = std::min(len - 1, v.size());
+            std::memcpy(buf, v.data(), k);
+            buf[k] = '\0';
+        };
+        put(s->fam[i].fid, fid, fid_len);
+        put(s->fam[i].iid, iid, iid_len);
+    });
+}
+
+int cs_samples_fam_phenotype(const cs_samples* s, double* y) {
+    return guarded([&] {
+        if (!s || !y) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_samples_fam_phenotype: null argument");
+        for (size_t i = 0; i < s->fam.size(); ++i) y[i] = s->fam[i].phenotype;
+    });
+}
+
+void cs_samples_destroy(cs_samples* s) { delete s; }
+
+int cs_pheno_load(const char* path, int32_t col_idx, double missing_code, cs_pheno** out) {
+    return guarded([&] {
+        if (!path || !out) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_pheno_load: null argument");
+        auto* p = new cs_pheno();
+        try {
+            p->table.load(path, col_idx, missing_code);
+            p->table.n_traits = 1;
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+int cs_pheno_load_matrix(const char* path, const int32_t* cols, int32_t n_cols, double missing_code,
+                         cs_pheno** out) {
+    return guarded([&] {
+        if (!path || !out || n_cols < 0 || (n_cols > 0 && !cols))
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_pheno_load_matrix: null argument");
+        auto* p = new cs_pheno();
+        try {
+            p->table.load_matrix(path, std::vector<int>(cols, cols + n_cols), missing_code);
+        } catch (...) {
+            delete p;
+            throw;
+        }
+        *out = p;
+    });
+}
+
+int cs_pheno_traits(const cs_pheno* p, int32_t* n_traits) {
+    return guarded([&] {
+        if (!p || !n_traits) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_pheno_traits: null argument");
+        *n_traits = p->table.n_traits;
+    });
+}
+
+int cs_pheno_align(const cs_pheno* p, const cs_samples* s, double* y, int64_t* matched) {
+    return guarded([&] {
+        if (!p || !s || !y) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_pheno_align: null argument");
+        const int64_t m = p->table.align(s->fam, y);
+        if (matched) *matched = m;
+    });
+}
+
+int cs_pheno_align_matrix(const cs_pheno* p, const cs_samples* s, double* Y, int64_t ldy,
+                          int64_t* matched) {
+    return guarded([&] {
+        if (!p || !s || !Y || ldy < (int64_t)s->fam.size())
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_pheno_align_matrix: bad argument");
+        const int64_t m = p->table.align_matrix(s->fam, Y, ldy);
+        if (matched) *matched = m;
+    });
+}
+
+void cs_pheno_destroy(cs_pheno* p) { delete p; }
+
+int cs_covar_load(const char* path, double missing_code, cs_covar** out) {
+    return guarded([&] {
+        if (!path || !out) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_covar_load: null argument");
+        auto* c = new cs_covar();
+        try {
+            c->table.load(path, missing_code);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int cs_covar_load_categorical(const char* path, const char* missing_token, cs_covar** out) {
+    return guarded([&] {
+        if (!path || !out) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_covar_load_categorical: null argument");
+        auto* c = new cs_covar();
+        try {
+            c->table.load_categorical(path, missing_token ? missing_token : "-9");
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int cs_covar_columns(const cs_covar* c, int32_t* p) {
+    return guarded([&] {
+        if (!c || !p) cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_covar_columns: null argument");
+        *p = c->table.n_cols;
+    });
+}
+
+int cs_covar_align(const cs_covar* c, const cs_samples* s, float* X, int64_t ldx, int64_t* matched) {
+    return guarded([&] {
+        if (!c || !s || (c->table.n_cols > 0 && (!X || ldx < (int64_t)s->fam.size())))
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "cs_covar_align: bad argument");
+        const int64_t m = c->table.align(s->fam, X, ldx);
+        if (matched) *matched = m;
+    });
+}
+
+void cs_covar_destroy(cs_covar* c) { delete c; }
+
+int cs_filter_samples(const double* y, int64_t n, const float* X, int64_t ldx, int32_t p,
+                      int32_t* keep, int64_t* n_keep) {
+    return guarded([&] {
+        if (n < 0 || p < 0 || (n > 0 && (!y || !keep)) || (p > 0 && (!X || ldx < n)) || !n_keep)
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "DataFilter: X and y dimension mismatch");
+        *n_keep = cs::filter_samples(y, n, X, ldx, p, keep);
     });
 }
 

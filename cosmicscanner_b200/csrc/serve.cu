@@ -165,6 +165,11 @@ void cs_server::gpu_loop() {
             std::unique_lock<std::mutex> lk(mu);
             cv.wait(lk, [&] { return !jobs.empty() || (stop && active == 0); });
             if (jobs.empty()) break;
+            if (opt.batch_window_ms > 0.0) {
+                // hold the stack open for the other running requests' applies
+                cv.wait_for(lk, std::chrono::duration<double, std::milli>(opt.batch_window_ms),
+                            [&] { return (int)jobs.size() >= active || stop; });
+            }
             while (!jobs.empty() &&
                    (batch.empty() || K + jobs.front()->k <= opt.max_batch_columns)) {
                 batch.push_back(jobs.front());
@@ -344,6 +349,7 @@ void server_default_options(cs_server_options* o) {
     o->max_batch_columns = 4096;
     o->memory_budget_gb = 64.0;
     o->max_active = 8;
+    o->batch_window_ms = 0.0;
 }
 
 cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_var,
@@ -353,7 +359,8 @@ cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t
     try {
         if (opt_in) sv->opt = *opt_in;
         else server_default_options(&sv->opt);
-        if (sv->opt.max_batch_columns < 1 || sv->opt.max_active < 1 || sv->opt.rank < 1)
+        if (sv->opt.max_batch_columns < 1 || sv->opt.max_active < 1 || sv->opt.rank < 1 ||
+            !(sv->opt.batch_window_ms >= 0.0))
             fail(CS_ERR_INVALID_ARGUMENT, "bad server options");
         CS_CUDA(cudaGetDevice(&sv->device));
         sv->g = g;

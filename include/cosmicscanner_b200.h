@@ -257,6 +257,8 @@ typedef struct cs_server_options {
     int64_t max_batch_columns; /* right-hand sides per stacked apply (4096) */
     double memory_budget_gb;   /* admission budget for request working sets (64) */
     int32_t max_active;        /* requests running at once (8) */
+    double batch_window_ms;    /* after the first pending apply, wait up to this long (or until
+                                  every running request waits on an apply) before stacking (0) */
 } cs_server_options;
 
 typedef struct cs_serve_request {
@@ -326,6 +328,53 @@ int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snp
 int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
                           const double* freq, const double* wald, const double* pvalue,
                           const double* beta, const double* cov);
+
+/* ---------------------------------------------------------------- input side
+ * The samples, phenotypes, covariates and keep list that the reference's association path
+ * builds before the engines run, with its parsing rules:
+ *   cs_fam_read           PlinkReader::readFam (libCosmicCore/src/plink_reader.cpp:34-48)
+ *   cs_pheno_load         PhenoReader::load (libCosmicCore/src/pheno_reader.cpp:13-61):
+ *                         column col_idx (1-based, after FID IID), missing code within 1e-6
+ *                         and NA / na / NaN / nan / NAN -> NaN
+ *   cs_pheno_align        PhenoReader::align (:138-187): y in .fam order (NaN unmatched);
+ *                         a constant trait (>= 2 finite values) -> CS_ERR_INVALID_ARGUMENT
+ *                         with the reference's message
+ *   cs_pheno_load_matrix  PhenoReader::loadMatrix (:63-125), cols 1-based (NULL = all)
+ *   cs_pheno_align_matrix PhenoReader::alignMatrix (:189-215): Y n x traits, column-major
+ *   cs_covar_load         CovarReader::load (libCosmicCore/src/covar_reader.cpp:19-62):
+ *                         quantitative covariates as float, missing code within 1e-8 -> NaN
+ *   cs_covar_load_categorical  CovarReader::loadCategorical (:64-176): k levels -> k - 1
+ *                         dummy columns, the alphabetically first level the reference
+ *   cs_covar_align        CovarReader::align (:468-500): X n x p float, column-major
+ *   cs_filter_samples     DataFilter::filterSamples (libCosmicCore/src/data_filter.h:21-41):
+ *                         the rows whose y and covariates are all non-NaN, ascending
+ * Counts and matched numbers come back through out-parameters; tables are freed by their
+ * destroy call. */
+typedef struct cs_samples cs_samples;
+typedef struct cs_pheno cs_pheno;
+typedef struct cs_covar cs_covar;
+int cs_fam_read(const char* fam_path, cs_samples** out);
+int cs_samples_count(const cs_samples* s, int64_t* n);
+/* FID and IID of sample i, NUL-terminated, truncated to the buffer sizes */
+int cs_samples_id(const cs_samples* s, int64_t i, char* fid, size_t fid_len, char* iid, size_t iid_len);
+/* the .fam phenotype column (the reference uses it when no phenotype file is given) */
+int cs_samples_fam_phenotype(const cs_samples* s, double* y);
+void cs_samples_destroy(cs_samples* s);
+int cs_pheno_load(const char* path, int32_t col_idx, double missing_code, cs_pheno** out);
+int cs_pheno_load_matrix(const char* path, const int32_t* cols, int32_t n_cols, double missing_code,
+                         cs_pheno** out);
+int cs_pheno_traits(const cs_pheno* p, int32_t* n_traits);
+int cs_pheno_align(const cs_pheno* p, const cs_samples* s, double* y, int64_t* matched);
+int cs_pheno_align_matrix(const cs_pheno* p, const cs_samples* s, double* Y, int64_t ldy,
+                          int64_t* matched);
+void cs_pheno_destroy(cs_pheno* p);
+int cs_covar_load(const char* path, double missing_code, cs_covar** out);
+int cs_covar_load_categorical(const char* path, const char* missing_token, cs_covar** out);
+int cs_covar_columns(const cs_covar* c, int32_t* p);
+int cs_covar_align(const cs_covar* c, const cs_samples* s, float* X, int64_t ldx, int64_t* matched);
+void cs_covar_destroy(cs_covar* c);
+int cs_filter_samples(const double* y, int64_t n, const float* X, int64_t ldx, int32_t p,
+                      int32_t* keep, int64_t* n_keep);
 
 /* ---------------------------------------------------------------- instrumentation
  * No reference counterpart beyond the stage timers of src/gwas_scanner.cpp:42-49 and

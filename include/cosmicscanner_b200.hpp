@@ -225,4 +225,105 @@ class LmmEngine {
     cs_lmm* h_ = nullptr;
 };
 
+// ---- input side: the .fam samples, phenotype / covariate tables aligned to them and the keep
+// list (PlinkReader::readFam, PhenoReader, CovarReader, DataFilter).  Matrices are
+// column-major, NaN marks missing values.
+class Samples {
+   public:
+    explicit Samples(const std::string& fam_path) { check(cs_fam_read(fam_path.c_str(), &h_)); }
+    ~Samples() { cs_samples_destroy(h_); }
+    Samples(const Samples&) = delete;
+    Samples& operator=(const Samples&) = delete;
+    int64_t size() const {
+        int64_t n = 0;
+        check(cs_samples_count(h_, &n));
+        return n;
+    }
+    std::vector<double> famPhenotype() const {
+        std::vector<double> y(size());
+        check(cs_samples_fam_phenotype(h_, y.data()));
+        return y;
+    }
+    const cs_samples* handle() const { return h_; }
+
+   private:
+    cs_samples* h_ = nullptr;
+};
+
+class PhenoReader {
+   public:
+    PhenoReader() = default;
+    ~PhenoReader() { cs_pheno_destroy(h_); }
+    PhenoReader(const PhenoReader&) = delete;
+    PhenoReader& operator=(const PhenoReader&) = delete;
+    void load(const std::string& path, int col_idx = 1, double missing_val = -9.0) {
+        cs_pheno_destroy(h_);
+        h_ = nullptr;
+        check(cs_pheno_load(path.c_str(), col_idx, missing_val, &h_));
+    }
+    void loadMatrix(const std::string& path, const std::vector<int32_t>& cols, double missing_val = -9.0) {
+        cs_pheno_destroy(h_);
+        h_ = nullptr;
+        check(cs_pheno_load_matrix(path.c_str(), cols.empty() ? nullptr : cols.data(),
+                                   (int32_t)cols.size(), missing_val, &h_));
+    }
+    // y in .fam order; returns the matched count
+    int64_t align(const Samples& s, std::vector<double>& y) const {
+        y.assign(s.size(), 0.0);
+        int64_t m = 0;
+        check(cs_pheno_align(h_, s.handle(), y.data(), &m));
+        return m;
+    }
+    int64_t alignMatrix(const Samples& s, std::vector<double>& Y, int32_t& n_traits) const {
+        check(cs_pheno_traits(h_, &n_traits));
+        Y.assign(s.size() * n_traits, 0.0);
+        int64_t m = 0;
+        check(cs_pheno_align_matrix(h_, s.handle(), Y.data(), s.size(), &m));
+        return m;
+    }
+
+   private:
+    cs_pheno* h_ = nullptr;
+};
+
+class CovarReader {
+   public:
+    CovarReader() = default;
+    ~CovarReader() { cs_covar_destroy(h_); }
+    CovarReader(const CovarReader&) = delete;
+    CovarReader& operator=(const CovarReader&) = delete;
+    void load(const std::string& path, double missing_val = -9.0) {
+        cs_covar_destroy(h_);
+        h_ = nullptr;
+        check(cs_covar_load(path.c_str(), missing_val, &h_));
+    }
+    void loadCategorical(const std::string& path, const std::string& missing_val = "-9") {
+        cs_covar_destroy(h_);
+        h_ = nullptr;
+        check(cs_covar_load_categorical(path.c_str(), missing_val.c_str(), &h_));
+    }
+    // X (n x p, column-major, float) in .fam order; returns the matched count
+    int64_t align(const Samples& s, std::vector<float>& X, int32_t& p) const {
+        check(cs_covar_columns(h_, &p));
+        X.assign(s.size() * p, 0.0f);
+        int64_t m = 0;
+        check(cs_covar_align(h_, s.handle(), p ? X.data() : nullptr, s.size(), &m));
+        return m;
+    }
+
+   private:
+    cs_covar* h_ = nullptr;
+};
+
+// DataFilter::filterSamples: rows of y / X (n x p, column-major) without NaN, ascending
+inline std::vector<int32_t> filterSamples(const std::vector<double>& y, const std::vector<float>& X,
+                                          int32_t p) {
+    std::vector<int32_t> keep(y.size());
+    int64_t n_keep = 0;
+    check(cs_filter_samples(y.data(), (int64_t)y.size(), p ? X.data() : nullptr, (int64_t)y.size(),
+                            p, keep.data(), &n_keep));
+    keep.resize(n_keep);
+    return keep;
+}
+
 }  // namespace cs

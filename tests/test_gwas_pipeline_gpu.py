@@ -1,0 +1,88 @@
+"""The association path end to end from files, as `cosmicscanner gwas --model lmm --fastlmm
+--fastlmm-matrix-free` runs it: .bed/.bim/.fam, a phenotype file with missing values, a
+quantitative and a categorical covariate file, the keep list of complete samples
+(src/models/univariate_model.cpp:389-426), leave-one-chromosome-out over the .bim's two
+chromosomes (src/gwas_scanner.cpp:299-314, 464-472) and OUT.assoc.txt
+(src/gwas_output.cpp:123-183).  Compared with the oracle's low-rank null model and scan on
+the same analysed samples; tolerances as the single-null path (mixed form)."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+cs = pytest.importorskip("cosmicscanner_b200")
+synth = pytest.importorskip("cosmicscanner_b200.synth")
+
+
+def test_gwas_lmm_from_files(tmp_path):
+    n, m = 640, 2000
+    d = synth.cohort(n, m, 31, missing=0.02, n_causal=40, h2=0.5)
+    prefix = str(tmp_path / "cohort")
+    open(prefix + ".bed", "wb").write(d["bed"].tobytes())
+    chrom = np.array(["1"] * 1100 + ["2"] * 900)
+    with open(prefix + ".bim", "w") as f:
+        for j in range(m):
+            f.write(f"{chrom[j]}\trs{j}\t0\t{1000 + 10 * j}\tA\tG\n")
+    with open(prefix + ".fam", "w") as f:
+        for i in range(n):
+            f.write(f"FAM{i} IND{i} 0 0 1 -9\n")
+    rng = np.random.default_rng(3)
+    y = d["y"]
+    drop_y = set(rng.choice(n, 12, replace=False).tolist())
+    drop_q = set(rng.choice(n, 5, replace=False).tolist())
+    age = np.round(rng.normal(50, 10, n), 3)
+    site = rng.choice(["north", "east", "west"], n)
+    with open(str(tmp_path / "y.txt"), "w") as f:
+        f.write("FID IID trait\n")
+        for i in range(n):
+            v = ("-9" if i % 2 else "NA") if i in drop_y else repr(float(y[i]))
+            f.write(f"FAM{i} IND{i} {v}\n")
+    with open(str(tmp_path / "q.txt"), "w") as f:
+        for i in range(n):
+            f.write(f"FAM{i} IND{i} {'-9' if i in drop_q else age[i]}\n")
+    with open(str(tmp_path / "c.txt"), "w") as f:
+        for i in range(n):
+            f.write(f"FAM{i} IND{i} {site[i]}\n")
+    out = str(tmp_path / "res")
+    res, diags, inputs = cs.run_gwas_lmm(prefix, out, pheno=str(tmp_path / "y.txt"),
+                                         qcovar=str(tmp_path / "q.txt"),
+                                         covar=str(tmp_path / "c.txt"), rank=30,
+                                         precision="mixed")
+    keep = np.array([i for i in range(n) if i not in drop_y and i not in drop_q], dtype=np.int32)
+    assert np.array_equal(inputs["keep"], keep)
+    X = np.column_stack([np.ones(len(keep)), age[keep].astype(np.float32),
+                         (site[keep] == "north"), (site[keep] == "west")]).astype(np.float64)
+    # east is the reference level; the covariate file's decimals are read as float (direct
+    # decimal -> float rounding may differ in the last bit from float64 -> float32)
+    assert np.array_equal(inputs["X"][:, [0, 2, 3]], X[:, [0, 2, 3]])
+    assert np.allclose(inputs["X"][:, 1], X[:, 1], rtol=1e-6, atol=0)
+    X = inputs["X"]
+    assert np.array_equal(inputs["y"], y[keep])
+    assert list(diags) == ["1", "2"]
+    rows = d["bed"][3:].reshape(m, -1)
+    ref = oracle.Bed(rows, n)
+    variants = cs.grm_variant_selection(cs.Genotypes.from_bed_bytes(d["bed"], n, m).stats(), 0.01)
+    for c in ["1", "2"]:
+        loco = variants[chrom[variants] != c]
+        U, lam, r = ref.lowrank_prepare(y[keep], X, 30, keep=keep, variants=loco, n_threads=8)
+        assert abs(diags[c]["sigma2_g"] - r.sigma2_g) <= 1e-5 * r.sigma2_g
+        assert abs(diags[c]["sigma2_e"] - r.sigma2_e) <= 1e-5 * r.sigma2_e
+        idx = np.flatnonzero(chrom == c)
+        sub = oracle.Bed(rows[idx[0]:idx[-1] + 1], n)
+        o = sub.scan_lowrank(keep, U, lam, r.residual_eigenvalue, r.sigma2_g, r.sigma2_e,
+                             y[keep], X)
+        t = res["tested"][idx]
+        assert np.array_equal(t, o["tested"])
+        assert np.array_equal(res["freq"][idx][t], o["freq"][t])
+        assert np.abs(res["log10p"][idx][t] - o["log10p"][t]).max() < 1e-3
+        assert np.abs(res["beta"][idx][t] - o["beta"][t]).max() <= 1e-5 * np.abs(o["beta"][t]).max()
+    # the result file: the reference's header, one row per tested SNP, N = kept samples
+    lines = open(out + ".assoc.txt").read().splitlines()
+    assert lines[0].split("\t")[:7] == ["CHR", "SNP", "BP", "A1", "A2", "FREQ", "N"]
+    body = [l.split("\t") for l in lines[1:]]
+    assert len(body) == int(res["tested"].sum())
+    assert all(r[6] == str(len(keep)) for r in body)
+    first = int(np.flatnonzero(res["tested"])[0])
+    assert body[0][1] == f"rs{first}" and body[0][0] == chrom[first]

@@ -78,7 +78,8 @@ def test_mix_equals_alone(data, precision):
         alone.wait(rid)
         solo.append([alone.result(rid, t) for t in range(Y.shape[1])])
     alone.close()
-    mix = cs.Server(g, variants, rank=30, precision=precision, max_active=5)
+    # a batching window holds each stack open until every running request waits on an apply
+    mix = cs.Server(g, variants, rank=30, precision=precision, max_active=5, batch_window_ms=50.0)
     ids = [mix.submit(S, Y, X, b, e) for S, Y, X, b, e in reqs]
     for rid in ids:
         assert mix.wait(rid)["state"] == 2
