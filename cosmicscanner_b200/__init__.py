@@ -874,6 +874,27 @@ def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=
     return res, diag
 
 
+def write_scan_meta(out_prefix: str, requested_rank: int = 256, trace_threshold: float = 0.95):
+    """OUT.scan.meta.txt of the matrix-free low-rank LMM (src/gwas_scanner.cpp:93-108)."""
+    _check(_abi.lib().cs_write_scan_meta(out_prefix.encode(), int(requested_rank),
+                                         float(trace_threshold)))
+
+
+def write_low_rank_meta(out_prefix: str, rows, n: int, error_tol: float = 1.0,
+                        fallback: str = "none"):
+    """OUT.low_rank.meta.tsv (src/gwas_scanner.cpp:109-115, 409-428): rows = [(scope,
+    diagnostics dict from prepareLowRankMatrixFree)], scope "GLOBAL" or the chromosome."""
+    rows = list(rows)
+    diags = (LowRankDiagnostics * max(1, len(rows)))()
+    scopes = (C.c_char_p * max(1, len(rows)))()
+    for i, (scope, dd) in enumerate(rows):
+        for name, _ in LowRankDiagnostics._fields_:
+            setattr(diags[i], name, dd[name])
+        scopes[i] = str(scope).encode()
+    _check(_abi.lib().cs_write_low_rank_meta(out_prefix.encode(), len(rows), scopes, diags,
+                                             int(n), float(error_tol), fallback.encode()))
+
+
 def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
                  covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
                  min_rank=1, min_maf=0.01, precision="mixed", loco=True):
@@ -882,8 +903,9 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
     the samples, phenotype, covariates and keep list as the reference prepares them
     (load_association_inputs), the .bed resident on the device, the low-rank matrix-free
     null model and scan (leave-one-chromosome-out when the .bim has more than one chromosome
-    and loco is set, as the reference's default), and OUT.assoc.txt (N = kept samples).
-    Returns (results, diagnostics, inputs)."""
+    and loco is set, as the reference's default), OUT.assoc.txt (N = kept samples) and the
+    run metadata OUT.scan.meta.txt / OUT.low_rank.meta.tsv.  Returns (results, diagnostics,
+    inputs)."""
     inputs = load_association_inputs(bfile, pheno=pheno, mpheno=mpheno, qcovar=qcovar, covar=covar)
     g = Genotypes.open_plink(bfile)
     try:
@@ -898,6 +920,9 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
                                         genotypes=g, chrom=bim["chrom"] if loco else None,
                                         loco=loco)
         write_assoc_txt(out + ".assoc.txt", bfile + ".bim", res, n_obs=len(inputs["keep"]))
+        write_scan_meta(out, rank, trace_threshold)
+        scoped = list(diag.items()) if "sigma2_g" not in diag else [("GLOBAL", diag)]
+        write_low_rank_meta(out, scoped, n=len(inputs["keep"]))
     finally:
         g.close()
     return res, diag, inputs

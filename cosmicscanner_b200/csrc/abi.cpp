@@ -62,6 +62,10 @@ void server_destroy(cs_server* sv);
 void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
                         const double* freq, const double* wald, const double* p, const double* beta,
                         const double* cov);
+void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
+void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
+                         const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
+                         const char* fallback);
 void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                      const double* freq, const double* beta, const double* se, const double* p,
                      const double* log10p, const int32_t* tested, int stcg_columns);
@@ -399,6 +403,18 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
                           const double* beta, const double* cov) {
     return guarded([&] {
         cs::write_assoc_mv_txt(out_path, bim_path, n_snps, d, freq, wald, pvalue, beta, cov);
+    });
+}
+
+int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold) {
+    return guarded([&] { cs::write_scan_meta(out_prefix, requested_rank, trace_threshold); });
+}
+
+int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
+                           const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
+                           const char* fallback) {
+    return guarded([&] {
+        cs::write_low_rank_meta(out_prefix, n_rows, scopes, diags, n, error_tol, fallback);
     });
 }
 

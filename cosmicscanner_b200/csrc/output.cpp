@@ -14,6 +14,7 @@
 // SE = sqrt of the Var(beta) diagonal; a negative or non-finite variance is an error).
 #include <cmath>
 #include <fstream>
+#include <iomanip>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -111,6 +112,59 @@ void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_sn
     }
     ofs.flush();
     if (!ofs) fail(CS_ERR_IO, "Error writing output file: " + std::string(out_path));
+}
+
+void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold) {
+    if (!out_prefix) fail(CS_ERR_INVALID_ARGUMENT, "write_scan_meta: null argument");
+    const std::string path = std::string(out_prefix) + ".scan.meta.txt";
+    std::ofstream meta(path);
+    if (!meta) fail(CS_ERR_IO, "Cannot open output file: " + path);
+    meta << "Item\tValue\n"
+         << "analysis_model\tunivariate_lmm\n"
+         << "requested_scan_tier\tlegacy_default\n"
+         << "resolved_scan_tier\tapprox\n"
+         << "snp_vc_strategy\tfixed_null\n"
+         << "SNP_MODEL\tadditive\n"
+         << "HWE_APPLIED\tfalse\n"
+         << "HWE_METHOD\tNONE\n"
+         << "HWE_REASON_IF_SKIPPED\tFILTER_DISABLED\n"
+         << "matrix_approximation\tfastlmm_auto_trace\n"
+         << "requested_rank\t" << requested_rank << "\n"
+         << "trace_threshold\t" << trace_threshold << "\n"
+         << "RANK_SELECTION\tAUTO_TRACE\n";
+    meta.flush();
+    if (!meta) fail(CS_ERR_IO, "Error writing output file: " + path);
+}
+
+void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
+                         const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
+                         const char* fallback) {
+    if (!out_prefix || n_rows < 0 || (n_rows > 0 && (!scopes || !diags)))
+        fail(CS_ERR_INVALID_ARGUMENT, "write_low_rank_meta: null argument");
+    const std::string path = std::string(out_prefix) + ".low_rank.meta.tsv";
+    std::ofstream meta(path);
+    if (!meta) fail(CS_ERR_IO, "Cannot open output file: " + path);
+    meta << "SCOPE\tALGORITHM\tREQUESTED_RANK\tEFFECTIVE_RANK\tSKETCH_SIZE"
+         << "\tRESIDUAL_EIGENVALUE\tRELATIVE_FROBENIUS_ERROR\tERROR_TOLERANCE"
+         << "\tDECOMPOSITION_SECONDS\tESTIMATED_PEAK_BYTES"
+         << "\tFULL_EIGEN_ESTIMATED_PEAK_BYTES\tSELECTED_RANK\tTOTAL_RANK"
+         << "\tTRACE_FRACTION\tRANK_SELECTION\tFALLBACK\n";
+    for (int32_t r = 0; r < n_rows; ++r) {
+        const cs_lowrank_diagnostics& d = diags[r];
+        const long long rank = d.effective_rank, sk = d.sketch_size;
+        const long long peak = 8LL * (2LL * n * sk + (long long)n * rank + sk * sk);
+        // one stream: the precision set before RESIDUAL_EIGENVALUE stays for the rest of the
+        // row and for the following rows, as in the reference
+        meta << (scopes[r] ? scopes[r] : "GLOBAL") << "\trandomized_subspace_iteration_tail_mean_woodbury"
+             << "\t" << d.effective_rank << "\t" << d.effective_rank << "\t" << d.sketch_size
+             << "\t" << std::setprecision(12) << d.residual_eigenvalue << "\t"
+             << d.relative_frobenius_error << "\t" << error_tol << "\t" << d.seconds << "\t" << peak
+             << "\t" << (24LL * n * n) << "\t" << d.effective_rank << "\t" << n << "\t"
+             << d.trace_fraction << "\tMATRIX_FREE_AUTO_TRACE\t" << (fallback ? fallback : "none")
+             << "\n";
+    }
+    meta.flush();
+    if (!meta) fail(CS_ERR_IO, "Error writing output file: " + path);
 }
 
 }  // namespace cs

@@ -329,6 +329,22 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
                           const double* freq, const double* wald, const double* pvalue,
                           const double* beta, const double* cov);
 
+/* Run metadata of the matrix-free low-rank LMM, as src/gwas_scanner.cpp writes them:
+ *   cs_write_scan_meta        OUT.scan.meta.txt (:93-108) for `--fastlmm
+ *                             --fastlmm-matrix-free` with default scan tier, additive model and
+ *                             no HWE filter; requested_rank = --fastlmm-max-rank
+ *   cs_write_low_rank_meta    OUT.low_rank.meta.tsv header (:109-115) and one row per null
+ *                             model (:409-428): scope "GLOBAL" or the LOCO chromosome, the
+ *                             diagnostics of cs_lmm_prepare_lowrank_matrix_free, the analysed
+ *                             sample count n, --lmm-low-rank-error-tol and the fallback label
+ *                             ("none" with --fastlmm-no-fallback).  Like the reference's
+ *                             matrix-free engine (src/lmm_engine.cpp:1077-1094), REQUESTED_RANK
+ *                             reports the selected rank. */
+int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
+int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
+                           const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
+                           const char* fallback);
+
 /* ---------------------------------------------------------------- input side
  * The samples, phenotypes, covariates and keep list that the reference's association path
  * builds before the engines run, with its parsing rules:

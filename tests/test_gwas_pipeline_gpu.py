@@ -86,3 +86,9 @@ def test_gwas_lmm_from_files(tmp_path):
     assert all(r[6] == str(len(keep)) for r in body)
     first = int(np.flatnonzero(res["tested"])[0])
     assert body[0][1] == f"rs{first}" and body[0][0] == chrom[first]
+    # run metadata: one low-rank row per LOCO null model
+    meta = [l.split("\t") for l in open(out + ".low_rank.meta.tsv").read().splitlines()]
+    assert [r[0] for r in meta[1:]] == ["1", "2"]
+    assert all(r[12] == str(len(keep)) and r[-1] == "none" for r in meta[1:])
+    assert [r[3] for r in meta[1:]] == [str(diags[c]["effective_rank"]) for c in ["1", "2"]]
+    assert "requested_rank\t30" in open(out + ".scan.meta.txt").read()

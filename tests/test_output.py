@@ -94,3 +94,36 @@ def test_assoc_mv_txt(tmp_path):
     res["cov"][0, 1, 1] = -1.0
     with pytest.raises(cs.CosmicError):
         cs.write_assoc_mv_txt(str(out), str(bim), res)
+
+
+def test_scan_and_low_rank_meta(tmp_path):
+    """OUT.scan.meta.txt (src/gwas_scanner.cpp:93-108) and OUT.low_rank.meta.tsv (:109-115,
+    409-428): the reference's items, columns and number formatting (default 6 significant
+    digits; 12 from RESIDUAL_EIGENVALUE on, kept for the following rows)."""
+    out = str(tmp_path / "run")
+    cs.write_scan_meta(out, 256, 0.95)
+    lines = open(out + ".scan.meta.txt").read().splitlines()
+    assert lines[0] == "Item\tValue"
+    items = dict(l.split("\t") for l in lines[1:])
+    assert items["analysis_model"] == "univariate_lmm"
+    assert items["resolved_scan_tier"] == "approx" and items["snp_vc_strategy"] == "fixed_null"
+    assert items["matrix_approximation"] == "fastlmm_auto_trace"
+    assert items["requested_rank"] == "256" and items["trace_threshold"] == "0.95"
+    assert items["RANK_SELECTION"] == "AUTO_TRACE" and items["HWE_APPLIED"] == "false"
+    base = dict(requested_rank=256, effective_rank=30, sketch_size=40, trace_threshold_met=1,
+                residual_eigenvalue=0.123456789012345, relative_frobenius_error=0.0123456789,
+                trace=1.0, trace_fraction=0.987654321, sigma2_g=0.5, sigma2_e=0.5, delta=1.0,
+                log_eta=0.0, reml_objective=0.0, seconds=1.5)
+    other = dict(base, effective_rank=28, residual_eigenvalue=0.2, seconds=2.25)
+    cs.write_low_rank_meta(out, [("1", base), ("2", other)], n=600)
+    rows = [l.split("\t") for l in open(out + ".low_rank.meta.tsv").read().splitlines()]
+    assert rows[0][:3] == ["SCOPE", "ALGORITHM", "REQUESTED_RANK"] and rows[0][-1] == "FALLBACK"
+    assert len(rows[0]) == 16
+    n = 600
+    for r, scope, d in ((rows[1], "1", base), (rows[2], "2", other)):
+        k, sk = d["effective_rank"], d["sketch_size"]
+        assert r == [scope, "randomized_subspace_iteration_tail_mean_woodbury", str(k), str(k),
+                     str(sk), "%.12g" % d["residual_eigenvalue"],
+                     "%.12g" % d["relative_frobenius_error"], "1", "%.12g" % d["seconds"],
+                     str(8 * (2 * n * sk + n * k + sk * sk)), str(24 * n * n), str(k), str(n),
+                     "%.12g" % d["trace_fraction"], "MATRIX_FREE_AUTO_TRACE", "none"]
