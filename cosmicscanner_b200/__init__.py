@@ -426,17 +426,49 @@ class StcgVce:
             pass
 
 
-def write_assoc_txt(path: str, bim_path: str, results: dict, n_obs: int, stcg_columns=False):
-    """Writes `.assoc.txt` (src/gwas_output.cpp:123-183) from a scan result dict."""
-    m = len(results["p"])
+ASSOC_LAYOUTS = {"unified": 0, "stcg": 1, "ssf": 2}
+
+
+def _result_arrays(results):
     arr = {k: np.ascontiguousarray(results[k], dtype=np.float64)
            for k in ("freq", "beta", "se", "p", "log10p")}
     tested = results.get("tested")
     tested = None if tested is None else np.ascontiguousarray(tested, dtype=np.int32)
-    _check(_abi.lib().cs_write_assoc_txt(path.encode(), bim_path.encode(), m, int(n_obs),
-                                         _ptr(arr["freq"]), _ptr(arr["beta"]), _ptr(arr["se"]),
-                                         _ptr(arr["p"]), _ptr(arr["log10p"]), _ptr(tested),
-                                         int(bool(stcg_columns))))
+    return arr, tested
+
+
+def write_assoc_txt(path: str, bim_path: str, results: dict, n_obs: int, stcg_columns=False,
+                    layout: str = None, gzip: bool = False, order=None):
+    """Writes `.assoc.txt` (src/gwas_output.cpp:123-183) from a scan result dict.  layout
+    "stcg" (or stcg_columns) gives `.stcg.assoc.txt`, "ssf" the `--out-ssf` GWAS-SSF rows;
+    gzip the `--out-gz` form; order the SNP indices in row order (default .bim order)."""
+    m = len(results["p"])
+    arr, tested = _result_arrays(results)
+    if layout is None:
+        layout = "stcg" if stcg_columns else "unified"
+    if layout not in ASSOC_LAYOUTS:
+        raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT, f"unknown layout {layout!r}")
+    if order is not None:
+        order = np.ascontiguousarray(order, dtype=np.int64)
+    _check(_abi.lib().cs_write_assoc(path.encode(), bim_path.encode(), m, int(n_obs),
+                                     _ptr(arr["freq"]), _ptr(arr["beta"]), _ptr(arr["se"]),
+                                     _ptr(arr["p"]), _ptr(arr["log10p"]), _ptr(tested),
+                                     _ptr(order), 0 if order is None else len(order),
+                                     ASSOC_LAYOUTS[layout], int(bool(gzip))))
+
+
+def append_cosmic_sumstats(path: str, bim_path: str, results: dict, n_obs: int,
+                           model: str = "LMM", append: bool = False, gzip: bool = False,
+                           created: str = None):
+    """`OUT.cosmic.sumstats` (GwasScanner::appendCosmicSumstats, src/gwas_output.cpp:186-234):
+    append=False replaces the file and writes the header (created: the "# Created:" text,
+    default the current UTC time), append=True adds the rows of another chromosome."""
+    m = len(results["p"])
+    arr, tested = _result_arrays(results)
+    _check(_abi.lib().cs_append_cosmic_sumstats(
+        path.encode(), bim_path.encode(), m, int(n_obs), _ptr(arr["freq"]), _ptr(arr["beta"]),
+        _ptr(arr["se"]), _ptr(arr["p"]), _ptr(arr["log10p"]), _ptr(tested), model.encode(),
+        int(bool(append)), int(bool(gzip)), None if created is None else created.encode()))
 
 
 # ---------------------------------------------------------------- serving loop
@@ -880,6 +912,15 @@ def write_scan_meta(out_prefix: str, requested_rank: int = 256, trace_threshold:
                                          float(trace_threshold)))
 
 
+def append_scan_common_meta(out_prefix: str, n: int, loco: bool, covariate_projection=True,
+                            vce_converged=True, model: str = "additive"):
+    """The lines appended to OUT.scan.meta.txt after the scan (src/gwas_output_schema.h:57-73,
+    src/gwas_scanner.cpp:507-509)."""
+    _check(_abi.lib().cs_append_scan_common_meta(out_prefix.encode(), model.encode(), int(n),
+                                                 int(bool(loco)), int(bool(covariate_projection)),
+                                                 int(bool(vce_converged))))
+
+
 def write_low_rank_meta(out_prefix: str, rows, n: int, error_tol: float = 1.0,
                         fallback: str = "none"):
     """OUT.low_rank.meta.tsv (src/gwas_scanner.cpp:109-115, 409-428): rows = [(scope,
@@ -897,15 +938,18 @@ def write_low_rank_meta(out_prefix: str, rows, n: int, error_tol: float = 1.0,
 
 def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
                  covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
-                 min_rank=1, min_maf=0.01, precision="mixed", loco=True):
+                 min_rank=1, min_maf=0.01, precision="mixed", loco=True, out_gz=False,
+                 out_ssf=False, created=None):
     """`cosmicscanner gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback
     --bfile BFILE --pheno PHENO --mpheno N [--qcovar Q] [--covar C] --out OUT` end to end:
     the samples, phenotype, covariates and keep list as the reference prepares them
     (load_association_inputs), the .bed resident on the device, the low-rank matrix-free
     null model and scan (leave-one-chromosome-out when the .bim has more than one chromosome
-    and loco is set, as the reference's default), OUT.assoc.txt (N = kept samples) and the
-    run metadata OUT.scan.meta.txt / OUT.low_rank.meta.tsv.  Returns (results, diagnostics,
-    inputs)."""
+    and loco is set, as the reference's default), OUT.assoc.txt (N = kept samples; rows
+    chromosome by chromosome under LOCO; GWAS-SSF rows with out_ssf, gzip with out_gz),
+    OUT.cosmic.sumstats (one append per chromosome under LOCO; created fixes its "# Created:"
+    line) and the run metadata OUT.scan.meta.txt / OUT.low_rank.meta.tsv.  Returns (results,
+    diagnostics, inputs)."""
     inputs = load_association_inputs(bfile, pheno=pheno, mpheno=mpheno, qcovar=qcovar, covar=covar)
     g = Genotypes.open_plink(bfile)
     try:
@@ -919,10 +963,25 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
                                         min_rank=min_rank, min_maf=min_maf, precision=precision,
                                         genotypes=g, chrom=bim["chrom"] if loco else None,
                                         loco=loco)
-        write_assoc_txt(out + ".assoc.txt", bfile + ".bim", res, n_obs=len(inputs["keep"]))
+        n_keep = len(inputs["keep"])
         write_scan_meta(out, rank, trace_threshold)
         scoped = list(diag.items()) if "sigma2_g" not in diag else [("GLOBAL", diag)]
-        write_low_rank_meta(out, scoped, n=len(inputs["keep"]))
+        write_low_rank_meta(out, scoped, n=n_keep)
+        chrom = np.asarray(bim["chrom"]).astype(str)
+        used_loco = "sigma2_g" not in diag
+        groups = ([np.flatnonzero(chrom == c) for c in sort_chrom_labels(chrom)] if used_loco
+                  else [np.arange(g.n_snps)])
+        for i, idx in enumerate(groups):
+            part = dict(res)
+            mask = np.zeros(g.n_snps, dtype=np.int32)
+            mask[idx] = np.asarray(res["tested"])[idx]
+            part["tested"] = mask
+            append_cosmic_sumstats(out + ".cosmic.sumstats", bfile + ".bim", part, n_keep,
+                                   append=i > 0, gzip=out_gz, created=created)
+        write_assoc_txt(out + ".assoc.txt", bfile + ".bim", res, n_obs=n_keep,
+                        layout="ssf" if out_ssf else "unified", gzip=out_gz,
+                        order=np.concatenate(groups))
+        append_scan_common_meta(out, n_keep, loco=used_loco)
     finally:
         g.close()
     return res, diag, inputs

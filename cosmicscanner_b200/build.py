@@ -102,7 +102,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     newest = max(os.path.getmtime(o) for o in objs)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         cmd = [_nvcc(), "-ccbin", _host_cxx(), *ARCH, "-shared", "-o", LIB, *objs,
-               "-lcublas", "-lcusolver", "-lcudart", "-Xcompiler", "-fopenmp"]
+               "-lcublas", "-lcusolver", "-lcudart", "-lz", "-Xcompiler", "-fopenmp"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

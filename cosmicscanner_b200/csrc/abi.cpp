@@ -69,6 +69,16 @@ void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* con
 void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                      const double* freq, const double* beta, const double* se, const double* p,
                      const double* log10p, const int32_t* tested, int stcg_columns);
+void write_assoc(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                 const double* freq, const double* beta, const double* se, const double* p,
+                 const double* log10p, const int32_t* tested, const int64_t* order,
+                 int64_t n_order, int layout, bool gzip);
+void append_cosmic_sumstats(const char* path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                            const double* freq, const double* beta, const double* se,
+                            const double* p, const double* log10p, const int32_t* tested,
+                            const char* model, bool append, bool gzip, const char* created);
+void append_scan_common_meta(const char* out_prefix, const char* model, int64_t n, bool loco,
+                             bool covariate_projection, bool vce_converged);
 }  // namespace cs
 
 namespace {
@@ -395,6 +405,35 @@ int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snp
     return guarded([&] {
         cs::write_assoc_txt(out_path, bim_path, n_snps, n_obs, freq, beta, se, pvalue, log10p,
                             tested, stcg_columns);
+    });
+}
+
+int cs_write_assoc(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                   const double* freq, const double* beta, const double* se, const double* pvalue,
+                   const double* log10p, const int32_t* tested, const int64_t* order,
+                   int64_t n_order, int layout, int gzip) {
+    return guarded([&] {
+        cs::write_assoc(out_path, bim_path, n_snps, n_obs, freq, beta, se, pvalue, log10p, tested,
+                        order, n_order, layout, gzip != 0);
+    });
+}
+
+int cs_append_cosmic_sumstats(const char* path, const char* bim_path, int64_t n_snps,
+                              int32_t n_obs, const double* freq, const double* beta,
+                              const double* se, const double* pvalue, const double* log10p,
+                              const int32_t* tested, const char* model, int append, int gzip,
+                              const char* created) {
+    return guarded([&] {
+        cs::append_cosmic_sumstats(path, bim_path, n_snps, n_obs, freq, beta, se, pvalue, log10p,
+                                   tested, model, append != 0, gzip != 0, created);
+    });
+}
+
+int cs_append_scan_common_meta(const char* out_prefix, const char* model, int64_t n, int loco,
+                               int covariate_projection, int vce_converged) {
+    return guarded([&] {
+        cs::append_scan_common_meta(out_prefix, model, n, loco != 0, covariate_projection != 0,
+                                    vce_converged != 0);
     });
 }
 

@@ -117,6 +117,8 @@ struct cs_kinship {
     cs::DeviceBuffer<uint8_t> own_packed;
     int64_t n_active = 0;                  // rows of `view` (selected variants with 1/sd != 0)
     std::vector<double> mean, inv_std;     // per view row
+    std::vector<int32_t> view_snp;         // per view row: its SNP (row of the .bed)
+    bool keep_identity = false;            // every sample, in .fam order
     std::vector<int32_t> counts;           // per view row: counts of codes 00,01,10,11
     cs::DeviceBuffer<double> d_lut;        // per view row: {(2-mu)s, 0, (1-mu)s, -mu s}
     cs::DeviceBuffer<double> d_lut_sq;     // squared entries (diagonal)
@@ -137,6 +139,9 @@ void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_
                             int64_t ldy, int precision, cudaStream_t s);
 void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                          int64_t ldy, cudaStream_t s);
+// The rows-pass output of the last mixed apply: W (R x k, column-major, ld R) with
+// W[t, c] = s_t^2 sum_i (G_ti - mu_t)[observed] x_ic; nullptr before any mixed apply.
+const double* mixed_rows_output(const cs_kinship* op, int64_t* R, int64_t* k);
 
 // The reference's Gaussian test matrix (std::normal_distribution over std::mt19937_64) on the
 // device, written row-major n x ld (omega.cu).

@@ -57,11 +57,14 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
         if (op->num_variants == 0) fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: no variants selected");
         cudaStream_t s = 0;
         std::vector<int32_t> active;
+        op->keep_identity = identity;
         if (!variants && identity) {
             op->view = cs_packed_view{g->packed.get(), M, N, g->stride};
             op->n_active = M;
             op->mean = g->mean;
             op->inv_std = g->inv_std;
+            op->view_snp.resize(M);
+            for (int64_t t = 0; t < M; ++t) op->view_snp[t] = (int32_t)t;
         } else {
             active.reserve(op->num_variants);
             for (int64_t t = 0; t < op->num_variants; ++t) {
@@ -90,6 +93,7 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
                 op->mean[t] = g->mean[active[t]];
                 op->inv_std[t] = g->inv_std[active[t]];
             }
+            op->view_snp = active;
         }
         const int64_t R = op->n_active;
         // code counts over the operator's samples (trace, mixed-form corrections)

@@ -836,6 +836,7 @@ struct MixedWorkspace {
 struct MixedOperator {
     MixedRows rows;
     MixedWorkspace ws;
+    int64_t last_k = 0;  // columns of ws.W from the last apply (0: none yet)
 };
 
 void destroy_mixed(MixedOperator* m) { delete m; }
@@ -1157,9 +1158,18 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     MixedOperator* m = mixed_for(op);
     m->ws.W.resize(R * k);
     // W^T = s o s o (Z-centred)^T X: the rows pass output already scaled for the samples pass
+    m->last_k = 0;
     rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s);
     samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s);
     check_status(m->ws, s);
+    m->last_k = k;
+}
+
+const double* mixed_rows_output(const cs_kinship* op, int64_t* R, int64_t* k) {
+    if (!op->mixed || op->mixed->last_k == 0) return nullptr;
+    *R = op->n_active;
+    *k = op->mixed->last_k;
+    return op->mixed->ws.W.get();
 }
 
 // Scan projection on tensor cores: T[t][c] = sum_i (g_ti - m_t)[observed] B[i][c] for every row

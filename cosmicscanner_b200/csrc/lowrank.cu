@@ -65,6 +65,15 @@ struct cs_lmm {
     cs_packed_view scan_view;
     std::vector<int32_t> scan_counts;
     cs::MixedScan* scan_mixed = nullptr;
+    // The last sketch apply's rows pass, kept for the scan (mixed form, every sample): the
+    // scan's U block is Z_c^T U = (Z_c^T Q) W_sel, so it needs no genotype pass.  d_ztq
+    // holds s_t^2 (Z_c^T Q)[t, :] per operator row t (R x sketch, column-major); snp_row maps
+    // a .bed row to its operator row (-1: none); d_s2inv = 1 / s_t^2 (0 where s_t = 0).
+    uint64_t sketch_g_uid = 0;
+    int64_t ztq_rows = 0, ztq_cols = 0;
+    cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u;
+    std::vector<int32_t> snp_row;
+    cs::DeviceBuffer<int32_t> d_win_rows;
     cs::DeviceBuffer<int32_t> d_counts, d_tested;
     cs::DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
     cs::DeviceBuffer<uint8_t> d_pass;
@@ -355,6 +364,20 @@ std::vector<double> project_on_basis(cs_lmm* l, const double* Z, int64_t m, cuda
 }
 
 // ---------------------------------------------------------------- scan kernels
+// T[j ldt + c] (c < r) = C[c + row_j r] / s_row^2, row_j = rows[j] (0 where row_j < 0): the
+// scan's U block from W_sel^T (Z_c^T Q)^T.
+__global__ void k_scan_u_block(const double* __restrict__ C, int64_t r, const int32_t* __restrict__ rows,
+                               const double* __restrict__ s2inv, int64_t M, double* __restrict__ T,
+                               int64_t ldt) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < M * r;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = e / r, c = e - j * r;
+        const int32_t row = rows[j];
+        T[j * ldt + c] = row >= 0 ? C[c + (int64_t)row * r] * s2inv[row] : 0.0;
+    }
+}
+
+
 // gamma_q / chisq_prob of src/lmm_engine.cpp:22-64 (series or continued fraction with a
 // 1e-7 relative stopping tolerance and at most 100 terms; 0 when neither converges).
 __device__ double d_gamma_q(double a, double x) {
@@ -565,6 +588,27 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     };
     lmm_prepare_lowrank_target(l, t, y, X, p, rank, oversample, seed, trace_threshold, min_rank,
                                diag, 0);
+    // keep the final sketch apply's rows pass for the scan (see cs_lmm::d_ztq)
+    int64_t R = 0, kq = 0;
+    const double* W = precision == CS_PRECISION_MIXED && op->keep_identity
+                          ? mixed_rows_output(op, &R, &kq)
+                          : nullptr;
+    if (W && kq == l->sketch_diag.sketch_size && R == (int64_t)op->view_snp.size() && R > 0) {
+        l->d_ztq.resize(R * kq);
+        CS_CUDA(cudaMemcpy(l->d_ztq.get(), W, 8 * R * kq, cudaMemcpyDeviceToDevice));
+        std::vector<double> s2inv(R);
+        l->snp_row.assign(op->g->n_snps, -1);
+        for (int64_t t2 = 0; t2 < R; ++t2) {
+            const double sv = op->inv_std[t2];
+            s2inv[t2] = sv != 0.0 ? 1.0 / (sv * sv) : 0.0;
+            l->snp_row[op->view_snp[t2]] = (int32_t)t2;
+        }
+        l->d_s2inv.resize(R);
+        CS_CUDA(cudaMemcpy(l->d_s2inv.get(), s2inv.data(), 8 * R, cudaMemcpyHostToDevice));
+        l->ztq_rows = R;
+        l->ztq_cols = kq;
+        l->sketch_g_uid = op->g->uid;
+    }
 }
 
 void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const double* y,
@@ -573,6 +617,8 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
                                 cs_lowrank_diagnostics* diag, cudaStream_t s) {
     const auto start = std::chrono::steady_clock::now();
     l->blas = shared_blas();  // the calling thread's handle
+    l->sketch_g_uid = 0;  // a new sketch: the kept rows pass (if any) no longer matches
+    l->ztq_cols = 0;
     const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
@@ -666,6 +712,8 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     l->d_U.resize(n * selected);
     CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_T, CUBLAS_OP_N, selected, (int)n, (int)sk, &one,
                         gram.get(), (int)sk, q.get(), (int)sk, &zero, l->d_U.get(), selected));
+    l->d_wsel.resize(sk * selected);  // W_sel (sk x selected, column-major) for the scan
+    CS_CUDA(cudaMemcpyAsync(l->d_wsel.get(), gram.get(), 8 * sk * selected, cudaMemcpyDeviceToDevice, s));
     l->n = n;
     l->rank = selected;
     l->lambda.assign(lead.begin(), lead.begin() + selected);
@@ -942,7 +990,44 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
             l->scan_mixed = nullptr;
             l->scan_mixed = mixed_scan_create(v, row_mean.data(), counts.data());
         }
-        mixed_scan_project(l->scan_mixed, Bm, bw, bw, l->d_T.get(), bw, s);
+        // The U block from the kept sketch apply when every analysed sample is in the
+        // operator (then the scan's centring means are the operator's) and every SNP that can
+        // be tested has an operator row; X and py still take one narrow genotype pass.
+        // (CS_B200_SCAN_REUSE=0 always takes the full projection)
+        const char* env = std::getenv("CS_B200_SCAN_REUSE");
+        bool reuse = !(env && env[0] == '0') && l->sketch_g_uid == g->uid && l->ztq_cols > 0 &&
+                     n_keep == g->n_samples && l->ztq_cols == l->sketch_diag.sketch_size;
+        for (int64_t i = 0; reuse && i < n_keep; ++i) reuse = keep[i] == i;
+        std::vector<int32_t> win_rows;
+        if (reuse) {
+            win_rows.resize(M);
+            for (int64_t j = 0; j < M; ++j) {
+                win_rows[j] = l->snp_row[snp_begin + j];
+                if (pass[j] && win_rows[j] < 0) reuse = false;
+            }
+        }
+        if (reuse) {
+            const int64_t R = l->ztq_rows, kq = l->ztq_cols;
+            const double one = 1.0, zero = 0.0;
+            l->d_ztq_u.resize(r * R);
+            // C (r x R) = W_sel^T (Z_c^T Q s^2)^T
+            CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_T, CUBLAS_OP_T, (int)r, (int)R, (int)kq, &one,
+                                l->d_wsel.get(), (int)kq, l->d_ztq.get(), (int)R, &zero,
+                                l->d_ztq_u.get(), (int)r));
+            l->d_win_rows.resize(M);
+            CS_CUDA(cudaMemcpyAsync(l->d_win_rows.get(), win_rows.data(), 4 * M,
+                                    cudaMemcpyHostToDevice, s));
+            {
+                prof::Scope ps("scan_u_block", s, 0.0, 16.0 * (double)M * r);
+                k_scan_u_block<<<(unsigned)std::min<int64_t>((M * r + 255) / 256, 32LL * num_sms()), 256,
+                                 0, s>>>(l->d_ztq_u.get(), r, l->d_win_rows.get(), l->d_s2inv.get(), M,
+                                         l->d_T.get(), bw);
+                CS_LAUNCH("scan_u_block");
+            }
+            mixed_scan_project(l->scan_mixed, Bm + r, bw, bw - r, l->d_T.get() + r, bw, s);
+        } else {
+            mixed_scan_project(l->scan_mixed, Bm, bw, bw, l->d_T.get(), bw, s);
+        }
     } else {
         Workspace ws;
         decode_gemm_rows_fp64(v, l->d_lut.get(), Bm, bw, bw, l->d_T.get(), bw, ws, s);

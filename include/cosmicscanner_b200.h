@@ -322,6 +322,34 @@ int cs_write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snp
                        const double* pvalue, const double* log10p, const int32_t* tested,
                        int stcg_columns);
 
+/* Row layouts of cs_write_assoc: the unified `.assoc.txt`, `.stcg.assoc.txt`, and the
+ * GWAS-SSF form of `--out-ssf` (src/gwas_output.cpp:81-82 header, :149-153 rows: chromosome,
+ * base_pair_location, effect_allele = A1, other_allele = A2, effect_allele_frequency,
+ * sample_size, beta, standard_error, p_value, variant_id). */
+enum { CS_ASSOC_UNIFIED = 0, CS_ASSOC_STCG = 1, CS_ASSOC_SSF = 2 };
+/* cs_write_assoc_txt with a layout, a row order and `--out-gz` (gzip != 0): the same text
+ * through zlib's gz writer as src/gzip_writer.cpp:12-55 opens it ("wb" +
+ * Z_DEFAULT_COMPRESSION, which zlib reads as level 1); the file name is the caller's (the
+ * reference keeps `.assoc.txt`).  order (NULL: .bim order) lists the SNP indices in the order
+ * their rows are written, each at most once — the reference writes the LOCO scan's rows
+ * chromosome by chromosome (src/gwas_scanner.cpp:449, 499). */
+int cs_write_assoc(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
+                   const double* freq, const double* beta, const double* se, const double* pvalue,
+                   const double* log10p, const int32_t* tested, const int64_t* order,
+                   int64_t n_order, int layout, int gzip);
+/* `OUT.cosmic.sumstats` as GwasScanner::appendCosmicSumstats writes it
+ * (src/gwas_output.cpp:186-234): append = 0 replaces the file and writes the comment header
+ * (version 1.0, "# Created: <created>" — NULL gives the current UTC time as
+ * "%Y-%m-%d %H:%M:%S UTC" — and "# Model: <model>" when model is not empty) and the column
+ * header; append = 1 adds rows only (the reference's later chromosomes; with gzip a new
+ * member).  One row per SNP with a non-NaN P and tested[j] != 0: BETA / SE / P at 10
+ * significant digits, AF / LOG10P / Z = BETA/SE / WEIGHT = 1/SE^2 at 6, INFO 1, WARNING ".". */
+int cs_append_cosmic_sumstats(const char* path, const char* bim_path, int64_t n_snps,
+                              int32_t n_obs, const double* freq, const double* beta,
+                              const double* se, const double* pvalue, const double* log10p,
+                              const int32_t* tested, const char* model, int append, int gzip,
+                              const char* created);
+
 /* `.assoc.mv.txt` of the multivariate model (src/models/multivariate_model.cpp:943-951,
  * src/models/multivariate_output.cpp:40-70) from cs_mvlmm_scan outputs: per SNP freq, wald,
  * p, beta (d), cov (d x d); rows with NaN P are skipped; SE_t = sqrt(cov[t][t]). */
@@ -341,6 +369,12 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
  *                             matrix-free engine (src/lmm_engine.cpp:1077-1094), REQUESTED_RANK
  *                             reports the selected rank. */
 int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
+/* The lines appended to OUT.scan.meta.txt after the scan (gwas_output::appendCommonMetadata,
+ * src/gwas_output_schema.h:57-73, called from src/gwas_scanner.cpp:507-509): MODEL ("additive"),
+ * N (analysed samples), the N / FREQ semantics, LOCO, COVARIATE_PROJECTION and VCE_CONVERGED
+ * (every null model converged; the low-rank route's REML either converges or fails). */
+int cs_append_scan_common_meta(const char* out_prefix, const char* model, int64_t n, int loco,
+                               int covariate_projection, int vce_converged);
 int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                            const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
                            const char* fallback);

@@ -103,6 +103,34 @@ def test_lowrank_mixed_matches_oracle():
     assert np.abs(out["log10p"][t] - exp["log10p"][t]).max() < 1e-3
 
 
+def test_lowrank_scan_reuses_sketch_rows(monkeypatch):
+    """With every sample analysed, the mixed scan takes its U block from the last sketch
+    apply ((Z^T Q) W_sel) and projects only X and Py through the genotypes; the result agrees
+    with the full projection (CS_B200_SCAN_REUSE=0) within the mixed tolerance, and the
+    LOCO-style operator (SNPs missing from it) falls back to the full projection."""
+    d = synth.cohort(1200, 3000, 41, missing=0.02, n_causal=40, h2=0.5)
+    n = d["n"]
+    g = cs.Genotypes.from_bed_bytes(d["bed"], n, d["m"])
+    y = d["y"]
+    X = d["X"].astype(np.float32).astype(np.float64)
+    keep = np.arange(n)
+    for variants in (None, np.arange(0, 2000, dtype=np.int32)):
+        op = cs.createKinshipOperator(g, None, variants)
+        eng = cs.LmmEngine()
+        eng.prepareLowRankMatrixFree(y, X, op, rank=50, precision="mixed")
+        a = eng.scan(g, keep, precision="mixed")
+        monkeypatch.setenv("CS_B200_SCAN_REUSE", "0")
+        b = eng.scan(g, keep, precision="mixed")
+        monkeypatch.delenv("CS_B200_SCAN_REUSE")
+        t = b["tested"]
+        assert np.array_equal(a["tested"], t) and t.sum() > 0.9 * d["m"]
+        assert np.array_equal(a["freq"][t], b["freq"][t])
+        for key in ("beta", "se"):
+            err = np.abs(a[key][t] - b[key][t]).max() / np.abs(b[key][t]).max()
+            assert err < 1e-6, (key, err)
+        assert np.abs(a["log10p"][t] - b["log10p"][t]).max() < 1e-4
+
+
 @pytest.mark.parametrize("mode", ["0", "1"])
 def test_operator_mixed_forced_cta_mode(mode):
     """CS_B200_CTA_PAIRS=0 (single CTAs for every width) and =1 (CTA pairs for every width)
