@@ -240,6 +240,14 @@ class LmmEngine:
         self._n = kinship.rows()
         return self.diagnostics
 
+    def prepareFromVce(self, vce: "EigenVce", use_residuals: bool = False):
+        """LmmEngine::prepareFromVce (src/lmm_engine.cpp:716-725): scan() then runs the exact
+        scan of lmm_engine.cpp:1363-1474 on the EigenVce's basis and null model
+        (use_residuals: the reference's setting for GRM algorithm 0)."""
+        _check(_abi.lib().cs_lmm_prepare_from_vce(self._h, vce._h, int(bool(use_residuals))))
+        self.diagnostics = dict(vce.result)
+        self._n = vce.n
+
     def getSigma2g(self):
         return self.diagnostics["sigma2_g"]
 
@@ -283,6 +291,172 @@ class LmmEngine:
     def close(self):
         if self._h:
             _abi.lib().cs_lmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- dense exact tier
+
+class GrmOptions(C.Structure):
+    _fields_ = [("min_maf", C.c_double), ("algorithm", C.c_int32)]
+
+
+class EigenVceResult(C.Structure):
+    _fields_ = [
+        ("sigma2_g", C.c_double), ("sigma2_e", C.c_double), ("delta", C.c_double),
+        ("sigma2_g_se", C.c_double), ("sigma2_e_se", C.c_double),
+        ("log_likelihood", C.c_double), ("max_score", C.c_double), ("n_eig", C.c_int64),
+        ("converged", C.c_int32), ("seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class GrmBuilder:
+    """GrmBuilder (libCosmicCore/src/grm_builder.h): the dense GRM over every sample of the
+    genotypes, resident on the device (algorithm 1 VanRaden by default; 0/3 Yang, 2 Zeng,
+    4 Vitezica, 5 TrueVar)."""
+
+    def __init__(self, min_maf: float = 0.01, algorithm: int = 1):
+        self.options = GrmOptions(float(min_maf), int(algorithm))
+        self._h = None
+
+    def compute(self, reader: Genotypes, variants=None):
+        self.close()
+        h = C.c_void_p()
+        v = None if variants is None else np.ascontiguousarray(variants, dtype=np.int32)
+        _check(_abi.lib().cs_grm_create(reader._h, _ptr(v), 0 if v is None else len(v),
+                                        C.byref(self.options), C.byref(h)))
+        self._h = h
+        return self
+
+    @classmethod
+    def from_matrix(cls, G) -> "GrmBuilder":
+        """A caller's own GRM (EigenVce::prepare accepts any symmetric G)."""
+        G = np.asfortranarray(G, dtype=np.float64)
+        b = cls()
+        h = C.c_void_p()
+        _check(_abi.lib().cs_grm_from_host(G.shape[0], _ptr(G), G.shape[0], C.byref(h)))
+        b._h = h
+        return b
+
+    @classmethod
+    def loco(cls, global_grm: "GrmBuilder", chrom_grm: "GrmBuilder") -> "GrmBuilder":
+        """The LOCO GRM of src/gwas_scanner.cpp:476-491 from the global GRM and the GRM of
+        one chromosome's SNPs (GrmBuilder::computeSplit's per-chromosome part)."""
+        b = cls(algorithm=global_grm.options.algorithm)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_grm_loco(global_grm._h, chrom_grm._h, C.byref(h)))
+        b._h = h
+        return b
+
+    def _info(self):
+        n, nv, s = C.c_int64(), C.c_int64(), C.c_double()
+        _check(_abi.lib().cs_grm_info(self._h, C.byref(n), C.byref(nv), C.byref(s)))
+        return n.value, nv.value, s.value
+
+    def getNumSamples(self) -> int:
+        return self._info()[0]
+
+    def getTotalSnps(self) -> int:
+        return self._info()[1]
+
+    def getSum2pq(self) -> float:
+        return self._info()[2]
+
+    def getGrm(self, keep=None) -> np.ndarray:
+        """G, or G[keep, keep] (DataFilter::subsetSquare), as a host array."""
+        if keep is None:
+            n = self.getNumSamples()
+            out = np.zeros((n, n), order="F")
+            _check(_abi.lib().cs_grm_copy(self._h, None, 0, _ptr(out), n))
+            return out
+        k = np.ascontiguousarray(keep, dtype=np.int32)
+        out = np.zeros((len(k), len(k)), order="F")
+        _check(_abi.lib().cs_grm_copy(self._h, _ptr(k), len(k), _ptr(out), len(k)))
+        return out
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_grm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class EigenVce:
+    """EigenVce (libCosmicCore/src/eigen_vce.h): prepare() = eigen_vce.cpp:19-63 on
+    G[keep, keep] (covariate projection by default), runNullModel() = the Brent branch
+    (eigen_vce.cpp:83-153, vce.cpp:3073-3175)."""
+
+    def __init__(self, use_covariate_projection: bool = True):
+        self.use_covariate_projection = bool(use_covariate_projection)
+        self._h = None
+        self.result = None
+
+    def prepare(self, y, X, grm: GrmBuilder, keep=None):
+        self.close()
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(np.asarray(X, dtype=np.float32).astype(np.float64))
+        k = None if keep is None else np.ascontiguousarray(keep, dtype=np.int32)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_eigen_vce_prepare(grm._h, _ptr(k), 0 if k is None else len(k),
+                                               _ptr(y), _ptr(X), X.shape[1],
+                                               int(self.use_covariate_projection), C.byref(h)))
+        self._h = h
+        n, ne, p = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(_abi.lib().cs_eigen_vce_dims(h, C.byref(n), C.byref(ne), C.byref(p)))
+        self.n, self.n_eig, self.p = n.value, ne.value, p.value
+        return self
+
+    def runNullModel(self) -> dict:
+        r = EigenVceResult()
+        _check(_abi.lib().cs_eigen_vce_run_null(self._h, C.byref(r)))
+        self.result = r.as_dict()
+        return self.result
+
+    def getSigma2g(self):
+        return self.result["sigma2_g"]
+
+    def getSigma2e(self):
+        return self.result["sigma2_e"]
+
+    def getDelta(self):
+        return self.result["delta"]
+
+    def _get(self, which):
+        D, Uty = np.zeros(self.n_eig), np.zeros(self.n_eig)
+        UtX = np.zeros((self.n_eig, self.p), order="F")
+        W = np.zeros((self.n, self.n_eig), order="F") if which == "W" else None
+        _check(_abi.lib().cs_eigen_vce_get(self._h, _ptr(D), _ptr(Uty), _ptr(UtX), _ptr(W),
+                                           self.n))
+        return {"D": D, "Uty": Uty, "UtX": UtX, "W": W}[which]
+
+    def getEigenvalues(self) -> np.ndarray:
+        return self._get("D")
+
+    def getUty(self) -> np.ndarray:
+        return self._get("Uty")
+
+    def getUtX(self) -> np.ndarray:
+        return self._get("UtX")
+
+    def getProjectedW(self) -> np.ndarray:
+        return self._get("W")
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_eigen_vce_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -906,8 +1080,70 @@ def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=
     return res, diag
 
 
-def write_scan_meta(out_prefix: str, requested_rank: int = 256, trace_threshold: float = 0.95):
-    """OUT.scan.meta.txt of the matrix-free low-rank LMM (src/gwas_scanner.cpp:93-108)."""
+def _chromosome_runs(chrom, c):
+    """The SNPs of chromosome c as contiguous [begin, end) runs of the .bim order."""
+    idx = np.flatnonzero(chrom == c)
+    breaks = np.flatnonzero(np.diff(idx) != 1)
+    return zip(np.r_[idx[0], idx[breaks + 1]], np.r_[idx[breaks] + 1, idx[-1] + 1])
+
+
+def run_lmm_exact(genotypes: Genotypes, y, X, keep=None, chrom=None, loco=True, min_maf=0.01,
+                  grm_algorithm=1, use_covariate_projection=True, precision="mixed"):
+    """The default `gwas --model lmm` route (src/gwas_scanner.cpp:131-215, 384-399, 458-499):
+    the dense GRM over every sample (GrmBuilder, VanRaden by default), G[keep, keep], EigenVce
+    (covariate projection, Brent null model), LmmEngine::prepareFromVce and the exact scan.
+    With chromosome labels spanning more than one chromosome and loco=True, per chromosome
+    the LOCO GRM G (S / S_loco) - raw_chr / S_loco, its own null model and the scan of that
+    chromosome's SNPs, in the reference's chromosome order.  use_residuals follows the
+    reference (GRM algorithm 0).  Returns (results dict, null-model dict; per chromosome
+    under LOCO)."""
+    g = genotypes
+    keep_arr = np.arange(g.n_samples, dtype=np.int32) if keep is None else np.asarray(keep, np.int32)
+    residuals = grm_algorithm == 0
+    glob = GrmBuilder(min_maf, grm_algorithm).compute(g)
+
+    def null_and_scan(grm, windows):
+        v = EigenVce(use_covariate_projection).prepare(y, X, grm, keep_arr)
+        r = v.runNullModel()
+        eng = LmmEngine()
+        eng.prepareFromVce(v, use_residuals=residuals)
+        parts = [(b, e, eng.scan_window(g, keep_arr, int(b), int(e), min_maf=min_maf,
+                                        precision=precision)) for b, e in windows]
+        eng.close()
+        v.close()
+        return r, parts
+
+    try:
+        m = g.n_snps
+        if chrom is not None and loco and len(set(str(c) for c in chrom)) > 1:
+            chrom = np.asarray(chrom).astype(str)
+            out = {k: np.full(m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
+            out["tested"] = np.zeros(m, dtype=bool)
+            diags = {}
+            for c in sort_chrom_labels(chrom):
+                chr_grm = GrmBuilder(min_maf, grm_algorithm).compute(
+                    g, np.flatnonzero(chrom == c).astype(np.int32))
+                loco_grm = GrmBuilder.loco(glob, chr_grm)
+                chr_grm.close()
+                diags[c], parts = null_and_scan(loco_grm, _chromosome_runs(chrom, c))
+                loco_grm.close()
+                for b, e, r in parts:
+                    for k in ("beta", "se", "p", "log10p", "freq", "tested"):
+                        out[k][b:e] = r[k]
+            return out, diags
+        diag, parts = null_and_scan(glob, [(0, m)])
+        return parts[0][2], diag
+    finally:
+        glob.close()
+
+
+def write_scan_meta(out_prefix: str, requested_rank: int = 256, trace_threshold: float = 0.95,
+                    full_eigen: bool = False):
+    """OUT.scan.meta.txt (src/gwas_scanner.cpp:93-108) of the matrix-free low-rank LMM, or of
+    the dense route with full_eigen."""
+    if full_eigen:
+        _check(_abi.lib().cs_write_scan_meta_full_eigen(out_prefix.encode()))
+        return
     _check(_abi.lib().cs_write_scan_meta(out_prefix.encode(), int(requested_rank),
                                          float(trace_threshold)))
 
@@ -939,7 +1175,7 @@ def write_low_rank_meta(out_prefix: str, rows, n: int, error_tol: float = 1.0,
 def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
                  covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
                  min_rank=1, min_maf=0.01, precision="mixed", loco=True, out_gz=False,
-                 out_ssf=False, created=None):
+                 out_ssf=False, created=None, exact=False):
     """`cosmicscanner gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback
     --bfile BFILE --pheno PHENO --mpheno N [--qcovar Q] [--covar C] --out OUT` end to end:
     the samples, phenotype, covariates and keep list as the reference prepares them
@@ -948,8 +1184,9 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
     and loco is set, as the reference's default), OUT.assoc.txt (N = kept samples; rows
     chromosome by chromosome under LOCO; GWAS-SSF rows with out_ssf, gzip with out_gz),
     OUT.cosmic.sumstats (one append per chromosome under LOCO; created fixes its "# Created:"
-    line) and the run metadata OUT.scan.meta.txt / OUT.low_rank.meta.tsv.  Returns (results,
-    diagnostics, inputs)."""
+    line) and the run metadata OUT.scan.meta.txt / OUT.low_rank.meta.tsv.  exact=True takes
+    the default dense route instead (`--model lmm` without --fastlmm: run_lmm_exact; no
+    .low_rank.meta.tsv).  Returns (results, diagnostics, inputs)."""
     inputs = load_association_inputs(bfile, pheno=pheno, mpheno=mpheno, qcovar=qcovar, covar=covar)
     g = Genotypes.open_plink(bfile)
     try:
@@ -957,16 +1194,22 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
             raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
                                   ".fam and .bed sample counts differ")
         bim = read_bim(bfile + ".bim")
-        res, diag = run_lmm_matrix_free(None, g.n_samples, g.n_snps, inputs["y"], inputs["X"],
-                                        keep=inputs["keep"], rank=rank, oversample=oversample,
-                                        seed=seed, trace_threshold=trace_threshold,
-                                        min_rank=min_rank, min_maf=min_maf, precision=precision,
-                                        genotypes=g, chrom=bim["chrom"] if loco else None,
-                                        loco=loco)
+        if exact:
+            res, diag = run_lmm_exact(g, inputs["y"], inputs["X"], keep=inputs["keep"],
+                                      chrom=bim["chrom"] if loco else None, loco=loco,
+                                      min_maf=min_maf, precision=precision)
+        else:
+            res, diag = run_lmm_matrix_free(None, g.n_samples, g.n_snps, inputs["y"], inputs["X"],
+                                            keep=inputs["keep"], rank=rank, oversample=oversample,
+                                            seed=seed, trace_threshold=trace_threshold,
+                                            min_rank=min_rank, min_maf=min_maf,
+                                            precision=precision, genotypes=g,
+                                            chrom=bim["chrom"] if loco else None, loco=loco)
         n_keep = len(inputs["keep"])
-        write_scan_meta(out, rank, trace_threshold)
-        scoped = list(diag.items()) if "sigma2_g" not in diag else [("GLOBAL", diag)]
-        write_low_rank_meta(out, scoped, n=n_keep)
+        write_scan_meta(out, rank, trace_threshold, full_eigen=exact)
+        if not exact:
+            scoped = list(diag.items()) if "sigma2_g" not in diag else [("GLOBAL", diag)]
+            write_low_rank_meta(out, scoped, n=n_keep)
         chrom = np.asarray(bim["chrom"]).astype(str)
         used_loco = "sigma2_g" not in diag
         groups = ([np.flatnonzero(chrom == c) for c in sort_chrom_labels(chrom)] if used_loco

@@ -40,6 +40,19 @@ _SIGNATURES = {
     "cs_kinship_diagonal": ([_P, _P], _I),
     "cs_kinship_destroy": ([_P], None),
     "cs_lmm_create": ([_P], _I),
+    "cs_grm_default_options": ([_P], None),
+    "cs_grm_create": ([_P, _P, _I64, _P, _P], _I),
+    "cs_grm_from_host": ([_I64, _P, _I64, _P], _I),
+    "cs_grm_loco": ([_P, _P, _P], _I),
+    "cs_grm_info": ([_P, _P, _P, _P], _I),
+    "cs_grm_copy": ([_P, _P, _I64, _P, _I64], _I),
+    "cs_grm_destroy": ([_P], None),
+    "cs_eigen_vce_prepare": ([_P, _P, _I64, _P, _P, _I64, _I, _P], _I),
+    "cs_eigen_vce_run_null": ([_P, _P], _I),
+    "cs_eigen_vce_dims": ([_P, _P, _P, _P], _I),
+    "cs_eigen_vce_get": ([_P, _P, _P, _P, _P, _I64], _I),
+    "cs_eigen_vce_destroy": ([_P], None),
+    "cs_lmm_prepare_from_vce": ([_P, _P, _I], _I),
     "cs_lmm_prepare_lowrank_matrix_free": (
         [_P, _P, _P, _P, _I64, _I, _I, _I64, _D, _I, _I, _P], _I),
     "cs_lmm_lowrank_basis": ([_P, _P, _I64, _P], _I),
@@ -69,6 +82,7 @@ _SIGNATURES = {
     "cs_write_assoc_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _I], _I),
     "cs_write_assoc_mv_txt": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P], _I),
     "cs_write_scan_meta": ([C.c_char_p, C.c_int32, _D], _I),
+    "cs_write_scan_meta_full_eigen": ([C.c_char_p], _I),
     "cs_write_assoc": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P, _P, _P, _I64,
                         _I, _I], _I),
     "cs_append_cosmic_sumstats": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P,

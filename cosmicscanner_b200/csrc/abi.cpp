@@ -6,6 +6,7 @@
 #include <string>
 
 #include "cs_internal.h"
+#include "dense_internal.h"
 #include "input_internal.h"
 
 namespace cs {
@@ -21,6 +22,16 @@ void kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t
                            int64_t ldy, cudaStream_t s);
 cs_lmm* lmm_create();
 void lmm_destroy(cs_lmm* l);
+cs_grm* grm_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
+                   const cs_grm_options* opt);
+cs_grm* grm_from_host(int64_t n, const double* G, int64_t ldg);
+cs_grm* grm_loco(const cs_grm* global, const cs_grm* chrom);
+void grm_copy(const cs_grm* grm, const int32_t* keep, int64_t n_keep, double* out, int64_t ld);
+cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                            const double* y, const double* X, int64_t p, bool projection);
+void eigen_run_null(cs_eigen_vce* v, cs_eigen_vce_result* out);
+void eigen_get(const cs_eigen_vce* v, double* D, double* Uty, double* UtX, double* W, int64_t ldw);
+void lmm_prepare_from_vce(cs_lmm* l, const cs_eigen_vce* v, bool use_residuals);
 void lmm_prepare_lowrank(cs_lmm* lmm, cs_kinship* op, const double* y, const double* X, int64_t p,
                          int rank, int oversample, int64_t seed, double trace_threshold,
                          int min_rank, int precision, cs_lowrank_diagnostics* diag);
@@ -62,7 +73,8 @@ void server_destroy(cs_server* sv);
 void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t d,
                         const double* freq, const double* wald, const double* p, const double* beta,
                         const double* cov);
-void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
+void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold,
+                     bool full_eigen);
 void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                          const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
                          const char* fallback);
@@ -263,6 +275,85 @@ int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, 
 
 void cs_lmm_destroy(cs_lmm* lmm) { cs::lmm_destroy(lmm); }
 
+void cs_grm_default_options(cs_grm_options* opt) {
+    if (!opt) return;
+    opt->min_maf = 0.01;
+    opt->algorithm = 1;
+}
+
+int cs_grm_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
+                  const cs_grm_options* opt, cs_grm** out) {
+    return guarded([&] {
+        require(g != nullptr && out != nullptr, "null argument");
+        *out = cs::grm_create(g, variants, n_variants, opt);
+    });
+}
+
+int cs_grm_loco(const cs_grm* global, const cs_grm* chrom, cs_grm** out) {
+    return guarded([&] {
+        require(out != nullptr, "null argument");
+        *out = cs::grm_loco(global, chrom);
+    });
+}
+
+int cs_grm_from_host(int64_t n, const double* G, int64_t ldg, cs_grm** out) {
+    return guarded([&] {
+        require(out != nullptr, "null argument");
+        *out = cs::grm_from_host(n, G, ldg);
+    });
+}
+
+int cs_grm_info(const cs_grm* grm, int64_t* n, int64_t* n_valid, double* sum_2pq) {
+    return guarded([&] {
+        require(grm != nullptr, "null argument");
+        if (n) *n = grm->n;
+        if (n_valid) *n_valid = grm->n_valid;
+        if (sum_2pq) *sum_2pq = grm->sum_2pq;
+    });
+}
+
+int cs_grm_copy(const cs_grm* grm, const int32_t* keep, int64_t n_keep, double* out, int64_t ld) {
+    return guarded([&] { cs::grm_copy(grm, keep, n_keep, out, ld); });
+}
+
+void cs_grm_destroy(cs_grm* grm) { delete grm; }
+
+int cs_eigen_vce_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep, const double* y,
+                         const double* X, int64_t p, int use_covariate_projection,
+                         cs_eigen_vce** out) {
+    return guarded([&] {
+        require(out != nullptr, "null argument");
+        *out = cs::eigen_prepare(grm, keep, n_keep, y, X, p, use_covariate_projection != 0);
+    });
+}
+
+int cs_eigen_vce_run_null(cs_eigen_vce* vce, cs_eigen_vce_result* out) {
+    return guarded([&] { cs::eigen_run_null(vce, out); });
+}
+
+int cs_eigen_vce_dims(const cs_eigen_vce* vce, int64_t* n, int64_t* n_eig, int64_t* p) {
+    return guarded([&] {
+        require(vce != nullptr && vce->d != nullptr, "null argument");
+        if (n) *n = vce->d->n;
+        if (n_eig) *n_eig = vce->d->n_eig;
+        if (p) *p = vce->d->p;
+    });
+}
+
+int cs_eigen_vce_get(const cs_eigen_vce* vce, double* D, double* Uty, double* UtX, double* W,
+                     int64_t ldw) {
+    return guarded([&] { cs::eigen_get(vce, D, Uty, UtX, W, ldw); });
+}
+
+void cs_eigen_vce_destroy(cs_eigen_vce* vce) { delete vce; }
+
+int cs_lmm_prepare_from_vce(cs_lmm* lmm, const cs_eigen_vce* vce, int use_residuals) {
+    return guarded([&] {
+        require(lmm != nullptr, "null argument");
+        cs::lmm_prepare_from_vce(lmm, vce, use_residuals != 0);
+    });
+}
+
 int cs_normal_matrix(uint64_t seed, int64_t n, int64_t cols, double* out) {
     return guarded([&] {
         require(n >= 0 && cols >= 0 && (out != nullptr || n * cols == 0), "bad arguments");
@@ -446,7 +537,11 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
 }
 
 int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold) {
-    return guarded([&] { cs::write_scan_meta(out_prefix, requested_rank, trace_threshold); });
+    return guarded([&] { cs::write_scan_meta(out_prefix, requested_rank, trace_threshold, false); });
+}
+
+int cs_write_scan_meta_full_eigen(const char* out_prefix) {
+    return guarded([&] { cs::write_scan_meta(out_prefix, 0, 0.0, true); });
 }
 
 int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,

@@ -24,6 +24,7 @@
 #include <random>
 
 #include "cs_internal.h"
+#include "dense_internal.h"
 #include "linalg_host.h"
 #include "vce_internal.h"
 
@@ -74,6 +75,11 @@ struct cs_lmm {
     cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u;
     std::vector<int32_t> snp_row;
     cs::DeviceBuffer<int32_t> d_win_rows;
+    // exact mode (LmmEngine::prepareFromVce): the dense eigenbasis and null model, and the
+    // scan's per-chunk buffers
+    std::shared_ptr<const cs::DenseNull> dense;
+    bool dense_residuals = false;
+    cs::DeviceBuffer<double> d_chunk, d_py, d_vinv, d_wutx, d_acc;
     cs::DeviceBuffer<int32_t> d_counts, d_tested;
     cs::DeviceBuffer<double> d_lut, d_T, d_gn2, d_cv, d_utx, d_inv, d_beta, d_se, d_p, d_l10;
     cs::DeviceBuffer<uint8_t> d_pass;
@@ -476,6 +482,80 @@ __global__ void k_scan_epilogue(ScanParams P) {
     }
 }
 
+// Exact scan (src/lmm_engine.cpp:1428-1474), one chunk of W_proj's columns at a time: per SNP
+// (one warp), score += T . Py, var += T^2 . V^-1 and xvg[a] += T . (V^-1 UtX)[:, a], with
+// T = W_proj[:, chunk]^T g_c.  acc is M x (2 + p).
+__global__ void k_exact_accumulate(const double* __restrict__ T, int64_t ldt, int64_t M,
+                                   int64_t kc, const double* __restrict__ py,
+                                   const double* __restrict__ vinv, const double* __restrict__ wutx,
+                                   int64_t ldw, int p, double* __restrict__ acc) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    constexpr int kMaxP = 16;
+    for (int64_t j = warp; j < M; j += n_warps) {
+        const double* t = T + j * ldt;
+        double sc = 0.0, var = 0.0, x[kMaxP];
+        for (int a = 0; a < p; ++a) x[a] = 0.0;
+        for (int64_t c = lane; c < kc; c += 32) {
+            const double tc = t[c];
+            sc += tc * py[c];
+            var += tc * tc * vinv[c];
+            for (int a = 0; a < p; ++a) x[a] += tc * wutx[c + a * ldw];
+        }
+        for (int off = 16; off; off >>= 1) {
+            sc += __shfl_xor_sync(0xffffffffu, sc, off);
+            var += __shfl_xor_sync(0xffffffffu, var, off);
+            for (int a = 0; a < p; ++a) x[a] += __shfl_xor_sync(0xffffffffu, x[a], off);
+        }
+        if (lane == 0) {
+            double* o = acc + j * (2 + p);
+            o[0] += sc;
+            o[1] += var;
+            for (int a = 0; a < p; ++a) o[2 + a] += x[a];
+        }
+    }
+}
+
+// Per SNP: var -= xvg^T (X^T V^-1 X)^-1 xvg unless use_residuals, then the Wald statistics
+// of src/lmm_engine.cpp:1439-1466 (no row unless var > 1e-12 and finite).
+__global__ void k_exact_finish(const double* __restrict__ acc, int p, int64_t M,
+                               const uint8_t* __restrict__ pass, const double* __restrict__ inv,
+                               int residuals, double* beta, double* se, double* pval,
+                               double* log10p, int32_t* tested) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < M;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        if (!pass[j]) {
+            tested[j] = 0;
+            continue;
+        }
+        const double* o = acc + j * (2 + p);
+        const double score = o[0];
+        double var = o[1];
+        if (!residuals && p > 0) {
+            double term2 = 0.0;
+            for (int a = 0; a < p; ++a) {
+                double mid = 0.0;
+                for (int b = 0; b < p; ++b) mid += inv[a + b * p] * o[2 + b];
+                term2 += o[2 + a] * mid;
+            }
+            var -= term2;
+        }
+        if (!(var > 1e-12) || !isfinite(var)) {
+            tested[j] = 0;
+            continue;
+        }
+        const double s = sqrt(var);
+        const double stat = score / s;
+        const double pv = d_chisq_prob(stat * stat, 1);
+        tested[j] = 1;
+        beta[j] = score / var;
+        se[j] = 1.0 / s;
+        pval[j] = pv;
+        log10p[j] = pv > 0.0 ? -log10(pv) : 300.0;
+    }
+}
+
 }  // namespace
 
 // Q (host, the tridiagonalising factor) and the QL rotations -> eigenvector matrix in l->d_eig.
@@ -619,6 +699,7 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     l->blas = shared_blas();  // the calling thread's handle
     l->sketch_g_uid = 0;  // a new sketch: the kept rows pass (if any) no longer matches
     l->ztq_cols = 0;
+    l->dense.reset();     // back to the low-rank mode
     const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
@@ -821,16 +902,244 @@ void lmm_scan(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_k
                     pvalue, log10p, freq, tested, 0);
 }
 
+// The analysed samples' packed view of SNPs [snp_begin, snp_end) with its code counts, cached
+// per (genotypes, window, keep) in l, and the per-SNP encoding of genotype_encoding.h:33-81
+// (additive, centred, missing -> the mean): FREQ, the MAF filter, the value table per code,
+// the row mean and ||g_c||^2.
+struct ScanEncoding {
+    std::vector<double> lut, gn2, fr, row_mean;
+    std::vector<uint8_t> pass;
+    bool cached = false;
+};
+
+static ScanEncoding scan_encoding(cs_lmm* l, const cs_genotypes* g, const int32_t* keep,
+                                  int64_t n_keep, int64_t snp_begin, int64_t snp_end,
+                                  double min_maf, cudaStream_t s) {
+    const int64_t M = snp_end - snp_begin;
+    ScanEncoding e;
+    const bool cached = l->scan_g_uid == g->uid && (int64_t)l->scan_keep.size() == n_keep &&
+                        l->scan_begin == snp_begin && l->scan_end == snp_end &&
+                        std::memcmp(l->scan_keep.data(), keep, 4 * n_keep) == 0;
+    if (!cached) {
+        mixed_scan_destroy(l->scan_mixed);
+        l->scan_mixed = nullptr;
+        bool identity = n_keep == g->n_samples;
+        for (int64_t i = 0; identity && i < n_keep; ++i) identity = keep[i] == i;
+        const uint8_t* first_row = g->packed.get() + snp_begin * g->stride;
+        l->scan_view = cs_packed_view{first_row, M, g->n_samples, g->stride};
+        if (!identity) {
+            const int64_t n = n_keep;
+            const int64_t stride = round_up((n + 3) / 4, kRowAlign);
+            l->scan_own.resize(std::max<int64_t>(1, M * stride));
+            DeviceBuffer<int32_t> d_keep;
+            d_keep.resize(n);
+            CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, 4 * n, cudaMemcpyHostToDevice, s));
+            repack(first_row, g->stride, nullptr, M, d_keep.get(), n, l->scan_own.get(),
+                   stride, s);
+            CS_CUDA(cudaStreamSynchronize(s));
+            l->scan_view = cs_packed_view{l->scan_own.get(), M, n, stride};
+        }
+        l->scan_counts.assign(4 * M, 0);
+        l->d_counts.resize(std::max<int64_t>(1, 4 * M));
+        if (M) {
+            row_code_counts(l->scan_view, l->d_counts.get(), s);
+            CS_CUDA(cudaMemcpyAsync(l->scan_counts.data(), l->d_counts.get(), 16 * M,
+                                    cudaMemcpyDeviceToHost, s));
+            CS_CUDA(cudaStreamSynchronize(s));
+        }
+        l->scan_g_uid = g->uid;
+        l->scan_begin = snp_begin;
+        l->scan_end = snp_end;
+        l->scan_keep.assign(keep, keep + n_keep);
+    }
+    e.cached = cached;
+    const std::vector<int32_t>& counts = l->scan_counts;
+    // ---- per-SNP encoding over the analysed samples (genotype_encoding.h:33-81)
+    e.lut.assign(4 * M, 0.0);
+    e.gn2.assign(M, 0.0);
+    e.fr.assign(M, 0.0);
+    e.row_mean.assign(M, 0.0);
+    e.pass.assign(M, 0);
+    std::vector<double>&lut = e.lut, &gn2 = e.gn2, &fr = e.fr, &row_mean = e.row_mean;
+    std::vector<uint8_t>& pass = e.pass;
+    for (int64_t j = 0; j < M; ++j) {
+        const int64_t c00 = counts[4 * j], c10 = counts[4 * j + 2], c11 = counts[4 * j + 3];
+        const int64_t obs = c00 + c10 + c11;
+        if (obs == 0) continue;
+        const int64_t isum = 2 * c00 + c10;
+        const double dosage_sum = (double)isum;
+        const double af = dosage_sum / (2.0 * (double)obs);
+        fr[j] = af;
+        pass[j] = obs >= 3 && std::min(af, 1.0 - af) >= min_maf;
+        // the encoded mean (additive model); rows that fail the filter are never reported
+        const double mean = dosage_sum / (double)obs;
+        row_mean[j] = mean;
+        lut[4 * j + 0] = 2.0 - mean;
+        lut[4 * j + 1] = 0.0;  // missing -> mean -> centred 0
+        lut[4 * j + 2] = 1.0 - mean;
+        lut[4 * j + 3] = 0.0 - mean;
+        const int64_t sq = 4 * c00 + c10;  // sum of squared dosages
+        gn2[j] = (double)(obs * sq - isum * isum) / (double)obs;
+    }
+    return e;
+}
+
+// Results to the caller's host arrays; untested SNPs get NaN statistics.
+static void scan_finish(cs_lmm* l, int64_t M, const std::vector<double>& fr, double* beta,
+                        double* se, double* pvalue, double* log10p, double* freq,
+                        int32_t* tested, cudaStream_t s) {
+    std::vector<int32_t> t(M);
+    CS_CUDA(cudaMemcpyAsync(t.data(), l->d_tested.get(), 4 * M, cudaMemcpyDeviceToHost, s));
+    if (beta) CS_CUDA(cudaMemcpyAsync(beta, l->d_beta.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (se) CS_CUDA(cudaMemcpyAsync(se, l->d_se.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (pvalue) CS_CUDA(cudaMemcpyAsync(pvalue, l->d_p.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    if (log10p) CS_CUDA(cudaMemcpyAsync(log10p, l->d_l10.get(), 8 * M, cudaMemcpyDeviceToHost, s));
+    CS_CUDA(cudaStreamSynchronize(s));
+    for (int64_t j = 0; j < M; ++j) {
+        if (tested) tested[j] = t[j];
+        if (freq) freq[j] = fr[j];
+        if (!t[j]) {
+            const double nan = std::numeric_limits<double>::quiet_NaN();
+            if (beta) beta[j] = nan;
+            if (se) se[j] = nan;
+            if (pvalue) pvalue[j] = nan;
+            if (log10p) log10p[j] = nan;
+        }
+    }
+}
+
+// LmmEngine::scan's exact branch (src/lmm_engine.cpp:1363-1474) over SNPs [snp_begin,
+// snp_end): the null quantities in the eigenbasis on the host (O(n p^2)), then per chunk of
+// W_proj's columns the projection T = W_proj[:, chunk]^T G_c of every SNP (tensor cores in the
+// mixed form, the FP64 decode-GEMM otherwise) folded into per-SNP sums.
+static void lmm_scan_exact(cs_lmm* l, const cs_genotypes* g, const int32_t* keep,
+                           int64_t n_keep, int64_t snp_begin, int64_t snp_end, double min_maf,
+                           int precision, double* beta, double* se, double* pvalue,
+                           double* log10p, double* freq, int32_t* tested, cudaStream_t s) {
+    const DenseNull& d = *l->dense;
+    const int64_t n = d.n, ne = d.n_eig, p = d.p, M = snp_end - snp_begin;
+    if (keep == nullptr || n_keep != n) fail(CS_ERR_INVALID_ARGUMENT, "Sample size mismatch in scan");
+    for (int64_t i = 0; i < n_keep; ++i)
+        if (keep[i] < 0 || keep[i] >= g->n_samples)
+            fail(CS_ERR_INVALID_ARGUMENT, "scan: sample index out of range");
+    CS_BLAS(cublasSetStream(l->blas, s));
+    std::vector<double> vinv(ne), wutx(ne * p), py(ne);
+    for (int64_t i = 0; i < ne; ++i) vinv[i] = 1.0 / (d.sigma2_g * d.D[i] + d.sigma2_e);
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t i = 0; i < ne; ++i) wutx[i + a * ne] = d.UtX[i + a * ne] * vinv[i];
+    std::vector<double> xvx_inv;
+    if (p > 0) {
+        std::vector<double> xvx(p * p, 0.0), L, Dl;
+        for (int64_t a = 0; a < p; ++a)
+            for (int64_t b = 0; b < p; ++b) {
+                double acc = 0.0;
+                for (int64_t i = 0; i < ne; ++i) acc += d.UtX[i + a * ne] * wutx[i + b * ne];
+                xvx[a + b * p] = acc;
+            }
+        if (!la::ldlt(xvx, (int)p, L, Dl))
+            fail(CS_ERR_NUMERIC, "LMM scan: X^T V^-1 X is singular");
+        xvx_inv = la::ldlt_inverse(L, Dl, (int)p);
+    }
+    std::vector<double> xvy(p, 0.0), bx(p, 0.0);
+    for (int64_t i = 0; i < ne; ++i)
+        for (int64_t a = 0; a < p; ++a) xvy[a] += vinv[i] * (d.UtX[i + a * ne] * d.Uty[i]);
+    for (int64_t a = 0; a < p; ++a)
+        for (int64_t b = 0; b < p; ++b) bx[a] += xvx_inv[a + b * p] * xvy[b];
+    for (int64_t i = 0; i < ne; ++i) {
+        double r = d.Uty[i];
+        for (int64_t a = 0; a < p; ++a) r -= d.UtX[i + a * ne] * bx[a];
+        py[i] = r * vinv[i];
+    }
+    prof::HostScope hs_scan("scan_host_setup");
+    ScanEncoding enc = scan_encoding(l, g, keep, n_keep, snp_begin, snp_end, min_maf, s);
+    for (auto* b : {&l->d_beta, &l->d_se, &l->d_p, &l->d_l10}) b->resize(std::max<int64_t>(1, M));
+    l->d_tested.resize(std::max<int64_t>(1, M));
+    if (M == 0) return;
+    l->d_lut.resize(4 * M);
+    l->d_pass.resize(M);
+    l->d_py.resize(std::max<int64_t>(1, ne));
+    l->d_vinv.resize(std::max<int64_t>(1, ne));
+    l->d_wutx.resize(std::max<int64_t>(1, ne * p));
+    l->d_inv.resize(std::max<int64_t>(1, p * p));
+    l->d_acc.resize(M * (2 + p));
+    CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), enc.lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), enc.pass.data(), M, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_py.get(), py.data(), 8 * ne, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaMemcpyAsync(l->d_vinv.get(), vinv.data(), 8 * ne, cudaMemcpyHostToDevice, s));
+    if (p) {
+        CS_CUDA(cudaMemcpyAsync(l->d_wutx.get(), wutx.data(), 8 * ne * p, cudaMemcpyHostToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(l->d_inv.get(), xvx_inv.data(), 8 * p * p, cudaMemcpyHostToDevice, s));
+    }
+    CS_CUDA(cudaMemsetAsync(l->d_acc.get(), 0, 8 * M * (2 + p), s));
+    if (precision == CS_PRECISION_MIXED && (!enc.cached || !l->scan_mixed)) {
+        mixed_scan_destroy(l->scan_mixed);
+        l->scan_mixed = nullptr;
+        l->scan_mixed = mixed_scan_create(l->scan_view, enc.row_mean.data(), l->scan_counts.data());
+    }
+    // chunk width: 1024 columns, fewer when the window is long (T stays within 4 GiB)
+    int64_t kc = std::min<int64_t>(1024, std::max<int64_t>(64, ((int64_t)1 << 29) / M));
+    kc = std::max<int64_t>(16, kc / 16 * 16);
+    kc = std::min<int64_t>(kc, round_up(ne, 16));
+    l->d_chunk.resize(n * kc);
+    l->d_T.resize(M * kc);
+    Workspace ws;
+    for (int64_t c0 = 0; c0 < ne; c0 += kc) {
+        const int64_t k = std::min<int64_t>(kc, ne - c0);
+        colmajor_to_rowmajor(d.W.get() + c0 * n, n, n, k, l->d_chunk.get(), kc, s);
+        if (precision == CS_PRECISION_MIXED)
+            mixed_scan_project(l->scan_mixed, l->d_chunk.get(), kc, k, l->d_T.get(), kc, s);
+        else
+            decode_gemm_rows_fp64(l->scan_view, l->d_lut.get(), l->d_chunk.get(), kc, k,
+                                  l->d_T.get(), kc, ws, s);
+        prof::Scope ps("exact_scan_accumulate", s, (4.0 + 2.0 * p) * M * k, 8.0 * M * k);
+        const int blocks = (int)std::min<int64_t>((M * 32 + 255) / 256, 64LL * num_sms());
+        k_exact_accumulate<<<std::max(blocks, 1), 256, 0, s>>>(
+            l->d_T.get(), kc, M, k, l->d_py.get() + c0, l->d_vinv.get() + c0,
+            l->d_wutx.get() + c0, ne, (int)p, l->d_acc.get());
+        CS_LAUNCH("exact_scan_accumulate");
+    }
+    {
+        prof::Scope ps("exact_scan_finish", s, 0.0, 8.0 * M * (2 + p));
+        k_exact_finish<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 16LL * num_sms())),
+                         256, 0, s>>>(l->d_acc.get(), (int)p, M, l->d_pass.get(), l->d_inv.get(),
+                                      l->dense_residuals ? 1 : 0, l->d_beta.get(), l->d_se.get(),
+                                      l->d_p.get(), l->d_l10.get(), l->d_tested.get());
+        CS_LAUNCH("exact_scan_finish");
+    }
+    scan_finish(l, M, enc.fr, beta, se, pvalue, log10p, freq, tested, s);
+}
+
+void lmm_prepare_from_vce(cs_lmm* l, const cs_eigen_vce* v, bool use_residuals) {
+    if (!l || !v || !v->d) fail(CS_ERR_INVALID_ARGUMENT, "prepareFromVce: null argument");
+    if (!v->d->solved)
+        fail(CS_ERR_INVALID_ARGUMENT, "prepareFromVce: the null model has not been run");
+    l->dense = v->d;
+    l->dense_residuals = use_residuals;
+    l->sigma2_g = v->d->sigma2_g;
+    l->sigma2_e = v->d->sigma2_e;
+    l->delta = v->d->delta;
+    l->n = v->d->n;
+    l->sketched = false;
+    l->prepared = false;
+    l->sketch_g_uid = 0;
+    l->ztq_cols = 0;
+}
+
 void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
                      int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
                      double* beta, double* se, double* pvalue, double* log10p, double* freq,
                      int32_t* tested, cudaStream_t s) {
     l->blas = shared_blas();  // the calling thread's handle
-    if (!l->prepared) fail(CS_ERR_INVALID_ARGUMENT, "low-rank model not prepared");
     if (precision != CS_PRECISION_FP64 && precision != CS_PRECISION_MIXED)
         fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
     if (snp_begin < 0 || snp_end > g->n_snps || snp_begin > snp_end)
         fail(CS_ERR_INVALID_ARGUMENT, "scan: SNP window out of range");
+    if (l->dense) {
+        lmm_scan_exact(l, g, keep, n_keep, snp_begin, snp_end, min_maf, precision, beta, se,
+                       pvalue, log10p, freq, tested, s);
+        return;
+    }
+    if (!l->prepared) fail(CS_ERR_INVALID_ARGUMENT, "low-rank model not prepared");
     const int64_t n = l->n, p = l->p, r = l->rank, M = snp_end - snp_begin;
     if (keep == nullptr || n_keep != n)
         fail(CS_ERR_INVALID_ARGUMENT, "Sample size mismatch in scan");
@@ -905,66 +1214,13 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
         CS_BLAS(cublasDgemv(l->blas, CUBLAS_OP_T, (int)r, (int)n, &one, l->d_U.get(), (int)r,
                             l->d_d.get(), 1, &one, Bm + r + p, (int)bw));
     }
-    // ---- packed view of the analysed samples over every SNP (cached per genotypes + keep)
     prof::HostScope hs_scan("scan_host_setup");
-    const bool cached = l->scan_g_uid == g->uid && (int64_t)l->scan_keep.size() == n_keep &&
-                        l->scan_begin == snp_begin && l->scan_end == snp_end &&
-                        std::memcmp(l->scan_keep.data(), keep, 4 * n_keep) == 0;
-    if (!cached) {
-        mixed_scan_destroy(l->scan_mixed);
-        l->scan_mixed = nullptr;
-        bool identity = n_keep == g->n_samples;
-        for (int64_t i = 0; identity && i < n_keep; ++i) identity = keep[i] == i;
-        const uint8_t* first_row = g->packed.get() + snp_begin * g->stride;
-        l->scan_view = cs_packed_view{first_row, M, g->n_samples, g->stride};
-        if (!identity) {
-            const int64_t stride = round_up((n + 3) / 4, kRowAlign);
-            l->scan_own.resize(std::max<int64_t>(1, M * stride));
-            DeviceBuffer<int32_t> d_keep;
-            d_keep.resize(n);
-            CS_CUDA(cudaMemcpyAsync(d_keep.get(), keep, 4 * n, cudaMemcpyHostToDevice, s));
-            repack(first_row, g->stride, nullptr, M, d_keep.get(), n, l->scan_own.get(),
-                   stride, s);
-            CS_CUDA(cudaStreamSynchronize(s));
-            l->scan_view = cs_packed_view{l->scan_own.get(), M, n, stride};
-        }
-        l->scan_counts.assign(4 * M, 0);
-        l->d_counts.resize(std::max<int64_t>(1, 4 * M));
-        if (M) {
-            row_code_counts(l->scan_view, l->d_counts.get(), s);
-            CS_CUDA(cudaMemcpyAsync(l->scan_counts.data(), l->d_counts.get(), 16 * M,
-                                    cudaMemcpyDeviceToHost, s));
-            CS_CUDA(cudaStreamSynchronize(s));
-        }
-        l->scan_g_uid = g->uid;
-        l->scan_begin = snp_begin;
-        l->scan_end = snp_end;
-        l->scan_keep.assign(keep, keep + n_keep);
-    }
+    ScanEncoding enc = scan_encoding(l, g, keep, n_keep, snp_begin, snp_end, min_maf, s);
+    const bool cached = enc.cached;
     const cs_packed_view& v = l->scan_view;
     const std::vector<int32_t>& counts = l->scan_counts;
-    // ---- per-SNP encoding over the analysed samples (genotype_encoding.h:33-81)
-    std::vector<double> lut(4 * M, 0.0), gn2(M, 0.0), fr(M, 0.0), row_mean(M, 0.0);
-    std::vector<uint8_t> pass(M, 0);
-    for (int64_t j = 0; j < M; ++j) {
-        const int64_t c00 = counts[4 * j], c10 = counts[4 * j + 2], c11 = counts[4 * j + 3];
-        const int64_t obs = c00 + c10 + c11;
-        if (obs == 0) continue;
-        const int64_t isum = 2 * c00 + c10;
-        const double dosage_sum = (double)isum;
-        const double af = dosage_sum / (2.0 * (double)obs);
-        fr[j] = af;
-        pass[j] = obs >= 3 && std::min(af, 1.0 - af) >= min_maf;
-        // the encoded mean (additive model); rows that fail the filter are never reported
-        const double mean = dosage_sum / (double)obs;
-        row_mean[j] = mean;
-        lut[4 * j + 0] = 2.0 - mean;
-        lut[4 * j + 1] = 0.0;  // missing -> mean -> centred 0
-        lut[4 * j + 2] = 1.0 - mean;
-        lut[4 * j + 3] = 0.0 - mean;
-        const int64_t sq = 4 * c00 + c10;  // sum of squared dosages
-        gn2[j] = (double)(obs * sq - isum * isum) / (double)obs;
-    }
+    std::vector<double>&lut = enc.lut, &gn2 = enc.gn2, &fr = enc.fr, &row_mean = enc.row_mean;
+    std::vector<uint8_t>& pass = enc.pass;
     l->d_lut.resize(std::max<int64_t>(1, 4 * M));
     l->d_T.resize(std::max<int64_t>(1, M * bw));
     l->d_gn2.resize(std::max<int64_t>(1, M));
@@ -1043,24 +1299,7 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
     prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
     k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
     CS_LAUNCH("scan_epilogue");
-    std::vector<int32_t> t(M);
-    CS_CUDA(cudaMemcpyAsync(t.data(), l->d_tested.get(), 4 * M, cudaMemcpyDeviceToHost, s));
-    if (beta) CS_CUDA(cudaMemcpyAsync(beta, l->d_beta.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (se) CS_CUDA(cudaMemcpyAsync(se, l->d_se.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (pvalue) CS_CUDA(cudaMemcpyAsync(pvalue, l->d_p.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    if (log10p) CS_CUDA(cudaMemcpyAsync(log10p, l->d_l10.get(), 8 * M, cudaMemcpyDeviceToHost, s));
-    CS_CUDA(cudaStreamSynchronize(s));
-    for (int64_t j = 0; j < M; ++j) {
-        if (tested) tested[j] = t[j];
-        if (freq) freq[j] = fr[j];
-        if (!t[j]) {
-            const double nan = std::numeric_limits<double>::quiet_NaN();
-            if (beta) beta[j] = nan;
-            if (se) se[j] = nan;
-            if (pvalue) pvalue[j] = nan;
-            if (log10p) log10p[j] = nan;
-        }
-    }
+    scan_finish(l, M, fr, beta, se, pvalue, log10p, freq, tested, s);
 }
 
 }  // namespace cs

@@ -276,7 +276,8 @@ void write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_sn
     if (!ofs) fail(CS_ERR_IO, "Error writing output file: " + std::string(out_path));
 }
 
-void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold) {
+void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold,
+                     bool full_eigen) {
     if (!out_prefix) fail(CS_ERR_INVALID_ARGUMENT, "write_scan_meta: null argument");
     const std::string path = std::string(out_prefix) + ".scan.meta.txt";
     std::ofstream meta(path);
@@ -290,10 +291,10 @@ void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trac
          << "HWE_APPLIED\tfalse\n"
          << "HWE_METHOD\tNONE\n"
          << "HWE_REASON_IF_SKIPPED\tFILTER_DISABLED\n"
-         << "matrix_approximation\tfastlmm_auto_trace\n"
-         << "requested_rank\t" << requested_rank << "\n"
-         << "trace_threshold\t" << trace_threshold << "\n"
-         << "RANK_SELECTION\tAUTO_TRACE\n";
+         << "matrix_approximation\t" << (full_eigen ? "full_eigen" : "fastlmm_auto_trace") << "\n"
+         << "requested_rank\t" << (full_eigen ? 0 : requested_rank) << "\n"
+         << "trace_threshold\t" << (full_eigen ? 0.0 : trace_threshold) << "\n"
+         << "RANK_SELECTION\t" << (full_eigen ? "FULL" : "AUTO_TRACE") << "\n";
     meta.flush();
     if (!meta) fail(CS_ERR_IO, "Error writing output file: " + path);
 }

@@ -139,6 +139,79 @@ int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, 
                        int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
 
+/* ---------------------------------------------------------------- dense exact tier
+ * The default `gwas --model lmm` route (src/gwas_scanner.cpp:131-215, 384-399; no LOCO):
+ * the dense GRM, EigenVce's eigenbasis and Brent null model, and LmmEngine::scan's exact
+ * branch.  All matrices stay on the device; host pointers in and out.
+ *
+ * cs_grm_create replaces GrmBuilder::compute (libCosmicCore/src/grm_builder.cpp:87-394) for
+ * one population, unit SNP weights and no HWE filter, over every sample of g: per SNP
+ * (variants in .bed order, NULL = all) the code counts decide validity (observed, MAF >=
+ * (float)min_maf and > 1e-8), the value map of the algorithm (0/3 Yang: (x - 2p) / sqrt(2pq);
+ * 1 VanRaden: x - 2p; 2 Zeng; 4 Vitezica; 5 TrueVar) with 2p rounded to float as the
+ * reference stores it, then G = sum Z Z^T divided by the valid-SNP count (0, 3), the mean
+ * diagonal (2) or the float-rounded sum of 2pq (1, 4, 5). */
+typedef struct cs_grm cs_grm;
+typedef struct cs_eigen_vce cs_eigen_vce;
+typedef struct {
+    double min_maf;     /* GrmBuilder::Options::min_maf (compared as float); default 0.01 */
+    int32_t algorithm;  /* GrmBuilder::Options::algorithm; default 1 (VanRaden) */
+} cs_grm_options;
+void cs_grm_default_options(cs_grm_options* opt);
+int cs_grm_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
+                  const cs_grm_options* opt, cs_grm** out);
+/* The LOCO GRM of src/gwas_scanner.cpp:476-491 from the global GRM and the GRM of one
+ * chromosome's SNPs (both cs_grm_create over the same genotypes and options; the reference's
+ * GrmBuilder::computeSplit keeps the chromosome's raw sum, here raw = G_chr x its divisor):
+ * G_loco = G (S / S_loco) - raw_chr / S_loco with S the valid-SNP count (algorithms 0, 3) or
+ * the 2pq sum, S_loco = S - S_chr; the global GRM unchanged when S_chr = 0 or S_loco <= 1e-6. */
+int cs_grm_loco(const cs_grm* global, const cs_grm* chrom, cs_grm** out);
+/* A caller's own n x n GRM (host, column-major, ld >= n), as EigenVce::prepare accepts any G. */
+int cs_grm_from_host(int64_t n, const double* G, int64_t ldg, cs_grm** out);
+/* getNumSamples / getTotalSnps / getSum2pq of the builder (valid = 0, sum = 0 for a host GRM). */
+int cs_grm_info(const cs_grm* grm, int64_t* n, int64_t* n_valid, double* sum_2pq);
+/* G[keep, keep] (DataFilter::subsetSquare, libCosmicCore/src/data_filter.h) to host
+ * (column-major, ld >= n_keep); keep = NULL copies all of G. */
+int cs_grm_copy(const cs_grm* grm, const int32_t* keep, int64_t n_keep, double* out, int64_t ld);
+void cs_grm_destroy(cs_grm* grm);
+
+/* EigenVce::prepare (libCosmicCore/src/eigen_vce.cpp:19-63) on G[keep, keep]: with
+ * use_covariate_projection and p > 0 the eigenbasis of the covariate-projected G — n - p
+ * eigenvalues D (ascending, negatives set to 0), W_proj (n x (n - p)) spanning the complement
+ * of X, Uty = W_proj^T y, no UtX; otherwise the eigenbasis of G with UtX = U^T X.  The
+ * complement is formed as P G P + alpha X(X^T X)^{-1} X^T with alpha above the spectrum, so
+ * the covariate directions separate from the rest without forming Q's complement; X must
+ * have full column rank.  y: n_keep, X: n_keep x p column-major (FP32-rounded values, as the
+ * reference's MatrixXf).  keep = NULL uses every sample of the GRM. */
+int cs_eigen_vce_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep, const double* y,
+                         const double* X, int64_t p, int use_covariate_projection,
+                         cs_eigen_vce** out);
+typedef struct {
+    double sigma2_g, sigma2_e, delta;  /* delta = sigma2_e / sigma2_g */
+    double sigma2_g_se, sigma2_e_se;   /* from the AI matrix; the simplified SEs when singular */
+    double log_likelihood;             /* REML log-likelihood at the estimate */
+    double max_score;                  /* max |score| at the estimate */
+    int64_t n_eig;
+    int32_t converged;
+    double seconds;
+} cs_eigen_vce_result;
+/* EigenVce::runNullModel with the Brent solver (eigen_vce.cpp:83-112): VCESolver::
+ * solveDiagonal's golden-section search over log10 delta in [-5, 5], tol 1e-5
+ * (libCosmicCore/src/vce.cpp:3073-3175), then updateRemlDiagnostics (eigen_vce.cpp:114-153). */
+int cs_eigen_vce_run_null(cs_eigen_vce* vce, cs_eigen_vce_result* out);
+int cs_eigen_vce_dims(const cs_eigen_vce* vce, int64_t* n, int64_t* n_eig, int64_t* p);
+/* getEigenvalues / getUty / getUtX / getProjectedW to host; any output may be NULL (W:
+ * n x n_eig column-major, ld >= n). */
+int cs_eigen_vce_get(const cs_eigen_vce* vce, double* D, double* Uty, double* UtX, double* W,
+                     int64_t ldw);
+void cs_eigen_vce_destroy(cs_eigen_vce* vce);
+/* LmmEngine::prepareFromVce (src/lmm_engine.cpp:716-725): cs_lmm_scan / cs_lmm_scan_window
+ * then run the exact scan (:1363-1474): per SNP UtG = W_proj^T g (tensor-core projection in
+ * mixed precision, FP64 decode-GEMM otherwise), score = UtG . P y, var = UtG^T V^-1 UtG minus
+ * the covariate term (skipped with use_residuals, the reference's setting for GRM algorithm
+ * 0), P = chisq(score^2 / var, 1).  The run must have gone through cs_eigen_vce_run_null. */
+int cs_lmm_prepare_from_vce(cs_lmm* lmm, const cs_eigen_vce* vce, int use_residuals);
+
 /* The test matrix of src/lmm_engine.cpp:917-922 (also libCosmicCore/src/rng.h:27-33):
  * n x cols standard normals drawn column by column from std::normal_distribution<double>
  * over std::mt19937_64(seed), generated on the device (engine, polar acceptance, transform)
@@ -369,6 +442,10 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
  *                             matrix-free engine (src/lmm_engine.cpp:1077-1094), REQUESTED_RANK
  *                             reports the selected rank. */
 int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
+/* The same file for the dense route (`--model lmm` without --fastlmm / --lmm-low-rank):
+ * matrix_approximation full_eigen, requested_rank 0, trace_threshold 0, RANK_SELECTION FULL;
+ * the reference writes no .low_rank.meta.tsv there. */
+int cs_write_scan_meta_full_eigen(const char* out_prefix);
 /* The lines appended to OUT.scan.meta.txt after the scan (gwas_output::appendCommonMetadata,
  * src/gwas_output_schema.h:57-73, called from src/gwas_scanner.cpp:507-509): MODEL ("additive"),
  * N (analysed samples), the N / FREQ semantics, LOCO, COVARIATE_PROJECTION and VCE_CONVERGED

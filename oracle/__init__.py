@@ -377,3 +377,240 @@ def scan_lowrank_blas(rows, n, U, lam, r0, sg2, se2, y, X, min_maf=0.01, block=5
             out[first:first + block] = -np.log10(np.maximum(
                 np.exp(-0.5 * score ** 2 / var), 1e-300))
     return out
+
+
+# ---------------------------------------------------------------- dense exact tier (numpy)
+# Restatements of the default `gwas --model lmm` route for small n: GrmBuilder::compute,
+# EigenVce::prepare / runNullModel (Brent) / updateRemlDiagnostics and LmmEngine::scan's exact
+# branch.  Float roundings are taken where the reference stores floats.
+
+def _codes(rows, n):
+    """(b, stride) packed rows -> (b, n) 2-bit codes."""
+    return np.stack([(rows >> (2 * q)) & 3 for q in range(4)], axis=2).reshape(rows.shape[0], -1)[:, :n]
+
+
+def grm_snp(c00, c10, c11, algorithm=1, min_maf=0.01):
+    """One SNP of GrmBuilder::compute (libCosmicCore/src/grm_builder.cpp:187-312): None when
+    filtered, else (value map for codes 0..3, float 2pq)."""
+    import math
+    f32 = lambda x: float(np.float32(x))
+    n_obs = c00 + c10 + c11
+    if n_obs == 0:
+        return None
+    freq = float(2 * c00 + c10) / (2.0 * n_obs)
+    maf = min(freq, 1.0 - freq)
+    if maf < f32(min_maf) or abs(maf) < 1e-8:
+        return None
+    weight = 1.0
+    p1, p2 = float(c10) / n_obs, float(c00) / n_obs
+    if algorithm == 4:
+        two_pq = f32(weight * 4.0 * freq * freq * (1.0 - freq) * (1.0 - freq))
+    elif algorithm == 5:
+        mu = p1 + 2.0 * p2
+        two_pq = f32(weight * (p1 + 4.0 * p2 - mu * mu))
+    else:
+        two_pq = f32(weight * 2.0 * freq * (1.0 - freq))
+    mean = f32(freq * 2.0)
+    scale = 1.0
+    if algorithm in (0, 3):
+        pq2 = 2.0 * freq * (1.0 - freq)
+        scale = f32(1.0 / math.sqrt(pq2) if pq2 > 1e-9 else 0.0)
+    elif algorithm == 5:
+        mu = p1 + 2.0 * p2
+        var = p1 + 4.0 * p2 - mu * mu
+        scale = f32(1.0 / math.sqrt(var) if var > 1e-9 else 0.0)
+    if algorithm == 4:
+        fp = mean / 2.0
+        fq = 1.0 - fp
+        vals = [(-2.0 * fq * fq) * scale, 0.0, (2.0 * fp * fq) * scale, (-2.0 * fp * fp) * scale]
+    elif algorithm == 2:
+        fp = mean / 2.0
+        vals = [(1.0 - fp) * scale, 0.0, (1.0 - 2.0 * fp) * scale, (-fp) * scale]
+    else:
+        vals = [(2.0 - mean) * scale, 0.0, (1.0 - mean) * scale, (0.0 - mean) * scale]
+    return vals, two_pq
+
+
+def grm_dense(bed: "Bed", min_maf=0.01, algorithm=1, variants=None, block_size=2048,
+              raw=False):
+    """GrmBuilder::compute (grm_builder.cpp:140-394), one population, unit weights, no HWE:
+    G = sum over 2048-SNP .bed blocks of Z Z^T, normalised (:383-391) unless raw (the
+    per-chromosome sums of GrmBuilder::computeSplit, :687-712).  Returns (G, n_valid,
+    sum_2pq)."""
+    n, m = bed.n, bed.m
+    sel = np.arange(m) if variants is None else np.asarray(variants, dtype=np.int64)
+    G = np.zeros((n, n))
+    total_2pq, total_valid = 0.0, 0
+    for b0 in range(0, m, block_size):
+        idx = sel[(sel >= b0) & (sel < b0 + block_size)]
+        if len(idx) == 0:
+            continue
+        codes = _codes(bed.rows[idx], n)
+        block_2pq, valid, vals = 0.0, [], []
+        for r, j in enumerate(idx):
+            c = np.bincount(codes[r], minlength=4)
+            st = grm_snp(int(c[0]), int(c[2]), int(c[3]), algorithm, min_maf)
+            if st is None:
+                continue
+            block_2pq += st[1]
+            valid.append(j)
+            vals.append(st[0])
+        if not valid:
+            continue
+        Z = _decode_block(bed.rows[np.asarray(valid)], n, np.asarray(vals))
+        G += Z @ Z.T
+        total_2pq += block_2pq
+        total_valid += len(valid)
+    if raw:
+        return G, total_valid, total_2pq
+    if algorithm in (0, 3):
+        if total_valid > 0:
+            G /= float(total_valid)
+    elif algorithm == 2:
+        tr = np.trace(G)
+        if tr > 0:
+            G /= tr / n
+    elif total_2pq > 0:
+        G /= total_2pq
+    return G, total_valid, total_2pq
+
+
+def grm_loco(G, n_valid, sum_2pq, raw_chr, n_chr, sum_chr, algorithm=1):
+    """The LOCO GRM of src/gwas_scanner.cpp:476-491."""
+    by_count = algorithm in (0, 3)
+    s = float(n_valid) if by_count else sum_2pq
+    s_chr = float(n_chr) if by_count else sum_chr
+    s_loco = s - s_chr
+    if s_chr > 0.0 and s_loco > 1e-6:
+        return G * (s / s_loco) - raw_chr / s_loco
+    return G.copy()
+
+
+def eigen_vce_prepare(G, y, X, projection=True):
+    """EigenVce::prepare (libCosmicCore/src/eigen_vce.cpp:19-63): Householder QR of X, its
+    complement A, eigh(A^T G A) with negative eigenvalues set to 0, W_proj = A U."""
+    y = np.asarray(y, dtype=np.float64)
+    X = np.asarray(X, dtype=np.float64).reshape(len(y), -1)
+    n, p = X.shape
+    if projection and p > 0:
+        Q, _ = np.linalg.qr(X, mode="complete")
+        A = Q[:, p:]
+        D, U = np.linalg.eigh(A.T @ G @ A)
+        D = np.maximum(D, 0.0)
+        return D, A @ U, U.T @ (A.T @ y), np.zeros((n - p, 0))
+    D, U = np.linalg.eigh(G)
+    D = np.maximum(D, 0.0)
+    return D, U, U.T @ y, U.T @ X
+
+
+def solve_diagonal(D, Uty, UtX):
+    """VCESolver::solveDiagonal (libCosmicCore/src/vce.cpp:3073-3175): golden-section search
+    of the REML objective over log10 delta in [-5, 5], tol 1e-5."""
+    import math
+    n, p = len(D), UtX.shape[1]
+    n_eff = float(n - p)
+
+    def fit(delta):
+        vd = D + delta
+        vinv = 1.0 / vd
+        xvx = UtX.T @ (vinv[:, None] * UtX)
+        xvy = UtX.T @ (vinv * Uty)
+        beta = np.linalg.solve(xvx, xvy) if p else np.zeros(0)
+        logdet_xvx = np.linalg.slogdet(xvx)[1] if p else 0.0
+        resid = Uty - UtX @ beta
+        return float((resid ** 2 * vinv).sum()), float(np.log(vd).sum()), logdet_xvx, beta
+
+    def neg(delta):
+        quad, ldv, ldx, _ = fit(delta)
+        return 0.5 * (ldv + ldx + n_eff * math.log(quad / n_eff) + n_eff)
+
+    lo, hi = -5.0, 5.0
+    gr = (math.sqrt(5.0) + 1.0) / 2.0
+    c, d = hi - (hi - lo) / gr, lo + (hi - lo) / gr
+    fc, fd = neg(10.0 ** c), neg(10.0 ** d)
+    while abs(c - d) > 1e-5:
+        if fc < fd:
+            hi, d, fd = d, c, fc
+            c = hi - (hi - lo) / gr
+            fc = neg(10.0 ** c)
+        else:
+            lo, c, fc = c, d, fd
+            d = lo + (hi - lo) / gr
+            fd = neg(10.0 ** d)
+    best = 10.0 ** ((lo + hi) / 2.0)
+    quad, _, _, beta = fit(best)
+    vg = quad / n_eff
+    ve = vg * best
+    return {"sigma2_g": vg, "sigma2_e": ve, "delta": ve / vg, "beta": beta,
+            "sigma2_g_se": vg * math.sqrt(2.0 / n_eff), "sigma2_e_se": ve * math.sqrt(2.0 / n_eff)}
+
+
+def reml_diagnostics(D, Uty, UtX, sg, se):
+    """EigenVce::updateRemlDiagnostics (eigen_vce.cpp:114-153) with the dense P."""
+    import math
+    n, p = len(D), UtX.shape[1]
+    cov = np.maximum(sg * D + se, 1e-12)
+    inv = 1.0 / cov
+    P = np.diag(inv)
+    log_det_fixed = 0.0
+    if p:
+        info = UtX.T @ (inv[:, None] * UtX)
+        P -= (inv[:, None] * UtX) @ np.linalg.inv(info) @ (UtX.T * inv[None, :])
+        log_det_fixed = np.linalg.slogdet(info)[1]
+    py = P @ Uty
+    kpy = D * py
+    score = [0.5 * (py @ kpy - (np.diag(P) * D).sum()), 0.5 * (py @ py - np.trace(P))]
+    ai = 0.5 * np.array([[kpy @ P @ kpy, kpy @ P @ py], [kpy @ P @ py, py @ P @ py]])
+    cinv = np.linalg.inv(ai)
+    return {"sigma2_g_se": math.sqrt(max(0.0, cinv[0, 0])),
+            "sigma2_e_se": math.sqrt(max(0.0, cinv[1, 1])),
+            "max_score": max(abs(score[0]), abs(score[1])),
+            "log_likelihood": -0.5 * (np.log(cov).sum() + log_det_fixed + Uty @ py +
+                                      (n - p) * math.log(2.0 * math.pi))}
+
+
+def scan_exact(bed: "Bed", keep, W, D, Uty, UtX, sg, se, min_maf=0.01, use_residuals=False,
+               block=512):
+    """LmmEngine::scan's exact branch (src/lmm_engine.cpp:1363-1474) over every SNP."""
+    keep = np.asarray(keep, dtype=np.int64)
+    n = len(keep)
+    p = UtX.shape[1]
+    vinv = 1.0 / (sg * D + se)
+    wutx = UtX * vinv[:, None]
+    inv = np.linalg.inv(UtX.T @ wutx) if p else np.zeros((0, 0))
+    bx = inv @ (UtX.T @ (vinv * Uty)) if p else np.zeros(0)
+    py = (Uty - UtX @ bx) * vinv
+    out = {k: np.full(bed.m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
+    out["tested"] = np.zeros(bed.m, dtype=bool)
+    for b0 in range(0, bed.m, block):
+        codes = _codes(bed.rows[b0:b0 + block], bed.n)[:, keep]
+        cols, idx = [], []
+        for r in range(codes.shape[0]):
+            raw = np.array([2.0, np.nan, 1.0, 0.0])[codes[r]]
+            ok, vals, f, _ = prepare_marker(raw, min_maf)
+            if not ok:
+                continue
+            cols.append(vals)
+            idx.append(b0 + r)
+            out["freq"][b0 + r] = f
+        if not cols:
+            continue
+        utg = W.T @ np.array(cols).T
+        scores = utg.T @ py
+        var = (utg * (utg * vinv[:, None])).sum(axis=0)
+        if not use_residuals and p:
+            xvg = wutx.T @ utg
+            var -= (xvg * (inv @ xvg)).sum(axis=0)
+        for c, j in enumerate(idx):
+            v = var[c]
+            if not (v > 1e-12) or not np.isfinite(v):
+                continue
+            s = np.sqrt(v)
+            stat = scores[c] / s
+            pv = chisq_prob(stat * stat, 1)
+            out["beta"][j] = scores[c] / v
+            out["se"][j] = 1.0 / s
+            out["p"][j] = pv
+            out["log10p"][j] = -np.log10(pv) if pv > 0 else 300.0
+            out["tested"][j] = True
+    return out

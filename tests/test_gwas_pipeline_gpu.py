@@ -91,4 +91,33 @@ def test_gwas_lmm_from_files(tmp_path):
     assert [r[0] for r in meta[1:]] == ["1", "2"]
     assert all(r[12] == str(len(keep)) and r[-1] == "none" for r in meta[1:])
     assert [r[3] for r in meta[1:]] == [str(diags[c]["effective_rank"]) for c in ["1", "2"]]
-    assert "requested_rank\t30" in open(out + ".scan.meta.txt").read()
+    meta_txt = open(out + ".scan.meta.txt").read().splitlines()
+    assert "requested_rank\t30" in meta_txt
+    assert meta_txt[-7:-4] == ["MODEL\tadditive", f"N\t{len(keep)}",
+                               "N_SEMANTICS\tanalysis_samples_after_phenotype_and_covariate_"
+                               "filtering;per-SNP_missing_genotypes_mean-imputed"]
+    assert meta_txt[-3] == "LOCO\ttrue"
+    # canonical sumstats: one block per chromosome, BETA at 10 significant digits
+    ss = open(out + ".cosmic.sumstats").read().splitlines()
+    assert ss[0] == "# CosmicScanner Summary Statistics v1.0" and ss[2] == "# Model: LMM"
+    rows = [l.split("\t") for l in ss[5:]]
+    assert len(rows) == int(res["tested"].sum())
+    tj = np.flatnonzero(res["tested"])
+    assert [r[1] for r in rows] == [f"rs{j}" for j in tj]
+    assert all(r[5] == "%.10g" % res["beta"][j] for r, j in zip(rows[:50], tj[:50]))
+    # the same run with --out-gz --out-ssf: gzip members of the same text, SSF rows
+    import gzip
+    out2 = str(tmp_path / "res_gz")
+    res2, _, _ = cs.run_gwas_lmm(prefix, out2, pheno=str(tmp_path / "y.txt"),
+                                 qcovar=str(tmp_path / "q.txt"), covar=str(tmp_path / "c.txt"),
+                                 rank=30, precision="mixed", out_gz=True, out_ssf=True,
+                                 created=ss[1][len("# Created: "):])
+    assert np.array_equal(res2["tested"], res["tested"])
+    ss2 = gzip.decompress(open(out2 + ".cosmic.sumstats", "rb").read()).decode().splitlines()
+    assert ss2[:5] == ss[:5]
+    rows2 = [l.split("\t") for l in ss2[5:]]
+    assert [r[1] for r in rows2] == [r[1] for r in rows]
+    assert all(r[5] == "%.10g" % res2["beta"][j] for r, j in zip(rows2[:50], tj[:50]))
+    ssf = gzip.decompress(open(out2 + ".assoc.txt", "rb").read()).decode().splitlines()
+    assert ssf[0].startswith("chromosome\tbase_pair_location") and len(ssf) == len(lines)
+    assert ssf[1].split("\t")[-1] == body[0][1]
