@@ -53,6 +53,9 @@ def parse():
                     help="requests in the serving stream measured after the job (0 skips)")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the one-step timing of the plain FP64 GPU form")
+    ap.add_argument("--dense-n", type=int, default=10000,
+                    help="samples of the dense exact-route measurement (0 = skip)")
+    ap.add_argument("--dense-m", type=int, default=50000, help="SNPs of the dense measurement")
     ap.add_argument("--aireml-iters", type=int, default=2,
                     help="AI-REML (PCG + Hutchinson) iterations timed per precision (0 skips)")
     return ap.parse_args()
@@ -306,6 +309,68 @@ def run_aireml(cs, op, d, args, iters=4, probes=64):
     return out
 
 
+def run_dense(cs, args):
+    """The dense exact route (`gwas --model lmm` without --fastlmm): GRM (VanRaden) over every
+    sample, EigenVce with the covariate projection, Brent null model and the exact scan of
+    every SNP, on its own synthetic cohort of --dense-n x --dense-m; seconds per stage (the
+    second of two runs), and a CPU estimate of the same stages from numpy-BLAS samples: one
+    2048-SNP GRM block, LAPACK eigh at n = 2000 scaled by n^3, one 512-SNP scan block."""
+    import torch
+
+    from cosmicscanner_b200 import synth
+
+    n, m = args.dense_n, args.dense_m
+    d = synth.cohort(n, m, 5, missing=0.02, n_causal=200, h2=0.4)
+    g = cs.Genotypes.from_bed_bytes(d["bed"], n, m)
+    y, X = d["y"], d["X"].astype(np.float32).astype(np.float64)
+    keep = np.arange(n, dtype=np.int32)
+    stages = None
+    for _ in range(2):
+        t = [time.perf_counter()]
+        b = cs.GrmBuilder().compute(g)
+        torch.cuda.synchronize()
+        t.append(time.perf_counter())
+        v = cs.EigenVce().prepare(y, X, b)
+        t.append(time.perf_counter())
+        r = v.runNullModel()
+        t.append(time.perf_counter())
+        eng = cs.LmmEngine()
+        eng.prepareFromVce(v)
+        out = eng.scan(g, keep, precision=args.precision)
+        t.append(time.perf_counter())
+        stages = {"grm_s": t[1] - t[0], "eigh_s": t[2] - t[1], "null_s": t[3] - t[2],
+                  "scan_s": t[4] - t[3], "total_s": t[4] - t[0]}
+        tested = int(out["tested"].sum())
+        eng.close()
+        v.close()
+        b.close()
+    g.close()
+    # CPU estimate (the reference's Eigen GEMMs / SelfAdjointEigenSolver as numpy-BLAS)
+    rng = np.random.default_rng(1)
+    Z = rng.standard_normal((n, 2048))
+    c0 = time.perf_counter()
+    _ = Z @ Z.T
+    grm_cpu = (time.perf_counter() - c0) * (m / 2048)
+    del Z
+    A = rng.standard_normal((2000, 2000))
+    c0 = time.perf_counter()
+    np.linalg.eigh(A + A.T)
+    eig_cpu = (time.perf_counter() - c0) * (n / 2000) ** 3
+    W = rng.standard_normal((n, 2048))
+    G = rng.standard_normal((n, 512))
+    c0 = time.perf_counter()
+    _ = W.T @ G
+    scan_cpu = (time.perf_counter() - c0) * (n / 2048) * (m / 512)
+    return {"n": n, "m": m, "precision": args.precision, **stages, "tested": tested,
+            "sigma2_g": r["sigma2_g"], "sigma2_e": r["sigma2_e"],
+            "cpu_estimate_s": {"grm": grm_cpu, "eigh": eig_cpu, "scan": scan_cpu,
+                               "total": grm_cpu + eig_cpu + scan_cpu,
+                               "cores": os.cpu_count() or 1,
+                               "sample": "numpy-BLAS: one 2048-SNP Z Z^T block x M/2048, "
+                                         "eigh at n=2000 x (N/2000)^3, one 512-SNP W^T G "
+                                         "block x (N/2048)(M/512)"}}
+
+
 def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
     """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
     (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
@@ -472,6 +537,7 @@ def main():
         torch.cuda.synchronize()
         fp64_s = a0.elapsed_time(a1) / 1e3
     serve = run_serve(cs, g, variants, d, args) if args.serve_requests > 0 and world == 1 else None
+    dense = run_dense(cs, args) if args.dense_n > 0 and world == 1 else None
     aireml = None
     if args.aireml_iters > 0 and world == 1:
         op_all = cs.KinshipOperator(g, None, None)
@@ -547,6 +613,7 @@ def main():
                 "note": "the same REML+scan step with FP64 kinship applies and scan projection"},
             "serve": serve,
             "aireml": aireml,
+            "dense": dense,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,

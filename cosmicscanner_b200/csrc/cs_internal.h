@@ -87,6 +87,7 @@ struct cs_genotypes {
     std::vector<double> mean, inv_std;
     std::vector<int32_t> count;
     std::vector<double> sum;
+    std::vector<int32_t> code_counts;  // per SNP over all samples: codes 00, 01, 10, 11
     int device = 0;
     uint64_t uid = 0;  // distinct for every matrix created in the process (cache keys)
 };

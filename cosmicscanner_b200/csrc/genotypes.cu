@@ -231,6 +231,7 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
         g->inv_std.assign(M, 0.0);
         g->count.assign(M, 0);
         g->sum.assign(M, 0.0);
+        g->code_counts.assign(4 * M, 0);
         if (M > 0) {
             DeviceBuffer<int32_t> counts, cnt;
             DeviceBuffer<double> sum;
@@ -248,6 +249,8 @@ cs_genotypes* genotypes_from_bed(const uint8_t* bed, size_t n_bytes, int64_t n_s
                                     cudaMemcpyDeviceToHost, s));
             CS_CUDA(cudaMemcpyAsync(g->count.data(), cnt.get(), M * 4, cudaMemcpyDeviceToHost, s));
             CS_CUDA(cudaMemcpyAsync(g->sum.data(), sum.get(), M * 8, cudaMemcpyDeviceToHost, s));
+            CS_CUDA(cudaMemcpyAsync(g->code_counts.data(), counts.get(), M * 16,
+                                    cudaMemcpyDeviceToHost, s));
             CS_CUDA(cudaStreamSynchronize(s));
         }
     } catch (...) {

@@ -96,10 +96,16 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
             op->view_snp = active;
         }
         const int64_t R = op->n_active;
+        if (identity && (int64_t)g->code_counts.size() != 4 * g->n_snps)
+            fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator: genotype statistics missing");
         // code counts over the operator's samples (trace, mixed-form corrections)
         op->counts.assign(4 * R, 0);
-        op->d_counts.resize(std::max<int64_t>(1, 4 * R));
-        if (R) {
+        if (identity) {
+            // every sample: the counts the statistics pass kept
+            for (int64_t t = 0; t < R; ++t)
+                std::copy_n(&g->code_counts[4 * (int64_t)op->view_snp[t]], 4, &op->counts[4 * t]);
+        } else if (R) {
+            op->d_counts.resize(std::max<int64_t>(1, 4 * R));
             row_code_counts(op->view, op->d_counts.get(), s);
             CS_CUDA(cudaMemcpyAsync(op->counts.data(), op->d_counts.get(), 16 * R,
                                     cudaMemcpyDeviceToHost, s));

@@ -433,48 +433,57 @@ struct ScanParams {
     int32_t* tested;
 };
 
-// One warp per SNP: the variance of lmm_engine.cpp:1309-1313 in the basis,
+// The variance of lmm_engine.cpp:1309-1313 in the basis,
 // var = b ||g||^2 + sum_j c_j t_j^2 - xvg^T I^{-1} xvg, xvg = b X^T g + (U^T X)^T diag(c) t.
+// A warp takes 32 SNPs: the sums over the basis are reduced across the warp one SNP at a
+// time, then each lane finishes its own SNP (the p-value's series / continued fraction runs
+// on all 32 lanes instead of one).
 __global__ void k_scan_epilogue(ScanParams P) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     constexpr int kMaxP = 16;
-    for (int64_t j = warp; j < P.n_snps; j += n_warps) {
-        if (!P.pass[j]) {
-            if (lane == 0) P.tested[j] = 0;
-            continue;
-        }
-        const double* t = P.T + j * P.ldt;
-        double quad = 0.0;
-        double xvg[kMaxP];
-        for (int a = 0; a < P.p; ++a) xvg[a] = 0.0;
-        for (int64_t q = lane; q < P.rank; q += 32) {
-            const double tq = t[q], cq = P.c[q];
-            quad += cq * tq * tq;
-            for (int a = 0; a < P.p; ++a) xvg[a] += P.UtX[q + a * P.rank] * cq * tq;
-        }
-        for (int off = 16; off; off >>= 1) {
-            quad += __shfl_xor_sync(0xffffffffu, quad, off);
-            for (int a = 0; a < P.p; ++a) xvg[a] += __shfl_xor_sync(0xffffffffu, xvg[a], off);
-        }
-        if (lane == 0) {
-            for (int a = 0; a < P.p; ++a) xvg[a] += P.base * t[P.rank + a];
-            double var = P.base * P.gnorm2[j] + quad;
-            for (int a = 0; a < P.p; ++a) {
-                double mid = 0.0;
-                for (int b = 0; b < P.p; ++b) mid += P.info_inv[a + b * P.p] * xvg[b];
-                var -= xvg[a] * mid;
+    for (int64_t first = warp * 32; first < P.n_snps; first += n_warps * 32) {
+        double my_score = 0.0, my_var = 0.0;
+        const int count = (int)min((int64_t)32, P.n_snps - first);
+        for (int s = 0; s < count; ++s) {
+            const int64_t j = first + s;
+            if (!P.pass[j]) continue;  // uniform across the warp
+            const double* t = P.T + j * P.ldt;
+            double quad = 0.0;
+            double xvg[kMaxP];
+            for (int a = 0; a < P.p; ++a) xvg[a] = 0.0;
+            for (int64_t q = lane; q < P.rank; q += 32) {
+                const double tq = t[q], cq = P.c[q];
+                quad += cq * tq * tq;
+                for (int a = 0; a < P.p; ++a) xvg[a] += P.UtX[q + a * P.rank] * cq * tq;
             }
-            const double score = t[P.rank + P.p];
-            if (!(var > 1e-12) || !isfinite(var)) {
+            for (int off = 16; off; off >>= 1) {
+                quad += __shfl_xor_sync(0xffffffffu, quad, off);
+                for (int a = 0; a < P.p; ++a) xvg[a] += __shfl_xor_sync(0xffffffffu, xvg[a], off);
+            }
+            if (lane == s) {
+                for (int a = 0; a < P.p; ++a) xvg[a] += P.base * t[P.rank + a];
+                double var = P.base * P.gnorm2[j] + quad;
+                for (int a = 0; a < P.p; ++a) {
+                    double mid = 0.0;
+                    for (int b = 0; b < P.p; ++b) mid += P.info_inv[a + b * P.p] * xvg[b];
+                    var -= xvg[a] * mid;
+                }
+                my_score = t[P.rank + P.p];
+                my_var = var;
+            }
+        }
+        if (lane < count) {
+            const int64_t j = first + lane;
+            if (!P.pass[j] || !(my_var > 1e-12) || !isfinite(my_var)) {
                 P.tested[j] = 0;
             } else {
-                const double statistic = score / sqrt(var);
+                const double statistic = my_score / sqrt(my_var);
                 const double pv = d_chisq_prob(statistic * statistic, 1);
                 P.tested[j] = 1;
-                P.beta[j] = score / var;
-                P.se[j] = 1.0 / sqrt(var);
+                P.beta[j] = my_score / my_var;
+                P.se[j] = 1.0 / sqrt(my_var);
                 P.pval[j] = pv;
                 P.log10p[j] = pv > 0.0 ? -log10(pv) : 300.0;
             }
@@ -940,8 +949,11 @@ static ScanEncoding scan_encoding(cs_lmm* l, const cs_genotypes* g, const int32_
             l->scan_view = cs_packed_view{l->scan_own.get(), M, n, stride};
         }
         l->scan_counts.assign(4 * M, 0);
-        l->d_counts.resize(std::max<int64_t>(1, 4 * M));
-        if (M) {
+        if (identity && (int64_t)g->code_counts.size() == 4 * g->n_snps) {
+            // every sample in .fam order: the counts of the statistics pass
+            std::copy_n(g->code_counts.begin() + 4 * snp_begin, 4 * M, l->scan_counts.begin());
+        } else if (M) {
+            l->d_counts.resize(std::max<int64_t>(1, 4 * M));
             row_code_counts(l->scan_view, l->d_counts.get(), s);
             CS_CUDA(cudaMemcpyAsync(l->scan_counts.data(), l->d_counts.get(), 16 * M,
                                     cudaMemcpyDeviceToHost, s));
@@ -1295,7 +1307,8 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
     P.beta = l->d_beta.get(); P.se = l->d_se.get(); P.pval = l->d_p.get();
     P.log10p = l->d_l10.get();
     P.tested = l->d_tested.get();
-    const int blocks = (int)std::min<int64_t>((M * 32 + 255) / 256, 64LL * num_sms());
+    // a warp per 32 SNPs
+    const int blocks = (int)std::min<int64_t>((M + 255) / 256, 64LL * num_sms());
     prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
     k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
     CS_LAUNCH("scan_epilogue");

@@ -196,7 +196,7 @@ def test_exact_route_from_files(tmp_path, data):
             f.write(f"{chrom[j]}\trs{j}\t0\t{100 + j}\tA\tG\n")
     with open(prefix + ".fam", "w") as f:
         for i in range(n):
-            f.write(f"F{i} I{i} 0 0 1 {d['y'][i]!r}\n")
+            f.write(f"F{i} I{i} 0 0 1 {float(d['y'][i])!r}\n")
     with open(str(tmp_path / "q.txt"), "w") as f:
         for i in range(n):
             f.write(f"F{i} I{i} {'-9' if i % 50 == 7 else round(float(d['X'][i, 1]), 4)}\n")
