@@ -61,6 +61,19 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The largest value over the ranks of the process group (a multi-GPU time is the slowest
+    rank's); the value itself with one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -492,11 +505,7 @@ def main():
     prof = cs.profile_summary()
     cs.profile_enable(False)
     launches = cs.launch_count() - launches0
-    ms = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(stop), world, device="cuda")
     sec_per_step = ms / 1e3 / args.steps
     value = sec_per_step / world
 
@@ -519,11 +528,7 @@ def main():
         e2e_ms.append(t0.elapsed_time(t1))
     e2e_prof = cs.profile_summary()
     cs.profile_enable(False)
-    e2e_s = float(np.mean(e2e_ms)) / 1e3
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(float(np.mean(e2e_ms)) / 1e3, world, device="cuda")
 
     # ---- the plain FP64 GPU form of the same job, one step (the north-star comparison)
     fp64_s = None
