@@ -218,6 +218,9 @@ int num_sms();
 struct LowRankTarget {
     int64_t rows = 0;
     double trace = 0.0;
+    // the final sketch apply also carries [X | y - mean(y)] (the scan then takes Z^T X and
+    // Z^T y from its rows pass instead of a narrow genotype pass)
+    bool fuse_scan_columns = false;
     std::function<void(const double* X, int64_t ldx, int64_t k, double* Y, int64_t ldy,
                        cudaStream_t s)>
         apply;

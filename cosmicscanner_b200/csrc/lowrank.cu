@@ -70,9 +70,12 @@ struct cs_lmm {
     // scan's U block is Z_c^T U = (Z_c^T Q) W_sel, so it needs no genotype pass.  d_ztq
     // holds s_t^2 (Z_c^T Q)[t, :] per operator row t (R x sketch, column-major); snp_row maps
     // a .bed row to its operator row (-1: none); d_s2inv = 1 / s_t^2 (0 where s_t = 0).
+    // With the fused final apply the next p + 1 columns hold s_t^2 Z_c^T [X | y - ybar] for
+    // the y / X recorded in fused_y / fused_X.
     uint64_t sketch_g_uid = 0;
-    int64_t ztq_rows = 0, ztq_cols = 0;
-    cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u;
+    int64_t ztq_rows = 0, ztq_cols = 0, ztq_sk = 0, fused_p = -1;
+    std::vector<double> fused_y, fused_X;
+    cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u, qx, sample_x, d_betax;
     std::vector<int32_t> snp_row;
     cs::DeviceBuffer<int32_t> d_win_rows;
     // exact mode (LmmEngine::prepareFromVce): the dense eigenbasis and null model, and the
@@ -370,6 +373,33 @@ std::vector<double> project_on_basis(cs_lmm* l, const double* Z, int64_t m, cuda
 }
 
 // ---------------------------------------------------------------- scan kernels
+// The X and py columns of the scan's T from the fused sketch apply: with F (R x (p + 1),
+// column-major, ld R) = s^2 o Z_c^T [X | y - ybar] and row = rows[j],
+//   T[j, a] = F[row, a] / s^2 (a < p),  T[j, p] = b (F[row, p] / s^2 - sum_a T[j, a] bX_a),
+// the U-block term of py added afterwards (0 where row < 0).
+__global__ void k_scan_fused_cols(const double* __restrict__ F, int64_t ldf, int p,
+                                  const int32_t* __restrict__ rows, const double* __restrict__ s2inv,
+                                  const double* __restrict__ betax, double base, int64_t M,
+                                  double* __restrict__ T, int64_t ldt) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < M;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t row = rows[j];
+        double* t = T + j * ldt;
+        if (row < 0) {
+            for (int a = 0; a <= p; ++a) t[a] = 0.0;
+            continue;
+        }
+        const double si = s2inv[row];
+        double fit = 0.0;
+        for (int a = 0; a < p; ++a) {
+            const double v = F[row + (int64_t)a * ldf] * si;
+            t[a] = v;
+            fit += v * betax[a];
+        }
+        t[p] = base * (F[row + (int64_t)p * ldf] * si - fit);
+    }
+}
+
 // T[j ldt + c] (c < r) = C[c + row_j r] / s_row^2, row_j = rows[j] (0 where row_j < 0): the
 // scan's U block from W_sel^T (Z_c^T Q)^T.
 __global__ void k_scan_u_block(const double* __restrict__ C, int64_t r, const int32_t* __restrict__ rows,
@@ -434,60 +464,63 @@ struct ScanParams {
 };
 
 // The variance of lmm_engine.cpp:1309-1313 in the basis,
-// var = b ||g||^2 + sum_j c_j t_j^2 - xvg^T I^{-1} xvg, xvg = b X^T g + (U^T X)^T diag(c) t.
-// A warp takes 32 SNPs: the sums over the basis are reduced across the warp one SNP at a
-// time, then each lane finishes its own SNP (the p-value's series / continued fraction runs
-// on all 32 lanes instead of one).
+// var = b ||g||^2 + sum_j c_j t_j^2 - xvg^T I^{-1} xvg, xvg = b X^T g + (U^T X)^T diag(c) t,
+// one warp per SNP (a streaming read of T's rows); score and var go to beta / se, which
+// k_scan_pvalues then turns into the statistics one thread per SNP (the p-value's series /
+// continued fraction on every lane).
 __global__ void k_scan_epilogue(ScanParams P) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     constexpr int kMaxP = 16;
-    for (int64_t first = warp * 32; first < P.n_snps; first += n_warps * 32) {
-        double my_score = 0.0, my_var = 0.0;
-        const int count = (int)min((int64_t)32, P.n_snps - first);
-        for (int s = 0; s < count; ++s) {
-            const int64_t j = first + s;
-            if (!P.pass[j]) continue;  // uniform across the warp
-            const double* t = P.T + j * P.ldt;
-            double quad = 0.0;
-            double xvg[kMaxP];
-            for (int a = 0; a < P.p; ++a) xvg[a] = 0.0;
-            for (int64_t q = lane; q < P.rank; q += 32) {
-                const double tq = t[q], cq = P.c[q];
-                quad += cq * tq * tq;
-                for (int a = 0; a < P.p; ++a) xvg[a] += P.UtX[q + a * P.rank] * cq * tq;
-            }
-            for (int off = 16; off; off >>= 1) {
-                quad += __shfl_xor_sync(0xffffffffu, quad, off);
-                for (int a = 0; a < P.p; ++a) xvg[a] += __shfl_xor_sync(0xffffffffu, xvg[a], off);
-            }
-            if (lane == s) {
-                for (int a = 0; a < P.p; ++a) xvg[a] += P.base * t[P.rank + a];
-                double var = P.base * P.gnorm2[j] + quad;
-                for (int a = 0; a < P.p; ++a) {
-                    double mid = 0.0;
-                    for (int b = 0; b < P.p; ++b) mid += P.info_inv[a + b * P.p] * xvg[b];
-                    var -= xvg[a] * mid;
-                }
-                my_score = t[P.rank + P.p];
-                my_var = var;
-            }
+    for (int64_t j = warp; j < P.n_snps; j += n_warps) {
+        if (!P.pass[j]) continue;
+        const double* t = P.T + j * P.ldt;
+        double quad = 0.0;
+        double xvg[kMaxP];
+        for (int a = 0; a < P.p; ++a) xvg[a] = 0.0;
+        for (int64_t q = lane; q < P.rank; q += 32) {
+            const double tq = t[q], cq = P.c[q];
+            quad += cq * tq * tq;
+            for (int a = 0; a < P.p; ++a) xvg[a] += P.UtX[q + a * P.rank] * cq * tq;
         }
-        if (lane < count) {
-            const int64_t j = first + lane;
-            if (!P.pass[j] || !(my_var > 1e-12) || !isfinite(my_var)) {
-                P.tested[j] = 0;
-            } else {
-                const double statistic = my_score / sqrt(my_var);
-                const double pv = d_chisq_prob(statistic * statistic, 1);
-                P.tested[j] = 1;
-                P.beta[j] = my_score / my_var;
-                P.se[j] = 1.0 / sqrt(my_var);
-                P.pval[j] = pv;
-                P.log10p[j] = pv > 0.0 ? -log10(pv) : 300.0;
-            }
+        for (int off = 16; off; off >>= 1) {
+            quad += __shfl_xor_sync(0xffffffffu, quad, off);
+            for (int a = 0; a < P.p; ++a) xvg[a] += __shfl_xor_sync(0xffffffffu, xvg[a], off);
         }
+        if (lane == 0) {
+            for (int a = 0; a < P.p; ++a) xvg[a] += P.base * t[P.rank + a];
+            double var = P.base * P.gnorm2[j] + quad;
+            for (int a = 0; a < P.p; ++a) {
+                double mid = 0.0;
+                for (int b = 0; b < P.p; ++b) mid += P.info_inv[a + b * P.p] * xvg[b];
+                var -= xvg[a] * mid;
+            }
+            P.beta[j] = t[P.rank + P.p];  // score
+            P.se[j] = var;
+        }
+    }
+}
+
+__global__ void k_scan_pvalues(ScanParams P) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < P.n_snps;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        if (!P.pass[j]) {
+            P.tested[j] = 0;
+            continue;
+        }
+        const double score = P.beta[j], var = P.se[j];
+        if (!(var > 1e-12) || !isfinite(var)) {
+            P.tested[j] = 0;
+            continue;
+        }
+        const double statistic = score / sqrt(var);
+        const double pv = d_chisq_prob(statistic * statistic, 1);
+        P.tested[j] = 1;
+        P.beta[j] = score / var;
+        P.se[j] = 1.0 / sqrt(var);
+        P.pval[j] = pv;
+        P.log10p[j] = pv > 0.0 ? -log10(pv) : 300.0;
     }
 }
 
@@ -675,6 +708,7 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
                               cudaStream_t st) {
         kinship_apply_rowmajor(op, X_, ldx, k, Y_, ldy, precision, st);
     };
+    t.fuse_scan_columns = precision == CS_PRECISION_MIXED && op->keep_identity;
     lmm_prepare_lowrank_target(l, t, y, X, p, rank, oversample, seed, trace_threshold, min_rank,
                                diag, 0);
     // keep the final sketch apply's rows pass for the scan (see cs_lmm::d_ztq)
@@ -682,7 +716,9 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
     const double* W = precision == CS_PRECISION_MIXED && op->keep_identity
                           ? mixed_rows_output(op, &R, &kq)
                           : nullptr;
-    if (W && kq == l->sketch_diag.sketch_size && R == (int64_t)op->view_snp.size() && R > 0) {
+    const int64_t sk = l->sketch_diag.sketch_size;
+    const bool fused = t.fuse_scan_columns && kq == sk + p + 1;
+    if (W && (kq == sk || fused) && R == (int64_t)op->view_snp.size() && R > 0) {
         l->d_ztq.resize(R * kq);
         CS_CUDA(cudaMemcpy(l->d_ztq.get(), W, 8 * R * kq, cudaMemcpyDeviceToDevice));
         std::vector<double> s2inv(R);
@@ -696,6 +732,12 @@ void lmm_prepare_lowrank(cs_lmm* l, cs_kinship* op, const double* y, const doubl
         CS_CUDA(cudaMemcpy(l->d_s2inv.get(), s2inv.data(), 8 * R, cudaMemcpyHostToDevice));
         l->ztq_rows = R;
         l->ztq_cols = kq;
+        l->ztq_sk = sk;
+        l->fused_p = fused ? p : -1;
+        if (fused) {
+            l->fused_y.assign(y, y + op->rows);
+            l->fused_X.assign(X, X + op->rows * p);
+        }
         l->sketch_g_uid = op->g->uid;
     }
 }
@@ -708,6 +750,7 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     l->blas = shared_blas();  // the calling thread's handle
     l->sketch_g_uid = 0;  // a new sketch: the kept rows pass (if any) no longer matches
     l->ztq_cols = 0;
+    l->fused_p = -1;
     l->dense.reset();     // back to the low-rank mode
     const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
@@ -738,7 +781,27 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
             target.apply(q.get(), sk, sk, sample.get(), sk, s);
         }
         cholesky_qr(l->blas, sample.get(), n, sk, q.get(), gram, l->qr_ws, s);
-        target.apply(q.get(), sk, sk, sample.get(), sk, s);
+        if (target.fuse_scan_columns) {
+            // [Q | X | y - ybar] in one apply: its rows pass is kept for the scan
+            const int64_t kx = sk + p + 1;
+            l->qx.resize(n * kx);
+            l->sample_x.resize(n * kx);
+            double ybar = 0.0;
+            for (int64_t i = 0; i < n; ++i) ybar += y[i];
+            ybar /= (double)n;
+            std::vector<double> h(n * (p + 1));
+            for (int64_t i = 0; i < n; ++i) {
+                for (int64_t a = 0; a < p; ++a) h[i * (p + 1) + a] = X[i + a * n];
+                h[i * (p + 1) + p] = y[i] - ybar;
+            }
+            CS_CUDA(cudaMemcpy2DAsync(l->qx.get(), 8 * kx, q.get(), 8 * sk, 8 * sk, n,
+                                      cudaMemcpyDeviceToDevice, s));
+            CS_CUDA(cudaMemcpy2DAsync(l->qx.get() + sk, 8 * kx, h.data(), 8 * (p + 1), 8 * (p + 1),
+                                      n, cudaMemcpyHostToDevice, s));
+            target.apply(l->qx.get(), kx, kx, l->sample_x.get(), kx, s);
+        } else {
+            target.apply(q.get(), sk, sk, sample.get(), sk, s);
+        }
         CS_CUDA(cudaStreamSynchronize(s));
     }
     std::optional<prof::HostScope> hs_stage;
@@ -746,8 +809,13 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     // B = Q^T K Q (sk x sk)
     small.resize(sk * sk);
     const double one = 1.0, zero = 0.0;
-    CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)sk, (int)sk, (int)n, &one, q.get(),
-                        (int)sk, sample.get(), (int)sk, &zero, small.get(), (int)sk));
+    {
+        const bool fx = target.fuse_scan_columns;
+        const double* ks = fx ? l->sample_x.get() : sample.get();
+        const int ldk = (int)(fx ? sk + p + 1 : sk);
+        CS_BLAS(cublasDgemm(l->blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)sk, (int)sk, (int)n, &one,
+                            q.get(), (int)sk, ks, ldk, &zero, small.get(), (int)sk));
+    }
     // eigendecomposition of B (its lower triangle): on the device by cuSOLVER, or on the host
     // (tridiagonalisation and QL, the QL rotations applied to the eigenvector matrix on the
     // device) when the device solver reports a failure or CS_B200_EIGH=host asks for it
@@ -1260,11 +1328,15 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
         }
         // The U block from the kept sketch apply when every analysed sample is in the
         // operator (then the scan's centring means are the operator's) and every SNP that can
-        // be tested has an operator row; X and py still take one narrow genotype pass.
+        // be tested has an operator row.  X and py come from the same apply when it carried
+        // [X | y - ybar] for this y and X (py = b resid + U (c o U^T resid), resid = y - X bX,
+        // and G_c^T 1 = 0), else from one narrow genotype pass.
         // (CS_B200_SCAN_REUSE=0 always takes the full projection)
         const char* env = std::getenv("CS_B200_SCAN_REUSE");
         bool reuse = !(env && env[0] == '0') && l->sketch_g_uid == g->uid && l->ztq_cols > 0 &&
-                     n_keep == g->n_samples && l->ztq_cols == l->sketch_diag.sketch_size;
+                     n_keep == g->n_samples && l->ztq_sk == l->sketch_diag.sketch_size;
+        const bool fused_cols = reuse && l->fused_p == p && l->ztq_cols == l->ztq_sk + p + 1 &&
+                                l->fused_y == l->y && l->fused_X == l->X;
         for (int64_t i = 0; reuse && i < n_keep; ++i) reuse = keep[i] == i;
         std::vector<int32_t> win_rows;
         if (reuse) {
@@ -1275,7 +1347,7 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
             }
         }
         if (reuse) {
-            const int64_t R = l->ztq_rows, kq = l->ztq_cols;
+            const int64_t R = l->ztq_rows, kq = l->ztq_sk;
             const double one = 1.0, zero = 0.0;
             l->d_ztq_u.resize(r * R);
             // C (r x R) = W_sel^T (Z_c^T Q s^2)^T
@@ -1292,7 +1364,27 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
                                          l->d_T.get(), bw);
                 CS_LAUNCH("scan_u_block");
             }
-            mixed_scan_project(l->scan_mixed, Bm + r, bw, bw - r, l->d_T.get() + r, bw, s);
+            if (fused_cols) {
+                l->d_betax.resize(std::max<int64_t>(1, p));
+                if (p)
+                    CS_CUDA(cudaMemcpyAsync(l->d_betax.get(), betaX.data(), 8 * p,
+                                            cudaMemcpyHostToDevice, s));
+                {
+                    prof::Scope ps("scan_fused_columns", s, 0.0, 8.0 * (double)M * (p + 2));
+                    k_scan_fused_cols<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(
+                                            (M + 255) / 256, 32LL * num_sms())),
+                                        256, 0, s>>>(l->d_ztq.get() + kq * R, R, (int)p,
+                                                     l->d_win_rows.get(), l->d_s2inv.get(),
+                                                     l->d_betax.get(), base, M, l->d_T.get() + r,
+                                                     bw);
+                    CS_LAUNCH("scan_fused_columns");
+                }
+                // py column += U block (c o U^T resid)
+                CS_BLAS(cublasDgemv(l->blas, CUBLAS_OP_T, (int)r, (int)M, &one, l->d_T.get(), (int)bw,
+                                    l->d_d.get(), 1, &one, l->d_T.get() + r + p, (int)bw));
+            } else {
+                mixed_scan_project(l->scan_mixed, Bm + r, bw, bw - r, l->d_T.get() + r, bw, s);
+            }
         } else {
             mixed_scan_project(l->scan_mixed, Bm, bw, bw, l->d_T.get(), bw, s);
         }
@@ -1307,11 +1399,19 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
     P.beta = l->d_beta.get(); P.se = l->d_se.get(); P.pval = l->d_p.get();
     P.log10p = l->d_l10.get();
     P.tested = l->d_tested.get();
-    // a warp per 32 SNPs
-    const int blocks = (int)std::min<int64_t>((M + 255) / 256, 64LL * num_sms());
-    prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
-    k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
-    CS_LAUNCH("scan_epilogue");
+    {
+        const int blocks = (int)std::min<int64_t>((M * 32 + 255) / 256, 64LL * num_sms());
+        prof::Scope ps("scan_epilogue", s, 0.0, 8.0 * (double)M * bw);
+        k_scan_epilogue<<<std::max(blocks, 1), 256, 0, s>>>(P);
+        CS_LAUNCH("scan_epilogue");
+    }
+    {
+        prof::Scope ps("scan_pvalues", s, 0.0, 37.0 * (double)M);
+        k_scan_pvalues<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((M + 127) / 128,
+                                                                            16LL * num_sms())),
+                         128, 0, s>>>(P);
+        CS_LAUNCH("scan_pvalues");
+    }
     scan_finish(l, M, fr, beta, se, pvalue, log10p, freq, tested, s);
 }
 
