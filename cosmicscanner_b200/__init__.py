@@ -800,6 +800,102 @@ def mvlmm_scan(genotypes: Genotypes, keep, W, D, Uty, UtX, Vg, Ve, snp_begin=0, 
     return {"beta": beta, "cov": cov, "wald": wald, "p": pv, "freq": fr, "status": st}
 
 
+class MvVceOptions(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("tol", C.c_double), ("aireml", C.c_int32),
+                ("em_min_iter", C.c_int32), ("ai_max_iter", C.c_int32), ("ai_tol", C.c_double)]
+
+
+class MvEigenVce:
+    """MvEigenVce (libCosmicCore/src/eigen_vce.h): prepare() = eigen_vce.cpp:496-549 on
+    G[keep, keep] (covariate projection by default), runNullModel() = EM or AI-REML
+    (:551-911, 1031-1065) with the multivariate model's defaults (--reml-maxit 1000,
+    --reml-tol 1e-8)."""
+
+    def __init__(self, use_projection: bool = True, aireml: bool = False, **options):
+        self.use_projection = bool(use_projection)
+        self.options = MvVceOptions()
+        _abi.lib().cs_mv_vce_default_options(C.byref(self.options))
+        self.options.aireml = int(bool(aireml))
+        for k, v in options.items():
+            setattr(self.options, k, v)
+        self._h = None
+
+    def prepare(self, Y, X, grm: GrmBuilder, keep=None):
+        self.close()
+        Y = np.asfortranarray(np.asarray(Y, dtype=np.float64).reshape(len(Y), -1))
+        X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(Y), -1))
+        k = None if keep is None else np.ascontiguousarray(keep, dtype=np.int32)
+        h = C.c_void_p()
+        _check(_abi.lib().cs_mv_eigen_vce_prepare(grm._h, _ptr(k), 0 if k is None else len(k),
+                                                  _ptr(Y), Y.shape[1], _ptr(X), X.shape[1],
+                                                  int(self.use_projection), C.byref(h)))
+        self._h = h
+        n, ne, d = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(_abi.lib().cs_mv_eigen_vce_dims(h, C.byref(n), C.byref(ne), C.byref(d)))
+        self.n, self.n_eig, self.d = n.value, ne.value, d.value
+        return self
+
+    def runNullModel(self) -> bool:
+        conv, it, logl = C.c_int32(), C.c_int32(), C.c_double()
+        _check(_abi.lib().cs_mv_eigen_vce_run_null(self._h, C.byref(self.options), C.byref(conv),
+                                                   C.byref(it), C.byref(logl)))
+        self.converged, self.iterations, self.logl = bool(conv.value), it.value, logl.value
+        return self.converged
+
+    def _get(self):
+        d = self.d
+        out = {k: np.zeros((d, d), order="F") for k in ("Vg", "Ve", "Vg_se", "Ve_se")}
+        out["D"] = np.zeros(self.n_eig)
+        out["Uty"] = np.zeros((self.n_eig, d), order="F")
+        _check(_abi.lib().cs_mv_eigen_vce_get(self._h, _ptr(out["Vg"]), _ptr(out["Ve"]),
+                                              _ptr(out["Vg_se"]), _ptr(out["Ve_se"]),
+                                              _ptr(out["D"]), _ptr(out["Uty"])))
+        return out
+
+    def getVg(self):
+        return self._get()["Vg"]
+
+    def getVe(self):
+        return self._get()["Ve"]
+
+    def getVgSE(self):
+        return self._get()["Vg_se"]
+
+    def getVeSE(self):
+        return self._get()["Ve_se"]
+
+    def getEigenvalues(self):
+        return self._get()["D"]
+
+    def getUty(self):
+        return self._get()["Uty"]
+
+    def scan(self, genotypes: Genotypes, keep, snp_begin=0, snp_end=None, precision="fp64"):
+        """MvLmmEngine::prepareFromVce + scan (src/mvlmm_engine.cpp:195-207, 756-931) with the
+        device eigenbasis; the outputs of mvlmm_scan()."""
+        keep = np.ascontiguousarray(keep, dtype=np.int32)
+        end = genotypes.n_snps if snp_end is None else int(snp_end)
+        m, d = end - int(snp_begin), self.d
+        beta, cov = np.zeros((m, d)), np.zeros((m, d, d))
+        wald, pv, fr = np.zeros(m), np.zeros(m), np.zeros(m)
+        st = np.zeros(m, dtype=np.int32)
+        _check(_abi.lib().cs_mvlmm_scan_vce(genotypes._h, _ptr(keep), len(keep), self._h,
+                                            int(snp_begin), end, _prec(precision), _ptr(beta),
+                                            _ptr(cov), _ptr(wald), _ptr(pv), _ptr(fr), _ptr(st)))
+        return {"beta": beta, "cov": cov, "wald": wald, "p": pv, "freq": fr, "status": st}
+
+    def close(self):
+        if self._h:
+            _abi.lib().cs_mv_eigen_vce_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def write_assoc_mv_txt(path: str, bim_path: str, results: dict):
     """Writes `.assoc.mv.txt` (src/models/multivariate_output.cpp:40-70) from mvlmm_scan()."""
     m, d = results["beta"].shape

@@ -41,6 +41,13 @@ _SIGNATURES = {
     "cs_kinship_destroy": ([_P], None),
     "cs_lmm_create": ([_P], _I),
     "cs_grm_default_options": ([_P], None),
+    "cs_mv_vce_default_options": ([_P], None),
+    "cs_mv_eigen_vce_prepare": ([_P, _P, _I64, _P, _I64, _P, _I64, _I, _P], _I),
+    "cs_mv_eigen_vce_run_null": ([_P, _P, _P, _P, _P], _I),
+    "cs_mv_eigen_vce_dims": ([_P, _P, _P, _P], _I),
+    "cs_mv_eigen_vce_get": ([_P, _P, _P, _P, _P, _P, _P], _I),
+    "cs_mv_eigen_vce_destroy": ([_P], None),
+    "cs_mvlmm_scan_vce": ([_P, _P, _I64, _P, _I64, _I64, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_grm_create": ([_P, _P, _I64, _P, _P], _I),
     "cs_grm_from_host": ([_I64, _P, _I64, _P], _I),
     "cs_grm_loco": ([_P, _P, _P], _I),

@@ -32,6 +32,15 @@ cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_ke
 void eigen_run_null(cs_eigen_vce* v, cs_eigen_vce_result* out);
 void eigen_get(const cs_eigen_vce* v, double* D, double* Uty, double* UtX, double* W, int64_t ldw);
 void lmm_prepare_from_vce(cs_lmm* l, const cs_eigen_vce* v, bool use_residuals);
+cs_mv_eigen_vce* mv_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                            const double* Y, int64_t d, const double* X, int64_t p,
+                            bool projection);
+bool mv_run_null(cs_mv_eigen_vce* v, const cs_mv_vce_options* opt);
+void mv_get(const cs_mv_eigen_vce* v, double* Vg, double* Ve, double* Vg_se, double* Ve_se,
+            double* D, double* Uty);
+void mv_scan(const cs_genotypes* g, const int32_t* keep, int64_t n_keep, const cs_mv_eigen_vce* v,
+             int64_t snp_begin, int64_t snp_end, int precision, double* beta, double* cov,
+             double* wald, double* pvalue, double* freq, int32_t* status);
 void lmm_prepare_lowrank(cs_lmm* lmm, cs_kinship* op, const double* y, const double* X, int64_t p,
                          int rank, int oversample, int64_t seed, double trace_threshold,
                          int min_rank, int precision, cs_lowrank_diagnostics* diag);
@@ -346,6 +355,62 @@ int cs_eigen_vce_get(const cs_eigen_vce* vce, double* D, double* Uty, double* Ut
 }
 
 void cs_eigen_vce_destroy(cs_eigen_vce* vce) { delete vce; }
+
+void cs_mv_vce_default_options(cs_mv_vce_options* opt) {
+    if (!opt) return;
+    opt->max_iter = 1000;
+    opt->tol = 1e-8;
+    opt->aireml = 0;
+    opt->em_min_iter = 10;
+    opt->ai_max_iter = 50;
+    opt->ai_tol = 1e-8;
+}
+
+int cs_mv_eigen_vce_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                            const double* Y, int64_t d, const double* X, int64_t p,
+                            int use_projection, cs_mv_eigen_vce** out) {
+    return guarded([&] {
+        require(out != nullptr, "null argument");
+        *out = cs::mv_prepare(grm, keep, n_keep, Y, d, X, p, use_projection != 0);
+    });
+}
+
+int cs_mv_eigen_vce_run_null(cs_mv_eigen_vce* vce, const cs_mv_vce_options* opt,
+                             int32_t* converged, int32_t* iterations, double* logl) {
+    return guarded([&] {
+        const bool ok = cs::mv_run_null(vce, opt);
+        if (converged) *converged = ok ? 1 : 0;
+        if (iterations) *iterations = vce->iterations;
+        if (logl) *logl = vce->logl;
+    });
+}
+
+int cs_mv_eigen_vce_dims(const cs_mv_eigen_vce* vce, int64_t* n, int64_t* n_eig, int64_t* d) {
+    return guarded([&] {
+        require(vce != nullptr && vce->d != nullptr, "null argument");
+        if (n) *n = vce->d->n;
+        if (n_eig) *n_eig = vce->d->n_eig;
+        if (d) *d = vce->traits;
+    });
+}
+
+int cs_mv_eigen_vce_get(const cs_mv_eigen_vce* vce, double* Vg, double* Ve, double* Vg_se,
+                        double* Ve_se, double* D, double* Uty) {
+    return guarded([&] { cs::mv_get(vce, Vg, Ve, Vg_se, Ve_se, D, Uty); });
+}
+
+void cs_mv_eigen_vce_destroy(cs_mv_eigen_vce* vce) { delete vce; }
+
+int cs_mvlmm_scan_vce(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                      const cs_mv_eigen_vce* vce, int64_t snp_begin, int64_t snp_end,
+                      int precision, double* beta, double* cov, double* wald, double* pvalue,
+                      double* freq, int32_t* status) {
+    return guarded([&] {
+        require(g != nullptr && keep != nullptr, "null argument");
+        cs::mv_scan(g, keep, n_keep, vce, snp_begin, snp_end, precision, beta, cov, wald, pvalue,
+                    freq, status);
+    });
+}
 
 int cs_lmm_prepare_from_vce(cs_lmm* lmm, const cs_eigen_vce* vce, int use_residuals) {
     return guarded([&] {

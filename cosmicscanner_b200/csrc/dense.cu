@@ -418,9 +418,10 @@ void grm_copy(const cs_grm* grm, const int32_t* keep, int64_t n_keep, double* ou
     CS_CUDA(cudaMemcpy2D(out, 8 * ld, sub.get(), 8 * n_keep, 8 * n_keep, n_keep, cudaMemcpyDeviceToHost));
 }
 
-cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
-                            const double* y, const double* X, int64_t p, bool projection) {
-    if (!grm || !y || p < 0 || (p > 0 && !X))
+std::shared_ptr<DenseNull> eigen_basis(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                                       const double* y, int64_t nt, const double* X, int64_t p,
+                                       bool projection) {
+    if (!grm || !y || nt < 1 || p < 0 || (p > 0 && !X))
         fail(CS_ERR_INVALID_ARGUMENT, "EigenVce::prepare: null argument");
     if (p > 16) fail(CS_ERR_UNSUPPORTED, "at most 16 covariate columns are supported");
     const int64_t N = grm->n;
@@ -435,10 +436,10 @@ cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_ke
     cudaStream_t s = 0;
     cublasHandle_t blas = shared_blas();
     CS_BLAS(cublasSetStream(blas, s));
-    auto* v = new cs_eigen_vce();
-    try {
+    {
         auto d = std::make_shared<DenseNull>();
         d->n = n;
+        d->traits = nt;
         DeviceBuffer<double>& A = d->W;  // G[keep, keep], then its eigenvectors
         A.resize(n * n);
         if (keep) {
@@ -541,30 +542,34 @@ cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_ke
         d->D.assign(evals.begin(), evals.begin() + d->n_eig);
         for (double& x : d->D)
             if (x < 0) x = 0;
-        // Uty = W^T y; UtX = W^T X (no projection)
+        // Uty = W^T Y (n_eig x nt); UtX = W^T X (no projection)
         {
             DeviceBuffer<double> dy, out;
-            dy.resize(n * std::max<int64_t>(1, 1 + d->p));
-            out.resize(d->n_eig * (1 + d->p));
-            CS_CUDA(cudaMemcpyAsync(dy.get(), y, 8 * n, cudaMemcpyHostToDevice, s));
+            dy.resize(n * (nt + d->p));
+            out.resize(d->n_eig * (nt + d->p));
+            CS_CUDA(cudaMemcpyAsync(dy.get(), y, 8 * n * nt, cudaMemcpyHostToDevice, s));
             if (d->p)
-                CS_CUDA(cudaMemcpyAsync(dy.get() + n, X, 8 * n * d->p, cudaMemcpyHostToDevice, s));
+                CS_CUDA(cudaMemcpyAsync(dy.get() + n * nt, X, 8 * n * d->p, cudaMemcpyHostToDevice, s));
             const double one = 1.0, zero = 0.0;
-            CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)d->n_eig, (int)(1 + d->p), (int)n,
+            CS_BLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, (int)d->n_eig, (int)(nt + d->p), (int)n,
                                 &one, A.get(), (int)n, dy.get(), (int)n, &zero, out.get(),
                                 (int)d->n_eig));
-            std::vector<double> h(d->n_eig * (1 + d->p));
+            std::vector<double> h(d->n_eig * (nt + d->p));
             CS_CUDA(cudaMemcpyAsync(h.data(), out.get(), 8 * h.size(), cudaMemcpyDeviceToHost, s));
             CS_CUDA(cudaStreamSynchronize(s));
-            d->Uty.assign(h.begin(), h.begin() + d->n_eig);
-            d->UtX.assign(h.begin() + d->n_eig, h.end());
+            d->Uty.assign(h.begin(), h.begin() + d->n_eig * nt);
+            d->UtX.assign(h.begin() + d->n_eig * nt, h.end());
         }
-        v->d = std::move(d);
-        v->result.n_eig = v->d->n_eig;
-    } catch (...) {
-        delete v;
-        throw;
+        return d;
     }
+}
+
+cs_eigen_vce* eigen_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                            const double* y, const double* X, int64_t p, bool projection) {
+    auto d = eigen_basis(grm, keep, n_keep, y, 1, X, p, projection);
+    auto* v = new cs_eigen_vce();
+    v->d = std::move(d);
+    v->result.n_eig = v->d->n_eig;
     return v;
 }
 

@@ -153,11 +153,15 @@ int condition_covariance(std::vector<double>& cov, int d) {
 
 }  // namespace
 
-void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* Wp, int64_t r,
-                const double* Dv, const double* Uty, int64_t d, const double* UtX, int64_t p,
-                const double* Vg, const double* Ve, int64_t snp_begin, int64_t snp_end,
-                int precision, double* beta, double* cov, double* wald, double* pvalue,
-                double* freq, int32_t* status) {
+// The scan with the eigenbasis already on the device: dW is n x r row-major (ld r), or
+// column-major with ld n when w_colmajor (then transposed here, in column chunks).
+void mvlmm_scan_device(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* dW,
+                       bool w_colmajor, int64_t r, const double* Dv, const double* Uty, int64_t d,
+                       const double* UtX, int64_t p, const double* Vg, const double* Ve,
+                       int64_t snp_begin, int64_t snp_end, int precision, double* beta,
+                       double* cov, double* wald, double* pvalue, double* freq,
+                       int32_t* status) {
+    const double* Wp = dW;
     if (!g || !keep || !Wp || !Dv || !Uty || !Vg || !Ve || n <= 0 || r <= 0 || d <= 0 || p < 0 ||
         (p > 0 && !UtX))
         fail(CS_ERR_INVALID_ARGUMENT, "MvLmmEngine::scan: bad arguments");
@@ -258,14 +262,12 @@ void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const dou
             wm[i + (d + l) * r] = w[i + l * r] * yt[i + l * r];
             for (int64_t j = 0; j < p; ++j) wm[i + ((2 + j) * d + l) * r] = UtX[i + j * r] * w[i + l * r];
         }
-    DeviceBuffer<double> dWp, dwm;
-    dWp.resize(n * r);
-    {
-        std::vector<double> wr(n * r);
-        for (int64_t i = 0; i < n; ++i)
-            for (int64_t c = 0; c < r; ++c) wr[i * r + c] = Wp[i + c * n];
-        CS_CUDA(cudaMemcpyAsync(dWp.get(), wr.data(), 8 * n * r, cudaMemcpyHostToDevice, s));
-        CS_CUDA(cudaStreamSynchronize(s));
+    DeviceBuffer<double> dWrow, dwm;
+    const double* dWp_ptr = dW;
+    if (w_colmajor) {
+        dWrow.resize(n * r);
+        colmajor_to_rowmajor(dW, n, n, r, dWrow.get(), r, s);
+        dWp_ptr = dWrow.get();
     }
     dwm.resize(r * nc);
     CS_CUDA(cudaMemcpyAsync(dwm.get(), wm.data(), 8 * r * nc, cudaMemcpyHostToDevice, s));
@@ -324,14 +326,14 @@ void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const dou
         if (precision == CS_PRECISION_MIXED) {
             MixedScan* mixed = mixed_scan_create(bv, mean.data() + b0, counts.data() + 4 * b0);
             try {
-                mixed_scan_project(mixed, dWp.get(), r, r, dS.get(), r, s);
+                mixed_scan_project(mixed, dWp_ptr, r, r, dS.get(), r, s);
             } catch (...) {
                 mixed_scan_destroy(mixed);
                 throw;
             }
             mixed_scan_destroy(mixed);
         } else {
-            decode_gemm_rows_fp64(bv, dlut.get() + 4 * b0, dWp.get(), r, r, dS.get(), r, ws, s);
+            decode_gemm_rows_fp64(bv, dlut.get() + 4 * b0, dWp_ptr, r, r, dS.get(), r, ws, s);
         }
         k_square<<<grid_for(mb * r), 256, 0, s>>>(dS.get(), mb * r, dS2.get());
         CS_LAUNCH("mvlmm_square");
@@ -447,6 +449,25 @@ void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const dou
                 for (int64_t a = 0; a < d * d; ++a) cov[o * d * d + a] = sinv[a];
         }
     }
+}
+
+void mvlmm_scan(const cs_genotypes* g, const int32_t* keep, int64_t n, const double* Wp, int64_t r,
+                const double* Dv, const double* Uty, int64_t d, const double* UtX, int64_t p,
+                const double* Vg, const double* Ve, int64_t snp_begin, int64_t snp_end,
+                int precision, double* beta, double* cov, double* wald, double* pvalue,
+                double* freq, int32_t* status) {
+    if (!Wp || n <= 0 || r <= 0) fail(CS_ERR_INVALID_ARGUMENT, "MvLmmEngine::scan: bad arguments");
+    // host W (column-major) -> device, row-major
+    DeviceBuffer<double> dWp;
+    dWp.resize(n * r);
+    {
+        std::vector<double> wr(n * r);
+        for (int64_t i = 0; i < n; ++i)
+            for (int64_t c = 0; c < r; ++c) wr[i * r + c] = Wp[i + c * n];
+        CS_CUDA(cudaMemcpy(dWp.get(), wr.data(), 8 * n * r, cudaMemcpyHostToDevice));
+    }
+    mvlmm_scan_device(g, keep, n, dWp.get(), false, r, Dv, Uty, d, UtX, p, Vg, Ve, snp_begin,
+                      snp_end, precision, beta, cov, wald, pvalue, freq, status);
 }
 
 }  // namespace cs

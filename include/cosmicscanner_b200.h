@@ -212,6 +212,46 @@ void cs_eigen_vce_destroy(cs_eigen_vce* vce);
  * 0), P = chisq(score^2 / var, 1).  The run must have gone through cs_eigen_vce_run_null. */
 int cs_lmm_prepare_from_vce(cs_lmm* lmm, const cs_eigen_vce* vce, int use_residuals);
 
+/* The multi-trait dense null (`--model multivariate`, src/models/multivariate_model.cpp:
+ * 955-1015): MvEigenVce (libCosmicCore/src/eigen_vce.cpp:496-911, 1031-1065) on the same
+ * device eigenbasis as cs_eigen_vce_prepare, then the mvLMM scan from it. */
+typedef struct cs_mv_eigen_vce cs_mv_eigen_vce;
+typedef struct {
+    int32_t max_iter;    /* MvEigenVce::Options::max_iter; the multivariate model passes
+                          * --reml-maxit (1000) */
+    double tol;          /* tol on the mean squared EM change (--reml-tol, 1e-8) */
+    int32_t aireml;      /* VceSolver::AIREML (--mv-aireml) instead of EM */
+    int32_t em_min_iter; /* EM warm-up of the AI-REML route (10) */
+    int32_t ai_max_iter; /* AI-REML iterations (50) */
+    double ai_tol;       /* AI-REML stop on |delta| / sqrt(parameters) (1e-8) */
+} cs_mv_vce_options;
+void cs_mv_vce_default_options(cs_mv_vce_options* opt);
+/* MvEigenVce::prepare (:496-549) on G[keep, keep] with Y (n_keep x d, column-major, 1 <= d <= 8)
+ * and X (n_keep x p): the eigenbasis (covariate projection when use_projection; covariates
+ * without it are not supported), U'Y, and the starting Vg = Ve = Cov(Y) / 2 with the
+ * reference's divisor (samples after the projection - 1). */
+int cs_mv_eigen_vce_prepare(const cs_grm* grm, const int32_t* keep, int64_t n_keep,
+                            const double* Y, int64_t d, const double* X, int64_t p,
+                            int use_projection, cs_mv_eigen_vce** out);
+/* runNullModel (:1031-1065): EM (updateEM :551-604) until the mean squared change of (Vg, Ve)
+ * is below tol — converged = 0 after max_iter updates, where the reference's driver stops with
+ * "Multivariate null model did not converge" — or runAireml (:631-911) with aireml.  logl is
+ * the REML log-likelihood of calcLogLikelihood (:613-629) at the result. */
+int cs_mv_eigen_vce_run_null(cs_mv_eigen_vce* vce, const cs_mv_vce_options* opt,
+                             int32_t* converged, int32_t* iterations, double* logl);
+int cs_mv_eigen_vce_dims(const cs_mv_eigen_vce* vce, int64_t* n, int64_t* n_eig, int64_t* d);
+/* getVg / getVe / their SEs (AI-REML only, else 0) as d x d, eigenvalues (n_eig), U'Y
+ * (n_eig x d); any output may be NULL. */
+int cs_mv_eigen_vce_get(const cs_mv_eigen_vce* vce, double* Vg, double* Ve, double* Vg_se,
+                        double* Ve_se, double* D, double* Uty);
+void cs_mv_eigen_vce_destroy(cs_mv_eigen_vce* vce);
+/* MvLmmEngine::prepareFromVce + scan (src/mvlmm_engine.cpp:195-207, 756-931) with the device
+ * eigenbasis of vce; outputs as cs_mvlmm_scan. */
+int cs_mvlmm_scan_vce(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                      const cs_mv_eigen_vce* vce, int64_t snp_begin, int64_t snp_end,
+                      int precision, double* beta, double* cov, double* wald, double* pvalue,
+                      double* freq, int32_t* status);
+
 /* The test matrix of src/lmm_engine.cpp:917-922 (also libCosmicCore/src/rng.h:27-33):
  * n x cols standard normals drawn column by column from std::normal_distribution<double>
  * over std::mt19937_64(seed), generated on the device (engine, polar acceptance, transform)

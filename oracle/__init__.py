@@ -614,3 +614,146 @@ def scan_exact(bed: "Bed", keep, W, D, Uty, UtX, sg, se, min_maf=0.01, use_resid
             out["log10p"][j] = -np.log10(pv) if pv > 0 else 300.0
             out["tested"][j] = True
     return out
+
+
+# ---------------------------------------------------------------- MvEigenVce (numpy)
+
+def mv_eigen_vce_prepare(G, Y, X, projection=True):
+    """MvEigenVce::prepare (libCosmicCore/src/eigen_vce.cpp:496-549): the eigenbasis of
+    eigen_vce_prepare with U'Y for every trait, and Vg = Ve = Cov(Y) / 2 divided by (samples
+    after the projection - 1)."""
+    Y = np.asarray(Y, dtype=np.float64)
+    D, W, UtY, UtX = eigen_vce_prepare(G, Y, X, projection)
+    n_after = len(D)
+    Yc = Y - Y.mean(axis=0)
+    cov = Yc.T @ Yc / (n_after - 1)
+    return D, W, UtY, UtX, 0.5 * cov, 0.5 * cov.copy()
+
+
+def mv_em_step(D, UtY, Vg, Ve):
+    """MvEigenVce::updateEM (:551-604) with no covariates left (after the projection)."""
+    n = len(D)
+    V = D[:, None, None] * Vg + Ve
+    P = np.linalg.inv(V)
+    Wg = D[:, None, None] * (Vg @ P)
+    u = np.einsum("iab,ib->ia", Wg, UtY)
+    pos = D > 1e-12
+    Sg = np.where(pos[:, None, None],
+                  np.einsum("ia,ib->iab", u, u) / np.where(pos, D, 1.0)[:, None, None]
+                  + Vg - Wg @ Vg, Vg).sum(axis=0)
+    We = Ve @ P
+    e = np.einsum("iab,ib->ia", We, UtY)
+    Se = (np.einsum("ia,ib->iab", e, e) + Ve - We @ Ve).sum(axis=0)
+    return Sg / n, Se / n
+
+
+def mv_loglik(D, UtY, Vg, Ve):
+    """MvEigenVce::calcLogLikelihood (:613-629)."""
+    d = Vg.shape[0]
+    V = D[:, None, None] * Vg + Ve + 1e-8 * np.eye(d)
+    sign, ld = np.linalg.slogdet(V)
+    sol = np.linalg.solve(V, UtY[:, :, None])[:, :, 0]
+    return float((-0.5 * (ld + (UtY * sol).sum(axis=1))).sum())
+
+
+def _near_pd(M):
+    ev, Q = np.linalg.eigh(M)
+    if ev.min() <= 1e-10:
+        return (Q * np.maximum(ev, 1e-10)) @ Q.T
+    return M
+
+
+def _mv_score_ai(D, UtY, Vg, Ve, pairs):
+    d = Vg.shape[0]
+    vs = len(pairs)
+    V = D[:, None, None] * Vg + Ve + 1e-8 * np.eye(d)
+    Vi = np.linalg.inv(V)
+    v = np.einsum("iab,ib->ia", Vi, UtY)
+    w = np.zeros((len(D), vs, d))
+    for a, (p, q) in enumerate(pairs):
+        w[:, a] = v[:, p, None] * Vi[:, :, p] if p == q else \
+            v[:, q, None] * Vi[:, :, p] + v[:, p, None] * Vi[:, :, q]
+    score = np.zeros(2 * vs)
+    AI = np.zeros((2 * vs, 2 * vs))
+    for a, (j, k) in enumerate(pairs):
+        vjvk = v[:, j] * v[:, k]
+        tr = Vi[:, j, j] if j == k else 2.0 * Vi[:, j, k]
+        quad = vjvk if j == k else 2.0 * vjvk
+        score[a] = (0.5 * D * (quad - tr)).sum()
+        score[a + vs] = (0.5 * (quad - tr)).sum()
+        for b in range(a, vs):
+            qv = v[:, j] * w[:, b, j] if j == k else v[:, j] * w[:, b, k] + v[:, k] * w[:, b, j]
+            qv = 0.5 * qv
+            AI[a, b] += (D * D * qv).sum()
+            AI[a, vs + b] += (D * qv).sum()
+            AI[vs + a, b] += (D * qv).sum()
+            AI[vs + a, vs + b] += qv.sum()
+    return score, 0.5 * (AI + AI.T)
+
+
+def mv_run_null(D, UtY, Vg, Ve, max_iter=1000, tol=1e-8, aireml=False, em_min_iter=10,
+                ai_max_iter=50, ai_tol=1e-8):
+    """MvEigenVce::runNullModel (:1031-1065): EM, or runAireml (:631-911).  Returns
+    (converged, iterations, Vg, Ve, Vg_se, Ve_se, logl)."""
+    d = Vg.shape[0]
+    zeros = np.zeros((d, d))
+
+    def em(Vg, Ve):
+        Vg_new, Ve_new = mv_em_step(D, UtY, Vg, Ve)
+        err = (((Vg_new - Vg) ** 2).sum() + ((Ve_new - Ve) ** 2).sum()) / max(1.0, 2.0 * d * d)
+        return Vg_new, Ve_new, err
+
+    if not aireml:
+        for it in range(max_iter):
+            Vg, Ve, err = em(Vg, Ve)
+            if err < tol:
+                return True, it + 1, Vg, Ve, zeros, zeros, mv_loglik(D, UtY, Vg, Ve)
+        return False, max_iter, Vg, Ve, zeros, zeros, mv_loglik(D, UtY, Vg, Ve)
+    pairs = [(j, k) for j in range(d) for k in range(j, d)]
+    vs = len(pairs)
+    em_iter = 0
+    while em_iter < max_iter:
+        Vg, Ve, err = em(Vg, Ve)
+        if err < tol and em_iter >= em_min_iter:
+            break
+        em_iter += 1
+    iters = min(em_iter + 1, max_iter)
+    Vg, Ve = _near_pd(Vg), _near_pd(Ve)
+    logl_old = mv_loglik(D, UtY, Vg, Ve)
+    logl_init, Vg0, Ve0 = logl_old, Vg.copy(), Ve.copy()
+    if not np.isfinite(logl_old):
+        return True, iters, Vg, Ve, zeros, zeros, logl_old
+    for it in range(ai_max_iter):
+        score, AI = _mv_score_ai(D, UtY, Vg, Ve, pairs)
+        AI[np.diag_indices_from(AI)] *= 1.0 + 1e-8
+        delta = np.linalg.solve(AI, score)
+        step, accepted = 1.0, False
+        for h in range(12):
+            Vg_t, Ve_t = Vg.copy(), Ve.copy()
+            for a, (j, k) in enumerate(pairs):
+                Vg_t[j, k] += step * delta[a]
+                Vg_t[k, j] = Vg_t[j, k]
+                Ve_t[j, k] += step * delta[a + vs]
+                Ve_t[k, j] = Ve_t[j, k]
+            Vg_t, Ve_t = _near_pd(Vg_t), _near_pd(Ve_t)
+            ll = mv_loglik(D, UtY, Vg_t, Ve_t)
+            if np.isfinite(ll) and ll >= logl_old - 1e-10:
+                accepted = True
+                break
+            step *= 0.5
+        if not accepted:
+            break
+        Vg, Ve = Vg_t, Ve_t
+        logl_old = mv_loglik(D, UtY, Vg, Ve)
+        if np.linalg.norm(delta) / np.sqrt(2 * vs) < ai_tol:
+            return True, iters, Vg, Ve, zeros, zeros, logl_old
+    if logl_old < logl_init + 1e-8:
+        Vg, Ve, logl_old = Vg0, Ve0, logl_init
+    score, AI = _mv_score_ai(D, UtY, Vg, Ve, pairs)
+    AI[np.diag_indices_from(AI)] *= 1.0 + 1e-8
+    inv = np.linalg.inv(AI)
+    Vg_se, Ve_se = np.zeros((d, d)), np.zeros((d, d))
+    for a, (j, k) in enumerate(pairs):
+        Vg_se[j, k] = Vg_se[k, j] = np.sqrt(abs(inv[a, a]))
+        Ve_se[j, k] = Ve_se[k, j] = np.sqrt(abs(inv[vs + a, vs + a]))
+    return True, iters, Vg, Ve, Vg_se, Ve_se, logl_old

@@ -79,3 +79,30 @@ def test_exact_scan_oracle_vs_dense_gls(small):
     assert t.sum() > 300
     np.testing.assert_allclose(out["beta"][t], (score / var)[t], rtol=1e-8, atol=1e-12)
     np.testing.assert_allclose(out["se"][t], (1 / np.sqrt(var))[t], rtol=1e-8)
+
+
+def test_mv_em_oracle_properties(small):
+    """MvEigenVce's EM restatement: the REML log-likelihood never decreases along the EM
+    iterations, AI-REML ends at least as high, and with one trait the EM fixed point is the
+    single-trait Brent REML estimate."""
+    d, bed = small
+    G, _, _ = oracle.grm_dense(bed)
+    rng = np.random.default_rng(5)
+    Y = np.column_stack([d["y"], 0.3 * d["y"] + rng.standard_normal(len(d["y"]))])
+    X = d["X"].astype(np.float32).astype(np.float64)
+    D, W, UtY, UtX, Vg, Ve = oracle.mv_eigen_vce_prepare(G, Y, X)
+    ll = [oracle.mv_loglik(D, UtY, Vg, Ve)]
+    for _ in range(30):
+        Vg, Ve = oracle.mv_em_step(D, UtY, Vg, Ve)
+        ll.append(oracle.mv_loglik(D, UtY, Vg, Ve))
+    assert all(b >= a - 1e-9 for a, b in zip(ll, ll[1:]))
+    D, W, UtY, UtX, Vg0, Ve0 = oracle.mv_eigen_vce_prepare(G, Y, X)
+    em = oracle.mv_run_null(D, UtY, Vg0, Ve0)
+    ai = oracle.mv_run_null(D, UtY, Vg0, Ve0, aireml=True)
+    assert em[0] and ai[6] >= em[6] - 1e-6
+    # one trait: EM -> the Brent REML estimate
+    D1, _, Uty1, UtX1, vg, ve = oracle.mv_eigen_vce_prepare(G, Y[:, :1], X)
+    r = oracle.mv_run_null(D1, Uty1, vg, ve, max_iter=20000, tol=1e-16)
+    b = oracle.solve_diagonal(D1, Uty1[:, 0], UtX1)
+    assert abs(r[2][0, 0] - b["sigma2_g"]) < 1e-3 * b["sigma2_g"]
+    assert abs(r[3][0, 0] - b["sigma2_e"]) < 1e-3 * b["sigma2_e"]
