@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--dense-n", type=int, default=10000,
                     help="samples of the dense exact-route measurement (0 = skip)")
     ap.add_argument("--dense-m", type=int, default=50000, help="SNPs of the dense measurement")
+    ap.add_argument("--dense-only", action="store_true",
+                    help="only the dense exact-route measurement (the case its ncu captures use)")
     ap.add_argument("--aireml-iters", type=int, default=2,
                     help="AI-REML (PCG + Hutchinson) iterations timed per precision (0 skips)")
     return ap.parse_args()
@@ -453,6 +455,14 @@ def main():
         return run_reference(args)
     if args.apply_only:
         return run_apply_only(args)
+    if args.dense_only:
+        import torch
+
+        import cosmicscanner_b200 as cs
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"dense": run_dense(cs, args)}))
+        return 0
     import torch
 
     world, rank, local = dist_setup()
