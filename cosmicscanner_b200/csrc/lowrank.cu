@@ -76,6 +76,7 @@ struct cs_lmm {
     int64_t ztq_rows = 0, ztq_cols = 0, ztq_sk = 0, fused_p = -1;
     std::vector<double> fused_y, fused_X;
     cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u, qx, sample_x, d_betax;
+    std::vector<double> utz;  // U^T [X | y] of the last fit (rank x (p + 1), column-major)
     std::vector<int32_t> snp_row;
     cs::DeviceBuffer<int32_t> d_win_rows;
     // exact mode (LmmEngine::prepareFromVce): the dense eigenbasis and null model, and the
@@ -752,6 +753,7 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     l->ztq_cols = 0;
     l->fused_p = -1;
     l->dense.reset();     // back to the low-rank mode
+    l->utz.clear();
     const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
@@ -924,6 +926,7 @@ void lmm_fit_reml(cs_lmm* l, const double* y, const double* X, int64_t p,
     std::memcpy(Z.data(), X, 8 * n * p);
     std::memcpy(Z.data() + n * p, y, 8 * n);
     std::vector<double> UtZ = project_on_basis(l, Z.data(), p + 1, s);
+    l->utz = UtZ;  // U^T [X | y], reused by the scan of this fit
     RemlData d;
     d.n = n; d.p = p; d.rank = selected; d.r0 = l->r0; d.lambda = l->lambda.data();
     d.X = l->X.data(); d.y = l->y.data();
@@ -1234,7 +1237,10 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
     std::vector<double> Z(n * (p + 1));
     std::memcpy(Z.data(), l->X.data(), 8 * n * p);
     std::memcpy(Z.data() + n * p, l->y.data(), 8 * n);
-    std::vector<double> UtZ = project_on_basis(l, Z.data(), p + 1, s);
+    // U^T [X | y]: kept by the fit for this y and X
+    const std::vector<double> UtZ = l->utz.size() == (size_t)(r * (p + 1))
+                                        ? l->utz
+                                        : project_on_basis(l, Z.data(), p + 1, s);
     const double* UtX = UtZ.data();
     const double* Uty = UtZ.data() + r * p;
     const double* X = l->X.data();
