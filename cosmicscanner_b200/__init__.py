@@ -147,6 +147,13 @@ class KinshipOperator:
         _check(_abi.lib().cs_kinship_apply(self._h, C.c_void_p(X_ptr), ldx, k, C.c_void_p(Y_ptr),
                                            ldy, _prec(precision), C.c_void_p(stream)))
 
+    def apply_device_f32(self, X_ptr: int, ldx: int, k: int, Y_ptr: int, ldy: int,
+                         precision="fp64", stream: int = 0):
+        """The FP32 device apply (float column-major X and Y, FP64 inside)."""
+        _check(_abi.lib().cs_kinship_apply_f32(self._h, C.c_void_p(X_ptr), ldx, k,
+                                               C.c_void_p(Y_ptr), ldy, _prec(precision),
+                                               C.c_void_p(stream)))
+
     def trace(self) -> float:
         t = C.c_double()
         _check(_abi.lib().cs_kinship_trace(self._h, C.byref(t)))

@@ -41,6 +41,7 @@ _SIGNATURES = {
     "cs_kinship_destroy": ([_P], None),
     "cs_lmm_create": ([_P], _I),
     "cs_grm_default_options": ([_P], None),
+    "cs_kinship_apply_f32": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
     "cs_mv_vce_default_options": ([_P], None),
     "cs_mv_eigen_vce_prepare": ([_P, _P, _I64, _P, _I64, _P, _I64, _I, _P], _I),
     "cs_mv_eigen_vce_run_null": ([_P, _P, _P, _P, _P], _I),

@@ -22,6 +22,8 @@ void kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t
                            int64_t ldy, cudaStream_t s);
 cs_lmm* lmm_create();
 void lmm_destroy(cs_lmm* l);
+void kinship_apply_f32(cs_kinship* op, const float* X, int64_t ldx, int64_t k, float* Y,
+                       int64_t ldy, int precision, cudaStream_t s);
 cs_grm* grm_create(const cs_genotypes* g, const int32_t* variants, int64_t n_variants,
                    const cs_grm_options* opt);
 cs_grm* grm_from_host(int64_t n, const double* G, int64_t ldg);
@@ -192,6 +194,14 @@ int cs_kinship_apply(cs_kinship* op, const double* X, int64_t ldx, int64_t k, do
     return guarded([&] {
         require(op != nullptr, "null kinship handle");
         cs::kinship_apply_colmajor(op, X, ldx, k, Y, ldy, precision, (cudaStream_t)stream);
+    });
+}
+
+int cs_kinship_apply_f32(cs_kinship* op, const float* X, int64_t ldx, int64_t k, float* Y,
+                         int64_t ldy, int precision, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        cs::kinship_apply_f32(op, X, ldx, k, Y, ldy, precision, (cudaStream_t)stream);
     });
 }
 

@@ -171,6 +171,52 @@ void kinship_apply_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_
         fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
 }
 
+// FP32 column-major (ld) <-> FP64 row-major (n x k) around the FP32 entry point.
+__global__ void k_f32col_to_f64row(const float* __restrict__ src, int64_t ld, int64_t n,
+                                   int64_t k, double* __restrict__ dst) {
+    const int64_t total = n * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = idx / k, c = idx - i * k;
+        dst[idx] = (double)src[i + c * ld];
+    }
+}
+
+__global__ void k_f64row_to_f32col(const double* __restrict__ src, int64_t n, int64_t k,
+                                   float* __restrict__ dst, int64_t ld) {
+    const int64_t total = n * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / n, i = idx - c * n;
+        dst[i + c * ld] = (float)src[i * k + c];
+    }
+}
+
+// FP32 apply (device pointers): the inputs widened to FP64, the FP64 or mixed apply, the
+// result rounded to FP32.  Y may alias X.
+void kinship_apply_f32(cs_kinship* op, const float* X, int64_t ldx, int64_t k, float* Y,
+                       int64_t ldy, int precision, cudaStream_t s) {
+    if (k < 0) fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+    if (k == 0) return;
+    if (ldx < op->rows || ldy < op->rows)
+        fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator::apply: dimension mismatch");
+    const int64_t n = op->rows;
+    op->buf_x.resize(n * k);
+    op->buf_y.resize(n * k);
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n * k + 255) / 256, 32LL * num_sms()));
+    {
+        prof::Scope ps("f32_to_f64", s, 0.0, 12.0 * n * k);
+        k_f32col_to_f64row<<<blocks, 256, 0, s>>>(X, ldx, n, k, op->buf_x.get());
+        CS_LAUNCH("f32_to_f64");
+    }
+    kinship_apply_rowmajor(op, op->buf_x.get(), k, k, op->buf_y.get(), k, precision, s);
+    {
+        prof::Scope ps("f64_to_f32", s, 0.0, 12.0 * n * k);
+        k_f64row_to_f32col<<<blocks, 256, 0, s>>>(op->buf_y.get(), n, k, Y, ldy);
+        CS_LAUNCH("f64_to_f32");
+    }
+}
+
 // Public column-major apply (device pointers): transposes in and out around the kernels.
 void kinship_apply_colmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                             int64_t ldy, int precision, cudaStream_t s) {

@@ -74,6 +74,11 @@ int cs_kinship_info(const cs_kinship* op, int64_t* rows, int64_t* num_variants);
  * Y = K X for X rows() x k.  Y may alias X.  k == 0 is a no-op.  Device pointers. */
 int cs_kinship_apply(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                      int64_t ldy, int precision, void* stream);
+/* The FP32 variant of cs_kinship_apply for callers that keep V in single precision: X and Y
+ * are float (device, column-major); the apply runs in the requested form on FP64-widened
+ * inputs and the result is rounded to float once.  Y may alias X. */
+int cs_kinship_apply_f32(cs_kinship* op, const float* X, int64_t ldx, int64_t k, float* Y,
+                         int64_t ldy, int precision, void* stream);
 /* Same with host pointers (synchronous). */
 int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                           int64_t ldy, int precision);

@@ -78,6 +78,24 @@ def test_device_alias_and_wide_rhs(fixture):
         compare(t.cpu().numpy().T, expect)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_device_f32(fixture, precision):
+    """cs_kinship_apply_f32: float X / Y (Y aliasing X) against the FP64 oracle rounded to
+    float: within 1e-6 of the largest entry (float rounding plus the mixed form's bound)."""
+    torch = pytest.importorskip("torch")
+    bed, omega, sels, rows, ref, g = fixture
+    op = cs.createKinshipOperator(g)
+    rng = np.random.default_rng(11)
+    for k in (1, 7, 41, 130):
+        X = rng.standard_normal((N, k)).astype(np.float32)
+        expect = ref.apply_block(X.astype(np.float64))
+        t = torch.tensor(X.T.copy(), device="cuda")
+        op.apply_device_f32(t.data_ptr(), N, k, t.data_ptr(), N, precision)
+        torch.cuda.synchronize()
+        got = t.cpu().numpy().T.astype(np.float64)
+        assert np.abs(got - expect).max() <= 1e-6 * np.abs(expect).max(), (k, precision)
+
+
 def test_selection_errors(fixture):
     *_, g = fixture
     with pytest.raises(cs.InvalidArgument):
