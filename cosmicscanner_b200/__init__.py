@@ -1148,15 +1148,17 @@ def sort_chrom_labels(labels) -> list:
 def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=256,
                         oversample=10, seed=42, trace_threshold=0.95, min_rank=1,
                         min_maf=0.01, precision="fp64", genotypes: Genotypes | None = None,
-                        chrom=None, loco=True):
+                        chrom=None, loco=True, no_fallback=True, error_tol=1.0):
     """The `gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback --no-loco`
     path (src/gwas_scanner.cpp:121-129, 254-346, 447) from host buffers: upload + stats,
     GRM variant selection, operator, low-rank REML null model, scan of every SNP.  With
     per-SNP chromosome labels spanning more than one chromosome (and loco=True) it runs the
     reference's default leave-one-chromosome-out loop (src/gwas_scanner.cpp:299-314,
     464-472): per chromosome, an operator without that chromosome's GRM variants, its own
-    null model, and the scan of that chromosome's SNPs.  Returns (results dict, diagnostics
-    dict; per chromosome under LOCO)."""
+    null model, and the scan of that chromosome's SNPs.  no_fallback=False lets a null whose
+    sketch misses the trace threshold (or exceeds error_tol) fall back as the reference does
+    (_prepare_with_fallback).  Returns (results dict, diagnostics dict; per chromosome under
+    LOCO), each with its "fallback" label."""
     g = genotypes if genotypes is not None else Genotypes.from_bed_bytes(bed, n_samples, n_snps)
     keep_arr = np.arange(n_samples, dtype=np.int32) if keep is None else np.asarray(keep, np.int32)
     variants = grm_variant_selection(g.stats(), min_maf)
@@ -1165,16 +1167,15 @@ def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=
                               "Matrix-free GRM selection produced no variants")
     if chrom is not None and loco and len(set(str(c) for c in chrom)) > 1:
         res, diag = _run_loco(g, keep, keep_arr, variants, np.asarray(chrom).astype(str), y, X,
-                              rank, oversample, seed, trace_threshold, min_rank, min_maf, precision)
+                              rank, oversample, seed, trace_threshold, min_rank, min_maf, precision,
+                              no_fallback, error_tol)
         if genotypes is None:
             g.close()
         return res, diag
     op = KinshipOperator(g, None if keep is None else keep_arr, variants)
-    rank_eff = max(1, min(rank, op.rows() - 1))
     eng = LmmEngine()
-    diag = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
-                                        seed=seed, trace_threshold=trace_threshold,
-                                        min_rank=min_rank, precision=precision)
+    diag = _prepare_with_fallback(eng, y, X, op, rank, oversample, seed, trace_threshold,
+                                  min_rank, precision, no_fallback, error_tol)
     res = eng.scan(g, keep_arr, min_maf=min_maf, precision=precision)
     op.close()
     eng.close()
@@ -1263,22 +1264,25 @@ def append_scan_common_meta(out_prefix: str, n: int, loco: bool, covariate_proje
 def write_low_rank_meta(out_prefix: str, rows, n: int, error_tol: float = 1.0,
                         fallback: str = "none"):
     """OUT.low_rank.meta.tsv (src/gwas_scanner.cpp:109-115, 409-428): rows = [(scope,
-    diagnostics dict from prepareLowRankMatrixFree)], scope "GLOBAL" or the chromosome."""
+    diagnostics dict from prepareLowRankMatrixFree)], scope "GLOBAL" or the chromosome; the
+    FALLBACK column is the dict's "fallback" entry when present, else `fallback`."""
     rows = list(rows)
     diags = (LowRankDiagnostics * max(1, len(rows)))()
     scopes = (C.c_char_p * max(1, len(rows)))()
+    labels = (C.c_char_p * max(1, len(rows)))()
     for i, (scope, dd) in enumerate(rows):
         for name, _ in LowRankDiagnostics._fields_:
             setattr(diags[i], name, dd[name])
         scopes[i] = str(scope).encode()
+        labels[i] = str(dd.get("fallback", fallback)).encode()
     _check(_abi.lib().cs_write_low_rank_meta(out_prefix.encode(), len(rows), scopes, diags,
-                                             int(n), float(error_tol), fallback.encode()))
+                                             int(n), float(error_tol), labels))
 
 
 def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
                  covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
                  min_rank=1, min_maf=0.01, precision="mixed", loco=True, out_gz=False,
-                 out_ssf=False, created=None, exact=False):
+                 out_ssf=False, created=None, exact=False, no_fallback=True, error_tol=1.0):
     """`cosmicscanner gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback
     --bfile BFILE --pheno PHENO --mpheno N [--qcovar Q] [--covar C] --out OUT` end to end:
     the samples, phenotype, covariates and keep list as the reference prepares them
@@ -1307,12 +1311,13 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
                                             seed=seed, trace_threshold=trace_threshold,
                                             min_rank=min_rank, min_maf=min_maf,
                                             precision=precision, genotypes=g,
-                                            chrom=bim["chrom"] if loco else None, loco=loco)
+                                            chrom=bim["chrom"] if loco else None, loco=loco,
+                                            no_fallback=no_fallback, error_tol=error_tol)
         n_keep = len(inputs["keep"])
         write_scan_meta(out, rank, trace_threshold, full_eigen=exact)
         if not exact:
             scoped = list(diag.items()) if "sigma2_g" not in diag else [("GLOBAL", diag)]
-            write_low_rank_meta(out, scoped, n=n_keep)
+            write_low_rank_meta(out, scoped, n=n_keep, error_tol=error_tol)
         chrom = np.asarray(bim["chrom"]).astype(str)
         used_loco = "sigma2_g" not in diag
         groups = ([np.flatnonzero(chrom == c) for c in sort_chrom_labels(chrom)] if used_loco
@@ -1333,8 +1338,39 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
     return res, diag, inputs
 
 
+def _prepare_with_fallback(eng, y, X, op, rank, oversample, seed, trace_threshold, min_rank,
+                           precision, no_fallback, error_tol):
+    """The low-rank null of src/gwas_scanner.cpp:318-383: the sketch with trace-fraction rank
+    selection; the run falls back ("trace_threshold" when the threshold is not met, unless
+    --fastlmm-no-fallback; "error_tolerance" when the relative Frobenius error exceeds
+    --lmm-low-rank-error-tol) to MatrixFreeVce, i.e. the same sketch at the fixed requested
+    rank with no rank selection (src/matrix_free_vce.cpp:32-123, 137-236).  The diagnostics of
+    the first sketch are returned with the fallback label, as the reference writes them."""
+    rank_eff = max(1, min(rank, op.rows() - 1))
+    diag = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
+                                        seed=seed, trace_threshold=trace_threshold,
+                                        min_rank=min_rank, precision=precision)
+    accepted = diag["relative_frobenius_error"] <= error_tol
+    fallback = "none"
+    if not diag["trace_threshold_met"]:
+        if not no_fallback:
+            accepted = False
+            fallback = "trace_threshold"
+    elif not accepted:
+        fallback = "error_tolerance"
+    diag = dict(diag, fallback=fallback)
+    if not accepted:
+        refit = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
+                                             seed=seed, trace_threshold=0.0, min_rank=min_rank,
+                                             precision=precision)
+        for key in ("sigma2_g", "sigma2_e", "delta", "log_eta", "reml_objective"):
+            diag[key] = refit[key]
+        eng.diagnostics = diag
+    return diag
+
+
 def _run_loco(g, keep, keep_arr, variants, chrom, y, X, rank, oversample, seed,
-              trace_threshold, min_rank, min_maf, precision):
+              trace_threshold, min_rank, min_maf, precision, no_fallback=True, error_tol=1.0):
     m = g.n_snps
     out = {k: np.full(m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
     out["tested"] = np.zeros(m, dtype=bool)
@@ -1347,10 +1383,9 @@ def _run_loco(g, keep, keep_arr, variants, chrom, y, X, rank, oversample, seed,
                                   "Matrix-free LOCO left no GRM variants for chromosome " + c)
         op = KinshipOperator(g, None if keep is None else keep_arr, loco_variants)
         eng = LmmEngine()
-        rank_eff = max(1, min(rank, op.rows() - 1))
-        diags[c] = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
-                                                seed=seed, trace_threshold=trace_threshold,
-                                                min_rank=min_rank, precision=precision)
+        diags[c] = _prepare_with_fallback(eng, y, X, op, rank, oversample, seed,
+                                          trace_threshold, min_rank, precision, no_fallback,
+                                          error_tol)
         idx = np.flatnonzero(chrom == c)
         # the chromosome's SNPs as contiguous runs of the .bim order
         breaks = np.flatnonzero(np.diff(idx) != 1)

@@ -96,7 +96,7 @@ _SIGNATURES = {
     "cs_append_cosmic_sumstats": ([C.c_char_p, C.c_char_p, _I64, C.c_int32, _P, _P, _P, _P, _P,
                                    _P, C.c_char_p, _I, _I, C.c_char_p], _I),
     "cs_append_scan_common_meta": ([C.c_char_p, C.c_char_p, _I64, _I, _I, _I], _I),
-    "cs_write_low_rank_meta": ([C.c_char_p, C.c_int32, _P, _P, _I64, _D, C.c_char_p], _I),
+    "cs_write_low_rank_meta": ([C.c_char_p, C.c_int32, _P, _P, _I64, _D, _P], _I),
     "cs_fam_read": ([C.c_char_p, _P], _I),
     "cs_samples_count": ([_P, _P], _I),
     "cs_samples_id": ([_P, _I64, C.c_char_p, C.c_size_t, C.c_char_p, C.c_size_t], _I),

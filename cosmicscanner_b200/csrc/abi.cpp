@@ -88,7 +88,7 @@ void write_scan_meta(const char* out_prefix, int32_t requested_rank, double trac
                      bool full_eigen);
 void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                          const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
-                         const char* fallback);
+                         const char* const* fallbacks);
 void write_assoc_txt(const char* out_path, const char* bim_path, int64_t n_snps, int32_t n_obs,
                      const double* freq, const double* beta, const double* se, const double* p,
                      const double* log10p, const int32_t* tested, int stcg_columns);
@@ -621,9 +621,9 @@ int cs_write_scan_meta_full_eigen(const char* out_prefix) {
 
 int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                            const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
-                           const char* fallback) {
+                           const char* const* fallbacks) {
     return guarded([&] {
-        cs::write_low_rank_meta(out_prefix, n_rows, scopes, diags, n, error_tol, fallback);
+        cs::write_low_rank_meta(out_prefix, n_rows, scopes, diags, n, error_tol, fallbacks);
     });
 }
 

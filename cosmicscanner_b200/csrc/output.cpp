@@ -319,7 +319,7 @@ void append_scan_common_meta(const char* out_prefix, const char* model, int64_t 
 
 void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                          const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
-                         const char* fallback) {
+                         const char* const* fallbacks) {
     if (!out_prefix || n_rows < 0 || (n_rows > 0 && (!scopes || !diags)))
         fail(CS_ERR_INVALID_ARGUMENT, "write_low_rank_meta: null argument");
     const std::string path = std::string(out_prefix) + ".low_rank.meta.tsv";
@@ -341,7 +341,8 @@ void write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* con
              << "\t" << std::setprecision(12) << d.residual_eigenvalue << "\t"
              << d.relative_frobenius_error << "\t" << error_tol << "\t" << d.seconds << "\t" << peak
              << "\t" << (24LL * n * n) << "\t" << d.effective_rank << "\t" << n << "\t"
-             << d.trace_fraction << "\tMATRIX_FREE_AUTO_TRACE\t" << (fallback ? fallback : "none")
+             << d.trace_fraction << "\tMATRIX_FREE_AUTO_TRACE\t"
+             << (fallbacks && fallbacks[r] ? fallbacks[r] : "none")
              << "\n";
     }
     meta.flush();

@@ -482,8 +482,10 @@ int cs_write_assoc_mv_txt(const char* out_path, const char* bim_path, int64_t n_
  *   cs_write_low_rank_meta    OUT.low_rank.meta.tsv header (:109-115) and one row per null
  *                             model (:409-428): scope "GLOBAL" or the LOCO chromosome, the
  *                             diagnostics of cs_lmm_prepare_lowrank_matrix_free, the analysed
- *                             sample count n, --lmm-low-rank-error-tol and the fallback label
- *                             ("none" with --fastlmm-no-fallback).  Like the reference's
+ *                             sample count n, --lmm-low-rank-error-tol and per row the fallback
+ *                             label (NULL: "none", as with --fastlmm-no-fallback;
+ *                             "trace_threshold" / "error_tolerance" when the run fell
+ *                             back, src/gwas_scanner.cpp:347-362).  Like the reference's
  *                             matrix-free engine (src/lmm_engine.cpp:1077-1094), REQUESTED_RANK
  *                             reports the selected rank. */
 int cs_write_scan_meta(const char* out_prefix, int32_t requested_rank, double trace_threshold);
@@ -499,7 +501,7 @@ int cs_append_scan_common_meta(const char* out_prefix, const char* model, int64_
                                int covariate_projection, int vce_converged);
 int cs_write_low_rank_meta(const char* out_prefix, int32_t n_rows, const char* const* scopes,
                            const cs_lowrank_diagnostics* diags, int64_t n, double error_tol,
-                           const char* fallback);
+                           const char* const* fallbacks);
 
 /* ---------------------------------------------------------------- input side
  * The samples, phenotypes, covariates and keep list that the reference's association path

@@ -121,3 +121,27 @@ def test_gwas_lmm_from_files(tmp_path):
     ssf = gzip.decompress(open(out2 + ".assoc.txt", "rb").read()).decode().splitlines()
     assert ssf[0].startswith("chromosome\tbase_pair_location") and len(ssf) == len(lines)
     assert ssf[1].split("\t")[-1] == body[0][1]
+
+
+def test_low_rank_fallback_labels():
+    """The fall-back decision of src/gwas_scanner.cpp:347-383: with --fastlmm-no-fallback the
+    sketch that misses the trace threshold is kept ("none"); without it the run falls back to
+    the fixed-rank MatrixFreeVce sketch ("trace_threshold"), which at the same requested rank
+    and seed gives the same null and scan; an error above --lmm-low-rank-error-tol falls back
+    with "error_tolerance"."""
+    n, m = 500, 1500
+    d = synth.cohort(n, m, 13, missing=0.02, n_causal=20, h2=0.5)
+    y, X = d["y"], d["X"].astype(np.float32).astype(np.float64)
+    a, da = cs.run_lmm_matrix_free(d["bed"], n, m, y, X, rank=20, precision="mixed")
+    assert not da["trace_threshold_met"] and da["fallback"] == "none"
+    b, db = cs.run_lmm_matrix_free(d["bed"], n, m, y, X, rank=20, precision="mixed",
+                                   no_fallback=False)
+    assert db["fallback"] == "trace_threshold"
+    assert abs(db["sigma2_g"] - da["sigma2_g"]) <= 1e-12 * da["sigma2_g"]
+    t = a["tested"]
+    assert np.array_equal(b["tested"], t)
+    assert np.abs(b["log10p"][t] - a["log10p"][t]).max() <= 1e-9
+    c, dc = cs.run_lmm_matrix_free(d["bed"], n, m, y, X, rank=20, precision="mixed",
+                                   trace_threshold=0.0, error_tol=0.0)
+    assert dc["fallback"] == "error_tolerance"
+    assert abs(dc["sigma2_g"] - da["sigma2_g"]) <= 1e-9 * da["sigma2_g"]
