@@ -221,8 +221,132 @@ class LmmEngine {
         return r;
     }
 
+    // scan() over SNPs [begin, end) (a LOCO chromosome's run).
+    ScanResult scanWindow(const Genotypes& g, const std::vector<int32_t>& keep, int64_t begin,
+                          int64_t end, double min_maf = 0.01, Precision prec = Precision::FP64) {
+        ScanResult r;
+        const int64_t m = end - begin;
+        for (auto* v : {&r.beta, &r.se, &r.p, &r.log10p, &r.freq}) v->resize(m > 0 ? m : 0);
+        r.tested.resize(m > 0 ? m : 0);
+        check(cs_lmm_scan_window(h_, g.handle(), keep.data(), (int64_t)keep.size(), begin, end,
+                                 min_maf, (int)prec, r.beta.data(), r.se.data(), r.p.data(),
+                                 r.log10p.data(), r.freq.data(), r.tested.data()));
+        return r;
+    }
+
+    // prepareFromVce(vce): the exact scan on EigenVce's basis and null model.
+    void prepareFromVce(const class EigenVce& vce, bool use_residuals = false);
+
+    cs_lmm* handle() { return h_; }
+
    private:
     cs_lmm* h_ = nullptr;
+};
+
+// ---- dense exact tier: GrmBuilder (libCosmicCore/src/grm_builder.h), EigenVce and MvEigenVce
+// (libCosmicCore/src/eigen_vce.h); every N x N matrix stays on the device.
+class GrmBuilder {
+   public:
+    explicit GrmBuilder(double min_maf = 0.01, int algorithm = 1) {
+        cs_grm_default_options(&opt_);
+        opt_.min_maf = min_maf;
+        opt_.algorithm = algorithm;
+    }
+    GrmBuilder(const GrmBuilder&) = delete;
+    GrmBuilder& operator=(const GrmBuilder&) = delete;
+    ~GrmBuilder() { cs_grm_destroy(h_); }
+    // compute(reader) over the given SNPs (empty: all) of every sample.
+    void compute(const Genotypes& g, const std::vector<int32_t>& variants = {}) {
+        cs_grm_destroy(h_);
+        h_ = nullptr;
+        check(cs_grm_create(g.handle(), variants.empty() ? nullptr : variants.data(),
+                            (int64_t)variants.size(), &opt_, &h_));
+    }
+    int64_t getTotalSnps() const {
+        int64_t v = 0;
+        check(cs_grm_info(h_, nullptr, &v, nullptr));
+        return v;
+    }
+    double getSum2pq() const {
+        double v = 0;
+        check(cs_grm_info(h_, nullptr, nullptr, &v));
+        return v;
+    }
+    // getGrm(), or G[keep, keep] (column-major).
+    std::vector<double> getGrm(const std::vector<int32_t>& keep = {}) const {
+        int64_t n = 0;
+        check(cs_grm_info(h_, &n, nullptr, nullptr));
+        const int64_t k = keep.empty() ? n : (int64_t)keep.size();
+        std::vector<double> out((size_t)(k * k));
+        check(cs_grm_copy(h_, keep.empty() ? nullptr : keep.data(), k, out.data(), k));
+        return out;
+    }
+    const cs_grm* handle() const { return h_; }
+
+   private:
+    cs_grm_options opt_{};
+    cs_grm* h_ = nullptr;
+};
+
+class EigenVce {
+   public:
+    explicit EigenVce(bool use_covariate_projection = true) : proj_(use_covariate_projection) {}
+    EigenVce(const EigenVce&) = delete;
+    EigenVce& operator=(const EigenVce&) = delete;
+    ~EigenVce() { cs_eigen_vce_destroy(h_); }
+    // prepare(y, X, G[keep, keep]); X column-major n x p (FP32-rounded values).
+    void prepare(const std::vector<double>& y, const std::vector<double>& X, int64_t p,
+                 const GrmBuilder& grm, const std::vector<int32_t>& keep = {}) {
+        cs_eigen_vce_destroy(h_);
+        h_ = nullptr;
+        check(cs_eigen_vce_prepare(grm.handle(), keep.empty() ? nullptr : keep.data(),
+                                   (int64_t)keep.size(), y.data(), X.empty() ? nullptr : X.data(),
+                                   p, proj_ ? 1 : 0, &h_));
+    }
+    // runNullModel() (Brent); the estimates and diagnostics.
+    cs_eigen_vce_result runNullModel() {
+        cs_eigen_vce_result r{};
+        check(cs_eigen_vce_run_null(h_, &r));
+        return r;
+    }
+    const cs_eigen_vce* handle() const { return h_; }
+
+   private:
+    bool proj_;
+    cs_eigen_vce* h_ = nullptr;
+};
+
+inline void LmmEngine::prepareFromVce(const EigenVce& vce, bool use_residuals) {
+    check(cs_lmm_prepare_from_vce(h_, vce.handle(), use_residuals ? 1 : 0));
+}
+
+class MvEigenVce {
+   public:
+    MvEigenVce() { cs_mv_vce_default_options(&opt_); }
+    MvEigenVce(const MvEigenVce&) = delete;
+    MvEigenVce& operator=(const MvEigenVce&) = delete;
+    ~MvEigenVce() { cs_mv_eigen_vce_destroy(h_); }
+    cs_mv_vce_options& options() { return opt_; }
+    // prepare(Y, X, G[keep, keep]): Y column-major n x d (d <= 8), X n x p.
+    void prepare(const std::vector<double>& Y, int64_t d, const std::vector<double>& X, int64_t p,
+                 const GrmBuilder& grm, const std::vector<int32_t>& keep = {}) {
+        cs_mv_eigen_vce_destroy(h_);
+        h_ = nullptr;
+        check(cs_mv_eigen_vce_prepare(grm.handle(), keep.empty() ? nullptr : keep.data(),
+                                      (int64_t)keep.size(), Y.data(), d,
+                                      X.empty() ? nullptr : X.data(), p, 1, &h_));
+    }
+    // runNullModel(): false when EM did not converge (the multivariate driver then stops).
+    bool runNullModel() {
+        int32_t conv = 0;
+        check(cs_mv_eigen_vce_run_null(h_, &opt_, &conv, nullptr, nullptr));
+        return conv != 0;
+    }
+    const cs_mv_eigen_vce* handle() const { return h_; }
+
+   private:
+    cs_mv_vce_options opt_{};
+    cs_mv_eigen_vce* h_ = nullptr;
 };
 
 // ---- input side: the .fam samples, phenotype / covariate tables aligned to them and the keep

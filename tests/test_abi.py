@@ -73,6 +73,18 @@ int main() {
         std::printf("invalid: %s\n", e.what());
     }
     cs_vce_options o = cs::StcgVce::default_options();
+    cs::MvEigenVce mv;
+    if (mv.options().max_iter != 1000 || mv.options().tol != 1e-8) return 4;
+    try {
+        cs::GrmBuilder grm;
+        cs::EigenVce vce;
+        vce.prepare({1.0}, {}, 0, grm);  // no GRM computed yet
+        return 5;
+    } catch (const std::invalid_argument& e) {
+        std::printf("invalid: %s\n", e.what());
+    } catch (const std::runtime_error& e) {
+        std::printf("error: %s\n", e.what());
+    }
     return (o.mc_samples == 20 && o.pcg_tol == 1e-10 && o.probe_seed == 20250101ull) ? 0 : 3;
 }
 ''')
