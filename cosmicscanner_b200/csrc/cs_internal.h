@@ -227,6 +227,9 @@ struct LowRankTarget {
 };
 cs_lmm* lmm_create();
 void lmm_destroy(cs_lmm* l);
+// The y columns (n x t) of the traits that the next scans of this sketch fit in turn: the first
+// scan projects all of them, the others reuse that projection (lowrank.cu).
+void lmm_set_scan_traits(cs_lmm* l, const double* Y, int64_t t);
 void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const double* y,
                                 const double* X, int64_t p, int rank, int oversample,
                                 int64_t seed, double trace_threshold, int min_rank,

@@ -77,6 +77,15 @@ struct cs_lmm {
     std::vector<double> fused_y, fused_X;
     cs::DeviceBuffer<double> d_ztq, d_wsel, d_s2inv, d_ztq_u, qx, sample_x, d_betax;
     std::vector<double> utz;  // U^T [X | y] of the last fit (rank x (p + 1), column-major)
+    // Several traits of one request (the serving loop): their y columns (n x t), and the
+    // projection [U | X | py | y_1 - ybar_1 .. y_t - ybar_t] of the first trait's scan, valid
+    // for the sketch generation, covariates, precision and scan view it was made with.
+    std::vector<double> trait_Y, tcache_X;
+    int64_t trait_t = 0;
+    uint64_t basis_gen = 0, tcache_gen = 0;
+    int tcache_prec = -1;
+    bool tcache_valid = false;
+    cs::DeviceBuffer<double> d_bt, d_tc;
     std::vector<int32_t> snp_row;
     cs::DeviceBuffer<int32_t> d_win_rows;
     // exact mode (LmmEngine::prepareFromVce): the dense eigenbasis and null model, and the
@@ -374,6 +383,20 @@ std::vector<double> project_on_basis(cs_lmm* l, const double* Z, int64_t m, cuda
 }
 
 // ---------------------------------------------------------------- scan kernels
+// The py column of one trait from the cached projection C (row-major, ld ldc):
+//   C[j, r + p] = b (C[j, ycol] - sum_a C[j, r + a] bX_a)  (the U-block term added afterwards).
+__global__ void k_scan_py_from_y(double* __restrict__ C, int64_t ldc, int64_t r, int p,
+                                 int64_t ycol, const double* __restrict__ betax, double base,
+                                 int64_t M) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < M;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        double* c = C + j * ldc;
+        double fit = 0.0;
+        for (int a = 0; a < p; ++a) fit += c[r + a] * betax[a];
+        c[r + p] = base * (c[ycol] - fit);
+    }
+}
+
 // The X and py columns of the scan's T from the fused sketch apply: with F (R x (p + 1),
 // column-major, ld R) = s^2 o Z_c^T [X | y - ybar] and row = rows[j],
 //   T[j, a] = F[row, a] / s^2 (a < p),  T[j, p] = b (F[row, p] / s^2 - sum_a T[j, a] bX_a),
@@ -754,6 +777,10 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
     l->fused_p = -1;
     l->dense.reset();     // back to the low-rank mode
     l->utz.clear();
+    ++l->basis_gen;
+    l->trait_t = 0;
+    l->trait_Y.clear();
+    l->tcache_valid = false;
     const int64_t n = target.rows;
     if (rank <= 0 || rank >= n || p < 0 || (p > 0 && X == nullptr))
         fail(CS_ERR_INVALID_ARGUMENT,
@@ -1208,6 +1235,14 @@ void lmm_prepare_from_vce(cs_lmm* l, const cs_eigen_vce* v, bool use_residuals) 
     l->ztq_cols = 0;
 }
 
+// The y columns of every trait of one request (n x t, column-major) that the following scans
+// of this sketch will fit one after the other; the first scan then projects them all.
+void lmm_set_scan_traits(cs_lmm* l, const double* Y, int64_t t) {
+    l->trait_t = Y && t > 1 ? t : 0;
+    l->trait_Y.assign(Y, Y + (l->trait_t ? l->n * t : 0));
+    l->tcache_valid = false;
+}
+
 void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
                      int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
                      double* beta, double* se, double* pvalue, double* log10p, double* freq,
@@ -1326,7 +1361,74 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
         CS_CUDA(cudaMemcpyAsync(l->d_inv.get(), info_inv.data(), 8 * p * p, cudaMemcpyHostToDevice, s));
     }
     // ---- T = G_c^T [U | X | py]: the per-SNP projections (the scan's GEMM)
-    if (precision == CS_PRECISION_MIXED) {
+    // Several traits of one request over the same basis, covariates and window: the first
+    // scan projects [U | X | py | y_1 - ybar_1 .. y_t - ybar_t] once; every later trait's py
+    // column follows from its y column (py = b (y - X bX) + U (c o U^T r), G_c^T 1 = 0)
+    // without a genotype pass.
+    int64_t trait = -1;
+    if (l->trait_t > 0 && (int64_t)l->trait_Y.size() == n * l->trait_t)
+        for (int64_t j = 0; j < l->trait_t && trait < 0; ++j)
+            if (std::memcmp(l->trait_Y.data() + j * n, y, 8 * n) == 0) trait = j;
+    const double* Tptr = l->d_T.get();
+    int64_t ldt = bw;
+    if (trait >= 0) {
+        const int64_t tc = l->trait_t, ldc = bw + tc;
+        const double one = 1.0;
+        const bool valid = cached && l->tcache_valid && l->tcache_gen == l->basis_gen &&
+                           l->tcache_prec == precision && l->tcache_X == l->X &&
+                           (precision != CS_PRECISION_MIXED || l->scan_mixed);
+        l->d_tc.resize(M * ldc);
+        if (!valid) {
+            l->d_bt.resize(n * ldc);
+            std::vector<double> hy(n * tc);
+            for (int64_t j = 0; j < tc; ++j) {
+                const double* yj = l->trait_Y.data() + j * n;
+                double mean = 0.0;
+                for (int64_t i = 0; i < n; ++i) mean += yj[i];
+                mean /= (double)n;
+                for (int64_t i = 0; i < n; ++i) hy[i * tc + j] = yj[i] - mean;
+            }
+            CS_CUDA(cudaMemcpy2DAsync(l->d_bt.get(), 8 * ldc, Bm, 8 * bw, 8 * bw, n,
+                                      cudaMemcpyDeviceToDevice, s));
+            CS_CUDA(cudaMemcpy2DAsync(l->d_bt.get() + bw, 8 * ldc, hy.data(), 8 * tc, 8 * tc, n,
+                                      cudaMemcpyHostToDevice, s));
+            if (precision == CS_PRECISION_MIXED) {
+                if (!cached || !l->scan_mixed) {
+                    mixed_scan_destroy(l->scan_mixed);
+                    l->scan_mixed = nullptr;
+                    l->scan_mixed = mixed_scan_create(v, row_mean.data(), counts.data());
+                }
+                mixed_scan_project(l->scan_mixed, l->d_bt.get(), ldc, ldc, l->d_tc.get(), ldc, s);
+            } else {
+                Workspace ws;
+                decode_gemm_rows_fp64(v, l->d_lut.get(), l->d_bt.get(), ldc, ldc, l->d_tc.get(),
+                                      ldc, ws, s);
+            }
+            CS_CUDA(cudaStreamSynchronize(s));  // hy is a host temporary
+            l->tcache_valid = true;
+            l->tcache_gen = l->basis_gen;
+            l->tcache_prec = precision;
+            l->tcache_X = l->X;
+        } else {
+            l->d_betax.resize(std::max<int64_t>(1, p));
+            if (p)
+                CS_CUDA(cudaMemcpyAsync(l->d_betax.get(), betaX.data(), 8 * p,
+                                        cudaMemcpyHostToDevice, s));
+            {
+                prof::Scope ps("scan_py_from_y", s, 0.0, 8.0 * (double)M * (p + 2));
+                k_scan_py_from_y<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>(
+                                       (M + 255) / 256, 32LL * num_sms())),
+                                   256, 0, s>>>(l->d_tc.get(), ldc, r, (int)p, bw + trait,
+                                                l->d_betax.get(), base, M);
+                CS_LAUNCH("scan_py_from_y");
+            }
+            // py column += U block (c o U^T resid)
+            CS_BLAS(cublasDgemv(l->blas, CUBLAS_OP_T, (int)r, (int)M, &one, l->d_tc.get(), (int)ldc,
+                                l->d_d.get(), 1, &one, l->d_tc.get() + r + p, (int)ldc));
+        }
+        Tptr = l->d_tc.get();
+        ldt = ldc;
+    } else if (precision == CS_PRECISION_MIXED) {
         if (!cached || !l->scan_mixed) {
             mixed_scan_destroy(l->scan_mixed);
             l->scan_mixed = nullptr;
@@ -1399,8 +1501,8 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
         decode_gemm_rows_fp64(v, l->d_lut.get(), Bm, bw, bw, l->d_T.get(), bw, ws, s);
     }
     ScanParams P;
-    P.n_snps = M; P.rank = r; P.p = p; P.ldt = bw; P.base = base;
-    P.T = l->d_T.get(); P.c = l->d_cv.get(); P.UtX = l->d_utx.get(); P.info_inv = l->d_inv.get();
+    P.n_snps = M; P.rank = r; P.p = p; P.ldt = ldt; P.base = base;
+    P.T = Tptr; P.c = l->d_cv.get(); P.UtX = l->d_utx.get(); P.info_inv = l->d_inv.get();
     P.gnorm2 = l->d_gn2.get(); P.pass = l->d_pass.get();
     P.beta = l->d_beta.get(); P.se = l->d_se.get(); P.pval = l->d_p.get();
     P.log10p = l->d_l10.get();

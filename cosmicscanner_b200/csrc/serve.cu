@@ -297,11 +297,13 @@ void cs_server::run_request(Request* r) {
         cs_lowrank_diagnostics d{};
         for (int32_t j = 0; j < r->t; ++j) {
             const double* yj = r->Y.data() + (int64_t)j * n;
-            if (j == 0)
+            if (j == 0) {
                 cs::lmm_prepare_lowrank_target(lmm, target, yj, r->X.data(), r->p, rank,
                                                opt.oversample, (int64_t)r->seed, opt.trace_threshold,
                                                opt.min_rank, &d, st);
-            else
+                // every trait's scan shares one projection of the window
+                cs::lmm_set_scan_traits(lmm, r->Y.data(), r->t);
+            } else
                 cs::lmm_fit_reml(lmm, yj, r->X.data(), r->p, &d, st);
             r->effective_rank = d.effective_rank;
             r->sigma2[2 * j] = d.sigma2_g;

@@ -110,3 +110,25 @@ def test_bad_requests_rejected(data):
     with pytest.raises(cs.InvalidArgument):
         srv.submit(np.r_[S[:-1], d["n"]], Y, X)  # sample out of range
     srv.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 1e-5)])
+def test_multi_trait_shares_projection(data, precision, tol):
+    """A request's later traits take their py column from the first scan's projection of
+    every trait's y; each agrees with the same trait requested alone (its own projection)."""
+    d, g, variants, ref = data
+    S, Y, X, b, e = make_request(d, 99, 600, 4)
+    srv = cs.Server(g, variants, rank=30, precision=precision, max_active=1)
+    rid = srv.submit(S, Y, X, b, e)
+    assert srv.wait(rid)["state"] == 2
+    multi = [srv.result(rid, t) for t in range(4)]
+    for t in range(4):
+        one = srv.submit(S, Y[:, t:t + 1].copy(), X, b, e)
+        assert srv.wait(one)["state"] == 2
+        alone = srv.result(one, 0)
+        m = alone["tested"]
+        assert np.array_equal(multi[t]["tested"], m)
+        assert abs(multi[t]["sigma2_g"] - alone["sigma2_g"]) <= 1e-12 * alone["sigma2_g"]
+        assert rel(multi[t]["beta"][m], alone["beta"][m]) < tol
+        assert np.abs(multi[t]["log10p"][m] - alone["log10p"][m]).max() < 10 * tol
+    srv.close()
