@@ -970,7 +970,9 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
     CS_CUDA(cudaMemcpyAsync(&status, ws.status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     CS_CUDA(cudaStreamSynchronize(s));
     if (status != 0) {
-        cudaMemset(ws.status.get(), 0, sizeof(int));
+        // cleared on the caller's stream: a non-blocking stream does not wait for the legacy one
+        cudaMemsetAsync(ws.status.get(), 0, sizeof(int), s);
+        cudaStreamSynchronize(s);
         fail(CS_ERR_CUDA, "tensor-core kinship kernel gave up waiting (status " +
                               std::to_string(status) + ")");
     }
@@ -1004,7 +1006,8 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
     ws.max_muw.resize(k);
     if (!ws.status.get()) {
         ws.status.resize(1);
-        CS_CUDA(cudaMemset(ws.status.get(), 0, sizeof(int)));
+        // on the pass's own stream, so the kernel never reads the pool's previous contents
+        CS_CUDA(cudaMemsetAsync(ws.status.get(), 0, sizeof(int), s));
     }
     // boxes of one column tile's rows (pairs: half of them)
     const int box = pairs ? tl.kc / 2 : tl.kc, box_last = pairs ? tl.kc_last / 2 : tl.kc_last;
