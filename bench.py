@@ -265,10 +265,10 @@ def run_serve(cs, g, variants, d, args):
 
     reqs = [request() for _ in range(args.serve_requests)]
     srv = cs.Server(g, variants, precision=args.precision, max_active=8)
-    # one untimed request (the server's threads, handles and buffers come up), then the
-    # service time of one request alone, which calibrates the arrival rate
+    # one untimed request (the server's threads, handles and buffers come up), then the mean
+    # service time of the first four requests run alone, which calibrates the arrival rate
     srv.wait(srv.submit(*reqs[0]))
-    single = srv.wait(srv.submit(*reqs[0]))["latency_s"]
+    single = float(np.mean([srv.wait(srv.submit(*q))["latency_s"] for q in reqs[:4]]))
     st0 = srv.stats()
     rate = 0.8 / single
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))

@@ -86,6 +86,12 @@ struct cs_lmm {
     int tcache_prec = -1;
     bool tcache_valid = false;
     cs::DeviceBuffer<double> d_bt, d_tc;
+    // the per-SNP encoding of the cached scan view and MAF threshold, and whether d_lut /
+    // d_gn2 / d_pass still hold it (a later trait of the same request reuses both)
+    std::vector<double> enc_lut, enc_gn2, enc_fr, enc_row_mean;
+    std::vector<uint8_t> enc_pass;
+    double enc_maf = -1.0;
+    bool enc_valid = false, enc_on_device = false;
     std::vector<int32_t> snp_row;
     cs::DeviceBuffer<int32_t> d_win_rows;
     // exact mode (LmmEngine::prepareFromVce): the dense eigenbasis and null model, and the
@@ -1017,6 +1023,7 @@ struct ScanEncoding {
     std::vector<double> lut, gn2, fr, row_mean;
     std::vector<uint8_t> pass;
     bool cached = false;
+    bool reused = false;  // the encoding of the previous scan of this view (and on the device)
 };
 
 static ScanEncoding scan_encoding(cs_lmm* l, const cs_genotypes* g, const int32_t* keep,
@@ -1027,6 +1034,18 @@ static ScanEncoding scan_encoding(cs_lmm* l, const cs_genotypes* g, const int32_
     const bool cached = l->scan_g_uid == g->uid && (int64_t)l->scan_keep.size() == n_keep &&
                         l->scan_begin == snp_begin && l->scan_end == snp_end &&
                         std::memcmp(l->scan_keep.data(), keep, 4 * n_keep) == 0;
+    if (cached && l->enc_valid && l->enc_maf == min_maf) {
+        e.cached = true;
+        e.reused = true;
+        e.lut = l->enc_lut;
+        e.gn2 = l->enc_gn2;
+        e.fr = l->enc_fr;
+        e.row_mean = l->enc_row_mean;
+        e.pass = l->enc_pass;
+        return e;
+    }
+    l->enc_valid = false;
+    l->enc_on_device = false;
     if (!cached) {
         mixed_scan_destroy(l->scan_mixed);
         l->scan_mixed = nullptr;
@@ -1172,6 +1191,7 @@ static void lmm_scan_exact(cs_lmm* l, const cs_genotypes* g, const int32_t* keep
     l->d_wutx.resize(std::max<int64_t>(1, ne * p));
     l->d_inv.resize(std::max<int64_t>(1, p * p));
     l->d_acc.resize(M * (2 + p));
+    l->enc_on_device = false;  // d_lut / d_pass now hold this scan's upload (not the cache's)
     CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), enc.lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
     CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), enc.pass.data(), M, cudaMemcpyHostToDevice, s));
     CS_CUDA(cudaMemcpyAsync(l->d_py.get(), py.data(), 8 * ne, cudaMemcpyHostToDevice, s));
@@ -1352,9 +1372,20 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
     for (auto* b : {&l->d_beta, &l->d_se, &l->d_p, &l->d_l10}) b->resize(std::max<int64_t>(1, M));
     l->d_tested.resize(std::max<int64_t>(1, M));
     if (M == 0) return;
-    CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
-    CS_CUDA(cudaMemcpyAsync(l->d_gn2.get(), gn2.data(), 8 * M, cudaMemcpyHostToDevice, s));
-    CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), pass.data(), M, cudaMemcpyHostToDevice, s));
+    if (!(enc.reused && l->enc_on_device)) {
+        CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(l->d_gn2.get(), gn2.data(), 8 * M, cudaMemcpyHostToDevice, s));
+        CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), pass.data(), M, cudaMemcpyHostToDevice, s));
+        // the host vectors must outlive the copies: keep them as the cached encoding
+        l->enc_lut = lut;
+        l->enc_gn2 = gn2;
+        l->enc_fr = fr;
+        l->enc_row_mean = row_mean;
+        l->enc_pass = pass;
+        l->enc_maf = min_maf;
+        l->enc_valid = true;
+        l->enc_on_device = true;
+    }
     CS_CUDA(cudaMemcpyAsync(l->d_cv.get(), c.data(), 8 * r, cudaMemcpyHostToDevice, s));
     if (p) {
         CS_CUDA(cudaMemcpyAsync(l->d_utx.get(), UtX, 8 * r * p, cudaMemcpyHostToDevice, s));
