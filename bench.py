@@ -84,7 +84,11 @@ def dist_setup():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region.
+
+    A timed region can be shorter than nvidia-smi's start-up and its 200 ms cadence, so entry
+    waits (up to 10 s) for the sampler's first line and exit waits (up to 1 s) for one sample
+    taken after the region began; the summary uses the samples from the region's start on."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -94,6 +98,7 @@ class ClockSampler:
         self.idx = device_index
         self.proc = None
         self.lines: list[str] = []
+        self.first = 0
 
     def __enter__(self):
         try:
@@ -105,6 +110,11 @@ class ClockSampler:
             self.t.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        t0 = time.perf_counter()
+        while not self.lines and self.proc.poll() is None and time.perf_counter() - t0 < 10.0:
+            time.sleep(0.01)
+        self.first = len(self.lines)
         return self
 
     def _read(self):
@@ -113,6 +123,10 @@ class ClockSampler:
 
     def __exit__(self, *exc):
         if self.proc:
+            t0 = time.perf_counter()
+            while (len(self.lines) <= self.first and self.proc.poll() is None
+                   and time.perf_counter() - t0 < 1.0):
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -122,7 +136,7 @@ class ClockSampler:
     def summary(self):
         sm, smax, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[self.first:]:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
