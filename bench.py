@@ -16,9 +16,15 @@ rank runs its own job; value = seconds per job for the whole machine.
 """
 from __future__ import annotations
 
+import os
+
+# The CPU restatement alternates OpenMP table decodes with multithreaded BLAS GEMMs; spinning
+# idle OpenMP threads would steal the cores the GEMMs run on (set before any OpenMP runtime
+# starts).
+os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+
 import argparse
 import json
-import os
 import statistics
 import subprocess
 import sys
@@ -58,6 +64,8 @@ def parse():
     ap.add_argument("--dense-m", type=int, default=50000, help="SNPs of the dense measurement")
     ap.add_argument("--dense-only", action="store_true",
                     help="only the dense exact-route measurement (the case its ncu captures use)")
+    ap.add_argument("--ref-budget", type=float, default=240.0,
+                    help="seconds of whole CPU jobs the reference arm runs (at least one)")
     ap.add_argument("--aireml-iters", type=int, default=2,
                     help="AI-REML (PCG + Hutchinson) iterations timed per precision (0 skips)")
     return ap.parse_args()
@@ -83,27 +91,43 @@ def dist_setup():
     return world, rank, local
 
 
+def gpu_uuid(local: int):
+    """The CUDA device's UUID in nvidia-smi's form (GPU-xxxxxxxx-...), or None."""
+    try:
+        import torch
+
+        u = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        return None
+    return u if u.startswith("GPU-") else "GPU-" + u
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region.
 
+    The GPU is selected by its UUID (nvidia-smi numbers GPUs in PCI order and ignores
+    CUDA_VISIBLE_DEVICES, so on a shared machine an index can name another user's GPU), and
+    every sample's UUID is checked against it; samples of any other GPU are dropped.
     A timed region can be shorter than nvidia-smi's start-up and its 200 ms cadence, so entry
     waits (up to 10 s) for the sampler's first line and exit waits (up to 1 s) for one sample
     taken after the region began; the summary uses the samples from the region's start on."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("uuid,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
-        self.idx = device_index
+    def __init__(self, local: int):
+        self.uuid = gpu_uuid(local)
+        self.idx = local
         self.proc = None
         self.lines: list[str] = []
         self.first = 0
 
     def __enter__(self):
+        ident = self.uuid if self.uuid else str(self.idx)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", f"--id={ident}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -134,24 +158,30 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, smax, reasons = [], 0.0, set()
+        sm, smax, reasons, other, idx = [], 0.0, set(), 0, None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines[self.first:]:
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
+                continue
+            if self.uuid and f[0] != self.uuid:
+                other += 1
                 continue
             try:
-                sm.append(float(f[1]))
-                smax = max(smax, float(f[2]))
+                sm.append(float(f[2]))
+                smax = max(smax, float(f[3]))
+                idx = int(f[1])
             except ValueError:
                 continue
-            for name, v in zip(names, f[5:9]):
+            for name, v in zip(names, f[6:10]):
                 if v.lower() == "active":
                     reasons.add(name)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"],
+                    "gpu_uuid": self.uuid}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "gpu_uuid": self.uuid, "nvidia_smi_index": idx,
+                "selected_by": "uuid" if self.uuid else "index", "other_gpu_samples": other}
 
 
 def measured_peaks():
@@ -410,67 +440,111 @@ def run_dense(cs, args):
                                          "block x (N/2048)(M/512)"}}
 
 
-def cpu_reference_sample(d, n_threads, m_sample=2048, k=RANK + OVERSAMPLE):
-    """Times the reference's CPU algorithm on the host cores over a bounded sample: apply_block
-    (512-SNP FP64 decode blocks, two GEMMs each, BLAS-threaded like Eigen) with 266 right-hand
-    sides and scanLowRank's block GEMMs, both over m_sample of the M SNPs; extrapolated to
-    the whole job (4 applies + the scan over all M SNPs).  QR, eigh and REML are excluded."""
+def job_config(n: int, m: int) -> dict:
+    """The workload both arms print (identical dicts)."""
+    return {"workload": f"lmm matrix-free low-rank REML+scan, N={n} M={m} rank={RANK} "
+                        f"sketch={RANK + OVERSAMPLE} p=3 (synthetic, 2 pops Fst=0.01, 2% missing)",
+            "n": n, "m": m, "rank": RANK, "sketch": RANK + OVERSAMPLE, "covariates": 3,
+            "l2": "inputs (packed genotypes) larger than L2; no flush"}
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_job(d, threads):
+    """One whole job on the host cores: the oracle's restatement of the reference's CPU path
+    (prepareLowRankMatrixFree + scanLowRank, numpy BLAS/LAPACK for Eigen, OpenMP decodes) on the
+    same inputs and GRM variant selection as the GPU job.  The per-SNP statistics (the upload's
+    counterpart) are computed before the clock starts.  Returns (seconds, result)."""
     import oracle
 
     n, m = d["n"], d["m"]
-    stride = (n + 3) // 4
-    rows = d["bed"][3:3 + m_sample * stride].reshape(m_sample, stride)
-    B = oracle.Bed(rows, n)
-    rng = np.random.default_rng(0)
-    Om = rng.standard_normal((n, k))
-    t0 = time.perf_counter()
-    oracle.apply_block_blas(rows, n, B.mean, B.inv_std, Om)
-    t_apply = time.perf_counter() - t0
-    U = np.linalg.qr(rng.standard_normal((n, RANK)))[0]
-    lam = np.sort(rng.uniform(1, 5, RANK))[::-1].copy()
+    B = oracle.Bed(d["bed"][3:].reshape(m, -1), n)
+    freq = B.mean / 2.0
+    maf = np.minimum(freq, 1.0 - freq)
+    variants = np.nonzero((B.inv_std != 0.0) & ~(maf < 0.01) & ~(np.abs(maf) < 1e-8))[0]
     X = d["X"].astype(np.float32).astype(np.float64)
     t0 = time.perf_counter()
-    oracle.scan_lowrank_blas(rows, n, U, lam, 0.9, 0.4, 0.6, d["y"], X)
-    t_scan = time.perf_counter() - t0
-    scale = m / m_sample
-    est = (4 * t_apply + t_scan) * scale
-    sample = (f"numpy-BLAS restatement of apply_block (266 RHS) + scanLowRank block GEMMs "
-              f"over {m_sample} of {m} SNPs at N={n}, x{scale:.1f} to 4 applies + scan "
-              f"(QR/eigh/REML excluded): apply {t_apply:.2f}s, scan {t_scan:.2f}s")
-    return est, sample, t_apply + t_scan
+    r = oracle.lowrank_job_blas(B, d["y"], X, variants=variants, rank=RANK,
+                                oversample=OVERSAMPLE, n_threads=threads)
+    return time.perf_counter() - t0, r
+
+
+CPU_SAMPLE = ("one whole job, not a sample: Omega, 4 kinship applies with 266 right-hand sides "
+              "(512-SNP FP64 decode blocks, two BLAS GEMMs each), 3 QRs, B = Q^T K Q, eigh, "
+              "REML grid + golden search, and the Woodbury scan of every SNP (one BLAS GEMM "
+              "G^T [U|X|Py] per 512-SNP block) -- the oracle's restatement of the reference's "
+              "CPU path with numpy's threaded OpenBLAS for Eigen")
 
 
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle's restatement; the reference itself cannot be
+    built here) timed as whole jobs on every host core.  A job takes a minute or more, so the
+    arm runs whole jobs until --ref-budget seconds have passed (at least one, at most --steps)
+    and reports how many it ran; it never scales a partial job."""
     world, rank, local = dist_setup()
     if rank != 0:
         return 0
     from cosmicscanner_b200 import synth
 
     d = synth.config2(n=args.n, m=args.m)
-    threads = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
-    for _ in range(args.warmup):
-        cpu_reference_sample(d, threads, m_sample=256)
-    vals = []
-    sample = ""
-    for _ in range(args.steps):
-        est, sample, _ = cpu_reference_sample(d, threads)
-        vals.append(est)
+    threads = host_threads()
+    # warm-up: the BLAS threads and decode tables on a small slice, not a whole job
+    import oracle
+
+    small = synth.cohort(2000, 2000, 3, missing=0.02, n_causal=20)
+    oracle.lowrank_job_blas(oracle.Bed(small["bed"][3:].reshape(2000, -1), 2000), small["y"],
+                            small["X"], rank=64, n_threads=threads)
+    vals, last = [], None
+    t_start = time.perf_counter()
+    while len(vals) < max(1, args.steps):
+        el, last = cpu_job(d, threads)
+        vals.append(el)
+        if time.perf_counter() - t_start + el > args.ref_budget:
+            break
     value = float(np.mean(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "lmm matrix-free low-rank REML+scan, N=50000 M=100000 "
-                               "rank=256 sketch=266 p=3 (synthetic, 2 pops Fst=0.01, 2% missing)",
-                   "n": args.n, "m": args.m},
+        "n_gpus": args.gpus, "steps": len(vals), "requested_steps": args.steps, "warmup": 0,
+        "warmup_note": "one small job (N=2000, M=2000) warms the BLAS threads; no full-size warm-up",
+        "ms_per_step": value * 1e3, "seconds_each": vals, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": job_config(args.n, args.m),
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": sample},
+                         "sample": CPU_SAMPLE, "stages_s": last["seconds"]},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "sigma2_g": last["sigma2_g"], "sigma2_e": last["sigma2_e"], "rank": last["rank"],
+        "tested": int(last["tested"].sum()),
     }
     print(json.dumps(line))
     return 0
+
+
+def accuracy(mixed_diag, mixed_res, fp_diag, fp_res):
+    """The mixed step's error against the FP64 GPU step on the same inputs: relative error of
+    the variance components, max |delta BETA| / max |BETA| and the same for SE over the SNPs
+    both test, max |delta -log10 P|, and the number of SNPs whose tested flag differs."""
+    t = fp_res["tested"] & mixed_res["tested"]
+    out = {}
+    for key in ("sigma2_g", "sigma2_e"):
+        out[f"{key}_rel"] = abs(mixed_diag[key] - fp_diag[key]) / abs(fp_diag[key])
+    for key in ("beta", "se"):
+        out[f"{key}_max_rel"] = float(np.abs(mixed_res[key][t] - fp_res[key][t]).max() /
+                                      np.abs(fp_res[key][t]).max())
+    out["beta_max_abs_over_se"] = float((np.abs(mixed_res["beta"][t] - fp_res["beta"][t]) /
+                                         fp_res["se"][t]).max())
+    out["log10p_max_abs"] = float(np.abs(mixed_res["log10p"][t] - fp_res["log10p"][t]).max())
+    out["tested_mismatch"] = int((fp_res["tested"] != mixed_res["tested"]).sum())
+    out["freq_equal"] = bool(np.array_equal(mixed_res["freq"][t], fp_res["freq"][t]))
+    out["bounds"] = {"vc_rel": 1e-5, "beta_se_rel": 1e-5, "log10p_abs": 1e-3}
+    out["within_bounds"] = bool(max(out["sigma2_g_rel"], out["sigma2_e_rel"]) <= 1e-5 and
+                                max(out["beta_max_rel"], out["se_max_rel"]) <= 1e-5 and
+                                out["log10p_max_abs"] <= 1e-3 and out["tested_mismatch"] == 0)
+    return out
 
 
 def main():
@@ -516,9 +590,11 @@ def main():
     op = cs.KinshipOperator(g, None, variants)
     eng = cs.LmmEngine()
 
+    diag = {}
+
     def step():
-        eng.prepareLowRankMatrixFree(y, X, op, rank=RANK, oversample=OVERSAMPLE,
-                                     precision=args.precision)
+        diag.update(eng.prepareLowRankMatrixFree(y, X, op, rank=RANK, oversample=OVERSAMPLE,
+                                                 precision=args.precision))
         return eng.scan(g, keep, min_maf=0.01, precision=args.precision)
 
     for _ in range(args.warmup):
@@ -564,17 +640,34 @@ def main():
     cs.profile_enable(False)
     e2e_s = max_over_ranks(float(np.mean(e2e_ms)) / 1e3, world, device="cuda")
 
-    # ---- the plain FP64 GPU form of the same job, one step (the north-star comparison)
-    fp64_s = None
+    # ---- the plain FP64 GPU form of the same job, one step (the north-star comparison), with
+    # its top kernel profiled and the mixed step's error against it
+    fp64 = None
     if not args.no_fp64_compare and args.precision != "fp64":
         torch.cuda.synchronize()
+        cs.profile_enable(True)
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record()
-        eng.prepareLowRankMatrixFree(y, X, op, rank=RANK, oversample=OVERSAMPLE, precision="fp64")
-        eng.scan(g, keep, min_maf=0.01, precision="fp64")
+        fp_diag = eng.prepareLowRankMatrixFree(y, X, op, rank=RANK, oversample=OVERSAMPLE,
+                                               precision="fp64")
+        fp_res = eng.scan(g, keep, min_maf=0.01, precision="fp64")
         a1.record()
         torch.cuda.synchronize()
+        fp_prof = cs.profile_summary()
+        cs.profile_enable(False)
         fp64_s = a0.elapsed_time(a1) / 1e3
+        ftop = max(fp_prof["kernels"], key=lambda k: k["ms"])
+        f_ms = ftop["ms"] / ftop["launches"]
+        f_ach = ftop["flops"] / ftop["launches"] / (f_ms * 1e-3) / 1e12
+        dgemm = fp64_peak_tflops(torch)
+        fp64 = {"value": fp64_s, "unit": "s", "speedup_mixed_over_fp64": fp64_s / sec_per_step,
+                "roofline": {"bound": "fp64", "kernel": ftop["name"], "achieved": f_ach,
+                             "peak": dgemm, "unit": "TFLOP/s", "frac": f_ach / dgemm,
+                             "peak_kind": "cuBLAS DGEMM 8192^3 measured in this run",
+                             "ms_per_launch": f_ms, "launches": ftop["launches"],
+                             "share_of_step": ftop["ms"] / (fp64_s * 1e3)},
+                "note": "the same REML+scan step with FP64 kinship applies and scan projection",
+                "accuracy_of_mixed": accuracy(diag, res, fp_diag, fp_res)}
     serve = run_serve(cs, g, variants, d, args) if args.serve_requests > 0 and world == 1 else None
     dense = run_dense(cs, args) if args.dense_n > 0 and world == 1 else None
     aireml = None
@@ -624,32 +717,31 @@ def main():
                                      "frac": ops / ipeak}
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            threads = os.cpu_count() or 1
-            est, sample, _ = cpu_reference_sample(d, threads)
-            cpu = {"value": est, "unit": "s", "cores": threads, "kind": "port", "sample": sample}
+            threads = host_threads()
+            el, cr = cpu_job(d, threads)
+            cpu = {"value": el, "unit": "s", "cores": threads, "kind": "port", "sample": CPU_SAMPLE,
+                   "stages_s": cr["seconds"], "sigma2_g": cr["sigma2_g"],
+                   "sigma2_e": cr["sigma2_e"], "rank": cr["rank"],
+                   "sigma2_g_rel_to_gpu": abs(cr["sigma2_g"] - diag["sigma2_g"]) / abs(cr["sigma2_g"])}
         h2d = bed.nbytes + y.nbytes + X.nbytes + keep.nbytes
         d2h = m * (5 * 8 + 4)
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_step * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f16x2/f32+f64",
+            "dtype": "f64" if args.precision == "fp64" else
+                     "i8xi8->i32 (tcgen05.mma kind::i8, right-hand sides as 3 int8 pieces) + f64 "
+                     "epilogue, QR, eigh, REML and scan statistics",
             "data": "synthetic",
-            "config": {"workload": "lmm matrix-free low-rank REML+scan, N=50000 M=100000 "
-                                   "rank=256 sketch=266 p=3 (synthetic, 2 pops Fst=0.01, "
-                                   "2% missing)",
-                       "n": n, "m": m, "precision": args.precision,
-                       "l2": "inputs (1.25 GB packed) larger than L2; no flush",
-                       "parallelism": f"replicas x{world}"},
+            "config": job_config(n, m),
+            "precision": args.precision, "parallelism": f"replicas x{world}",
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_s / world, "unit": "s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "pinned_host": bool(pinned),
                     "ms_each": e2e_ms, "host_stages": e2e_prof.get("host", [])},
-            "fp64_gpu": None if fp64_s is None else {
-                "value": fp64_s, "unit": "s",
-                "speedup_mixed_over_fp64": fp64_s / sec_per_step,
-                "note": "the same REML+scan step with FP64 kinship applies and scan projection"},
+            "fp64_gpu": fp64,
+            "accuracy": None if fp64 is None else fp64["accuracy_of_mixed"],
             "serve": serve,
             "aireml": aireml,
             "dense": dense,

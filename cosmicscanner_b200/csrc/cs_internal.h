@@ -4,6 +4,7 @@
 #include <stdint.h>
 
 #include <functional>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -26,6 +27,34 @@ inline void check_cuda(cudaError_t e, const char* what) {
 }
 #define CS_CUDA(call) ::cs::check_cuda((call), #call)
 #define CS_LAUNCH(what) ::cs::check_cuda(cudaGetLastError(), what)
+
+// Function attributes (e.g. the dynamic shared-memory limit) belong to one device: a setup
+// done once per process would leave every other device at its defaults.  PerDeviceOnce runs
+// a setup once for each device it is used on (the current device at the call), from any
+// thread, and reports the setup's status on every call.
+struct PerDeviceOnce {
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu;
+    uint64_t done = 0;  // bit d: device d set up
+    cudaError_t err[kMaxDevices] = {};
+};
+template <class F>
+void once_per_device(PerDeviceOnce& o, F&& setup, const char* what) {
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), what);
+    if (dev < 0 || dev >= PerDeviceOnce::kMaxDevices)
+        fail(CS_ERR_UNSUPPORTED, std::string(what) + ": device ordinal out of range");
+    cudaError_t e;
+    {
+        std::lock_guard<std::mutex> lk(o.mu);
+        if (!((o.done >> dev) & 1u)) {
+            o.err[dev] = setup();
+            o.done |= uint64_t(1) << dev;
+        }
+        e = o.err[dev];
+    }
+    check_cuda(e, what);
+}
 
 // PLINK 2-bit codes (libCosmicCore/src/plink_reader.cpp:12-21):
 // 00 -> 2 copies of A1, 01 -> missing, 10 -> 1, 11 -> 0.

@@ -279,11 +279,10 @@ void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, in
     using C = Cfg<BM, BN, TM, TN>;
     const size_t smem = C::smem_a + C::smem_b + (ROWS ? C::smem_p : 0);
     auto kern = ROWS ? k_rows_fp64<BM, BN, TM, TN> : k_samples_fp64<BM, BN, TM, TN>;
-    static bool configured = false;
-    if (!configured) {
-        CS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
+    static PerDeviceOnce configured;
+    once_per_device(configured, [&] {
+        return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }, "configure FP64 decode-GEMM kernel");
     const int64_t R = ROWS ? v.n_rows : v.n_samples;   // output rows
     const int64_t K = ROWS ? v.n_samples : v.n_rows;   // contraction length
     const int64_t gx = (R + BM - 1) / BM, gy = (k + BN - 1) / BN;

@@ -850,15 +850,14 @@ cudaError_t allow_smem() {
 }
 
 void configure_kernels() {
-    static std::once_flag once;
-    static cudaError_t err = cudaSuccess;
-    std::call_once(once, [] {
-        err = allow_smem<true, false>();
+    static PerDeviceOnce configured;
+    once_per_device(configured, [] {
+        cudaError_t err = allow_smem<true, false>();
         if (err == cudaSuccess) err = allow_smem<false, false>();
         if (err == cudaSuccess) err = allow_smem<true, true>();
         if (err == cudaSuccess) err = allow_smem<false, true>();
-    });
-    check_cuda(err, "configure tensor-core kernels");
+        return err;
+    }, "configure tensor-core kernels");
 }
 
 // Clusters of two CTAs that can be resident at once (an SM without a partner in its GPC

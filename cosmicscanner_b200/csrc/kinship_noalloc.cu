@@ -13,6 +13,11 @@
 // code the array's name is only a host-side stand-in, so its device address is looked up
 // with cudaGetSymbolAddress once per device (with that device current) on the first call
 // made on that device; that first call should therefore come before any stream capture.
+// The cached address belongs to the device's current context: the library must not be used
+// across a cudaDeviceReset (or any other teardown of that context).
+// The operator's device must be the current device: its packed rows and lookup table live
+// there, and the scratch address is that device's; a call made with another device current
+// is refused with CS_ERR_INVALID_ARGUMENT rather than run on the wrong GPU.
 // All calls share the one array and it keeps the previous call's contents: every scratch
 // element a call reads is first written by the same call, so nothing needs clearing, but
 // two calls whose work overlaps on the GPU (different streams, or different host threads
@@ -70,6 +75,13 @@ void kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t
     if (k < 0) fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
     if (ldx < op->rows || ldy < op->rows)
         fail(CS_ERR_INVALID_ARGUMENT, "PlinkKinshipOperator::apply: dimension mismatch");
+    int dev = 0;
+    CS_CUDA(cudaGetDevice(&dev));
+    if (dev != op->g->device)
+        fail(CS_ERR_INVALID_ARGUMENT,
+             "cs_kinship_apply_noalloc: the operator lives on device " +
+                 std::to_string(op->g->device) + " but device " + std::to_string(dev) +
+                 " is current");
     if (k == 0) return;
     const int64_t n = op->rows, R = op->n_active;
     const int64_t need = (2 * n + R) * k;

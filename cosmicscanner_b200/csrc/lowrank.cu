@@ -648,13 +648,11 @@ static void rotate_eigenvectors(cs_lmm* l, const std::vector<double>& Qh,
     CS_CUDA(cudaMemcpyAsync(l->d_rot_i.get(), ri.data(), 4 * ri.size(), cudaMemcpyHostToDevice, s));
     CS_CUDA(cudaMemcpyAsync(l->d_rot_cs.get(), rcs.data(), 16 * rcs.size(), cudaMemcpyHostToDevice, s));
     const size_t smem = (size_t)n * 32 * sizeof(double);
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_rotate_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    static PerDeviceOnce configured;
+    once_per_device(configured, [] {
+        return cudaFuncSetAttribute(k_rotate_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     200 * 1024);
-    });
-    check_cuda(attr, "configure eigenvector rotation kernel");
+    }, "configure eigenvector rotation kernel");
     if (smem > 200 * 1024) fail(CS_ERR_UNSUPPORTED, "sketch too wide for the rotation kernel");
     prof::Scope ps("eigvec_rotations", s, 6.0 * (double)nr * n, 0.0);
     k_rotate_rows<<<(unsigned)((n + 31) / 32), 32, smem, s>>>(
@@ -1376,7 +1374,9 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
         CS_CUDA(cudaMemcpyAsync(l->d_lut.get(), lut.data(), 32 * M, cudaMemcpyHostToDevice, s));
         CS_CUDA(cudaMemcpyAsync(l->d_gn2.get(), gn2.data(), 8 * M, cudaMemcpyHostToDevice, s));
         CS_CUDA(cudaMemcpyAsync(l->d_pass.get(), pass.data(), M, cudaMemcpyHostToDevice, s));
-        // the host vectors must outlive the copies: keep them as the cached encoding
+        // cached so that later traits over the same window reuse this encoding (the copies
+        // above are staged from pageable memory before they return, so nothing here keeps
+        // their sources alive; pinned sources would have to be kept until the copy ends)
         l->enc_lut = lut;
         l->enc_gn2 = gn2;
         l->enc_fr = fr;

@@ -89,7 +89,9 @@ int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t 
  * (2 * rows() + selected variants) * k <= 2^21 doubles, else CS_ERR_INVALID_ARGUMENT.
  * Allocates nothing.  The first call on a device looks up the array's device address and
  * should come before any stream capture.  Calls share the array: calls whose work
- * overlaps on the GPU race and must be serialised by the caller.  Device pointers. */
+ * overlaps on the GPU race and must be serialised by the caller.  The operator's device
+ * must be current (else CS_ERR_INVALID_ARGUMENT), and the library must not be used across a
+ * cudaDeviceReset of that device (the array's address is looked up once).  Device pointers. */
 int cs_kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                              int64_t ldy, void* stream);
 /* trace() and getDiagonal() (kinship_operator.cpp:306-368); diag is a host array. */

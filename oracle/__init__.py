@@ -94,6 +94,9 @@ def lib():
         L.orc_stcg_vce.argtypes = [_P, _I64, _I64, _I64, _P, _P, _P, _I64, C.c_int, _P, _P, _I64,
                                    _P, _P, _P, _P, _P]
         L.orc_stcg_vce.restype = C.c_int
+        L.orc_stcg_vce_dense.argtypes = [_P, _I64, _P, _I64, C.c_int, _P, _P, _I64, _P, _P, _P,
+                                         _P, _P]
+        L.orc_stcg_vce_dense.restype = C.c_int
         L.orc_stcg_scan.argtypes = [_P, _I64, _I64, _P, _I64, _P, _P, _I64, _P, _P, _I64,
                                     C.c_double, C.c_double, C.c_double, C.c_double, _I64, _I64,
                                     _P, _P, _P, _P, _P, _P]
@@ -101,6 +104,10 @@ def lib():
         L.orc_mvlmm_scan.argtypes = [_P, _I64, _I64, _P, _I64, _P, _I64, _P, _P, _I64, _P, _I64,
                                      _P, _P, _I64, _I64, _P, _P, _P, _P, _P, _P]
         L.orc_mvlmm_scan.restype = C.c_int
+        L.orc_decode_z_cols.argtypes = [_P, _I64, _P, _P, _P, _I64, _I64, _P, _I64, C.c_int]
+        L.orc_scan_encode_cols.argtypes = [_P, _I64, _I64, _I64, _I64, C.c_double, _P, _I64, _P,
+                                           _P, _P, C.c_int]
+        L.orc_chisq_prob_vec.argtypes = [_P, _I64, C.c_int, _P, C.c_int]
         _lib = L
     return _lib
 
@@ -229,9 +236,10 @@ class Bed:
 
 def stcg_vce(bed: "Bed", y, X, rec_to_row=None, with_pe=False, max_iter=50, tol=1e-6,
              mc_samples=20, pcg_tol=1e-10, pcg_max_iter=2000, slq_probes=30, slq_steps=15,
-             probe_seed=20250101):
+             probe_seed=20250101, dense_k=None):
     """STCG_VCE::solve restated (libCosmicCore/src/stcg_vce.cpp:157-407); returns
-    (result dict, beta, a_rows, pe_rows)."""
+    (result dict, beta, a_rows, pe_rows).  dense_k: the kinship operator as a dense
+    K = Z Z^T / M (bed.n x bed.n), applied as one matrix-vector product per CG step."""
     y = np.ascontiguousarray(y, dtype=np.float64)
     X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
     rmap = None if rec_to_row is None else np.ascontiguousarray(rec_to_row, dtype=np.int32)
@@ -241,10 +249,16 @@ def stcg_vce(bed: "Bed", y, X, rec_to_row=None, with_pe=False, max_iter=50, tol=
     beta = np.zeros(X.shape[1])
     a = np.zeros(bed.n)
     pe = np.zeros(bed.n)
-    rc = lib().orc_stcg_vce(_ptr(bed.rows), bed.n, bed.stride, bed.m, _ptr(bed.mean),
-                            _ptr(bed.inv_std), _ptr(rmap), len(y), int(bool(with_pe)), _ptr(y),
-                            _ptr(X), X.shape[1], C.byref(opt), C.byref(res), _ptr(beta), _ptr(a),
-                            _ptr(pe))
+    if dense_k is not None:
+        K = np.asfortranarray(dense_k, dtype=np.float64)
+        rc = lib().orc_stcg_vce_dense(_ptr(K), bed.n, _ptr(rmap), len(y), int(bool(with_pe)),
+                                      _ptr(y), _ptr(X), X.shape[1], C.byref(opt), C.byref(res),
+                                      _ptr(beta), _ptr(a), _ptr(pe))
+    else:
+        rc = lib().orc_stcg_vce(_ptr(bed.rows), bed.n, bed.stride, bed.m, _ptr(bed.mean),
+                                _ptr(bed.inv_std), _ptr(rmap), len(y), int(bool(with_pe)), _ptr(y),
+                                _ptr(X), X.shape[1], C.byref(opt), C.byref(res), _ptr(beta),
+                                _ptr(a), _ptr(pe))
     if rc != 0:
         raise RuntimeError("oracle stcg_vce failed")
     out = {name: getattr(res, name) for name, _ in res._fields_}
@@ -329,9 +343,9 @@ def prepare_marker(raw, min_maf=0.01):
 
 
 # ---------------------------------------------------------------- BLAS restatements
-# Timed CPU baseline: the reference's block algorithms with its GEMMs done by numpy's
-# multithreaded BLAS, standing in for Eigen's blocked GEMM (src/kinship_operator.cpp:225-302,
-# src/lmm_engine.cpp:1269-1361).  Decode tables follow src/kinship_operator.cpp:276-283.
+# Timed CPU baseline: the whole low-rank job with numpy's multithreaded BLAS/LAPACK standing in
+# for Eigen's GEMMs, Householder QR and eigensolver, and OpenMP table decodes in liboracle.
+# Decode tables follow src/kinship_operator.cpp:276-283.
 
 def _decode_block(rows, n, values):
     """rows: (b, stride) packed bytes; values: (b, 4) per-row code values -> (n, b) FP64."""
@@ -339,43 +353,198 @@ def _decode_block(rows, n, values):
     return np.take_along_axis(values, codes.astype(np.int64), axis=1).T.copy()
 
 
-def apply_block_blas(rows, n, mean, inv_std, X, block=512):
-    """K X over all rows of `rows` (m x stride packed, magic skipped), FP64, BLAS GEMMs."""
-    m = rows.shape[0]
-    out = np.zeros((n, X.shape[1]))
-    for first in range(0, m, block):
-        r = rows[first:first + block]
-        mu, s = mean[first:first + block], inv_std[first:first + block]
-        vals = np.stack([(2.0 - mu) * s, np.zeros_like(mu), (1.0 - mu) * s, -mu * s], axis=1)
-        z = _decode_block(r, n, vals)
-        out += z @ (z.T @ X)
-    return out / m
+def _threads(n_threads):
+    if n_threads:
+        return int(n_threads)
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
-def scan_lowrank_blas(rows, n, U, lam, r0, sg2, se2, y, X, min_maf=0.01, block=512):
-    """scanLowRank (identity keep) with BLAS GEMMs per 512-SNP block; returns -log10 P."""
+def _reml_search(lam, r0, n, p, yty, Xty, XtX, Uty, UtX, y, X):
+    """The low-rank REML objective and search of src/lmm_engine.cpp:1010-1073 (81-point grid
+    on log eta in [-12, 12], then at most 80 golden-section steps to 1e-8), with the
+    projections U^T y, U^T X precomputed so that each evaluation is O(rank p^2)."""
+    df = n - p
+    rank = len(lam)
+
+    def objective(log_eta, want_q=False):
+        eta = np.exp(log_eta)
+        base = 1.0 / (1.0 + eta * r0)
+        c = 1.0 / (1.0 + eta * lam) - base
+        info = base * XtX + UtX.T @ (c[:, None] * UtX)
+        rhs = base * Xty + UtX.T @ (c * Uty)
+        try:
+            L = np.linalg.cholesky(info)
+        except np.linalg.LinAlgError:
+            return (np.inf, None) if want_q else np.inf
+        beta = np.linalg.solve(info, rhs)
+        r = y - X @ beta
+        Utr = Uty - UtX @ beta
+        q = base * float(r @ r) + float(Utr @ (c * Utr))
+        if not (q > 0.0) or not np.isfinite(q):
+            return (np.inf, None) if want_q else np.inf
+        logdet = (n - rank) * np.log1p(eta * r0) + np.log1p(eta * lam).sum()
+        logdet += 2.0 * np.log(np.abs(np.diag(L))).sum()
+        v = logdet + df * np.log(q / df)
+        return (v, q) if want_q else v
+
+    grid = 81
+    vals = [objective(-12.0 + 24.0 * i / (grid - 1)) for i in range(grid)]
+    best = int(np.argmin(vals))
+    left = -12.0 + 24.0 * max(0, best - 1) / (grid - 1)
+    right = -12.0 + 24.0 * min(grid - 1, best + 1) / (grid - 1)
+    golden = (np.sqrt(5.0) - 1.0) / 2.0
+    c = right - golden * (right - left)
+    d = left + golden * (right - left)
+    fc, fd = objective(c), objective(d)
+    for _ in range(80):
+        if right - left <= 1e-8:
+            break
+        if fc < fd:
+            right, d, fd = d, c, fc
+            c = right - golden * (right - left)
+            fc = objective(c)
+        else:
+            left, c, fc = c, d, fd
+            d = left + golden * (right - left)
+            fd = objective(d)
+    log_eta = 0.5 * (left + right)
+    _, q = objective(log_eta, want_q=True)
+    se2 = q / df
+    return {"log_eta": log_eta, "sigma2_e": se2, "sigma2_g": np.exp(log_eta) * se2,
+            "delta": np.exp(-log_eta)}
+
+
+def lowrank_job_blas(bed: "Bed", y, X, variants=None, rank=256, oversample=10, seed=42,
+                     min_maf=0.01, trace_threshold=0.95, min_rank=1, block=512, n_threads=None):
+    """The whole `gwas --model lmm --fastlmm --fastlmm-matrix-free --no-loco` job on the CPU for
+    every sample in .fam order: LmmEngine::prepareLowRankMatrixFree (src/lmm_engine.cpp:897-1095:
+    Omega from mt19937_64 + normal_distribution, K Omega, two power iterations with QR, a final
+    QR, B = Q^T K Q, its eigendecomposition, trace-fraction rank selection, tail-mean residual
+    eigenvalue, REML grid + golden search) and LmmEngine::scanLowRank over every SNP of the file
+    (src/lmm_engine.cpp:1269-1361), with Eigen's dense kernels as numpy BLAS/LAPACK calls.
+
+    Each kinship apply is apply_block (src/kinship_operator.cpp:225-302): per block of 512
+    selected SNPs, decode Z (n x 512) once and accumulate Z (Z^T V).  The scan forms, per block of
+    512 SNPs, G^T [U | X | Py] with one GEMM and reads V^-1 g's quadratic forms from it
+    (g^T V^-1 g = base g^T g + sum_j c_j (u_j^T g)^2), the same quantities as the reference's
+    V^-1 G block without materialising it.  Returns a dict with sigma2_g / sigma2_e, the rank,
+    per-SNP beta / se / log10p / freq / tested, and per-stage seconds."""
+    import time
+
+    threads = _threads(n_threads)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(len(y), -1))
+    n, p = X.shape
+    if n != bed.n:
+        raise ValueError("lowrank_job_blas: every sample in .fam order is required")
+    sel = (np.arange(bed.m, dtype=np.int32) if variants is None
+           else np.ascontiguousarray(variants, dtype=np.int32))
+    m_sel = len(sel)
+    sk = min(n, rank + max(0, oversample))
+    t = {}
+    t0 = time.perf_counter()
+    omega = normal_matrix(seed, n, sk)
+    t["omega"] = time.perf_counter() - t0
+    L = lib()
+    zbuf = np.empty((n, block), order="F")
+    trace_acc = [0.0]
+
+    def apply(V, want_trace=False):
+        out = np.zeros((n, V.shape[1]), order="F")
+        for first in range(0, m_sel, block):
+            cnt = min(block, m_sel - first)
+            snps = sel[first:first + cnt]
+            z = zbuf[:, :cnt]
+            L.orc_decode_z_cols(_ptr(bed.rows), bed.stride, _ptr(bed.mean), _ptr(bed.inv_std),
+                                _ptr(snps), cnt, n, z.ctypes.data, n, threads)
+            proj = z.T @ V
+            out += z @ proj
+            if want_trace:
+                trace_acc[0] += float(np.einsum("ij,ij->", z, z))
+        out *= 1.0 / m_sel
+        return out
+
+    t0 = time.perf_counter()
+    sample = apply(omega, want_trace=True)
+    total_trace = trace_acc[0] / m_sel
+    for _ in range(2):
+        q, _ = np.linalg.qr(sample)
+        sample = apply(q)
+    q, _ = np.linalg.qr(sample)
+    kq = apply(q)
+    t["applies_qr"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    small = q.T @ kq
+    small = 0.5 * (small + small.T)
+    evals, evecs = np.linalg.eigh(small)
+    lead = np.maximum(0.0, evals[::-1][:rank])
+    selected = rank
+    met = trace_threshold <= 0.0
+    if trace_threshold > 0.0 and total_trace > 0.0:
+        retained = np.cumsum(lead) / total_trace
+        first_allowed = min(rank, max(1, min_rank))
+        ok = np.nonzero((np.arange(1, rank + 1) >= first_allowed) & (retained >= trace_threshold))[0]
+        if len(ok):
+            selected = int(ok[0]) + 1
+            met = True
+    lam = lead[:selected].copy()
+    U = np.asfortranarray(q @ evecs[:, ::-1][:, :selected])
+    r0 = max(0.0, (total_trace - lam.sum()) / (n - selected))
+    UtX = U.T @ X
+    Uty = U.T @ y
+    reml = _reml_search(lam, r0, n, p, float(y @ y), X.T @ y, X.T @ X, Uty, UtX, y, X)
+    t["eigh_reml"] = time.perf_counter() - t0
+
+    # ---- scanLowRank (src/lmm_engine.cpp:1269-1361)
+    t0 = time.perf_counter()
+    sg2, se2 = reml["sigma2_g"], reml["sigma2_e"]
     base = 1.0 / max(1e-12, sg2 * r0 + se2)
-    corr = 1.0 / (sg2 * lam + se2) - base
-    vinv = lambda R: base * R + U @ (corr[:, None] * (U.T @ R))
-    vx = vinv(X)
-    info_inv = np.linalg.inv(X.T @ vx)
-    beta = info_inv @ (X.T @ vinv(y[:, None])).ravel()
-    py = vinv((y - X @ beta)[:, None]).ravel()
-    out = np.full(rows.shape[0], np.nan)
-    for first in range(0, rows.shape[0], block):
-        r = rows[first:first + block]
-        raw = _decode_block(r, n, np.tile(np.array([2.0, np.nan, 1.0, 0.0]), (r.shape[0], 1)))
-        obs = ~np.isnan(raw)
-        cnt = obs.sum(axis=0)
-        mean = np.nansum(raw, axis=0) / np.maximum(cnt, 1)
-        G = np.where(obs, raw - mean, 0.0)
-        vg = vinv(G)
-        score = G.T @ py
-        xvg = X.T @ vg
-        var = (G * vg).sum(axis=0) - (xvg * (info_inv @ xvg)).sum(axis=0)
+    c = 1.0 / (sg2 * lam + se2) - base
+    info = base * (X.T @ X) + UtX.T @ (c[:, None] * UtX)
+    info_inv = np.linalg.inv(info)
+    vy = base * (X.T @ y) + UtX.T @ (c * Uty)
+    beta_x = info_inv @ vy
+    resid = y - X @ beta_x
+    py = base * resid + U @ (c * (U.T @ resid))
+    B = np.asfortranarray(np.column_stack([U, X, py]))
+    m = bed.m
+    out = {k: np.full(m, np.nan) for k in ("beta", "se", "log10p", "freq")}
+    tested = np.zeros(m, dtype=bool)
+    gbuf = np.empty((n, block), order="F")
+    freq = np.empty(block)
+    passed = np.empty(block, dtype=np.int32)
+    gsq = np.empty(block)
+    for first in range(0, m, block):
+        cnt = min(block, m - first)
+        G = gbuf[:, :cnt]
+        L.orc_scan_encode_cols(_ptr(bed.rows), bed.stride, first, cnt, n, float(min_maf),
+                               G.ctypes.data, n, _ptr(freq), _ptr(passed), _ptr(gsq), threads)
+        A = G.T @ B                                  # cnt x (r + p + 1)
+        UtG = A[:, :selected]
+        XtG = A[:, selected:selected + p]
+        score = A[:, selected + p]
+        XtVG = base * XtG + UtG @ (c[:, None] * UtX)
+        var = base * gsq[:cnt] + (UtG * UtG) @ c - np.einsum("ja,ab,jb->j", XtVG, info_inv, XtVG)
+        ok = (passed[:cnt] != 0) & (var > 1e-12) & np.isfinite(var)
+        sl = slice(first, first + cnt)
+        out["freq"][sl] = np.where(ok, freq[:cnt], np.nan)
         with np.errstate(invalid="ignore", divide="ignore"):
-            out[first:first + block] = -np.log10(np.maximum(
-                np.exp(-0.5 * score ** 2 / var), 1e-300))
+            out["beta"][sl] = np.where(ok, score / var, np.nan)
+            out["se"][sl] = np.where(ok, 1.0 / np.sqrt(var), np.nan)
+            stat = np.where(ok, score * score / var, 0.0)
+        pv = np.empty(cnt)
+        L.orc_chisq_prob_vec(_ptr(np.ascontiguousarray(stat)), cnt, 1, _ptr(pv), threads)
+        with np.errstate(divide="ignore"):
+            out["log10p"][sl] = np.where(ok, np.where(pv > 0.0, -np.log10(np.maximum(pv, 1e-300)), 300.0), np.nan)
+        tested[sl] = ok
+    t["scan"] = time.perf_counter() - t0
+    out["tested"] = tested
+    out.update({"sigma2_g": sg2, "sigma2_e": se2, "rank": selected, "sketch": sk,
+                "residual_eigenvalue": r0, "trace": total_trace, "trace_threshold_met": bool(met),
+                "seconds": t, "threads": threads})
     return out
 
 

@@ -318,6 +318,7 @@ extern "C" {
 
 void orc_compute_stats(const uint8_t* bed, int64_t n_samples, int64_t n_snps, int64_t stride,
                        double* mean, double* inv_std, int32_t* count_out, double* sum_out) {
+#pragma omp parallel for schedule(static)
     for (int64_t j = 0; j < n_snps; ++j) {
         const uint8_t* col = bed + j * stride;
         double sum = 0.0, sum_sq = 0.0;
@@ -885,7 +886,20 @@ struct GenoMatrix {
     int64_t n, m, stride;
     const double* mean;
     const double* inv_std;
+    // Optional precomputed dense K = Z Z^T / m (n x n, column-major): the same operator applied
+    // as one matrix-vector product (rows summed in a fixed order), for sizes where the two
+    // genotype passes per CG step would make the restatement too slow to serve as a checker.
+    const double* dense_k = nullptr;
     void apply_G(const double* u, double* out) const {
+        if (dense_k) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int64_t j = 0; j < n; ++j) acc += dense_k[j + i * n] * u[j];
+                out[i] = acc;
+            }
+            return;
+        }
         std::vector<double> t(m);
         for (int64_t j = 0; j < m; ++j) {
             const double is = inv_std[j];
@@ -1120,13 +1134,12 @@ struct Stcg {
 
 extern "C" {
 
-int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
-                 const double* mean, const double* inv_std, const int32_t* rec_to_ind,
-                 int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
-                 const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
-                 double* a_ind_out, double* pe_ind_out) {
-    Stcg st{GenoMatrix{bed, n_fam, n_snps, stride, mean, inv_std}, rec_to_ind, n_rec, p,
-            with_pe != 0, y, X};
+static int stcg_vce_impl(const GenoMatrix& geno, const int32_t* rec_to_ind, int64_t n_rec,
+                         int with_pe, const double* y, const double* X, int64_t p,
+                         const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                         double* a_ind_out, double* pe_ind_out) {
+    const int64_t n_fam = geno.n;
+    Stcg st{geno, rec_to_ind, n_rec, p, with_pe != 0, y, X};
     st.pcg_tol = opt->pcg_tol;
     st.pcg_max_iter = opt->pcg_max_iter;
     const int64_t n = n_rec;
@@ -1345,6 +1358,25 @@ int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_sn
     res->sigma2_e = st.ve;
     res->pcg_iterations = st.pcg_iterations;
     return 0;
+}
+
+int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_snps,
+                 const double* mean, const double* inv_std, const int32_t* rec_to_ind,
+                 int64_t n_rec, int with_pe, const double* y, const double* X, int64_t p,
+                 const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                 double* a_ind_out, double* pe_ind_out) {
+    return stcg_vce_impl(GenoMatrix{bed, n_fam, n_snps, stride, mean, inv_std}, rec_to_ind, n_rec,
+                         with_pe, y, X, p, opt, res, beta_out, a_ind_out, pe_ind_out);
+}
+
+int orc_stcg_vce_dense(const double* K, int64_t n_fam, const int32_t* rec_to_ind, int64_t n_rec,
+                       int with_pe, const double* y, const double* X, int64_t p,
+                       const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                       double* a_ind_out, double* pe_ind_out) {
+    GenoMatrix geno{nullptr, n_fam, 0, 0, nullptr, nullptr};
+    geno.dense_k = K;
+    return stcg_vce_impl(geno, rec_to_ind, n_rec, with_pe, y, X, p, opt, res, beta_out, a_ind_out,
+                         pe_ind_out);
 }
 
 }  // extern "C"
@@ -1619,6 +1651,78 @@ int orc_mvlmm_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const int3
         for (int64_t a = 0; a < d * d; ++a) cov[o * d * d + a] = sinv[a];
     }
     return 0;
+}
+
+
+// ---------------------------------------------------------------- timed CPU restatement helpers
+// Byte-at-a-time table decode of SNP columns snps[0..count) (every sample), as the reference's
+// apply_block does per 512-SNP block (kinship_operator.cpp:265-285).
+void orc_decode_z_cols(const uint8_t* bed, int64_t stride, const double* mean,
+                       const double* inv_std, const int32_t* snps, int64_t count, int64_t n,
+                       double* z, int64_t ldz, int n_threads) {
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static)
+    for (int64_t j = 0; j < count; ++j) {
+        const int64_t snp = snps[j];
+        const double mu = mean[snp], is = inv_std[snp];
+        double* dest = z + j * ldz;
+        if (is == 0.0) {
+            std::fill(dest, dest + n, 0.0);
+            continue;
+        }
+        const double values[4] = {(2.0 - mu) * is, 0.0, (1.0 - mu) * is, -mu * is};
+        double quad[256][4];
+        for (int b = 0; b < 256; ++b)
+            for (int q = 0; q < 4; ++q) quad[b][q] = values[(b >> (2 * q)) & 3];
+        const uint8_t* col = bed + snp * stride;
+        const int64_t full = n >> 2;
+        for (int64_t b = 0; b < full; ++b) std::memcpy(dest + 4 * b, quad[col[b]], 32);
+        for (int64_t r = full << 2; r < n; ++r) dest[r] = values[code_at(col, r)];
+    }
+}
+
+// genotype_encoding.h:33-81 for every sample: raw dosage 2/1/0 (NaN for code 01), observed
+// count, A1 frequency = sum / (2 obs), pass = obs >= 3 and MAF >= min_maf; the encoded
+// column is raw - mean with missing calls at the mean (so 0 after centring); gsq = its
+// sum of squares.
+void orc_scan_encode_cols(const uint8_t* bed, int64_t stride, int64_t first, int64_t count,
+                          int64_t n, double min_maf, double* g, int64_t ldg, double* freq,
+                          int32_t* pass, double* gsq, int n_threads) {
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static)
+    for (int64_t j = 0; j < count; ++j) {
+        const uint8_t* col = bed + (first + j) * stride;
+        double* dest = g + j * ldg;
+        double sum = 0.0;
+        int observed = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            const int code = code_at(col, i);
+            if (code == 1) continue;
+            sum += code == 0 ? 2.0 : (code == 2 ? 1.0 : 0.0);
+            ++observed;
+        }
+        freq[j] = 0.0;
+        pass[j] = 0;
+        gsq[j] = 0.0;
+        if (observed == 0) {
+            std::fill(dest, dest + n, 0.0);
+            continue;
+        }
+        const double af = sum / (2.0 * observed);
+        freq[j] = af;
+        pass[j] = observed >= 3 && std::min(af, 1.0 - af) >= min_maf;
+        const double m = sum / observed;
+        const double values[4] = {2.0 - m, 0.0, 1.0 - m, 0.0 - m};
+        double sq = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            dest[i] = values[code_at(col, i)];
+            sq += dest[i] * dest[i];
+        }
+        gsq[j] = sq;
+    }
+}
+
+void orc_chisq_prob_vec(const double* stat, int64_t count, int df, double* out, int n_threads) {
+#pragma omp parallel for num_threads(std::max(1, n_threads)) schedule(static)
+    for (int64_t j = 0; j < count; ++j) out[j] = orc_chisq_prob(stat[j], df);
 }
 
 }  // extern "C"

@@ -165,6 +165,13 @@ int orc_stcg_vce(const uint8_t* bed, int64_t n_fam, int64_t stride, int64_t n_sn
                  const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
                  double* a_ind_out, double* pe_ind_out);
 
+/* orc_stcg_vce with the kinship operator given as a dense K = Z Z^T / M (n_fam x n_fam,
+ * column-major), each application one matrix-vector product. */
+int orc_stcg_vce_dense(const double* K, int64_t n_fam, const int32_t* rec_to_ind, int64_t n_rec,
+                       int with_pe, const double* y, const double* X, int64_t p,
+                       const orc_stcg_options* opt, orc_stcg_result* res, double* beta_out,
+                       double* a_ind_out, double* pe_ind_out);
+
 /* src/models/repeatability_scan_stcg.cpp:42-140 (scan_stcg_with_grm) with a given q x q
  * subject GRM G (column-major) for SNPs [snp_begin, snp_end); maf_out = folded MAF. */
 int orc_stcg_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const double* G, int64_t q,
@@ -180,6 +187,22 @@ int orc_mvlmm_scan(const uint8_t* bed, int64_t n_fam, int64_t stride, const int3
                    int64_t d, const double* UtX, int64_t p, const double* Vg, const double* Ve,
                    int64_t snp_begin, int64_t snp_end, double* beta, double* cov, double* wald,
                    double* pvalue, double* freq, int32_t* status);
+
+/* Helpers of the timed CPU restatement of the whole low-rank job (bench.py's CPU legs), every
+ * sample in .fam order, OpenMP over SNPs:
+ *  - orc_decode_z_cols: columns snps[0..count) of Z (n x count, ld ldz) with the decode
+ *    values of src/kinship_operator.cpp:276-283 ({(2-mu)s, 0, (1-mu)s, -mu s});
+ *  - orc_scan_encode_cols: genetics::prepareAssociationMarker (src/genetics/genotype_encoding.h:
+ *    33-81) for SNPs first..first+count-1: mean-imputed, centred dosages, A1 frequency, pass
+ *    flag and the column's sum of squares;
+ *  - orc_chisq_prob_vec: chisq_prob (src/lmm_engine.cpp:22-64) over an array. */
+void orc_decode_z_cols(const uint8_t* bed, int64_t stride, const double* mean,
+                       const double* inv_std, const int32_t* snps, int64_t count, int64_t n,
+                       double* z, int64_t ldz, int n_threads);
+void orc_scan_encode_cols(const uint8_t* bed, int64_t stride, int64_t first, int64_t count,
+                          int64_t n, double min_maf, double* g, int64_t ldg, double* freq,
+                          int32_t* pass, double* gsq, int n_threads);
+void orc_chisq_prob_vec(const double* stat, int64_t count, int df, double* out, int n_threads);
 
 #ifdef __cplusplus
 }
