@@ -57,6 +57,15 @@ def parse():
     ap.add_argument("--k", type=int, default=68, help="right-hand sides for --apply-only")
     ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests in the serving stream measured after the job (0 skips)")
+    ap.add_argument("--serve-config5", action="store_true",
+                    help="serve on the serving configuration's resident matrix (--serve-n x "
+                         "--serve-m) instead of the job's")
+    ap.add_argument("--serve-n", type=int, default=200000)
+    ap.add_argument("--serve-m", type=int, default=500000)
+    ap.add_argument("--serve-fp64-sample", type=int, default=4,
+                    help="requests the plain FP64 form serves one at a time beside the stream")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="only the serving measurement")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the one-step timing of the plain FP64 GPU form")
     ap.add_argument("--dense-n", type=int, default=10000,
@@ -66,8 +75,10 @@ def parse():
                     help="only the dense exact-route measurement (the case its ncu captures use)")
     ap.add_argument("--ref-budget", type=float, default=240.0,
                     help="seconds of whole CPU jobs the reference arm runs (at least one)")
-    ap.add_argument("--aireml-iters", type=int, default=2,
-                    help="AI-REML (PCG + Hutchinson) iterations timed per precision (0 skips)")
+    ap.add_argument("--aireml-iters", type=int, default=50,
+                    help="AI-REML (PCG + Hutchinson) iterations of the timed full run (0 skips)")
+    ap.add_argument("--precond-rank", type=int, default=64,
+                    help="rank of the AI-REML's low-rank deflation preconditioner (0: scalar)")
     return ap.parse_args()
 
 
@@ -284,16 +295,19 @@ def run_apply_only(args):
     return 0
 
 
-def run_serve(cs, g, variants, d, args):
+def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp64_sample=0,
+              label=""):
     """A Poisson stream of association requests against the resident genotypes: subsets of
-    log-uniform size 5,000..N, 1..16 traits, an intercept and 2..5 N(0,1) covariates, full
-    low-rank REML on all SNPs and a scan of a random contiguous window of M/2 SNPs (the
-    serving configuration's shapes, scaled to the resident matrix).  Arrivals at 80 % of the
-    single-request service rate.  Returns the server's latency / throughput statistics."""
+    log-uniform size 5,000..N, 1..16 traits with h2 ~ U(0.1, 0.7), an intercept and 2..5 N(0,1)
+    covariates, full low-rank REML on all SNPs and a scan of a random contiguous window
+    (`window` SNPs, default M/2).  Arrivals at 80 % of the server's measured capacity.  With
+    `fp64_sample` > 0, the plain FP64 form serves that many of the same requests one at a time
+    (a bounded sample of the stream: its per-request latency gives its throughput).  Returns
+    the server's latency / throughput statistics."""
     n, m = d["n"], d["m"]
     rng = np.random.default_rng(20261208)
     base = (d["y"] - d["y"].mean()) / d["y"].std()
-    window = max(1, m // 2)
+    window = max(1, m // 2) if window is None else min(window, m)
 
     def request():
         n_sub = int(np.exp(rng.uniform(np.log(min(5000, n // 2)), np.log(n))))
@@ -308,7 +322,8 @@ def run_serve(cs, g, variants, d, args):
         return S, Y, X.astype(np.float32).astype(np.float64), b, b + window
 
     reqs = [request() for _ in range(args.serve_requests)]
-    srv = cs.Server(g, variants, precision=args.precision, max_active=8)
+    srv = cs.Server(g, variants, precision=args.precision, max_active=8,
+                    max_batch_columns=max_batch_columns)
     # one untimed request (the server's threads, handles and buffers come up); the service time
     # of one request alone; the capacity: eight requests submitted at once, completed per
     # second.  Arrivals come at 80 % of that capacity.
@@ -319,6 +334,8 @@ def run_serve(cs, g, variants, d, args):
     for rid in cal:
         srv.wait(rid)
     capacity = len(cal) / (time.perf_counter() - c0)
+    for rid in cal:
+        srv.release(rid)
     st0 = srv.stats()
     rate = 0.8 * capacity
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
@@ -330,51 +347,122 @@ def run_serve(cs, g, variants, d, args):
             time.sleep(delay)
         t_sub.append(time.perf_counter())
         ids.append(srv.submit(S, Y, X, b, e))
-    lat = np.array([srv.wait(rid)["latency_s"] for rid in ids])
+    lat = []
+    for rid in ids:
+        lat.append(srv.wait(rid)["latency_s"])
+        srv.release(rid)
+    lat = np.array(lat)
     st = srv.stats()
     srv.close()
     wall = float(np.max(np.array(t_sub) + lat) - t_sub[0])
     applies = st["applies"] - st0["applies"]
-    return {
+    sizes = np.array([len(q[0]) for q in reqs])
+    out = {
         "requests": len(reqs), "req_per_s": len(reqs) / wall,
         "p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
         "mean_ms": float(lat.mean()) * 1e3,
         "single_request_ms": single * 1e3, "capacity_rps": capacity, "arrival_rate_per_s": rate,
-        "applies": applies,
-        "mean_columns_per_apply": (st["apply_columns"] - st0["apply_columns"]) / max(1, applies),
+        "stacked_applies": applies,
+        "mean_columns_per_stacked_apply": (st["apply_columns"] - st0["apply_columns"]) / max(1, applies),
         "max_requests_per_apply": st["max_requests_per_apply"],
+        "own_view_requests": st["own_view_requests"], "memory_budget_gb": st["memory_budget_gb"],
         "max_concurrent": st["max_concurrent"], "failed": st["failed"],
-        "config": f"resident N={n} M={m}; subsets log-U[5000,{n}], traits U{{1..16}}, "
-                  f"intercept + U{{2..5}} N(0,1) covariates, window {window} SNPs, "
-                  f"Poisson arrivals at 80% of the capacity (8 requests at once), {args.precision}",
+        "cohort_size_median": float(np.median(sizes)), "cohort_size_mean": float(sizes.mean()),
+        "config": f"{label}resident N={n} M={m}; {len(reqs)} requests; subsets log-U[5000,{n}], "
+                  f"traits U{{1..16}}, intercept + U{{2..5}} N(0,1) covariates, window {window} "
+                  f"SNPs, Poisson arrivals at 80% of the capacity (8 requests at once), "
+                  f"{args.precision}; cohorts below N/2 on their own repacked subset operator",
     }
+    if fp64_sample > 0:
+        one = cs.Server(g, variants, precision="fp64", max_active=1,
+                        max_batch_columns=max_batch_columns)
+        lat64 = []
+        for q in reqs[:fp64_sample]:
+            rid = one.submit(*q)
+            lat64.append(one.wait(rid)["latency_s"])
+            one.release(rid)
+        one.close()
+        lat64 = np.array(lat64)
+        mixed_same = lat[:fp64_sample]
+        out["fp64_one_at_a_time"] = {
+            "requests": fp64_sample, "mean_ms": float(lat64.mean()) * 1e3,
+            "req_per_s": 1.0 / float(lat64.mean()),
+            "p50_ms": float(np.percentile(lat64, 50)) * 1e3,
+            "sample": f"the first {fp64_sample} requests of the stream, one at a time (the "
+                      f"whole stream would take ~{lat64.mean() * len(reqs) / 60:.0f} min)",
+            "throughput_ratio_mixed_batched_over_fp64": (len(reqs) / wall) * float(lat64.mean()),
+            "mixed_latency_same_requests_ms": float(mixed_same.mean()) * 1e3}
+    return out
 
 
-def run_aireml(cs, op, d, args, iters=4, probes=64):
-    """The PCG + Hutchinson AI-REML route (STCG_VCE with the single-record design, the
-    configuration's 64 Rademacher probes and 1 + p right-hand sides, absolute CG tolerance
-    1e-10): `iters` AI-REML iterations in the mixed form and in the FP64 form, seconds per
-    iteration each (the same probes, so the same CG systems)."""
+def run_serve_config5(cs, args):
+    """The serving configuration at its stated shape: a resident N=200,000 x M=500,000 packed
+    matrix (~25 GB; MAF U(0.01, 0.5), three Balding-Nichols populations at Fst 0.02, 1% missing)
+    and a stream of --serve-requests requests with 50,000-SNP scan windows."""
     import torch
 
-    out = {}
-    for prec in (args.precision, "fp64") if args.precision != "fp64" else ("fp64",):
+    from cosmicscanner_b200 import synth
+
+    t0 = time.perf_counter()
+    d = synth.cohort(args.serve_n, args.serve_m, 20261203 + 5, maf_lo=0.01, n_pops=3, fst=0.02,
+                     missing=0.01, n_causal=1000, h2=0.5)
+    gen_s = time.perf_counter() - t0
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    variants = cs.grm_variant_selection(g.stats(), 0.01)
+    del d["bed"]
+    torch.cuda.synchronize()
+    out = run_serve(cs, g, variants, d, args, window=50000, max_batch_columns=1024,
+                    fp64_sample=args.serve_fp64_sample, label="serving configuration: ")
+    out["generation_s"] = gen_s
+    g.close()
+    return out
+
+
+def run_aireml(cs, op, d, args, iters=50, probes=64, precond_rank=64, compare_iters=6):
+    """The PCG + Hutchinson AI-REML route (STCG_VCE with the single-record design, the
+    configuration's 64 Rademacher probes, 1 + p right-hand sides, absolute CG tolerance 1e-10):
+      * `full`: the reference's default run -- up to 50 iterations (probes are redrawn each
+        iteration, so it seldom stops early), SLQ log-likelihood (30 probes x 15 steps) -- in the
+        mixed form with the low-rank deflation preconditioner, timed end to end;
+      * `compare`: `compare_iters` iterations (4 EM + AI steps, no SLQ) in the mixed form and the
+        FP64 form with the same probes and preconditioner, and in the mixed form with the
+        reference's scalar preconditioner: seconds per iteration, CG iterations per solve,
+        kinship applies and their mean width, and the mixed form's VC error against FP64."""
+    import torch
+
+    def one(prec, it, slq, rank):
         vce = cs.StcgVce()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r = vce.solve(op, d["y"], d["X"], kinship_divisor=float(d["m"]), max_iter=iters,
-                      mc_samples=probes, slq_probes=0, precision=prec)
+        r = vce.solve(op, d["y"], d["X"], kinship_divisor=float(d["m"]), max_iter=it,
+                      mc_samples=probes, slq_probes=slq, precision=prec, precond_rank=rank)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        out[prec] = {"s_per_iteration": dt / max(1, r["iterations"]), "iterations": r["iterations"],
-                     "sigma2_g": r["sigma2_g"], "sigma2_e": r["sigma2_e"],
-                     "kinship_applies": r["operator_applies"],
-                     "rhs_per_apply": r["operator_columns"] / max(1, r["operator_applies"])}
         vce.close()
-    if len(out) == 2:
-        out["speedup_mixed_over_fp64"] = out["fp64"]["s_per_iteration"] / out[args.precision]["s_per_iteration"]
+        solves = (1 + d["X"].shape[1] + probes + 3) * max(1, r["iterations"])
+        return {"seconds": dt, "s_per_iteration": dt / max(1, r["iterations"]),
+                "iterations": r["iterations"], "converged": bool(r["converged"]),
+                "sigma2_g": r["sigma2_g"], "sigma2_e": r["sigma2_e"], "logl": r["logl"],
+                "pcg_iterations": r["pcg_iterations"],
+                "cg_iterations_per_solve": r["pcg_iterations"] / solves,
+                "kinship_applies": r["operator_applies"],
+                "rhs_per_apply": r["operator_columns"] / max(1, r["operator_applies"]),
+                "ms_per_apply": 1e3 * dt / max(1, r["operator_applies"]),
+                "precond_rank": rank, "precision": prec}
+
+    out = {"full": one(args.precision, iters, 30, precond_rank)}
+    cmp = {"mixed": one(args.precision, compare_iters, 0, precond_rank),
+           "fp64": one("fp64", compare_iters, 0, precond_rank),
+           "mixed_scalar_precond": one(args.precision, compare_iters, 0, 0)}
+    for key in ("sigma2_g", "sigma2_e"):
+        cmp[f"{key}_rel_mixed_vs_fp64"] = abs(cmp["mixed"][key] - cmp["fp64"][key]) / abs(cmp["fp64"][key])
+    cmp["speedup_mixed_over_fp64"] = cmp["fp64"]["s_per_iteration"] / cmp["mixed"]["s_per_iteration"]
+    cmp["speedup_deflation_over_scalar"] = (cmp["mixed_scalar_precond"]["s_per_iteration"] /
+                                            cmp["mixed"]["s_per_iteration"])
+    out["compare"] = cmp
     out["config"] = (f"N={d['n']} M={d['m']}, {probes} probes + y + {d['X'].shape[1]} covariates, "
-                     f"pcg_tol 1e-10 absolute, {iters} iterations (EM warm-up steps)")
+                     f"pcg_tol 1e-10 absolute; full: up to {iters} iterations with SLQ (30 x 15), "
+                     f"low-rank deflation rank {precond_rank}; compare: {compare_iters} iterations")
     return out
 
 
@@ -553,6 +641,14 @@ def main():
         return run_reference(args)
     if args.apply_only:
         return run_apply_only(args)
+    if args.serve_only:
+        import torch
+
+        import cosmicscanner_b200 as cs
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"serve": run_serve_config5(cs, args) if args.serve_config5 else None}))
+        return 0
     if args.dense_only:
         import torch
 
@@ -668,12 +764,16 @@ def main():
                              "share_of_step": ftop["ms"] / (fp64_s * 1e3)},
                 "note": "the same REML+scan step with FP64 kinship applies and scan projection",
                 "accuracy_of_mixed": accuracy(diag, res, fp_diag, fp_res)}
-    serve = run_serve(cs, g, variants, d, args) if args.serve_requests > 0 and world == 1 else None
+    serve = None
+    if args.serve_requests > 0 and world == 1:
+        serve = (run_serve_config5(cs, args) if args.serve_config5 else
+                 run_serve(cs, g, variants, d, args, fp64_sample=args.serve_fp64_sample))
     dense = run_dense(cs, args) if args.dense_n > 0 and world == 1 else None
     aireml = None
     if args.aireml_iters > 0 and world == 1:
         op_all = cs.KinshipOperator(g, None, None)
-        aireml = run_aireml(cs, op_all, d, args, iters=args.aireml_iters)
+        aireml = run_aireml(cs, op_all, d, args, iters=args.aireml_iters,
+                            precond_rank=args.precond_rank)
         op_all.close()
 
     if rank == 0:

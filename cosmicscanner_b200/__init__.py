@@ -154,6 +154,30 @@ class KinshipOperator:
                                                C.c_void_p(Y_ptr), ldy, _prec(precision),
                                                C.c_void_p(stream)))
 
+    def multiply_Zt_v(self, X, precision="fp64") -> np.ndarray:
+        """GenotypeMatrix::multiply_Zt_v (libCosmicCore/src/matrix_adapter.h:40-53): Z^T X over
+        the selection, X (rows,) or (rows, k) -> (numVariants,) or (numVariants, k)."""
+        X = np.asarray(X, dtype=np.float64)
+        vec = X.ndim == 1
+        Xf = np.asfortranarray(X.reshape(-1, 1) if vec else X)
+        k = Xf.shape[1]
+        out = np.zeros((self._m, k), order="F")
+        _check(_abi.lib().cs_genotype_multiply_zt_host(self._h, _ptr(Xf), Xf.shape[0], k,
+                                                       _ptr(out), self._m, _prec(precision)))
+        return out[:, 0] if vec else out
+
+    def multiply_Z_v(self, V, precision="fp64") -> np.ndarray:
+        """GenotypeMatrix::multiply_Z_v: Z V over the selection, V (numVariants,) or
+        (numVariants, k) -> (rows,) or (rows, k)."""
+        V = np.asarray(V, dtype=np.float64)
+        vec = V.ndim == 1
+        Vf = np.asfortranarray(V.reshape(-1, 1) if vec else V)
+        k = Vf.shape[1]
+        out = np.zeros((self._rows, k), order="F")
+        _check(_abi.lib().cs_genotype_multiply_z_host(self._h, _ptr(Vf), Vf.shape[0], k,
+                                                      _ptr(out), self._rows, _prec(precision)))
+        return out[:, 0] if vec else out
+
     def trace(self) -> float:
         t = C.c_double()
         _check(_abi.lib().cs_kinship_trace(self._h, C.byref(t)))
@@ -489,13 +513,35 @@ def pcg_solve_device(op: KinshipOperator, B_ptr: int, ldb: int, k: int, X_ptr: i
     return it[:k]
 
 
+def pcg_solve_records_device(op: KinshipOperator, rec_to_row, n_records: int, B_ptr: int,
+                            ldb: int, k: int, X_ptr: int, ldx: int, sigma2_g: float,
+                            sigma2_e: float, sigma2_pe: float = 0.0, with_pe: bool = False,
+                            tol: float = 1e-10, max_iter: int = 2000, relative: bool = False,
+                            precision="fp64", kinship_divisor: float = 0.0,
+                            stream: int = 0) -> np.ndarray:
+    """MatrixFreePCG::solve with STCG_VCE's record-level covariance (stcg_vce.cpp:80-126):
+    V = sigma2_g Zr K Zr^T + sigma2_pe Zr Zr^T + sigma2_e I; returns iterations per column."""
+    rmap = None if rec_to_row is None else np.ascontiguousarray(rec_to_row, dtype=np.int32)
+    it = np.zeros(max(k, 1), dtype=np.int32)
+    _check(_abi.lib().cs_pcg_solve_records(
+        op._h, float(kinship_divisor), _ptr(rmap), int(n_records), int(bool(with_pe)),
+        float(sigma2_g), float(sigma2_pe), float(sigma2_e), C.c_void_p(B_ptr), ldb, k,
+        C.c_void_p(X_ptr), ldx, float(tol), int(relative), int(max_iter), _prec(precision),
+        _ptr(it), C.c_void_p(stream)))
+    return it[:k]
+
+
 class MatrixFreePCG:
-    """Host-array convenience over :func:`pcg_solve_device` (device memory through torch)."""
+    """Host-array convenience over :func:`pcg_solve_device` (device memory through torch).
+    With ``rec_to_row`` (and optionally ``with_pe`` / ``sigma2_pe``) the system is STCG_VCE's
+    record-level covariance."""
 
     def __init__(self, op: KinshipOperator, sigma2_g: float, sigma2_e: float, precision="fp64",
-                 kinship_divisor: float = 0.0):
+                 kinship_divisor: float = 0.0, rec_to_row=None, with_pe: bool = False,
+                 sigma2_pe: float = 0.0):
         self.op, self.sg2, self.se2 = op, sigma2_g, sigma2_e
         self.precision, self.divisor = precision, kinship_divisor
+        self.rec_to_row, self.with_pe, self.spe2 = rec_to_row, with_pe, sigma2_pe
         self.iterations = None
 
     def solve(self, b, tol: float = 1e-8, max_iter: int = 1000, relative: bool = False):
@@ -507,10 +553,16 @@ class MatrixFreePCG:
         n, k = B.shape
         dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()  # column-major n x k
         dX = torch.zeros_like(dB)
-        self.iterations = pcg_solve_device(self.op, dB.data_ptr(), n, k, dX.data_ptr(), n,
-                                           self.sg2, self.se2, tol, max_iter, relative,
-                                           self.precision, self.divisor,
-                                           torch.cuda.current_stream().cuda_stream)
+        stream = torch.cuda.current_stream().cuda_stream
+        if self.rec_to_row is None and not self.with_pe:
+            self.iterations = pcg_solve_device(self.op, dB.data_ptr(), n, k, dX.data_ptr(), n,
+                                               self.sg2, self.se2, tol, max_iter, relative,
+                                               self.precision, self.divisor, stream)
+        else:
+            self.iterations = pcg_solve_records_device(
+                self.op, self.rec_to_row, n, dB.data_ptr(), n, k, dX.data_ptr(), n, self.sg2,
+                self.se2, self.spe2, self.with_pe, tol, max_iter, relative, self.precision,
+                self.divisor, stream)
         torch.cuda.current_stream().synchronize()
         x = dX.cpu().numpy().T
         return x[:, 0].copy() if vec else np.asfortranarray(x)
@@ -521,7 +573,7 @@ class VceOptions(C.Structure):
         ("max_iter", C.c_int32), ("tol", C.c_double), ("mc_samples", C.c_int32),
         ("pcg_tol", C.c_double), ("pcg_relative", C.c_int32), ("pcg_max_iter", C.c_int32),
         ("slq_probes", C.c_int32), ("slq_steps", C.c_int32), ("probe_seed", C.c_uint64),
-        ("precision", C.c_int32),
+        ("precision", C.c_int32), ("precond_rank", C.c_int32),
     ]
 
 
@@ -660,6 +712,7 @@ class ServerOptions(C.Structure):
         ("min_rank", C.c_int32), ("min_maf", C.c_double), ("precision", C.c_int32),
         ("max_batch_columns", C.c_int64), ("memory_budget_gb", C.c_double),
         ("max_active", C.c_int32), ("batch_window_ms", C.c_double),
+        ("subset_fraction", C.c_double),
     ]
 
 
@@ -682,7 +735,8 @@ class ServerStatistics(C.Structure):
         ("p50_s", C.c_double), ("p99_s", C.c_double), ("mean_s", C.c_double),
         ("throughput_rps", C.c_double), ("wall_s", C.c_double), ("applies", C.c_int64),
         ("apply_columns", C.c_int64), ("max_requests_per_apply", C.c_int64),
-        ("max_concurrent", C.c_int64),
+        ("max_concurrent", C.c_int64), ("own_view_requests", C.c_int64),
+        ("memory_budget_gb", C.c_double),
     ]
 
 
@@ -1145,43 +1199,108 @@ def sort_chrom_labels(labels) -> list:
     return sorted(set(str(x) for x in labels), key=functools.cmp_to_key(before))
 
 
+class LmmRunOptions(C.Structure):
+    _fields_ = [
+        ("rank", C.c_int32), ("oversample", C.c_int32), ("seed", C.c_int64),
+        ("trace_threshold", C.c_double), ("min_rank", C.c_int32), ("min_maf", C.c_double),
+        ("precision", C.c_int32), ("loco", C.c_int32), ("no_fallback", C.c_int32),
+        ("error_tol", C.c_double),
+    ]
+
+
+class LmmRunScope(C.Structure):
+    _fields_ = [("label", C.c_char * 32), ("diag", LowRankDiagnostics), ("fallback", C.c_int32)]
+
+
+_FALLBACKS = {0: "none", 1: "trace_threshold", 2: "error_tolerance"}
+
+
+def _run_options(rank, oversample, seed, trace_threshold, min_rank, min_maf, precision, loco,
+                 no_fallback, error_tol) -> LmmRunOptions:
+    o = LmmRunOptions()
+    _abi.lib().cs_lmm_run_default_options(C.byref(o))
+    o.rank, o.oversample, o.seed = int(rank), int(oversample), int(seed)
+    o.trace_threshold, o.min_rank, o.min_maf = float(trace_threshold), int(min_rank), float(min_maf)
+    o.precision, o.loco, o.no_fallback = _prec(precision), int(bool(loco)), int(bool(no_fallback))
+    o.error_tol = float(error_tol)
+    return o
+
+
 def run_lmm_matrix_free(bed, n_samples: int, n_snps: int, y, X, keep=None, rank=256,
                         oversample=10, seed=42, trace_threshold=0.95, min_rank=1,
                         min_maf=0.01, precision="fp64", genotypes: Genotypes | None = None,
                         chrom=None, loco=True, no_fallback=True, error_tol=1.0):
     """The `gwas --model lmm --fastlmm --fastlmm-matrix-free --fastlmm-no-fallback --no-loco`
-    path (src/gwas_scanner.cpp:121-129, 254-346, 447) from host buffers: upload + stats,
-    GRM variant selection, operator, low-rank REML null model, scan of every SNP.  With
-    per-SNP chromosome labels spanning more than one chromosome (and loco=True) it runs the
-    reference's default leave-one-chromosome-out loop (src/gwas_scanner.cpp:299-314,
-    464-472): per chromosome, an operator without that chromosome's GRM variants, its own
-    null model, and the scan of that chromosome's SNPs.  no_fallback=False lets a null whose
-    sketch misses the trace threshold (or exceeds error_tol) fall back as the reference does
-    (_prepare_with_fallback).  Returns (results dict, diagnostics dict; per chromosome under
-    LOCO), each with its "fallback" label."""
+    path (src/gwas_scanner.cpp:121-129, 254-346, 447) from host buffers: upload + stats, then
+    the library's C++ job (cs_run_lmm_matrix_free): GRM variant selection, operator, low-rank
+    REML null model, scan of every SNP.  With per-SNP chromosome labels spanning more than one
+    chromosome (and loco=True) it runs the reference's default leave-one-chromosome-out loop
+    (src/gwas_scanner.cpp:299-314, 464-472): per chromosome, an operator without that
+    chromosome's GRM variants, its own null model, and the scan of that chromosome's SNPs.
+    no_fallback=False lets a null whose sketch misses the trace threshold (or exceeds
+    error_tol) fall back as the reference does.  Returns (results dict, diagnostics dict; per
+    chromosome under LOCO), each diagnostics dict with its "fallback" label."""
     g = genotypes if genotypes is not None else Genotypes.from_bed_bytes(bed, n_samples, n_snps)
-    keep_arr = np.arange(n_samples, dtype=np.int32) if keep is None else np.asarray(keep, np.int32)
-    variants = grm_variant_selection(g.stats(), min_maf)
-    if len(variants) == 0:
-        raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
-                              "Matrix-free GRM selection produced no variants")
-    if chrom is not None and loco and len(set(str(c) for c in chrom)) > 1:
-        res, diag = _run_loco(g, keep, keep_arr, variants, np.asarray(chrom).astype(str), y, X,
-                              rank, oversample, seed, trace_threshold, min_rank, min_maf, precision,
-                              no_fallback, error_tol)
+    try:
+        m = g.n_snps
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        X = np.asfortranarray(np.asarray(X, dtype=np.float32).astype(np.float64).reshape(len(y), -1))
+        keep_arr = None if keep is None else np.ascontiguousarray(keep, dtype=np.int32)
+        labels = None
+        if chrom is not None:
+            enc = [str(c).encode() for c in chrom]
+            labels = (C.c_char_p * len(enc))(*enc)
+        out = {k: np.zeros(m) for k in ("beta", "se", "p", "log10p", "freq")}
+        tested = np.zeros(m, dtype=np.int32)
+        scopes = (LmmRunScope * 128)()
+        n_sc = C.c_int32()
+        o = _run_options(rank, oversample, seed, trace_threshold, min_rank, min_maf, precision,
+                         loco, no_fallback, error_tol)
+        _check(_abi.lib().cs_run_lmm_matrix_free(
+            g._h, _ptr(keep_arr), 0 if keep_arr is None else len(keep_arr), _ptr(y), _ptr(X),
+            X.shape[1], labels, C.byref(o), _ptr(out["beta"]), _ptr(out["se"]), _ptr(out["p"]),
+            _ptr(out["log10p"]), _ptr(out["freq"]), _ptr(tested), scopes, len(scopes),
+            C.byref(n_sc)))
+        out["tested"] = tested.astype(bool)
+        diags = {}
+        for i in range(min(n_sc.value, len(scopes))):
+            sc = scopes[i]
+            diags[sc.label.decode()] = dict(sc.diag.as_dict(), fallback=_FALLBACKS[sc.fallback])
+        if list(diags) == ["GLOBAL"]:
+            return out, diags["GLOBAL"]
+        return out, diags
+    finally:
         if genotypes is None:
             g.close()
-        return res, diag
-    op = KinshipOperator(g, None if keep is None else keep_arr, variants)
-    eng = LmmEngine()
-    diag = _prepare_with_fallback(eng, y, X, op, rank, oversample, seed, trace_threshold,
-                                  min_rank, precision, no_fallback, error_tol)
-    res = eng.scan(g, keep_arr, min_maf=min_maf, precision=precision)
-    op.close()
-    eng.close()
-    if genotypes is None:
-        g.close()
-    return res, diag
+
+
+class GwasLmmOptions(C.Structure):
+    _fields_ = [
+        ("bfile", C.c_char_p), ("out", C.c_char_p), ("pheno", C.c_char_p), ("mpheno", C.c_int32),
+        ("qcovar", C.c_char_p), ("covar", C.c_char_p), ("missing_code", C.c_double),
+        ("run", LmmRunOptions), ("out_gz", C.c_int32), ("out_ssf", C.c_int32),
+        ("created", C.c_char_p),
+    ]
+
+
+def gwas_lmm_files(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcovar: str = None,
+                   covar: str = None, rank=256, oversample=10, seed=42, trace_threshold=0.95,
+                   min_rank=1, min_maf=0.01, precision="mixed", loco=True, out_gz=False,
+                   out_ssf=False, created=None, no_fallback=True, error_tol=1.0):
+    """The whole `gwas --model lmm --fastlmm --fastlmm-matrix-free` run from files to files in
+    the library's C++ (cs_run_gwas_lmm): inputs, null model(s), scan and every result file.
+    Returns (kept samples, null models)."""
+    o = GwasLmmOptions()
+    _abi.lib().cs_gwas_lmm_default_options(C.byref(o))
+    enc = lambda v: None if v is None else str(v).encode()
+    o.bfile, o.out, o.pheno, o.mpheno = enc(bfile), enc(out), enc(pheno), int(mpheno)
+    o.qcovar, o.covar, o.created = enc(qcovar), enc(covar), enc(created)
+    o.run = _run_options(rank, oversample, seed, trace_threshold, min_rank, min_maf, precision,
+                         loco, no_fallback, error_tol)
+    o.out_gz, o.out_ssf = int(bool(out_gz)), int(bool(out_ssf))
+    nk, ns = C.c_int64(), C.c_int32()
+    _check(_abi.lib().cs_run_gwas_lmm(C.byref(o), C.byref(nk), C.byref(ns)))
+    return nk.value, ns.value
 
 
 def _chromosome_runs(chrom, c):
@@ -1338,63 +1457,3 @@ def run_gwas_lmm(bfile: str, out: str, pheno: str = None, mpheno: int = 1, qcova
     return res, diag, inputs
 
 
-def _prepare_with_fallback(eng, y, X, op, rank, oversample, seed, trace_threshold, min_rank,
-                           precision, no_fallback, error_tol):
-    """The low-rank null of src/gwas_scanner.cpp:318-383: the sketch with trace-fraction rank
-    selection; the run falls back ("trace_threshold" when the threshold is not met, unless
-    --fastlmm-no-fallback; "error_tolerance" when the relative Frobenius error exceeds
-    --lmm-low-rank-error-tol) to MatrixFreeVce, i.e. the same sketch at the fixed requested
-    rank with no rank selection (src/matrix_free_vce.cpp:32-123, 137-236).  The diagnostics of
-    the first sketch are returned with the fallback label, as the reference writes them."""
-    rank_eff = max(1, min(rank, op.rows() - 1))
-    diag = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
-                                        seed=seed, trace_threshold=trace_threshold,
-                                        min_rank=min_rank, precision=precision)
-    accepted = diag["relative_frobenius_error"] <= error_tol
-    fallback = "none"
-    if not diag["trace_threshold_met"]:
-        if not no_fallback:
-            accepted = False
-            fallback = "trace_threshold"
-    elif not accepted:
-        fallback = "error_tolerance"
-    diag = dict(diag, fallback=fallback)
-    if not accepted:
-        refit = eng.prepareLowRankMatrixFree(y, X, op, rank=rank_eff, oversample=oversample,
-                                             seed=seed, trace_threshold=0.0, min_rank=min_rank,
-                                             precision=precision)
-        for key in ("sigma2_g", "sigma2_e", "delta", "log_eta", "reml_objective"):
-            diag[key] = refit[key]
-        eng.diagnostics = diag
-    return diag
-
-
-def _run_loco(g, keep, keep_arr, variants, chrom, y, X, rank, oversample, seed,
-              trace_threshold, min_rank, min_maf, precision, no_fallback=True, error_tol=1.0):
-    m = g.n_snps
-    out = {k: np.full(m, np.nan) for k in ("beta", "se", "p", "log10p", "freq")}
-    out["tested"] = np.zeros(m, dtype=bool)
-    diags = {}
-    var_chrom = chrom[variants]
-    for c in sort_chrom_labels(chrom):
-        loco_variants = variants[var_chrom != c]
-        if len(loco_variants) == 0:
-            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT,
-                                  "Matrix-free LOCO left no GRM variants for chromosome " + c)
-        op = KinshipOperator(g, None if keep is None else keep_arr, loco_variants)
-        eng = LmmEngine()
-        diags[c] = _prepare_with_fallback(eng, y, X, op, rank, oversample, seed,
-                                          trace_threshold, min_rank, precision, no_fallback,
-                                          error_tol)
-        idx = np.flatnonzero(chrom == c)
-        # the chromosome's SNPs as contiguous runs of the .bim order
-        breaks = np.flatnonzero(np.diff(idx) != 1)
-        starts = np.r_[idx[0], idx[breaks + 1]]
-        ends = np.r_[idx[breaks] + 1, idx[-1] + 1]
-        for b, e in zip(starts, ends):
-            r = eng.scan_window(g, keep_arr, int(b), int(e), min_maf=min_maf, precision=precision)
-            for k in ("beta", "se", "p", "log10p", "freq", "tested"):
-                out[k][b:e] = r[k]
-        op.close()
-        eng.close()
-    return out, diags

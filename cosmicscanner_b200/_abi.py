@@ -36,6 +36,10 @@ _SIGNATURES = {
     "cs_kinship_apply": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
     "cs_kinship_apply_host": ([_P, _P, _I64, _I64, _P, _I64, _I], _I),
     "cs_kinship_apply_noalloc": ([_P, _P, _I64, _I64, _P, _I64, _P], _I),
+    "cs_genotype_multiply_zt": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
+    "cs_genotype_multiply_z": ([_P, _P, _I64, _I64, _P, _I64, _I, _P], _I),
+    "cs_genotype_multiply_zt_host": ([_P, _P, _I64, _I64, _P, _I64, _I], _I),
+    "cs_genotype_multiply_z_host": ([_P, _P, _I64, _I64, _P, _I64, _I], _I),
     "cs_kinship_trace": ([_P, _P], _I),
     "cs_kinship_diagonal": ([_P, _P], _I),
     "cs_kinship_destroy": ([_P], None),
@@ -68,7 +72,14 @@ _SIGNATURES = {
     "cs_lmm_scan_window": ([_P, _P, _P, _I64, _I64, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_lmm_destroy": ([_P], None),
     "cs_normal_matrix": ([C.c_uint64, _I64, _I64, _P], _I),
+    "cs_lmm_run_default_options": ([_P], None),
+    "cs_run_lmm_matrix_free": ([_P, _P, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                _I, _P], _I),
+    "cs_gwas_lmm_default_options": ([_P], None),
+    "cs_run_gwas_lmm": ([_P, _P, _P], _I),
     "cs_pcg_solve": ([_P, _D, _D, _D, _P, _I64, _I64, _P, _I64, _D, _I, _I, _I, _P, _P], _I),
+    "cs_pcg_solve_records": ([_P, _D, _P, _I64, _I, _D, _D, _D, _P, _I64, _I64, _P, _I64, _D, _I,
+                              _I, _I, _P, _P], _I),
     "cs_vce_default_options": ([_P], None),
     "cs_vce_create": ([_P], _I),
     "cs_vce_solve_stcg": ([_P, _P, _D, _P, _I64, _I, _P, _P, _I64, _P, _P], _I),

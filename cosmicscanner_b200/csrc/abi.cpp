@@ -61,6 +61,15 @@ void vce_history(const cs_vce* v, double* out, int64_t* n_iter);
 void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, const double* B,
                       int64_t ldb, int64_t k, double* X, int64_t ldx, double tol, int relative,
                       int max_iter, int precision, int32_t* iterations, cudaStream_t s);
+void pcg_solve_records_public(cs_kinship* op, double divisor, const int32_t* rec_to_row,
+                              int64_t n_rec, bool with_pe, double sg2, double spe2, double se2,
+                              const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx,
+                              double tol, int relative, int max_iter, int precision,
+                              int32_t* iterations, cudaStream_t s);
+void genotype_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                          int64_t ldu, int precision, cudaStream_t s);
+void genotype_multiply_z(cs_kinship* op, const double* V, int64_t ldv, int64_t k, double* Y,
+                         int64_t ldy, int precision, cudaStream_t s);
 void stcg_scan(const cs_genotypes* g, const double* G, int64_t q, const int32_t* subject_rows,
                const int32_t* obs_to_subject, int64_t n_obs, const double* y, const double* X,
                int64_t p, double vg, double vpe, double ve, double min_maf, int64_t snp_begin,
@@ -128,6 +137,10 @@ void require(bool ok, const char* msg) {
     if (!ok) cs::fail(CS_ERR_INVALID_ARGUMENT, msg);
 }
 }  // namespace
+
+namespace cs {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace cs
 
 extern "C" {
 
@@ -227,6 +240,58 @@ int cs_kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64
     return guarded([&] {
         require(op != nullptr, "null kinship handle");
         cs::kinship_apply_noalloc(op, X, ldx, k, Y, ldy, (cudaStream_t)stream);
+    });
+}
+
+int cs_genotype_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                            int64_t ldu, int precision, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        cs::genotype_multiply_zt(op, X, ldx, k, U, ldu, precision, (cudaStream_t)stream);
+    });
+}
+
+int cs_genotype_multiply_z(cs_kinship* op, const double* V, int64_t ldv, int64_t k, double* Y,
+                           int64_t ldy, int precision, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        cs::genotype_multiply_z(op, V, ldv, k, Y, ldy, precision, (cudaStream_t)stream);
+    });
+}
+
+int cs_genotype_multiply_zt_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k,
+                                 double* U, int64_t ldu, int precision) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        if (k < 0) cs::fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+        if (ldx < op->rows || ldu < op->num_variants)
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Zt_v");
+        if (k == 0) return;
+        const int64_t n = op->rows, nv = op->num_variants;
+        cs::DeviceBuffer<double> dx, du;
+        dx.resize(n * k);
+        du.resize(nv * k);
+        CS_CUDA(cudaMemcpy2D(dx.get(), n * 8, X, ldx * 8, n * 8, k, cudaMemcpyHostToDevice));
+        cs::genotype_multiply_zt(op, dx.get(), n, k, du.get(), nv, precision, 0);
+        CS_CUDA(cudaMemcpy2D(U, ldu * 8, du.get(), nv * 8, nv * 8, k, cudaMemcpyDeviceToHost));
+    });
+}
+
+int cs_genotype_multiply_z_host(cs_kinship* op, const double* V, int64_t ldv, int64_t k,
+                                double* Y, int64_t ldy, int precision) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        if (k < 0) cs::fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+        if (ldv < op->num_variants || ldy < op->rows)
+            cs::fail(CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Z_v");
+        if (k == 0) return;
+        const int64_t n = op->rows, nv = op->num_variants;
+        cs::DeviceBuffer<double> dv, dy;
+        dv.resize(nv * k);
+        dy.resize(n * k);
+        CS_CUDA(cudaMemcpy2D(dv.get(), nv * 8, V, ldv * 8, nv * 8, k, cudaMemcpyHostToDevice));
+        cs::genotype_multiply_z(op, dv.get(), nv, k, dy.get(), n, precision, 0);
+        CS_CUDA(cudaMemcpy2D(Y, ldy * 8, dy.get(), n * 8, n * 8, k, cudaMemcpyDeviceToHost));
     });
 }
 
@@ -451,6 +516,21 @@ int cs_pcg_solve(cs_kinship* op, double kinship_divisor, double sigma2_g, double
         require(k == 0 || (B != nullptr && X != nullptr), "null argument");
         cs::pcg_solve_public(op, kinship_divisor, sigma2_g, sigma2_e, B, ldb, k, X, ldx, tol,
                              relative, max_iter, precision, iterations, (cudaStream_t)stream);
+    });
+}
+
+int cs_pcg_solve_records(cs_kinship* op, double kinship_divisor, const int32_t* rec_to_row,
+                         int64_t n_records, int with_pe, double sigma2_g, double sigma2_pe,
+                         double sigma2_e, const double* B, int64_t ldb, int64_t k, double* X,
+                         int64_t ldx, double tol, int relative, int max_iter, int precision,
+                         int32_t* iterations, void* stream) {
+    return guarded([&] {
+        require(op != nullptr, "null kinship handle");
+        require(k == 0 || (B != nullptr && X != nullptr), "null argument");
+        cs::pcg_solve_records_public(op, kinship_divisor, rec_to_row, n_records, with_pe != 0,
+                                     sigma2_g, sigma2_pe, sigma2_e, B, ldb, k, X, ldx, tol,
+                                     relative, max_iter, precision, iterations,
+                                     (cudaStream_t)stream);
     });
 }
 

@@ -22,6 +22,9 @@ struct Error : std::runtime_error {
 
 [[noreturn]] inline void fail(int code, const std::string& msg) { throw Error(code, msg); }
 
+// The calling thread's message for cs_last_error() (abi.cpp).
+void set_last_error(const std::string& msg);
+
 inline void check_cuda(cudaError_t e, const char* what) {
     if (e != cudaSuccess) fail(CS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
@@ -148,6 +151,8 @@ struct cs_kinship {
     int64_t n_active = 0;                  // rows of `view` (selected variants with 1/sd != 0)
     std::vector<double> mean, inv_std;     // per view row
     std::vector<int32_t> view_snp;         // per view row: its SNP (row of the .bed)
+    std::vector<int32_t> view_pos;         // per view row: its position among the selected variants
+    cs::DeviceBuffer<int32_t> d_view_pos;
     bool keep_identity = false;            // every sample, in .fam order
     std::vector<int32_t> counts;           // per view row: counts of codes 00,01,10,11
     cs::DeviceBuffer<double> d_lut;        // per view row: {(2-mu)s, 0, (1-mu)s, -mu s}
@@ -172,6 +177,12 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
 // The rows-pass output of the last mixed apply: W (R x k, column-major, ld R) with
 // W[t, c] = s_t^2 sum_i (G_ti - mu_t)[observed] x_ic; nullptr before any mixed apply.
 const double* mixed_rows_output(const cs_kinship* op, int64_t* R, int64_t* k);
+// GenotypeMatrix half-passes on tensor cores over the view rows: U (R x k, row-major) = Z^T X,
+// and Y (rows x k, row-major) = Z V given W = s o V column-major (R x k).
+void mixed_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                       int64_t ldu, cudaStream_t s);
+void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, int64_t ldy,
+                      cudaStream_t s);
 
 // The reference's Gaussian test matrix (std::normal_distribution over std::mt19937_64) on the
 // device, written row-major n x ld (omega.cu).
@@ -265,6 +276,12 @@ void lmm_prepare_lowrank_target(cs_lmm* l, const LowRankTarget& target, const do
                                 cs_lowrank_diagnostics* diag, cudaStream_t s);
 void lmm_fit_reml(cs_lmm* l, const double* y, const double* X, int64_t p,
                   cs_lowrank_diagnostics* diag, cudaStream_t s);
+// The last sketch's basis: selected rank, U (n x rank, row-major, device), its eigenvalues
+// (largest first) and the tail-mean residual eigenvalue.
+int64_t lmm_rank(const cs_lmm* l);
+const double* lmm_basis_device(const cs_lmm* l);
+std::vector<double> lmm_eigenvalues(const cs_lmm* l);
+double lmm_residual_eigenvalue(const cs_lmm* l);
 // Scan of SNPs [snp_begin, snp_end) of g; per-SNP outputs have snp_end - snp_begin entries.
 void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
                      int64_t snp_begin, int64_t snp_end, double min_maf, int precision,

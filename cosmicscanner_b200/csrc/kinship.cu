@@ -65,11 +65,15 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
             op->inv_std = g->inv_std;
             op->view_snp.resize(M);
             for (int64_t t = 0; t < M; ++t) op->view_snp[t] = (int32_t)t;
+            op->view_pos = op->view_snp;
         } else {
             active.reserve(op->num_variants);
             for (int64_t t = 0; t < op->num_variants; ++t) {
                 const int32_t j = variants ? variants[t] : (int32_t)t;
-                if (g->inv_std[j] != 0.0) active.push_back(j);
+                if (g->inv_std[j] != 0.0) {
+                    active.push_back(j);
+                    op->view_pos.push_back((int32_t)t);
+                }
             }
             op->n_active = (int64_t)active.size();
             const int64_t stride = round_up((op->rows + 3) / 4, kRowAlign);
@@ -127,6 +131,10 @@ cs_kinship* kinship_create(const cs_genotypes* g, const int32_t* keep, int64_t n
                      op->counts[4 * t + 3] * lut_sq[4 * t + 3];
         }
         op->trace = total / (double)op->num_variants;
+        op->d_view_pos.resize(std::max<int64_t>(1, R));
+        if (R)
+            CS_CUDA(cudaMemcpy(op->d_view_pos.get(), op->view_pos.data(), 4 * R,
+                               cudaMemcpyHostToDevice));
         op->d_lut.resize(std::max<int64_t>(1, 4 * R));
         op->d_lut_sq.resize(std::max<int64_t>(1, 4 * R));
         op->d_mean.resize(std::max<int64_t>(1, R));
@@ -229,6 +237,121 @@ void kinship_apply_colmajor(cs_kinship* op, const double* X, int64_t ldx, int64_
     op->buf_y.resize(n * k);
     colmajor_to_rowmajor(X, ldx, n, k, op->buf_x.get(), k, s);
     kinship_apply_rowmajor(op, op->buf_x.get(), k, k, op->buf_y.get(), k, precision, s);
+    rowmajor_to_colmajor(op->buf_y.get(), k, n, k, Y, ldy, s);
+}
+
+// ---------------------------------------------------------------- GenotypeMatrix half-passes
+// PlinkReader::multiply_Zt_v / multiply_Z_v (libCosmicCore/src/plink_reader.cpp:241-438, the
+// GenotypeMatrix interface of libCosmicCore/src/matrix_adapter.h:40-53) over the operator's
+// selection: Z is rows() x numVariants(), standardised with the all-sample statistics, missing
+// calls 0, variants with 1/sd == 0 all zero; no 1/M scaling.
+
+// out[pos[t] * ldo + c] = in[t * ldi + c] (view row t -> its selection position), c < k.
+__global__ void k_scatter_rows(const double* __restrict__ in, int64_t ldi, int64_t R, int64_t k,
+                               const int32_t* __restrict__ pos, double* __restrict__ out,
+                               int64_t ldo) {
+    const int64_t total = R * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t t = idx / k, c = idx - t * k;
+        out[(int64_t)pos[t] * ldo + c] = in[t * ldi + c];
+    }
+}
+
+// FP64 operand: W[t * k + c] = V[pos[t] * ldv + c]; tensor-core operand (column-major,
+// s-scaled): W[c * R + t] = s_t V[pos[t] * ldv + c].
+__global__ void k_gather_rows(const double* __restrict__ V, int64_t ldv, int64_t R, int64_t k,
+                              const int32_t* __restrict__ pos, const double* __restrict__ s_row,
+                              double* __restrict__ W, int colmajor) {
+    const int64_t total = R * k;
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        if (colmajor) {
+            const int64_t c = idx / R, t = idx - c * R;
+            W[idx] = s_row[t] * V[(int64_t)pos[t] * ldv + c];
+        } else {
+            const int64_t t = idx / k, c = idx - t * k;
+            W[idx] = V[(int64_t)pos[t] * ldv + c];
+        }
+    }
+}
+
+static unsigned grid_for(int64_t work) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 32LL * num_sms()));
+}
+
+// U (numVariants x k, row-major ldu) = Z^T X for X (rows x k, row-major ldx).
+void genotype_multiply_zt_rowmajor(cs_kinship* op, const double* X, int64_t ldx, int64_t k,
+                                   double* U, int64_t ldu, int precision, cudaStream_t s) {
+    const int64_t R = op->n_active, nv = op->num_variants;
+    CS_CUDA(cudaMemset2DAsync(U, ldu * 8, 0, k * 8, nv, s));
+    if (R == 0 || k == 0) return;
+    op->buf_u.resize(R * k);
+    if (precision == CS_PRECISION_MIXED)
+        mixed_multiply_zt(op, X, ldx, k, op->buf_u.get(), k, s);
+    else if (precision == CS_PRECISION_FP64)
+        decode_gemm_rows_fp64(op->view, op->d_lut.get(), X, ldx, k, op->buf_u.get(), k, op->ws, s);
+    else
+        fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    prof::Scope ps("scatter_rows", s, 0.0, 16.0 * R * k);
+    k_scatter_rows<<<grid_for(R * k), 256, 0, s>>>(op->buf_u.get(), k, R, k, op->d_view_pos.get(),
+                                                   U, ldu);
+    CS_LAUNCH("scatter_rows");
+}
+
+// Y (rows x k, row-major ldy) = Z V for V (numVariants x k, row-major ldv).
+void genotype_multiply_z_rowmajor(cs_kinship* op, const double* V, int64_t ldv, int64_t k,
+                                  double* Y, int64_t ldy, int precision, cudaStream_t s) {
+    const int64_t R = op->n_active;
+    if (k == 0) return;
+    if (R == 0) {
+        CS_CUDA(cudaMemset2DAsync(Y, ldy * 8, 0, k * 8, op->rows, s));
+        return;
+    }
+    if (precision != CS_PRECISION_MIXED && precision != CS_PRECISION_FP64)
+        fail(CS_ERR_INVALID_ARGUMENT, "unknown precision mode");
+    const bool mixed = precision == CS_PRECISION_MIXED;
+    op->buf_u.resize(R * k);
+    {
+        prof::Scope ps("gather_rows", s, 0.0, 16.0 * R * k);
+        k_gather_rows<<<grid_for(R * k), 256, 0, s>>>(V, ldv, R, k, op->d_view_pos.get(),
+                                                      op->d_inv_std.get(), op->buf_u.get(),
+                                                      mixed ? 1 : 0);
+        CS_LAUNCH("gather_rows");
+    }
+    if (mixed)
+        mixed_multiply_z(op, op->buf_u.get(), k, Y, ldy, s);
+    else
+        decode_gemm_samples_fp64(op->view, op->d_lut.get(), op->buf_u.get(), k, k, Y, ldy, 1.0,
+                                 op->ws, s);
+}
+
+// Column-major public forms (device pointers): transposes around the row-major passes.
+void genotype_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                          int64_t ldu, int precision, cudaStream_t s) {
+    if (k < 0) fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+    if (ldx < op->rows || ldu < op->num_variants)
+        fail(CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Zt_v");
+    if (k == 0) return;
+    const int64_t n = op->rows, nv = op->num_variants;
+    op->buf_x.resize(n * k);
+    op->buf_y.resize(nv * k);
+    colmajor_to_rowmajor(X, ldx, n, k, op->buf_x.get(), k, s);
+    genotype_multiply_zt_rowmajor(op, op->buf_x.get(), k, k, op->buf_y.get(), k, precision, s);
+    rowmajor_to_colmajor(op->buf_y.get(), k, nv, k, U, ldu, s);
+}
+
+void genotype_multiply_z(cs_kinship* op, const double* V, int64_t ldv, int64_t k, double* Y,
+                         int64_t ldy, int precision, cudaStream_t s) {
+    if (k < 0) fail(CS_ERR_INVALID_ARGUMENT, "negative column count");
+    if (ldv < op->num_variants || ldy < op->rows)
+        fail(CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Z_v");
+    if (k == 0) return;
+    const int64_t n = op->rows, nv = op->num_variants;
+    op->buf_x.resize(nv * k);
+    op->buf_y.resize(n * k);
+    colmajor_to_rowmajor(V, ldv, nv, k, op->buf_x.get(), k, s);
+    genotype_multiply_z_rowmajor(op, op->buf_x.get(), k, k, op->buf_y.get(), k, precision, s);
     rowmajor_to_colmajor(op->buf_y.get(), k, n, k, Y, ldy, s);
 }
 

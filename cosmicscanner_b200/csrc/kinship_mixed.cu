@@ -1167,6 +1167,78 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     m->last_k = k;
 }
 
+// Column maxima of |W| and |mu o W| for a column-major R x k W (the samples-pass operand
+// scales): atomicMax on the bits of non-negative doubles (order independent).
+__global__ void __launch_bounds__(256)
+k_col_absmax(const double* __restrict__ W, int64_t R, int64_t k, const double* __restrict__ mu,
+             unsigned long long* __restrict__ max_w, unsigned long long* __restrict__ max_muw) {
+    __shared__ double red_w[8], red_m[8];
+    const int64_t c = blockIdx.y;
+    double mw = 0.0, mm = 0.0;
+    const int64_t t0 = (int64_t)blockIdx.x * 2048;
+    for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) {
+        const double v = W[c * R + t];
+        mw = fmax(mw, fabs(v));
+        mm = fmax(mm, fabs(mu[t] * v));
+    }
+    for (int off = 16; off; off >>= 1) {
+        mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
+        mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red_w[threadIdx.x >> 5] = mw;
+        red_m[threadIdx.x >> 5] = mm;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < 8; ++j) {
+            mw = fmax(mw, red_w[j]);
+            mm = fmax(mm, red_m[j]);
+        }
+        atomicMax(max_w + c, (unsigned long long)__double_as_longlong(mw));
+        atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(mm));
+    }
+}
+
+// GenotypeMatrix::multiply_Zt_v on tensor cores: U (R x k, row-major ldu) = Z^T X over the
+// operator's view rows, X (rows x k, row-major ldx).
+void mixed_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                       int64_t ldu, cudaStream_t s) {
+    if (k <= 0 || op->n_active == 0) return;
+    MixedOperator* m = mixed_for(op);
+    m->last_k = 0;
+    rows_pass(m->rows, m->ws, X, ldx, k, U, ldu, false, 1, false, s);
+    check_status(m->ws, s);
+}
+
+// GenotypeMatrix::multiply_Z_v on tensor cores: Y (rows x k, row-major ldy) = Z V with
+// W = s o V over the view rows given column-major (R x k, leading dimension R).
+void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, int64_t ldy,
+                      cudaStream_t s) {
+    if (k <= 0) return;
+    const int64_t R = op->n_active;
+    MixedOperator* m = mixed_for(op);
+    m->last_k = 0;
+    MixedWorkspace& ws = m->ws;
+    ws.max_w.resize(k);
+    ws.max_muw.resize(k);
+    if (!ws.status.get()) {
+        ws.status.resize(1);
+        CS_CUDA(cudaMemsetAsync(ws.status.get(), 0, sizeof(int), s));
+    }
+    CS_CUDA(cudaMemsetAsync(ws.max_w.get(), 0, 8 * k, s));
+    CS_CUDA(cudaMemsetAsync(ws.max_muw.get(), 0, 8 * k, s));
+    {
+        prof::Scope ps("mixed_col_absmax", s, 0.0, 8.0 * R * k);
+        dim3 g((unsigned)((R + 2047) / 2048), (unsigned)k);
+        k_col_absmax<<<g, 256, 0, s>>>(Wcol, R, k, m->rows.mu.get(), ws.max_w.get(),
+                                       ws.max_muw.get());
+        CS_LAUNCH("col_absmax");
+    }
+    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s);
+    check_status(ws, s);
+}
+
 const double* mixed_rows_output(const cs_kinship* op, int64_t* R, int64_t* k) {
     if (!op->mixed || op->mixed->last_k == 0) return nullptr;
     *R = op->n_active;

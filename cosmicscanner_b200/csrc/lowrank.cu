@@ -994,6 +994,11 @@ void lmm_fit_reml(cs_lmm* l, const double* y, const double* X, int64_t p,
     }
 }
 
+int64_t lmm_rank(const cs_lmm* l) { return l->rank; }
+const double* lmm_basis_device(const cs_lmm* l) { return l->d_U.get(); }
+std::vector<double> lmm_eigenvalues(const cs_lmm* l) { return l->lambda; }
+double lmm_residual_eigenvalue(const cs_lmm* l) { return l->r0; }
+
 void lmm_lowrank_basis(const cs_lmm* l, double* U, int64_t ldu, double* lambda) {
     if (!l->prepared) fail(CS_ERR_INVALID_ARGUMENT, "low-rank model not prepared");
     const int64_t n = l->n, r = l->rank;

@@ -113,6 +113,17 @@ __global__ void k_beta(const double* __restrict__ part_rr, const double* __restr
     rsold[c] = b;
 }
 
+// p = z + beta p
+__global__ void k_direction_z(double* __restrict__ P, const double* __restrict__ Z, int64_t ld,
+                              int64_t n, int64_t k, const double* __restrict__ beta) {
+    const int64_t total = n * k;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / k, c = e - r * k;
+        P[r * ld + c] = Z[r * ld + c] + beta[c] * P[r * ld + c];
+    }
+}
+
 // p = r / diag + beta p
 __global__ void k_direction(double* __restrict__ P, const double* __restrict__ R, int64_t ld,
                             int64_t n, int64_t k, double diag, const double* __restrict__ beta) {
@@ -344,10 +355,41 @@ void column_dots(const double* A, int64_t lda, const double* B, int64_t ldb, int
     CS_CUDA(cudaStreamSynchronize(s));
 }
 
+// ---------------------------------------------------------------- low-rank preconditioner
+void LowRankPreconditioner::set_components(double vg, double ve, cudaStream_t s) {
+    base = 1.0 / std::max(1e-300, vg * r0 + ve);
+    std::vector<double> h(std::max<int64_t>(1, r));
+    for (int64_t j = 0; j < r; ++j) h[j] = 1.0 / (vg * lambda[j] + ve) - base;
+    c.resize(std::max<int64_t>(1, r));
+    CS_CUDA(cudaMemcpyAsync(c.get(), h.data(), 8 * r, cudaMemcpyHostToDevice, s));
+    CS_CUDA(cudaStreamSynchronize(s));  // h is a local
+}
+
+void LowRankPreconditioner::apply(const double* R, int64_t ldr, int64_t k, double* Z, int64_t ldz,
+                                  cudaStream_t s) {
+    if (k <= 0) return;
+    cublasHandle_t blas = shared_blas();
+    CS_BLAS(cublasSetStream(blas, s));
+    T.resize(std::max<int64_t>(1, r * k));
+    prof::Scope ps("lowrank_precondition", s, 4.0 * (double)n * r * k, 8.0 * (2.0 * n * k + n * r));
+    // column-major views: R^T (k x n, ld ldr), U^T (r x n, ld r)
+    const double one = 1.0, zero = 0.0;
+    // T^T (k x r) = R^T U
+    CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, (int)k, (int)r, (int)n, &one, R, (int)ldr,
+                        U.get(), (int)r, &zero, T.get(), (int)k));
+    // T^T[:, j] *= c_j
+    CS_BLAS(cublasDdgmm(blas, CUBLAS_SIDE_RIGHT, (int)k, (int)r, T.get(), (int)k, c.get(), 1,
+                        T.get(), (int)k));
+    // Z^T = base R^T + T^T U^T
+    CS_CUDA(cudaMemcpy2DAsync(Z, 8 * ldz, R, 8 * ldr, 8 * k, n, cudaMemcpyDeviceToDevice, s));
+    CS_BLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)k, (int)n, (int)r, &one, T.get(),
+                        (int)k, U.get(), (int)r, &base, Z, (int)ldz));
+}
+
 // ---------------------------------------------------------------- block PCG
 void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, int64_t k,
                      double* X, int64_t ldx, double tol, bool relative, int max_iter,
-                     PcgWorkspace& ws, PcgStats& st, cudaStream_t s) {
+                     PcgWorkspace& ws, PcgStats& st, cudaStream_t s, LowRankPreconditioner* M) {
     st.iterations.assign(k, 0);
     if (k <= 0) return;
     const int64_t n = A.rm->n_rec;
@@ -368,6 +410,10 @@ void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, in
     k_cg_init<<<grid_for(n * k), 256, 0, s>>>(B, ldb, ws.idx.get(), ws.R.get(), ws.P.get(), k, n, k,
                                               diag);
     CS_LAUNCH("cg_init");
+    if (M) {
+        ws.Zp.resize(n * k);
+        M->apply(ws.R.get(), k, k, ws.P.get(), k, s);  // p0 = z0 = M^-1 r0
+    }
     // ||b||^2 and rsold = r . z
     std::vector<double> rr(k), rs(k);
     column_dots(ws.R.get(), k, ws.R.get(), k, n, k, rr.data(), ws, s);
@@ -424,6 +470,13 @@ void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, in
                                                ws.R.get(), ka, n, ka, chunk, ws.alpha.get(), diag,
                                                ws.partial_a.get(), ws.partial_b.get());
             CS_LAUNCH("cg_update");
+            if (M) {
+                // z = M^-1 r and r . z in place of the scalar form's r . r / diag
+                M->apply(ws.R.get(), ka, ka, ws.Zp.get(), ka, s);
+                k_dot_partial<<<grid, block, 0, s>>>(ws.R.get(), ka, ws.Zp.get(), ka, n, ka, chunk,
+                                                     ws.partial_b.get());
+                CS_LAUNCH("cg_rz");
+            }
             k_beta<<<(unsigned)((ka + 127) / 128), 128, 0, s>>>(ws.partial_a.get(), ws.partial_b.get(),
                                                                 nb, ka, ws.rsold.get(), ws.beta.get(),
                                                                 ws.rr.get());
@@ -439,8 +492,12 @@ void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, in
         if (keep_pos.empty()) break;
         {
             prof::Scope ps("cg_direction", s, 2.0 * n * ka, 24.0 * n * ka);
-            k_direction<<<grid_for(n * ka), 256, 0, s>>>(ws.P.get(), ws.R.get(), ka, n, ka, diag,
-                                                         ws.beta.get());
+            if (M)
+                k_direction_z<<<grid_for(n * ka), 256, 0, s>>>(ws.P.get(), ws.Zp.get(), ka, n, ka,
+                                                               ws.beta.get());
+            else
+                k_direction<<<grid_for(n * ka), 256, 0, s>>>(ws.P.get(), ws.R.get(), ka, n, ka,
+                                                             diag, ws.beta.get());
             CS_LAUNCH("cg_direction");
         }
         if ((int64_t)keep_pos.size() < ka) {

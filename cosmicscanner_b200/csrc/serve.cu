@@ -18,6 +18,18 @@
 // request's columns never mix with another's: each output column depends only on its own
 // input column, so a result is the same alone and in the mix up to the order of FP64 slice
 // sums.
+//
+// Small cohorts.  Embedding costs the full operator's work (all N samples) for every column;
+// a request whose cohort is below `subset_fraction` of N instead gets its own operator over a
+// repacked copy of its samples (the same K_S: statistics and 1/M from the full matrix) and
+// runs its applies on its own stream, so its tensor work scales with its own sample count.
+// Whether a request is embedded or repacked depends only on its size, so it takes the same
+// path alone and in the mix.
+//
+// Admission.  Requests are admitted FIFO while a worker slot is free and their estimated
+// working set (sketch blocks, scan window and, for repacked requests, the packed copy and
+// its tensor-core operands) fits the memory budget: by default the device's free memory at
+// server creation less a 4 GB reserve.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -59,6 +71,7 @@ struct ApplyJob {
 
 struct Request {
     int64_t id = 0;
+    bool own_view = false;  // repacked subset operator instead of the shared full-space applies
     std::vector<int32_t> samples;
     std::vector<double> Y, X;  // column-major n x t, n x p
     int32_t t = 0, p = 0;
@@ -108,6 +121,8 @@ unsigned grid_for(int64_t total) {
 struct cs_server {
     const cs_genotypes* g = nullptr;
     cs_kinship* op = nullptr;
+    std::vector<int32_t> variants;  // the GRM selection (empty: every SNP)
+    int64_t budget_bytes = 0;
     std::vector<double> diag_full;
     cs_server_options opt{};
     int device = 0;
@@ -123,7 +138,7 @@ struct cs_server {
     std::thread gpu_thread, dispatch_thread;
     // statistics
     int64_t applies = 0, apply_cols = 0, submitted = 0, completed = 0, failed = 0;
-    int64_t max_jobs_per_apply = 0, max_active = 0;
+    int64_t max_jobs_per_apply = 0, max_active = 0, own_view_requests = 0;
     std::vector<double> latencies;
     double first_submit = -1.0, last_done = 0.0;
     cs::DeviceBuffer<double> xs, ys;
@@ -247,8 +262,7 @@ void cs_server::dispatch_loop() {
                 if (stop) return true;
                 if (queue.empty() || active >= opt.max_active) return false;
                 const Request* f = reqs[queue.front()].get();
-                const int64_t budget = (int64_t)(opt.memory_budget_gb * 1e9);
-                return active == 0 || mem_in_use + f->est_bytes <= budget;
+                return active == 0 || mem_in_use + f->est_bytes <= budget_bytes;
             });
             if (stop) break;
             r = reqs[queue.front()].get();
@@ -280,15 +294,33 @@ void cs_server::run_request(Request* r) {
         for (int32_t i : r->samples) tr += diag_full[i];
         target.trace = tr;
         const int32_t* rows = d_rows.get();
-        target.apply = [this, rows, n](const double* X, int64_t ldx, int64_t k, double* Y,
-                                       int64_t ldy, cudaStream_t s) {
-            apply(rows, n, X, ldx, k, Y, ldy, s);
-        };
+        std::unique_ptr<cs_kinship> sub;
+        if (r->own_view) {
+            sub.reset(cs::kinship_create(g, r->samples.data(), n,
+                                         variants.empty() ? nullptr : variants.data(),
+                                         (int64_t)variants.size()));
+            cs_kinship* so = sub.get();
+            const int prec = opt.precision;
+            target.apply = [so, prec](const double* X, int64_t ldx, int64_t k, double* Y,
+                                      int64_t ldy, cudaStream_t s) {
+                cs::kinship_apply_rowmajor(so, X, ldx, k, Y, ldy, prec, s);
+            };
+        } else {
+            target.apply = [this, rows, n](const double* X, int64_t ldx, int64_t k, double* Y,
+                                           int64_t ldy, cudaStream_t s) {
+                apply(rows, n, X, ldx, k, Y, ldy, s);
+            };
+        }
         cs_lmm* lmm = cs::lmm_create();
         struct Guard {
             cs_lmm* l;
             ~Guard() { cs::lmm_destroy(l); }
         } guard{lmm};
+        // destroyed first: on an error, the request's stream drains before its buffers go
+        struct SyncGuard {
+            cudaStream_t s;
+            ~SyncGuard() { cudaStreamSynchronize(s); }
+        } sync_guard{st};
         const int rank = std::max(1, std::min<int>(opt.rank, (int)n - 1));
         const int64_t W = r->end - r->begin;
         r->sigma2.assign(2 * r->t, 0.0);
@@ -349,9 +381,10 @@ void server_default_options(cs_server_options* o) {
     o->min_maf = 0.01;
     o->precision = CS_PRECISION_MIXED;
     o->max_batch_columns = 4096;
-    o->memory_budget_gb = 64.0;
+    o->memory_budget_gb = 0.0;
     o->max_active = 8;
     o->batch_window_ms = 0.0;
+    o->subset_fraction = 0.5;
 }
 
 cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t n_var,
@@ -362,11 +395,19 @@ cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t
         if (opt_in) sv->opt = *opt_in;
         else server_default_options(&sv->opt);
         if (sv->opt.max_batch_columns < 1 || sv->opt.max_active < 1 || sv->opt.rank < 1 ||
-            !(sv->opt.batch_window_ms >= 0.0))
+            !(sv->opt.batch_window_ms >= 0.0) || !(sv->opt.subset_fraction >= 0.0))
             fail(CS_ERR_INVALID_ARGUMENT, "bad server options");
         CS_CUDA(cudaGetDevice(&sv->device));
         sv->g = g;
         sv->op = kinship_create(g, nullptr, 0, variants, n_var);
+        if (variants && n_var > 0) sv->variants.assign(variants, variants + n_var);
+        if (sv->opt.memory_budget_gb > 0.0) {
+            sv->budget_bytes = (int64_t)(sv->opt.memory_budget_gb * 1e9);
+        } else {
+            size_t free_b = 0, total_b = 0;
+            CS_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            sv->budget_bytes = std::max<int64_t>(0, (int64_t)free_b - (int64_t)4e9);
+        }
         sv->diag_full.resize(sv->op->rows);
         kinship_diagonal(sv->op, sv->diag_full.data());
         sv->gpu_thread = std::thread([sv] { sv->gpu_loop(); });
@@ -404,12 +445,22 @@ int64_t server_submit(cs_server* sv, const cs_serve_request* q) {
     r->seed = q->seed;
     const int64_t sk = std::min<int64_t>(n, sv->opt.rank + sv->opt.oversample);
     const int64_t W = r->end - r->begin;
+    r->own_view = (double)n < sv->opt.subset_fraction * (double)N;
     r->est_bytes = 8 * n * sk * 4 + W * ((n + 3) / 4 + 64 + 8 * (sk + r->p + 2)) + 64 * n;
+    if (r->own_view) {
+        // the packed copy of the cohort's columns, the right-hand-side pieces of both passes
+        // and the FP64 slice partials of the tensor-core form
+        const int64_t rows = sv->op->num_variants, n_pad = round_up(n, 256);
+        const int64_t kp = round_up(sk + r->p + 1, 16);
+        r->est_bytes += rows * round_up((n + 3) / 4, kRowAlign) + 3 * kp * n_pad +
+                        6 * kp * round_up(rows, 256) + 8 * 8 * kp * std::max(n_pad, rows);
+    }
     std::lock_guard<std::mutex> lk(sv->mu);
     r->id = sv->next_id++;
     r->t_submit = now_s();
     if (sv->first_submit < 0) sv->first_submit = r->t_submit;
     const int64_t id = r->id;
+    if (r->own_view) ++sv->own_view_requests;
     sv->reqs[id] = std::move(r);
     sv->queue.push_back(id);
     ++sv->submitted;
@@ -484,6 +535,8 @@ void server_stats(cs_server* sv, cs_server_statistics* out) {
     out->apply_columns = sv->apply_cols;
     out->max_requests_per_apply = sv->max_jobs_per_apply;
     out->max_concurrent = sv->max_active;
+    out->own_view_requests = sv->own_view_requests;
+    out->memory_budget_gb = (double)sv->budget_bytes / 1e9;
     std::vector<double> l = sv->latencies;
     std::sort(l.begin(), l.end());
     auto pct = [&](double q) {

@@ -31,6 +31,7 @@ struct cs_vce {
     cs::RademacherStream probes, slq_rng;
     cs::DeviceBuffer<double> rhsA, solA, W, IN, DG, DP, rhsB, solB, Q, small, cm;
     cs::DeviceBuffer<double> lz, lw;  // Lanczos blocks
+    cs::LowRankPreconditioner precond;
     std::vector<double> beta, a_rows, pe_rows, hist;
     int64_t p = 0, n_rows = 0;
     bool solved = false;
@@ -185,6 +186,7 @@ void vce_default_options(cs_vce_options* o) {
     o->slq_steps = 15;
     o->probe_seed = 20250101ull;
     o->precision = CS_PRECISION_FP64;
+    o->precond_rank = 0;
 }
 
 cs_vce* vce_create() {
@@ -366,6 +368,46 @@ void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* re
     V.vg = vg_guess;
     V.vpe = V.with_pe ? pe_guess : 0.0;
 
+    // ---- optional low-rank deflation preconditioner (records one-to-one with rows)
+    cs::LowRankPreconditioner* M = nullptr;
+    if (opt.precond_rank > 0 && v->rm.identity) {
+        const int rank = (int)std::min<int64_t>(opt.precond_rank, std::max<int64_t>(1, n - 2));
+        prof::HostScope hs("stcg_precond_sketch");
+        cs_lmm* l = lmm_create();
+        try {
+            LowRankTarget t;
+            t.rows = n;
+            t.trace = op->trace;  // of Z Z^T / num_variants; eigenvalues scaled by fac below
+            const int prec = opt.precision;
+            t.apply = [op, prec](const double* X_, int64_t ldx, int64_t k, double* Y_, int64_t ldy,
+                                 cudaStream_t st2) {
+                kinship_apply_rowmajor(op, X_, ldx, k, Y_, ldy, prec, st2);
+            };
+            std::vector<double> Xc(std::max<int64_t>(1, n * p));
+            std::copy(X, X + n * p, Xc.begin());
+            lmm_prepare_lowrank_target(l, t, y, p > 0 ? Xc.data() : nullptr, p, rank, 10, 42, 0.0,
+                                       rank, nullptr, s);
+            cs::LowRankPreconditioner& P = v->precond;
+            P.n = n;
+            P.r = lmm_rank(l);
+            P.U.resize(n * P.r);
+            CS_CUDA(cudaMemcpyAsync(P.U.get(), lmm_basis_device(l), 8 * n * P.r,
+                                    cudaMemcpyDeviceToDevice, s));
+            P.lambda = lmm_eigenvalues(l);
+            for (double& x : P.lambda) x *= V.fac;
+            P.r0 = lmm_residual_eigenvalue(l) * V.fac;
+            CS_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            lmm_destroy(l);
+            throw;
+        }
+        lmm_destroy(l);
+        M = &v->precond;
+    }
+    auto set_precond = [&]() {
+        if (M) M->set_components(V.vg, V.ve + (V.with_pe ? V.vpe : 0.0), s);
+    };
+
     // ---- constant columns of the first block: [y | X | probes]
     v->rhsA.resize(n * kA);
     v->solA.resize(n * kA);
@@ -403,10 +445,11 @@ void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* re
     res->logl = std::numeric_limits<double>::quiet_NaN();
     for (int iter = 0; iter < opt.max_iter; ++iter) {
         const double diag = diag_of();
+        set_precond();
         // ---- block A: V^-1 [y | X | z]
         v->probes.draw(n, S, v->rhsA.get() + 1 + p, kA, s);
         pcg_solve_block(V, diag, v->rhsA.get(), kA, kA, v->solA.get(), kA, opt.pcg_tol,
-                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s);
+                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s, M);
         pcg_total += st.column_iterations;
         // X^T [V^-1 y | V^-1 X | V^-1 z]
         const std::vector<double> xts =
@@ -441,7 +484,7 @@ void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* re
         if (V.with_pe) copy_cols(v->DP.get(), kIn, n, 0, 1, v->rhsB.get(), kB, 1, s);
         copy_cols(v->W.get(), kIn, n, 0, 1, v->rhsB.get(), kB, kB - 1, s);
         pcg_solve_block(V, diag, v->rhsB.get(), kB, kB, v->solB.get(), kB, opt.pcg_tol,
-                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s);
+                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s, M);
         pcg_total += st.column_iterations;
         {
             const std::vector<double> xtb =
@@ -538,9 +581,10 @@ void vce_solve_stcg(cs_vce* v, cs_kinship* op, double divisor, const int32_t* re
     // ---- final BLUE / BLUP (stcg_vce.cpp:364-406)
     {
         const double diag = diag_of();
+        set_precond();
         const int64_t k0 = 1 + p;
         pcg_solve_block(V, diag, v->rhsA.get(), kA, k0, v->solA.get(), kA, opt.pcg_tol,
-                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s);
+                        opt.pcg_relative != 0, opt.pcg_max_iter, v->pw, st, s, M);
         pcg_total += st.column_iterations;
         const std::vector<double> xts =
             cross(v->blas, v->rhsA.get(), kA, 1, p, v->solA.get(), kA, 0, k0, n, v->small, s);
@@ -617,6 +661,42 @@ void pcg_solve_public(cs_kinship* op, double divisor, double sg2, double se2, co
     const double diag = std::max(se2, 1e-12) + std::max(sg2, 1e-12);
     pcg_solve_block(V, diag, b.get(), k, k, x.get(), k, tol, relative != 0, max_iter, ws, st, s);
     rowmajor_to_colmajor(x.get(), k, n, k, X, ldx, s);
+    CS_CUDA(cudaStreamSynchronize(s));
+    if (iterations) std::copy(st.iterations.begin(), st.iterations.end(), iterations);
+}
+
+// The record-level covariance of STCG_VCE (stcg_vce.cpp:80-126) behind MatrixFreePCG.
+void pcg_solve_records_public(cs_kinship* op, double divisor, const int32_t* rec_to_row,
+                              int64_t n_rec, bool with_pe, double sg2, double spe2, double se2,
+                              const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx,
+                              double tol, int relative, int max_iter, int precision,
+                              int32_t* iterations, cudaStream_t s) {
+    if (!rec_to_row) n_rec = op->rows;
+    if (k < 0 || n_rec <= 0 || ldb < n_rec || ldx < n_rec || max_iter < 1)
+        fail(CS_ERR_INVALID_ARGUMENT, "MatrixFreePCG: bad dimensions");
+    if (k == 0) return;
+    if (!(divisor > 0.0)) divisor = (double)op->num_variants;
+    RecordMap rm;
+    rm.build(rec_to_row, n_rec, op->rows);
+    VOperator V;
+    V.op = op;
+    V.rm = &rm;
+    V.fac = (double)op->num_variants / divisor;
+    V.vg = sg2;
+    V.vpe = with_pe ? spe2 : 0.0;
+    V.ve = se2;
+    V.with_pe = with_pe;
+    V.precision = precision;
+    PcgWorkspace ws;
+    PcgStats st;
+    DeviceBuffer<double> b, x;
+    b.resize(n_rec * k);
+    x.resize(n_rec * k);
+    colmajor_to_rowmajor(B, ldb, n_rec, k, b.get(), k, s);
+    double diag = std::max(se2, 1e-12) + std::max(sg2, 1e-12);
+    if (with_pe) diag += std::max(spe2, 1e-12);
+    pcg_solve_block(V, diag, b.get(), k, k, x.get(), k, tol, relative != 0, max_iter, ws, st, s);
+    rowmajor_to_colmajor(x.get(), k, n_rec, k, X, ldx, s);
     CS_CUDA(cudaStreamSynchronize(s));
     if (iterations) std::copy(st.iterations.begin(), st.iterations.end(), iterations);
 }

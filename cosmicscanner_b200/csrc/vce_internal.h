@@ -65,8 +65,26 @@ struct VOperator {
     const double* gather(const double* in, int64_t ldi, int64_t k, cudaStream_t s);
 };
 
+// Low-rank deflation preconditioner for V = vg K + ve I on single-record blocks: with the
+// top r eigenpairs (U, lambda) of K from a randomized sketch and the tail mean r0 standing in
+// for the rest of the spectrum, M = vg (U diag(lambda) U^T + r0 (I - U U^T)) + ve I and
+//   M^-1 = base I + U diag(c) U^T,  base = 1 / (vg r0 + ve),  c_j = 1 / (vg lambda_j + ve) - base
+// (the Woodbury form the low-rank LMM uses for V^-1, lmm_engine.cpp:1097-1105).  Applying it
+// to a k-column block is two GEMMs of n x r x k; it removes the few large eigenvalues that
+// population structure gives K, which set the iteration count of the scalar preconditioner.
+struct LowRankPreconditioner {
+    DeviceBuffer<double> U;       // n x r, row-major
+    std::vector<double> lambda;   // r eigenvalues of K
+    double r0 = 0.0, base = 0.0;
+    int64_t n = 0, r = 0;
+    DeviceBuffer<double> c, T;
+    void set_components(double vg, double ve, cudaStream_t s);
+    // Z (n x ldz, row-major) = M^-1 R (n x ldr), k columns; Z must not alias R.
+    void apply(const double* R, int64_t ldr, int64_t k, double* Z, int64_t ldz, cudaStream_t s);
+};
+
 struct PcgWorkspace {
-    DeviceBuffer<double> R, P, AP, T, partial_a, partial_b;
+    DeviceBuffer<double> R, P, AP, T, Zp, partial_a, partial_b;
     DeviceBuffer<double> alpha, beta, rsold, rr, rz;
     DeviceBuffer<int32_t> map, idx;
 };
@@ -81,9 +99,11 @@ struct PcgStats {
 // column runs its own CG recurrence with the scalar preconditioner 1/diag and stops when
 // ||r|| < tol (absolute; relative: tol * ||b||) or at max_iter.  Converged columns leave the
 // operator applies.  B, X: row-major (n_rec x ld).
+// With a preconditioner M, z = M^-1 r replaces r / diag.
 void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, int64_t k,
                      double* X, int64_t ldx, double tol, bool relative, int max_iter,
-                     PcgWorkspace& ws, PcgStats& st, cudaStream_t s);
+                     PcgWorkspace& ws, PcgStats& st, cudaStream_t s,
+                     LowRankPreconditioner* M = nullptr);
 
 // Column dot products of two row-major blocks: out[c] = sum_i A[i, c] * B[i, c] (host),
 // in a fixed summation order.

@@ -94,6 +94,21 @@ int cs_kinship_apply_host(cs_kinship* op, const double* X, int64_t ldx, int64_t 
  * cudaDeviceReset of that device (the array's address is looked up once).  Device pointers. */
 int cs_kinship_apply_noalloc(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* Y,
                              int64_t ldy, void* stream);
+/* GenotypeMatrix::multiply_Zt_v / multiply_Z_v (libCosmicCore/src/matrix_adapter.h:40-53, as
+ * PlinkReader implements them, plink_reader.cpp:241-438 with the keep-subset forms) over the
+ * operator's selection: Z is rows() x numVariants(), z = (dosage - mean) / sd with the
+ * all-sample statistics, missing calls 0, variants with 1/sd == 0 all zero, no 1/M scaling.
+ * multiply_zt: U (numVariants x k) = Z^T X for X (rows x k); multiply_z: Y (rows x k) = Z V for
+ * V (numVariants x k).  Column-major device pointers; precision as cs_kinship_apply.  The
+ * _host forms take host arrays and return when the result is there. */
+int cs_genotype_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
+                            int64_t ldu, int precision, void* stream);
+int cs_genotype_multiply_z(cs_kinship* op, const double* V, int64_t ldv, int64_t k, double* Y,
+                           int64_t ldy, int precision, void* stream);
+int cs_genotype_multiply_zt_host(cs_kinship* op, const double* X, int64_t ldx, int64_t k,
+                                 double* U, int64_t ldu, int precision);
+int cs_genotype_multiply_z_host(cs_kinship* op, const double* V, int64_t ldv, int64_t k,
+                                double* Y, int64_t ldy, int precision);
 /* trace() and getDiagonal() (kinship_operator.cpp:306-368); diag is a host array. */
 int cs_kinship_trace(const cs_kinship* op, double* trace);
 int cs_kinship_diagonal(cs_kinship* op, double* diag);
@@ -145,6 +160,62 @@ int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, 
                        double* beta, double* se, double* pvalue, double* log10p, double* freq,
                        int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
+
+/* ---------------------------------------------------------------- the whole job
+ * GwasScanner::runLocoScan's PLINK matrix-free branch (src/gwas_scanner.cpp:74-509) in the
+ * library's C++: GRM variant selection from the all-sample statistics (:258-277), one null
+ * model (or, when chrom spans more than one chromosome and loco is set, the
+ * leave-one-chromosome-out loop of :299-314, 464-472 in sort_chrom_labels order, :62-72), each
+ * with the low-rank fall-back rule of :347-383, then the scan of every SNP. */
+typedef struct cs_lmm_run_options {
+    int32_t rank;            /* --fastlmm-max-rank (256) */
+    int32_t oversample;      /* --lmm-low-rank-oversample (10) */
+    int64_t seed;            /* --lmm-low-rank-seed (42) */
+    double trace_threshold;  /* --fastlmm-trace-threshold (0.95) */
+    int32_t min_rank;        /* (1) */
+    double min_maf;          /* --maf (0.01): GRM selection and scan filter */
+    int32_t precision;       /* CS_PRECISION_MIXED (default) or CS_PRECISION_FP64 */
+    int32_t loco;            /* 1: leave one chromosome out when there are several (--no-loco: 0) */
+    int32_t no_fallback;     /* --fastlmm-no-fallback (1) */
+    double error_tol;        /* --lmm-low-rank-error-tol (1.0) */
+} cs_lmm_run_options;
+enum { CS_FALLBACK_NONE = 0, CS_FALLBACK_TRACE_THRESHOLD = 1, CS_FALLBACK_ERROR_TOLERANCE = 2 };
+typedef struct cs_lmm_run_scope {
+    char label[32];                 /* "GLOBAL" or the left-out chromosome */
+    cs_lowrank_diagnostics diag;    /* the first sketch's diagnostics, refit VCs on fall-back */
+    int32_t fallback;               /* CS_FALLBACK_* */
+} cs_lmm_run_scope;
+void cs_lmm_run_default_options(cs_lmm_run_options* opt);
+/* g resident; keep (NULL: every sample) lists the analysed samples in the order of y; X is
+ * n_keep x p column-major (FP32-rounded values where the caller mirrors the reference's
+ * MatrixXf covariates); chrom (NULL: one chromosome) holds each SNP's .bim label.  Per-SNP host
+ * outputs of g's SNP count (NaN / tested 0 where the reference writes no row); scopes receives
+ * up to max_scopes null models and n_scopes their number.  Host pointers. */
+int cs_run_lmm_matrix_free(const cs_genotypes* g, const int32_t* keep, int64_t n_keep,
+                           const double* y, const double* X, int64_t p, const char* const* chrom,
+                           const cs_lmm_run_options* opt, double* beta, double* se,
+                           double* pvalue, double* log10p, double* freq, int32_t* tested,
+                           cs_lmm_run_scope* scopes, int32_t max_scopes, int32_t* n_scopes);
+/* `cosmicscanner gwas --model lmm --fastlmm --fastlmm-matrix-free --bfile B --out O
+ * [--pheno P --mpheno k] [--qcovar Q] [--covar C]` from files to files: the .fam samples,
+ * phenotype (.fam column without --pheno), [1 | quantitative | categorical dummies] as
+ * float and the complete-sample keep list (src/models/univariate_model.cpp:389-426), the job
+ * above, then O.assoc.txt (rows chromosome by chromosome under LOCO; GWAS-SSF with out_ssf,
+ * gzip with out_gz), O.cosmic.sumstats, O.scan.meta.txt and O.low_rank.meta.tsv. */
+typedef struct cs_gwas_lmm_options {
+    const char* bfile;       /* PLINK prefix */
+    const char* out;         /* output prefix */
+    const char* pheno;       /* NULL: the .fam phenotype */
+    int32_t mpheno;          /* 1-based phenotype column (1) */
+    const char* qcovar;      /* quantitative covariates (NULL: none) */
+    const char* covar;       /* categorical covariates (NULL: none) */
+    double missing_code;     /* -9 */
+    cs_lmm_run_options run;
+    int32_t out_gz, out_ssf;
+    const char* created;     /* "# Created:" of .cosmic.sumstats (NULL: now, UTC) */
+} cs_gwas_lmm_options;
+void cs_gwas_lmm_default_options(cs_gwas_lmm_options* opt);
+int cs_run_gwas_lmm(const cs_gwas_lmm_options* opt, int64_t* n_kept, int32_t* n_scopes);
 
 /* ---------------------------------------------------------------- dense exact tier
  * The default `gwas --model lmm` route (src/gwas_scanner.cpp:131-215, 384-399; no LOCO):
@@ -279,6 +350,19 @@ int cs_pcg_solve(cs_kinship* op, double kinship_divisor, double sigma2_g, double
                  const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx, double tol,
                  int relative, int max_iter, int precision, int32_t* iterations, void* stream);
 
+/* MatrixFreePCG::solve (matrix_free_pcg.h:20-68) with the covariance STCG_VCE hands it
+ * (libCosmicCore/src/stcg_vce.cpp:80-126): V = sigma2_g Zr K Zr^T + sigma2_pe Zr Zr^T +
+ * sigma2_e I over n_records records, Zr mapping record i to operator row rec_to_row[i] (-1: no
+ * genotype row; NULL: record i is row i, n_records == rows()), K = Z Z^T / kinship_divisor, the
+ * permanent-environment term only with with_pe, the scalar preconditioner
+ * 1/(sigma2_g + [sigma2_pe] + sigma2_e).  B and X are device, column-major
+ * (n_records x k); stopping as cs_pcg_solve. */
+int cs_pcg_solve_records(cs_kinship* op, double kinship_divisor, const int32_t* rec_to_row,
+                         int64_t n_records, int with_pe, double sigma2_g, double sigma2_pe,
+                         double sigma2_e, const double* B, int64_t ldb, int64_t k, double* X,
+                         int64_t ldx, double tol, int relative, int max_iter, int precision,
+                         int32_t* iterations, void* stream);
+
 /* Options of the matrix-free AI-REML (VCEConfig, libCosmicCore/src/vce.h:139-160, as
  * src/models/repeatability_model.cpp:604-612 fills it). */
 typedef struct cs_vce_options {
@@ -292,6 +376,10 @@ typedef struct cs_vce_options {
     int32_t slq_steps;    /* Lanczos steps per SLQ probe (15) */
     uint64_t probe_seed;  /* mt19937_64 seed of the trace probes (20250101) */
     int32_t precision;    /* CS_PRECISION_FP64 or CS_PRECISION_MIXED for the kinship applies */
+    int32_t precond_rank; /* 0: the reference's scalar preconditioner 1/(sum of components);
+                             r > 0: low-rank deflation M^-1 = base I + U diag(c) U^T with the
+                             top r eigenpairs of K from a randomized sketch (records that map
+                             one-to-one onto operator rows only; otherwise the scalar one) */
 } cs_vce_options;
 
 typedef struct cs_vce_result {
@@ -375,10 +463,14 @@ typedef struct cs_server_options {
     double min_maf;            /* scan MAF filter (0.01) */
     int32_t precision;         /* kinship applies and scan projection (CS_PRECISION_MIXED) */
     int64_t max_batch_columns; /* right-hand sides per stacked apply (4096) */
-    double memory_budget_gb;   /* admission budget for request working sets (64) */
+    double memory_budget_gb;   /* admission budget for request working sets in GB (0: the
+                                  device's free memory at server creation less 4 GB) */
     int32_t max_active;        /* requests running at once (8) */
     double batch_window_ms;    /* after the first pending apply, wait up to this long (or until
                                   every running request waits on an apply) before stacking (0) */
+    double subset_fraction;    /* cohorts smaller than this fraction of the resident samples get
+                                  their own repacked subset operator instead of sharing the
+                                  stacked full-space applies (0.5; 0: always stack) */
 } cs_server_options;
 
 typedef struct cs_serve_request {
@@ -405,6 +497,8 @@ typedef struct cs_server_statistics {
     double throughput_rps, wall_s; /* completed / (last completion - first submit) */
     int64_t applies, apply_columns;
     int64_t max_requests_per_apply, max_concurrent;
+    int64_t own_view_requests;     /* requests that ran on their own subset operator */
+    double memory_budget_gb;       /* the admission budget in force */
 } cs_server_statistics;
 
 typedef struct cs_server cs_server;

@@ -2,6 +2,7 @@
 // interfaces so its call sites can swap in without semantic change:
 //   cs::Genotypes        ~ cosmic::PlinkReader (libCosmicCore/src/plink_reader.h)
 //   cs::KinshipOperator  ~ cosmic::KinshipOperator (src/kinship_operator.h:18-46)
+//   cs::GenotypeMatrix   ~ cosmic::GenotypeMatrix (libCosmicCore/src/matrix_adapter.h:40-53)
 //   cs::pcg_solve        ~ cosmic::MatrixFreePCG::solve (libCosmicCore/src/matrix_free_pcg.h)
 //   cs::StcgVce          ~ cosmic::STCG_VCE (libCosmicCore/src/stcg_vce.h:7-54)
 //   cs::LmmEngine        ~ LmmEngine::prepareLowRankMatrixFree / scan (src/lmm_engine.h)
@@ -125,6 +126,38 @@ class KinshipOperator {
     int64_t rows_ = 0, m_ = 0;
 };
 
+// GenotypeMatrix (matrix_adapter.h:40-53) over a kinship operator's selection: rows() samples x
+// cols() selected variants, z = (dosage - mean) / sd with the all-sample statistics, missing
+// calls 0 (PlinkReader::multiply_Z_v / multiply_Zt_v, plink_reader.cpp:241-438).  Host vectors;
+// `n_threads` is accepted for signature parity and ignored (the GPU does the work).
+class GenotypeMatrix {
+   public:
+    explicit GenotypeMatrix(const KinshipOperator& op, Precision p = Precision::FP64)
+        : op_(&op), p_(p) {}
+    int rows() const { return op_->rows(); }
+    int cols() const { return op_->numVariants(); }
+    // y = Z v: v has cols() entries, y gets rows()
+    void multiply_Z_v(const std::vector<double>& v, std::vector<double>& y, int n_threads = 1) const {
+        (void)n_threads;
+        if ((int64_t)v.size() != cols()) throw std::runtime_error("Dimension mismatch in multiply_Z_v");
+        y.resize(rows());
+        check(cs_genotype_multiply_z_host(op_->handle(), v.data(), cols(), 1, y.data(), rows(),
+                                          (int)p_));
+    }
+    // y = Z^T v: v has rows() entries, y gets cols()
+    void multiply_Zt_v(const std::vector<double>& v, std::vector<double>& y, int n_threads = 1) const {
+        (void)n_threads;
+        if ((int64_t)v.size() != rows()) throw std::runtime_error("Dimension mismatch in multiply_Zt_v");
+        y.resize(cols());
+        check(cs_genotype_multiply_zt_host(op_->handle(), v.data(), rows(), 1, y.data(), cols(),
+                                           (int)p_));
+    }
+
+   private:
+    const KinshipOperator* op_;
+    Precision p_;
+};
+
 // MatrixFreePCG::solve on (sigma2_g K + sigma2_e I) X = B, device column-major blocks.
 inline std::vector<int32_t> pcg_solve(const KinshipOperator& op, double sigma2_g, double sigma2_e,
                                       const double* B, int64_t ldb, int64_t k, double* X,
@@ -134,6 +167,26 @@ inline std::vector<int32_t> pcg_solve(const KinshipOperator& op, double sigma2_g
     std::vector<int32_t> it(k > 0 ? k : 1);
     check(cs_pcg_solve(op.handle(), kinship_divisor, sigma2_g, sigma2_e, B, ldb, k, X, ldx, tol,
                        relative ? 1 : 0, max_iter, (int)p, it.data(), stream));
+    it.resize(k);
+    return it;
+}
+
+// MatrixFreePCG::solve on STCG_VCE's record-level covariance (stcg_vce.cpp:80-126):
+// V = sigma2_g Zr K Zr^T + sigma2_pe Zr Zr^T + sigma2_e I, records mapped by rec_to_row (empty:
+// one record per operator row).  Device column-major blocks of n_records rows.
+inline std::vector<int32_t> pcg_solve_records(const KinshipOperator& op,
+                                              const std::vector<int32_t>& rec_to_row,
+                                              int64_t n_records, bool with_pe, double sigma2_g,
+                                              double sigma2_pe, double sigma2_e, const double* B,
+                                              int64_t ldb, int64_t k, double* X, int64_t ldx,
+                                              double tol = 1e-10, int max_iter = 2000,
+                                              bool relative = false, Precision p = Precision::FP64,
+                                              double kinship_divisor = 0.0, void* stream = nullptr) {
+    std::vector<int32_t> it(k > 0 ? k : 1);
+    check(cs_pcg_solve_records(op.handle(), kinship_divisor,
+                               rec_to_row.empty() ? nullptr : rec_to_row.data(), n_records,
+                               with_pe ? 1 : 0, sigma2_g, sigma2_pe, sigma2_e, B, ldb, k, X, ldx,
+                               tol, relative ? 1 : 0, max_iter, (int)p, it.data(), stream));
     it.resize(k);
     return it;
 }

@@ -738,6 +738,118 @@ def reml_diagnostics(D, Uty, UtX, sg, se):
                                       (n - p) * math.log(2.0 * math.pi))}
 
 
+def eigen_vce_iterative_reml(D, Uty, UtX, average_information=True, max_iter=100, tol=1e-6):
+    """EigenVce::runIterativeReml (libCosmicCore/src/eigen_vce.cpp:155-252): exact FP64 REML
+    in the eigenbasis from theta = (var/2, var/2), var = |U'y|^2 / df; AI steps with up to 40
+    halvings while the log-likelihood drops by more than 1e-10 (EM: the 0.5-blended ratio
+    update), stopping when the largest relative change < tol.  Returns sigma2_g, sigma2_e,
+    their AI standard errors, the log-likelihood, the score, iterations and converged."""
+    import math
+    D = np.asarray(D, dtype=np.float64)
+    Uty = np.asarray(Uty, dtype=np.float64)
+    UtX = np.asarray(UtX, dtype=np.float64).reshape(len(D), -1)
+    n, p = len(D), UtX.shape[1]
+    df = n - p
+    if df < 2:
+        raise ValueError("EigenVce REML requires residual degrees of freedom")
+    pvar = max(1e-10, float(Uty @ Uty) / df)
+    lower = pvar * 1e-10
+
+    def evaluate(theta):
+        cov = np.maximum(theta[0] * D + theta[1], lower)
+        inv = 1.0 / cov
+        if p:
+            info = UtX.T @ (inv[:, None] * UtX)
+            info_inv = np.linalg.inv(info)
+            log_det_fixed = float(np.linalg.slogdet(info)[1])
+            B = inv[:, None] * UtX              # diag(inv) U'X
+
+            def P(v):
+                return inv * v - B @ (info_inv @ (B.T @ v))
+            pdiag = inv - np.einsum("ia,ab,ib->i", B, info_inv, B)
+        else:
+            log_det_fixed = 0.0
+
+            def P(v):
+                return inv * v
+            pdiag = inv
+        py = P(Uty)
+        kpy = D * py
+        t = {"trace_g": float((pdiag * D).sum()), "trace_e": float(pdiag.sum()),
+             "quad_g": float(py @ kpy), "quad_e": float(py @ py)}
+        t["score"] = np.array([0.5 * (t["quad_g"] - t["trace_g"]), 0.5 * (t["quad_e"] - t["trace_e"])])
+        pk, pp = P(kpy), P(py)
+        t["ai"] = 0.5 * np.array([[kpy @ pk, kpy @ pp], [kpy @ pp, py @ pp]])
+        t["logl"] = -0.5 * (float(np.log(cov).sum()) + log_det_fixed + float(Uty @ py) +
+                            df * math.log(2.0 * math.pi))
+        return t
+
+    theta = np.array([0.5 * pvar, 0.5 * pvar])
+    cur = evaluate(theta)
+    converged, iterations = False, 0
+    for it in range(max_iter):
+        prop = theta.copy()
+        if average_information:
+            try:
+                step = np.linalg.solve(cur["ai"], cur["score"])
+            except np.linalg.LinAlgError:
+                break
+            frac = 1.0
+            for _ in range(40):
+                prop = np.maximum(theta + frac * step, lower)
+                if evaluate(prop)["logl"] >= cur["logl"] - 1e-10:
+                    break
+                frac *= 0.5
+        else:
+            prop = np.array([theta[0] * cur["quad_g"] / max(1e-12, cur["trace_g"]),
+                             theta[1] * cur["quad_e"] / max(1e-12, cur["trace_e"])])
+            prop = np.maximum(0.5 * theta + 0.5 * prop, lower)
+        change = float((np.abs(prop - theta) / (np.abs(theta) + pvar * 1e-8)).max())
+        theta = prop
+        cur = evaluate(theta)
+        iterations = it + 1
+        if change < tol:
+            converged = True
+            break
+    sg = max(0.0, 0.0 if theta[0] <= 1.01 * lower else theta[0])
+    se = max(0.0, 0.0 if theta[1] <= 1.01 * lower else theta[1])
+    cinv = np.linalg.inv(cur["ai"])
+    return {"sigma2_g": sg, "sigma2_e": se, "logl": cur["logl"],
+            "sigma2_g_se": math.sqrt(max(0.0, cinv[0, 0])),
+            "sigma2_e_se": math.sqrt(max(0.0, cinv[1, 1])),
+            "score": cur["score"], "ai": cur["ai"], "iterations": iterations,
+            "converged": converged}
+
+
+def hutchinson_vc_sd(K, X, sigma2_g, sigma2_e, probes):
+    """Predicted standard deviation of the variance components that a REML fit with
+    Hutchinson trace estimates (Rademacher probes, `probes` per trace) settles on, around the
+    exact REML solution: the trace estimates z'P K z / S and z'P z / S carry the covariance
+    2/S sum_{i!=j} A_ij B_ij of their symmetrised matrices A = (PK + KP)/2, B = P, the score
+    error is -1/2 of it, and the fitted components move by AI^-1 times the score error
+    (AI the exact average information, P = V^-1 - V^-1 X (X'V^-1 X)^-1 X'V^-1 at the solution).
+    Dense n x n algebra: for n of a few thousand."""
+    n = K.shape[0]
+    X = np.asarray(X, dtype=np.float64).reshape(n, -1)
+    V = sigma2_g * K + sigma2_e * np.eye(n)
+    Vi = np.linalg.inv(V)
+    ViX = Vi @ X
+    P = Vi - ViX @ np.linalg.solve(X.T @ ViX, ViX.T)
+    PK = P @ K
+    A = 0.5 * (PK + PK.T)
+    mats = [A, P]
+    cov = np.zeros((2, 2))
+    for a in range(2):
+        for b in range(2):
+            Ma, Mb = mats[a], mats[b]
+            cov[a, b] = 2.0 * ((Ma * Mb).sum() - (np.diag(Ma) * np.diag(Mb)).sum()) / probes
+    score_cov = 0.25 * cov
+    ai = 0.5 * np.array([[np.sum(PK * PK.T), np.sum(PK * P.T)], [np.sum(PK * P.T), np.sum(P * P)]])
+    aiinv = np.linalg.inv(ai)
+    vc_cov = aiinv @ score_cov @ aiinv.T
+    return np.sqrt(np.maximum(np.diag(vc_cov), 0.0))
+
+
 def scan_exact(bed: "Bed", keep, W, D, Uty, UtX, sg, se, min_maf=0.01, use_residuals=False,
                block=512):
     """LmmEngine::scan's exact branch (src/lmm_engine.cpp:1363-1474) over every SNP."""

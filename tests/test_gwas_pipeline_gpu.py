@@ -145,3 +145,41 @@ def test_low_rank_fallback_labels():
                                    trace_threshold=0.0, error_tol=0.0)
     assert dc["fallback"] == "error_tolerance"
     assert abs(dc["sigma2_g"] - da["sigma2_g"]) <= 1e-9 * da["sigma2_g"]
+
+
+def test_cpp_job_writes_the_same_files(tmp_path):
+    """cs_run_gwas_lmm (inputs, LOCO null models, scan and result files orchestrated in the
+    library's C++) writes byte-identical files to the same run assembled from the individual
+    entry points."""
+    n, m = 500, 1600
+    d = synth.cohort(n, m, 37, missing=0.02, n_causal=30, h2=0.5)
+    prefix = str(tmp_path / "c")
+    open(prefix + ".bed", "wb").write(d["bed"].tobytes())
+    chrom = np.array(["2"] * 700 + ["10"] * 500 + ["X"] * 400)
+    with open(prefix + ".bim", "w") as f:
+        for j in range(m):
+            f.write(f"{chrom[j]}\trs{j}\t0\t{1000 + 10 * j}\tA\tG\n")
+    rng = np.random.default_rng(8)
+    with open(prefix + ".fam", "w") as f:
+        for i in range(n):
+            v = "-9" if i % 37 == 5 else repr(float(d["y"][i]))
+            f.write(f"F{i} I{i} 0 0 1 {v}\n")
+    with open(str(tmp_path / "q.txt"), "w") as f:
+        for i in range(n):
+            f.write(f"F{i} I{i} {rng.normal():.4f}\n")
+    created = "2026-01-01 00:00:00 UTC"
+    a = str(tmp_path / "py")
+    res, diags, inputs = cs.run_gwas_lmm(prefix, a, qcovar=str(tmp_path / "q.txt"), rank=25,
+                                         precision="mixed", created=created)
+    b = str(tmp_path / "cpp")
+    n_kept, n_scopes = cs.gwas_lmm_files(prefix, b, qcovar=str(tmp_path / "q.txt"), rank=25,
+                                         precision="mixed", created=created)
+    assert n_kept == len(inputs["keep"]) and n_scopes == 3 == len(diags)
+    for ext in (".assoc.txt", ".cosmic.sumstats", ".scan.meta.txt"):
+        assert open(a + ext, "rb").read() == open(b + ext, "rb").read(), ext
+    # .low_rank.meta.tsv: equal but for DECOMPOSITION_SECONDS (a wall-clock time)
+    ra, rb = ([l.split("\t") for l in open(p + ".low_rank.meta.tsv").read().splitlines()]
+              for p in (a, b))
+    col = ra[0].index("DECOMPOSITION_SECONDS")
+    assert [r[:col] + r[col + 1:] for r in ra] == [r[:col] + r[col + 1:] for r in rb]
+    assert [r[0] for r in rb[1:]] == ["2", "10", "X"]

@@ -5,8 +5,9 @@ kinship, REML per trait, scan of a SNP window).  Checks: one request against the
 of the same job (src/lmm_engine.cpp:897-1361 restated; variance components 1e-5 relative, BETA 1e-5, -log10 P
 1e-4); every request of a concurrent mix
 against the same request run alone (the stacked applies keep columns independent, so the
-results agree to FP64 rounding: 1e-9); the batcher really stacked requests; bad requests
-fail before any work.
+results agree to FP64 rounding: 1e-9); the batcher really stacked requests; cohorts below
+half the resident samples run on their own repacked subset operator; bad requests fail
+before any work.
 """
 import numpy as np
 import pytest
@@ -42,13 +43,17 @@ def make_request(d, seed, n_sub, traits):
     return S, Y, X, b, b + 600
 
 
-def test_request_matches_oracle(data):
+@pytest.mark.parametrize("n_sub", [640, 300])
+def test_request_matches_oracle(data, n_sub):
+    """640 of 900 samples share the full-space applies; 300 (below half) run on their own
+    repacked subset operator."""
     d, g, variants, ref = data
-    S, Y, X, b, e = make_request(d, 1, 640, 2)
+    S, Y, X, b, e = make_request(d, 1, n_sub, 2)
     srv = cs.Server(g, variants, rank=40, precision="fp64", max_active=2)
     rid = srv.submit(S, Y, X, b, e)
     st = srv.wait(rid)
     assert st["state"] == 2 and st["latency_s"] > 0
+    assert srv.stats()["own_view_requests"] == (1 if n_sub < 450 else 0)
     wbed = oracle.Bed(d["bed"][3:].reshape(d["m"], -1)[b:e], d["n"])
     for t in range(2):
         U, lam, res = ref.lowrank_prepare(Y[:, t], X, 40, keep=S, variants=variants, n_threads=8)
@@ -86,6 +91,8 @@ def test_mix_equals_alone(data, precision):
     stats = mix.stats()
     assert stats["completed"] == len(reqs) and stats["failed"] == 0
     assert stats["max_requests_per_apply"] >= 2  # applies of different requests were stacked
+    assert stats["own_view_requests"] == 1      # the 300-sample cohort (< N / 2)
+    assert stats["memory_budget_gb"] > 0
     assert 0 < stats["p50_s"] <= stats["p99_s"]
     for rid, (S, Y, X, b, e), ref_out in zip(ids, reqs, solo):
         for t in range(Y.shape[1]):
