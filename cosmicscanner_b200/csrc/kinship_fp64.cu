@@ -15,10 +15,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "cs_internal.h"
 
 namespace cs {
+
+void decode_dmma_fp64(bool rows_pass, const cs_packed_view& v, const double* lut, const double* in,
+                      int64_t ldi, int64_t k, double* out, int64_t ldo, double scale,
+                      Workspace& ws, cudaStream_t s, int64_t max_splits);
 
 namespace {
 
@@ -324,11 +329,27 @@ void launch_cfg(const cs_packed_view& v, const double* lut, const double* in, in
     }
 }
 
+// The FP64 tensor (DMMA) form for 8 or more right-hand sides (CS_B200_FP64_DMMA=0 keeps the
+// SIMT form everywhere, =1 uses DMMA from one column on).
+int64_t dmma_min_columns() {
+    static const int64_t v = [] {
+        const char* e = std::getenv("CS_B200_FP64_DMMA");
+        if (e && e[0] == '0') return (int64_t)1 << 40;
+        if (e && e[0] == '1') return (int64_t)1;
+        return (int64_t)8;
+    }();
+    return v;
+}
+
 template <bool ROWS>
 void dispatch(const cs_packed_view& v, const double* lut, const double* in, int64_t ldi,
               int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s,
               int64_t max_splits = 64) {
     if (k <= 0) return;
+    if (k >= dmma_min_columns()) {
+        decode_dmma_fp64(ROWS, v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
+        return;
+    }
     if (k == 1)
         launch_cfg<256, 1, 1, 1, ROWS>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
     else if (k <= 8)
