@@ -160,6 +160,8 @@ class KinshipOperator:
         X = np.asarray(X, dtype=np.float64)
         vec = X.ndim == 1
         Xf = np.asfortranarray(X.reshape(-1, 1) if vec else X)
+        if Xf.shape[0] != self._rows:
+            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Zt_v")
         k = Xf.shape[1]
         out = np.zeros((self._m, k), order="F")
         _check(_abi.lib().cs_genotype_multiply_zt_host(self._h, _ptr(Xf), Xf.shape[0], k,
@@ -172,6 +174,8 @@ class KinshipOperator:
         V = np.asarray(V, dtype=np.float64)
         vec = V.ndim == 1
         Vf = np.asfortranarray(V.reshape(-1, 1) if vec else V)
+        if Vf.shape[0] != self._m:
+            raise InvalidArgument(_abi.CS_ERR_INVALID_ARGUMENT, "Dimension mismatch in multiply_Z_v")
         k = Vf.shape[1]
         out = np.zeros((self._rows, k), order="F")
         _check(_abi.lib().cs_genotype_multiply_z_host(self._h, _ptr(Vf), Vf.shape[0], k,
