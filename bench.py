@@ -848,6 +848,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "kernels": kernels,
+            "autotune": prof.get("autotune", []),
             "host_stages": prof.get("host", []),
             "sigma2_g": eng.getSigma2g(), "sigma2_e": eng.getSigma2e(),
             "tested": int(res["tested"].sum()),

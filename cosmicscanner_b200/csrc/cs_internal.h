@@ -163,6 +163,7 @@ struct cs_kinship {
     cs::Workspace ws;
     cs::DeviceBuffer<double> buf_x, buf_u, buf_y;
     cs::MixedOperator* mixed = nullptr;
+    bool autotune = true;  // the tensor-core passes may tune their plan on new shapes
     ~cs_kinship() { cs::destroy_mixed(mixed); }
 };
 
@@ -287,6 +288,9 @@ void lmm_scan_window(cs_lmm* l, const cs_genotypes* g, const int32_t* keep, int6
                      int64_t snp_begin, int64_t snp_end, double min_maf, int precision,
                      double* beta, double* se, double* pvalue, double* log10p, double* freq,
                      int32_t* tested, cudaStream_t s);
+
+// The tensor-core autotuner's table as JSON (kinship_mixed.cu).
+std::string autotune_json();
 
 namespace prof {
 // Counts one kernel launch; with profiling enabled, times it with events on stream s.

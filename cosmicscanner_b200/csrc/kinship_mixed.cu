@@ -31,8 +31,11 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
+#include <vector>
 
 #include "cs_internal.h"
 #include "sm100.cuh"
@@ -977,21 +980,148 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
     }
 }
 
+// ---------------------------------------------------------------- pass plans and the autotuner
+// A pass runs with a plan: CTA pairs or single CTAs, the column-tile width cap and the number of
+// K slices.  The default plan is the heuristic (pairs above 32 right-hand sides; widths 80 /
+// 48 / 80 / 80 for rows-single / samples-single / rows-pair / samples-pair; slices so that
+// about 8 units per CTA cover the GPU).  The autotuner times the pairs x width candidates of a
+// shape once (shapes bucketed: rows and samples by factors of 1.25, columns to multiples of 16)
+// and keeps the fastest.  It never changes the slice count, which is the only plan parameter
+// that changes floating-point results (the order of the slice sums), so a tuned pass returns
+// the same bits as the default one.  CS_B200_AUTOTUNE=0 turns it off.
+struct PassPlan {
+    bool pairs = false;
+    int max_w = 0;
+    int splits = 1;
+};
+
+PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
+    PassPlan p;
+    p.pairs = use_cta_pairs(k) && tiles % 2 == 0;
+    p.max_w = rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
+    const Tiling tl = tiling_for(k, p.max_w);
+    p.splits = p.pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
+                       : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    return p;
+}
+
+bool autotune_env() {
+    static const bool on = [] {
+        const char* v = std::getenv("CS_B200_AUTOTUNE");
+        return !(v && std::strcmp(v, "0") == 0);
+    }();
+    return on;
+}
+
+struct TuneKey {
+    int rows;
+    int64_t rb, nb, kb16;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(rows, rb, nb, kb16) < std::tie(o.rows, o.rb, o.nb, o.kb16);
+    }
+};
+struct TuneEntry {
+    PassPlan plan;
+    double ms_best = 0.0, ms_default = 0.0;
+    int64_t R = 0, n = 0, k = 0;  // the shape it was tuned on
+    int candidates = 0;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tuned;
+
+int64_t bucket(int64_t x) { return (int64_t)std::floor(std::log((double)std::max<int64_t>(x, 1)) / std::log(1.25)); }
+
+// The plan for a pass of this shape: the tuned one (tuning it now when the shape is new and the
+// pass may be timed: autotuning on, the stream not capturing, the work large enough to matter),
+// or the default.  `run` executes the pass with a plan.
+template <class Run>
+PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int64_t tiles, int kb,
+                     cudaStream_t s, Run&& run) {
+    const PassPlan def = default_plan(rows, tiles, kb, k);
+    if (!allow || !autotune_env() || 2.0 * (double)R * (double)n * (double)k < 2e10) return def;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return def;
+    const TuneKey key{rows ? 1 : 0, bucket(R), bucket(n), (k + 15) / 16};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            PassPlan p = it->second.plan;
+            p.splits = def.splits;
+            return p;
+        }
+    }
+    std::vector<PassPlan> cands;
+    const int mode = pair_mode();
+    for (int pr = 0; pr < 2; ++pr) {
+        if (pr == 1 && (mode == 0 || tiles % 2 != 0 || num_sms() < 2)) continue;
+        if (pr == 0 && mode == 2) continue;
+        const int cap_w = rows ? (pr ? kPairRowsW : kRowsW) : (pr ? kPairSamplesW : kSamplesW);
+        int last_kp = -1, last_ct = -1;
+        for (int w = 32; w <= cap_w; w += 16) {
+            const Tiling tl = tiling_for(k, w);
+            if (tl.kp == last_kp && tl.n_ctiles == last_ct) continue;  // same tiling as a narrower cap
+            last_kp = (int)tl.kp;
+            last_ct = tl.n_ctiles;
+            PassPlan p;
+            p.pairs = pr == 1;
+            p.max_w = w;
+            p.splits = def.splits;
+            cands.push_back(p);
+        }
+    }
+    cudaEvent_t e0, e1;
+    CS_CUDA(cudaEventCreate(&e0));
+    CS_CUDA(cudaEventCreate(&e1));
+    TuneEntry best;
+    best.plan = def;
+    best.ms_best = 1e30;
+    try {
+        run(def);  // warm: maps, function attributes, operand buffers
+        for (const PassPlan& p : cands) {
+            CS_CUDA(cudaEventRecord(e0, s));
+            run(p);
+            CS_CUDA(cudaEventRecord(e1, s));
+            CS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (p.pairs == def.pairs && p.max_w == def.max_w) best.ms_default = ms;
+            if (ms < best.ms_best) {
+                best.ms_best = ms;
+                best.plan = p;
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    best.R = R;
+    best.n = n;
+    best.k = k;
+    best.candidates = (int)cands.size();
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned.emplace(key, best);
+    }
+    return best.plan;
+}
+
 // Rows pass over a MixedRows context: for X (n x k, row-major ldx),
 //   out_tc = s_t^spow ( sum_i (G_ti - mu_t)[obs] x_ic )  (mean-imputed centred dosages)
 // written column-major (out[c * out_ld + t]) or row-major.  With want_max, also the
 // per-column maxima of |out| and |mu out| (samples-pass operand scales).
-void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, int64_t k,
-               double* out, int64_t out_ld, bool colmajor, int spow, bool want_max,
-               cudaStream_t s) {
+void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, const double* X,
+                    int64_t ldx, int64_t k, double* out, int64_t out_ld, bool colmajor, int spow,
+                    bool want_max, cudaStream_t s) {
     const int64_t tiles = r.r_pad / kTile;
-    const bool pairs = use_cta_pairs(k) && tiles % 2 == 0;
-    const Tiling tl = tiling_for(k, pairs ? kPairRowsW : kRowsW);
+    const bool pairs = plan.pairs;
+    const Tiling tl = tiling_for(k, plan.max_w);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(n_pad / kKBlock);
-    // about 8 units per CTA (pairs: per cluster of two)
-    const int splits = pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
-                             : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    const int splits = plan.splits;
     const int kbs = (kb + splits - 1) / splits;
     const int rt = (int)((n_pad + kPrepRows - 1) / kPrepRows);
     const int nst = (int)((n + kPrepRows - 1) / kPrepRows);  // row tiles of the column stats
@@ -1070,15 +1200,14 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
 
 // Samples pass: Y (n x k, row-major ldy) = (Z W) / M for W^T (k x R, column-major) with the
 // per-column maxima computed by rows_pass(want_max).
-void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
-                  double* Y, int64_t ldy, cudaStream_t s) {
+void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, const double* Wt,
+                       int64_t k, double inv_m, double* Y, int64_t ldy, cudaStream_t s) {
     const int64_t tiles = r.n_pad / kTile;
-    const bool pairs = use_cta_pairs(k) && tiles % 2 == 0;
-    const Tiling tl = tiling_for(k, pairs ? kPairSamplesW : kSamplesW);
+    const bool pairs = plan.pairs;
+    const Tiling tl = tiling_for(k, plan.max_w);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(r_pad / kKBlock);
-    const int splits = pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
-                             : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
+    const int splits = plan.splits;
     const int kbs = (kb + splits - 1) / splits;
     const int nrb = (int)((r_pad + 2047) / 2048);
     ws.b2.resize(6 * kp * r_pad);
@@ -1134,6 +1263,27 @@ void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k,
     }
 }
 
+void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, int64_t k,
+               double* out, int64_t out_ld, bool colmajor, int spow, bool want_max,
+               cudaStream_t s, bool allow_tune) {
+    const int64_t tiles = r.r_pad / kTile;
+    const int kb = (int)(r.n_pad / kKBlock);
+    const PassPlan plan = choose_plan(true, allow_tune, r.R, r.n, k, tiles, kb, s, [&](const PassPlan& p) {
+        rows_pass_plan(p, r, ws, X, ldx, k, out, out_ld, colmajor, spow, want_max, s);
+    });
+    rows_pass_plan(plan, r, ws, X, ldx, k, out, out_ld, colmajor, spow, want_max, s);
+}
+
+void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
+                  double* Y, int64_t ldy, cudaStream_t s, bool allow_tune) {
+    const int64_t tiles = r.n_pad / kTile;
+    const int kb = (int)(r.r_pad / kKBlock);
+    const PassPlan plan = choose_plan(false, allow_tune, r.R, r.n, k, tiles, kb, s, [&](const PassPlan& p) {
+        samples_pass_plan(p, r, ws, Wt, k, inv_m, Y, ldy, s);
+    });
+    samples_pass_plan(plan, r, ws, Wt, k, inv_m, Y, ldy, s);
+}
+
 }  // namespace
 
 static MixedOperator* mixed_for(cs_kinship* op) {
@@ -1161,8 +1311,9 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     m->ws.W.resize(R * k);
     // W^T = s o s o (Z-centred)^T X: the rows pass output already scaled for the samples pass
     m->last_k = 0;
-    rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s);
-    samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s);
+    rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s, op->autotune);
+    samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s,
+                 op->autotune);
     check_status(m->ws, s);
     m->last_k = k;
 }
@@ -1207,7 +1358,7 @@ void mixed_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, 
     if (k <= 0 || op->n_active == 0) return;
     MixedOperator* m = mixed_for(op);
     m->last_k = 0;
-    rows_pass(m->rows, m->ws, X, ldx, k, U, ldu, false, 1, false, s);
+    rows_pass(m->rows, m->ws, X, ldx, k, U, ldu, false, 1, false, s, op->autotune);
     check_status(m->ws, s);
 }
 
@@ -1235,8 +1386,29 @@ void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, 
                                        ws.max_muw.get());
         CS_LAUNCH("col_absmax");
     }
-    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s);
+    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune);
     check_status(ws, s);
+}
+
+// The autotuner's table as JSON (reported with the profile summary).
+std::string autotune_json() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::string out = "[";
+    char buf[320];
+    bool first = true;
+    for (const auto& kv : g_tuned) {
+        const TuneEntry& e = kv.second;
+        std::snprintf(buf, sizeof buf,
+                      "%s{\"pass\": \"%s\", \"R\": %lld, \"n\": %lld, \"k\": %lld, "
+                      "\"pairs\": %s, \"max_width\": %d, \"slices\": %d, \"candidates\": %d, "
+                      "\"ms_best\": %.4f, \"ms_default\": %.4f}",
+                      first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
+                      (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
+                      e.plan.max_w, e.plan.splits, e.candidates, e.ms_best, e.ms_default);
+        out += buf;
+        first = false;
+    }
+    return out + "]";
 }
 
 const double* mixed_rows_output(const cs_kinship* op, int64_t* R, int64_t* k) {
@@ -1268,7 +1440,7 @@ void mixed_scan_destroy(MixedScan* m) { delete m; }
 
 void mixed_scan_project(MixedScan* m, const double* B, int64_t ldb, int64_t k, double* T,
                         int64_t ldt, cudaStream_t s) {
-    rows_pass(m->rows, m->ws, B, ldb, k, T, ldt, false, 1, false, s);
+    rows_pass(m->rows, m->ws, B, ldb, k, T, ldt, false, 1, false, s, true);
     check_status(m->ws, s);
 }
 

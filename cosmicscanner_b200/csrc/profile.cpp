@@ -132,7 +132,7 @@ std::string summary_json() {
         out += buf;
         first = false;
     }
-    out += "]}";
+    out += "], \"autotune\": " + autotune_json() + "}";
     return out;
 }
 
