@@ -73,6 +73,14 @@ def parse():
     ap.add_argument("--dense-m", type=int, default=50000, help="SNPs of the dense measurement")
     ap.add_argument("--dense-only", action="store_true",
                     help="only the dense exact-route measurement (the case its ncu captures use)")
+    ap.add_argument("--config1", type=int, default=1,
+                    help="run the small single-trait configuration leg (0 skips)")
+    ap.add_argument("--config3", action="store_true",
+                    help="run the multi-trait configuration leg (N=100k, M=500k, 8 traits)")
+    ap.add_argument("--config3-iters", type=int, default=3)
+    ap.add_argument("--config4", action="store_true",
+                    help="run the repeatability configuration leg (N=100k, ~300k records, M=300k)")
+    ap.add_argument("--config4-iters", type=int, default=6)
     ap.add_argument("--ref-budget", type=float, default=240.0,
                     help="seconds of whole CPU jobs the reference arm runs (at least one)")
     ap.add_argument("--aireml-iters", type=int, default=50,
@@ -466,6 +474,143 @@ def run_aireml(cs, op, d, args, iters=50, probes=64, precond_rank=64, compare_it
     return out
 
 
+def run_config1(cs, args):
+    """The small single-trait configuration (N=2,000, M=10,000, 1% missing, X = [1, N(0,1)],
+    100 causal SNPs, h2 0.5): the low-rank REML + scan job in the mixed and FP64 GPU forms and
+    the oracle's CPU restatement on the host cores, and the PCG + Hutchinson AI-REML with the
+    configuration's 30 probes (reference defaults: up to 50 iterations, SLQ log-likelihood).
+    Seconds per job (the second of two runs for the GPU forms)."""
+    import torch
+
+    import oracle
+    from cosmicscanner_b200 import synth
+
+    d = synth.config1()
+    n, m = d["n"], d["m"]
+    X = d["X"].astype(np.float32).astype(np.float64)
+    g = cs.Genotypes.from_bed_bytes(d["bed"], n, m)
+    variants = cs.grm_variant_selection(g.stats(), 0.01)
+    op = cs.KinshipOperator(g, None, variants)
+    keep = np.arange(n, dtype=np.int32)
+    out = {"n": n, "m": m}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        eng = cs.LmmEngine()
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            diag = eng.prepareLowRankMatrixFree(d["y"], X, op, rank=RANK, oversample=OVERSAMPLE,
+                                                precision=prec)
+            r = eng.scan(g, keep, min_maf=0.01, precision=prec)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        res[prec] = (diag, r)
+        out[f"lowrank_{prec}_s"] = dt
+        eng.close()
+    out["lowrank_accuracy_mixed_vs_fp64"] = accuracy(res["mixed"][0], res["mixed"][1],
+                                                     res["fp64"][0], res["fp64"][1])
+    B = oracle.Bed(d["bed"][3:].reshape(m, -1), n)
+    t0 = time.perf_counter()
+    cj = oracle.lowrank_job_blas(B, d["y"], X, variants=variants, rank=RANK, oversample=OVERSAMPLE,
+                                 n_threads=host_threads())
+    out["lowrank_cpu_restatement_s"] = time.perf_counter() - t0
+    out["cpu_cores"] = host_threads()
+    out["sigma2_g"] = {"mixed": res["mixed"][0]["sigma2_g"], "fp64": res["fp64"][0]["sigma2_g"],
+                       "cpu": cj["sigma2_g"]}
+    op_all = cs.KinshipOperator(g, None, None)
+    for prec in ("mixed", "fp64"):
+        vce = cs.StcgVce()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rv = vce.solve(op_all, d["y"], X, kinship_divisor=float(m), max_iter=50, mc_samples=30,
+                       slq_probes=30, precision=prec)
+        torch.cuda.synchronize()
+        out[f"aireml_{prec}"] = {"seconds": time.perf_counter() - t0,
+                                 "iterations": rv["iterations"], "sigma2_g": rv["sigma2_g"],
+                                 "sigma2_e": rv["sigma2_e"], "logl": rv["logl"],
+                                 "pcg_iterations": rv["pcg_iterations"]}
+        vce.close()
+    op_all.close()
+    op.close()
+    g.close()
+    return out
+
+
+def run_config3(cs, args):
+    """The multi-trait configuration: N=100,000, M=500,000 (MAF U(0.01, 0.5)), 8 traits with
+    LKJ(2) genetic correlation, h2 U(0.2, 0.6), residual correlation 0.3; the multi-trait
+    matrix-free REML (EM on Vg (x) K + Ve (x) I with 32 probes: every kinship apply carries
+    8 x (1 + 32) = 264 right-hand sides) in the mixed form, --config3-iters EM iterations.
+    The reference's route (MvEigenVce) needs the dense N x N eigendecomposition (80 GB at
+    N = 100,000) and is not run."""
+    import torch
+
+    from cosmicscanner_b200 import synth
+
+    t0 = time.perf_counter()
+    d = synth.config3()
+    gen_s = time.perf_counter() - t0
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    op = cs.KinshipOperator(g, None, None)
+    del d["bed"]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Vg, Ve, r = cs.mv_stcg_solve(op, d["Y"], d["X"], kinship_divisor=float(d["m"]),
+                                 max_iter=args.config3_iters, tol=0.0, mc_samples=32,
+                                 precision=args.precision)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    op.close()
+    g.close()
+    h2_est = np.diag(Vg) / (np.diag(Vg) + np.diag(Ve))
+    return {"n": d["n"], "m": d["m"], "traits": int(d["Y"].shape[1]), "seconds": dt,
+            "s_per_iteration": dt / max(1, r["iterations"]), "iterations": r["iterations"],
+            "kinship_applies": r["operator_applies"],
+            "rhs_per_apply": r["operator_columns"] / max(1, r["operator_applies"]),
+            "ms_per_apply": 1e3 * dt / max(1, r["operator_applies"]),
+            "cg_iterations": r["pcg_iterations"], "h2_true": d["h2"].tolist(),
+            "h2_after_iterations": h2_est.tolist(), "generation_s": gen_s,
+            "precision": args.precision}
+
+
+def run_config4(cs, args):
+    """The repeatability configuration: N=100,000 individuals with 1..5 records each (~300k
+    records), M=300,000 SNPs, y = X b + Zr (g + pe) + e with h2 0.3 and repeatability 0.5, fixed
+    effects intercept, N(0,1) and a 4-level factor; the three-component matrix-free AI-REML
+    (V = sg2 Zr K Zr' + spe2 Zr Zr' + se2 I) in the mixed form with 32 probes, --config4-iters
+    iterations with the SLQ log-likelihood.  The record-level scan (scanSTCG) needs the dense
+    q x q subject GRM as the reference builds it (80 GB at q = 100,000) and is not run here."""
+    import torch
+
+    from cosmicscanner_b200 import synth
+
+    t0 = time.perf_counter()
+    d = synth.config4()
+    gen_s = time.perf_counter() - t0
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    op = cs.KinshipOperator(g, None, None)
+    del d["bed"]
+    vce = cs.StcgVce()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = vce.solve(op, d["y"], d["X"], rec_to_row=d["rec_to_row"], with_pe=True,
+                  kinship_divisor=float(d["m"]), max_iter=args.config4_iters, mc_samples=32,
+                  slq_probes=30, precision=args.precision)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    vce.close()
+    op.close()
+    g.close()
+    return {"n": d["n"], "records": int(len(d["y"])), "m": d["m"], "seconds": dt,
+            "s_per_iteration": dt / max(1, r["iterations"]), "iterations": r["iterations"],
+            "sigma2_g": r["sigma2_g"], "sigma2_pe": r["sigma2_pe"], "sigma2_e": r["sigma2_e"],
+            "logl": r["logl"], "pcg_iterations": r["pcg_iterations"],
+            "kinship_applies": r["operator_applies"],
+            "rhs_per_apply": r["operator_columns"] / max(1, r["operator_applies"]),
+            "generation_s": gen_s, "precision": args.precision,
+            "scan": "not run: scanSTCG needs the dense q x q subject GRM (80 GB at q = 100,000)"}
+
+
 def run_dense(cs, args):
     """The dense exact route (`gwas --model lmm` without --fastlmm): GRM (VanRaden) over every
     sample, EigenVce with the covariate projection, Brent null model and the exact scan of
@@ -769,6 +914,9 @@ def main():
         serve = (run_serve_config5(cs, args) if args.serve_config5 else
                  run_serve(cs, g, variants, d, args, fp64_sample=args.serve_fp64_sample))
     dense = run_dense(cs, args) if args.dense_n > 0 and world == 1 else None
+    config1 = run_config1(cs, args) if args.config1 and world == 1 else None
+    config3 = run_config3(cs, args) if args.config3 and world == 1 else None
+    config4 = run_config4(cs, args) if args.config4 and world == 1 else None
     aireml = None
     if args.aireml_iters > 0 and world == 1:
         op_all = cs.KinshipOperator(g, None, None)
@@ -844,6 +992,9 @@ def main():
             "accuracy": None if fp64 is None else fp64["accuracy_of_mixed"],
             "serve": serve,
             "aireml": aireml,
+            "config1": config1,
+            "config3": config3,
+            "config4": config4,
             "dense": dense,
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),

@@ -572,6 +572,40 @@ class MatrixFreePCG:
         return x[:, 0].copy() if vec else np.asfortranarray(x)
 
 
+class MvStcgOptions(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32), ("tol", C.c_double), ("mc_samples", C.c_int32),
+        ("pcg_tol", C.c_double), ("pcg_relative", C.c_int32), ("pcg_max_iter", C.c_int32),
+        ("probe_seed", C.c_uint64), ("precision", C.c_int32),
+    ]
+
+
+class MvStcgResult(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int32), ("converged", C.c_int32), ("pcg_iterations", C.c_int64),
+        ("operator_applies", C.c_int64), ("operator_columns", C.c_int64), ("seconds", C.c_double),
+    ]
+
+
+def mv_stcg_solve(op: "KinshipOperator", Y, X, kinship_divisor: float = 0.0, **options):
+    """The multi-trait matrix-free REML (cs_mv_stcg_solve): MvEigenVce's EM for
+    Vg (x) K + Ve (x) I from kinship applies, CG and Hutchinson probes.  Y (n, d), X (n, p).
+    Returns (Vg, Ve, result dict)."""
+    Y = np.asfortranarray(np.asarray(Y, dtype=np.float64).reshape(op.rows(), -1))
+    X = np.asfortranarray(np.asarray(X, dtype=np.float64).reshape(op.rows(), -1))
+    d = Y.shape[1]
+    o = MvStcgOptions()
+    _abi.lib().cs_mv_stcg_default_options(C.byref(o))
+    for k, v in options.items():
+        setattr(o, k, _prec(v) if k == "precision" else v)
+    Vg = np.zeros((d, d), order="F")
+    Ve = np.zeros((d, d), order="F")
+    r = MvStcgResult()
+    _check(_abi.lib().cs_mv_stcg_solve(op._h, float(kinship_divisor), _ptr(Y), d, _ptr(X),
+                                       X.shape[1], C.byref(o), _ptr(Vg), _ptr(Ve), C.byref(r)))
+    return Vg, Ve, {f[0]: getattr(r, f[0]) for f in r._fields_}
+
+
 class VceOptions(C.Structure):
     _fields_ = [
         ("max_iter", C.c_int32), ("tol", C.c_double), ("mc_samples", C.c_int32),

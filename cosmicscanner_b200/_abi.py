@@ -72,6 +72,8 @@ _SIGNATURES = {
     "cs_lmm_scan_window": ([_P, _P, _P, _I64, _I64, _I64, _D, _I, _P, _P, _P, _P, _P, _P], _I),
     "cs_lmm_destroy": ([_P], None),
     "cs_normal_matrix": ([C.c_uint64, _I64, _I64, _P], _I),
+    "cs_mv_stcg_default_options": ([_P], None),
+    "cs_mv_stcg_solve": ([_P, _D, _P, C.c_int32, _P, _I64, _P, _P, _P, _P], _I),
     "cs_lmm_run_default_options": ([_P], None),
     "cs_run_lmm_matrix_free": ([_P, _P, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                 _I, _P], _I),

@@ -66,6 +66,10 @@ void pcg_solve_records_public(cs_kinship* op, double divisor, const int32_t* rec
                               const double* B, int64_t ldb, int64_t k, double* X, int64_t ldx,
                               double tol, int relative, int max_iter, int precision,
                               int32_t* iterations, cudaStream_t s);
+void mv_stcg_default_options(cs_mv_stcg_options* o);
+void mv_stcg_solve(cs_kinship* op, double divisor, const double* Y, int32_t d, const double* X,
+                   int64_t p, const cs_mv_stcg_options* opt, double* Vg, double* Ve,
+                   cs_mv_stcg_result* res);
 void genotype_multiply_zt(cs_kinship* op, const double* X, int64_t ldx, int64_t k, double* U,
                           int64_t ldu, int precision, cudaStream_t s);
 void genotype_multiply_z(cs_kinship* op, const double* V, int64_t ldv, int64_t k, double* Y,
@@ -531,6 +535,19 @@ int cs_pcg_solve_records(cs_kinship* op, double kinship_divisor, const int32_t* 
                                      sigma2_g, sigma2_pe, sigma2_e, B, ldb, k, X, ldx, tol,
                                      relative, max_iter, precision, iterations,
                                      (cudaStream_t)stream);
+    });
+}
+
+void cs_mv_stcg_default_options(cs_mv_stcg_options* opt) {
+    if (opt) cs::mv_stcg_default_options(opt);
+}
+
+int cs_mv_stcg_solve(cs_kinship* op, double kinship_divisor, const double* Y, int32_t d,
+                     const double* X, int64_t p, const cs_mv_stcg_options* opt, double* Vg,
+                     double* Ve, cs_mv_stcg_result* res) {
+    return guarded([&] {
+        require(op != nullptr && res != nullptr, "null argument");
+        cs::mv_stcg_solve(op, kinship_divisor, Y, d, X, p, opt, Vg, Ve, res);
     });
 }
 

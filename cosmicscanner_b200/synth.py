@@ -8,6 +8,9 @@ The workload shapes follow the benchmark configurations:
   beta = (0, 0.5), 100 causal SNPs, h2 = 0.5.
 * ``config2``: N=50,000, M=100,000, two Balding-Nichols populations (Fst 0.01, 50/50),
   2% missing, X = [1, N(0,1), Bernoulli(0.5)], h2 = 0.4 from 1,000 causal SNPs.
+* ``config3``: N=100,000, M=500,000, MAF ~ U(0.01, 0.5), 8 traits with LKJ(2) genetic
+  correlation, h2 ~ U(0.2, 0.6), exchangeable residual correlation 0.3.
+* ``config4``: N=100,000 individuals with 1..5 records each, M=300,000 (repeatability).
 """
 from __future__ import annotations
 
@@ -104,6 +107,59 @@ def config1(seed=20261203 + 1):
 def config2(seed=20261203 + 2, n=50000, m=100000):
     return cohort(n, m, seed, maf_lo=0.05, n_pops=2, fst=0.01, missing=0.02, n_causal=1000,
                   h2=0.4, covariates="intercept+normal+bernoulli")
+
+
+def lkj_correlation(d, eta, rng):
+    """A d x d correlation matrix from the LKJ(eta) distribution by the C-vine construction of
+    Lewandowski, Kurowicka and Joe (2009): partial correlations drawn as 2 Beta(b, b) - 1 with b
+    starting at eta + (d - 1) / 2 and lowered by 1/2 per vine level, then turned into
+    correlations along the vine."""
+    b = eta + (d - 1) / 2.0
+    P = np.zeros((d, d))
+    R = np.eye(d)
+    for k in range(d - 1):
+        b -= 0.5
+        for i in range(k + 1, d):
+            P[k, i] = 2.0 * rng.beta(b, b) - 1.0
+            r = P[k, i]
+            for l in range(k - 1, -1, -1):
+                r = r * np.sqrt((1.0 - P[l, i] ** 2) * (1.0 - P[l, k] ** 2)) + P[l, i] * P[l, k]
+            R[k, i] = R[i, k] = r
+    return R
+
+
+def multi_trait_cohort(n, m, seed, d=8, eta=2.0, h2_range=(0.2, 0.6), resid_corr=0.3,
+                       maf_lo=0.01, missing=0.01, n_causal=200):
+    """d correlated traits: genetic correlation ~ LKJ(eta), h2_t ~ U(h2_range), exchangeable
+    residual correlation resid_corr; each trait's polygenic score from its own n_causal SNPs
+    (N(0,1) effects on standardised genotypes), mixed by the genetic correlation's Cholesky
+    factor.  X = [1, N(0,1)].  Returns dict(bed, n, m, Y, X, Rg, h2)."""
+    rng = np.random.default_rng(seed)
+    freq = allele_frequencies(m, maf_lo, 1, 0.0, rng)
+    pop = np.zeros(n, np.int32)
+    bed = genotype_bed(n, m, seed, freq, pop, missing)
+    causal = rng.choice(m, size=min(d * n_causal, m), replace=False).astype(np.int32)
+    scores = np.zeros((n, d))
+    for t in range(d):
+        snps = np.sort(causal[t * n_causal:(t + 1) * n_causal])
+        G = decode(bed, n, snps)
+        mu = np.nanmean(G, axis=0)
+        sd = np.nanstd(G, axis=0)
+        sd[sd == 0] = 1.0
+        s = np.where(np.isnan(G), 0.0, (G - mu) / sd) @ rng.standard_normal(len(snps))
+        scores[:, t] = (s - s.mean()) / (s.std() or 1.0)
+    Rg = lkj_correlation(d, eta, rng)
+    Re = np.full((d, d), resid_corr) + (1.0 - resid_corr) * np.eye(d)
+    h2 = rng.uniform(h2_range[0], h2_range[1], size=d)
+    g = scores @ np.linalg.cholesky(Rg).T
+    e = rng.standard_normal((n, d)) @ np.linalg.cholesky(Re).T
+    X = np.column_stack([np.ones(n), rng.standard_normal(n)])
+    Y = X @ np.vstack([np.zeros(d), np.full(d, 0.5)]) + g * np.sqrt(h2) + e * np.sqrt(1.0 - h2)
+    return {"bed": bed, "n": n, "m": m, "Y": Y, "X": X, "Rg": Rg, "h2": h2}
+
+
+def config3(seed=20261203 + 3, n=100000, m=500000):
+    return multi_trait_cohort(n, m, seed)
 
 
 def repeatability_cohort(n, m, seed, max_records=5, h2=0.3, repeatability=0.5, maf_lo=0.01,

@@ -161,6 +161,39 @@ int cs_lmm_scan_window(cs_lmm* lmm, const cs_genotypes* g, const int32_t* keep, 
                        int32_t* tested);
 void cs_lmm_destroy(cs_lmm* lmm);
 
+/* ---------------------------------------------------------------- multi-trait matrix-free REML
+ * The multivariate null model of `--model multivariate` (MvEigenVce::runNullModel's EM,
+ * libCosmicCore/src/eigen_vce.cpp:551-604, 1031-1065) without the dense N x N eigenbasis:
+ * vec(Y) ~ N((I_d (x) X) b, Vg (x) K + Ve (x) I), K = Z Z^T / kinship_divisor over the operator's
+ * samples.  Each EM iteration solves (Q V Q) x = Q [Y | Z_1 .. Z_S] by conjugate gradients
+ * (Q = I - X (X'X)^-1 X' per trait; P = Q (Q V Q)^+ Q), S Rademacher probes of n x d redrawn per
+ * iteration from mt19937_64(probe_seed), so every kinship apply carries (1 + S) d columns; one
+ * more apply K [PY | Z] gives (PY)' K (PY) and the Hutchinson estimates of tr(P (E_ab (x) K)).
+ * Update Vg += Vg (Qg - Tg) Vg / (n - p), Ve likewise; starting values Cov(Y) / 2; stop when
+ * (|dVg|^2 + |dVe|^2) / max(1, 2 d^2) < tol.  Y n x d and X n x p column-major host arrays; Vg, Ve
+ * d x d column-major outputs. */
+typedef struct cs_mv_stcg_options {
+    int32_t max_iter;      /* EM iterations (100) */
+    double tol;            /* the reference's EM stopping threshold (1e-8) */
+    int32_t mc_samples;    /* probes per iteration (32) */
+    double pcg_tol;        /* CG threshold (1e-8) */
+    int32_t pcg_relative;  /* 1: ||r|| < pcg_tol ||b|| per probe / trait group (default); 0: absolute */
+    int32_t pcg_max_iter;  /* (2000) */
+    uint64_t probe_seed;   /* (20250101) */
+    int32_t precision;     /* CS_PRECISION_FP64 or CS_PRECISION_MIXED for the kinship applies */
+} cs_mv_stcg_options;
+typedef struct cs_mv_stcg_result {
+    int32_t iterations, converged;
+    int64_t pcg_iterations;    /* CG iterations summed over probe / trait groups */
+    int64_t operator_applies;  /* kinship applies */
+    int64_t operator_columns;  /* right-hand sides they carried */
+    double seconds;
+} cs_mv_stcg_result;
+void cs_mv_stcg_default_options(cs_mv_stcg_options* opt);
+int cs_mv_stcg_solve(cs_kinship* op, double kinship_divisor, const double* Y, int32_t d,
+                     const double* X, int64_t p, const cs_mv_stcg_options* opt, double* Vg,
+                     double* Ve, cs_mv_stcg_result* res);
+
 /* ---------------------------------------------------------------- the whole job
  * GwasScanner::runLocoScan's PLINK matrix-free branch (src/gwas_scanner.cpp:74-509) in the
  * library's C++: GRM variant selection from the all-sample statistics (:258-277), one null

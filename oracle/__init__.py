@@ -108,6 +108,7 @@ def lib():
         L.orc_scan_encode_cols.argtypes = [_P, _I64, _I64, _I64, _I64, C.c_double, _P, _I64, _P,
                                            _P, _P, C.c_int]
         L.orc_chisq_prob_vec.argtypes = [_P, _I64, C.c_int, _P, C.c_int]
+        L.orc_rademacher.argtypes = [C.c_uint64, _I64, _I64, _I64, _P]
         _lib = L
     return _lib
 
@@ -326,6 +327,14 @@ def kinship_batch_fixture(n=37, m=1031, seed=8128, rows=None, widths=(1, 7, 41))
 def normal_matrix(seed, n, cols):
     out = np.zeros((n, cols), order="F")
     lib().orc_normal_matrix(seed, n, cols, _ptr(out))
+    return out
+
+
+def rademacher(seed, skip, n, cols):
+    """n x cols +-1 block from mt19937_64(seed) + uniform_int_distribution<int>(0, 1) after
+    `skip` draws, column by column (the probe stream of the matrix-free REML estimators)."""
+    out = np.zeros((n, cols), order="F")
+    lib().orc_rademacher(int(seed), int(skip), int(n), int(cols), _ptr(out))
     return out
 
 
@@ -935,6 +944,66 @@ def mv_loglik(D, UtY, Vg, Ve):
     sign, ld = np.linalg.slogdet(V)
     sol = np.linalg.solve(V, UtY[:, :, None])[:, :, 0]
     return float((-0.5 * (ld + (UtY * sol).sum(axis=1))).sum())
+
+
+def mv_stcg_em(K, Y, X, max_iter=10, tol=1e-8, mc_samples=32, probe_seed=20250101,
+               exact_traces=False):
+    """The multi-trait REML-EM of MvEigenVce::updateEM (libCosmicCore/src/eigen_vce.cpp:551-604)
+    written for a general covariance V = Vg (x) K + Ve (x) I instead of the eigenbasis, with the
+    covariates kept in P = V^-1 - V^-1 Xf (Xf' V^-1 Xf)^-1 Xf' V^-1, Xf = I_d (x) X:
+        Vg <- Vg + Vg (Qg - Tg) Vg / (n - p),  Ve <- Ve + Ve (Qe - Te) Ve / (n - p),
+        Qg = (PY)' K (PY), Qe = (PY)' (PY), Tg[a, b] = tr(P (E_ab (x) K)), Te[a, b] = tr(P (E_ab (x) I))
+    (in the eigenbasis this is the reference's per-sample update).  The traces are Hutchinson
+    estimates with mc_samples Rademacher probes of n x d per iteration, redrawn every iteration
+    from one mt19937_64 stream (probe s, trait a = column s d + a), unless exact_traces.  Dense
+    n d x n d algebra: the checker of the matrix-free GPU form at small n.  Starting values
+    Vg = Ve = Cov(Y) / 2 over n - p - 1 (:536-548); stop when
+    (|dVg|^2 + |dVe|^2) / max(1, 2 d^2) < tol.  Returns (Vg, Ve, iterations, converged)."""
+    K = np.asarray(K, dtype=np.float64)
+    Y = np.asarray(Y, dtype=np.float64)
+    n, d = Y.shape
+    X = np.asarray(X, dtype=np.float64).reshape(n, -1)
+    p = X.shape[1]
+    Yc = Y - Y.mean(axis=0)
+    cov = Yc.T @ Yc / (n - p - 1)
+    Vg, Ve = 0.5 * cov, 0.5 * cov.copy()
+    I = np.eye(n)
+    Xf = np.kron(np.eye(d), X)
+    drawn = 0
+    for it in range(max_iter):
+        V = np.kron(Vg, K) + np.kron(Ve, I)
+        Vi = np.linalg.inv(V)
+        ViX = Vi @ Xf
+        info = Xf.T @ ViX
+        P = Vi - ViX @ np.linalg.solve(info, ViX.T)
+        PY = (P @ Y.reshape(-1, order="F")).reshape(n, d, order="F")
+        Qg, Qe = PY.T @ K @ PY, PY.T @ PY
+        if exact_traces:
+            Tg = np.array([[np.trace(P[b * n:(b + 1) * n, a * n:(a + 1) * n] @ K) for b in range(d)]
+                           for a in range(d)])
+            Te = np.array([[np.trace(P[b * n:(b + 1) * n, a * n:(a + 1) * n]) for b in range(d)]
+                           for a in range(d)])
+        else:
+            Z = rademacher(probe_seed, drawn, n, mc_samples * d)
+            drawn += n * mc_samples * d
+            Tg = np.zeros((d, d))
+            Te = np.zeros((d, d))
+            for s_ in range(mc_samples):
+                Zs = Z[:, s_ * d:(s_ + 1) * d]
+                PZ = (P @ Zs.reshape(-1, order="F")).reshape(n, d, order="F")
+                Tg += PZ.T @ (K @ Zs)
+                Te += PZ.T @ Zs
+            Tg /= mc_samples
+            Te /= mc_samples
+        Tg, Te = 0.5 * (Tg + Tg.T), 0.5 * (Te + Te.T)
+        Vg_new = Vg + Vg @ (Qg - Tg) @ Vg / (n - p)
+        Ve_new = Ve + Ve @ (Qe - Te) @ Ve / (n - p)
+        Vg_new, Ve_new = 0.5 * (Vg_new + Vg_new.T), 0.5 * (Ve_new + Ve_new.T)
+        err = (((Vg_new - Vg) ** 2).sum() + ((Ve_new - Ve) ** 2).sum()) / max(1.0, 2.0 * d * d)
+        Vg, Ve = Vg_new, Ve_new
+        if err < tol:
+            return Vg, Ve, it + 1, True
+    return Vg, Ve, max_iter, False
 
 
 def _near_pd(M):

@@ -1725,4 +1725,16 @@ void orc_chisq_prob_vec(const double* stat, int64_t count, int df, double* out, 
     for (int64_t j = 0; j < count; ++j) out[j] = orc_chisq_prob(stat[j], df);
 }
 
+
+// A Rademacher block from std::mt19937_64(seed) through std::uniform_int_distribution<int>(0, 1)
+// (libCosmicCore/src/stcg_vce.cpp:215-216, 249-251): after `skip` draws, column c (c < cols) of
+// the n x cols column-major output takes the next draws c*n .. c*n + n - 1, mapped 1 -> +1,
+// 0 -> -1.  The multi-trait matrix-free REML's probes follow this stream.
+void orc_rademacher(uint64_t seed, int64_t skip, int64_t n, int64_t cols, double* out) {
+    std::mt19937_64 rng(seed);
+    std::uniform_int_distribution<int> bit(0, 1);
+    for (int64_t i = 0; i < skip; ++i) (void)bit(rng);
+    for (int64_t c = 0; c < cols; ++c)
+        for (int64_t i = 0; i < n; ++i) out[i + c * n] = bit(rng) ? 1.0 : -1.0;
+}
 }  // extern "C"

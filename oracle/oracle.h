@@ -204,6 +204,10 @@ void orc_scan_encode_cols(const uint8_t* bed, int64_t stride, int64_t first, int
                           int32_t* pass, double* gsq, int n_threads);
 void orc_chisq_prob_vec(const double* stat, int64_t count, int df, double* out, int n_threads);
 
+/* Rademacher probes from std::mt19937_64(seed) + uniform_int_distribution<int>(0, 1) after
+ * `skip` draws: n x cols column-major, column by column. */
+void orc_rademacher(uint64_t seed, int64_t skip, int64_t n, int64_t cols, double* out);
+
 #ifdef __cplusplus
 }
 #endif
