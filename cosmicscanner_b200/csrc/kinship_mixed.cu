@@ -1057,11 +1057,15 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
         if (pr == 1 && (mode == 0 || tiles % 2 != 0 || num_sms() < 2)) continue;
         if (pr == 0 && mode == 2) continue;
         const int cap_w = rows ? (pr ? kPairRowsW : kRowsW) : (pr ? kPairSamplesW : kSamplesW);
-        int last_kp = -1, last_ct = -1;
+        int last_kc = -1, last_kl = -1, last_ct = -1;
         for (int w = 32; w <= cap_w; w += 16) {
             const Tiling tl = tiling_for(k, w);
-            if (tl.kp == last_kp && tl.n_ctiles == last_ct) continue;  // same tiling as a narrower cap
-            last_kp = (int)tl.kp;
+            // a wider cap that gives the same tiling as a narrower one is the same plan
+            if (tl.kc == last_kc && tl.kc_last == last_kl && tl.n_ctiles == last_ct &&
+                !(pr == (def.pairs ? 1 : 0) && w == def.max_w))
+                continue;
+            last_kc = tl.kc;
+            last_kl = tl.kc_last;
             last_ct = tl.n_ctiles;
             PassPlan p;
             p.pairs = pr == 1;
@@ -1078,6 +1082,9 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
     best.ms_best = 1e30;
     try {
         run(def);  // warm: maps, function attributes, operand buffers
+        bool have_default = false;
+        for (const PassPlan& p : cands) have_default = have_default || (p.pairs == def.pairs && p.max_w == def.max_w);
+        if (!have_default) cands.insert(cands.begin(), def);
         for (const PassPlan& p : cands) {
             CS_CUDA(cudaEventRecord(e0, s));
             run(p);

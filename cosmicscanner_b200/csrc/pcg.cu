@@ -391,6 +391,8 @@ void pcg_solve_block(VOperator& A, double diag, const double* B, int64_t ldb, in
                      double* X, int64_t ldx, double tol, bool relative, int max_iter,
                      PcgWorkspace& ws, PcgStats& st, cudaStream_t s, LowRankPreconditioner* M) {
     st.iterations.assign(k, 0);
+    st.sweeps = 0;  // counts of this solve only
+    st.column_iterations = 0;
     if (k <= 0) return;
     const int64_t n = A.rm->n_rec;
     CS_CUDA(cudaMemset2DAsync(X, ldx * 8, 0, k * 8, n, s));
