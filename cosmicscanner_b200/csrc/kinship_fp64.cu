@@ -24,6 +24,9 @@ namespace cs {
 void decode_dmma_fp64(bool rows_pass, const cs_packed_view& v, const double* lut, const double* in,
                       int64_t ldi, int64_t k, double* out, int64_t ldo, double scale,
                       Workspace& ws, cudaStream_t s, int64_t max_splits);
+void decode_narrow_fp64(bool rows_pass, const cs_packed_view& v, const double* lut,
+                        const double* in, int64_t ldi, int64_t k, double* out, int64_t ldo,
+                        double scale, Workspace& ws, cudaStream_t s);
 
 namespace {
 
@@ -341,11 +344,26 @@ int64_t dmma_min_columns() {
     return v;
 }
 
+// The decode-GEMV form for up to 4 right-hand sides (CS_B200_FP64_NARROW=0 keeps the tile
+// kernels).  It needs a partials workspace, so the single-slice (workspace-free) callers keep
+// the tile kernels.
+bool narrow_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("CS_B200_FP64_NARROW");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 template <bool ROWS>
 void dispatch(const cs_packed_view& v, const double* lut, const double* in, int64_t ldi,
               int64_t k, double* out, int64_t ldo, double scale, Workspace& ws, cudaStream_t s,
               int64_t max_splits = 64) {
     if (k <= 0) return;
+    if (k <= 4 && max_splits > 1 && narrow_enabled()) {
+        decode_narrow_fp64(ROWS, v, lut, in, ldi, k, out, ldo, scale, ws, s);
+        return;
+    }
     if (k >= dmma_min_columns()) {
         decode_dmma_fp64(ROWS, v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
         return;

@@ -119,3 +119,25 @@ def test_larger_random_matrix():
         X = rng.standard_normal((op.rows(), 70))
         compare(op.apply(X), ref.apply_block(X, kp, vp, n_threads=8))
         assert abs(op.trace() - ref.trace(kp, vp)) < 1e-9 * abs(ref.trace(kp, vp))
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 4])
+def test_narrow_fp64_apply(k):
+    """One to four right-hand sides take the decode-GEMV passes (every thread keeps its run of
+    samples' values in registers): same result as the oracle, ragged sample counts across
+    CTA chunks, a sample subset and a variant selection, bitwise repeatable."""
+    synth = pytest.importorskip("cosmicscanner_b200.synth")
+    d = synth.cohort(9000, 2100, 91, missing=0.02, n_causal=10)
+    ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    rng = np.random.default_rng(k)
+    keep = np.sort(rng.choice(d["n"], 8301, replace=False)).astype(np.int32)
+    variants = np.sort(rng.choice(d["m"], 1900, replace=False)).astype(np.int32)
+    for kp, vs in ((None, None), (keep, variants)):
+        op = cs.createKinshipOperator(g, kp, vs)
+        X = rng.standard_normal((op.rows(), k))
+        E = ref.apply_block(X, kp, vs, n_threads=8)
+        Y = op.apply(X)
+        assert (np.abs(Y - E).max(axis=0) / np.abs(E).max(axis=0)).max() < 1e-12
+        assert np.array_equal(op.apply(X), Y)
+        op.close()
