@@ -279,6 +279,15 @@ void decode_dmma_fp64(bool rows_pass, const cs_packed_view& v, const double* lut
                       int64_t ldi, int64_t k, double* out, int64_t ldo, double scale,
                       Workspace& ws, cudaStream_t s, int64_t max_splits) {
     if (k <= 0) return;
+    if (k > 128 && k % 128 != 0) {
+        // whole 128-column tiles, then the remainder in a narrower tile (k = 266: 2 x 128 + 32
+        // instead of 3 x 128, a third less padding)
+        const int64_t full = k / 128 * 128;
+        decode_dmma_fp64(rows_pass, v, lut, in, ldi, full, out, ldo, scale, ws, s, max_splits);
+        decode_dmma_fp64(rows_pass, v, lut, in + full, ldi, k - full, out + full, ldo, scale, ws,
+                         s, max_splits);
+        return;
+    }
     if (rows_pass) {
         if (k <= 32) launch_dmma<true, 32>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
         else if (k <= 64) launch_dmma<true, 64>(v, lut, in, ldi, k, out, ldo, scale, ws, s, max_splits);
