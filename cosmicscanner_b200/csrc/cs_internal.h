@@ -77,9 +77,11 @@ constexpr int64_t kRowAlign = 64;
 // block (the same guarantee cudaFree gives).
 void* device_alloc(size_t bytes);
 void device_free(void* p) noexcept;
-// For threads that synchronise their own streams before any buffer is released (the request
-// workers of the serving loop): frees then skip the device-wide synchronisation.
-void set_thread_owns_its_streams(bool on);
+// For a thread whose device work all runs on one stream of its own (a request worker of the
+// serving loop): the thread's frees are ordered on that stream (cudaFreeAsync there) instead of
+// waiting for the whole device, so a buffer is only reused after the work queued before its
+// release has finished.  nullptr restores the device-wide synchronisation.
+void set_thread_free_stream(cudaStream_t s);
 
 // Device allocation that frees itself.
 template <typename T>

@@ -57,16 +57,20 @@ cusolverDnHandle_t shared_solver() {
 }
 
 namespace {
-thread_local bool g_free_without_device_sync = false;
+thread_local cudaStream_t g_free_stream = nullptr;
 }
 
-void set_thread_owns_its_streams(bool on) { g_free_without_device_sync = on; }
+void set_thread_free_stream(cudaStream_t s) { g_free_stream = s; }
 
 void device_free(void* p) noexcept {
     if (!p) return;
-    // A thread that synchronises its own (non-blocking) streams before releasing buffers
-    // frees without stalling the other threads' work on the device.
-    if (!g_free_without_device_sync) cudaDeviceSynchronize();
+    if (g_free_stream) {
+        // ordered after the work this thread queued on its stream (the pool reuses the block
+        // only once the free has executed)
+        cudaFreeAsync(p, g_free_stream);
+        return;
+    }
+    cudaDeviceSynchronize();
     cudaFreeAsync(p, 0);
 }
 

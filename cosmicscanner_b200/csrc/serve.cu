@@ -279,11 +279,11 @@ void cs_server::dispatch_loop() {
 
 void cs_server::run_request(Request* r) {
     cudaSetDevice(device);
-    cs::set_thread_owns_its_streams(true);
     cudaStream_t st = nullptr;
     std::string err;
     try {
         CS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        cs::set_thread_free_stream(st);
         const int64_t n = (int64_t)r->samples.size();
         cs::DeviceBuffer<int32_t> d_rows;
         d_rows.resize(n);
@@ -350,6 +350,7 @@ void cs_server::run_request(Request* r) {
     } catch (const std::exception& e) {
         err = e.what();
     }
+    cs::set_thread_free_stream(nullptr);
     if (st) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
