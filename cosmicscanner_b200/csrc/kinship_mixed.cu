@@ -1,29 +1,43 @@
 // Tensor-core (mixed-precision) form of the kinship operator Y = Z Z^T X / M.
 //
 // Arithmetic.  Both passes run on tcgen05.mma kind::i8 with exact int32 accumulation:
-//  * the genotype tile enters as int8 dosages G in {0, 1, 2} (missing -> 0) together with
-//    an int8 missing-indicator tile, both decoded from the packed 2-bit rows in shared
-//    memory (a 128-SNP x 128-sample tile, 128-byte swizzled);
+//  * the genotype tile enters as int8 imputed codes e = Q G in {0, Q, 2Q} (Q = 63) for
+//    observed calls and e = q_t = rint(Q mu_t) for missing ones, so that e / Q is the
+//    mean-imputed dosage up to the row's residual r_t = mu_t - q_t / Q (|r_t| <= 1 / 2Q),
+//    together with an int8 missing-indicator tile, both decoded from the packed 2-bit rows in
+//    shared memory (a 128-SNP x 128-sample tile, 128-byte swizzled) through a per-row
+//    byte-permute table;
 //  * right-hand sides are quantised per column into three int8 pieces (base 254) after
 //    centring: x' = (x - mean) * 127 / max|x - mean| ~ q1 + q2/254 + q3/254^2, i.e. about
 //    23 significant bits, so the only rounding is this quantisation (~6e-8 of the column
-//    maximum per element); all products and sums up to 2^31 are exact.
+//    maximum per element); products and sums are exact while a K slice holds at most
+//    kMaxKbPerAccum K-blocks (|e q| <= 126 * 127 per element, plus 127 for the residual).
+// With G_ti + mu_t miss_ti = e_ti / Q + r_t miss_ti, the residual term carries the factor
+// |r_t| <= 1/126, so two pieces of its operand match the precision of the main term's three:
+// per missing call the residual's rounding is at most 1.6e-5 (rows pass) / 3.1e-5 (samples
+// pass) of a first-piece step, against up to 1.55e-5 per element for the main term's own.
+// Five operand sets per K-block instead of the six of a separate dosage and missing-call
+// product.
 // Rows pass (U = Z^T X): with S_t, n_t the exact allele sum and observed count of row t,
-//   u_t / s_t = mean * (S_t - mu_t n_t) + ( sum_i G_ti x'_i + mu_t sum_{i missing} x'_i
+//   u_t / s_t = mean * (S_t - mu_t n_t) + ( sum_i e_ti x'_i / Q + r_t sum_{i missing} x'_i
 //               - mu_t sum_i x'_i ) / scale
 // (the centring identity of src/kinship_operator.cpp:135 with the missing-call terms split
 // out).  Samples pass (Y = Z W / M, W = s o U):
-//   y_i = ( sum_t G_ti w_t + sum_t miss_ti mu_t w_t - sum_t mu_t w_t ) / M
-// with W and (mu o W) quantised the same way.  Each pass is one MMA of the dosage tile
-// against the pieces plus one of the missing-indicator tile (same pieces in the rows pass,
-// the (mu o W) pieces in the samples pass).
+//   y_i = ( sum_t e_ti w_t / Q + sum_t miss_ti r_t w_t - sum_t mu_t w_t ) / M
+// with W f and (Q r o W) f quantised with one factor f = 127 / max|w| (|Q r_t| <= 1/2 keeps
+// the second operand's first piece within 64), three pieces of the first and two of the
+// second accumulating into the same TMEM columns.  Each pass is one MMA of the imputed-code
+// tile against three pieces (N = 3 kc) plus one of the missing-indicator tile against two
+// (N = 2 kc): the first two pieces of the same operand in the rows pass (own accumulator,
+// scaled by r_t in the epilogue), the residual pieces in the samples pass.
 //
 // Kernel structure (one CTA per SM, 15 warps): warp 14 issues TMA loads of the packed
 // tiles (from HBM) into a deep ring of their own, warp 0 those of the quantised pieces (L2
 // resident) into a ring of stages; warps 2-9 decode; warp 1 issues the MMAs from one thread
-// into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.  The decoded tile (SNP rows x samples) serves as a K-major A
-// operand in the rows pass and as an MN-major A operand in the samples pass.  Every wait
-// is bounded; a timeout leaves a status code that the host reports as an error.
+// into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.
+// The decoded tile (SNP rows x samples) serves as a K-major A operand in the rows pass and
+// as an MN-major A operand in the samples pass.  Every wait is bounded; a timeout leaves a
+// status code that the host reports as an error.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -48,7 +62,7 @@ using namespace sm100;
 
 constexpr int kTile = 128;        // MMA M, and SNP rows / samples per decoded tile
 constexpr int kKBlock = 128;      // K elements (int8) per stage: one 128-byte swizzle row
-constexpr int kMaxKc = 80;        // column-tile width cap (TMEM: rows pass 6 x 80 columns)
+constexpr int kMaxKc = 80;        // column-tile width cap (MMA N = 3 kc <= 256)
 constexpr int kWarps = 15;
 constexpr int kThreads = kWarps * 32;
 constexpr int kDecodeWarp0 = 2, kDecodeWarps = 8;
@@ -56,39 +70,53 @@ constexpr int kEpiWarp0 = 10;
 constexpr int kPackedWarp = 14;
 constexpr uint32_t kTmemCols = 512;
 constexpr double kBase = 254.0;
+constexpr int kImputeQ = 63;          // dosage scale of the imputed-code tile
+constexpr int kMaxKbPerAccum = 1024;  // K-blocks one int32 accumulation may hold:
+                                      // 1024 * 128 * (126 * 127 + 127) < 2^31
 
 constexpr int kATileBytes = kTile * kKBlock;     // 16 KB
 constexpr int kPackedBytes = kTile * 32;         // 128 rows x 32 B
 
-// Shared memory: a ring of decoded tiles {dosages, missing indicators}, a deep ring of
+// Shared memory: a ring of decoded tiles {imputed codes, missing indicators}, a deep ring of
 // packed tiles (HBM latency is the longest, so they are requested furthest ahead) and a ring
 // of B stages (the quantised pieces, re-read by every CTA from L2).  The rows pass has 3 B
-// pieces and two accumulators of 3 kc TMEM columns (main and missing-call sums kept apart);
-// the samples pass has 6 B pieces (W and mu o W with one scale) and one accumulator of 3 kc
-// columns, double-buffered.
+// pieces and accumulators of 3 kc + 2 kc TMEM columns (main and missing-call sums kept
+// apart); the samples pass has 5 B pieces (W and Q r o W with one scale) and one accumulator
+// of 3 kc columns, double-buffered.
 //
 // CTA pairs (cta_group::2): a cluster of two CTAs shares each MMA, M = 256 rows (128 from
 // each CTA's decoded tile) by N = 3 kc, and each CTA holds only half of the B pieces (rows
-// [1.5 kc r, 1.5 kc (r + 1)) of every 3 kc-row set, r = CTA rank).  The tensor core then
+// [1.5 kc r, 1.5 kc (r + 1)) of the 3 kc-row set, r = CTA rank).  The tensor core then
 // reads half the B bytes per MAC from each SM's shared memory, which is what bounds the
 // single-CTA MMAs (about 68 bytes of operands per clock per SM); the smaller B stages leave
 // room for wider column tiles and a deeper decode ring, which covers the extra hop of the
 // cross-CTA handshakes.
+// Narrow single-CTA layouts (column tiles of at most 32): the small B stages leave room for
+// a decode ring twice as deep and, in the rows pass, a second accumulator, for widths where the
+// MMAs are short and the per-K-block handshakes set the pace.
 // Pipeline depths {column-tile width cap, B stages, packed stages, decode stages}:
 constexpr int kRowsW = 80, kRowsST = 4, kRowsSP = 8, kRowsSD = 2;
 constexpr int kSamplesW = 48, kSamplesST = 3, kSamplesSP = 12, kSamplesSD = 2;
 constexpr int kPairRowsW = 80, kPairRowsST = 4, kPairRowsSP = 8, kPairRowsSD = 4;
 constexpr int kPairSamplesW = 80, kPairSamplesST = 3, kPairSamplesSP = 6, kPairSamplesSD = 3;
+constexpr int kNarrowRowsW = 32, kNarrowRowsST = 4, kNarrowRowsSP = 8, kNarrowRowsSD = 4;
+static_assert(kNarrowRowsW == 32, "the plans use one narrow width for both passes");
+constexpr int kNarrowSamplesW = 32, kNarrowSamplesST = 3, kNarrowSamplesSP = 8, kNarrowSamplesSD = 4;
 
-template <bool ROWS, bool PAIR>
+template <bool ROWS, bool PAIR, bool NARROW = false>
 struct Layout {
-    static constexpr int kPieces = ROWS ? 3 : 6;  // per column tile, over the pair
-    static constexpr int kMaxW = PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
-    static constexpr int kAccCols = ROWS ? 6 * kMaxW : 3 * kMaxW;
-    static constexpr int kAccBufs = ROWS ? 1 : 2;
+    static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
+    static constexpr int kPieces = ROWS ? 3 : 5;  // per column tile, over the pair
+    static constexpr int kMaxW = NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
+                                 : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
+    static constexpr int kTmaStages = NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
+                                      : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
+    static constexpr int kPackedStages = NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
+                                         : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
+    static constexpr int kDecodeStages = NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
+                                         : PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
+    static constexpr int kAccCols = ROWS ? 5 * kMaxW : 3 * kMaxW;
+    static constexpr int kAccBufs = (ROWS && !NARROW) ? 1 : 2;
     static constexpr uint32_t kAccStride = 256;
     static constexpr int kBBytes = kPieces * kMaxW * 128 / (PAIR ? 2 : 1);  // this CTA's share
     static constexpr int kTmaBytes = kBBytes;
@@ -111,7 +139,7 @@ struct Layout {
     }
     static_assert(kSmem <= 227 * 1024, "mixed pass exceeds shared memory");
     static_assert(kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
-    static_assert(ROWS ? kAccCols <= (int)kTmemCols : kAccCols <= (int)kAccStride,
+    static_assert(kAccBufs == 1 ? kAccCols <= (int)kTmemCols : kAccCols <= (int)kAccStride,
                   "accumulators exceed TMEM");
     static_assert(kMaxW % 16 == 0 && kMaxW <= kMaxKc, "column tiles are multiples of 16, at most 80");
 };
@@ -121,23 +149,25 @@ struct PassArgs {
     int kb_total, kb_per_split;  // K-blocks of the contraction, per slice
     int kc, kp;                  // column tile width, padded column count
     int kc_last;                 // width of the last column tile (a multiple of 16, <= kc)
-    const double* mu;            // rows pass: mu_t per SNP row (epilogue)
-    const double* inv_f;         // samples pass: 1 / quantisation factor per column
+    const uint32_t* lut;         // per SNP row: imputed code of each 2-bit code (byte-permute table)
+    const double* resid;         // rows pass: r_t = mu_t - q_t / Q per SNP row (epilogue)
+    const double* inv_f;         // samples pass: 1 / (Q f) per column
     double* part;                // [n_splits][kp][ld] FP64 slice partials
     int64_t ld;                  // padded output rows
     int* status;
 };
 
-// 16 codes (one 32-bit word, code j in bits 2j..2j+1) -> 16 int8 dosages and 16 missing
-// indicators in the interleaved sample order 0 2 4 .. 14 1 3 .. 15 within the group: the
-// even codes, masked in place, are already byte-permute selectors (one nibble each), and
-// so are the odd codes after one shift.  sample_at(p) / position_of(s) convert.
-__device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint4& dos, uint4& mis) {
+// 16 codes (one 32-bit word, code j in bits 2j..2j+1) -> 16 int8 imputed codes (byte c of
+// the row's table `lut` for code c) and 16 missing indicators in the interleaved sample order
+// 0 2 4 .. 14 1 3 .. 15 within the group: the even codes, masked in place, are already
+// byte-permute selectors (one nibble each), and so are the odd codes after one shift.
+// sample_at(p) / position_of(s) convert.
+__device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint32_t lut, uint4& dos, uint4& mis) {
     const uint32_t se = w & 0x33333333u, so = (w >> 2) & 0x33333333u;
-    dos.x = __byte_perm(0x00010002u, 0u, se);
-    dos.y = __byte_perm(0x00010002u, 0u, se >> 16);
-    dos.z = __byte_perm(0x00010002u, 0u, so);
-    dos.w = __byte_perm(0x00010002u, 0u, so >> 16);
+    dos.x = __byte_perm(lut, 0u, se);
+    dos.y = __byte_perm(lut, 0u, se >> 16);
+    dos.z = __byte_perm(lut, 0u, so);
+    dos.w = __byte_perm(lut, 0u, so >> 16);
     mis.x = __byte_perm(0x00000100u, 0u, se);
     mis.y = __byte_perm(0x00000100u, 0u, se >> 16);
     mis.z = __byte_perm(0x00000100u, 0u, so);
@@ -147,11 +177,11 @@ __device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint4& dos, 
 __host__ __device__ __forceinline__ int sample_at(int p) { return p < 8 ? 2 * p : 2 * (p - 8) + 1; }
 __host__ __device__ __forceinline__ int position_of(int s) { return (s & 1) ? 8 + (s >> 1) : s >> 1; }
 
-template <bool ROWS, bool PAIR>
+template <bool ROWS, bool PAIR, bool NARROW>
 __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
-    using L = Layout<ROWS, PAIR>;
+    using L = Layout<ROWS, PAIR, NARROW>;
     constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -255,17 +285,28 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                     if (!(ok = wait_commit(&empty_t[s], ((j / ST) & 1) ^ 1, kTimeoutTma))) break;
                     mbar_arrive_expect_tx(&full_t[s], bytes);
                     if (PAIR) {
-                        // half-pieces [p0a p0b p1a p1b p2a p2b] of each set (w / 2 rows each):
-                        // this CTA loads 3 r .. 3 r + 2
-                        const int hw = w / 2;
+                        const int hw = w / 2;  // rows of one half-piece
+                        if (ROWS) {
+                            // half r of each piece, [p0(r) p1(r) p2(r)]: the missing-call MMA
+                            // (N = 2 w) then finds [p0(r) p1(r)] at the start of each CTA's stage
 #pragma unroll
-                        for (int set = 0; set < L::kPieces / 3; ++set)
+                            for (int c = 0; c < 3; ++c)
+                                tma_load_2d(smem + L::b(s) + c * hw * 128, mb, kb * kKBlock,
+                                            c * kp + ct * kc + (int)rank * hw, &full_t[s]);
+                        } else {
+                            // main set: half-pieces [p0a p0b p1a p1b p2a p2b], this CTA loads
+                            // 3 r .. 3 r + 2; residual set: piece 3 + r whole
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
                                 const int h = 3 * (int)rank + c, q = h >> 1;
-                                tma_load_2d(smem + L::b(s) + (set * 3 + c) * hw * 128, mb, kb * kKBlock,
-                                            (set * 3 + q) * kp + ct * kc + (h & 1) * hw, &full_t[s]);
+                                tma_load_2d(smem + L::b(s) + c * hw * 128, mb, kb * kKBlock,
+                                            q * kp + ct * kc + (h & 1) * hw, &full_t[s]);
                             }
+#pragma unroll
+                            for (int c = 0; c < 2; ++c)
+                                tma_load_2d(smem + L::b(s) + (3 + c) * hw * 128, mb, kb * kKBlock,
+                                            (3 + (int)rank) * kp + ct * kc + c * hw, &full_t[s]);
+                        }
                     } else {
                         for (int q = 0; q < L::kPieces; ++q)
                             tma_load_2d(smem + L::b(s) + q * w * 128, mb, kb * kKBlock,
@@ -282,7 +323,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         if ((!PAIR || rank == 0) && elect_one()) {
             // s8 x s8 -> s32; rows pass: K-major A (SNP rows x samples); samples pass:
             // MN-major A (the same tile read as samples x SNPs); N = 3 w (the three pieces
-            // of a column tile side by side), M = 128 (pair: 256)
+            // of a column tile side by side) for the imputed codes and 2 w for the missing
+            // indicators, M = 128 (pair: 256)
             const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
                                     ((uint32_t)((PAIR ? 2 : 1) * kTile >> 4) << 24);
             uint32_t j = 0;
@@ -293,6 +335,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 const int w = width(ct);
                 const uint32_t idesc = idesc0 | ((uint32_t)((3 * w) >> 3) << 17);
+                const uint32_t idesc_m = idesc0 | ((uint32_t)((2 * w) >> 3) << 17);
                 const int buf = ui % NB;
                 if (!(ok = wait_peer(&acc_empty[buf], ((ui / NB) & 1) ^ 1, kTimeoutMma))) break;
                 tc_fence_after();
@@ -306,7 +349,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                     const uint32_t a = smem_addr(smem + L::a(d));
                     const uint32_t am = smem_addr(smem + L::am(d));
                     const uint32_t b = smem_addr(smem + L::b(s));
-                    // samples pass: the (mu o W) set follows the W set (this CTA's share)
+                    // rows pass: the first two pieces (this CTA's halves of them); samples
+                    // pass: the residual set after the W set (this CTA's share)
                     const uint32_t bm = ROWS ? b : b + 3 * w * 128 / (PAIR ? 2 : 1);
 #pragma unroll
                     for (int ks = 0; ks < kKBlock / 32; ++ks) {
@@ -316,13 +360,14 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                         const uint64_t dm = smem_desc_sw128(am + aoff, 16, 1024);
                         const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
                         const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
-                        // rows pass: separate missing-call sums; samples pass: same columns
+                        // rows pass: separate missing-call sums; samples pass: the first two
+                        // piece columns of the same accumulator
                         if (PAIR) {
                             mma_i8_pair(acc_main, da, db, idesc, first);
-                            mma_i8_pair(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
+                            mma_i8_pair(acc_miss, dm, dbm, idesc_m, ROWS ? first : 1u);
                         } else {
                             mma_i8(acc_main, da, db, idesc, first);
-                            mma_i8(acc_miss, dm, dbm, idesc, ROWS ? first : 1u);
+                            mma_i8(acc_miss, dm, dbm, idesc_m, ROWS ? first : 1u);
                         }
                     }
                     if (PAIR) {
@@ -357,8 +402,12 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         for (int u = u0; u < units && ok; u += ustep) {
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
+            // the row's imputed-code table: rows pass SNP tile * 128 + r, samples pass
+            // kb * 128 + r (the packed tile's row)
+            uint32_t lut = ROWS ? __ldg(P.lut + (int64_t)tile * kTile + r) : 0u;
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
                 const int sp = j % SP, d = j % SD;
+                if (!ROWS) lut = __ldg(P.lut + (int64_t)kb * kKBlock + r);
                 if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
                 if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
                 const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
@@ -368,7 +417,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
 #pragma unroll
                 for (int cj = 0; cj < 4; ++cj) {
                     uint4 dos, mis;
-                    decode_word_interleaved(words[cj], dos, mis);
+                    decode_word_interleaved(words[cj], lut, dos, mis);
                     const int chunk = 4 * h + cj;  // 16 samples per 16-byte chunk
                     const int off = rbase + ((chunk ^ (r & 7)) << 4);
                     *reinterpret_cast<uint4*>(a + off) = dos;
@@ -432,29 +481,44 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             const int lp = 32 * q + lane;
             const int64_t row = (int64_t)tile * kTile + (ROWS ? lp : (lp & ~15) + sample_at(lp & 15));
             const uint32_t tb = tmem_base + buf * L::kAccStride + ((uint32_t)(32 * q) << 16);
-            const double mu = ROWS ? P.mu[row] : 0.0;
             const int w = width(ct);
             double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
-            for (int c0 = 0; c0 < w; c0 += 16) {
-                int32_t m1[16], m2[16], m3[16];
-                tmem_ld16i(tb + c0, m1);
-                tmem_ld16i(tb + w + c0, m2);
-                tmem_ld16i(tb + 2 * w + c0, m3);
-                if (ROWS) {
+            if (ROWS) {
+                // TMEM columns: single CTA [p0 p1 p2 | m0 m1] (w each); pair, w / 2 = hw each,
+                // [p0a p1a p2a p0b p1b p2b | m0a m1a m0b m1b] (half a from the leader's B)
+                constexpr int CH = PAIR ? 8 : 16;
+                const double rt = P.resid[row];
+                const double inv_q = 1.0 / (double)kImputeQ;
+                const int hw = w / 2;
+                for (int c0 = 0; c0 < w; c0 += CH) {
+                    const bool hb = PAIR && c0 >= hw;
+                    const int cc = hb ? c0 - hw : c0;
+                    const int step = PAIR ? hw : w;
+                    const uint32_t cm = PAIR ? (hb ? 3 * hw : 0) + cc : c0;
+                    const uint32_t cx = 3 * w + (PAIR ? (hb ? 2 * hw : 0) + cc : c0);
+                    int32_t m1[CH], m2[CH], m3[CH];
+                    tmem_ld_cols<CH>(tb + cm, m1);
+                    tmem_ld_cols<CH>(tb + cm + step, m2);
+                    tmem_ld_cols<CH>(tb + cm + 2 * step, m3);
                     // main sums first, then the missing-call sums (fewer live registers)
-                    double mv[16];
+                    double mv[CH];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
+                    for (int i = 0; i < CH; ++i)
                         mv[i] = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
-                    tmem_ld16i(tb + 3 * w + c0, m1);
-                    tmem_ld16i(tb + 4 * w + c0, m2);
-                    tmem_ld16i(tb + 5 * w + c0, m3);
+                    tmem_ld_cols<CH>(tb + cx, m1);
+                    tmem_ld_cols<CH>(tb + cx + step, m2);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const double xv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
-                        dst[(int64_t)(c0 + i) * P.ld] = mv[i] + mu * xv;
+                    for (int i = 0; i < CH; ++i) {
+                        const double xv = (double)m1[i] + (double)m2[i] * ib;
+                        dst[(int64_t)(c0 + i) * P.ld] = mv[i] * inv_q + rt * xv;
                     }
-                } else {
+                }
+            } else {
+                for (int c0 = 0; c0 < w; c0 += 16) {
+                    int32_t m1[16], m2[16], m3[16];
+                    tmem_ld16i(tb + c0, m1);
+                    tmem_ld16i(tb + w + c0, m2);
+                    tmem_ld16i(tb + 2 * w + c0, m3);
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const double mv = (double)m1[i] + (double)m2[i] * ib + (double)m3[i] * ib2;
@@ -505,6 +569,13 @@ __device__ __forceinline__ double quantise3(double v, int8_t& q1, int8_t& q2, in
     q2 = (int8_t)b;
     q3 = (int8_t)c;
     return a + b / kBase + c / (kBase * kBase);
+}
+
+// Two int8 pieces of base 254 (the residual operand of the samples pass, |v| <= 63.5).
+__device__ __forceinline__ void quantise2(double v, int8_t& q1, int8_t& q2) {
+    const double a = rint(v);
+    q1 = (int8_t)a;
+    q2 = (int8_t)rint((v - a) * kBase);
 }
 
 __device__ __forceinline__ double quant_factor(unsigned long long bits) {
@@ -640,21 +711,20 @@ k_split_rows_operand(const double* __restrict__ X, int64_t ld, int64_t n, int64_
 // Rows-pass reduction, one column per blockIdx.y and 2048 rows per blockIdx.x:
 //   inner_tc = (sum_z part[z][c][t] - mu_t Q_c) / f_c + mean_c exc_t
 // out = inner * s_t^spow written column-major (out[c * out_ld + t]) or row-major
-// (out[t * out_ld + c]); optional maxima of |out| and |mu out| per column.
+// (out[t * out_ld + c]); optional maxima of |out| per column.
 __global__ void __launch_bounds__(256)
 k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t ld, int64_t R,
               int64_t k, const double* __restrict__ s_row, int spow,
               const double* __restrict__ exc_row, const double* __restrict__ mu,
               const double* __restrict__ mean, const double* __restrict__ qsum,
               const unsigned long long* __restrict__ maxbits_in, double* __restrict__ out,
-              int64_t out_ld, int colmajor, unsigned long long* __restrict__ max_w,
-              unsigned long long* __restrict__ max_muw) {
-    __shared__ double red_w[8], red_m[8];
+              int64_t out_ld, int colmajor, unsigned long long* __restrict__ max_w) {
+    __shared__ double red_w[8];
     const int64_t c = blockIdx.y;
     const double f = quant_factor(maxbits_in[c]);
     const double inv_f = f > 0.0 ? 1.0 / f : 0.0;
     const double mc = mean[c], qc = qsum[c];
-    double mw = 0.0, mm = 0.0;
+    double mw = 0.0;
     const int64_t t0 = (int64_t)blockIdx.x * 2048;
     for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) {
         double acc = 0.0;
@@ -667,52 +737,41 @@ k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t l
         if (colmajor) out[c * out_ld + t] = v;
         else out[t * out_ld + c] = v;
         mw = fmax(mw, fabs(v));
-        mm = fmax(mm, fabs(mu[t] * v));
     }
     if (max_w) {
-        for (int off = 16; off; off >>= 1) {
-            mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
-            mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, off));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            red_w[threadIdx.x >> 5] = mw;
-            red_m[threadIdx.x >> 5] = mm;
-        }
+        for (int off = 16; off; off >>= 1) mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
+        if ((threadIdx.x & 31) == 0) red_w[threadIdx.x >> 5] = mw;
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int j = 1; j < 8; ++j) {
-                mw = fmax(mw, red_w[j]);
-                mm = fmax(mm, red_m[j]);
-            }
+            for (int j = 1; j < 8; ++j) mw = fmax(mw, red_w[j]);
             atomicMax(max_w + c, (unsigned long long)__double_as_longlong(mw));
-            atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(mm));
         }
     }
 }
 
-// Samples-pass operand from W^T (column-major, k x R): pieces of W f (rows q kp + c) and of
-// (mu o W) f (rows (3 + q) kp + c), t < r_pad, with ONE factor f = 127 / max(|W|, |mu W|)
-// per column so that both MMAs accumulate into the same TMEM columns; 1/f per column; and
-// per-block sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].
+// Samples-pass operand from W^T (column-major, k x R): three pieces of W f (rows q kp + c)
+// and two of (Q r o W) f (rows (3 + q) kp + c), t < r_pad, with ONE factor f = 127 / max|W|
+// per column so that both MMAs accumulate into the same TMEM columns (|Q r_t| <= 1/2); 1/(Q f)
+// per column; and per-block sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].
 // Grid: (r_pad / 2048, kp).
 __global__ void __launch_bounds__(256)
 k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int64_t kp,
                         int64_t r_pad, const double* __restrict__ mu,
-                        const unsigned long long* __restrict__ max_w,
-                        const unsigned long long* __restrict__ max_muw, int8_t* __restrict__ B,
+                        const double* __restrict__ resid,
+                        const unsigned long long* __restrict__ max_w, int8_t* __restrict__ B,
                         double* __restrict__ inv_f, double* __restrict__ cpart) {
     __shared__ double red[8];
     const int64_t c = blockIdx.y;
-    const double f = c < k ? quant_factor(max(max_w[c], max_muw[c])) : 0.0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) inv_f[c] = f > 0.0 ? 1.0 / f : 0.0;
+    const double f = c < k ? quant_factor(max_w[c]) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) inv_f[c] = f > 0.0 ? 1.0 / (f * kImputeQ) : 0.0;
     double cs = 0.0;
     const int64_t t0 = (int64_t)blockIdx.x * 2048;
     for (int64_t t = t0 + threadIdx.x; t < min(r_pad, t0 + 2048); t += 256) {
-        int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0;
+        int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0;
         if (c < k && t < R) {
             const double w = Wt[c * R + t];
             quantise3(w * f, a1, a2, a3);
-            quantise3(mu[t] * w * f, b1, b2, b3);
+            quantise2(kImputeQ * resid[t] * w * f, b1, b2);
             cs += mu[t] * w;
         }
         B[c * r_pad + t] = a1;
@@ -720,7 +779,6 @@ k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int
         B[(2 * kp + c) * r_pad + t] = a3;
         B[(3 * kp + c) * r_pad + t] = b1;
         B[(4 * kp + c) * r_pad + t] = b2;
-        B[(5 * kp + c) * r_pad + t] = b3;
     }
     for (int off = 16; off; off >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cs;
@@ -799,6 +857,14 @@ int pair_mode() {
     }();
     return mode;
 }
+// The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
+bool narrow_layouts() {
+    static const bool on = [] {
+        const char* v = std::getenv("CS_B200_NARROW");
+        return !(v && std::strcmp(v, "0") == 0);
+    }();
+    return on;
+}
 bool use_cta_pairs(int64_t k) {
     const int mode = pair_mode();
     return mode != 0 && (mode == 2 || k >= kPairMinColumns) && num_sms() >= 2;
@@ -808,10 +874,12 @@ int blocks_for(int64_t work) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 16LL * num_sms()));
 }
 
-// Number of K slices so that about `target` work units cover the GPU.
+// Number of K slices so that about `target` work units cover the GPU, and at least enough that
+// no slice holds more than kMaxKbPerAccum K-blocks (the int32 accumulators' exact range).
 int choose_splits(int64_t units_per_split, int kb_total, int64_t target) {
     int64_t s = (target + units_per_split - 1) / units_per_split;
     s = std::max<int64_t>(1, std::min<int64_t>(s, std::max(1, kb_total / 8)));
+    s = std::max<int64_t>(s, (kb_total + kMaxKbPerAccum - 1) / kMaxKbPerAccum);
     return (int)s;
 }
 
@@ -820,14 +888,15 @@ int choose_splits(int64_t units_per_split, int kb_total, int64_t target) {
 struct MixedRows {
     // a packed view with per-row centring statistics, ready for the rows pass
     int64_t R = 0, n = 0, r_pad = 0, n_pad = 0;
-    DeviceBuffer<double> mu, exc, s;
+    DeviceBuffer<double> mu, exc, s, resid;
+    DeviceBuffer<uint32_t> lut;  // imputed code of each 2-bit code, one byte per code
     CUtensorMap tm{};
 };
 
 struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
-    DeviceBuffer<unsigned long long> max1, max_w, max_muw;
+    DeviceBuffer<unsigned long long> max1, max_w;
     CUtensorMap tm_b1{}, tm_b2{};
     CUtensorMap tm_b1t{}, tm_b2t{};  // boxes of the last column tile's width
     const void* tm_b1_base = nullptr;
@@ -846,10 +915,11 @@ void destroy_mixed(MixedOperator* m) { delete m; }
 
 namespace {
 
-template <bool ROWS, bool PAIR>
+template <bool ROWS, bool PAIR, bool NARROW = false>
 cudaError_t allow_smem() {
-    return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Layout<ROWS, PAIR>::kSmem);
+    return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR, NARROW>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                Layout<ROWS, PAIR, NARROW>::kSmem);
 }
 
 void configure_kernels() {
@@ -859,6 +929,8 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<false, false>();
         if (err == cudaSuccess) err = allow_smem<true, true>();
         if (err == cudaSuccess) err = allow_smem<false, true>();
+        if (err == cudaSuccess) err = allow_smem<true, false, true>();
+        if (err == cudaSuccess) err = allow_smem<false, false, true>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -885,14 +957,14 @@ int resident_pairs() {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true>, &cfg));
+        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true, false>, &cfg));
         n = std::max(1, std::min(clusters, num_sms() / 2));
     }
     return n;
 }
 
 // One CTA per SM, or (PAIR) as many clusters of two CTAs as are resident together.
-template <bool ROWS, bool PAIR>
+template <bool ROWS, bool PAIR, bool NARROW = false>
 void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
                  const PassArgs& P, cudaStream_t s) {
     if (PAIR) {
@@ -908,14 +980,17 @@ void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true>, ta, tb, tbt, P));
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false>, ta, tb, tbt, P));
     } else {
-        k_mixed_pass<ROWS, false><<<num_sms(), kThreads, Layout<ROWS, false>::kSmem, s>>>(ta, tb, tbt, P);
+        k_mixed_pass<ROWS, false, NARROW><<<num_sms(), kThreads, Layout<ROWS, false, NARROW>::kSmem, s>>>(
+            ta, tb, tbt, P);
     }
 }
 
 // Per-row statistics: mu_t, exc_t = S_t - mu_t n_t (from code counts c00, c01, c10, c11),
-// optional multiplier s_t.
+// optional multiplier s_t, and the imputed-code table: codes 00 / 01 (missing) / 10 / 11 ->
+// 2Q / q_t / Q / 0 with q_t = rint(Q mu_t), and the residual r_t = mu_t - q_t / Q.  Padding
+// rows decode to zeros.
 void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const int32_t* counts,
                const double* s_or_null) {
     configure_kernels();
@@ -926,10 +1001,15 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     // samples padded to 256: the samples pass runs on pairs of 128-sample tiles (packed rows
     // hold a multiple of 256 samples, so the padding tiles read missing codes)
     r.n_pad = round_up(std::max<int64_t>(r.n, 1), 2 * kTile);
-    std::vector<double> mu(r.r_pad, 0.0), ex(r.r_pad, 0.0), sv(r.r_pad, 0.0);
+    std::vector<double> mu(r.r_pad, 0.0), ex(r.r_pad, 0.0), sv(r.r_pad, 0.0), rs(r.r_pad, 0.0);
+    std::vector<uint32_t> lut(r.r_pad, 0u);
     for (int64_t t = 0; t < r.R; ++t) {
         const double mt = mean[t];
         mu[t] = mt;
+        const double qd = std::isfinite(mt) ? std::rint(kImputeQ * mt) : 0.0;
+        const uint32_t q = (uint32_t)std::min(std::max(qd, 0.0), 2.0 * kImputeQ);
+        lut[t] = (uint32_t)(2 * kImputeQ) | (q << 8) | ((uint32_t)kImputeQ << 16);
+        rs[t] = std::isfinite(mt) ? mt - (double)q / kImputeQ : 0.0;
         const int64_t c00 = counts[4 * t], c10 = counts[4 * t + 2], c11 = counts[4 * t + 3];
         ex[t] = (double)(2 * c00 + c10) - mt * (double)(c00 + c10 + c11);
         sv[t] = s_or_null ? s_or_null[t] : 1.0;
@@ -937,6 +1017,10 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     r.mu.resize(r.r_pad);
     r.exc.resize(r.r_pad);
     r.s.resize(r.r_pad);
+    r.resid.resize(r.r_pad);
+    r.lut.resize(r.r_pad);
+    CS_CUDA(cudaMemcpy(r.resid.get(), rs.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemcpy(r.lut.get(), lut.data(), 4 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.mu.get(), mu.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.exc.get(), ex.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.s.get(), sv.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
@@ -982,23 +1066,29 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 
 // ---------------------------------------------------------------- pass plans and the autotuner
 // A pass runs with a plan: CTA pairs or single CTAs, the column-tile width cap and the number of
-// K slices.  The default plan is the heuristic (pairs above 32 right-hand sides; widths 80 /
-// 48 / 80 / 80 for rows-single / samples-single / rows-pair / samples-pair; slices so that
-// about 8 units per CTA cover the GPU).  The autotuner times the pairs x width candidates of a
-// shape once (shapes bucketed: rows and samples by factors of 1.25, columns to multiples of 16)
-// and keeps the fastest.  It never changes the slice count, which is the only plan parameter
+// K slices.  The default plan is the heuristic (pairs above 32 right-hand sides, the narrow
+// single-CTA layout at 32 or fewer; widths 80 / 48 / 80 / 80 for rows-single / samples-single /
+// rows-pair / samples-pair, 32 narrow; slices so that about 8 units per CTA cover the GPU).  The
+// autotuner times the layout x width candidates of a shape once (shapes bucketed: rows and
+// samples by factors of 1.25, columns to multiples of 16) and keeps the fastest.  It never changes the slice count, which is the only plan parameter
 // that changes floating-point results (the order of the slice sums), so a tuned pass returns
 // the same bits as the default one.  CS_B200_AUTOTUNE=0 turns it off.
 struct PassPlan {
     bool pairs = false;
+    bool narrow = false;  // single-CTA layout for column tiles of at most 32
     int max_w = 0;
     int splits = 1;
+    bool same_kernel(const PassPlan& o) const {
+        return pairs == o.pairs && narrow == o.narrow && max_w == o.max_w;
+    }
 };
 
 PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
     PassPlan p;
     p.pairs = use_cta_pairs(k) && tiles % 2 == 0;
-    p.max_w = rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
+    p.narrow = !p.pairs && k <= kNarrowRowsW && narrow_layouts();
+    p.max_w = p.narrow ? kNarrowRowsW
+                       : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
     const Tiling tl = tiling_for(k, p.max_w);
     p.splits = p.pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
                        : choose_splits(tiles * tl.n_ctiles, kb, 8LL * num_sms());
@@ -1053,6 +1143,14 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
     }
     std::vector<PassPlan> cands;
     const int mode = pair_mode();
+    if (mode != 2 && narrow_layouts())
+        for (int w = 16; w <= kNarrowRowsW; w += 16) {
+            PassPlan p;
+            p.narrow = true;
+            p.max_w = w;
+            p.splits = def.splits;
+            cands.push_back(p);
+        }
     for (int pr = 0; pr < 2; ++pr) {
         if (pr == 1 && (mode == 0 || tiles % 2 != 0 || num_sms() < 2)) continue;
         if (pr == 0 && mode == 2) continue;
@@ -1062,7 +1160,7 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
             const Tiling tl = tiling_for(k, w);
             // a wider cap that gives the same tiling as a narrower one is the same plan
             if (tl.kc == last_kc && tl.kc_last == last_kl && tl.n_ctiles == last_ct &&
-                !(pr == (def.pairs ? 1 : 0) && w == def.max_w))
+                !(pr == (def.pairs ? 1 : 0) && !def.narrow && w == def.max_w))
                 continue;
             last_kc = tl.kc;
             last_kl = tl.kc_last;
@@ -1083,7 +1181,7 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
     try {
         run(def);  // warm: maps, function attributes, operand buffers
         bool have_default = false;
-        for (const PassPlan& p : cands) have_default = have_default || (p.pairs == def.pairs && p.max_w == def.max_w);
+        for (const PassPlan& p : cands) have_default = have_default || p.same_kernel(def);
         if (!have_default) cands.insert(cands.begin(), def);
         for (const PassPlan& p : cands) {
             CS_CUDA(cudaEventRecord(e0, s));
@@ -1092,7 +1190,7 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
             CS_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
             CS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (p.pairs == def.pairs && p.max_w == def.max_w) best.ms_default = ms;
+            if (p.same_kernel(def)) best.ms_default = ms;
             if (ms < best.ms_best) {
                 best.ms_best = ms;
                 best.plan = p;
@@ -1128,8 +1226,9 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
     const Tiling tl = tiling_for(k, plan.max_w);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(n_pad / kKBlock);
-    const int splits = plan.splits;
-    const int kbs = (kb + splits - 1) / splits;
+    const int kbs = (kb + plan.splits - 1) / plan.splits;
+    const int splits = (kb + kbs - 1) / kbs;  // no empty slice
+    if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "rows pass: K slice exceeds the exact int32 range");
     const int rt = (int)((n_pad + kPrepRows - 1) / kPrepRows);
     const int nst = (int)((n + kPrepRows - 1) / kPrepRows);  // row tiles of the column stats
     ws.b1.resize(3 * kp * n_pad);
@@ -1139,7 +1238,6 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
     ws.qsum.resize(k);
     ws.max1.resize(k);
     ws.max_w.resize(k);
-    ws.max_muw.resize(k);
     if (!ws.status.get()) {
         ws.status.resize(1);
         // on the pass's own stream, so the kernel never reads the pool's previous contents
@@ -1175,7 +1273,8 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
     P.kc = tl.kc;
     P.kc_last = tl.kc_last;
     P.kp = (int)kp;
-    P.mu = r.mu.get();
+    P.lut = r.lut.get();
+    P.resid = r.resid.get();
     P.part = ws.part.get();
     P.ld = r_pad;
     P.status = ws.status.get();
@@ -1185,22 +1284,20 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+        else if (plan.narrow)
+            launch_pass<true, false, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else
             launch_pass<true, false>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         CS_LAUNCH("kinship_rows_tc");
     }
-    if (want_max) {
-        CS_CUDA(cudaMemsetAsync(ws.max_w.get(), 0, 8 * k, s));
-        CS_CUDA(cudaMemsetAsync(ws.max_muw.get(), 0, 8 * k, s));
-    }
+    if (want_max) CS_CUDA(cudaMemsetAsync(ws.max_w.get(), 0, 8 * k, s));
     {
         prof::Scope ps("mixed_reduce_rows", s, 0.0, 8.0 * splits * kp * R + 8.0 * R * k);
         dim3 g((unsigned)((R + 2047) / 2048), (unsigned)k);
         k_reduce_rows<<<g, 256, 0, s>>>(ws.part.get(), splits, kp, r_pad, R, k, r.s.get(), spow,
                                         r.exc.get(), r.mu.get(), ws.mean1.get(), ws.qsum.get(),
                                         ws.max1.get(), out, out_ld, colmajor ? 1 : 0,
-                                        want_max ? ws.max_w.get() : nullptr,
-                                        want_max ? ws.max_muw.get() : nullptr);
+                                        want_max ? ws.max_w.get() : nullptr);
         CS_LAUNCH("reduce_rows");
     }
 }
@@ -1214,10 +1311,11 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     const Tiling tl = tiling_for(k, plan.max_w);
     const int64_t n = r.n, R = r.R, n_pad = r.n_pad, r_pad = r.r_pad, kp = tl.kp;
     const int kb = (int)(r_pad / kKBlock);
-    const int splits = plan.splits;
-    const int kbs = (kb + splits - 1) / splits;
+    const int kbs = (kb + plan.splits - 1) / plan.splits;
+    const int splits = (kb + kbs - 1) / kbs;  // no empty slice
+    if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "samples pass: K slice exceeds the exact int32 range");
     const int nrb = (int)((r_pad + 2047) / 2048);
-    ws.b2.resize(6 * kp * r_pad);
+    ws.b2.resize(5 * kp * r_pad);
     ws.part.resize((int64_t)splits * kp * n_pad);
     ws.colpart.resize((int64_t)nrb * k);
     ws.inv_f.resize(kp);
@@ -1226,16 +1324,16 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     const int box = pairs ? tl.kc / 2 : tl.kc, box_last = pairs ? tl.kc_last / 2 : tl.kc_last;
     const int64_t key = ((kp * 1000003 + r_pad) * 131 + box_last) * 131 + box;
     if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
-        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, box, true);
-        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 6 * kp, r_pad, kKBlock, box_last, true);
+        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 5 * kp, r_pad, kKBlock, box, true);
+        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 5 * kp, r_pad, kKBlock, box_last, true);
         ws.tm_b2_base = ws.b2.get();
         ws.tm_b2_key = key;
     }
     {
-        prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + 6.0 * kp * r_pad);
+        prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + 5.0 * kp * r_pad);
         dim3 g((unsigned)nrb, (unsigned)kp);
-        k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), ws.max_w.get(),
-                                                  ws.max_muw.get(), ws.b2.get(), ws.inv_f.get(),
+        k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), r.resid.get(),
+                                                  ws.max_w.get(), ws.b2.get(), ws.inv_f.get(),
                                                   ws.colpart.get());
         k_sum_partials<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get());
         CS_LAUNCH("mixed samples operand");
@@ -1249,6 +1347,7 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     P.kc = tl.kc;
     P.kc_last = tl.kc_last;
     P.kp = (int)kp;
+    P.lut = r.lut.get();
     P.inv_f = ws.inv_f.get();
     P.part = ws.part.get();
     P.ld = n_pad;
@@ -1258,6 +1357,8 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
+        else if (plan.narrow)
+            launch_pass<false, false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         else
             launch_pass<false, false>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         CS_LAUNCH("kinship_samples_tc");
@@ -1325,36 +1426,21 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     m->last_k = k;
 }
 
-// Column maxima of |W| and |mu o W| for a column-major R x k W (the samples-pass operand
-// scales): atomicMax on the bits of non-negative doubles (order independent).
+// Column maxima of |W| for a column-major R x k W (the samples-pass operand scales):
+// atomicMax on the bits of non-negative doubles (order independent).
 __global__ void __launch_bounds__(256)
-k_col_absmax(const double* __restrict__ W, int64_t R, int64_t k, const double* __restrict__ mu,
-             unsigned long long* __restrict__ max_w, unsigned long long* __restrict__ max_muw) {
-    __shared__ double red_w[8], red_m[8];
+k_col_absmax(const double* __restrict__ W, int64_t R, int64_t k, unsigned long long* __restrict__ max_w) {
+    __shared__ double red_w[8];
     const int64_t c = blockIdx.y;
-    double mw = 0.0, mm = 0.0;
+    double mw = 0.0;
     const int64_t t0 = (int64_t)blockIdx.x * 2048;
-    for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) {
-        const double v = W[c * R + t];
-        mw = fmax(mw, fabs(v));
-        mm = fmax(mm, fabs(mu[t] * v));
-    }
-    for (int off = 16; off; off >>= 1) {
-        mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
-        mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, off));
-    }
-    if ((threadIdx.x & 31) == 0) {
-        red_w[threadIdx.x >> 5] = mw;
-        red_m[threadIdx.x >> 5] = mm;
-    }
+    for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) mw = fmax(mw, fabs(W[c * R + t]));
+    for (int off = 16; off; off >>= 1) mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
+    if ((threadIdx.x & 31) == 0) red_w[threadIdx.x >> 5] = mw;
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int j = 1; j < 8; ++j) {
-            mw = fmax(mw, red_w[j]);
-            mm = fmax(mm, red_m[j]);
-        }
+        for (int j = 1; j < 8; ++j) mw = fmax(mw, red_w[j]);
         atomicMax(max_w + c, (unsigned long long)__double_as_longlong(mw));
-        atomicMax(max_muw + c, (unsigned long long)__double_as_longlong(mm));
     }
 }
 
@@ -1379,18 +1465,15 @@ void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, 
     m->last_k = 0;
     MixedWorkspace& ws = m->ws;
     ws.max_w.resize(k);
-    ws.max_muw.resize(k);
     if (!ws.status.get()) {
         ws.status.resize(1);
         CS_CUDA(cudaMemsetAsync(ws.status.get(), 0, sizeof(int), s));
     }
     CS_CUDA(cudaMemsetAsync(ws.max_w.get(), 0, 8 * k, s));
-    CS_CUDA(cudaMemsetAsync(ws.max_muw.get(), 0, 8 * k, s));
     {
         prof::Scope ps("mixed_col_absmax", s, 0.0, 8.0 * R * k);
         dim3 g((unsigned)((R + 2047) / 2048), (unsigned)k);
-        k_col_absmax<<<g, 256, 0, s>>>(Wcol, R, k, m->rows.mu.get(), ws.max_w.get(),
-                                       ws.max_muw.get());
+        k_col_absmax<<<g, 256, 0, s>>>(Wcol, R, k, ws.max_w.get());
         CS_LAUNCH("col_absmax");
     }
     samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune);
@@ -1401,17 +1484,18 @@ void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, 
 std::string autotune_json() {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     std::string out = "[";
-    char buf[320];
+    char buf[384];
     bool first = true;
     for (const auto& kv : g_tuned) {
         const TuneEntry& e = kv.second;
         std::snprintf(buf, sizeof buf,
                       "%s{\"pass\": \"%s\", \"R\": %lld, \"n\": %lld, \"k\": %lld, "
-                      "\"pairs\": %s, \"max_width\": %d, \"slices\": %d, \"candidates\": %d, "
-                      "\"ms_best\": %.4f, \"ms_default\": %.4f}",
+                      "\"pairs\": %s, \"narrow\": %s, \"max_width\": %d, \"slices\": %d, "
+                      "\"candidates\": %d, \"ms_best\": %.4f, \"ms_default\": %.4f}",
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
-                      e.plan.max_w, e.plan.splits, e.candidates, e.ms_best, e.ms_default);
+                      e.plan.narrow ? "true" : "false", e.plan.max_w, e.plan.splits, e.candidates,
+                      e.ms_best, e.ms_default);
         out += buf;
         first = false;
     }

@@ -4,6 +4,7 @@
 #include <cusolverDn.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 
 #include "cs_internal.h"
@@ -23,6 +24,17 @@ void prepare_pool(int dev) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     });
 }
+
+// CS_B200_POISON_ALLOC=1 fills every new block with 0xFF bytes (NaN as FP64), so that a read of
+// memory no kernel has written shows up in the results instead of depending on what the pool
+// held before.
+bool poison_allocations() {
+    static const bool on = [] {
+        const char* v = std::getenv("CS_B200_POISON_ALLOC");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
 }  // namespace
 
 void* device_alloc(size_t bytes) {
@@ -31,6 +43,7 @@ void* device_alloc(size_t bytes) {
     if (dev >= 0 && dev < kMaxDevices) prepare_pool(dev);
     void* p = nullptr;
     CS_CUDA(cudaMallocAsync(&p, bytes, 0));
+    if (poison_allocations()) CS_CUDA(cudaMemsetAsync(p, 0xFF, bytes, 0));
     // usable from every stream once the allocation is ordered on the legacy stream
     CS_CUDA(cudaStreamSynchronize(0));
     return p;

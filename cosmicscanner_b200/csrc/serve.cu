@@ -456,7 +456,7 @@ int64_t server_submit(cs_server* sv, const cs_serve_request* q) {
         const int64_t rows = sv->op->num_variants, n_pad = round_up(n, 256);
         const int64_t kp = round_up(sk + r->p + 1, 16);
         r->est_bytes += rows * round_up((n + 3) / 4, kRowAlign) + 3 * kp * n_pad +
-                        6 * kp * round_up(rows, 256) + 8 * 8 * kp * std::max(n_pad, rows);
+                        5 * kp * round_up(rows, 256) + 8 * 8 * kp * std::max(n_pad, rows);
     }
     std::lock_guard<std::mutex> lk(sv->mu);
     r->id = sv->next_id++;

@@ -172,6 +172,28 @@ __device__ __forceinline__ void tmem_ld16i(uint32_t taddr, int32_t (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __float_as_int(f[i]);
 }
 
+// Warp-wide load of 8 consecutive 32-bit TMEM columns of this warp's 32 lanes.
+__device__ __forceinline__ void tmem_ld8i(uint32_t taddr, int32_t (&v)[8]) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = (int32_t)r[i];
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t taddr, int32_t (&v)[N]) {
+    static_assert(N == 8 || N == 16, "8 or 16 columns");
+    if constexpr (N == 16)
+        tmem_ld16i(taddr, v);
+    else
+        tmem_ld8i(taddr, v);
+}
+
 // ---------------------------------------------------------------- CTA pairs (cta_group::2)
 // A cluster of two CTAs shares one MMA: rank 0 (the leader) issues tcgen05.mma.cta_group::2
 // with M = 256 (128 rows from each CTA's shared memory) and N split between the CTAs' shared

@@ -141,3 +141,21 @@ def test_narrow_fp64_apply(k):
         assert (np.abs(Y - E).max(axis=0) / np.abs(E).max(axis=0)).max() < 1e-12
         assert np.array_equal(op.apply(X), Y)
         op.close()
+
+
+@pytest.mark.parametrize("k", [1, 16, 40])
+def test_mixed_small_cohort_many_slices(k):
+    """A small cohort against many SNPs: the tensor-core passes split the SNP contraction into
+    many K slices to fill the GPU (300 samples are 3 tiles, 60,000 SNPs 469 K-blocks), with
+    none left empty; the result equals the FP64 form to the mixed tolerance."""
+    synth = pytest.importorskip("cosmicscanner_b200.synth")
+    d = synth.cohort(300, 60000, 29, missing=0.02, n_causal=10)
+    g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+    op = cs.createKinshipOperator(g)
+    rng = np.random.default_rng(k)
+    X = rng.standard_normal((op.rows(), k))
+    E = op.apply(X, precision="fp64")
+    Y = op.apply(X, precision="mixed")
+    assert (np.abs(Y - E).max(axis=0) / np.abs(E).max(axis=0)).max() < 1e-6
+    assert np.array_equal(op.apply(X, precision="mixed"), Y)
+    op.close()
