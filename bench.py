@@ -952,13 +952,13 @@ def main():
                      "ms_per_launch": per_launch_ms,
                      "share_of_step": top["ms"] / ms})
         if "_tc" in top["name"]:
-            # the int8 datapath: 6 MMAs per useful multiply-add (3 right-hand-side pieces x
-            # {dosage, missing} tiles) on columns padded to the column tile
+            # the int8 datapath: 5 MMA columns per useful multiply-add (3 right-hand-side pieces
+            # against the imputed-code tile, 2 against the missing-indicator tile) on columns
+            # padded to the column tiles (80-wide tiles and a last one rounded up to 16)
             k_rhs = RANK + OVERSAMPLE
             tiles = -(-k_rhs // 80)
-            per_tile = -(-k_rhs // tiles)
-            kc = -(-per_tile // 16) * 16
-            ops = achieved * 6 * (tiles * kc) / k_rhs
+            padded = 80 * (tiles - 1) + -(-(k_rhs - 80 * (tiles - 1)) // 16) * 16
+            ops = achieved * 5 * padded / k_rhs
             ipeak = int8_peak_tops(torch)
             roof["int8_datapath"] = {"mma_tops": ops, "peak_tops": ipeak,
                                      "peak_kind": "cuBLASLt int8 GEMM 8192^3 measured in this run",

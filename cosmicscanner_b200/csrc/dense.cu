@@ -140,15 +140,16 @@ GrmSnp grm_snp(const int32_t* cnt, int algorithm, float min_maf) {
     const double freq = (double)sum_x / (2.0 * n_obs);
     const double maf = std::min(freq, 1.0 - freq);
     if (maf < min_maf || std::abs(maf) < 1e-8) return out;
-    const double weight = 1.0f;
+    // float-rounded 2pq (or its algorithm variant) as the reference stores it: the GRM's
+    // block sums of these floats must group identically for parity
     if (algorithm == 4) {
-        out.two_pq = (float)(weight * 4.0 * freq * freq * (1.0 - freq) * (1.0 - freq));
+        out.two_pq = (float)(4.0 * freq * freq * (1.0 - freq) * (1.0 - freq));
     } else if (algorithm == 5) {
         const double p1 = (double)n_het / n_obs, p2 = (double)n_hom1 / n_obs;
         const double mu = p1 + 2.0 * p2;
-        out.two_pq = (float)(weight * (p1 + 4.0 * p2 - mu * mu));
+        out.two_pq = (float)(p1 + 4.0 * p2 - mu * mu);
     } else {
-        out.two_pq = (float)(weight * 2.0 * freq * (1.0 - freq));
+        out.two_pq = (float)(2.0 * freq * (1.0 - freq));
     }
     const float mean_f = (float)(freq * 2.0);
     float scale_f = 1.0f;
@@ -161,9 +162,8 @@ GrmSnp grm_snp(const int32_t* cnt, int algorithm, float min_maf) {
         const double var = p1 + 4.0 * p2 - mu * mu;
         scale_f = (float)((var > 1e-9) ? (1.0 / std::sqrt(var)) : 0.0);
     }
-    const float w = std::sqrt(1.0f);
     const double mean = mean_f;
-    const double scale = scale_f * w;
+    const double scale = scale_f;
     if (algorithm == 4) {
         const double fp = mean / 2.0, fq = 1.0 - fp;
         out.lut[0] = (-2.0 * fq * fq) * scale;
