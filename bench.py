@@ -355,26 +355,34 @@ def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp6
             time.sleep(delay)
         t_sub.append(time.perf_counter())
         ids.append(srv.submit(S, Y, X, b, e))
-    lat = []
+    lat, failed = [], []
     for rid in ids:
-        lat.append(srv.wait(rid)["latency_s"])
+        try:
+            lat.append(srv.wait(rid)["latency_s"])
+        except cs.CosmicError as e:  # counted and reported, the stream goes on
+            failed.append(str(e))
+            lat.append(float("nan"))
         srv.release(rid)
     lat = np.array(lat)
+    ok = ~np.isnan(lat)
     st = srv.stats()
     srv.close()
-    wall = float(np.max(np.array(t_sub) + lat) - t_sub[0])
+    done = np.array(t_sub)[ok] + lat[ok]
+    wall = float(np.max(done) - t_sub[0]) if ok.any() else float("nan")
     applies = st["applies"] - st0["applies"]
     sizes = np.array([len(q[0]) for q in reqs])
+    lok = lat[ok] if ok.any() else np.array([float("nan")])
     out = {
-        "requests": len(reqs), "req_per_s": len(reqs) / wall,
-        "p50_ms": float(np.percentile(lat, 50)) * 1e3, "p99_ms": float(np.percentile(lat, 99)) * 1e3,
-        "mean_ms": float(lat.mean()) * 1e3,
+        "requests": len(reqs), "completed": int(ok.sum()), "req_per_s": int(ok.sum()) / wall,
+        "p50_ms": float(np.percentile(lok, 50)) * 1e3, "p99_ms": float(np.percentile(lok, 99)) * 1e3,
+        "mean_ms": float(lok.mean()) * 1e3,
         "single_request_ms": single * 1e3, "capacity_rps": capacity, "arrival_rate_per_s": rate,
         "stacked_applies": applies,
         "mean_columns_per_stacked_apply": (st["apply_columns"] - st0["apply_columns"]) / max(1, applies),
         "max_requests_per_apply": st["max_requests_per_apply"],
         "own_view_requests": st["own_view_requests"], "memory_budget_gb": st["memory_budget_gb"],
         "max_concurrent": st["max_concurrent"], "failed": st["failed"],
+        "failure_messages": sorted(set(failed))[:3],
         "cohort_size_median": float(np.median(sizes)), "cohort_size_mean": float(sizes.mean()),
         "config": f"{label}resident N={n} M={m}; {len(reqs)} requests; subsets log-U[5000,{n}], "
                   f"traits U{{1..16}}, intercept + U{{2..5}} N(0,1) covariates, window {window} "
@@ -398,8 +406,8 @@ def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp6
             "p50_ms": float(np.percentile(lat64, 50)) * 1e3,
             "sample": f"the first {fp64_sample} requests of the stream, one at a time (the "
                       f"whole stream would take ~{lat64.mean() * len(reqs) / 60:.0f} min)",
-            "throughput_ratio_mixed_batched_over_fp64": (len(reqs) / wall) * float(lat64.mean()),
-            "mixed_latency_same_requests_ms": float(mixed_same.mean()) * 1e3}
+            "throughput_ratio_mixed_batched_over_fp64": out["req_per_s"] * float(lat64.mean()),
+            "mixed_latency_same_requests_ms": float(np.nanmean(mixed_same)) * 1e3}
     return out
 
 

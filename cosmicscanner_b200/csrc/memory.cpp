@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
+#include <string>
 
 #include "cs_internal.h"
 
@@ -42,7 +43,23 @@ void* device_alloc(size_t bytes) {
     CS_CUDA(cudaGetDevice(&dev));
     if (dev >= 0 && dev < kMaxDevices) prepare_pool(dev);
     void* p = nullptr;
-    CS_CUDA(cudaMallocAsync(&p, bytes, 0));
+    cudaError_t e = cudaMallocAsync(&p, bytes, 0);
+    if (e == cudaErrorMemoryAllocation) {
+        // The pool keeps freed blocks reserved; when the device has no room left for a new
+        // block, hand the reserved free blocks back (after the device has finished with them)
+        // and try once more.
+        cudaGetLastError();
+        cudaMemPool_t pool;
+        if (cudaDeviceSynchronize() == cudaSuccess &&
+            cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+            cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
+            e = cudaMallocAsync(&p, bytes, 0);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CS_ERR_CUDA, std::string("device allocation of ") + std::to_string(bytes) +
+                              " bytes failed: " + cudaGetErrorString(e));
+    }
     if (poison_allocations()) CS_CUDA(cudaMemsetAsync(p, 0xFF, bytes, 0));
     // usable from every stream once the allocation is ordered on the legacy stream
     CS_CUDA(cudaStreamSynchronize(0));

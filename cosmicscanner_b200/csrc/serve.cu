@@ -27,9 +27,11 @@
 // path alone and in the mix.
 //
 // Admission.  Requests are admitted FIFO while a worker slot is free and their estimated
-// working set (sketch blocks, scan window and, for repacked requests, the packed copy and
-// its tensor-core operands) fits the memory budget: by default the device's free memory at
-// server creation less a 4 GB reserve.
+// working set (sketch blocks, scan window and, for repacked requests, the packed copy, its
+// tensor-core operands and the sketch rows kept for the scan) fits the memory budget: by
+// default the device's free memory at server creation less a 4 GB reserve and less the shared
+// apply's own buffers at the full column budget (stacked blocks in and out, the rows-pass
+// output, operand pieces and slice partials over all N samples and M SNPs).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -409,7 +411,12 @@ cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t
         } else {
             size_t free_b = 0, total_b = 0;
             CS_CUDA(cudaMemGetInfo(&free_b, &total_b));
-            sv->budget_bytes = std::max<int64_t>(0, (int64_t)free_b - (int64_t)4e9);
+            const int64_t N = sv->op->rows, R = sv->op->n_active;
+            const int64_t B = round_up(sv->opt.max_batch_columns, 16) + 16;
+            const int64_t n_pad = round_up(N, 256), r_pad = round_up(R, 256);
+            const int64_t shared = 8 * B * (2 * N + R + r_pad + 4 * n_pad) + 3 * B * n_pad +
+                                   5 * B * r_pad;
+            sv->budget_bytes = std::max<int64_t>(0, (int64_t)free_b - (int64_t)4e9 - shared);
         }
         sv->diag_full.resize(sv->op->rows);
         kinship_diagonal(sv->op, sv->diag_full.data());
@@ -456,7 +463,8 @@ int64_t server_submit(cs_server* sv, const cs_serve_request* q) {
         const int64_t rows = sv->op->num_variants, n_pad = round_up(n, 256);
         const int64_t kp = round_up(sk + r->p + 1, 16);
         r->est_bytes += rows * round_up((n + 3) / 4, kRowAlign) + 3 * kp * n_pad +
-                        5 * kp * round_up(rows, 256) + 8 * 8 * kp * std::max(n_pad, rows);
+                        5 * kp * round_up(rows, 256) + 8 * 8 * kp * std::max(n_pad, rows) +
+                        3 * 8 * kp * rows;  // rows-pass output, its copy for the scan, buf_u
     }
     std::lock_guard<std::mutex> lk(sv->mu);
     r->id = sv->next_id++;
