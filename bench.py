@@ -336,7 +336,11 @@ def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp6
     # of one request alone; the capacity: eight requests submitted at once, completed per
     # second.  Arrivals come at 80 % of that capacity.
     srv.wait(srv.submit(*reqs[0]))
-    single = srv.wait(srv.submit(*reqs[0]))["latency_s"]
+    solo_id = srv.submit(*reqs[0])
+    single = srv.wait(solo_id)["latency_s"]
+    n_traits0 = reqs[0][1].shape[1]
+    solo = [srv.result(solo_id, t) for t in range(n_traits0)]
+    srv.release(solo_id)
     c0 = time.perf_counter()
     cal = [srv.submit(*q) for q in reqs[:8]]
     for rid in cal:
@@ -356,9 +360,23 @@ def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp6
         t_sub.append(time.perf_counter())
         ids.append(srv.submit(S, Y, X, b, e))
     lat, failed = [], []
-    for rid in ids:
+    mix_vs_alone = None
+    for i, rid in enumerate(ids):
         try:
             lat.append(srv.wait(rid)["latency_s"])
+            if i == 0:
+                # the stream's first request was also served alone: same result in the mix
+                dp, dv = 0.0, 0.0
+                for t in range(n_traits0):
+                    a, b = srv.result(rid, t), solo[t]
+                    tested = np.asarray(b["tested"], bool)
+                    if not np.array_equal(np.asarray(a["tested"], bool), tested):
+                        dp = float("inf")
+                    else:
+                        dp = max(dp, float(np.max(np.abs(a["log10p"][tested] - b["log10p"][tested]),
+                                                  initial=0.0)))
+                    dv = max(dv, abs(a["sigma2_g"] - b["sigma2_g"]) / max(abs(b["sigma2_g"]), 1e-300))
+                mix_vs_alone = {"traits": n_traits0, "sigma2_g_rel": dv, "log10p_max_abs": dp}
         except cs.CosmicError as e:  # counted and reported, the stream goes on
             failed.append(str(e))
             lat.append(float("nan"))
@@ -383,6 +401,7 @@ def run_serve(cs, g, variants, d, args, window=None, max_batch_columns=4096, fp6
         "own_view_requests": st["own_view_requests"], "memory_budget_gb": st["memory_budget_gb"],
         "max_concurrent": st["max_concurrent"], "failed": st["failed"],
         "failure_messages": sorted(set(failed))[:3],
+        "first_request_mix_vs_alone": mix_vs_alone,
         "cohort_size_median": float(np.median(sizes)), "cohort_size_mean": float(sizes.mean()),
         "config": f"{label}resident N={n} M={m}; {len(reqs)} requests; subsets log-U[5000,{n}], "
                   f"traits U{{1..16}}, intercept + U{{2..5}} N(0,1) covariates, window {window} "

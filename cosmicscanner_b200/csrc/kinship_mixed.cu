@@ -192,7 +192,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
     uint64_t* full_p = empty_t + ST;      // packed tile landed (1 arrival + tx bytes)
     uint64_t* empty_p = full_p + SP;      // packed tile decoded (one arrival per decode warp)
     uint64_t* full_d = empty_p + SP;      // decoded (one arrival per decode warp; pair: the
-                                          // leader's counts both CTAs' warps)
+                                          // leader's counts both CTAs' warps and the other
+                                          // CTA's B-stage-landed arrival)
     uint64_t* empty_d = full_d + SD;      // MMAs reading the decoded tile done (commit)
     uint64_t* acc_full = empty_d + SD;    // accumulator ready for the epilogue (commit)
     uint64_t* acc_empty = acc_full + NB;  // accumulator drained (one arrival per epilogue warp)
@@ -212,7 +213,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             mbar_init(&empty_p[s], kDecodeWarps);
         }
         for (int d = 0; d < SD; ++d) {
-            mbar_init(&full_d[d], (PAIR ? 2 : 1) * kDecodeWarps);
+            mbar_init(&full_d[d], PAIR ? 2 * kDecodeWarps + 1 : kDecodeWarps);
             mbar_init(&empty_d[d], 1);
         }
         for (int b = 0; b < NB; ++b) {
@@ -390,6 +391,24 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             else
                 mma_commit(drained);
             mbar_wait(drained, 0, P.status, kTimeoutMma, 1u << 20);
+        } else if (PAIR && rank == 1 && elect_one()) {
+            // The leader's MMA also reads this CTA's half of each B stage: once the stage has
+            // landed here, tell the leader (one arrival on its full_d, after the decoders'),
+            // so that no decoder waits for the B copy of the K-block it has just decoded.
+            // Like a decoder, wait until the decode stage is free so that the arrival counts
+            // toward that stage's next phase.
+            uint32_t j = 0;
+            bool ok = true;
+            for (int u = u0; u < units && ok; u += ustep) {
+                int tile, ct, split, kb0, kb1;
+                unit_coords(u, tile, ct, split, kb0, kb1);
+                for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                    const int s = j % ST, d = j % SD;
+                    if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
+                    if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
+                    mbar_arrive_remote(mapa_shared(&full_d[d], 0));
+                }
+            }
         }
     } else if (warp < kEpiWarp0) {
         // ------------------------------------------------------------ decoders
@@ -425,12 +444,6 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
-                if (PAIR) {
-                    // the leader's MMA also reads this CTA's half of B: its stage must have
-                    // landed before the arrival below completes the leader's full_d
-                    const int s = j % ST;
-                    if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
-                }
                 if (lane == 0) {
                     if (PAIR)
                         mbar_arrive_remote(mapa_shared(&full_d[d], 0));

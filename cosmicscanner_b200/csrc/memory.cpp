@@ -1,4 +1,4 @@
-// Device memory pool and shared cuBLAS handles.
+// Device memory pool and the per-thread cuBLAS / cuSOLVER handles.
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
@@ -36,6 +36,19 @@ bool poison_allocations() {
     }();
     return on;
 }
+
+thread_local cublasHandle_t t_blas[kMaxDevices] = {};
+thread_local cusolverDnHandle_t t_solver[kMaxDevices] = {};
+
+// Gives the pool's reserved free blocks back to the device (after the device has finished
+// with them), when an allocation found no room: the pool keeps freed blocks reserved, which
+// neither a block of another size nor the libraries' own allocations can use.
+void trim_pool(int dev) {
+    cudaMemPool_t pool;
+    if (cudaDeviceSynchronize() == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
+}
 }  // namespace
 
 void* device_alloc(size_t bytes) {
@@ -46,14 +59,10 @@ void* device_alloc(size_t bytes) {
     cudaError_t e = cudaMallocAsync(&p, bytes, 0);
     if (e == cudaErrorMemoryAllocation) {
         // The pool keeps freed blocks reserved; when the device has no room left for a new
-        // block, hand the reserved free blocks back (after the device has finished with them)
-        // and try once more.
+        // block, hand the reserved free blocks back and try once more.
         cudaGetLastError();
-        cudaMemPool_t pool;
-        if (cudaDeviceSynchronize() == cudaSuccess &&
-            cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
-            cudaMemPoolTrimTo(pool, 0) == cudaSuccess)
-            e = cudaMallocAsync(&p, bytes, 0);
+        trim_pool(dev);
+        e = cudaMallocAsync(&p, bytes, 0);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -67,23 +76,47 @@ void* device_alloc(size_t bytes) {
 }
 
 cublasHandle_t shared_blas() {
-    thread_local cublasHandle_t handles[kMaxDevices] = {};
     int dev = 0;
     CS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
-    if (!handles[dev] && cublasCreate(&handles[dev]) != CUBLAS_STATUS_SUCCESS)
-        fail(CS_ERR_CUDA, "cublasCreate failed");
-    return handles[dev];
+    if (!t_blas[dev] && cublasCreate(&t_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
+        t_blas[dev] = nullptr;
+        trim_pool(dev);
+        if (cublasCreate(&t_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
+            t_blas[dev] = nullptr;
+            fail(CS_ERR_CUDA, "cublasCreate failed");
+        }
+    }
+    return t_blas[dev];
 }
 
 cusolverDnHandle_t shared_solver() {
-    thread_local cusolverDnHandle_t handles[kMaxDevices] = {};
     int dev = 0;
     CS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
-    if (!handles[dev] && cusolverDnCreate(&handles[dev]) != CUSOLVER_STATUS_SUCCESS)
-        fail(CS_ERR_CUDA, "cusolverDnCreate failed");
-    return handles[dev];
+    if (!t_solver[dev] && cusolverDnCreate(&t_solver[dev]) != CUSOLVER_STATUS_SUCCESS) {
+        t_solver[dev] = nullptr;
+        trim_pool(dev);
+        if (cusolverDnCreate(&t_solver[dev]) != CUSOLVER_STATUS_SUCCESS) {
+            t_solver[dev] = nullptr;
+            fail(CS_ERR_CUDA, "cusolverDnCreate failed");
+        }
+    }
+    return t_solver[dev];
+}
+
+void release_thread_handles() noexcept {
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    for (int d = 0; d < kMaxDevices; ++d) {
+        if (!t_blas[d] && !t_solver[d]) continue;
+        if (d != cur) cudaSetDevice(d);
+        if (t_blas[d]) cublasDestroy(t_blas[d]);
+        if (t_solver[d]) cusolverDnDestroy(t_solver[d]);
+        t_blas[d] = nullptr;
+        t_solver[d] = nullptr;
+        if (d != cur) cudaSetDevice(cur);
+    }
 }
 
 namespace {

@@ -232,6 +232,8 @@ void cs_server::gpu_loop() {
         }
         cv.notify_all();
     }
+    cudaStreamSynchronize(s);
+    cs::release_thread_handles();
     cudaStreamDestroy(s);
 }
 
@@ -353,10 +355,10 @@ void cs_server::run_request(Request* r) {
         err = e.what();
     }
     cs::set_thread_free_stream(nullptr);
-    if (st) {
-        cudaStreamSynchronize(st);
-        cudaStreamDestroy(st);
-    }
+    if (st) cudaStreamSynchronize(st);
+    // this thread ends here: its library handles (and their workspaces) go with it
+    cs::release_thread_handles();
+    if (st) cudaStreamDestroy(st);
     {
         std::lock_guard<std::mutex> lk(mu);
         r->t_done = now_s();
