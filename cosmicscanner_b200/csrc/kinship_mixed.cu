@@ -102,26 +102,41 @@ constexpr int kPairSamplesW = 80, kPairSamplesST = 3, kPairSamplesSP = 6, kPairS
 constexpr int kNarrowRowsW = 32, kNarrowRowsST = 4, kNarrowRowsSP = 8, kNarrowRowsSD = 4;
 static_assert(kNarrowRowsW == 32, "the plans use one narrow width for both passes");
 constexpr int kNarrowSamplesW = 32, kNarrowSamplesST = 3, kNarrowSamplesSP = 8, kNarrowSamplesSD = 4;
+// The narrow rows pass with its A operand in tensor memory (TMEMA): the decoders store the
+// imputed-code and missing-indicator tiles into TMEM (tcgen05.st) and the MMAs read them
+// there, so shared memory carries only the packed tiles and the B pieces.  TMEM: two
+// accumulators of 5 x 32 columns, then three A stages of 64 columns (32 per tile: 128 int8
+// K elements per lane).
+constexpr int kTmemARowsST = 8, kTmemARowsSP = 16, kTmemARowsSD = 3;
+constexpr uint32_t kTmemAccStride = 5 * kNarrowRowsW, kTmemAStage = 64;
 
-template <bool ROWS, bool PAIR, bool NARROW = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
+    static_assert(!TMEMA || (ROWS && NARROW), "A in TMEM: the narrow rows pass only");
     static constexpr int kPieces = ROWS ? 3 : 5;  // per column tile, over the pair
     static constexpr int kMaxW = NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
+    static constexpr int kTmaStages = TMEMA ? kTmemARowsST
+                                      : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
+    static constexpr int kPackedStages = TMEMA ? kTmemARowsSP
+                                         : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
+    static constexpr int kDecodeStages = TMEMA ? kTmemARowsSD
+                                         : NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
                                          : PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
     static constexpr int kAccCols = ROWS ? 5 * kMaxW : 3 * kMaxW;
     static constexpr int kAccBufs = (ROWS && !NARROW) ? 1 : 2;
-    static constexpr uint32_t kAccStride = 256;
+    static constexpr uint32_t kAccStride = TMEMA ? kTmemAccStride : 256;
+    // TMEM columns of decode stage d's imputed-code / missing-indicator tiles (TMEMA)
+    static constexpr uint32_t kTmemA0 = kAccBufs * kAccStride;
+    static __host__ __device__ constexpr uint32_t ta(int d) { return kTmemA0 + d * kTmemAStage; }
+    static __host__ __device__ constexpr uint32_t tam(int d) { return ta(d) + kTmemAStage / 2; }
     static constexpr int kBBytes = kPieces * kMaxW * 128 / (PAIR ? 2 : 1);  // this CTA's share
     static constexpr int kTmaBytes = kBBytes;
     static constexpr int kDecBytes = 2 * kATileBytes;
-    static constexpr int kDecodeRegion = kDecodeStages * kDecBytes;
+    static constexpr int kDecodeRegion = TMEMA ? 0 : kDecodeStages * kDecBytes;
     // barriers: full / empty per B, packed and decode stage, full / empty per accumulator,
     // `drained`, then the TMEM slot
     static constexpr int kBarBytes =
@@ -141,6 +156,7 @@ struct Layout {
     static_assert(kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
     static_assert(kAccBufs == 1 ? kAccCols <= (int)kTmemCols : kAccCols <= (int)kAccStride,
                   "accumulators exceed TMEM");
+    static_assert(!TMEMA || ta(kDecodeStages) <= kTmemCols, "A stages exceed TMEM");
     static_assert(kMaxW % 16 == 0 && kMaxW <= kMaxKc, "column tiles are multiples of 16, at most 80");
 };
 
@@ -177,11 +193,11 @@ __device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint32_t lut
 __host__ __device__ __forceinline__ int sample_at(int p) { return p < 8 ? 2 * p : 2 * (p - 8) + 1; }
 __host__ __device__ __forceinline__ int position_of(int s) { return (s & 1) ? 8 + (s >> 1) : s >> 1; }
 
-template <bool ROWS, bool PAIR, bool NARROW>
+template <bool ROWS, bool PAIR, bool NARROW, bool TMEMA>
 __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
-    using L = Layout<ROWS, PAIR, NARROW>;
+    using L = Layout<ROWS, PAIR, NARROW, TMEMA>;
     constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -356,11 +372,17 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
 #pragma unroll
                     for (int ks = 0; ks < kKBlock / 32; ++ks) {
                         const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
+                        const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
+                        const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
+                        if constexpr (TMEMA) {
+                            // A from TMEM: 32 K elements = 8 columns per MMA
+                            mma_i8_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
+                            mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m, first);
+                            continue;
+                        }
                         const uint32_t aoff = ROWS ? ks * 32 : ks * 4096;  // 32 K elements
                         const uint64_t da = smem_desc_sw128(a + aoff, 16, 1024);
                         const uint64_t dm = smem_desc_sw128(am + aoff, 16, 1024);
-                        const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
-                        const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
                         // rows pass: separate missing-call sums; samples pass: the first two
                         // piece columns of the same accumulator
                         if (PAIR) {
@@ -412,9 +434,11 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         }
     } else if (warp < kEpiWarp0) {
         // ------------------------------------------------------------ decoders
-        // thread dt: SNP row dt % 128, 64 samples (16 packed bytes) starting at 64 * (dt / 128)
+        // thread dt: SNP row dt % 128, 64 samples (16 packed bytes) starting at 64 * (dt / 128);
+        // TMEMA: row 32 (warp % 4) + lane, the TMEM lane quarter this warp may access
         const int dt = threadIdx.x - kDecodeWarp0 * 32;
-        const int r = dt & 127, h = dt >> 7;
+        const int r = TMEMA ? 32 * (warp & 3) + lane : dt & 127;
+        const int h = TMEMA ? (warp - kDecodeWarp0) >> 2 : dt >> 7;
         const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
         uint32_t j = 0;
         bool ok = true;
@@ -430,19 +454,37 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
                 if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
                 const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
-                unsigned char* a = smem + L::a(d);
-                unsigned char* am = smem + L::am(d);
                 const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
+                if constexpr (TMEMA) {
+                    // 64 K elements of this lane = 16 TMEM columns of each tile
+                    uint32_t ev[16], mv[16];
 #pragma unroll
-                for (int cj = 0; cj < 4; ++cj) {
-                    uint4 dos, mis;
-                    decode_word_interleaved(words[cj], lut, dos, mis);
-                    const int chunk = 4 * h + cj;  // 16 samples per 16-byte chunk
-                    const int off = rbase + ((chunk ^ (r & 7)) << 4);
-                    *reinterpret_cast<uint4*>(a + off) = dos;
-                    *reinterpret_cast<uint4*>(am + off) = mis;
+                    for (int cj = 0; cj < 4; ++cj) {
+                        uint4 dos, mis;
+                        decode_word_interleaved(words[cj], lut, dos, mis);
+                        ev[4 * cj] = dos.x; ev[4 * cj + 1] = dos.y; ev[4 * cj + 2] = dos.z; ev[4 * cj + 3] = dos.w;
+                        mv[4 * cj] = mis.x; mv[4 * cj + 1] = mis.y; mv[4 * cj + 2] = mis.z; mv[4 * cj + 3] = mis.w;
+                    }
+                    tc_fence_after();  // after the MMA's release of this stage (empty_d)
+                    const uint32_t lane_base = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + 16 * h;
+                    tmem_st16(lane_base + L::ta(d), ev);
+                    tmem_st16(lane_base + L::tam(d), mv);
+                    tmem_wait_st();
+                    tc_fence_before();
+                } else {
+                    unsigned char* a = smem + L::a(d);
+                    unsigned char* am = smem + L::am(d);
+#pragma unroll
+                    for (int cj = 0; cj < 4; ++cj) {
+                        uint4 dos, mis;
+                        decode_word_interleaved(words[cj], lut, dos, mis);
+                        const int chunk = 4 * h + cj;  // 16 samples per 16-byte chunk
+                        const int off = rbase + ((chunk ^ (r & 7)) << 4);
+                        *reinterpret_cast<uint4*>(a + off) = dos;
+                        *reinterpret_cast<uint4*>(am + off) = mis;
+                    }
+                    fence_proxy_async_smem();
                 }
-                fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
                     if (PAIR)
@@ -870,6 +912,15 @@ int pair_mode() {
     }();
     return mode;
 }
+// The narrow rows pass with A in TMEM (CS_B200_TMEM_A=0: A in shared memory).  Measured at
+// N=50k, M=100k: 0.70 vs 1.03 ms per pass at k <= 16, 0.81 vs 1.09 at k = 32.
+bool tmem_a_default() {
+    static const bool on = [] {
+        const char* v = std::getenv("CS_B200_TMEM_A");
+        return !(v && std::strcmp(v, "0") == 0);
+    }();
+    return on;
+}
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
 bool narrow_layouts() {
     static const bool on = [] {
@@ -928,11 +979,11 @@ void destroy_mixed(MixedOperator* m) { delete m; }
 
 namespace {
 
-template <bool ROWS, bool PAIR, bool NARROW = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
 cudaError_t allow_smem() {
-    return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR, NARROW>,
+    return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR, NARROW, TMEMA>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                Layout<ROWS, PAIR, NARROW>::kSmem);
+                                Layout<ROWS, PAIR, NARROW, TMEMA>::kSmem);
 }
 
 void configure_kernels() {
@@ -944,6 +995,7 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<false, true>();
         if (err == cudaSuccess) err = allow_smem<true, false, true>();
         if (err == cudaSuccess) err = allow_smem<false, false, true>();
+        if (err == cudaSuccess) err = allow_smem<true, false, true, true>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -970,14 +1022,14 @@ int resident_pairs() {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true, false>, &cfg));
+        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true, false, false>, &cfg));
         n = std::max(1, std::min(clusters, num_sms() / 2));
     }
     return n;
 }
 
 // One CTA per SM, or (PAIR) as many clusters of two CTAs as are resident together.
-template <bool ROWS, bool PAIR, bool NARROW = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
 void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
                  const PassArgs& P, cudaStream_t s) {
     if (PAIR) {
@@ -993,9 +1045,10 @@ void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false>, ta, tb, tbt, P));
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false, false>, ta, tb, tbt, P));
     } else {
-        k_mixed_pass<ROWS, false, NARROW><<<num_sms(), kThreads, Layout<ROWS, false, NARROW>::kSmem, s>>>(
+        k_mixed_pass<ROWS, false, NARROW, TMEMA>
+            <<<num_sms(), kThreads, Layout<ROWS, false, NARROW, TMEMA>::kSmem, s>>>(
             ta, tb, tbt, P);
     }
 }
@@ -1089,10 +1142,11 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 struct PassPlan {
     bool pairs = false;
     bool narrow = false;  // single-CTA layout for column tiles of at most 32
+    bool tmem_a = false;  // narrow rows pass with the A operand in TMEM
     int max_w = 0;
     int splits = 1;
     bool same_kernel(const PassPlan& o) const {
-        return pairs == o.pairs && narrow == o.narrow && max_w == o.max_w;
+        return pairs == o.pairs && narrow == o.narrow && tmem_a == o.tmem_a && max_w == o.max_w;
     }
 };
 
@@ -1100,6 +1154,7 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
     PassPlan p;
     p.pairs = use_cta_pairs(k) && tiles % 2 == 0;
     p.narrow = !p.pairs && k <= kNarrowRowsW && narrow_layouts();
+    p.tmem_a = rows && p.narrow && tmem_a_default();
     p.max_w = p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
     const Tiling tl = tiling_for(k, p.max_w);
@@ -1157,13 +1212,15 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
     std::vector<PassPlan> cands;
     const int mode = pair_mode();
     if (mode != 2 && narrow_layouts())
-        for (int w = 16; w <= kNarrowRowsW; w += 16) {
-            PassPlan p;
-            p.narrow = true;
-            p.max_w = w;
-            p.splits = def.splits;
-            cands.push_back(p);
-        }
+        for (int w = 16; w <= kNarrowRowsW; w += 16)
+            for (int t = 0; t < (rows && tmem_a_default() ? 2 : 1); ++t) {
+                PassPlan p;
+                p.narrow = true;
+                p.tmem_a = t == 1;
+                p.max_w = w;
+                p.splits = def.splits;
+                cands.push_back(p);
+            }
     for (int pr = 0; pr < 2; ++pr) {
         if (pr == 1 && (mode == 0 || tiles % 2 != 0 || num_sms() < 2)) continue;
         if (pr == 0 && mode == 2) continue;
@@ -1297,6 +1354,8 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+        else if (plan.narrow && plan.tmem_a)
+            launch_pass<true, false, true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else if (plan.narrow)
             launch_pass<true, false, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else
@@ -1503,11 +1562,12 @@ std::string autotune_json() {
         const TuneEntry& e = kv.second;
         std::snprintf(buf, sizeof buf,
                       "%s{\"pass\": \"%s\", \"R\": %lld, \"n\": %lld, \"k\": %lld, "
-                      "\"pairs\": %s, \"narrow\": %s, \"max_width\": %d, \"slices\": %d, "
+                      "\"pairs\": %s, \"narrow\": %s, \"tmem_a\": %s, \"max_width\": %d, \"slices\": %d, "
                       "\"candidates\": %d, \"ms_best\": %.4f, \"ms_default\": %.4f}",
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
-                      e.plan.narrow ? "true" : "false", e.plan.max_w, e.plan.splits, e.candidates,
+                      e.plan.narrow ? "true" : "false", e.plan.tmem_a ? "true" : "false", e.plan.max_w,
+                      e.plan.splits, e.candidates,
                       e.ms_best, e.ms_default);
         out += buf;
         first = false;
