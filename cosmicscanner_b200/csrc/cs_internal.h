@@ -82,8 +82,9 @@ void device_free(void* p) noexcept;
 // waiting for the whole device, so a buffer is only reused after the work queued before its
 // release has finished.  nullptr restores the device-wide synchronisation.
 void set_thread_free_stream(cudaStream_t s);
-// Destroys the calling thread's cuBLAS / cuSOLVER handles (created on first use per thread and
-// device); threads that end while the process goes on (the serving workers) call it last.
+// Gives the calling thread's cuBLAS / cuSOLVER handles (created on first use per thread and
+// device) back to a free list that later threads take them from; threads that end while the
+// process goes on (the serving workers) call it last.
 void release_thread_handles() noexcept;
 
 // Device allocation that frees itself.

@@ -102,33 +102,37 @@ constexpr int kPairSamplesW = 80, kPairSamplesST = 3, kPairSamplesSP = 6, kPairS
 constexpr int kNarrowRowsW = 32, kNarrowRowsST = 4, kNarrowRowsSP = 8, kNarrowRowsSD = 4;
 static_assert(kNarrowRowsW == 32, "the plans use one narrow width for both passes");
 constexpr int kNarrowSamplesW = 32, kNarrowSamplesST = 3, kNarrowSamplesSP = 8, kNarrowSamplesSD = 4;
-// The narrow rows pass with its A operand in tensor memory (TMEMA): the decoders store the
-// imputed-code and missing-indicator tiles into TMEM (tcgen05.st) and the MMAs read them
-// there, so shared memory carries only the packed tiles and the B pieces.  TMEM: two
-// accumulators of 5 x 32 columns, then three A stages of 64 columns (32 per tile: 128 int8
-// K elements per lane).
+// Narrow passes with their A operand in tensor memory (TMEMA): the decoders store the two
+// genotype tiles into TMEM (tcgen05.st) and the MMAs read them there, so shared memory
+// carries only the packed tiles and the B pieces.  A TMEM operand must be K-major, so the
+// samples pass then reads a sample-major copy of the packed matrix (rows = samples, four
+// SNPs per byte) and decodes it like the rows pass, with the fixed dosage table (the per-SNP
+// imputed codes cannot share one byte-permute table along K): its B carries W and mu o W,
+// three pieces each, the six-set form.  TMEM: two accumulators (5 x 32 columns rows, 3 x 32
+// samples), then A stages of 64 columns (32 per tile: 128 int8 K elements per lane).
 constexpr int kTmemARowsST = 8, kTmemARowsSP = 16, kTmemARowsSD = 3;
-constexpr uint32_t kTmemAccStride = 5 * kNarrowRowsW, kTmemAStage = 64;
+constexpr int kTmemASamplesST = 4, kTmemASamplesSP = 16, kTmemASamplesSD = 4;
+constexpr uint32_t kTmemAStage = 64;
 
 template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
-    static_assert(!TMEMA || (ROWS && NARROW), "A in TMEM: the narrow rows pass only");
-    static constexpr int kPieces = ROWS ? 3 : 5;  // per column tile, over the pair
+    static_assert(!TMEMA || (NARROW && !PAIR), "A in TMEM: the narrow single-CTA passes");
+    static constexpr int kPieces = ROWS ? 3 : (TMEMA ? 6 : 5);  // per column tile, over the pair
     static constexpr int kMaxW = NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = TMEMA ? kTmemARowsST
+    static constexpr int kTmaStages = TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
                                       : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = TMEMA ? kTmemARowsSP
+    static constexpr int kPackedStages = TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
                                          : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = TMEMA ? kTmemARowsSD
+    static constexpr int kDecodeStages = TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
                                          : NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
                                          : PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
     static constexpr int kAccCols = ROWS ? 5 * kMaxW : 3 * kMaxW;
     static constexpr int kAccBufs = (ROWS && !NARROW) ? 1 : 2;
-    static constexpr uint32_t kAccStride = TMEMA ? kTmemAccStride : 256;
+    static constexpr uint32_t kAccStride = TMEMA ? (uint32_t)kAccCols : 256;
     // TMEM columns of decode stage d's imputed-code / missing-indicator tiles (TMEMA)
     static constexpr uint32_t kTmemA0 = kAccBufs * kAccStride;
     static __host__ __device__ constexpr uint32_t ta(int d) { return kTmemA0 + d * kTmemAStage; }
@@ -198,6 +202,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
     using L = Layout<ROWS, PAIR, NARROW, TMEMA>;
+    // K-major A tiles decoded from rows of K elements: the rows pass, and the samples pass over
+    // the sample-major copy
+    constexpr bool KMAJOR = ROWS || TMEMA;
     constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -342,7 +349,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             // MN-major A (the same tile read as samples x SNPs); N = 3 w (the three pieces
             // of a column tile side by side) for the imputed codes and 2 w for the missing
             // indicators, M = 128 (pair: 256)
-            const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((ROWS ? 0u : 1u) << 15) |
+            const uint32_t idesc0 = (2u << 4) | (1u << 7) | (1u << 10) | ((KMAJOR ? 0u : 1u) << 15) |
                                     ((uint32_t)((PAIR ? 2 : 1) * kTile >> 4) << 24);
             uint32_t j = 0;
             int ui = 0;
@@ -352,7 +359,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 const int w = width(ct);
                 const uint32_t idesc = idesc0 | ((uint32_t)((3 * w) >> 3) << 17);
-                const uint32_t idesc_m = idesc0 | ((uint32_t)((2 * w) >> 3) << 17);
+                // the missing-indicator MMA: two pieces, or the three of mu o W (samples, TMEMA)
+                const uint32_t idesc_m = idesc0 | ((uint32_t)(((!ROWS && TMEMA ? 3 : 2) * w) >> 3) << 17);
                 const int buf = ui % NB;
                 if (!(ok = wait_peer(&acc_empty[buf], ((ui / NB) & 1) ^ 1, kTimeoutMma))) break;
                 tc_fence_after();
@@ -377,7 +385,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                         if constexpr (TMEMA) {
                             // A from TMEM: 32 K elements = 8 columns per MMA
                             mma_i8_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
-                            mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m, first);
+                            mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
+                                          ROWS ? first : 1u);
                             continue;
                         }
                         const uint32_t aoff = ROWS ? ks * 32 : ks * 4096;  // 32 K elements
@@ -447,10 +456,11 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             unit_coords(u, tile, ct, split, kb0, kb1);
             // the row's imputed-code table: rows pass SNP tile * 128 + r, samples pass
             // kb * 128 + r (the packed tile's row)
-            uint32_t lut = ROWS ? __ldg(P.lut + (int64_t)tile * kTile + r) : 0u;
+            // (samples pass over the sample-major copy: the fixed dosage table 2 / 0 / 1 / 0)
+            uint32_t lut = ROWS ? __ldg(P.lut + (int64_t)tile * kTile + r) : 0x00010002u;
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
                 const int sp = j % SP, d = j % SD;
-                if (!ROWS) lut = __ldg(P.lut + (int64_t)kb * kKBlock + r);
+                if (!KMAJOR) lut = __ldg(P.lut + (int64_t)kb * kKBlock + r);
                 if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
                 if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
                 const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
@@ -508,8 +518,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                     const int sp = j % SP;
                     if (!(ok = mbar_wait(&empty_p[sp], ((j / SP) & 1) ^ 1, P.status, kTimeoutTma))) break;
                     mbar_arrive_expect_tx(&full_p[sp], (uint32_t)kPackedBytes);
-                    // packed tile: 128 SNP rows x 32 bytes (128 samples)
-                    if (ROWS)
+                    // packed tile: 128 rows x 32 bytes (128 K elements)
+                    if (KMAJOR)
                         tma_load_2d(smem + L::p(sp), &tm_a, kb * 32, tile * kTile, &full_p[sp]);
                     else
                         tma_load_2d(smem + L::p(sp), &tm_a, tile * 32, kb * kKBlock, &full_p[sp]);
@@ -534,7 +544,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             // rows pass: TMEM lane = SNP row; samples pass: lane = position in the decoded
             // tile, whose samples are interleaved within each group of 16
             const int lp = 32 * q + lane;
-            const int64_t row = (int64_t)tile * kTile + (ROWS ? lp : (lp & ~15) + sample_at(lp & 15));
+            const int64_t row = (int64_t)tile * kTile + (KMAJOR ? lp : (lp & ~15) + sample_at(lp & 15));
             const uint32_t tb = tmem_base + buf * L::kAccStride + ((uint32_t)(32 * q) << 16);
             const int w = width(ct);
             double* dst = P.part + ((int64_t)split * kp + (int64_t)ct * kc) * P.ld + row;
@@ -844,6 +854,100 @@ k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int
     }
 }
 
+// Sample-major copy of a packed view for the samples pass with A in TMEM: dst row i (sample,
+// i < n_pad) holds the 2-bit codes of SNPs 0..r_pad-1, four per byte (SNP t at bits
+// 2 (t % 4) of byte t / 4), stride r_pad / 4.  SNP rows past R read as code 0 (they meet zero
+// B rows); samples past the analysed ones keep the rows' missing-code padding.  One CTA per
+// 128-SNP x 128-sample tile: the tile's 128 x 32 packed bytes through shared memory, each
+// thread writing 16 bytes of one output row.
+__global__ void __launch_bounds__(256)
+k_transpose_packed(const uint8_t* __restrict__ src, int64_t R, int64_t stride,
+                   uint8_t* __restrict__ dst, int64_t stride_t) {
+    __shared__ uint8_t tile[kTile][32];
+    const int64_t t0 = (int64_t)blockIdx.x * kTile, b0 = (int64_t)blockIdx.y * 32;
+    for (int e = threadIdx.x; e < kTile * 32; e += 256) {
+        const int rr = e >> 5, cb = e & 31;
+        tile[rr][cb] = (t0 + rr < R) ? src[(t0 + rr) * stride + b0 + cb] : (uint8_t)0;
+    }
+    __syncthreads();
+    const int i = threadIdx.x >> 1;         // sample within the tile
+    const int g0 = (threadIdx.x & 1) * 16;  // first output byte (four SNPs each)
+    const int col = i >> 2, sh = 2 * (i & 3);
+    uint32_t out[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int g = 0; g < 16; ++g) {
+        uint32_t byte = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            byte |= (uint32_t)((tile[4 * (g0 + g) + j][col] >> sh) & 3) << (2 * j);
+        out[g >> 2] |= byte << (8 * (g & 3));
+    }
+    uint8_t* d = dst + (b0 * 4 + i) * stride_t + t0 / 4 + g0;
+    *reinterpret_cast<uint4*>(d) = make_uint4(out[0], out[1], out[2], out[3]);
+}
+
+// Column maxima of max(|W|, |mu o W|) for a column-major R x k W (the six-set samples operand).
+__global__ void __launch_bounds__(256)
+k_col_absmax_mu(const double* __restrict__ W, int64_t R, const double* __restrict__ mu,
+                unsigned long long* __restrict__ max_w) {
+    __shared__ double red_w[8];
+    const int64_t c = blockIdx.y;
+    double mw = 0.0;
+    const int64_t t0 = (int64_t)blockIdx.x * 2048;
+    for (int64_t t = t0 + threadIdx.x; t < min(R, t0 + 2048); t += 256) {
+        const double v = fabs(W[c * R + t]);
+        mw = fmax(mw, fmax(v, mu[t] * v));
+    }
+    for (int off = 16; off; off >>= 1) mw = fmax(mw, __shfl_xor_sync(0xffffffffu, mw, off));
+    if ((threadIdx.x & 31) == 0) red_w[threadIdx.x >> 5] = mw;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < 8; ++j) mw = fmax(mw, red_w[j]);
+        atomicMax(max_w + c, (unsigned long long)__double_as_longlong(mw));
+    }
+}
+
+// Six-set samples operand (A in TMEM over the sample-major copy): pieces of W f (rows q kp + c)
+// and of (mu o W) f (rows (3 + q) kp + c) at the K positions of the decoded tiles (SNPs
+// interleaved within groups of 16 like samples in the rows pass), f = 127 / max(|W|, |mu W|)
+// per column; 1/f per column; per-block sums of mu_t W[t][c] in cpart[blockIdx.x][c].
+// Grid: (r_pad / 2048, kp).
+__global__ void __launch_bounds__(256)
+k_split_samples_t_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int64_t kp,
+                          int64_t r_pad, const double* __restrict__ mu,
+                          const unsigned long long* __restrict__ max_wmu, int8_t* __restrict__ B,
+                          double* __restrict__ inv_f, double* __restrict__ cpart) {
+    __shared__ double red[8];
+    const int64_t c = blockIdx.y;
+    const double f = c < k ? quant_factor(max_wmu[c]) : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) inv_f[c] = f > 0.0 ? 1.0 / f : 0.0;
+    double cs = 0.0;
+    const int64_t t0 = (int64_t)blockIdx.x * 2048;
+    for (int64_t t = t0 + threadIdx.x; t < min(r_pad, t0 + 2048); t += 256) {
+        int8_t a1 = 0, a2 = 0, a3 = 0, b1 = 0, b2 = 0, b3 = 0;
+        if (c < k && t < R) {
+            const double w = Wt[c * R + t];
+            quantise3(w * f, a1, a2, a3);
+            quantise3(mu[t] * w * f, b1, b2, b3);
+            cs += mu[t] * w;
+        }
+        const int64_t pos = (t & ~(int64_t)15) + position_of((int)(t & 15));
+        B[c * r_pad + pos] = a1;
+        B[(kp + c) * r_pad + pos] = a2;
+        B[(2 * kp + c) * r_pad + pos] = a3;
+        B[(3 * kp + c) * r_pad + pos] = b1;
+        B[(4 * kp + c) * r_pad + pos] = b2;
+        B[(5 * kp + c) * r_pad + pos] = b3;
+    }
+    for (int off = 16; off; off >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cs;
+    __syncthreads();
+    if (threadIdx.x == 0 && c < k) {
+        for (int j = 1; j < 8; ++j) cs += red[j];
+        cpart[(int64_t)blockIdx.x * k + c] = cs;
+    }
+}
+
 // Samples-pass reduction: Y[i][c] = (sum_z part[z][c][i] - c0_c) / M.
 __global__ void k_reduce_samples(const double* __restrict__ part, int splits, int64_t kp,
                                  int64_t ld, int64_t n, int64_t k, const double* __restrict__ c0,
@@ -955,12 +1059,17 @@ struct MixedRows {
     DeviceBuffer<double> mu, exc, s, resid;
     DeviceBuffer<uint32_t> lut;  // imputed code of each 2-bit code, one byte per code
     CUtensorMap tm{};
+    const uint8_t* rows = nullptr;  // the view's packed rows (owned by the operator)
+    int64_t stride = 0;
+    // sample-major copy for the narrow samples pass with A in TMEM (made on first use)
+    DeviceBuffer<uint8_t> packed_t;
+    CUtensorMap tm_t{};
 };
 
 struct MixedWorkspace {
     DeviceBuffer<int8_t> b1, b2;
     DeviceBuffer<double> part, colpart, mean1, qsum, c0, W, inv_f;
-    DeviceBuffer<unsigned long long> max1, max_w;
+    DeviceBuffer<unsigned long long> max1, max_w, max_wmu;
     CUtensorMap tm_b1{}, tm_b2{};
     CUtensorMap tm_b1t{}, tm_b2t{};  // boxes of the last column tile's width
     const void* tm_b1_base = nullptr;
@@ -996,6 +1105,7 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<true, false, true>();
         if (err == cudaSuccess) err = allow_smem<false, false, true>();
         if (err == cudaSuccess) err = allow_smem<true, false, true, true>();
+        if (err == cudaSuccess) err = allow_smem<false, false, true, true>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -1093,6 +1203,22 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     // packed tiles: 32 bytes (128 samples) x 128 SNP rows; rows past R read as zeros and
     // either land in discarded output rows (rows pass) or meet zero B rows (samples pass)
     r.tm = make_map_u8(v.rows, v.stride, std::max<int64_t>(r.R, 1), v.stride, 32, kTile, false);
+    r.rows = v.rows;
+    r.stride = v.stride;
+}
+
+// The sample-major copy of the view (once per context): n_pad rows of r_pad / 4 bytes.
+void ensure_transposed(MixedRows& r, cudaStream_t s) {
+    if (r.packed_t.get()) return;
+    const int64_t stride_t = r.r_pad / 4;
+    r.packed_t.resize((size_t)(r.n_pad * stride_t));
+    {
+        prof::Scope ps("transpose_packed", s, 0.0, 2.0 * (double)r.n_pad * (double)stride_t);
+        dim3 g((unsigned)(r.r_pad / kTile), (unsigned)(r.n_pad / kTile));
+        k_transpose_packed<<<g, 256, 0, s>>>(r.rows, r.R, r.stride, r.packed_t.get(), stride_t);
+        CS_LAUNCH("transpose_packed");
+    }
+    r.tm_t = make_map_u8(r.packed_t.get(), stride_t, r.n_pad, stride_t, 32, kTile, false);
 }
 
 struct Tiling {
@@ -1154,7 +1280,7 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
     PassPlan p;
     p.pairs = use_cta_pairs(k) && tiles % 2 == 0;
     p.narrow = !p.pairs && k <= kNarrowRowsW && narrow_layouts();
-    p.tmem_a = rows && p.narrow && tmem_a_default();
+    p.tmem_a = p.narrow && tmem_a_default();
     p.max_w = p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
     const Tiling tl = tiling_for(k, p.max_w);
@@ -1213,7 +1339,7 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
     const int mode = pair_mode();
     if (mode != 2 && narrow_layouts())
         for (int w = 16; w <= kNarrowRowsW; w += 16)
-            for (int t = 0; t < (rows && tmem_a_default() ? 2 : 1); ++t) {
+            for (int t = 0; t < (tmem_a_default() ? 2 : 1); ++t) {
                 PassPlan p;
                 p.narrow = true;
                 p.tmem_a = t == 1;
@@ -1387,26 +1513,40 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     const int splits = (kb + kbs - 1) / kbs;  // no empty slice
     if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "samples pass: K slice exceeds the exact int32 range");
     const int nrb = (int)((r_pad + 2047) / 2048);
-    ws.b2.resize(5 * kp * r_pad);
+    // A in TMEM: the six-set form over the sample-major copy
+    const bool tmem_a = plan.narrow && plan.tmem_a;
+    const int pieces = tmem_a ? 6 : 5;
+    if (tmem_a) ensure_transposed(r, s);
+    ws.b2.resize(pieces * kp * r_pad);
     ws.part.resize((int64_t)splits * kp * n_pad);
     ws.colpart.resize((int64_t)nrb * k);
     ws.inv_f.resize(kp);
     ws.c0.resize(k);
     // boxes of one column tile's rows (pairs: half of them)
     const int box = pairs ? tl.kc / 2 : tl.kc, box_last = pairs ? tl.kc_last / 2 : tl.kc_last;
-    const int64_t key = ((kp * 1000003 + r_pad) * 131 + box_last) * 131 + box;
+    const int64_t key = (((kp * 1000003 + r_pad) * 131 + box_last) * 131 + box) * 7 + pieces;
     if (ws.tm_b2_base != ws.b2.get() || ws.tm_b2_key != key) {
-        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, 5 * kp, r_pad, kKBlock, box, true);
-        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, 5 * kp, r_pad, kKBlock, box_last, true);
+        ws.tm_b2 = make_map_u8(ws.b2.get(), r_pad, pieces * kp, r_pad, kKBlock, box, true);
+        ws.tm_b2t = make_map_u8(ws.b2.get(), r_pad, pieces * kp, r_pad, kKBlock, box_last, true);
         ws.tm_b2_base = ws.b2.get();
         ws.tm_b2_key = key;
     }
     {
-        prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + 5.0 * kp * r_pad);
+        prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + pieces * kp * r_pad);
         dim3 g((unsigned)nrb, (unsigned)kp);
-        k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), r.resid.get(),
-                                                  ws.max_w.get(), ws.b2.get(), ws.inv_f.get(),
-                                                  ws.colpart.get());
+        if (tmem_a) {
+            ws.max_wmu.resize(k);
+            CS_CUDA(cudaMemsetAsync(ws.max_wmu.get(), 0, 8 * k, s));
+            k_col_absmax_mu<<<dim3((unsigned)nrb, (unsigned)k), 256, 0, s>>>(Wt, R, r.mu.get(),
+                                                                            ws.max_wmu.get());
+            k_split_samples_t_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(),
+                                                        ws.max_wmu.get(), ws.b2.get(),
+                                                        ws.inv_f.get(), ws.colpart.get());
+        } else {
+            k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), r.resid.get(),
+                                                      ws.max_w.get(), ws.b2.get(), ws.inv_f.get(),
+                                                      ws.colpart.get());
+        }
         k_sum_partials<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get());
         CS_LAUNCH("mixed samples operand");
     }
@@ -1429,6 +1569,8 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
+        else if (tmem_a)
+            launch_pass<false, false, true, true>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
         else if (plan.narrow)
             launch_pass<false, false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         else

@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "cs_internal.h"
 
@@ -39,6 +40,11 @@ bool poison_allocations() {
 
 thread_local cublasHandle_t t_blas[kMaxDevices] = {};
 thread_local cusolverDnHandle_t t_solver[kMaxDevices] = {};
+// Handles given back by threads that ended (release_thread_handles), reused by new threads:
+// creating and destroying them per request thread costs device-wide synchronisations.
+std::mutex g_handle_mu;
+std::vector<cublasHandle_t> g_free_blas[kMaxDevices];
+std::vector<cusolverDnHandle_t> g_free_solver[kMaxDevices];
 
 // Gives the pool's reserved free blocks back to the device (after the device has finished
 // with them), when an allocation found no room: the pool keeps freed blocks reserved, which
@@ -79,6 +85,13 @@ cublasHandle_t shared_blas() {
     int dev = 0;
     CS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
+    if (!t_blas[dev]) {
+        std::lock_guard<std::mutex> lk(g_handle_mu);
+        if (!g_free_blas[dev].empty()) {
+            t_blas[dev] = g_free_blas[dev].back();
+            g_free_blas[dev].pop_back();
+        }
+    }
     if (!t_blas[dev] && cublasCreate(&t_blas[dev]) != CUBLAS_STATUS_SUCCESS) {
         t_blas[dev] = nullptr;
         trim_pool(dev);
@@ -94,6 +107,13 @@ cusolverDnHandle_t shared_solver() {
     int dev = 0;
     CS_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) fail(CS_ERR_CUDA, "device ordinal out of range");
+    if (!t_solver[dev]) {
+        std::lock_guard<std::mutex> lk(g_handle_mu);
+        if (!g_free_solver[dev].empty()) {
+            t_solver[dev] = g_free_solver[dev].back();
+            g_free_solver[dev].pop_back();
+        }
+    }
     if (!t_solver[dev] && cusolverDnCreate(&t_solver[dev]) != CUSOLVER_STATUS_SUCCESS) {
         t_solver[dev] = nullptr;
         trim_pool(dev);
@@ -106,16 +126,20 @@ cusolverDnHandle_t shared_solver() {
 }
 
 void release_thread_handles() noexcept {
-    int cur = 0;
-    if (cudaGetDevice(&cur) != cudaSuccess) return;
+    // back to the free lists, bound to the legacy stream (the thread's own stream is about to
+    // be destroyed; every user sets its stream before use)
+    std::lock_guard<std::mutex> lk(g_handle_mu);
     for (int d = 0; d < kMaxDevices; ++d) {
-        if (!t_blas[d] && !t_solver[d]) continue;
-        if (d != cur) cudaSetDevice(d);
-        if (t_blas[d]) cublasDestroy(t_blas[d]);
-        if (t_solver[d]) cusolverDnDestroy(t_solver[d]);
-        t_blas[d] = nullptr;
-        t_solver[d] = nullptr;
-        if (d != cur) cudaSetDevice(cur);
+        if (t_blas[d]) {
+            cublasSetStream(t_blas[d], 0);
+            g_free_blas[d].push_back(t_blas[d]);
+            t_blas[d] = nullptr;
+        }
+        if (t_solver[d]) {
+            cusolverDnSetStream(t_solver[d], 0);
+            g_free_solver[d].push_back(t_solver[d]);
+            t_solver[d] = nullptr;
+        }
     }
 }
 

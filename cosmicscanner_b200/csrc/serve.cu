@@ -356,7 +356,7 @@ void cs_server::run_request(Request* r) {
     }
     cs::set_thread_free_stream(nullptr);
     if (st) cudaStreamSynchronize(st);
-    // this thread ends here: its library handles (and their workspaces) go with it
+    // this thread ends here: its library handles go back to the free list for the next worker
     cs::release_thread_handles();
     if (st) cudaStreamDestroy(st);
     {
