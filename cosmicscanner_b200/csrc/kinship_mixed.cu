@@ -108,30 +108,39 @@ constexpr int kNarrowSamplesW = 32, kNarrowSamplesST = 3, kNarrowSamplesSP = 8, 
 // samples pass then reads a sample-major copy of the packed matrix (rows = samples, four
 // SNPs per byte) and decodes it like the rows pass, with the fixed dosage table (the per-SNP
 // imputed codes cannot share one byte-permute table along K): its B carries W and mu o W,
-// three pieces each, the six-set form.  TMEM: two accumulators (5 x 32 columns rows, 3 x 32
-// samples), then A stages of 64 columns (32 per tile: 128 int8 K elements per lane).
+// three pieces each, the six-set form.  TMEMA = 1: column tiles of at most 32, two
+// accumulators (5 x 32 columns rows, 3 x 32 samples); TMEMA = 2: tiles of at most 64, one
+// accumulator (5 x 64 / 3 x 64), for 33 to 64 right-hand sides.  Then A stages of 64 TMEM
+// columns (32 per tile: 128 int8 K elements per lane).
 constexpr int kTmemARowsST = 8, kTmemARowsSP = 16, kTmemARowsSD = 3;
 constexpr int kTmemASamplesST = 4, kTmemASamplesSP = 16, kTmemASamplesSD = 4;
+constexpr int kTmemA64W = 64;
+constexpr int kTmemA64RowsST = 6, kTmemA64RowsSP = 12, kTmemA64RowsSD = 3;
+constexpr int kTmemA64SamplesST = 3, kTmemA64SamplesSP = 12, kTmemA64SamplesSD = 4;
 constexpr uint32_t kTmemAStage = 64;
 
-template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
     static_assert(!TMEMA || (NARROW && !PAIR), "A in TMEM: the narrow single-CTA passes");
     static constexpr int kPieces = ROWS ? 3 : (TMEMA ? 6 : 5);  // per column tile, over the pair
-    static constexpr int kMaxW = NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
+    static constexpr int kMaxW = TMEMA == 2 ? kTmemA64W
+                                 : NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
+    static constexpr int kTmaStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsST : kTmemA64SamplesST)
+                                      : TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
                                       : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
+    static constexpr int kPackedStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsSP : kTmemA64SamplesSP)
+                                         : TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
                                          : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
+    static constexpr int kDecodeStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsSD : kTmemA64SamplesSD)
+                                         : TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
                                          : NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
                                          : PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
     static constexpr int kAccCols = ROWS ? 5 * kMaxW : 3 * kMaxW;
-    static constexpr int kAccBufs = (ROWS && !NARROW) ? 1 : 2;
+    static constexpr int kAccBufs = ((ROWS && !NARROW) || TMEMA == 2) ? 1 : 2;
     static constexpr uint32_t kAccStride = TMEMA ? (uint32_t)kAccCols : 256;
     // TMEM columns of decode stage d's imputed-code / missing-indicator tiles (TMEMA)
     static constexpr uint32_t kTmemA0 = kAccBufs * kAccStride;
@@ -197,14 +206,14 @@ __device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint32_t lut
 __host__ __device__ __forceinline__ int sample_at(int p) { return p < 8 ? 2 * p : 2 * (p - 8) + 1; }
 __host__ __device__ __forceinline__ int position_of(int s) { return (s & 1) ? 8 + (s >> 1) : s >> 1; }
 
-template <bool ROWS, bool PAIR, bool NARROW, bool TMEMA>
+template <bool ROWS, bool PAIR, bool NARROW, int TMEMA>
 __global__ void __launch_bounds__(kThreads, 1)
 k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
              const __grid_constant__ CUtensorMap tm_bt, PassArgs P) {
     using L = Layout<ROWS, PAIR, NARROW, TMEMA>;
     // K-major A tiles decoded from rows of K elements: the rows pass, and the samples pass over
     // the sample-major copy
-    constexpr bool KMAJOR = ROWS || TMEMA;
+    constexpr bool KMAJOR = ROWS || TMEMA != 0;
     constexpr int ST = L::kTmaStages, SP = L::kPackedStages, SD = L::kDecodeStages, NB = L::kAccBufs;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -1016,15 +1025,21 @@ int pair_mode() {
     }();
     return mode;
 }
-// The narrow rows pass with A in TMEM (CS_B200_TMEM_A=0: A in shared memory).  Measured at
-// N=50k, M=100k: 0.70 vs 1.03 ms per pass at k <= 16, 0.81 vs 1.09 at k = 32.
-bool tmem_a_default() {
-    static const bool on = [] {
+// The narrow passes with A in TMEM, and the 64-wide form of them for 33 to 64 right-hand sides
+// instead of CTA pairs (CS_B200_TMEM_A=0: A in shared memory; =1: the 32-wide form only).
+// Measured at N=50k, M=100k, per pass (rows / samples): k <= 16 0.70 / 0.80 ms against
+// 1.03 / 1.14 with A in shared memory; k = 34 0.90 / 1.07 against 1.15 / 1.24 on CTA pairs;
+// k = 64 1.02 / 1.21 against 1.22 / 1.25.
+int tmem_a_mode() {
+    static const int mode = [] {
         const char* v = std::getenv("CS_B200_TMEM_A");
-        return !(v && std::strcmp(v, "0") == 0);
+        if (v && std::strcmp(v, "0") == 0) return 0;
+        if (v && std::strcmp(v, "1") == 0) return 1;
+        return 2;
     }();
-    return on;
+    return mode;
 }
+bool tmem_a_default() { return tmem_a_mode() != 0; }
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
 bool narrow_layouts() {
     static const bool on = [] {
@@ -1088,7 +1103,7 @@ void destroy_mixed(MixedOperator* m) { delete m; }
 
 namespace {
 
-template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 cudaError_t allow_smem() {
     return cudaFuncSetAttribute(k_mixed_pass<ROWS, PAIR, NARROW, TMEMA>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1104,8 +1119,10 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<false, true>();
         if (err == cudaSuccess) err = allow_smem<true, false, true>();
         if (err == cudaSuccess) err = allow_smem<false, false, true>();
-        if (err == cudaSuccess) err = allow_smem<true, false, true, true>();
-        if (err == cudaSuccess) err = allow_smem<false, false, true, true>();
+        if (err == cudaSuccess) err = allow_smem<true, false, true, 1>();
+        if (err == cudaSuccess) err = allow_smem<false, false, true, 1>();
+        if (err == cudaSuccess) err = allow_smem<true, false, true, 2>();
+        if (err == cudaSuccess) err = allow_smem<false, false, true, 2>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -1132,14 +1149,14 @@ int resident_pairs() {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true, false, false>, &cfg));
+        CS_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_mixed_pass<ROWS, true, false, 0>, &cfg));
         n = std::max(1, std::min(clusters, num_sms() / 2));
     }
     return n;
 }
 
 // One CTA per SM, or (PAIR) as many clusters of two CTAs as are resident together.
-template <bool ROWS, bool PAIR, bool NARROW = false, bool TMEMA = false>
+template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
                  const PassArgs& P, cudaStream_t s) {
     if (PAIR) {
@@ -1155,7 +1172,7 @@ void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false, false>, ta, tb, tbt, P));
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false, 0>, ta, tb, tbt, P));
     } else {
         k_mixed_pass<ROWS, false, NARROW, TMEMA>
             <<<num_sms(), kThreads, Layout<ROWS, false, NARROW, TMEMA>::kSmem, s>>>(
@@ -1268,7 +1285,7 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 struct PassPlan {
     bool pairs = false;
     bool narrow = false;  // single-CTA layout for column tiles of at most 32
-    bool tmem_a = false;  // narrow rows pass with the A operand in TMEM
+    int tmem_a = 0;       // narrow passes with the A operand in TMEM: 1 (tiles <= 32), 2 (<= 64)
     int max_w = 0;
     int splits = 1;
     bool same_kernel(const PassPlan& o) const {
@@ -1280,8 +1297,15 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
     PassPlan p;
     p.pairs = use_cta_pairs(k) && tiles % 2 == 0;
     p.narrow = !p.pairs && k <= kNarrowRowsW && narrow_layouts();
-    p.tmem_a = p.narrow && tmem_a_default();
-    p.max_w = p.narrow ? kNarrowRowsW
+    p.tmem_a = p.narrow && tmem_a_default() ? 1 : 0;
+    if (tmem_a_mode() == 2 && narrow_layouts() && k > kNarrowRowsW && k <= kTmemA64W &&
+        pair_mode() != 2) {
+        p.pairs = false;
+        p.narrow = true;
+        p.tmem_a = 2;
+    }
+    p.max_w = p.tmem_a == 2 ? kTmemA64W
+              : p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
     const Tiling tl = tiling_for(k, p.max_w);
     p.splits = p.pairs ? choose_splits(tiles / 2 * tl.n_ctiles, kb, 4LL * num_sms())
@@ -1342,11 +1366,20 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
             for (int t = 0; t < (tmem_a_default() ? 2 : 1); ++t) {
                 PassPlan p;
                 p.narrow = true;
-                p.tmem_a = t == 1;
+                p.tmem_a = t;
                 p.max_w = w;
                 p.splits = def.splits;
                 cands.push_back(p);
             }
+    if (mode != 2 && narrow_layouts() && tmem_a_default() && k > kNarrowRowsW)
+        for (int w = 48; w <= kTmemA64W; w += 16) {
+            PassPlan p;
+            p.narrow = true;
+            p.tmem_a = 2;
+            p.max_w = w;
+            p.splits = def.splits;
+            cands.push_back(p);
+        }
     for (int pr = 0; pr < 2; ++pr) {
         if (pr == 1 && (mode == 0 || tiles % 2 != 0 || num_sms() < 2)) continue;
         if (pr == 0 && mode == 2) continue;
@@ -1480,8 +1513,10 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+        else if (plan.narrow && plan.tmem_a == 2)
+            launch_pass<true, false, true, 2>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else if (plan.narrow && plan.tmem_a)
-            launch_pass<true, false, true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+            launch_pass<true, false, true, 1>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else if (plan.narrow)
             launch_pass<true, false, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else
@@ -1514,7 +1549,7 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "samples pass: K slice exceeds the exact int32 range");
     const int nrb = (int)((r_pad + 2047) / 2048);
     // A in TMEM: the six-set form over the sample-major copy
-    const bool tmem_a = plan.narrow && plan.tmem_a;
+    const bool tmem_a = plan.narrow && plan.tmem_a != 0;
     const int pieces = tmem_a ? 6 : 5;
     if (tmem_a) ensure_transposed(r, s);
     ws.b2.resize(pieces * kp * r_pad);
@@ -1569,8 +1604,10 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
                        (double)R * (double)((n + 3) / 4));
         if (pairs)
             launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
+        else if (tmem_a && plan.tmem_a == 2)
+            launch_pass<false, false, true, 2>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
         else if (tmem_a)
-            launch_pass<false, false, true, true>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
+            launch_pass<false, false, true, 1>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
         else if (plan.narrow)
             launch_pass<false, false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         else
@@ -1708,7 +1745,7 @@ std::string autotune_json() {
                       "\"candidates\": %d, \"ms_best\": %.4f, \"ms_default\": %.4f}",
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
-                      e.plan.narrow ? "true" : "false", e.plan.tmem_a ? "true" : "false", e.plan.max_w,
+                      e.plan.narrow ? "true" : "false", e.plan.tmem_a ? (e.plan.tmem_a == 2 ? "64" : "32") : "false", e.plan.max_w,
                       e.plan.splits, e.candidates,
                       e.ms_best, e.ms_default);
         out += buf;
