@@ -170,6 +170,9 @@ struct cs_kinship {
     cs::DeviceBuffer<double> buf_x, buf_u, buf_y;
     cs::MixedOperator* mixed = nullptr;
     bool autotune = true;  // the tensor-core passes may tune their plan on new shapes
+    // every mixed samples pass uses the five-set arithmetic (no six-set TMEM form), so a column's
+    // result does not depend on how many columns share its apply (the serving loop's stacking)
+    bool width_independent = false;
     ~cs_kinship() { cs::destroy_mixed(mixed); }
 };
 

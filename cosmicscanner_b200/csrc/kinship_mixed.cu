@@ -1634,12 +1634,24 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
 }
 
 void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
-                  double* Y, int64_t ldy, cudaStream_t s, bool allow_tune) {
+                  double* Y, int64_t ldy, cudaStream_t s, bool allow_tune,
+                  bool width_independent = false) {
     const int64_t tiles = r.n_pad / kTile;
     const int kb = (int)(r.r_pad / kKBlock);
-    const PassPlan plan = choose_plan(false, allow_tune, r.R, r.n, k, tiles, kb, s, [&](const PassPlan& p) {
-        samples_pass_plan(p, r, ws, Wt, k, inv_m, Y, ldy, s);
-    });
+    PassPlan plan = choose_plan(false, allow_tune && !width_independent, r.R, r.n, k, tiles, kb, s,
+                                [&](const PassPlan& p) {
+                                    samples_pass_plan(p, r, ws, Wt, k, inv_m, Y, ldy, s);
+                                });
+    if (width_independent && plan.tmem_a) {
+        // the five-set form at every width: A in shared memory (narrow up to 32 columns,
+        // otherwise the general layouts); the slice count stays the default plan's
+        plan.tmem_a = 0;
+        if (plan.max_w > kNarrowSamplesW) {
+            plan.narrow = false;
+            plan.pairs = use_cta_pairs(k) && tiles % 2 == 0;
+            plan.max_w = plan.pairs ? kPairSamplesW : kSamplesW;
+        }
+    }
     samples_pass_plan(plan, r, ws, Wt, k, inv_m, Y, ldy, s);
 }
 
@@ -1672,7 +1684,7 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     m->last_k = 0;
     rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s, op->autotune);
     samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s,
-                 op->autotune);
+                 op->autotune, op->width_independent);
     check_status(m->ws, s);
     m->last_k = k;
 }
@@ -1727,7 +1739,7 @@ void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, 
         k_col_absmax<<<g, 256, 0, s>>>(Wcol, R, k, ws.max_w.get());
         CS_LAUNCH("col_absmax");
     }
-    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune);
+    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune, op->width_independent);
     check_status(ws, s);
 }
 

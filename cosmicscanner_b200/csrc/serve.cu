@@ -304,6 +304,7 @@ void cs_server::run_request(Request* r) {
                                          variants.empty() ? nullptr : variants.data(),
                                          (int64_t)variants.size()));
             sub->autotune = false;  // per-request shapes: the default plans, no tuning passes
+            sub->width_independent = true;  // same result alone and in a stack
             cs_kinship* so = sub.get();
             const int prec = opt.precision;
             target.apply = [so, prec](const double* X, int64_t ldx, int64_t k, double* Y,
@@ -407,6 +408,7 @@ cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t
         sv->g = g;
         sv->op = kinship_create(g, nullptr, 0, variants, n_var);
         sv->op->autotune = false;  // stacked widths vary from apply to apply
+        sv->op->width_independent = true;  // same result alone and in a stack
         if (variants && n_var > 0) sv->variants.assign(variants, variants + n_var);
         if (sv->opt.memory_budget_gb > 0.0) {
             sv->budget_bytes = (int64_t)(sv->opt.memory_budget_gb * 1e9);
