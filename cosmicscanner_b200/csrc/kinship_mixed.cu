@@ -36,8 +36,13 @@
 // resident) into a ring of stages; warps 2-9 decode; warp 1 issues the MMAs from one thread
 // into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.
 // The decoded tile (SNP rows x samples) serves as a K-major A operand in the rows pass and
-// as an MN-major A operand in the samples pass.  Every wait is bounded; a timeout leaves a
-// status code that the host reports as an error.
+// as an MN-major A operand in the samples pass.  Blocks of up to 64 columns (TMEMA layouts)
+// decode into tensor memory instead (tcgen05.st) and the MMAs read A from there; the samples
+// pass then reads a sample-major copy of the packed matrix, where A is K-major too, with the
+// fixed dosage table and W / mu o W in six operand sets.  Wide blocks run on CTA pairs
+// (cta_group::2): the partner CTA's MMA warp forwards each of its landed B stages to the
+// leader.  Every wait is bounded; a timeout leaves a status code that the host reports as an
+// error.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
