@@ -122,30 +122,37 @@ constexpr int kTmemASamplesST = 4, kTmemASamplesSP = 16, kTmemASamplesSD = 4;
 constexpr int kTmemA64W = 64;
 constexpr int kTmemA64RowsST = 6, kTmemA64RowsSP = 12, kTmemA64RowsSD = 3;
 constexpr int kTmemA64SamplesST = 3, kTmemA64SamplesSP = 12, kTmemA64SamplesSD = 4;
+// TMEMA = 3: the rows pass on CTA pairs with A in TMEM, column tiles of at most 64 (each CTA
+// holds half of the B pieces, as in the shared-memory pair form).
+constexpr int kTmemAPairRowsST = 8, kTmemAPairRowsSP = 16, kTmemAPairRowsSD = 3;
 constexpr uint32_t kTmemAStage = 64;
 
 template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
-    static_assert(!TMEMA || (NARROW && !PAIR), "A in TMEM: the narrow single-CTA passes");
+    static_assert(!TMEMA || (TMEMA == 3 ? (ROWS && PAIR && !NARROW) : (NARROW && !PAIR)),
+                  "A in TMEM: the narrow single-CTA passes, or the rows pass on CTA pairs");
     static constexpr int kPieces = ROWS ? 3 : (TMEMA ? 6 : 5);  // per column tile, over the pair
-    static constexpr int kMaxW = TMEMA == 2 ? kTmemA64W
+    static constexpr int kMaxW = TMEMA >= 2 ? kTmemA64W
                                  : NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsST : kTmemA64SamplesST)
+    static constexpr int kTmaStages = TMEMA == 3 ? kTmemAPairRowsST
+                                      : TMEMA == 2 ? (ROWS ? kTmemA64RowsST : kTmemA64SamplesST)
                                       : TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
                                       : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsSP : kTmemA64SamplesSP)
+    static constexpr int kPackedStages = TMEMA == 3 ? kTmemAPairRowsSP
+                                         : TMEMA == 2 ? (ROWS ? kTmemA64RowsSP : kTmemA64SamplesSP)
                                          : TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
                                          : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = TMEMA == 2 ? (ROWS ? kTmemA64RowsSD : kTmemA64SamplesSD)
+    static constexpr int kDecodeStages = TMEMA == 3 ? kTmemAPairRowsSD
+                                         : TMEMA == 2 ? (ROWS ? kTmemA64RowsSD : kTmemA64SamplesSD)
                                          : TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
                                          : NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
                                          : PAIR ? (ROWS ? kPairRowsSD : kPairSamplesSD) : (ROWS ? kRowsSD : kSamplesSD);
     static constexpr int kAccCols = ROWS ? 5 * kMaxW : 3 * kMaxW;
-    static constexpr int kAccBufs = ((ROWS && !NARROW) || TMEMA == 2) ? 1 : 2;
+    static constexpr int kAccBufs = ((ROWS && !NARROW) || TMEMA >= 2) ? 1 : 2;
     static constexpr uint32_t kAccStride = TMEMA ? (uint32_t)kAccCols : 256;
     // TMEM columns of decode stage d's imputed-code / missing-indicator tiles (TMEMA)
     static constexpr uint32_t kTmemA0 = kAccBufs * kAccStride;
@@ -396,11 +403,17 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                         const uint32_t first = (kb == kb0 && ks == 0) ? 0u : 1u;
                         const uint64_t db = smem_desc_sw128(b + ks * 32, 16, 1024);
                         const uint64_t dbm = smem_desc_sw128(bm + ks * 32, 16, 1024);
-                        if constexpr (TMEMA) {
+                        if constexpr (TMEMA != 0) {
                             // A from TMEM: 32 K elements = 8 columns per MMA
-                            mma_i8_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
-                            mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
-                                          ROWS ? first : 1u);
+                            if constexpr (PAIR) {
+                                mma_i8_pair_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
+                                mma_i8_pair_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
+                                                   first);
+                            } else {
+                                mma_i8_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
+                                mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
+                                              ROWS ? first : 1u);
+                            }
                             continue;
                         }
                         const uint32_t aoff = ROWS ? ks * 32 : ks * 4096;  // 32 K elements
@@ -1045,6 +1058,16 @@ int tmem_a_mode() {
     return mode;
 }
 bool tmem_a_default() { return tmem_a_mode() != 0; }
+// The rows pass on CTA pairs with A in TMEM (column tiles of at most 64) as the default pair
+// plan (CS_B200_TMEM_A_PAIRS=0: A in shared memory).  Measured at N=50k, M=100k per rows pass:
+// k = 96 1.76 vs 2.31 ms, k = 128 1.88 vs 2.33, k = 192 2.77 vs 3.41, k = 266 4.63 vs 4.92.
+bool tmem_a_pairs_default() {
+    static const bool on = [] {
+        const char* v = std::getenv("CS_B200_TMEM_A_PAIRS");
+        return !(v && std::strcmp(v, "0") == 0);
+    }();
+    return on;
+}
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
 bool narrow_layouts() {
     static const bool on = [] {
@@ -1128,6 +1151,7 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<false, false, true, 1>();
         if (err == cudaSuccess) err = allow_smem<true, false, true, 2>();
         if (err == cudaSuccess) err = allow_smem<false, false, true, 2>();
+        if (err == cudaSuccess) err = allow_smem<true, true, false, 3>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -1164,11 +1188,11 @@ int resident_pairs() {
 template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap& tbt,
                  const PassArgs& P, cudaStream_t s) {
-    if (PAIR) {
+    if constexpr (PAIR) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(2 * resident_pairs<ROWS>()));
         cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = Layout<ROWS, true>::kSmem;
+        cfg.dynamicSmemBytes = Layout<ROWS, true, false, TMEMA>::kSmem;
         cfg.stream = s;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1177,7 +1201,7 @@ void launch_pass(const CUtensorMap& ta, const CUtensorMap& tb, const CUtensorMap
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false, 0>, ta, tb, tbt, P));
+        CS_CUDA(cudaLaunchKernelEx(&cfg, k_mixed_pass<ROWS, true, false, TMEMA>, ta, tb, tbt, P));
     } else {
         k_mixed_pass<ROWS, false, NARROW, TMEMA>
             <<<num_sms(), kThreads, Layout<ROWS, false, NARROW, TMEMA>::kSmem, s>>>(
@@ -1309,7 +1333,8 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
         p.narrow = true;
         p.tmem_a = 2;
     }
-    p.max_w = p.tmem_a == 2 ? kTmemA64W
+    if (rows && p.pairs && tmem_a_default() && tmem_a_pairs_default()) p.tmem_a = 3;
+    p.max_w = p.tmem_a >= 2 ? kTmemA64W
               : p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
     const Tiling tl = tiling_for(k, p.max_w);
@@ -1376,6 +1401,15 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
                 p.splits = def.splits;
                 cands.push_back(p);
             }
+    if (rows && mode != 0 && tiles % 2 == 0 && num_sms() >= 2 && tmem_a_default())
+        for (int w = 48; w <= kTmemA64W; w += 16) {
+            PassPlan p;
+            p.pairs = true;
+            p.tmem_a = 3;
+            p.max_w = w;
+            p.splits = def.splits;
+            cands.push_back(p);
+        }
     if (mode != 2 && narrow_layouts() && tmem_a_default() && k > kNarrowRowsW)
         for (int w = 48; w <= kTmemA64W; w += 16) {
             PassPlan p;
@@ -1516,7 +1550,9 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        if (pairs)
+        if (pairs && plan.tmem_a == 3)
+            launch_pass<true, true, false, 3>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
+        else if (pairs)
             launch_pass<true, true>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
         else if (plan.narrow && plan.tmem_a == 2)
             launch_pass<true, false, true, 2>(r.tm, ws.tm_b1, ws.tm_b1t, P, s);
@@ -1762,7 +1798,9 @@ std::string autotune_json() {
                       "\"candidates\": %d, \"ms_best\": %.4f, \"ms_default\": %.4f}",
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
-                      e.plan.narrow ? "true" : "false", e.plan.tmem_a ? (e.plan.tmem_a == 2 ? "64" : "32") : "false", e.plan.max_w,
+                      e.plan.narrow ? "true" : "false",
+                      e.plan.tmem_a == 3 ? "\"pair64\"" : e.plan.tmem_a == 2 ? "64" : e.plan.tmem_a ? "32" : "false",
+                      e.plan.max_w,
                       e.plan.splits, e.candidates,
                       e.ms_best, e.ms_default);
         out += buf;

@@ -348,6 +348,16 @@ __device__ __forceinline__ void mma_i8_pair(uint32_t tmem_d, uint64_t adesc, uin
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
+// Leader only, A in tensor memory (each CTA's 128 rows in its own TMEM at the same address).
+__device__ __forceinline__ void mma_i8_pair_tmem_a(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
+                                                   uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
 // Leader only: once the pair's MMAs issued so far complete, arrive on the mbarrier at this
 // shared-memory offset in every CTA of cta_mask.
 __device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t cta_mask) {
