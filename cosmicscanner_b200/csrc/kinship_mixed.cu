@@ -125,28 +125,35 @@ constexpr int kTmemA64SamplesST = 3, kTmemA64SamplesSP = 12, kTmemA64SamplesSD =
 // TMEMA = 3: the rows pass on CTA pairs with A in TMEM, column tiles of at most 64 (each CTA
 // holds half of the B pieces, as in the shared-memory pair form).
 constexpr int kTmemAPairRowsST = 8, kTmemAPairRowsSP = 16, kTmemAPairRowsSD = 3;
+// TMEMA = 4: the samples pass on CTA pairs over the sample-major copy (six operand sets, each
+// CTA holding half of each set).
+constexpr int kTmemAPairSamplesST = 4, kTmemAPairSamplesSP = 16, kTmemAPairSamplesSD = 4;
 constexpr uint32_t kTmemAStage = 64;
 
 template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
-    static_assert(!TMEMA || (TMEMA == 3 ? (ROWS && PAIR && !NARROW) : (NARROW && !PAIR)),
-                  "A in TMEM: the narrow single-CTA passes, or the rows pass on CTA pairs");
+    static_assert(!TMEMA || (TMEMA == 3 ? (ROWS && PAIR && !NARROW)
+                             : TMEMA == 4 ? (!ROWS && PAIR && !NARROW) : (NARROW && !PAIR)),
+                  "A in TMEM: the narrow single-CTA passes, or the passes on CTA pairs");
     static constexpr int kPieces = ROWS ? 3 : (TMEMA ? 6 : 5);  // per column tile, over the pair
     static constexpr int kMaxW = TMEMA >= 2 ? kTmemA64W
                                  : NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = TMEMA == 3 ? kTmemAPairRowsST
+    static constexpr int kTmaStages = TMEMA == 4 ? kTmemAPairSamplesST
+                                      : TMEMA == 3 ? kTmemAPairRowsST
                                       : TMEMA == 2 ? (ROWS ? kTmemA64RowsST : kTmemA64SamplesST)
                                       : TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
                                       : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = TMEMA == 3 ? kTmemAPairRowsSP
+    static constexpr int kPackedStages = TMEMA == 4 ? kTmemAPairSamplesSP
+                                         : TMEMA == 3 ? kTmemAPairRowsSP
                                          : TMEMA == 2 ? (ROWS ? kTmemA64RowsSP : kTmemA64SamplesSP)
                                          : TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
                                          : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = TMEMA == 3 ? kTmemAPairRowsSD
+    static constexpr int kDecodeStages = TMEMA == 4 ? kTmemAPairSamplesSD
+                                         : TMEMA == 3 ? kTmemAPairRowsSD
                                          : TMEMA == 2 ? (ROWS ? kTmemA64RowsSD : kTmemA64SamplesSD)
                                          : TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
                                          : NARROW ? (ROWS ? kNarrowRowsSD : kNarrowSamplesSD)
@@ -340,17 +347,27 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                                             c * kp + ct * kc + (int)rank * hw, &full_t[s]);
                         } else {
                             // main set: half-pieces [p0a p0b p1a p1b p2a p2b], this CTA loads
-                            // 3 r .. 3 r + 2; residual set: piece 3 + r whole
+                            // 3 r .. 3 r + 2; residual set: piece 3 + r whole (TMEMA: the
+                            // mu o W set split like the main one)
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
                                 const int h = 3 * (int)rank + c, q = h >> 1;
                                 tma_load_2d(smem + L::b(s) + c * hw * 128, mb, kb * kKBlock,
                                             q * kp + ct * kc + (h & 1) * hw, &full_t[s]);
                             }
+                            if constexpr (TMEMA != 0) {
 #pragma unroll
-                            for (int c = 0; c < 2; ++c)
-                                tma_load_2d(smem + L::b(s) + (3 + c) * hw * 128, mb, kb * kKBlock,
-                                            (3 + (int)rank) * kp + ct * kc + c * hw, &full_t[s]);
+                                for (int c = 0; c < 3; ++c) {
+                                    const int h = 3 * (int)rank + c, q = h >> 1;
+                                    tma_load_2d(smem + L::b(s) + (3 + c) * hw * 128, mb, kb * kKBlock,
+                                                (3 + q) * kp + ct * kc + (h & 1) * hw, &full_t[s]);
+                                }
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 2; ++c)
+                                    tma_load_2d(smem + L::b(s) + (3 + c) * hw * 128, mb, kb * kKBlock,
+                                                (3 + (int)rank) * kp + ct * kc + c * hw, &full_t[s]);
+                            }
                         }
                     } else {
                         for (int q = 0; q < L::kPieces; ++q)
@@ -408,7 +425,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                             if constexpr (PAIR) {
                                 mma_i8_pair_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
                                 mma_i8_pair_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
-                                                   first);
+                                                   ROWS ? first : 1u);
                             } else {
                                 mma_i8_tmem_a(acc_main, tmem_base + L::ta(d) + ks * 8, db, idesc, first);
                                 mma_i8_tmem_a(acc_miss, tmem_base + L::tam(d) + ks * 8, dbm, idesc_m,
@@ -1058,16 +1075,21 @@ int tmem_a_mode() {
     return mode;
 }
 bool tmem_a_default() { return tmem_a_mode() != 0; }
-// The rows pass on CTA pairs with A in TMEM (column tiles of at most 64) as the default pair
-// plan (CS_B200_TMEM_A_PAIRS=0: A in shared memory).  Measured at N=50k, M=100k per rows pass:
-// k = 96 1.76 vs 2.31 ms, k = 128 1.88 vs 2.33, k = 192 2.77 vs 3.41, k = 266 4.63 vs 4.92.
-bool tmem_a_pairs_default() {
-    static const bool on = [] {
+// The passes on CTA pairs with A in TMEM (column tiles of at most 64; the samples pass over the
+// sample-major copy, six operand sets) as the default pair plans (CS_B200_TMEM_A_PAIRS=0: A in
+// shared memory; =1: the rows pass only).  Measured at N=50k, M=100k, rows / samples per pass
+// against A in shared memory: k = 96 1.75 / 1.93 vs 2.31 / 2.48 ms, k = 128 1.89 / 2.12 vs
+// 2.33 / 2.52, k = 192 2.81 / 3.15 vs 3.41 / 3.70, k = 266 4.62 / 5.28 vs 4.92 / 5.47.
+int tmem_a_pairs_mode() {
+    static const int mode = [] {
         const char* v = std::getenv("CS_B200_TMEM_A_PAIRS");
-        return !(v && std::strcmp(v, "0") == 0);
+        if (v && std::strcmp(v, "0") == 0) return 0;
+        if (v && std::strcmp(v, "1") == 0) return 1;
+        return 2;
     }();
-    return on;
+    return mode;
 }
+bool tmem_a_pairs_default() { return tmem_a_pairs_mode() != 0; }
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
 bool narrow_layouts() {
     static const bool on = [] {
@@ -1152,6 +1174,7 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<true, false, true, 2>();
         if (err == cudaSuccess) err = allow_smem<false, false, true, 2>();
         if (err == cudaSuccess) err = allow_smem<true, true, false, 3>();
+        if (err == cudaSuccess) err = allow_smem<false, true, false, 4>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -1334,6 +1357,7 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
         p.tmem_a = 2;
     }
     if (rows && p.pairs && tmem_a_default() && tmem_a_pairs_default()) p.tmem_a = 3;
+    if (!rows && p.pairs && tmem_a_default() && tmem_a_pairs_mode() == 2) p.tmem_a = 4;
     p.max_w = p.tmem_a >= 2 ? kTmemA64W
               : p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
@@ -1401,11 +1425,11 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
                 p.splits = def.splits;
                 cands.push_back(p);
             }
-    if (rows && mode != 0 && tiles % 2 == 0 && num_sms() >= 2 && tmem_a_default())
+    if (mode != 0 && tiles % 2 == 0 && num_sms() >= 2 && tmem_a_default())
         for (int w = 48; w <= kTmemA64W; w += 16) {
             PassPlan p;
             p.pairs = true;
-            p.tmem_a = 3;
+            p.tmem_a = rows ? 3 : 4;
             p.max_w = w;
             p.splits = def.splits;
             cands.push_back(p);
@@ -1590,7 +1614,7 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "samples pass: K slice exceeds the exact int32 range");
     const int nrb = (int)((r_pad + 2047) / 2048);
     // A in TMEM: the six-set form over the sample-major copy
-    const bool tmem_a = plan.narrow && plan.tmem_a != 0;
+    const bool tmem_a = plan.tmem_a != 0;  // narrow single-CTA forms, or 4 on CTA pairs
     const int pieces = tmem_a ? 6 : 5;
     if (tmem_a) ensure_transposed(r, s);
     ws.b2.resize(pieces * kp * r_pad);
@@ -1643,7 +1667,9 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        if (pairs)
+        if (pairs && tmem_a)
+            launch_pass<false, true, false, 4>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
+        else if (pairs)
             launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
         else if (tmem_a && plan.tmem_a == 2)
             launch_pass<false, false, true, 2>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
@@ -1799,7 +1825,7 @@ std::string autotune_json() {
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
                       e.plan.narrow ? "true" : "false",
-                      e.plan.tmem_a == 3 ? "\"pair64\"" : e.plan.tmem_a == 2 ? "64" : e.plan.tmem_a ? "32" : "false",
+                      e.plan.tmem_a >= 3 ? "\"pair64\"" : e.plan.tmem_a == 2 ? "64" : e.plan.tmem_a ? "32" : "false",
                       e.plan.max_w,
                       e.plan.splits, e.candidates,
                       e.ms_best, e.ms_default);
