@@ -980,15 +980,22 @@ def main():
                      "ms_per_launch": per_launch_ms,
                      "share_of_step": top["ms"] / ms})
         if "_tc" in top["name"]:
-            # the int8 datapath: 5 MMA columns per useful multiply-add (3 right-hand-side pieces
-            # against the imputed-code tile, 2 against the missing-indicator tile) on columns
-            # padded to the column tiles (80-wide tiles and a last one rounded up to 16)
+            # the int8 datapath: MMA columns per useful multiply-add on columns padded to the
+            # plan's column tiles (width cap w, a last tile rounded up to 16): 5 (3 right-hand-
+            # side pieces against the imputed-code tile, 2 against the missing-indicator tile),
+            # or 6 in a samples pass with A in tensor memory (W and mu o W, 3 pieces each)
             k_rhs = RANK + OVERSAMPLE
-            tiles = -(-k_rhs // 80)
-            padded = 80 * (tiles - 1) + -(-(k_rhs - 80 * (tiles - 1)) // 16) * 16
-            ops = achieved * 5 * padded / k_rhs
+            plan = next((e for e in (prof.get("autotune") or [])
+                         if e["pass"] == ("rows" if "rows" in top["name"] else "samples")
+                         and abs(e["k"] - k_rhs) < 16), None)
+            w = plan["max_width"] if plan else 80
+            sets = 6 if ("samples" in top["name"] and plan and plan.get("tmem_a")) else 5
+            tiles = -(-k_rhs // w)
+            padded = w * (tiles - 1) + -(-(k_rhs - w * (tiles - 1)) // 16) * 16
+            ops = achieved * sets * padded / k_rhs
             ipeak = int8_peak_tops(torch)
-            roof["int8_datapath"] = {"mma_tops": ops, "peak_tops": ipeak,
+            roof["int8_datapath"] = {"mma_tops": ops, "peak_tops": ipeak, "operand_sets": sets,
+                                     "column_tile": w,
                                      "peak_kind": "cuBLASLt int8 GEMM 8192^3 measured in this run",
                                      "frac": ops / ipeak}
         cpu = None

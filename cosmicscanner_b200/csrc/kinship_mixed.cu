@@ -1326,18 +1326,20 @@ void check_status(MixedWorkspace& ws, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- pass plans and the autotuner
-// A pass runs with a plan: CTA pairs or single CTAs, the column-tile width cap and the number of
-// K slices.  The default plan is the heuristic (pairs above 32 right-hand sides, the narrow
-// single-CTA layout at 32 or fewer; widths 80 / 48 / 80 / 80 for rows-single / samples-single /
-// rows-pair / samples-pair, 32 narrow; slices so that about 8 units per CTA cover the GPU).  The
-// autotuner times the layout x width candidates of a shape once (shapes bucketed: rows and
-// samples by factors of 1.25, columns to multiples of 16) and keeps the fastest.  It never changes the slice count, which is the only plan parameter
-// that changes floating-point results (the order of the slice sums), so a tuned pass returns
+// A pass runs with a plan: CTA pairs or single CTAs, the layout (A in shared memory or in TMEM),
+// the column-tile width cap and the number of K slices.  The default plan is the heuristic: up
+// to 32 right-hand sides the narrow single-CTA layout with A in TMEM, 33 to 64 its 64-wide
+// form, above that CTA pairs with A in TMEM (tiles of at most 64); slices so that about 8
+// units per CTA cover the GPU.  The autotuner times the layout x width candidates of a shape
+// once (shapes bucketed: rows and samples by factors of 1.25, columns to multiples of 16) and
+// keeps the fastest.  It never changes the slice count (the order of the slice sums) nor, in
+// the samples pass, the arithmetic form (five or six operand sets), so a tuned pass returns
 // the same bits as the default one.  CS_B200_AUTOTUNE=0 turns it off.
 struct PassPlan {
     bool pairs = false;
     bool narrow = false;  // single-CTA layout for column tiles of at most 32
-    int tmem_a = 0;       // narrow passes with the A operand in TMEM: 1 (tiles <= 32), 2 (<= 64)
+    int tmem_a = 0;       // A operand in TMEM: 1 / 2 single CTA (tiles <= 32 / 64), 3 / 4 CTA
+                          // pairs (rows / samples, tiles <= 64)
     int max_w = 0;
     int splits = 1;
     bool same_kernel(const PassPlan& o) const {
@@ -1463,6 +1465,15 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
             p.splits = def.splits;
             cands.push_back(p);
         }
+    }
+    // Samples-pass plans with A in TMEM compute the six-set form (W and mu o W), the others the
+    // five-set form: only plans of the default's form are candidates, so a tuned pass returns
+    // the same bits as the default one.
+    if (!rows) {
+        const bool six = def.tmem_a != 0;
+        cands.erase(std::remove_if(cands.begin(), cands.end(),
+                                   [six](const PassPlan& p) { return (p.tmem_a != 0) != six; }),
+                    cands.end());
     }
     cudaEvent_t e0, e1;
     CS_CUDA(cudaEventCreate(&e0));
