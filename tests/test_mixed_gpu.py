@@ -131,11 +131,18 @@ def test_lowrank_scan_reuses_sketch_rows(monkeypatch):
         assert np.abs(a["log10p"][t] - b["log10p"][t]).max() < 1e-4
 
 
-@pytest.mark.parametrize("mode", ["0", "1"])
+@pytest.mark.parametrize("mode", [
+    {"CS_B200_CTA_PAIRS": "0"},                                  # single CTAs, every width
+    {"CS_B200_CTA_PAIRS": "1"},                                  # CTA pairs, every width
+    {"CS_B200_TMEM_A": "0", "CS_B200_TMEM_A_PAIRS": "0"},        # A in shared memory
+    {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "1"},     # pairs: rows in TMEM only
+    {"CS_B200_TMEM_A": "1"},                                     # the 32-wide TMEM form only
+], ids=["single", "pairs", "smem-a", "pairs-rows-tmem", "tmem32"])
 def test_operator_mixed_forced_cta_mode(mode):
-    """CS_B200_CTA_PAIRS=0 (single CTAs for every width) and =1 (CTA pairs for every width)
-    give the same operator as the default width-based choice, within the mixed tolerance;
-    the mode is read once per process, so each runs in a child interpreter."""
+    """Forced plan families (single CTAs or CTA pairs for every width, the A operand in shared
+    memory or in tensor memory, five- or six-set samples passes) give the same operator as the
+    oracle within the mixed tolerance; the switches are read once per process, so each runs in
+    a child interpreter."""
     import json
     import os
     import subprocess
@@ -150,20 +157,20 @@ d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
 g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
 op = cs.createKinshipOperator(g)
 out = {}
-for k in (16, 68):
+for k in (16, 40, 68):
     X = np.random.default_rng(k).standard_normal((d["n"], k))
     out[k] = op.apply(X, precision="mixed").tolist()
 print(json.dumps(out))
 '''
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    env = dict(os.environ, CS_B200_CTA_PAIRS=mode)
+    env = dict(os.environ, **mode)
     res = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True,
                          text=True, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
     forced = json.loads(res.stdout.strip().splitlines()[-1])
     d = synth.cohort(2600, 3000, 17, missing=0.02, n_causal=10)
     ref = oracle.Bed(d["bed"][3:].reshape(d["m"], -1), d["n"])
-    for k in (16, 68):
+    for k in (16, 40, 68):
         X = np.random.default_rng(k).standard_normal((d["n"], k))
         E = ref.apply_block(X, n_threads=8)
         Y = np.array(forced[str(k)])
