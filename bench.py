@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--profile-out", default="")
     ap.add_argument("--apply-only", action="store_true",
                     help="time kinship applies alone (the profiling case), not the REML+scan job")
-    ap.add_argument("--k", type=int, default=68, help="right-hand sides for --apply-only")
+    ap.add_argument("--k", default="68",
+                    help="right-hand sides for --apply-only (a comma-separated list: one line each)")
     ap.add_argument("--serve-requests", type=int, default=32,
                     help="requests in the serving stream measured after the job (0 skips)")
     ap.add_argument("--serve-config5", action="store_true",
@@ -278,28 +279,29 @@ def run_apply_only(args):
     d = synth.cohort(args.n, args.m, 20261203, n_pops=2, fst=0.01, missing=0.02, n_causal=100)
     g = cs.Genotypes.from_bed_bytes(d["bed"], args.n, args.m)
     op = cs.KinshipOperator(g, None, None)
-    X = torch.randn(args.k, args.n, dtype=torch.float64, device="cuda")  # column-major n x k
-    Y = torch.empty_like(X)
     stream = torch.cuda.current_stream().cuda_stream
-    for _ in range(args.warmup):
-        op.apply_device(X.data_ptr(), args.n, args.k, Y.data_ptr(), args.n, args.precision, stream)
-    torch.cuda.synchronize()
-    cs.profile_enable(True)
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s.record()
-    for _ in range(args.steps):
-        op.apply_device(X.data_ptr(), args.n, args.k, Y.data_ptr(), args.n, args.precision, stream)
-    e.record()
-    torch.cuda.synchronize()
-    prof = cs.profile_summary()
-    cs.profile_enable(False)
-    ms = s.elapsed_time(e) / args.steps
-    flops = 4.0 * args.n * args.m * args.k
-    print(json.dumps({"metric": "kinship apply ms", "value": ms, "unit": "ms", "n": args.n,
-                      "m": args.m, "k": args.k, "precision": args.precision,
-                      "tflops": flops / (ms * 1e-3) / 1e12,
-                      "kernels": [(k["name"], k["launches"], k["ms"] / k["launches"])
-                                  for k in prof["kernels"]]}))
+    for kk in [int(v) for v in str(args.k).split(",")]:
+        X = torch.randn(kk, args.n, dtype=torch.float64, device="cuda")  # column-major n x k
+        Y = torch.empty_like(X)
+        for _ in range(args.warmup):
+            op.apply_device(X.data_ptr(), args.n, kk, Y.data_ptr(), args.n, args.precision, stream)
+        torch.cuda.synchronize()
+        cs.profile_enable(True)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(args.steps):
+            op.apply_device(X.data_ptr(), args.n, kk, Y.data_ptr(), args.n, args.precision, stream)
+        e.record()
+        torch.cuda.synchronize()
+        prof = cs.profile_summary()
+        cs.profile_enable(False)
+        ms = s.elapsed_time(e) / args.steps
+        flops = 4.0 * args.n * args.m * kk
+        print(json.dumps({"metric": "kinship apply ms", "value": ms, "unit": "ms", "n": args.n,
+                          "m": args.m, "k": kk, "precision": args.precision,
+                          "tflops": flops / (ms * 1e-3) / 1e12,
+                          "kernels": [(k["name"], k["launches"], k["ms"] / k["launches"])
+                                      for k in prof["kernels"]]}), flush=True)
     return 0
 
 
@@ -983,13 +985,15 @@ def main():
             # the int8 datapath: MMA columns per useful multiply-add on columns padded to the
             # plan's column tiles (width cap w, a last tile rounded up to 16): 5 (3 right-hand-
             # side pieces against the imputed-code tile, 2 against the missing-indicator tile),
-            # or 6 in a samples pass with A in tensor memory (W and mu o W, 3 pieces each)
+            # or 6 in a samples pass over the sample-major copy with the fixed dosage table (W and
+            # mu o W, 3 pieces each)
             k_rhs = RANK + OVERSAMPLE
             plan = next((e for e in (prof.get("autotune") or [])
                          if e["pass"] == ("rows" if "rows" in top["name"] else "samples")
                          and abs(e["k"] - k_rhs) < 16), None)
             w = plan["max_width"] if plan else 80
-            sets = 6 if ("samples" in top["name"] and plan and plan.get("tmem_a")) else 5
+            sets = 6 if ("samples" in top["name"] and plan
+                         and plan.get("tmem_a") in (32, 64, "pair64")) else 5
             tiles = -(-k_rhs // w)
             padded = w * (tiles - 1) + -(-(k_rhs - w * (tiles - 1)) // 16) * 16
             ops = achieved * sets * padded / k_rhs

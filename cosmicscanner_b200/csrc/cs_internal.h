@@ -170,9 +170,11 @@ struct cs_kinship {
     cs::DeviceBuffer<double> buf_x, buf_u, buf_y;
     cs::MixedOperator* mixed = nullptr;
     bool autotune = true;  // the tensor-core passes may tune their plan on new shapes
-    // every mixed samples pass uses the five-set arithmetic (no six-set TMEM form), so a column's
-    // result does not depend on how many columns share its apply (the serving loop's stacking)
-    bool width_independent = false;
+    // the samples pass may keep a sample-major copy of the packed view (one more packed matrix
+    // in HBM) and read its A operand from tensor memory (six operand sets at the widths where
+    // that is the default); otherwise A stays in shared memory and every samples pass runs the
+    // five-set form, so a column's result does not depend on how many columns share its apply
+    bool sample_major_copy = true;
     ~cs_kinship() { cs::destroy_mixed(mixed); }
 };
 

@@ -36,10 +36,12 @@
 // resident) into a ring of stages; warps 2-9 decode; warp 1 issues the MMAs from one thread
 // into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.
 // The decoded tile (SNP rows x samples) serves as a K-major A operand in the rows pass and
-// as an MN-major A operand in the samples pass.  Blocks of up to 64 columns (TMEMA layouts)
-// decode into tensor memory instead (tcgen05.st) and the MMAs read A from there; the samples
-// pass then reads a sample-major copy of the packed matrix, where A is K-major too, with the
-// fixed dosage table and W / mu o W in six operand sets.  Wide blocks run on CTA pairs
+// as an MN-major A operand in the samples pass.  The TMEMA layouts decode into tensor memory
+// instead (tcgen05.st) and the MMAs read A from there; the samples pass then reads a
+// sample-major copy of the packed matrix, where A is K-major too, either with the fixed
+// dosage table and W / mu o W in six operand sets, or (TMEMA = 5) with each SNP's imputed
+// code put in along K under a per-byte missing-call mask (the five sets, and the int32 sums,
+// of the shared-memory form).  Wide blocks run on CTA pairs
 // (cta_group::2): the partner CTA's MMA warp forwards each of its landed B stages to the
 // leader.  Every wait is bounded; a timeout leaves a status code that the host reports as an
 // error.
@@ -111,9 +113,10 @@ constexpr int kNarrowSamplesW = 32, kNarrowSamplesST = 3, kNarrowSamplesSP = 8, 
 // genotype tiles into TMEM (tcgen05.st) and the MMAs read them there, so shared memory
 // carries only the packed tiles and the B pieces.  A TMEM operand must be K-major, so the
 // samples pass then reads a sample-major copy of the packed matrix (rows = samples, four
-// SNPs per byte) and decodes it like the rows pass, with the fixed dosage table (the per-SNP
-// imputed codes cannot share one byte-permute table along K): its B carries W and mu o W,
-// three pieces each, the six-set form.  TMEMA = 1: column tiles of at most 32, two
+// SNPs per byte).  Along its K the SNPs change every two bits, so one byte-permute table
+// cannot carry the per-SNP imputed codes: these passes decode with the fixed dosage table and
+// carry the missing calls with W and mu o W, three pieces each (the six-set form), except
+// TMEMA = 5 below.  TMEMA = 1: column tiles of at most 32, two
 // accumulators (5 x 32 columns rows, 3 x 32 samples); TMEMA = 2: tiles of at most 64, one
 // accumulator (5 x 64 / 3 x 64), for 33 to 64 right-hand sides.  Then A stages of 64 TMEM
 // columns (32 per tile: 128 int8 K elements per lane).
@@ -126,7 +129,11 @@ constexpr int kTmemA64SamplesST = 3, kTmemA64SamplesSP = 12, kTmemA64SamplesSD =
 // holds half of the B pieces, as in the shared-memory pair form).
 constexpr int kTmemAPairRowsST = 8, kTmemAPairRowsSP = 16, kTmemAPairRowsSD = 3;
 // TMEMA = 4: the samples pass on CTA pairs over the sample-major copy (six operand sets, each
-// CTA holding half of each set).
+// CTA holding half of each set).  TMEMA = 5: the same in the five-set form: the decoder
+// permutes with the observed-call table (missing -> 0) and a missing-call mask table and ORs
+// in q_t from a per-SNP byte array in the decoded K order (a third operation per four codes,
+// and the K-block's 128 codes staged with each packed tile); B as in the shared-memory pair
+// form.
 constexpr int kTmemAPairSamplesST = 4, kTmemAPairSamplesSP = 16, kTmemAPairSamplesSD = 4;
 constexpr uint32_t kTmemAStage = 64;
 
@@ -134,25 +141,27 @@ template <bool ROWS, bool PAIR, bool NARROW = false, int TMEMA = 0>
 struct Layout {
     static_assert(!(PAIR && NARROW), "narrow layouts are single-CTA");
     static_assert(!TMEMA || (TMEMA == 3 ? (ROWS && PAIR && !NARROW)
-                             : TMEMA == 4 ? (!ROWS && PAIR && !NARROW) : (NARROW && !PAIR)),
+                             : TMEMA >= 4 ? (!ROWS && PAIR && !NARROW) : (NARROW && !PAIR)),
                   "A in TMEM: the narrow single-CTA passes, or the passes on CTA pairs");
-    static constexpr int kPieces = ROWS ? 3 : (TMEMA ? 6 : 5);  // per column tile, over the pair
+    // samples passes over the sample-major copy with the fixed dosage table: W and mu o W
+    static constexpr bool kSixSets = !ROWS && (TMEMA == 1 || TMEMA == 2 || TMEMA == 4);
+    static constexpr int kPieces = ROWS ? 3 : (kSixSets ? 6 : 5);  // per column tile, over the pair
     static constexpr int kMaxW = TMEMA >= 2 ? kTmemA64W
                                  : NARROW ? (ROWS ? kNarrowRowsW : kNarrowSamplesW)
                                  : PAIR ? (ROWS ? kPairRowsW : kPairSamplesW) : (ROWS ? kRowsW : kSamplesW);
-    static constexpr int kTmaStages = TMEMA == 4 ? kTmemAPairSamplesST
+    static constexpr int kTmaStages = TMEMA >= 4 ? kTmemAPairSamplesST
                                       : TMEMA == 3 ? kTmemAPairRowsST
                                       : TMEMA == 2 ? (ROWS ? kTmemA64RowsST : kTmemA64SamplesST)
                                       : TMEMA ? (ROWS ? kTmemARowsST : kTmemASamplesST)
                                       : NARROW ? (ROWS ? kNarrowRowsST : kNarrowSamplesST)
                                       : PAIR ? (ROWS ? kPairRowsST : kPairSamplesST) : (ROWS ? kRowsST : kSamplesST);
-    static constexpr int kPackedStages = TMEMA == 4 ? kTmemAPairSamplesSP
+    static constexpr int kPackedStages = TMEMA >= 4 ? kTmemAPairSamplesSP
                                          : TMEMA == 3 ? kTmemAPairRowsSP
                                          : TMEMA == 2 ? (ROWS ? kTmemA64RowsSP : kTmemA64SamplesSP)
                                          : TMEMA ? (ROWS ? kTmemARowsSP : kTmemASamplesSP)
                                          : NARROW ? (ROWS ? kNarrowRowsSP : kNarrowSamplesSP)
                                          : PAIR ? (ROWS ? kPairRowsSP : kPairSamplesSP) : (ROWS ? kRowsSP : kSamplesSP);
-    static constexpr int kDecodeStages = TMEMA == 4 ? kTmemAPairSamplesSD
+    static constexpr int kDecodeStages = TMEMA >= 4 ? kTmemAPairSamplesSD
                                          : TMEMA == 3 ? kTmemAPairRowsSD
                                          : TMEMA == 2 ? (ROWS ? kTmemA64RowsSD : kTmemA64SamplesSD)
                                          : TMEMA ? (ROWS ? kTmemARowsSD : kTmemASamplesSD)
@@ -169,20 +178,26 @@ struct Layout {
     static constexpr int kTmaBytes = kBBytes;
     static constexpr int kDecBytes = 2 * kATileBytes;
     static constexpr int kDecodeRegion = TMEMA ? 0 : kDecodeStages * kDecBytes;
+    // samples pass over the sample-major copy: the K-block's 128 imputed codes (P.qperm) ride
+    // in each packed stage, so the decoders read them from shared memory
+    static constexpr int kQBytes = TMEMA == 5 ? kKBlock : 0;
     // barriers: full / empty per B, packed and decode stage, full / empty per accumulator,
     // `drained`, then the TMEM slot
     static constexpr int kBarBytes =
         (2 * (kTmaStages + kPackedStages + kDecodeStages + kAccBufs) + 1) * 8 + 8;
     static constexpr int kSmem = kDecodeRegion + kTmaStages * kTmaBytes +
-                                 kPackedStages * kPackedBytes + 1024 + kBarBytes;
+                                 kPackedStages * (kPackedBytes + kQBytes) + 1024 + kBarBytes;
     static __host__ __device__ constexpr int a(int d) { return d * kDecBytes; }
     static __host__ __device__ constexpr int am(int d) { return d * kDecBytes + kATileBytes; }
     static __host__ __device__ constexpr int b(int s) { return kDecodeRegion + s * kTmaBytes; }
     static __host__ __device__ constexpr int p(int s) {
         return kDecodeRegion + kTmaStages * kTmaBytes + s * kPackedBytes;
     }
+    static __host__ __device__ constexpr int q(int s) {
+        return kDecodeRegion + kTmaStages * kTmaBytes + kPackedStages * kPackedBytes + s * kQBytes;
+    }
     static __host__ __device__ constexpr int bars() {
-        return kDecodeRegion + kTmaStages * kTmaBytes + kPackedStages * kPackedBytes;
+        return kDecodeRegion + kTmaStages * kTmaBytes + kPackedStages * (kPackedBytes + kQBytes);
     }
     static_assert(kSmem <= 227 * 1024, "mixed pass exceeds shared memory");
     static_assert(kTmaBytes % 1024 == 0, "TMA stages must keep 1024-byte alignment");
@@ -198,11 +213,15 @@ struct PassArgs {
     int kc, kp;                  // column tile width, padded column count
     int kc_last;                 // width of the last column tile (a multiple of 16, <= kc)
     const uint32_t* lut;         // per SNP row: imputed code of each 2-bit code (byte-permute table)
+    const uint4* qperm;          // samples pass over the sample-major copy: q_t of each SNP at
+                                 // its position in the decoded K order, 16 SNPs per uint4
     const double* resid;         // rows pass: r_t = mu_t - q_t / Q per SNP row (epilogue)
     const double* inv_f;         // samples pass: 1 / (Q f) per column
     double* part;                // [n_splits][kp][ld] FP64 slice partials
     int64_t ld;                  // padded output rows
     int* status;
+    uint32_t poll_ns;            // pairs: pause between polls of the long, off-critical-path waits
+    uint32_t poll_dec_ns;        // pairs: pause between the decoders' polls for a free stage
 };
 
 // 16 codes (one 32-bit word, code j in bits 2j..2j+1) -> 16 int8 imputed codes (byte c of
@@ -220,6 +239,23 @@ __device__ __forceinline__ void decode_word_interleaved(uint32_t w, uint32_t lut
     mis.y = __byte_perm(0x00000100u, 0u, se >> 16);
     mis.z = __byte_perm(0x00000100u, 0u, so);
     mis.w = __byte_perm(0x00000100u, 0u, so >> 16);
+}
+// The same for 16 codes of 16 different SNPs (a word of the sample-major copy): the observed
+// calls through the fixed table 2Q / 0 / Q / 0, a 0xFF byte per missing call, and the SNPs'
+// imputed codes q (four per word, in the interleaved order) put in under that mask.  The mask
+// itself is the missing-indicator tile, as int8 -1: the samples operand of this form carries
+// the residual pieces negated, so the products are those of the +1 tile.
+constexpr uint32_t kObservedCodes = (uint32_t)(2 * kImputeQ) | ((uint32_t)kImputeQ << 16);
+__device__ __forceinline__ void decode_word_imputed(uint32_t w, const uint4& q, uint4& dos, uint4& mis) {
+    const uint32_t se = w & 0x33333333u, so = (w >> 2) & 0x33333333u;
+    mis.x = __byte_perm(0x0000FF00u, 0u, se);
+    mis.y = __byte_perm(0x0000FF00u, 0u, se >> 16);
+    mis.z = __byte_perm(0x0000FF00u, 0u, so);
+    mis.w = __byte_perm(0x0000FF00u, 0u, so >> 16);
+    dos.x = __byte_perm(kObservedCodes, 0u, se) | (mis.x & q.x);
+    dos.y = __byte_perm(kObservedCodes, 0u, se >> 16) | (mis.y & q.y);
+    dos.z = __byte_perm(kObservedCodes, 0u, so) | (mis.z & q.z);
+    dos.w = __byte_perm(kObservedCodes, 0u, so >> 16) | (mis.w & q.w);
 }
 // position p (0..15) of the interleaved order -> sample offset in the group, and back
 __host__ __device__ __forceinline__ int sample_at(int p) { return p < 8 ? 2 * p : 2 * (p - 8) + 1; }
@@ -317,6 +353,12 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         return PAIR ? mbar_poll_cluster(bar, parity, P.status, code)
                     : mbar_wait(bar, parity, P.status, code);
     };
+    // commit barriers that a warp waits on long and off the critical path (the epilogue's
+    // accumulator, the B producer's free stage, the partner CTA's forwarding)
+    auto wait_idle = [&](uint64_t* bar, uint32_t parity, int code) {
+        return PAIR ? mbar_poll_sleep(bar, parity, P.status, code, P.poll_ns)
+                    : mbar_wait(bar, parity, P.status, code);
+    };
 
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer (B)
@@ -334,7 +376,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 const uint32_t bytes = (uint32_t)(L::kPieces * w * 128 / (PAIR ? 2 : 1));
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST;
-                    if (!(ok = wait_commit(&empty_t[s], ((j / ST) & 1) ^ 1, kTimeoutTma))) break;
+                    if (!(ok = wait_idle(&empty_t[s], ((j / ST) & 1) ^ 1, kTimeoutTma))) break;
                     mbar_arrive_expect_tx(&full_t[s], bytes);
                     if (PAIR) {
                         const int hw = w / 2;  // rows of one half-piece
@@ -347,7 +389,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                                             c * kp + ct * kc + (int)rank * hw, &full_t[s]);
                         } else {
                             // main set: half-pieces [p0a p0b p1a p1b p2a p2b], this CTA loads
-                            // 3 r .. 3 r + 2; residual set: piece 3 + r whole (TMEMA: the
+                            // 3 r .. 3 r + 2; residual set: piece 3 + r whole (six sets: the
                             // mu o W set split like the main one)
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
@@ -355,7 +397,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                                 tma_load_2d(smem + L::b(s) + c * hw * 128, mb, kb * kKBlock,
                                             q * kp + ct * kc + (h & 1) * hw, &full_t[s]);
                             }
-                            if constexpr (TMEMA != 0) {
+                            if constexpr (L::kSixSets) {
 #pragma unroll
                                 for (int c = 0; c < 3; ++c) {
                                     const int h = 3 * (int)rank + c, q = h >> 1;
@@ -397,8 +439,8 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 const int w = width(ct);
                 const uint32_t idesc = idesc0 | ((uint32_t)((3 * w) >> 3) << 17);
-                // the missing-indicator MMA: two pieces, or the three of mu o W (samples, TMEMA)
-                const uint32_t idesc_m = idesc0 | ((uint32_t)(((!ROWS && TMEMA ? 3 : 2) * w) >> 3) << 17);
+                // the missing-indicator MMA: two pieces, or the three of mu o W (six sets)
+                const uint32_t idesc_m = idesc0 | ((uint32_t)(((L::kSixSets ? 3 : 2) * w) >> 3) << 17);
                 const int buf = ui % NB;
                 if (!(ok = wait_peer(&acc_empty[buf], ((ui / NB) & 1) ^ 1, kTimeoutMma))) break;
                 tc_fence_after();
@@ -479,7 +521,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 unit_coords(u, tile, ct, split, kb0, kb1);
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int s = j % ST, d = j % SD;
-                    if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
+                    if (!(ok = wait_idle(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
                     if (!(ok = mbar_wait(&full_t[s], (j / ST) & 1, P.status, kTimeoutDecode))) break;
                     mbar_arrive_remote(mapa_shared(&full_d[d], 0));
                 }
@@ -499,23 +541,38 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
             // the row's imputed-code table: rows pass SNP tile * 128 + r, samples pass
-            // kb * 128 + r (the packed tile's row)
-            // (samples pass over the sample-major copy: the fixed dosage table 2 / 0 / 1 / 0)
+            // kb * 128 + r (the packed tile's row); over the sample-major copy the fixed dosage
+            // table 2 / 0 / 1 / 0 (six sets) or the K-block's imputed codes staged with the
+            // packed tile (TMEMA = 5)
             uint32_t lut = ROWS ? __ldg(P.lut + (int64_t)tile * kTile + r) : 0x00010002u;
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
                 const int sp = j % SP, d = j % SD;
                 if (!KMAJOR) lut = __ldg(P.lut + (int64_t)kb * kKBlock + r);
-                if (!(ok = wait_commit(&empty_d[d], ((j / SD) & 1) ^ 1, kTimeoutDecode))) break;
+                if (!(ok = PAIR ? mbar_poll_sleep(&empty_d[d], ((j / SD) & 1) ^ 1, P.status,
+                                                  kTimeoutDecode, P.poll_dec_ns)
+                                : mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode)))
+                    break;
                 if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
                 const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
                 const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
+                // imputed codes of the 64 SNPs this thread decodes (the same for every lane of
+                // the warp: shared-memory broadcasts)
+                uint4 qv[4];
+                if constexpr (TMEMA == 5) {
+#pragma unroll
+                    for (int cj = 0; cj < 4; ++cj)
+                        qv[cj] = *reinterpret_cast<const uint4*>(smem + L::q(sp) + h * 64 + cj * 16);
+                }
                 if constexpr (TMEMA) {
                     // 64 K elements of this lane = 16 TMEM columns of each tile
                     uint32_t ev[16], mv[16];
 #pragma unroll
                     for (int cj = 0; cj < 4; ++cj) {
                         uint4 dos, mis;
-                        decode_word_interleaved(words[cj], lut, dos, mis);
+                        if constexpr (TMEMA == 5)
+                            decode_word_imputed(words[cj], qv[cj], dos, mis);
+                        else
+                            decode_word_interleaved(words[cj], lut, dos, mis);
                         ev[4 * cj] = dos.x; ev[4 * cj + 1] = dos.y; ev[4 * cj + 2] = dos.z; ev[4 * cj + 3] = dos.w;
                         mv[4 * cj] = mis.x; mv[4 * cj + 1] = mis.y; mv[4 * cj + 2] = mis.z; mv[4 * cj + 3] = mis.w;
                     }
@@ -561,12 +618,16 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                 for (int kb = kb0; kb < kb1; ++kb, ++j) {
                     const int sp = j % SP;
                     if (!(ok = mbar_wait(&empty_p[sp], ((j / SP) & 1) ^ 1, P.status, kTimeoutTma))) break;
-                    mbar_arrive_expect_tx(&full_p[sp], (uint32_t)kPackedBytes);
+                    mbar_arrive_expect_tx(&full_p[sp], (uint32_t)(kPackedBytes + L::kQBytes));
                     // packed tile: 128 rows x 32 bytes (128 K elements)
                     if (KMAJOR)
                         tma_load_2d(smem + L::p(sp), &tm_a, kb * 32, tile * kTile, &full_p[sp]);
                     else
                         tma_load_2d(smem + L::p(sp), &tm_a, tile * 32, kb * kKBlock, &full_p[sp]);
+                    if constexpr (L::kQBytes != 0)
+                        bulk_load_1d(smem + L::q(sp), reinterpret_cast<const unsigned char*>(P.qperm) +
+                                                          (int64_t)kb * kKBlock,
+                                     (uint32_t)L::kQBytes, &full_p[sp]);
                 }
             }
             // leave no copy in flight
@@ -583,7 +644,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             int tile, ct, split, kb0, kb1;
             unit_coords(u, tile, ct, split, kb0, kb1);
             const int buf = ui % NB;
-            if (!(ok = wait_commit(&acc_full[buf], (ui / NB) & 1, kTimeoutEpilogue))) break;
+            if (!(ok = wait_idle(&acc_full[buf], (ui / NB) & 1, kTimeoutEpilogue))) break;
             tc_fence_after();
             // rows pass: TMEM lane = SNP row; samples pass: lane = position in the decoded
             // tile, whose samples are interleaved within each group of 16
@@ -862,13 +923,17 @@ k_reduce_rows(const double* __restrict__ part, int splits, int64_t kp, int64_t l
 // and two of (Q r o W) f (rows (3 + q) kp + c), t < r_pad, with ONE factor f = 127 / max|W|
 // per column so that both MMAs accumulate into the same TMEM columns (|Q r_t| <= 1/2); 1/(Q f)
 // per column; and per-block sums of mu_t W[t][c] (the centring term) in cpart[blockIdx.x][c].
+// `interleave` (A in TMEM, over the sample-major copy): SNP t sits at K position
+// (t & ~15) + position_of(t & 15), the order in which the decoder writes each group of 16, and
+// the residual pieces are negated (that decoder's missing-indicator tile holds -1).
 // Grid: (r_pad / 2048, kp).
 __global__ void __launch_bounds__(256)
 k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int64_t kp,
                         int64_t r_pad, const double* __restrict__ mu,
                         const double* __restrict__ resid,
-                        const unsigned long long* __restrict__ max_w, int8_t* __restrict__ B,
-                        double* __restrict__ inv_f, double* __restrict__ cpart) {
+                        const unsigned long long* __restrict__ max_w, int interleave,
+                        int8_t* __restrict__ B, double* __restrict__ inv_f,
+                        double* __restrict__ cpart) {
     __shared__ double red[8];
     const int64_t c = blockIdx.y;
     const double f = c < k ? quant_factor(max_w[c]) : 0.0;
@@ -880,14 +945,15 @@ k_split_samples_operand(const double* __restrict__ Wt, int64_t R, int64_t k, int
         if (c < k && t < R) {
             const double w = Wt[c * R + t];
             quantise3(w * f, a1, a2, a3);
-            quantise2(kImputeQ * resid[t] * w * f, b1, b2);
+            quantise2((interleave ? -kImputeQ : kImputeQ) * resid[t] * w * f, b1, b2);
             cs += mu[t] * w;
         }
-        B[c * r_pad + t] = a1;
-        B[(kp + c) * r_pad + t] = a2;
-        B[(2 * kp + c) * r_pad + t] = a3;
-        B[(3 * kp + c) * r_pad + t] = b1;
-        B[(4 * kp + c) * r_pad + t] = b2;
+        const int64_t pos = interleave ? (t & ~(int64_t)15) + position_of((int)(t & 15)) : t;
+        B[c * r_pad + pos] = a1;
+        B[(kp + c) * r_pad + pos] = a2;
+        B[(2 * kp + c) * r_pad + pos] = a3;
+        B[(3 * kp + c) * r_pad + pos] = b1;
+        B[(4 * kp + c) * r_pad + pos] = b2;
     }
     for (int off = 16; off; off >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, off);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cs;
@@ -1077,17 +1143,40 @@ int tmem_a_mode() {
 bool tmem_a_default() { return tmem_a_mode() != 0; }
 // The passes on CTA pairs with A in TMEM (column tiles of at most 64; the samples pass over the
 // sample-major copy, six operand sets) as the default pair plans (CS_B200_TMEM_A_PAIRS=0: A in
-// shared memory; =1: the rows pass only).  Measured at N=50k, M=100k, rows / samples per pass
-// against A in shared memory: k = 96 1.75 / 1.93 vs 2.31 / 2.48 ms, k = 128 1.89 / 2.12 vs
-// 2.33 / 2.52, k = 192 2.81 / 3.15 vs 3.41 / 3.70, k = 266 4.62 / 5.28 vs 4.92 / 5.47.
+// shared memory; =1: the rows pass only; =3: the samples pass in the five-set form, TMEMA = 5).
+// Measured at N=50k, M=100k, rows / samples per pass against A in shared memory: k = 96
+// 1.75 / 1.93 vs 2.31 / 2.48 ms, k = 128 1.89 / 2.12 vs 2.33 / 2.52, k = 192 2.81 / 3.15 vs
+// 3.41 / 3.70, k = 266 4.62 / 5.28 vs 4.92 / 5.47.
 int tmem_a_pairs_mode() {
     static const int mode = [] {
         const char* v = std::getenv("CS_B200_TMEM_A_PAIRS");
         if (v && std::strcmp(v, "0") == 0) return 0;
         if (v && std::strcmp(v, "1") == 0) return 1;
+        if (v && std::strcmp(v, "3") == 0) return 3;
         return 2;
     }();
     return mode;
+}
+// Pauses between polls in the pair kernels, in nanoseconds: the long waits (the epilogue's
+// accumulator, the B producer's free stage, the partner CTA's forwarding;
+// CS_B200_POLL_SLEEP_NS, default 128) and the decoders' waits for a free stage
+// (CS_B200_POLL_SLEEP_DEC_NS, default 32).  A warp that polls without pause takes issue slots
+// from the decoders and the MMA thread on its scheduler.  Measured per pass (rows / samples)
+// at N=50k, M=100k, k=266 against no pauses: 4.46 / 5.24 vs 4.76-4.91 / 5.48-5.63 ms; k=96
+// 1.67 / 1.88 vs 1.82 / 2.02; 512 ns pauses are slower than none.
+uint32_t env_ns(const char* name, uint32_t def) {
+    const char* v = std::getenv(name);
+    if (!v || !*v) return def;
+    const long x = std::strtol(v, nullptr, 10);
+    return (uint32_t)std::max(0L, std::min(x, 100000L));
+}
+uint32_t poll_sleep_ns() {
+    static const uint32_t ns = env_ns("CS_B200_POLL_SLEEP_NS", 128u);
+    return ns;
+}
+uint32_t poll_dec_sleep_ns() {
+    static const uint32_t ns = env_ns("CS_B200_POLL_SLEEP_DEC_NS", 32u);
+    return ns;
 }
 bool tmem_a_pairs_default() { return tmem_a_pairs_mode() != 0; }
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
@@ -1123,6 +1212,9 @@ struct MixedRows {
     int64_t R = 0, n = 0, r_pad = 0, n_pad = 0;
     DeviceBuffer<double> mu, exc, s, resid;
     DeviceBuffer<uint32_t> lut;  // imputed code of each 2-bit code, one byte per code
+    // q_t (byte 1 of lut[t]) at K position (t & ~15) + position_of(t & 15): the samples pass
+    // over the sample-major copy reads the imputed codes of 16 SNPs per uint4
+    DeviceBuffer<uint4> qperm;
     CUtensorMap tm{};
     const uint8_t* rows = nullptr;  // the view's packed rows (owned by the operator)
     int64_t stride = 0;
@@ -1175,6 +1267,7 @@ void configure_kernels() {
         if (err == cudaSuccess) err = allow_smem<false, false, true, 2>();
         if (err == cudaSuccess) err = allow_smem<true, true, false, 3>();
         if (err == cudaSuccess) err = allow_smem<false, true, false, 4>();
+        if (err == cudaSuccess) err = allow_smem<false, true, false, 5>();
         return err;
     }, "configure tensor-core kernels");
 }
@@ -1248,12 +1341,14 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     r.n_pad = round_up(std::max<int64_t>(r.n, 1), 2 * kTile);
     std::vector<double> mu(r.r_pad, 0.0), ex(r.r_pad, 0.0), sv(r.r_pad, 0.0), rs(r.r_pad, 0.0);
     std::vector<uint32_t> lut(r.r_pad, 0u);
+    std::vector<uint8_t> qp(r.r_pad, 0u);
     for (int64_t t = 0; t < r.R; ++t) {
         const double mt = mean[t];
         mu[t] = mt;
         const double qd = std::isfinite(mt) ? std::rint(kImputeQ * mt) : 0.0;
         const uint32_t q = (uint32_t)std::min(std::max(qd, 0.0), 2.0 * kImputeQ);
         lut[t] = (uint32_t)(2 * kImputeQ) | (q << 8) | ((uint32_t)kImputeQ << 16);
+        qp[(t & ~(int64_t)15) + position_of((int)(t & 15))] = (uint8_t)q;
         rs[t] = std::isfinite(mt) ? mt - (double)q / kImputeQ : 0.0;
         const int64_t c00 = counts[4 * t], c10 = counts[4 * t + 2], c11 = counts[4 * t + 3];
         ex[t] = (double)(2 * c00 + c10) - mt * (double)(c00 + c10 + c11);
@@ -1264,8 +1359,10 @@ void init_rows(MixedRows& r, const cs_packed_view& v, const double* mean, const 
     r.s.resize(r.r_pad);
     r.resid.resize(r.r_pad);
     r.lut.resize(r.r_pad);
+    r.qperm.resize(r.r_pad / 16);
     CS_CUDA(cudaMemcpy(r.resid.get(), rs.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.lut.get(), lut.data(), 4 * r.r_pad, cudaMemcpyHostToDevice));
+    CS_CUDA(cudaMemcpy(r.qperm.get(), qp.data(), r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.mu.get(), mu.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.exc.get(), ex.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
     CS_CUDA(cudaMemcpy(r.s.get(), sv.data(), 8 * r.r_pad, cudaMemcpyHostToDevice));
@@ -1339,13 +1436,17 @@ struct PassPlan {
     bool pairs = false;
     bool narrow = false;  // single-CTA layout for column tiles of at most 32
     int tmem_a = 0;       // A operand in TMEM: 1 / 2 single CTA (tiles <= 32 / 64), 3 / 4 CTA
-                          // pairs (rows / samples, tiles <= 64)
+                          // pairs (rows / samples, tiles <= 64), 5 the five-set samples pairs
     int max_w = 0;
     int splits = 1;
     bool same_kernel(const PassPlan& o) const {
         return pairs == o.pairs && narrow == o.narrow && tmem_a == o.tmem_a && max_w == o.max_w;
     }
 };
+
+// the samples-pass form of a plan: six operand sets over the sample-major copy with the fixed
+// dosage table (TMEMA 1, 2, 4), five otherwise
+bool six_set_samples(const PassPlan& p) { return p.tmem_a == 1 || p.tmem_a == 2 || p.tmem_a == 4; }
 
 PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
     PassPlan p;
@@ -1359,7 +1460,8 @@ PassPlan default_plan(bool rows, int64_t tiles, int kb, int64_t k) {
         p.tmem_a = 2;
     }
     if (rows && p.pairs && tmem_a_default() && tmem_a_pairs_default()) p.tmem_a = 3;
-    if (!rows && p.pairs && tmem_a_default() && tmem_a_pairs_mode() == 2) p.tmem_a = 4;
+    if (!rows && p.pairs && tmem_a_default() && tmem_a_pairs_mode() >= 2)
+        p.tmem_a = tmem_a_pairs_mode() == 3 ? 5 : 4;
     p.max_w = p.tmem_a >= 2 ? kTmemA64W
               : p.narrow ? kNarrowRowsW
                        : rows ? (p.pairs ? kPairRowsW : kRowsW) : (p.pairs ? kPairSamplesW : kSamplesW);
@@ -1431,7 +1533,7 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
         for (int w = 48; w <= kTmemA64W; w += 16) {
             PassPlan p;
             p.pairs = true;
-            p.tmem_a = rows ? 3 : 4;
+            p.tmem_a = rows ? 3 : (def.tmem_a == 5 ? 5 : 4);
             p.max_w = w;
             p.splits = def.splits;
             cands.push_back(p);
@@ -1466,13 +1568,13 @@ PassPlan choose_plan(bool rows, bool allow, int64_t R, int64_t n, int64_t k, int
             cands.push_back(p);
         }
     }
-    // Samples-pass plans with A in TMEM compute the six-set form (W and mu o W), the others the
-    // five-set form: only plans of the default's form are candidates, so a tuned pass returns
-    // the same bits as the default one.
+    // Samples-pass plans over the sample-major copy with the fixed dosage table compute the
+    // six-set form (W and mu o W), the others the five-set form: only plans of the default's
+    // form are candidates, so a tuned pass returns the same bits as the default one.
     if (!rows) {
-        const bool six = def.tmem_a != 0;
+        const bool six = six_set_samples(def);
         cands.erase(std::remove_if(cands.begin(), cands.end(),
-                                   [six](const PassPlan& p) { return (p.tmem_a != 0) != six; }),
+                                   [six](const PassPlan& p) { return six_set_samples(p) != six; }),
                     cands.end());
     }
     cudaEvent_t e0, e1;
@@ -1581,6 +1683,8 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
     P.part = ws.part.get();
     P.ld = r_pad;
     P.status = ws.status.get();
+    P.poll_ns = poll_sleep_ns();
+    P.poll_dec_ns = poll_dec_sleep_ns();
     {
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
@@ -1624,9 +1728,11 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     const int splits = (kb + kbs - 1) / kbs;  // no empty slice
     if (kbs > kMaxKbPerAccum) fail(CS_ERR_UNSUPPORTED, "samples pass: K slice exceeds the exact int32 range");
     const int nrb = (int)((r_pad + 2047) / 2048);
-    // A in TMEM: the six-set form over the sample-major copy
-    const bool tmem_a = plan.tmem_a != 0;  // narrow single-CTA forms, or 4 on CTA pairs
-    const int pieces = tmem_a ? 6 : 5;
+    // A in TMEM: over the sample-major copy, B in the decoded K order; six sets with the fixed
+    // dosage table, five with the imputed codes (TMEMA = 5)
+    const bool tmem_a = plan.tmem_a != 0;  // narrow single-CTA forms, or 4 / 5 on CTA pairs
+    const bool six = six_set_samples(plan);
+    const int pieces = six ? 6 : 5;
     if (tmem_a) ensure_transposed(r, s);
     ws.b2.resize(pieces * kp * r_pad);
     ws.part.resize((int64_t)splits * kp * n_pad);
@@ -1645,7 +1751,7 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     {
         prof::Scope ps("mixed_prep_samples_operand", s, 0.0, 8.0 * R * k + pieces * kp * r_pad);
         dim3 g((unsigned)nrb, (unsigned)kp);
-        if (tmem_a) {
+        if (six) {
             ws.max_wmu.resize(k);
             CS_CUDA(cudaMemsetAsync(ws.max_wmu.get(), 0, 8 * k, s));
             k_col_absmax_mu<<<dim3((unsigned)nrb, (unsigned)k), 256, 0, s>>>(Wt, R, r.mu.get(),
@@ -1655,8 +1761,8 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
                                                         ws.inv_f.get(), ws.colpart.get());
         } else {
             k_split_samples_operand<<<g, 256, 0, s>>>(Wt, R, k, kp, r_pad, r.mu.get(), r.resid.get(),
-                                                      ws.max_w.get(), ws.b2.get(), ws.inv_f.get(),
-                                                      ws.colpart.get());
+                                                      ws.max_w.get(), tmem_a ? 1 : 0, ws.b2.get(),
+                                                      ws.inv_f.get(), ws.colpart.get());
         }
         k_sum_partials<<<(unsigned)((k + 7) / 8), 256, 0, s>>>(ws.colpart.get(), nrb, k, 1.0, ws.c0.get());
         CS_LAUNCH("mixed samples operand");
@@ -1671,14 +1777,19 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     P.kc_last = tl.kc_last;
     P.kp = (int)kp;
     P.lut = r.lut.get();
+    P.qperm = r.qperm.get();
     P.inv_f = ws.inv_f.get();
     P.part = ws.part.get();
     P.ld = n_pad;
     P.status = ws.status.get();
+    P.poll_ns = poll_sleep_ns();
+    P.poll_dec_ns = poll_dec_sleep_ns();
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));
-        if (pairs && tmem_a)
+        if (pairs && plan.tmem_a == 5)
+            launch_pass<false, true, false, 5>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
+        else if (pairs && tmem_a)
             launch_pass<false, true, false, 4>(r.tm_t, ws.tm_b2, ws.tm_b2t, P, s);
         else if (pairs)
             launch_pass<false, true>(r.tm, ws.tm_b2, ws.tm_b2t, P, s);
@@ -1712,17 +1823,16 @@ void rows_pass(MixedRows& r, MixedWorkspace& ws, const double* X, int64_t ldx, i
 }
 
 void samples_pass(MixedRows& r, MixedWorkspace& ws, const double* Wt, int64_t k, double inv_m,
-                  double* Y, int64_t ldy, cudaStream_t s, bool allow_tune,
-                  bool width_independent = false) {
+                  double* Y, int64_t ldy, cudaStream_t s, bool allow_tune, bool sample_major_copy) {
     const int64_t tiles = r.n_pad / kTile;
     const int kb = (int)(r.r_pad / kKBlock);
-    PassPlan plan = choose_plan(false, allow_tune && !width_independent, r.R, r.n, k, tiles, kb, s,
+    PassPlan plan = choose_plan(false, allow_tune && sample_major_copy, r.R, r.n, k, tiles, kb, s,
                                 [&](const PassPlan& p) {
                                     samples_pass_plan(p, r, ws, Wt, k, inv_m, Y, ldy, s);
                                 });
-    if (width_independent && plan.tmem_a) {
-        // the five-set form at every width: A in shared memory (narrow up to 32 columns,
-        // otherwise the general layouts); the slice count stays the default plan's
+    if (!sample_major_copy && plan.tmem_a) {
+        // A in shared memory (narrow up to 32 columns, otherwise the general layouts): the same
+        // int32 sums without the copy; the slice count stays the default plan's
         plan.tmem_a = 0;
         if (plan.max_w > kNarrowSamplesW) {
             plan.narrow = false;
@@ -1762,7 +1872,7 @@ void kinship_apply_mixed(cs_kinship* op, const double* X, int64_t ldx, int64_t k
     m->last_k = 0;
     rows_pass(m->rows, m->ws, X, ldx, k, m->ws.W.get(), R, true, 2, true, s, op->autotune);
     samples_pass(m->rows, m->ws, m->ws.W.get(), k, 1.0 / (double)op->num_variants, Y, ldy, s,
-                 op->autotune, op->width_independent);
+                 op->autotune, op->sample_major_copy);
     check_status(m->ws, s);
     m->last_k = k;
 }
@@ -1817,7 +1927,7 @@ void mixed_multiply_z(cs_kinship* op, const double* Wcol, int64_t k, double* Y, 
         k_col_absmax<<<g, 256, 0, s>>>(Wcol, R, k, ws.max_w.get());
         CS_LAUNCH("col_absmax");
     }
-    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune, op->width_independent);
+    samples_pass(m->rows, ws, Wcol, k, 1.0, Y, ldy, s, op->autotune, op->sample_major_copy);
     check_status(ws, s);
 }
 
@@ -1836,7 +1946,8 @@ std::string autotune_json() {
                       first ? "" : ", ", kv.first.rows ? "rows" : "samples", (long long)e.R,
                       (long long)e.n, (long long)e.k, e.plan.pairs ? "true" : "false",
                       e.plan.narrow ? "true" : "false",
-                      e.plan.tmem_a >= 3 ? "\"pair64\"" : e.plan.tmem_a == 2 ? "64" : e.plan.tmem_a ? "32" : "false",
+                      e.plan.tmem_a == 5 ? "\"pair64_five\"" : e.plan.tmem_a >= 3 ? "\"pair64\""
+                      : e.plan.tmem_a == 2 ? "64" : e.plan.tmem_a ? "32" : "false",
                       e.plan.max_w,
                       e.plan.splits, e.candidates,
                       e.ms_best, e.ms_default);

@@ -304,7 +304,9 @@ void cs_server::run_request(Request* r) {
                                          variants.empty() ? nullptr : variants.data(),
                                          (int64_t)variants.size()));
             sub->autotune = false;  // per-request shapes: the default plans, no tuning passes
-            sub->width_independent = true;  // same result alone and in a stack
+            // the five-set form at every width (same result alone and in a stack), and no
+            // sample-major copy (memory the admission budget does not count)
+            sub->sample_major_copy = false;
             cs_kinship* so = sub.get();
             const int prec = opt.precision;
             target.apply = [so, prec](const double* X, int64_t ldx, int64_t k, double* Y,
@@ -408,7 +410,9 @@ cs_server* server_create(const cs_genotypes* g, const int32_t* variants, int64_t
         sv->g = g;
         sv->op = kinship_create(g, nullptr, 0, variants, n_var);
         sv->op->autotune = false;  // stacked widths vary from apply to apply
-        sv->op->width_independent = true;  // same result alone and in a stack
+        // the five-set form at every width (same result alone and in a stack), and no second
+        // resident copy of the matrix
+        sv->op->sample_major_copy = false;
         if (variants && n_var > 0) sv->variants.assign(variants, variants + n_var);
         if (sv->opt.memory_budget_gb > 0.0) {
             sv->budget_bytes = (int64_t)(sv->opt.memory_budget_gb * 1e9);

@@ -65,6 +65,14 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
         : "memory");
 }
+// Plain bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global
+// into this CTA's shared memory, completing on `bar` like a tensor load.
+__device__ __forceinline__ void bulk_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
 __device__ __forceinline__ void prefetch_tensormap(const CUtensorMap* map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
@@ -307,6 +315,20 @@ __device__ __forceinline__ bool mbar_poll(uint64_t* bar, uint32_t parity, int* s
                                           uint32_t limit = (1u << 26)) {
     for (uint32_t i = 0; i < limit; ++i) {
         if (mbar_test_wait(bar, parity)) return true;
+        if ((i & 1023u) == 1023u && *(volatile int*)status != kOk) return false;
+    }
+    atomicCAS(status, kOk, code);
+    return false;
+}
+// Bounded polls with a pause of `ns` nanoseconds between them, for waits that are long and
+// not on the critical path (an accumulator that fills once per work unit, a producer far
+// ahead of its consumer): a warp spinning without pause takes issue slots from the warps that
+// share its scheduler.
+__device__ __forceinline__ bool mbar_poll_sleep(uint64_t* bar, uint32_t parity, int* status, int code,
+                                                uint32_t ns, uint32_t limit = (1u << 26)) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        if (mbar_test_wait(bar, parity)) return true;
+        if (ns) __nanosleep(ns);
         if ((i & 1023u) == 1023u && *(volatile int*)status != kOk) return false;
     }
     atomicCAS(status, kOk, code);

@@ -137,7 +137,8 @@ def test_lowrank_scan_reuses_sketch_rows(monkeypatch):
     {"CS_B200_TMEM_A": "0", "CS_B200_TMEM_A_PAIRS": "0"},        # A in shared memory
     {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "1"},     # pairs: rows in TMEM only
     {"CS_B200_TMEM_A": "1"},                                     # the 32-wide TMEM form only
-], ids=["single", "pairs", "smem-a", "pairs-rows-tmem", "tmem32"])
+    {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "3"},     # pairs: five-set TMEM samples
+], ids=["single", "pairs", "smem-a", "pairs-rows-tmem", "tmem32", "pairs-five-set-tmem"])
 def test_operator_mixed_forced_cta_mode(mode):
     """Forced plan families (single CTAs or CTA pairs for every width, the A operand in shared
     memory or in tensor memory, five- or six-set samples passes) give the same operator as the
@@ -175,3 +176,40 @@ print(json.dumps(out))
         E = ref.apply_block(X, n_threads=8)
         Y = np.array(forced[str(k)])
         assert colwise_rel(Y, E).max() < 1e-6
+
+
+def test_tensor_memory_forms_bitwise():
+    """The five-set samples pass over the sample-major copy (A in tensor memory, each SNP's
+    imputed code put in along K under the missing-call mask) forms the same int32 sums as the
+    shared-memory form, and so does the rows pass: on CTA pairs with the same K slices the two
+    plan families return the same bits (64- or 80-wide column tiles; k = 16 and 96)."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    code = r'''
+import json, sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import cosmicscanner_b200 as cs
+from cosmicscanner_b200 import synth
+d = synth.cohort(2600, 3000, 23, missing=0.03, n_causal=10)
+g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+op = cs.createKinshipOperator(g)
+out = {}
+for k in (16, 96):
+    X = np.random.default_rng(k).standard_normal((d["n"], k))
+    out[k] = op.apply(X, precision="mixed").tobytes().hex()
+print(json.dumps(out))
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    runs = []
+    for mode in ({"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "3"},
+                 {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "0"}):
+        env = dict(os.environ, CS_B200_AUTOTUNE="0", **mode)
+        res = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True,
+                             text=True, timeout=600)
+        assert res.returncode == 0, res.stderr[-2000:]
+        runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
+    for k in ("16", "96"):
+        assert runs[0][k] == runs[1][k], f"k={k}: tensor-memory and shared-memory forms differ"
