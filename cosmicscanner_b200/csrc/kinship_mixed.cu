@@ -33,7 +33,8 @@
 //
 // Kernel structure (one CTA per SM, 15 warps): warp 14 issues TMA loads of the packed
 // tiles (from HBM) into a deep ring of their own, warp 0 those of the quantised pieces (L2
-// resident) into a ring of stages; warps 2-9 decode; warp 1 issues the MMAs from one thread
+// resident) into a ring of stages; warps 2-9 decode (with A in TMEM as two groups of four
+// that take alternate K-blocks); warp 1 issues the MMAs from one thread
 // into a TMEM accumulator; warps 10-13 drain it (tcgen05.ld) and write FP64 slice partials.
 // The decoded tile (SNP rows x samples) serves as a K-major A operand in the rows pass and
 // as an MN-major A operand in the samples pass.  The TMEMA layouts decode into tensor memory
@@ -222,6 +223,7 @@ struct PassArgs {
     int* status;
     uint32_t poll_ns;            // pairs: pause between polls of the long, off-critical-path waits
     uint32_t poll_dec_ns;        // pairs: pause between the decoders' polls for a free stage
+    int decode_alt;              // TMEMA: two groups of four decoder warps take alternate K-blocks
 };
 
 // 16 codes (one 32-bit word, code j in bits 2j..2j+1) -> 16 int8 imputed codes (byte c of
@@ -290,6 +292,11 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kc = P.kc, kp = P.kp;
     const uint32_t rank = PAIR ? cluster_ctarank() : 0u;
+    // TMEMA: the decoder warps either share every K-block (each its lane quarter and one half of
+    // K) or split into two groups of four that take alternate K-blocks whole, so that two
+    // K-blocks are in decode at once
+    const bool alt = TMEMA != 0 && P.decode_alt != 0;
+    const uint32_t dec_arrivals = alt ? 4u : (uint32_t)kDecodeWarps;
     if (threadIdx.x == 0) {
         for (int s = 0; s < ST; ++s) {
             mbar_init(&full_t[s], 1);
@@ -297,10 +304,10 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         }
         for (int s = 0; s < SP; ++s) {
             mbar_init(&full_p[s], 1);
-            mbar_init(&empty_p[s], kDecodeWarps);
+            mbar_init(&empty_p[s], dec_arrivals);
         }
         for (int d = 0; d < SD; ++d) {
-            mbar_init(&full_d[d], PAIR ? 2 * kDecodeWarps + 1 : kDecodeWarps);
+            mbar_init(&full_d[d], PAIR ? 2 * dec_arrivals + 1 : dec_arrivals);
             mbar_init(&empty_d[d], 1);
         }
         for (int b = 0; b < NB; ++b) {
@@ -533,7 +540,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
         // TMEMA: row 32 (warp % 4) + lane, the TMEM lane quarter this warp may access
         const int dt = threadIdx.x - kDecodeWarp0 * 32;
         const int r = TMEMA ? 32 * (warp & 3) + lane : dt & 127;
-        const int h = TMEMA ? (warp - kDecodeWarp0) >> 2 : dt >> 7;
+        const int h = TMEMA ? (warp - kDecodeWarp0) >> 2 : dt >> 7;  // alt: the warp's group
         const int rbase = (r >> 3) * 1024 + (r & 7) * 128;
         uint32_t j = 0;
         bool ok = true;
@@ -546,6 +553,7 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
             // packed tile (TMEMA = 5)
             uint32_t lut = ROWS ? __ldg(P.lut + (int64_t)tile * kTile + r) : 0x00010002u;
             for (int kb = kb0; kb < kb1; ++kb, ++j) {
+                if (alt && (int)(j & 1u) != h) continue;  // the other group's K-block
                 const int sp = j % SP, d = j % SD;
                 if (!KMAJOR) lut = __ldg(P.lut + (int64_t)kb * kKBlock + r);
                 if (!(ok = PAIR ? mbar_poll_sleep(&empty_d[d], ((j / SD) & 1) ^ 1, P.status,
@@ -553,36 +561,46 @@ k_mixed_pass(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ C
                                 : mbar_wait(&empty_d[d], ((j / SD) & 1) ^ 1, P.status, kTimeoutDecode)))
                     break;
                 if (!(ok = mbar_wait(&full_p[sp], (j / SP) & 1, P.status, kTimeoutDecode))) break;
-                const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
-                const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
-                // imputed codes of the 64 SNPs this thread decodes (the same for every lane of
-                // the warp: shared-memory broadcasts)
-                uint4 qv[4];
-                if constexpr (TMEMA == 5) {
-#pragma unroll
-                    for (int cj = 0; cj < 4; ++cj)
-                        qv[cj] = *reinterpret_cast<const uint4*>(smem + L::q(sp) + h * 64 + cj * 16);
-                }
                 if constexpr (TMEMA) {
-                    // 64 K elements of this lane = 16 TMEM columns of each tile
-                    uint32_t ev[16], mv[16];
-#pragma unroll
-                    for (int cj = 0; cj < 4; ++cj) {
-                        uint4 dos, mis;
-                        if constexpr (TMEMA == 5)
-                            decode_word_imputed(words[cj], qv[cj], dos, mis);
-                        else
-                            decode_word_interleaved(words[cj], lut, dos, mis);
-                        ev[4 * cj] = dos.x; ev[4 * cj + 1] = dos.y; ev[4 * cj + 2] = dos.z; ev[4 * cj + 3] = dos.w;
-                        mv[4 * cj] = mis.x; mv[4 * cj + 1] = mis.y; mv[4 * cj + 2] = mis.z; mv[4 * cj + 3] = mis.w;
-                    }
                     tc_fence_after();  // after the MMA's release of this stage (empty_d)
-                    const uint32_t lane_base = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + 16 * h;
-                    tmem_st16(lane_base + L::ta(d), ev);
-                    tmem_st16(lane_base + L::tam(d), mv);
+                    // one K half of this lane: 64 K elements = 16 TMEM columns of each tile
+                    auto decode_half = [&](int hq) {
+                        const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + hq * 16);
+                        const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
+                        // imputed codes of these 64 SNPs (the same for every lane of the warp:
+                        // shared-memory broadcasts)
+                        uint4 qv[4];
+                        if constexpr (TMEMA == 5) {
+#pragma unroll
+                            for (int cj = 0; cj < 4; ++cj)
+                                qv[cj] = *reinterpret_cast<const uint4*>(smem + L::q(sp) + hq * 64 + cj * 16);
+                        }
+                        uint32_t ev[16], mv[16];
+#pragma unroll
+                        for (int cj = 0; cj < 4; ++cj) {
+                            uint4 dos, mis;
+                            if constexpr (TMEMA == 5)
+                                decode_word_imputed(words[cj], qv[cj], dos, mis);
+                            else
+                                decode_word_interleaved(words[cj], lut, dos, mis);
+                            ev[4 * cj] = dos.x; ev[4 * cj + 1] = dos.y; ev[4 * cj + 2] = dos.z; ev[4 * cj + 3] = dos.w;
+                            mv[4 * cj] = mis.x; mv[4 * cj + 1] = mis.y; mv[4 * cj + 2] = mis.z; mv[4 * cj + 3] = mis.w;
+                        }
+                        const uint32_t lane_base = tmem_base + ((uint32_t)(32 * (warp & 3)) << 16) + 16 * hq;
+                        tmem_st16(lane_base + L::ta(d), ev);
+                        tmem_st16(lane_base + L::tam(d), mv);
+                    };
+                    if (alt) {  // both halves of the K-block (this group's K-blocks only)
+                        decode_half(0);
+                        decode_half(1);
+                    } else {
+                        decode_half(h);
+                    }
                     tmem_wait_st();
                     tc_fence_before();
                 } else {
+                    const uint4 packed = *reinterpret_cast<const uint4*>(smem + L::p(sp) + r * 32 + h * 16);
+                    const uint32_t words[4] = {packed.x, packed.y, packed.z, packed.w};
                     unsigned char* a = smem + L::a(d);
                     unsigned char* am = smem + L::am(d);
 #pragma unroll
@@ -1178,6 +1196,20 @@ uint32_t poll_dec_sleep_ns() {
     static const uint32_t ns = env_ns("CS_B200_POLL_SLEEP_DEC_NS", 32u);
     return ns;
 }
+// Passes with A in TMEM: the decoder warps in two groups of four taking alternate K-blocks
+// whole (default), or all eight on every K-block, each one half of K for its lane quarter
+// (CS_B200_DECODE_ALT=0).  With one K-block per warp at a time, a K-block's decode latency
+// (the packed-tile read, the byte permutes, two tcgen05.st and their wait) set the pace of the
+// TMEM passes; two groups keep two K-blocks in decode.  Measured at N=50k, M=100k, rows /
+// samples per pass (ms), alternate vs shared, same box: k=16 0.70 / 0.73 vs 1.00 / 1.07; k=48
+// 0.93 / 1.06 vs 1.01 / 1.09; k=96 1.66 / 1.97 vs 2.09 / 2.25; k=266 4.23 / 5.06 vs 5.24 / 5.75.
+int decode_alt_mode() {
+    static const int mode = [] {
+        const char* v = std::getenv("CS_B200_DECODE_ALT");
+        return (v && std::strcmp(v, "0") == 0) ? 0 : 1;
+    }();
+    return mode;
+}
 bool tmem_a_pairs_default() { return tmem_a_pairs_mode() != 0; }
 // The narrow single-CTA layout for 32 or fewer right-hand sides (CS_B200_NARROW=0: never).
 bool narrow_layouts() {
@@ -1685,6 +1717,7 @@ void rows_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, cons
     P.status = ws.status.get();
     P.poll_ns = poll_sleep_ns();
     P.poll_dec_ns = poll_dec_sleep_ns();
+    P.decode_alt = decode_alt_mode();
     {
         // algorithmic work: 2 n R k flops, one pass over the packed rows
         prof::Scope ps("kinship_rows_tc", s, 2.0 * (double)n * (double)R * (double)k,
@@ -1784,6 +1817,7 @@ void samples_pass_plan(const PassPlan& plan, MixedRows& r, MixedWorkspace& ws, c
     P.status = ws.status.get();
     P.poll_ns = poll_sleep_ns();
     P.poll_dec_ns = poll_dec_sleep_ns();
+    P.decode_alt = decode_alt_mode();
     {
         prof::Scope ps("kinship_samples_tc", s, 2.0 * (double)n * (double)R * (double)k,
                        (double)R * (double)((n + 3) / 4));

@@ -138,7 +138,10 @@ def test_lowrank_scan_reuses_sketch_rows(monkeypatch):
     {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "1"},     # pairs: rows in TMEM only
     {"CS_B200_TMEM_A": "1"},                                     # the 32-wide TMEM form only
     {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "3"},     # pairs: five-set TMEM samples
-], ids=["single", "pairs", "smem-a", "pairs-rows-tmem", "tmem32", "pairs-five-set-tmem"])
+    {"CS_B200_DECODE_ALT": "0"},                                 # all decoders on every K-block
+    {"CS_B200_DECODE_ALT": "1"},                                 # decoder groups alternate
+], ids=["single", "pairs", "smem-a", "pairs-rows-tmem", "tmem32", "pairs-five-set-tmem",
+        "decode-shared", "decode-alternate"])
 def test_operator_mixed_forced_cta_mode(mode):
     """Forced plan families (single CTAs or CTA pairs for every width, the A operand in shared
     memory or in tensor memory, five- or six-set samples passes) give the same operator as the
@@ -213,3 +216,39 @@ print(json.dumps(out))
         runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
     for k in ("16", "96"):
         assert runs[0][k] == runs[1][k], f"k={k}: tensor-memory and shared-memory forms differ"
+
+
+def test_decoder_groups_bitwise():
+    """Whether the decoder warps share every K-block or split into two groups that take
+    alternate K-blocks changes only who writes which part of the tensor-memory tiles, so the
+    applies are bitwise equal (narrow and 64-wide single-CTA plans, CTA pairs in both forms)."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    code = r'''
+import json, sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import cosmicscanner_b200 as cs
+from cosmicscanner_b200 import synth
+d = synth.cohort(2600, 3000, 29, missing=0.02, n_causal=10)
+g = cs.Genotypes.from_bed_bytes(d["bed"], d["n"], d["m"])
+op = cs.createKinshipOperator(g)
+out = {}
+for k in (16, 48, 96):
+    X = np.random.default_rng(k).standard_normal((d["n"], k))
+    out[k] = op.apply(X, precision="mixed").tobytes().hex()
+print(json.dumps(out))
+'''
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for extra in ({}, {"CS_B200_CTA_PAIRS": "1", "CS_B200_TMEM_A_PAIRS": "3"}):
+        runs = []
+        for alt in ("0", "1"):
+            env = dict(os.environ, CS_B200_AUTOTUNE="0", CS_B200_DECODE_ALT=alt, **extra)
+            res = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True,
+                                 text=True, timeout=600)
+            assert res.returncode == 0, res.stderr[-2000:]
+            runs.append(json.loads(res.stdout.strip().splitlines()[-1]))
+        for k in ("16", "48", "96"):
+            assert runs[0][k] == runs[1][k], f"k={k} {extra}: decoder groups changed the result"
