@@ -1182,11 +1182,13 @@ int tmem_a_pairs_mode() {
 // from the decoders and the MMA thread on its scheduler.  Measured per pass (rows / samples)
 // at N=50k, M=100k, k=266 against no pauses: 4.46 / 5.24 vs 4.76-4.91 / 5.48-5.63 ms; k=96
 // 1.67 / 1.88 vs 1.82 / 2.02; 512 ns pauses are slower than none.
+// At most 1 us: a wait gives up after 2^26 polls, so the pause sets how long a stalled pass
+// takes to report its timeout (about 12 s at the 128 ns default, 70 s at the cap).
 uint32_t env_ns(const char* name, uint32_t def) {
     const char* v = std::getenv(name);
     if (!v || !*v) return def;
     const long x = std::strtol(v, nullptr, 10);
-    return (uint32_t)std::max(0L, std::min(x, 100000L));
+    return (uint32_t)std::max(0L, std::min(x, 1000L));
 }
 uint32_t poll_sleep_ns() {
     static const uint32_t ns = env_ns("CS_B200_POLL_SLEEP_NS", 128u);
